@@ -1,0 +1,303 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 spin-update hot path.
+
+Workload (one "step" = one stochastic LLG-Heun step of the whole system):
+FCC 100^3 unit cells (4,000,000 spins), a=0.354 nm, periodic, two materials
+at random 50/50, nearest-neighbour 3x3 tensor exchange (J_AA=J_BB=11.2e-21 J,
+J_AB=5e-21 J) plus the reference's three-site DMI with D=0.1 J, cubic
+anisotropy Kc=1e-24 J/atom, alpha=0.05, dt=1e-16 s, T=300 K, H=0, spins FP32
+SoA with FP64 reductions.  Synthetic, seeded inputs (no dataset is involved).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  value = spin-steps/s over all ranks, timed
+on the device with CUDA events on the library's stream between barriers
+(max over ranks).  N>1 runs one independent system per GPU (weak scaling,
+no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "spin-steps/s on 1 B200 (LLG & MC), batched/adjoint vs plain, % HBM roofline"
+UNIT = "spin-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--L", type=int, default=100, help="FCC cells per side (100 = 4M spins)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=200)
+    return ap.parse_args()
+
+
+def workload_config(L, n_gpus):
+    return {"workload": f"FCC {L}^3 LLG-Heun, tensor exchange + 3-site DMI, 2 materials, cubic Kc, T=300K",
+            "spins_per_gpu": 4 * L ** 3, "lattice": "fcc", "cells": [L, L, L], "a_nm": 0.354,
+            "materials": 2, "exchange": "tensor+DMI (nn, z=12)", "anisotropy": "cubic", "temperature_K": 300.0,
+            "dt_s": 1e-16, "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single GPU",
+            "l2": "inputs larger than L2 (state 96 MB + topology 960 MB per GPU)"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index=0):
+        self.dev = device_index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.dev), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return self.summary()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, nm in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def measured_peak_hbm():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def traffic_from_profiles(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    p = REPO / "profiles" / "ncu_traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get(kernel)
+        except Exception:
+            return None
+    return None
+
+
+def byte_model(z=12, b_J=12, multi_mat=True, dipole=False):
+    """Algorithmic HBM bytes per spin per pass (FP32 SoA state, int32 index):
+    predictor reads s0 and writes s'; corrector reads s0 and s' and writes s1;
+    each pass streams the neighbour indices, the per-bond DMI vector, the
+    material id and (with the dipole field) the cell id; neighbour spins are
+    L2-served; noise is regenerated in-register (0 B)."""
+    gather = 4 * (z + 1) + b_J * z + 4 * int(multi_mat) + 4 * int(dipole)
+    return {"predictor": 24 + gather, "corrector": 36 + gather}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import cpu_baseline as B
+    cfg = workload_config(args.L, args.gpus)
+    procs = os.cpu_count() or 1
+    steps = max(10, min(args.steps, 100))
+    try:
+        r = B.reference_rate(L=20, steps=steps, procs=procs)
+    except Exception as e:  # binary absent: fall back to the restatement
+        try:
+            r = B.port_rate(L=16, steps=20)
+        except Exception as e2:
+            print(json.dumps({"impl": "reference", "unavailable": f"{e}; {e2}"}))
+            return
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 0, "steps": steps,
+            "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg, "impl": "reference",
+            "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                             "sample": r["sample"]},
+            "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    from vampire_b200 import build as vbuild
+    from vampire_b200 import system as S
+    from vampire_b200 import vgpu
+    vbuild.build()
+    torch.cuda.set_device(local)
+    sysm = S.config_fcc_tensor(L=args.L, seed=2024 + rank)
+    sim = vgpu.Simulation(sysm, device=local, precision="fp32", noise_seed=1000 + rank)
+    mask_id = sim.add_mask(*sysm.masks["system"])
+    stream = torch.cuda.ExternalStream(sim.stream_ptr(), device=local)
+
+    # warm-up
+    sim.llg_heun(args.warmup)
+    sim.synchronize()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    sim.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    sim.profile(True)
+    ev0.record(stream)
+    sim.llg_heun(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    sim.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    prof = sim.profile_read()
+    sim.profile(False)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    n = sysm.n
+    value = n * args.steps * world / (ms * 1e-3)
+
+    # --- roofline of the dominant kernel --------------------------------
+    bm = byte_model()
+    kern = max(("predictor", "corrector"), key=lambda k: prof[k]["ms"])
+    avg_ms = prof[kern]["ms"] / max(1, prof[kern]["count"])
+    peak, peak_kind = measured_peak_hbm()
+    achieved = bm[kern] * n / (avg_ms * 1e-3) / 1e9
+    traffic = traffic_from_profiles(kern)
+    step_gbs = (bm["predictor"] + bm["corrector"]) * n * args.steps / (ms * 1e-3) / 1e9
+
+    # --- e2e through the C ABI with host buffers ------------------------
+    e2e = None
+    if not args.no_e2e:
+        import numpy as np
+        host_spins = np.ascontiguousarray(sysm.spins)
+        K = args.e2e_steps
+        barrier()
+        sim.synchronize()
+        t0 = time.perf_counter()
+        sim.set_spins(host_spins)                 # H2D: initial spins from host
+        m_trace = []
+        for _ in range(K):
+            sim.set_params(sysm.params)           # H2D: step parameters (material table)
+            sim.llg_heun(1)
+            sim.stats_update(magnetization=True)
+            m, _, _ = sim.magnetization(mask_id)  # D2H: the step's result
+            m_trace.append(m[3])
+        final = sim.spins()                       # D2H: final spins to host
+        t1 = time.perf_counter()
+        e2e_s = t1 - t0
+        if dist:
+            t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        h2d = (3 * n * 8) / K + 2 * 144
+        d2h = 4 * 8 * 1 + (3 * n * 8) / K
+        e2e = {"value": n * K * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "steps": K,
+               "path": "vgpu_set_spins, then per step vgpu_set_params + vgpu_llg_heun(1) + "
+                       "vgpu_stats_update + vgpu_stats_get_magnetization, then vgpu_get_spins"}
+        assert np.isfinite(final).all()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import cpu_baseline as B
+            cpu = B.best_available(L=20, steps=100, procs=1)
+            cpu.pop("wall_s", None)
+        except Exception as e:
+            cpu = {"value": None, "unavailable": str(e)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args.L, world),
+            "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_spin": bm,
+                         "avg_launch_ms": {k: prof[k]["ms"] / max(1, prof[k]["count"])
+                                           for k in ("predictor", "corrector")},
+                         "step_achieved_gbs": step_gbs},
+            "gpu_launches": prof["kernel_launches"],
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

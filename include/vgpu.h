@@ -1,0 +1,237 @@
+/*
+ * vgpu.h -- C ABI of libvgpu.so, the B200 (sm_100a) spin-update library.
+ *
+ * This is the boundary a VAMPIRE host binds to.  It replaces the body of the
+ * reference's CUDA backend (namespace vcuda, hdr/cuda.hpp:12-43, implemented
+ * in src/cuda/*.cu), which the reference's gpu:: facade (hdr/gpu.hpp:13-58,
+ * src/gpu/*.cpp) dispatches to.  The reference host reads its physics from
+ * globals (atoms::, mp::material, sim::, dipole::, cells::, stats::); the
+ * vcuda shim (vampire_b200/host/vcuda_b200.cpp) marshals those globals into
+ * the plain descriptors below.  No torch or CUDA types appear here: plain
+ * pointers to host memory and sizes only.  The library copies on upload and on
+ * download; the caller owns every host buffer.
+ *
+ * Every function returns an int status: VGPU_OK (0) or a negative VGPU_ERR_*.
+ * vgpu_last_error() gives the message of the last failure on a handle (or the
+ * last failure of a handle-less call when h is NULL).  Calls on one handle
+ * must be serialised by the caller (the reference is single-threaded);
+ * different handles are independent.  No call blocks forever: device-side
+ * waits are bounded and surface as VGPU_ERR_TIMEOUT.
+ */
+#ifndef VGPU_H_
+#define VGPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VGPU_OK            0
+#define VGPU_ERR_ARG      -1  /* invalid argument or descriptor              */
+#define VGPU_ERR_CUDA     -2  /* CUDA runtime error                          */
+#define VGPU_ERR_OOM      -3  /* device allocation failed                    */
+#define VGPU_ERR_TIMEOUT  -4  /* a bounded device-side wait gave up          */
+#define VGPU_ERR_NAN      -5  /* non-finite spin detected                    */
+#define VGPU_ERR_STATE    -6  /* call out of order (e.g. no system uploaded) */
+
+/* exchange representation of the per-bond list, as exchange::internal::exchange_type
+ * (hdr/exchange_types.hpp): isotropic = 0, vectorial = 1, tensorial = 2 */
+#define VGPU_EXCH_ISOTROPIC 0
+#define VGPU_EXCH_VECTORIAL 1
+#define VGPU_EXCH_TENSORIAL 2
+
+/* arithmetic of the device state */
+#define VGPU_PREC_FP32 0      /* production: FP32 state, FP64 reductions       */
+#define VGPU_PREC_FP64 1      /* debug/oracle build: FP64 everywhere           */
+
+/* source of the Gaussian thermal noise */
+#define VGPU_NOISE_PHILOX 0   /* counter-based Philox4x32-10, in-register      */
+#define VGPU_NOISE_REPLAY 1   /* host-supplied 3N values (x|y|z blocks), for    *
+                               * replaying the reference mtrandom stream        */
+
+typedef struct vgpu_ctx* vgpu_handle;
+
+/* Per-material constants, as the reference derives them in
+ * set_derived_parameters (src/main/initialise_variables.cpp:423-432) and
+ * anisotropy::initialize (src/anisotropy/initialize.cpp:60-76). */
+typedef struct {
+   double alpha;                   /* Gilbert damping                                   */
+   double gamma_rel;               /* relative gyromagnetic ratio                       */
+   double mu_s_SI;                 /* moment [J/T]                                      */
+   double one_oneplusalpha_sq;     /* -gamma_rel/(1+alpha^2)                            */
+   double alpha_oneplusalpha_sq;   /* alpha * one_oneplusalpha_sq                       */
+   double H_th_sigma;              /* sqrt(2 alpha kB/(mu_s gamma_rel dt))              */
+   double temperature_rescaling_alpha;
+   double temperature_rescaling_Tc;
+   double ku2;                     /* reduced 2nd-order uniaxial constant Ku/mu_s [T]   */
+   double ku_vector[3];            /* uniaxial easy axis (unit vector)                  */
+   double kc4;                     /* reduced 4th-order cubic constant Kc/mu_s [T]      */
+   double temperature;             /* material temperature (used if local_temperature)  */
+   double applied_field[3];        /* material local applied field [T]                  */
+   int32_t non_magnetic;           /* non-zero: excluded from cell moments              */
+   int32_t pad_;
+} vgpu_material;
+
+/* One spin system: the reference's CSR neighbour list and unrolled exchange
+ * list (src/exchange/initialize.cpp:70-117, unroll_normalised.cpp:37-140). */
+typedef struct {
+   int32_t num_atoms;
+   int32_t num_materials;
+   int32_t exchange_type;          /* VGPU_EXCH_*                                       */
+   int32_t uniaxial_enabled;       /* anisotropy::internal::enable_uniaxial_second_order */
+   int32_t cubic_enabled;          /* anisotropy::internal::enable_cubic_fourth_order    */
+   int32_t pad_;
+   int64_t num_bonds;              /* atoms::total_num_neighbours                       */
+   const int32_t* nl_start;        /* [num_atoms] atoms::neighbour_list_start_index      */
+   const int32_t* nl_end;          /* [num_atoms] atoms::neighbour_list_end_index (incl.)*/
+   const int32_t* nl;              /* [num_bonds] atoms::neighbour_list_array            */
+   const int32_t* nl_type;         /* [num_bonds] interaction id, or NULL = bond index   */
+   int64_t num_exchange;           /* entries in jlist                                   */
+   const double* jlist;            /* [num_exchange * {1,3,9}] J in Tesla (i/v/t list;   *
+                                    * tensors row-major Jij[a][b])                        */
+   const int32_t* type;            /* [num_atoms] material id (atoms::type_array)        */
+   const vgpu_material* materials; /* [num_materials]                                    */
+   const double* sx;               /* [num_atoms] initial spin (unit vectors)            */
+   const double* sy;
+   const double* sz;
+} vgpu_system_desc;
+
+/* Simulation parameters (namespace sim / mp in the reference). */
+typedef struct {
+   double dt;                      /* reduced time step mp::dt = dt_SI * gamma_SI       */
+   double temperature;             /* sim::temperature [K]                              */
+   double H_applied;               /* sim::H_applied [T]                                */
+   double H_vec[3];                /* sim::H_vec                                        */
+   int32_t thermal_enabled;        /* sim::hamiltonian_simulation_flags[3]              */
+   int32_t applied_enabled;        /* sim::hamiltonian_simulation_flags[2]              */
+   int32_t local_temperature;      /* sim::local_temperature                            */
+   int32_t local_applied_field;    /* sim::local_applied_field                          */
+} vgpu_sim_params;
+
+/* ---- life cycle --------------------------------------------------------- */
+
+/* Create a context on CUDA device `device` (-1: current device) with its own
+ * stream.  precision is VGPU_PREC_FP32 or VGPU_PREC_FP64.
+ * Replaces vcuda::initialize device selection (src/cuda/initialize.cu:84-105). */
+int vgpu_create(int device, int precision, vgpu_handle* out);
+
+/* Free every device buffer of the handle.  Replaces vcuda::finalize
+ * (src/cuda/finalize.cu). */
+int vgpu_destroy(vgpu_handle h);
+
+/* Copy the message of the last error into buf (NUL-terminated). */
+int vgpu_last_error(vgpu_handle h, char* buf, size_t n);
+
+/* Library version string, e.g. "vgpu 0.1 sm_100a". */
+const char* vgpu_version(void);
+
+/* ---- system upload ------------------------------------------------------ */
+
+/* Upload atoms, CSR, exchange list, materials and spins.  Re-uploading
+ * replaces the system.  Validates the CSR on the host first (monotone,
+ * 0 <= neighbour < num_atoms) and returns VGPU_ERR_ARG with a message if it
+ * is malformed.  Replaces vcuda::initialize's marshalling of atoms, fields,
+ * materials and topology (src/cuda/initialize.cu:398-515). */
+int vgpu_upload_system(vgpu_handle h, const vgpu_system_desc* desc);
+
+/* Host-only check of a descriptor (no device needed): CSR rows inside
+ * [0, num_bonds), neighbours and interaction ids in range, materials in
+ * range, finite spins.  VGPU_ERR_ARG / VGPU_ERR_NAN with a message for
+ * vgpu_last_error(NULL, ...).  vgpu_upload_system runs the same check. */
+int vgpu_validate_system(const vgpu_system_desc* desc);
+
+/* Set time step, temperature and applied field; may be called between steps. */
+int vgpu_set_params(vgpu_handle h, const vgpu_sim_params* p);
+
+/* ---- spin access -------------------------------------------------------- */
+
+/* Overwrite the device spins from host arrays of num_atoms doubles. */
+int vgpu_set_spins(vgpu_handle h, const double* sx, const double* sy, const double* sz);
+
+/* Copy the device spins to host arrays (num_atoms doubles each).  Replaces
+ * vcuda::transfer_spin_positions_from_gpu_to_cpu and
+ * vcuda::config::synchronise (src/cuda/transfer.cu, src/cuda/config.cu:25-34). */
+int vgpu_get_spins(vgpu_handle h, double* sx, double* sy, double* sz);
+
+/* ---- LLG-Heun ----------------------------------------------------------- */
+
+/* Noise source.  VGPU_NOISE_PHILOX with a 64-bit seed (the default, seed 0),
+ * or VGPU_NOISE_REPLAY: the next step uses the 3*num_atoms values last given
+ * to vgpu_set_noise_replay (x block, then y, then z: the order of
+ * calculate_thermal_fields, src/simulate/fields.cpp:274-276). */
+int vgpu_set_noise(vgpu_handle h, int mode, uint64_t seed);
+int vgpu_set_noise_replay(vgpu_handle h, const double* xi);
+
+/* Step counter that keys the Philox stream (counter = (atom, step)).  Resume
+ * from a checkpoint by restoring it. */
+int vgpu_set_step(vgpu_handle h, uint64_t step);
+int vgpu_get_step(vgpu_handle h, uint64_t* step);
+
+/* Advance n_steps stochastic Heun steps (src/simulate/LLGHeun.cpp:160-282):
+ * one fused predictor and one fused corrector launch per step.  Replaces
+ * vcuda::llg_heun (src/cuda/llg_heun.cu:32-42,121-208). */
+int vgpu_llg_heun(vgpu_handle h, uint64_t n_steps);
+
+/* Write the 3*num_atoms Gaussians (x|y|z blocks) that the Philox stream
+ * gives the thermal field at step `step` -- the values the fused kernels
+ * regenerate in-register.  For tests and for replaying a run elsewhere. */
+int vgpu_thermal_noise(vgpu_handle h, uint64_t step, double* xi);
+
+/* Total (spin + external) field the predictor sees at the current spins, in
+ * Tesla, with thermal noise excluded (debug/parity aid). */
+int vgpu_get_fields(vgpu_handle h, double* hx, double* hy, double* hz);
+
+/* ---- statistics (masked reductions, FP64) -------------------------------- */
+
+/* Register a statistics mask: mask[i] in [0, mask_size) is the bin of atom i
+ * (the masks of magnetization_statistic_t::set_mask /
+ * energy_statistic_t::set_mask, src/statistics/magnetization.cpp:54-116).
+ * Returns its id.  Replaces the mask upload of vcuda::initialize
+ * (src/cuda/initialize.cu:533-588). */
+int vgpu_stats_add_mask(vgpu_handle h, const int32_t* mask, int32_t mask_size, int32_t* id_out);
+
+/* Compute every registered mask on the device and add to the running means.
+ * flags: bit 0 magnetisation (magnetization.cpp:134-180), bit 1 energy
+ * (statistics/energy.cpp:141-258).  Replaces vcuda::stats::update
+ * (src/cuda/statistics.cu:30-78), which computed magnetisation only. */
+int vgpu_stats_update(vgpu_handle h, int32_t flags);
+
+/* Magnetisation of mask `id`: m[4*bin + {0,1,2,3}] = (m_hat_x, m_hat_y,
+ * m_hat_z, |m|/m_sat), empty bins zero; mean = running sum of those; counter =
+ * number of updates summed.  Either output may be NULL.  Replaces
+ * vcuda::stats::get (src/cuda/statistics.cu:252-284). */
+int vgpu_stats_get_magnetization(vgpu_handle h, int32_t id, double* m, double* mean, int64_t* counter);
+
+/* Energies of mask `id` in Tesla*muB: e[k*mask_size + bin], k = total,
+ * exchange, anisotropy, applied, magnetostatic (exchange and magnetostatic
+ * halved for the double sum); mean likewise. */
+int vgpu_stats_get_energy(vgpu_handle h, int32_t id, double* e, double* mean, int64_t* counter);
+
+/* Zero the running means and counters.  Replaces vcuda::stats::reset. */
+int vgpu_stats_reset(vgpu_handle h);
+
+/* ---- streams, timing ----------------------------------------------------- */
+
+/* The cudaStream_t (as void*) every call of this handle runs on. */
+int vgpu_get_stream(vgpu_handle h, void** stream);
+
+/* Wait for the handle's stream; reports VGPU_ERR_NAN if a pass flagged a
+ * non-finite spin since the last check. */
+int vgpu_synchronize(vgpu_handle h);
+
+/* enable != 0: time every launch with CUDA events on the handle's stream
+ * (resets the accumulators and the kernel-launch counter). */
+int vgpu_profile(vgpu_handle h, int enable);
+
+/* Accumulated device milliseconds and launch counts per kind
+ * (0 predictor, 1 corrector, 2 statistics, 3 dipole, 4 Monte Carlo, 5 other)
+ * and the number of kernels launched since vgpu_profile(). */
+int vgpu_profile_read(vgpu_handle h, double* ms, int64_t* count, int32_t n_kinds, int64_t* kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VGPU_H_ */

@@ -1,0 +1,237 @@
+"""Oracle access for tests, smoke() and the CPU baseline of bench.py.
+
+TEST INFRASTRUCTURE ONLY.  Two checkers live here:
+
+* ``liboracle.so`` -- oracle/vref.c, the FP64 CPU restatement of the
+  reference spin update (compiled with gcc on first use, or by
+  ``__graft_entry__.build()``);
+* ``vampire-harness`` -- the reference program's own objects driven by
+  oracle/harness.cpp (built by oracle/build_ref.py where the reference tree
+  is present).  Fixtures it produced are committed under tests/golden/.
+
+The product (vampire_b200) never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent
+LIB_PATH = HERE / "liboracle.so"
+HARNESS = HERE / "_ref" / "vampire-harness"
+SERIAL = HERE / "_ref" / "vampire-serial"
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+
+
+class VRefSys(C.Structure):
+    _fields_ = [
+        ("n", C.c_int), ("nmat", C.c_int), ("exch_type", C.c_int),
+        ("uniaxial", C.c_int), ("cubic", C.c_int), ("thermal", C.c_int), ("applied", C.c_int),
+        ("pad_", C.c_int),
+        ("start", _I), ("end", _I), ("nl", _I), ("nltype", _I), ("jlist", _D), ("type", _I),
+        ("A", _D), ("B", _D), ("sigma", _D), ("ku2", _D), ("kux", _D), ("kuy", _D), ("kuz", _D),
+        ("kc4", _D), ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double), ("hloc", _D),
+        ("hdx", _D), ("hdy", _D), ("hdz", _D), ("hmx", _D), ("hmy", _D), ("hmz", _D),
+        ("dt", C.c_double), ("half_dt", C.c_double), ("H_applied", C.c_double),
+        ("H_vec", C.c_double * 3),
+    ]
+
+
+def build_lib(force: bool = False) -> Path:
+    src = HERE / "vref.c"
+    if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < src.stat().st_mtime:
+        cmd = ["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", str(LIB_PATH), str(src), "-lm"]
+        subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build_lib()
+        _lib = C.CDLL(str(LIB_PATH))
+        for name in ("vref_spin_fields", "vref_external_fields", "vref_llg_heun", "vref_magnetization",
+                     "vref_energy", "vref_spin_energy"):
+            getattr(_lib, name).restype = None
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t) if a is not None else C.cast(None, t)
+
+
+class OracleSystem:
+    """A vref_sys view of a vampire_b200.system.SpinSystem (arrays kept alive)."""
+
+    def __init__(self, s, dipole_field=None, demag_field=None):
+        self.s = s
+        m = s.materials
+        p = s.params
+        keep = {}
+
+        def arr(name, a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            keep[name] = a
+            return a
+
+        st = VRefSys()
+        st.n = s.n
+        st.nmat = m.size
+        st.exch_type = s.exch_type
+        st.uniaxial = int(s.uniaxial)
+        st.cubic = int(s.cubic)
+        st.thermal = int(p.thermal)
+        st.applied = int(p.applied)
+        st.start = _p(arr("start", s.nl_start, np.int32), _I)
+        st.end = _p(arr("end", s.nl_end, np.int32), _I)
+        st.nl = _p(arr("nl", s.nl, np.int32), _I)
+        st.nltype = _p(arr("nltype", s.nl_type, np.int32), _I) if s.nl_type is not None else _p(None, _I)
+        st.jlist = _p(arr("jlist", s.jlist, np.float64), _D)
+        st.type = _p(arr("type", s.type, np.int32), _I)
+        st.A = _p(arr("A", m["one_oneplusalpha_sq"], np.float64), _D)
+        st.B = _p(arr("B", m["alpha_oneplusalpha_sq"], np.float64), _D)
+        st.sigma = _p(arr("sigma", s.sigma(), np.float64), _D)
+        st.ku2 = _p(arr("ku2", m["ku2"], np.float64), _D)
+        kv = arr("kv", m["ku_vector"], np.float64)
+        st.kux = _p(arr("kux", kv[:, 0], np.float64), _D)
+        st.kuy = _p(arr("kuy", kv[:, 1], np.float64), _D)
+        st.kuz = _p(arr("kuz", kv[:, 2], np.float64), _D)
+        st.kc4 = _p(arr("kc4", m["kc4"], np.float64), _D)
+        hv = np.asarray(p.H_vec, dtype=np.float64)
+        st.hx, st.hy, st.hz = (p.H_vec[0] * p.H_applied, p.H_vec[1] * p.H_applied, p.H_vec[2] * p.H_applied)
+        st.hloc = _p(arr("hloc", m["applied_field"], np.float64), _D) if p.local_applied_field else _p(None, _D)
+        if dipole_field is not None:
+            st.hdx = _p(arr("hdx", dipole_field[0], np.float64), _D)
+            st.hdy = _p(arr("hdy", dipole_field[1], np.float64), _D)
+            st.hdz = _p(arr("hdz", dipole_field[2], np.float64), _D)
+        if demag_field is not None:
+            st.hmx = _p(arr("hmx", demag_field[0], np.float64), _D)
+            st.hmy = _p(arr("hmy", demag_field[1], np.float64), _D)
+            st.hmz = _p(arr("hmz", demag_field[2], np.float64), _D)
+        st.dt = p.dt
+        st.half_dt = 0.5 * p.dt
+        st.H_applied = p.H_applied
+        for k in range(3):
+            st.H_vec[k] = hv[k]
+        self.st = st
+        self.keep = keep
+
+    def llg_heun(self, spins: np.ndarray, n_steps: int, xi: Optional[np.ndarray] = None) -> np.ndarray:
+        s = np.ascontiguousarray(spins, dtype=np.float64).copy()
+        xi_c = np.ascontiguousarray(xi, dtype=np.float64) if xi is not None else None
+        lib().vref_llg_heun(C.byref(self.st), _p(s[0], _D), _p(s[1], _D), _p(s[2], _D),
+                            _p(xi_c, _D), C.c_int64(n_steps))
+        return s
+
+    def spin_fields(self, spins: np.ndarray) -> np.ndarray:
+        s = np.ascontiguousarray(spins, dtype=np.float64)
+        h = np.zeros((3, self.s.n))
+        lib().vref_spin_fields(C.byref(self.st), _p(s[0], _D), _p(s[1], _D), _p(s[2], _D),
+                               _p(h[0], _D), _p(h[1], _D), _p(h[2], _D))
+        return h
+
+    def external_fields(self, xi=None) -> np.ndarray:
+        h = np.zeros((3, self.s.n))
+        xi_c = np.ascontiguousarray(xi, dtype=np.float64) if xi is not None else None
+        lib().vref_external_fields(C.byref(self.st), _p(xi_c, _D), _p(h[0], _D), _p(h[1], _D),
+                                   _p(h[2], _D))
+        return h
+
+    def magnetization(self, spins, mask, size) -> np.ndarray:
+        s = np.ascontiguousarray(spins, dtype=np.float64)
+        mm = np.ascontiguousarray(self.s.mu_s_muB(), dtype=np.float64)
+        mk = np.ascontiguousarray(mask, dtype=np.int32)
+        out = np.zeros(4 * size)
+        lib().vref_magnetization(C.c_int(self.s.n), _p(mk, _I), C.c_int(size), _p(s[0], _D),
+                                 _p(s[1], _D), _p(s[2], _D), _p(mm, _D), _p(out, _D))
+        return out
+
+    def energy(self, spins, mask, size) -> np.ndarray:
+        s = np.ascontiguousarray(spins, dtype=np.float64)
+        mm = np.ascontiguousarray(self.s.mu_s_muB(), dtype=np.float64)
+        mk = np.ascontiguousarray(mask, dtype=np.int32)
+        out = np.zeros(5 * size)
+        lib().vref_energy(C.byref(self.st), _p(mk, _I), C.c_int(size), _p(s[0], _D), _p(s[1], _D),
+                          _p(s[2], _D), _p(mm, _D), _p(out, _D))
+        return out
+
+
+# ----------------------------------------------------------------------------
+# reference harness
+# ----------------------------------------------------------------------------
+
+def harness_available() -> bool:
+    return HARNESS.exists()
+
+
+def load_dump(d: Path) -> dict:
+    out = {}
+    for line in (Path(d) / "manifest.txt").read_text().splitlines():
+        name, dt, cnt = line.split()
+        out[name] = np.fromfile(Path(d) / f"{name}.bin", dtype=dt, count=int(cnt))
+    return out
+
+
+def run_harness(input_text: str, files: dict, args: list, workdir: Optional[str] = None,
+                timeout: float = 600) -> dict:
+    """Write `input` and material files into a scratch directory, run the
+    reference harness there and return its dumped arrays."""
+    if not harness_available():
+        raise RuntimeError("reference harness not built (python oracle/build_ref.py)")
+    tmp = workdir or tempfile.mkdtemp(prefix="vref_")
+    Path(tmp, "input").write_text(input_text)
+    for name, text in files.items():
+        Path(tmp, name).write_text(text)
+    out = Path(tmp, "out")
+    out.mkdir(exist_ok=True)
+    r = subprocess.run([str(HARNESS), "--out", str(out)] + [str(a) for a in args], cwd=tmp,
+                       capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"harness failed rc={r.returncode}: {r.stdout[-2000:]} {r.stderr[-2000:]}")
+    return load_dump(out)
+
+
+def system_from_dump(d: dict, params=None):
+    """Build a SpinSystem from a reference dump (harness --system)."""
+    from vampire_b200 import system as S
+    meta = d["meta"]
+    n, nnz, nmat, et, uni, cub = [int(x) for x in meta[:6]]
+    m16 = d["materials"].reshape(nmat, 16)
+    mats = np.zeros(nmat, dtype=S.MATERIAL_DTYPE)
+    for i in range(nmat):
+        mats[i]["alpha"], mats[i]["gamma_rel"], mats[i]["mu_s_SI"] = m16[i, 0:3]
+        mats[i]["one_oneplusalpha_sq"], mats[i]["alpha_oneplusalpha_sq"], mats[i]["H_th_sigma"] = m16[i, 3:6]
+        mats[i]["temperature_rescaling_alpha"], mats[i]["temperature_rescaling_Tc"] = m16[i, 6:8]
+        mats[i]["ku2"] = m16[i, 8]
+        mats[i]["ku_vector"] = m16[i, 9:12]
+        mats[i]["kc4"] = m16[i, 12]
+        mats[i]["non_magnetic"] = int(m16[i, 13])
+    simc = d["sim"]
+    if params is None:
+        params = S.SimParams(dt_SI=simc[2], gamma_SI=simc[3], temperature=simc[4], H_applied=simc[5],
+                             H_vec=tuple(simc[6:9]), thermal=bool(meta[8]), applied=bool(meta[9]))
+    spins = np.stack([d["sx_0"], d["sy_0"], d["sz_0"]])
+    s = S.SpinSystem(n=n, nl_start=d["nl_start"].astype(np.int32), nl_end=d["nl_end"].astype(np.int32),
+                     nl=d["nl"].astype(np.int32), jlist=d["jlist"], exch_type=et,
+                     type=d["type"].astype(np.int32), materials=mats, spins=spins, params=params,
+                     uniaxial=bool(uni), cubic=bool(cub),
+                     coords=np.stack([d["cx"], d["cy"], d["cz"]]))
+    nt = d["nl_type"].astype(np.int32)
+    if not np.array_equal(nt, np.arange(nt.size, dtype=np.int32)):
+        s.nl_type = nt
+    if "mask_system" in d:
+        s.masks["system"] = (d["mask_system"].astype(np.int32), int(d["sat_system"].size))
+        s.masks["material"] = (d["mask_material"].astype(np.int32), int(d["sat_material"].size))
+    return s

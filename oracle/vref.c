@@ -1,0 +1,281 @@
+/*
+ * vref.c -- FP64 CPU restatement of the reference VAMPIRE spin-update path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker that the CUDA path in vampire_b200 is
+ * compared with.  Nothing in the product links or calls it.  It is pinned
+ * against the reference itself: tests/golden/ holds fixtures produced by the
+ * reference program (oracle/_ref/vampire-harness, reference objects built by
+ * oracle/build_ref.py) and tests/test_oracle_pinned.py checks this file
+ * against them.
+ *
+ * Each function follows the reference file:line cited beside it, with the
+ * same operation order so that FP64 results agree to rounding.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "vref.h"
+
+/* exchange::internal::exchange_fields (src/exchange/exchange_fields.cpp:29-168):
+ * H_i += sum_j J_ij s_j over the CSR row [start, end] (end inclusive). */
+static void exchange_fields(const vref_sys* s, const double* sx, const double* sy, const double* sz,
+                            double* hx, double* hy, double* hz) {
+   for (int atom = 0; atom < s->n; ++atom) {
+      double fx = 0.0, fy = 0.0, fz = 0.0;
+      const int start = s->start[atom];
+      const int end = s->end[atom] + 1;
+      for (int nn = start; nn < end; ++nn) {
+         const int natom = s->nl[nn];
+         const int iid = s->nltype ? s->nltype[nn] : nn;
+         if (s->exch_type == 0) {
+            const double J = s->jlist[iid];
+            fx += J * sx[natom];
+            fy += J * sy[natom];
+            fz += J * sz[natom];
+         } else if (s->exch_type == 1) {
+            const double* J = s->jlist + 3 * (int64_t)iid;
+            fx += J[0] * sx[natom];
+            fy += J[1] * sy[natom];
+            fz += J[2] * sz[natom];
+         } else {
+            const double* J = s->jlist + 9 * (int64_t)iid;
+            const double S0 = sx[natom], S1 = sy[natom], S2 = sz[natom];
+            fx += (J[0] * S0 + J[1] * S1 + J[2] * S2);
+            fy += (J[3] * S0 + J[4] * S1 + J[5] * S2);
+            fz += (J[6] * S0 + J[7] * S1 + J[8] * S2);
+         }
+      }
+      hx[atom] += fx;
+      hy[atom] += fy;
+      hz[atom] += fz;
+   }
+}
+
+/* calculate_spin_fields (src/simulate/fields.cpp:67-118): zero, exchange, then
+ * anisotropy::fields -> uniaxial_second_order_fields
+ * (src/anisotropy/uniaxial_second_order.cpp:51-98, H += 2 ku2 (s.e) e) and
+ * cubic_fourth_order_fields (src/anisotropy/cubic_fourth_order.cpp:34-73,
+ * H += 2 kc4 s^3). */
+void vref_spin_fields(const vref_sys* s, const double* sx, const double* sy, const double* sz,
+                      double* hx, double* hy, double* hz) {
+   memset(hx, 0, sizeof(double) * s->n);
+   memset(hy, 0, sizeof(double) * s->n);
+   memset(hz, 0, sizeof(double) * s->n);
+   exchange_fields(s, sx, sy, sz, hx, hy, hz);
+   if (s->uniaxial) {
+      for (int atom = 0; atom < s->n; atom++) {
+         const int mat = s->type[atom];
+         const double ex = s->kux[mat], ey = s->kuy[mat], ez = s->kuz[mat];
+         const double sdote = (sx[atom] * ex + sy[atom] * ey + sz[atom] * ez);
+         const double k2 = 2.0 * s->ku2[mat] * sdote;
+         hx[atom] += ex * k2;
+         hy[atom] += ey * k2;
+         hz[atom] += ez * k2;
+      }
+   }
+   if (s->cubic) {
+      for (int atom = 0; atom < s->n; atom++) {
+         const int mat = s->type[atom];
+         const double k4 = 0.5 * 4.0 * s->kc4[mat];
+         const double x = sx[atom], y = sy[atom], z = sz[atom];
+         hx[atom] += x * x * x * k4;
+         hy[atom] += y * y * y * k4;
+         hz[atom] += z * z * z * k4;
+      }
+   }
+}
+
+/* calculate_external_fields (src/simulate/fields.cpp:120-169): thermal
+ * (246-289: xi * sqrt(T_resc) * H_th_sigma, xi in x|y|z blocks), applied
+ * (171-244: global H plus optional per-material local field) and dipolar
+ * (291-316: per-atom field).  sigma[mat] = sqrt(T_resc) * H_th_sigma. */
+void vref_external_fields(const vref_sys* s, const double* xi, double* hx, double* hy, double* hz) {
+   const int n = s->n;
+   for (int atom = 0; atom < n; atom++) {
+      if (xi && s->thermal) {
+         const double sg = s->sigma[s->type[atom]];
+         hx[atom] = xi[atom] * sg;
+         hy[atom] = xi[n + atom] * sg;
+         hz[atom] = xi[2 * n + atom] * sg;
+      } else {
+         hx[atom] = 0.0; hy[atom] = 0.0; hz[atom] = 0.0;
+      }
+   }
+   if (s->applied) {
+      for (int atom = 0; atom < n; atom++) {
+         double ax = s->hx, ay = s->hy, az = s->hz;
+         if (s->hloc) {
+            const int m = s->type[atom];
+            ax += s->hloc[3 * m + 0]; ay += s->hloc[3 * m + 1]; az += s->hloc[3 * m + 2];
+         }
+         hx[atom] += ax; hy[atom] += ay; hz[atom] += az;
+      }
+   }
+   if (s->hdx) {
+      for (int atom = 0; atom < n; atom++) {
+         hx[atom] += s->hdx[atom]; hy[atom] += s->hdy[atom]; hz[atom] += s->hdz[atom];
+      }
+   }
+}
+
+/* Landau-Lifshitz-Gilbert right-hand side as written in LLGHeun.cpp:201-203. */
+static inline void llg_rhs(double A, double B, const double S[3], const double H[3], double d[3]) {
+   d[0] = A * (S[1] * H[2] - S[2] * H[1]) + B * (S[1] * (S[0] * H[1] - S[1] * H[0]) - S[2] * (S[2] * H[0] - S[0] * H[2]));
+   d[1] = A * (S[2] * H[0] - S[0] * H[2]) + B * (S[2] * (S[1] * H[2] - S[2] * H[1]) - S[0] * (S[0] * H[1] - S[1] * H[0]));
+   d[2] = A * (S[0] * H[1] - S[1] * H[0]) + B * (S[0] * (S[2] * H[0] - S[0] * H[2]) - S[1] * (S[1] * H[2] - S[2] * H[1]));
+}
+
+/* sim::LLG_Heun (src/simulate/LLGHeun.cpp:160-282): one stochastic Heun step.
+ * xi: 3n Gaussians for this step (NULL = no thermal term).  work: 15n doubles. */
+void vref_llg_heun_step(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,
+                        double* work) {
+   const int n = s->n;
+   double* hsx = work;          double* hsy = work + n;      double* hsz = work + 2 * n;
+   double* hex = work + 3 * n;  double* hey = work + 4 * n;  double* hez = work + 5 * n;
+   double* ix = work + 6 * n;   double* iy = work + 7 * n;   double* iz = work + 8 * n;
+   double* ex = work + 9 * n;   double* ey = work + 10 * n;  double* ez = work + 11 * n;
+   double* hux = work + 12 * n; double* huy = work + 13 * n; double* huz = work + 14 * n;
+   memcpy(ix, sx, sizeof(double) * n);
+   memcpy(iy, sy, sizeof(double) * n);
+   memcpy(iz, sz, sizeof(double) * n);
+   vref_spin_fields(s, sx, sy, sz, hsx, hsy, hsz);
+   vref_external_fields(s, xi, hex, hey, hez);
+   for (int atom = 0; atom < n; atom++) {
+      const int m = s->type[atom];
+      const double S[3] = {sx[atom], sy[atom], sz[atom]};
+      const double H[3] = {hsx[atom] + hex[atom], hsy[atom] + hey[atom], hsz[atom] + hez[atom]};
+      double d[3];
+      llg_rhs(s->A[m], s->B[m], S, H, d);
+      ex[atom] = d[0]; ey[atom] = d[1]; ez[atom] = d[2];
+      double Sn[3] = {S[0] + d[0] * s->dt, S[1] + d[1] * s->dt, S[2] + d[2] * s->dt};
+      const double mod = 1.0 / sqrt(Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2]);
+      hux[atom] = Sn[0] * mod; huy[atom] = Sn[1] * mod; huz[atom] = Sn[2] * mod;
+   }
+   memcpy(sx, hux, sizeof(double) * n);
+   memcpy(sy, huy, sizeof(double) * n);
+   memcpy(sz, huz, sizeof(double) * n);
+   vref_spin_fields(s, sx, sy, sz, hsx, hsy, hsz);
+   for (int atom = 0; atom < n; atom++) {
+      const int m = s->type[atom];
+      const double S[3] = {sx[atom], sy[atom], sz[atom]};
+      const double H[3] = {hsx[atom] + hex[atom], hsy[atom] + hey[atom], hsz[atom] + hez[atom]};
+      double d[3];
+      llg_rhs(s->A[m], s->B[m], S, H, d);
+      hux[atom] = d[0]; huy[atom] = d[1]; huz[atom] = d[2];
+   }
+   for (int atom = 0; atom < n; atom++) {
+      double Sn[3] = {ix[atom] + s->half_dt * (ex[atom] + hux[atom]),
+                      iy[atom] + s->half_dt * (ey[atom] + huy[atom]),
+                      iz[atom] + s->half_dt * (ez[atom] + huz[atom])};
+      const double mod = 1.0 / sqrt(Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2]);
+      sx[atom] = Sn[0] * mod; sy[atom] = Sn[1] * mod; sz[atom] = Sn[2] * mod;
+   }
+}
+
+/* n_steps deterministic (T=0 or given-noise) steps; xi may be NULL or hold
+ * n_steps * 3n values. */
+void vref_llg_heun(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,
+                   int64_t n_steps) {
+   double* work = (double*)malloc(sizeof(double) * 15 * (size_t)s->n);
+   for (int64_t t = 0; t < n_steps; t++)
+      vref_llg_heun_step(s, sx, sy, sz, xi ? xi + t * 3 * (int64_t)s->n : NULL, work);
+   free(work);
+}
+
+/* Energies of one spin in Tesla, as sim::calculate_spin_energy
+ * (src/simulate/energy.cpp:147-174): exchange (exchange/energy.cpp:27-140),
+ * anisotropy (uniaxial_second_order.cpp:104-121: -ku2 (s.e)^2;
+ * cubic_fourth_order.cpp:80-95: -kc4/2 sum s^4), applied (-H.s) and
+ * magnetostatic (-Hd.s).  Out: e[0]=exchange, [1]=anisotropy, [2]=applied,
+ * [3]=magnetostatic. */
+void vref_spin_energy(const vref_sys* s, const double* sx, const double* sy, const double* sz,
+                      int atom, double Sx, double Sy, double Sz, double* e) {
+   double ex = 0.0;
+   for (int nn = s->start[atom]; nn <= s->end[atom]; ++nn) {
+      const int natom = s->nl[nn];
+      const int iid = s->nltype ? s->nltype[nn] : nn;
+      if (s->exch_type == 0) {
+         const double J = s->jlist[iid];
+         ex -= J * (sx[natom] * Sx + sy[natom] * Sy + sz[natom] * Sz);
+      } else if (s->exch_type == 1) {
+         const double* J = s->jlist + 3 * (int64_t)iid;
+         ex -= (J[0] * sx[natom] * Sx + J[1] * sy[natom] * Sy + J[2] * sz[natom] * Sz);
+      } else {
+         const double* J = s->jlist + 9 * (int64_t)iid;
+         const double S0 = sx[natom], S1 = sy[natom], S2 = sz[natom];
+         ex -= (J[0] * S0 * Sx + J[1] * S1 * Sx + J[2] * S2 * Sx + J[3] * S0 * Sy + J[4] * S1 * Sy +
+                J[5] * S2 * Sy + J[6] * S0 * Sz + J[7] * S1 * Sz + J[8] * S2 * Sz);
+      }
+   }
+   const int m = s->type[atom];
+   double an = 0.0;
+   if (s->uniaxial) {
+      const double sdote = Sx * s->kux[m] + Sy * s->kuy[m] + Sz * s->kuz[m];
+      an += -s->ku2[m] * (sdote * sdote);
+   }
+   if (s->cubic) {
+      const double sx4 = Sx * Sx * Sx * Sx, sy4 = Sy * Sy * Sy * Sy, sz4 = Sz * Sz * Sz * Sz;
+      an += -0.5 * s->kc4[m] * (sx4 + sy4 + sz4);
+   }
+   e[0] = ex;
+   e[1] = an;
+   e[2] = -s->H_applied * (s->H_vec[0] * Sx + s->H_vec[1] * Sy + s->H_vec[2] * Sz);
+   e[3] = s->hmx ? -(s->hmx[atom] * Sx + s->hmy[atom] * Sy + s->hmz[atom] * Sz) : 0.0;
+}
+
+/* magnetization_statistic_t::calculate_magnetization
+ * (src/statistics/magnetization.cpp:134-180): per mask bin sum(mu s), sum(mu),
+ * normalised to (m_hat, |m|/m_sat); empty bins zeroed.  out: 4*mask_size. */
+void vref_magnetization(int n, const int* mask, int mask_size, const double* sx, const double* sy,
+                        const double* sz, const double* mm, double* out) {
+   memset(out, 0, sizeof(double) * 4 * mask_size);
+   for (int atom = 0; atom < n; ++atom) {
+      const int id = mask[atom];
+      out[4 * id + 0] += sx[atom] * mm[atom];
+      out[4 * id + 1] += sy[atom] * mm[atom];
+      out[4 * id + 2] += sz[atom] * mm[atom];
+      out[4 * id + 3] += mm[atom];
+   }
+   for (int id = 0; id < mask_size; ++id) {
+      const double msat = out[4 * id + 3];
+      const double magm = sqrt(out[4 * id + 0] * out[4 * id + 0] + out[4 * id + 1] * out[4 * id + 1] +
+                               out[4 * id + 2] * out[4 * id + 2]);
+      if (msat == 0.0) {  /* zero_list: empty bins */
+         out[4 * id + 0] = out[4 * id + 1] = out[4 * id + 2] = out[4 * id + 3] = 0.0;
+         continue;
+      }
+      out[4 * id + 0] /= magm;
+      out[4 * id + 1] /= magm;
+      out[4 * id + 2] /= magm;
+      out[4 * id + 3] = magm / msat;
+   }
+}
+
+/* energy_statistic_t::calculate (src/statistics/energy.cpp:141-258): per mask
+ * bin, sums of mu * E over atoms; exchange and magnetostatic halved.
+ * out: 5*mask_size as [total | exchange | anisotropy | applied | magnetostatic]. */
+void vref_energy(const vref_sys* s, const int* mask, int mask_size, const double* sx,
+                 const double* sy, const double* sz, const double* mm, double* out) {
+   double* tot = out;
+   double* exc = out + mask_size;
+   double* ani = out + 2 * mask_size;
+   double* app = out + 3 * mask_size;
+   double* mst = out + 4 * mask_size;
+   memset(out, 0, sizeof(double) * 5 * mask_size);
+   for (int atom = 0; atom < s->n; ++atom) {
+      double e[4];
+      vref_spin_energy(s, sx, sy, sz, atom, sx[atom], sy[atom], sz[atom], e);
+      const int id = mask[atom];
+      exc[id] += e[0] * mm[atom];
+      ani[id] += e[1] * mm[atom];
+      app[id] += e[2] * mm[atom];
+      mst[id] += e[3] * mm[atom];
+   }
+   for (int id = 0; id < mask_size; ++id) {
+      exc[id] *= 0.5;
+      mst[id] *= 0.5;
+      tot[id] = exc[id] + ani[id] + app[id] + mst[id];
+   }
+}

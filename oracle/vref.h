@@ -1,0 +1,57 @@
+/*
+ * vref.h -- FP64 CPU restatement of the reference spin-update path.
+ * TEST INFRASTRUCTURE ONLY (the oracle the CUDA path is checked against).
+ */
+#ifndef VREF_H_
+#define VREF_H_
+#include <stdint.h>
+
+typedef struct {
+   int n;                 /* atoms */
+   int nmat;              /* materials */
+   int exch_type;         /* 0 isotropic, 1 vectorial, 2 tensorial */
+   int uniaxial, cubic;   /* anisotropy terms enabled */
+   int thermal, applied;  /* hamiltonian_simulation_flags[3], [2] */
+   int pad_;
+   const int* start;      /* CSR: neighbour_list_start_index */
+   const int* end;        /* CSR: neighbour_list_end_index (inclusive) */
+   const int* nl;         /* neighbour_list_array */
+   const int* nltype;     /* interaction id per bond, or NULL (= bond index) */
+   const double* jlist;   /* per interaction: 1, 3 or 9 doubles [T] */
+   const int* type;       /* material per atom */
+   const double* A;       /* per material one_oneplusalpha_sq */
+   const double* B;       /* per material alpha_oneplusalpha_sq */
+   const double* sigma;   /* per material sqrt(T_rescaled) * H_th_sigma */
+   const double* ku2;     /* per material reduced uniaxial constant [T] */
+   const double* kux;
+   const double* kuy;
+   const double* kuz;
+   const double* kc4;     /* per material reduced cubic constant [T] */
+   double hx, hy, hz;     /* global applied field H_applied * H_vec [T] */
+   const double* hloc;    /* per material local applied field (3 each) or NULL */
+   const double* hdx;     /* per atom dipolar B field or NULL */
+   const double* hdy;
+   const double* hdz;
+   const double* hmx;     /* per atom mu0 Hd field (magnetostatic energy) or NULL */
+   const double* hmy;
+   const double* hmz;
+   double dt, half_dt;    /* reduced time step */
+   double H_applied;      /* for the applied-field energy */
+   double H_vec[3];
+} vref_sys;
+
+void vref_spin_fields(const vref_sys* s, const double* sx, const double* sy, const double* sz,
+                      double* hx, double* hy, double* hz);
+void vref_external_fields(const vref_sys* s, const double* xi, double* hx, double* hy, double* hz);
+void vref_llg_heun_step(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,
+                        double* work);
+void vref_llg_heun(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,
+                   int64_t n_steps);
+void vref_spin_energy(const vref_sys* s, const double* sx, const double* sy, const double* sz,
+                      int atom, double Sx, double Sy, double Sz, double* e);
+void vref_magnetization(int n, const int* mask, int mask_size, const double* sx, const double* sy,
+                        const double* sz, const double* mm, double* out);
+void vref_energy(const vref_sys* s, const int* mask, int mask_size, const double* sx,
+                 const double* sy, const double* sz, const double* mm, double* out);
+
+#endif

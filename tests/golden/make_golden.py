@@ -1,0 +1,115 @@
+"""Generate the golden fixtures in tests/golden/ from the reference program.
+
+Needs the reference harness (python oracle/build_ref.py, which compiles the
+reference sources in place).  Each fixture is an .npz holding what the
+reference itself built and produced: its CSR neighbour list, unrolled exchange
+list, material constants, initial spins, spins after N of its own
+sim::LLG_Heun() steps, the Gaussian stream it consumed (captured by the
+harness through MTRand get_state/set_state) and its statistics.
+
+    python tests/golden/make_golden.py            # all fixtures
+    python tests/golden/make_golden.py sc10_t300  # one
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent.parent))
+
+from oracle import oracle as O  # noqa: E402
+from oracle.refinputs import SC_MAT, fcc_input, fcc_mat, sc_input  # noqa: E402
+
+
+SYSTEM_KEYS = ["meta", "nl_start", "nl_end", "nl", "nl_type", "type", "m_spin", "cx", "cy", "cz", "jlist",
+               "materials", "sim", "mask_system", "sat_system", "mask_material", "sat_material"]
+
+
+def save(name: str, d: dict, keep: list) -> None:
+    out = {k: d[k] for k in SYSTEM_KEYS if k in d}
+    for k in keep:
+        out[k] = d[k]
+    # per-bond exchange of a regular lattice is highly repetitive; npz-compress everything
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print(f"{name}: {sum(v.nbytes for v in out.values()) / 1e6:.2f} MB raw")
+
+
+def sc20_t0():
+    """Config-0 system (SC 20^3 periodic), T=0: the reference trajectory at
+    steps 1, 100 and 10,000 (deterministic check)."""
+    d = O.run_harness(sc_input(20), {"m.mat": SC_MAT},
+                      ["--system", "--steps", 10000, "--snaps", "1,100,10000", "--stats", "0,10000"])
+    keep = [f"s{c}_{t}" for t in (0, 1, 100, 10000) for c in "xyz"]
+    keep += ["mag_system_0", "energy_system_0", "mag_system_10000", "energy_system_10000",
+             "mag_material_10000", "energy_material_10000"]
+    save("sc20_t0", d, keep)
+
+
+def sc8_t0():
+    """SC 8^3 periodic at T=0: reference spins at many steps (fast checks)."""
+    d = O.run_harness(sc_input(8), {"m.mat": SC_MAT},
+                      ["--system", "--steps", 2000, "--snaps", "1,2,10,100,1000,2000"])
+    keep = [f"s{c}_{t}" for t in (0, 1, 2, 10, 100, 1000, 2000) for c in "xyz"]
+    save("sc8_t0", d, keep)
+
+
+def sc10_t300():
+    """SC 10^3 periodic at T=300 K: one and two replayed stochastic steps."""
+    d = O.run_harness(sc_input(10, T=300.0), {"m.mat": SC_MAT},
+                      ["--system", "--steps", 2, "--snaps", "1,2", "--noise", 2])
+    keep = [f"s{c}_{t}" for t in (0, 1, 2) for c in "xyz"] + ["xi_1", "xi_2"]
+    save("sc10_t300", d, keep)
+
+
+def sc6_open_t300():
+    """SC 6^3 with open boundaries (ragged CSR rows) at T=300 K, replayed noise."""
+    d = O.run_harness(sc_input(6, T=300.0, periodic=False), {"m.mat": SC_MAT},
+                      ["--system", "--steps", 3, "--snaps", "1,3", "--noise", 3, "--stats", "3"])
+    keep = [f"s{c}_{t}" for t in (0, 1, 3) for c in "xyz"] + ["xi_1", "xi_2", "xi_3",
+                                                              "mag_system_3", "energy_system_3"]
+    save("sc6_open_t300", d, keep)
+
+
+def fcc4_dmi_t300():
+    """FCC 4^3 periodic random A/B alloy, nn tensor exchange + three-site DMI +
+    cubic anisotropy, T=300 K: one replayed step, plus stats."""
+    d = O.run_harness(fcc_input(4, T=300.0), {"m.mat": fcc_mat()},
+                      ["--system", "--steps", 2, "--snaps", "1,2", "--noise", 2, "--stats", "0,2"])
+    keep = [f"s{c}_{t}" for t in (0, 1, 2) for c in "xyz"] + ["xi_1", "xi_2", "mag_system_2",
+                                                              "energy_system_2", "mag_material_2",
+                                                              "energy_material_2"]
+    save("fcc4_dmi_t300", d, keep)
+
+
+def fcc4_dmi_t0():
+    """Same FCC alloy at T=0: 200 deterministic steps."""
+    d = O.run_harness(fcc_input(4, T=0.0), {"m.mat": fcc_mat()},
+                      ["--system", "--steps", 200, "--snaps", "1,200"])
+    keep = [f"s{c}_{t}" for t in (0, 1, 200) for c in "xyz"]
+    save("fcc4_dmi_t0", d, keep)
+
+
+def single_spin_applied():
+    """The reference's own known-answer setup (tests/physical/AppliedField):
+    one spin along x, H=10 T along z, alpha=1, T=0, dt=1e-16 s."""
+    inp = ("create:single-spin\nmaterial:file=m.mat\nsim:temperature=0.0\nsim:time-step=1.0E-16\n"
+           "sim:applied-field-strength=10.0 !T\nsim:applied-field-unit-vector=0,0,1\n"
+           "sim:program=time-series\nsim:integrator=llg-heun\n")
+    mat = ("material:num-materials=1\nmaterial[1]:material-name=Co\nmaterial[1]:damping-constant=1\n"
+           "material[1]:exchange-matrix[1]=11.2e-21\nmaterial[1]:atomic-spin-moment=1.72 !muB\n"
+           "material[1]:uniaxial-anisotropy-constant=0.0\nmaterial[1]:initial-spin-direction=1,0,0\n")
+    d = O.run_harness(inp, {"m.mat": mat}, ["--system", "--steps", 10000, "--snaps", "50,1000,5000,10000"])
+    keep = [f"s{c}_{t}" for t in (0, 50, 1000, 5000, 10000) for c in "xyz"]
+    save("single_spin_applied", d, keep)
+
+
+ALL = [sc20_t0, sc8_t0, sc10_t300, sc6_open_t300, fcc4_dmi_t300, fcc4_dmi_t0, single_spin_applied]
+
+if __name__ == "__main__":
+    names = sys.argv[1:]
+    for f in ALL:
+        if not names or f.__name__ in names:
+            f()

@@ -1,0 +1,198 @@
+"""Parity of the fused CUDA LLG-Heun path with the reference.
+
+Every test calls the CUDA kernels through the C ABI (vampire_b200.vgpu) and
+compares with the reference's own trajectories (tests/golden, produced by the
+reference objects) or with the FP64 oracle that those fixtures pin.
+
+Tolerances (max per-spin component deviation):
+  FP32 build: 1e-5;  FP64 build: 1e-12 (1e-11 for 200 FCC DMI steps).
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden, ref_spins
+
+pytestmark = pytest.mark.gpu
+
+TOL32 = 1e-5
+TOL64 = 1e-12
+
+
+@pytest.fixture(scope="module")
+def V(vgpu_lib):
+    from vampire_b200 import vgpu
+    return vgpu
+
+
+@pytest.mark.parametrize("name", ["sc8_t0", "sc6_open_t300", "fcc4_dmi_t0", "sc20_t0"])
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_fields_match_oracle(V, name, prec):
+    """Total field (exchange incl. DMI tensor + anisotropy + applied) at the
+    reference's initial spins."""
+    from oracle import oracle as O
+    s, d = load_golden(name)
+    with V.Simulation(s, precision=prec) as sim:
+        got = sim.fields()
+    o = O.OracleSystem(s)
+    want = o.spin_fields(s.spins) + o.external_fields(None)
+    scale = np.abs(want).max()
+    tol = 2e-6 if prec == "fp32" else 1e-12
+    assert np.abs(got - want).max() <= tol * scale
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("fp32", TOL32)])
+def test_sc8_t0_trajectory(V, prec, tol):
+    s, d = load_golden("sc8_t0")
+    with V.Simulation(s, precision=prec) as sim:
+        done = 0
+        for t in (1, 2, 10, 100, 1000, 2000):
+            sim.llg_heun(t - done)
+            done = t
+            err = np.abs(sim.spins() - ref_spins(d, t)).max()
+            assert err <= tol, (t, err)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("fp32", TOL32)])
+def test_config0_t0_10000_steps(V, prec, tol):
+    """Config 0 (SC 20^3 periodic, J=11.2e-21 J, Ku=6.69e-24 J, H=0.1 T,
+    alpha=0.1, dt=1e-16 s) from the reference's random initial state: the
+    GPU trajectory stays within tolerance of the reference for 10,000 steps."""
+    s, d = load_golden("sc20_t0")
+    with V.Simulation(s, precision=prec) as sim:
+        done = 0
+        errs = {}
+        for t in (1, 100, 10000):
+            sim.llg_heun(t - done)
+            done = t
+            errs[t] = float(np.abs(sim.spins() - ref_spins(d, t)).max())
+    print(f"config0 {prec} max per-spin error vs reference: {errs}")
+    assert max(errs.values()) <= tol, errs
+
+
+@pytest.mark.parametrize("name,steps", [("sc10_t300", 2), ("sc6_open_t300", 3), ("fcc4_dmi_t300", 2)])
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("fp32", TOL32)])
+def test_replayed_noise(V, name, steps, prec, tol):
+    """T>0 with the reference's own Gaussian stream (noise-replay mode): each
+    stochastic Heun step matches the reference."""
+    s, d = load_golden(name)
+    with V.Simulation(s, precision=prec) as sim:
+        for t in range(1, steps + 1):
+            sim.set_noise_replay(d[f"xi_{t}"])
+            sim.llg_heun(1)
+            if f"sx_{t}" in d:
+                err = np.abs(sim.spins() - ref_spins(d, t)).max()
+                assert err <= tol, (t, err)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("fp32", TOL32)])
+def test_fcc_dmi_200_steps(V, prec, tol):
+    s, d = load_golden("fcc4_dmi_t0")
+    with V.Simulation(s, precision=prec) as sim:
+        sim.llg_heun(200)
+        err = np.abs(sim.spins() - ref_spins(d, 200)).max()
+    assert err <= tol, err
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-6), ("fp32", 2e-5)])
+def test_single_spin_known_answer(V, prec, tol):
+    """The reference's applied-field known-answer test on the GPU: analytic
+    precession/relaxation of one spin in 10 T (tests/physical/AppliedField)."""
+    s, d = load_golden("single_spin_applied")
+    lam, H, g, dt = 1.0, 10.0, 1.76e11, 1e-16
+    with V.Simulation(s, precision=prec) as sim:
+        done = 0
+        for t in (50, 1000, 5000, 10000):
+            sim.llg_heun(t - done)
+            done = t
+            got = sim.spins()[:, 0]
+            arg = g * H * t * dt / (1 + lam * lam)
+            exact = np.array([np.cos(arg) / np.cosh(lam * arg), np.sin(arg) / np.cosh(lam * arg),
+                              np.tanh(lam * arg)])
+            assert np.abs(got - exact).max() < tol
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_philox_noise_matches_restatement(V, prec):
+    """The in-register Philox Gaussians equal an independent NumPy restatement."""
+    from oracle import philox as P
+    s, _ = load_golden("sc10_t300")
+    with V.Simulation(s, precision=prec, noise_seed=0x1234_5678_9ABC) as sim:
+        for step in (0, 1, 2**33 + 5):
+            got = sim.thermal_noise(step)
+            want = P.thermal_gaussians(s.n, step, seed=0x1234_5678_9ABC, fp64=(prec == "fp64"))
+            assert np.abs(got - want).max() < (2e-5 if prec == "fp32" else 1e-12)
+
+
+@pytest.mark.parametrize("name", ["sc10_t300", "fcc4_dmi_t300"])
+def test_philox_step_matches_oracle(V, name):
+    """One T>0 step with the built-in Philox noise equals the oracle's step
+    driven by the same Gaussians (predictor and corrector regenerate them)."""
+    from oracle import oracle as O
+    s, _ = load_golden(name)
+    with V.Simulation(s, precision="fp64", noise_seed=99) as sim:
+        sim.step = 17
+        xi = sim.thermal_noise(17)
+        sim.llg_heun(1)
+        got = sim.spins()
+        assert sim.step == 18
+    want = O.OracleSystem(s).llg_heun(s.spins, 1, xi=xi)
+    assert np.abs(got - want).max() < 1e-12
+
+
+def test_counter_based_resume(V):
+    """Resuming from (spins, step) reproduces the uninterrupted run bit for bit."""
+    s, _ = load_golden("sc10_t300")
+    with V.Simulation(s, noise_seed=5) as a:
+        a.llg_heun(20)
+        ref = a.spins()
+    with V.Simulation(s, noise_seed=5) as b:
+        b.llg_heun(8)
+        mid, st = b.spins(), b.step
+    with V.Simulation(s, noise_seed=5) as c:
+        c.set_spins(mid)
+        c.step = st
+        c.llg_heun(12)
+        # spins pass through FP64 on the host; FP32 round trip is exact
+        assert np.array_equal(c.spins(), ref)
+
+
+def test_thermal_equilibrium_single_spin_boltzmann(V):
+    """Philox thermal noise gives the Boltzmann distribution: many independent
+    uniaxial macrospins (no exchange) at T sample
+    P(theta) ~ sin(theta) exp(Ku sin^2(theta)/kT)... checked through <s_z^2>
+    against the numerically integrated expectation (the concept of the
+    reference's tests/physical/Thermal, with kB = 1.3806503e-23)."""
+    from vampire_b200 import system as S
+    n = 20000
+    m = S.Material(alpha=1.0, mu_s_muB=1.72, Ku=1e-23)
+    T = 50.0
+    # dt = 1e-14 s: gamma H_K dt ~ 0.02 rad, relaxation in ~1e3 steps
+    p = S.SimParams(dt_SI=1e-14, temperature=T, H_applied=0.0)
+    sys_ = S.build("sc", n, 1, 1, 10.0, [m], [[0.0]], p, periodic=(False, False, False),
+                   spins=np.tile(np.array([[0.0], [0.0], [1.0]]), (1, n)))
+    with V.Simulation(sys_, noise_seed=11) as sim:
+        sim.llg_heun(10000)
+        sz2 = []
+        for _ in range(20):
+            sim.llg_heun(1000)
+            sz2.append(np.mean(sim.spins()[2] ** 2))
+    # expectation of cos^2 over P(theta) ~ sin exp(K cos^2 / kT) (up to a constant)
+    K = 1e-23 / (S.KB * T)
+    c = np.linspace(-1, 1, 200001)
+    w = np.exp(K * c * c)
+    want = np.trapezoid(c * c * w, c) / np.trapezoid(w, c)
+    got = float(np.mean(sz2))
+    assert abs(got - want) < 0.01, (got, want)
+
+
+def test_status_flags_nonfinite(V):
+    """A spin state that cannot be normalised is reported, not hidden."""
+    s, _ = load_golden("sc8_t0")
+    with V.Simulation(s) as sim:
+        bad = s.spins.copy()
+        bad[:, 3] = 0.0  # zero-length spin -> 0/0 in the corrector
+        sim.set_spins(bad)
+        sim.llg_heun(1)
+        with pytest.raises(V.VGPUError) as e:
+            sim.spins()
+        assert e.value.code == V.ERR_NAN

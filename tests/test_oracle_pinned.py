@@ -1,0 +1,93 @@
+"""The FP64 CPU oracle (oracle/vref.c) against the reference program itself.
+
+The golden fixtures were produced by the reference's own objects (see
+tests/golden/make_golden.py); the oracle must reproduce them to FP64
+rounding.  This pins the checker that the GPU tests use.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden, ref_spins
+from oracle import oracle as O
+
+
+@pytest.mark.parametrize("steps", [1, 2, 10, 100, 1000, 2000])
+def test_sc8_t0_trajectory(steps):
+    s, d = load_golden("sc8_t0")
+    o = O.OracleSystem(s)
+    got = o.llg_heun(s.spins, steps)
+    assert np.abs(got - ref_spins(d, steps)).max() < 1e-12
+
+
+def test_sc20_t0_config0_trajectory():
+    """Config-0 system, 10,000 deterministic steps: the oracle follows the
+    reference step for step."""
+    s, d = load_golden("sc20_t0")
+    o = O.OracleSystem(s)
+    got = s.spins
+    for a, b in [(0, 1), (1, 100), (100, 10000)]:
+        got = o.llg_heun(got, b - a)
+        assert np.abs(got - ref_spins(d, b)).max() < 1e-12, b
+
+
+@pytest.mark.parametrize("name,steps", [("sc10_t300", 2), ("sc6_open_t300", 3), ("fcc4_dmi_t300", 2)])
+def test_replayed_noise_steps(name, steps):
+    """T>0: with the reference's own Gaussian stream the oracle reproduces its
+    stochastic Heun steps (thermal field sigma*sqrt(T)*xi, x|y|z blocks)."""
+    s, d = load_golden(name)
+    o = O.OracleSystem(s)
+    got = s.spins
+    for t in range(1, steps + 1):
+        got = o.llg_heun(got, 1, xi=d[f"xi_{t}"])
+        if f"sx_{t}" in d:
+            assert np.abs(got - ref_spins(d, t)).max() < 1e-12, t
+
+
+def test_fcc_dmi_t0_200_steps():
+    s, d = load_golden("fcc4_dmi_t0")
+    o = O.OracleSystem(s)
+    got = o.llg_heun(s.spins, 200)
+    assert np.abs(got - ref_spins(d, 200)).max() < 1e-11
+
+
+def test_single_spin_known_answer():
+    """The reference's own known-answer test (tests/physical/AppliedField,
+    applied_field_errors.py): Sx = sech(l a) cos a, Sy = sech(l a) sin a,
+    Sz = tanh(l a), a = gamma H t/(1+l^2); max error < 1e-6."""
+    s, d = load_golden("single_spin_applied")
+    o = O.OracleSystem(s)
+    lam, H, g, dt = 1.0, 10.0, 1.76e11, 1e-16
+    for t in (50, 1000, 5000, 10000):
+        got = o.llg_heun(s.spins, t)[:, 0]
+        assert np.abs(got - ref_spins(d, t)[:, 0]).max() < 1e-13
+        arg = g * H * t * dt / (1 + lam * lam)
+        exact = np.array([np.cos(arg) / np.cosh(lam * arg), np.sin(arg) / np.cosh(lam * arg), np.tanh(lam * arg)])
+        assert np.abs(got - exact).max() < 1e-6
+
+
+@pytest.mark.parametrize("name,step", [("sc20_t0", 10000), ("fcc4_dmi_t300", 2), ("sc6_open_t300", 3)])
+def test_statistics(name, step):
+    """Magnetisation and energy reductions (statistics/magnetization.cpp:134,
+    statistics/energy.cpp:141) on the reference's own masks."""
+    s, d = load_golden(name)
+    o = O.OracleSystem(s)
+    sp = ref_spins(d, step)
+    mask, size = s.masks["system"]
+    np.testing.assert_allclose(o.magnetization(sp, mask, size), d[f"mag_system_{step}"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(o.energy(sp, mask, size), d[f"energy_system_{step}"], rtol=1e-11, atol=1e-9)
+    if f"mag_material_{step}" in d:
+        mask, size = s.masks["material"]
+        np.testing.assert_allclose(o.magnetization(sp, mask, size), d[f"mag_material_{step}"], rtol=1e-12,
+                                   atol=1e-12)
+        np.testing.assert_allclose(o.energy(sp, mask, size), d[f"energy_material_{step}"], rtol=1e-11, atol=1e-9)
+
+
+def test_oracle_detects_a_planted_error():
+    """A mistake planted in the oracle's inputs (one bond's coupling) must
+    show up against the reference fixture: the checker is not vacuous."""
+    s, d = load_golden("sc8_t0")
+    bad = s.copy()
+    bad.jlist = bad.jlist.copy()
+    bad.jlist[7] *= 1.001
+    got = O.OracleSystem(bad).llg_heun(bad.spins, 10)
+    assert np.abs(got - ref_spins(d, 10)).max() > 1e-9

@@ -1,0 +1,58 @@
+"""Device magnetisation and energy reductions (K4) against the reference's
+own statistics (computed by the reference objects on the same spins)."""
+import numpy as np
+import pytest
+
+from conftest import load_golden, ref_spins
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name,step", [("sc20_t0", 10000), ("fcc4_dmi_t300", 2), ("sc6_open_t300", 3)])
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_stats_match_reference(vgpu_lib, name, step, prec):
+    from vampire_b200 import vgpu
+    s, d = load_golden(name)
+    sp = ref_spins(d, step)
+    with vgpu.Simulation(s, precision=prec) as sim:
+        sim.set_spins(sp)
+        ids = {k: sim.add_mask(*s.masks[k]) for k in ("system", "material")}
+        sim.stats_update(magnetization=True, energy=True)
+        sim.stats_update(magnetization=True, energy=True)
+        for k, mid in ids.items():
+            m, mean, cnt = sim.magnetization(mid)
+            e, emean, ecnt = sim.energy(mid)
+            assert cnt == 2 and ecnt == 2
+            if f"mag_{k}_{step}" in d:
+                want = d[f"mag_{k}_{step}"]
+                tol = 2e-6 if prec == "fp32" else 1e-12
+                assert np.abs(m - want).max() < tol
+                assert np.abs(mean - 2 * want).max() < 2 * tol
+            if f"energy_{k}_{step}" in d:
+                want = d[f"energy_{k}_{step}"]
+                scale = np.abs(want).max() + 1.0
+                tol = 2e-6 if prec == "fp32" else 1e-11
+                assert np.abs(e - want).max() < tol * scale, (e, want)
+        sim.stats_reset()
+        _, mean, cnt = sim.magnetization(ids["system"])
+        assert cnt == 0 and np.all(mean == 0)
+
+
+def test_stats_at_scale_checksum(vgpu_lib):
+    """4M-spin FCC system: device reduction equals a float64 NumPy reduction
+    of the downloaded spins (size-independent property)."""
+    from vampire_b200 import system as S
+    from vampire_b200 import vgpu
+    s = S.config_fcc_tensor(L=60)
+    with vgpu.Simulation(s) as sim:
+        sim.llg_heun(5)
+        sp = sim.spins()
+        mid = sim.add_mask(*s.masks["material"])
+        sim.stats_update()
+        m, _, _ = sim.magnetization(mid)
+    mu = s.mu_s_muB()
+    for b in range(2):
+        sel = s.type == b
+        v = (sp[:, sel] * mu[sel]).sum(1)
+        want = np.r_[v / np.linalg.norm(v), np.linalg.norm(v) / mu[sel].sum()]
+        assert np.abs(m[4 * b:4 * b + 4] - want).max() < 1e-9

@@ -1,0 +1,147 @@
+// Device helpers shared by the fused LLG, statistics, Monte Carlo and adjoint
+// kernels: the SELL-32 exchange gather, anisotropy and external fields, the
+// LLG right-hand side, and in-register Philox thermal noise.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "philox.cuh"
+#include "vgpu_internal.cuh"
+
+namespace vgpu {
+
+template <typename R> __device__ __forceinline__ R rsqrt_(R x);
+template <> __device__ __forceinline__ float rsqrt_<float>(float x) { return rsqrtf(x); }
+template <> __device__ __forceinline__ double rsqrt_<double>(double x) { return 1.0 / sqrt(x); }
+
+template <typename R>
+__device__ __forceinline__ void thermal_xi(const LLGArgs<R>& a, int i, R& gx, R& gy, R& gz) {
+   if (a.noise_mode == VGPU_NOISE_REPLAY) {
+      gx = a.xi[i];
+      gy = a.xi[a.n + i];
+      gz = a.xi[2 * a.n + i];
+      return;
+   }
+   u32x4 c = {(uint32_t)i, (uint32_t)a.step, (uint32_t)(a.step >> 32), RNG_THERMAL};
+   u32x4 r = philox4x32_10(c, a.seed_lo, a.seed_hi);
+   if (sizeof(R) == 4) {
+      float s1, c1, s2, c2;
+      const float r1 = sqrtf(-2.0f * logf(u01f(r.x)));
+      const float r2 = sqrtf(-2.0f * logf(u01f(r.z)));
+      sincospif(2.0f * u01f(r.y), &s1, &c1);
+      sincospif(2.0f * u01f(r.w), &s2, &c2);
+      gx = (R)(r1 * c1);
+      gy = (R)(r1 * s1);
+      gz = (R)(r2 * c2);
+   } else {
+      double s1, c1, s2, c2;
+      const double r1 = sqrt(-2.0 * log(u01d(r.x)));
+      const double r2 = sqrt(-2.0 * log(u01d(r.z)));
+      sincospi(2.0 * u01d(r.y), &s1, &c1);
+      sincospi(2.0 * u01d(r.w), &s2, &c2);
+      gx = (R)(r1 * c1);
+      gy = (R)(r1 * s1);
+      gz = (R)(r2 * c2);
+   }
+}
+
+// exchange gather of atom i over its SELL row, sources (sx,sy,sz)
+template <typename R, int FMT>
+__device__ __forceinline__ void exchange_gather(const LLGArgs<R>& a, int i, int mi, const R* __restrict__ sx,
+                                                const R* __restrict__ sy, const R* __restrict__ sz, R& hx,
+                                                R& hy, R& hz) {
+   const int sl = i >> 5, lane = i & 31;
+   const int off = __ldg(a.slice_off + sl);
+   const int w = (__ldg(a.slice_off + sl + 1) - off) >> 5;
+   const int base = off + lane;
+   const R* __restrict__ tab = a.jtab;
+#pragma unroll 4
+   for (int k = 0; k < w; ++k) {
+      const int e = base + 32 * k;
+      const int c = __ldg(a.col + e);
+      const int j = c & a.idx_mask;
+      const R x = __ldg(sx + j), y = __ldg(sy + j), z = __ldg(sz + j);
+      if (FMT == FMT_ISO_TAB) {
+         const int mj = a.mat_shift ? (c >> a.mat_shift) : 0;
+         const R J = __ldg(tab + mi * a.M + mj);
+         hx += J * x; hy += J * y; hz += J * z;
+      } else if (FMT == FMT_ISO_BOND) {
+         const R J = __ldg(a.jb[0] + e);
+         hx += J * x; hy += J * y; hz += J * z;
+      } else if (FMT == FMT_VEC_TAB) {
+         const int mj = a.mat_shift ? (c >> a.mat_shift) : 0;
+         const R* t = tab + 3 * (mi * a.M + mj);
+         hx += __ldg(t) * x; hy += __ldg(t + 1) * y; hz += __ldg(t + 2) * z;
+      } else if (FMT == FMT_VEC_BOND) {
+         hx += __ldg(a.jb[0] + e) * x; hy += __ldg(a.jb[1] + e) * y; hz += __ldg(a.jb[2] + e) * z;
+      } else if (FMT == FMT_DMI_TAB) {
+         const int mj = a.mat_shift ? (c >> a.mat_shift) : 0;
+         const R* t = tab + 3 * (mi * a.M + mj);
+         const R dx = __ldg(a.jb[0] + e), dy = __ldg(a.jb[1] + e), dz = __ldg(a.jb[2] + e);
+         // diag part plus the antisymmetric part written as d x s_j
+         hx += __ldg(t) * x + (dy * z - dz * y);
+         hy += __ldg(t + 1) * y + (dz * x - dx * z);
+         hz += __ldg(t + 2) * z + (dx * y - dy * x);
+      } else {  // FMT_TENSOR_BOND
+         const R t0 = __ldg(a.jb[0] + e), t1 = __ldg(a.jb[1] + e), t2 = __ldg(a.jb[2] + e);
+         const R t3 = __ldg(a.jb[3] + e), t4 = __ldg(a.jb[4] + e), t5 = __ldg(a.jb[5] + e);
+         const R t6 = __ldg(a.jb[6] + e), t7 = __ldg(a.jb[7] + e), t8 = __ldg(a.jb[8] + e);
+         hx += (t0 * x + t1 * y + t2 * z);
+         hy += (t3 * x + t4 * y + t5 * z);
+         hz += (t6 * x + t7 * y + t8 * z);
+      }
+   }
+}
+
+// spin-dependent field of atom i at spin S: exchange + anisotropy
+// (calculate_spin_fields, src/simulate/fields.cpp:67-118)
+template <typename R, int FMT>
+__device__ __forceinline__ void spin_field(const LLGArgs<R>& a, int i, int mi, const MatParams<R>& m,
+                                           const R* sx, const R* sy, const R* sz, const R S[3], R H[3]) {
+   R hx = 0, hy = 0, hz = 0;
+   exchange_gather<R, FMT>(a, i, mi, sx, sy, sz, hx, hy, hz);
+   if (a.uniaxial) {
+      const R sdote = S[0] * m.kux + S[1] * m.kuy + S[2] * m.kuz;
+      const R k2 = (R)2 * m.ku2 * sdote;
+      hx += m.kux * k2; hy += m.kuy * k2; hz += m.kuz * k2;
+   }
+   if (a.cubic) {
+      const R k4 = (R)2 * m.kc4;
+      hx += S[0] * S[0] * S[0] * k4;
+      hy += S[1] * S[1] * S[1] * k4;
+      hz += S[2] * S[2] * S[2] * k4;
+   }
+   H[0] = hx; H[1] = hy; H[2] = hz;
+}
+
+// external field (calculate_external_fields, fields.cpp:120-169)
+template <typename R>
+__device__ __forceinline__ void external_field(const LLGArgs<R>& a, int i, const MatParams<R>& m, bool with_noise,
+                                               R E[3]) {
+   R ex = 0, ey = 0, ez = 0;
+   if (a.thermal && with_noise) {
+      R gx, gy, gz;
+      thermal_xi(a, i, gx, gy, gz);
+      ex = gx * m.sigma; ey = gy * m.sigma; ez = gz * m.sigma;
+   }
+   if (a.local_field) { ex += a.hx + m.hlx; ey += a.hy + m.hly; ez += a.hz + m.hlz; }
+   else { ex += a.hx; ey += a.hy; ez += a.hz; }
+   if (a.cell) {
+      const int c = __ldg(a.cell + i);
+      ex += __ldg(a.cell_field + c);
+      ey += __ldg(a.cell_field + a.ncells + c);
+      ez += __ldg(a.cell_field + 2 * a.ncells + c);
+   } else if (a.hd_atom) {
+      ex += __ldg(a.hd_atom + i); ey += __ldg(a.hd_atom + a.n + i); ez += __ldg(a.hd_atom + 2 * a.n + i);
+   }
+   E[0] = ex; E[1] = ey; E[2] = ez;
+}
+
+// LLG right-hand side exactly as LLGHeun.cpp:201-203
+template <typename R>
+__device__ __forceinline__ void llg_rhs(R A, R B, const R S[3], const R H[3], R d[3]) {
+   d[0] = A * (S[1] * H[2] - S[2] * H[1]) + B * (S[1] * (S[0] * H[1] - S[1] * H[0]) - S[2] * (S[2] * H[0] - S[0] * H[2]));
+   d[1] = A * (S[2] * H[0] - S[0] * H[2]) + B * (S[2] * (S[1] * H[2] - S[2] * H[1]) - S[0] * (S[0] * H[1] - S[1] * H[0]));
+   d[2] = A * (S[0] * H[1] - S[1] * H[0]) + B * (S[0] * (S[2] * H[0] - S[0] * H[2]) - S[1] * (S[1] * H[2] - S[2] * H[1]));
+}
+
+}  // namespace vgpu

@@ -1,0 +1,116 @@
+// Fused stochastic LLG-Heun passes (sm_100a).
+//
+// The reference step (src/simulate/LLGHeun.cpp:160-282) makes two full field
+// evaluations and four streaming loops over 12 SoA arrays per step; its CUDA
+// backend (src/cuda/llg_heun.cu:121-208) makes 11 launches and 3 copies.
+// Here a step is two launches, each one HBM pass:
+//
+//   predictor  s'  = n(s0 + dt * f(s0, H(s0) + H_ext))          reads s0, writes s'
+//   corrector  s1  = n(s0 + dt/2 (f(s0,..) + f(s', H(s') + H_ext)))
+//                                                 reads s0 and s', writes s1 over s0
+//
+// H(s) is the exchange gather over a sliced-ELL (SELL-32) copy of the CSR
+// list (a warp = 32 consecutive atoms; bond k of lane l sits at
+// slice_off + 32 k + l, so every index/coupling load of a warp is one 128-byte
+// line) plus uniaxial and cubic anisotropy; H_ext is thermal noise
+// regenerated in-register from Philox (no noise buffer), applied field and the
+// macrocell dipole field looked up by cell id.  The predictor's
+// f(s0, ...) dt is not stored: since f is perpendicular to s0 and
+// s' = (s0 + f dt)/|s0 + f dt|, the corrector recovers
+// f dt = s' |s0|^2 / (s'.s0) - s0 exactly from the two states it reads anyway.
+#include <cuda_runtime.h>
+
+#include "llg_device.cuh"
+
+namespace vgpu {
+
+template <typename R, int FMT, int MODE>
+__global__ void __launch_bounds__(256) llg_pass_kernel(const LLGArgs<R> a) {
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= a.n) return;
+   const int mi = a.mat ? __ldg(a.mat + i) : 0;
+   const MatParams<R> m = a.mp[mi];
+   const R S0[3] = {a.ax[i], a.ay[i], a.az[i]};
+   if (MODE == PASS_PREDICTOR || MODE == PASS_FIELD) {
+      R H[3], E[3];
+      spin_field<R, FMT>(a, i, mi, m, a.ax, a.ay, a.az, S0, H);
+      external_field<R>(a, i, m, MODE == PASS_PREDICTOR, E);
+      H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
+      if (MODE == PASS_FIELD) {
+         a.fx[i] = H[0]; a.fy[i] = H[1]; a.fz[i] = H[2];
+         return;
+      }
+      R d[3];
+      llg_rhs<R>(m.A, m.B, S0, H, d);
+      R Sn[3] = {S0[0] + d[0] * a.dt, S0[1] + d[1] * a.dt, S0[2] + d[2] * a.dt};
+      const R r = rsqrt_<R>(Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2]);
+      a.bx[i] = Sn[0] * r; a.by[i] = Sn[1] * r; a.bz[i] = Sn[2] * r;
+   } else {
+      const R S1[3] = {a.bx[i], a.by[i], a.bz[i]};
+      R H[3], E[3];
+      spin_field<R, FMT>(a, i, mi, m, a.bx, a.by, a.bz, S1, H);
+      external_field<R>(a, i, m, true, E);
+      H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
+      R d[3];
+      llg_rhs<R>(m.A, m.B, S1, H, d);
+      // recover the predictor increment f(s0) dt from s0 and s'
+      const R s00 = S0[0] * S0[0] + S0[1] * S0[1] + S0[2] * S0[2];
+      const R c = s00 / (S1[0] * S0[0] + S1[1] * S0[1] + S1[2] * S0[2]);
+      R Sn[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+         const R e = S1[k] * c - S0[k];
+         Sn[k] = S0[k] + ((R)0.5 * e + a.half_dt * d[k]);
+      }
+      const R n2 = Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2];
+      const R r = rsqrt_<R>(n2);
+      if (!(n2 > (R)0.25 && n2 < (R)4)) atomicOr(a.status, 1);  // non-finite or runaway
+      a.ax[i] = Sn[0] * r; a.ay[i] = Sn[1] * r; a.az[i] = Sn[2] * r;
+   }
+}
+
+template <typename R, int FMT>
+static cudaError_t launch_fmt(const LLGArgs<R>& a, int mode, cudaStream_t st) {
+   const int bs = 256;
+   const int grid = (a.n + bs - 1) / bs;
+   if (grid == 0) return cudaSuccess;
+   if (mode == PASS_PREDICTOR) llg_pass_kernel<R, FMT, PASS_PREDICTOR><<<grid, bs, 0, st>>>(a);
+   else if (mode == PASS_CORRECTOR) llg_pass_kernel<R, FMT, PASS_CORRECTOR><<<grid, bs, 0, st>>>(a);
+   else llg_pass_kernel<R, FMT, PASS_FIELD><<<grid, bs, 0, st>>>(a);
+   return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_llg_pass(const LLGArgs<R>& a, int fmt, int mode, int nslices, cudaStream_t st) {
+   (void)nslices;
+   switch (fmt) {
+      case FMT_ISO_TAB: return launch_fmt<R, FMT_ISO_TAB>(a, mode, st);
+      case FMT_ISO_BOND: return launch_fmt<R, FMT_ISO_BOND>(a, mode, st);
+      case FMT_VEC_TAB: return launch_fmt<R, FMT_VEC_TAB>(a, mode, st);
+      case FMT_VEC_BOND: return launch_fmt<R, FMT_VEC_BOND>(a, mode, st);
+      case FMT_DMI_TAB: return launch_fmt<R, FMT_DMI_TAB>(a, mode, st);
+      default: return launch_fmt<R, FMT_TENSOR_BOND>(a, mode, st);
+   }
+}
+
+template <typename R>
+__global__ void thermal_noise_kernel(const LLGArgs<R> a) {
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= a.n) return;
+   R gx, gy, gz;
+   thermal_xi(a, i, gx, gy, gz);
+   a.fx[i] = gx; a.fy[i] = gy; a.fz[i] = gz;
+}
+
+template <typename R>
+cudaError_t launch_thermal_noise(const LLGArgs<R>& a, cudaStream_t st) {
+   thermal_noise_kernel<R><<<(a.n + 255) / 256, 256, 0, st>>>(a);
+   return cudaGetLastError();
+}
+template cudaError_t launch_thermal_noise<float>(const LLGArgs<float>&, cudaStream_t);
+template cudaError_t launch_thermal_noise<double>(const LLGArgs<double>&, cudaStream_t);
+
+template cudaError_t launch_llg_pass<float>(const LLGArgs<float>&, int, int, int, cudaStream_t);
+template cudaError_t launch_llg_pass<double>(const LLGArgs<double>&, int, int, int, cudaStream_t);
+
+}  // namespace vgpu

@@ -1,0 +1,58 @@
+// Counter-based Philox4x32-10 generator (Salmon, Moraes, Dror, Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC'11) and the Box-Muller
+// transform, for in-register thermal noise.  The stream is keyed by a 64-bit
+// seed; the counter is (atom, step_lo, step_hi, purpose), so a step's noise
+// can be regenerated anywhere (the corrector recomputes what the predictor
+// used) and a run resumes bit-exactly from (seed, step).
+#pragma once
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define VGPU_HD __host__ __device__ __forceinline__
+#else
+#define VGPU_HD inline
+#endif
+
+namespace vgpu {
+
+// purposes (4th counter word)
+enum : uint32_t { RNG_THERMAL = 0u, RNG_MC_MOVE = 1u, RNG_MC_ACCEPT = 2u, RNG_THERMAL_HI = 3u };
+
+struct u32x4 { uint32_t x, y, z, w; };
+
+VGPU_HD void mulhilo32(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo) {
+#ifdef __CUDA_ARCH__
+   lo = a * b;
+   hi = __umulhi(a, b);
+#else
+   uint64_t p = (uint64_t)a * (uint64_t)b;
+   lo = (uint32_t)p;
+   hi = (uint32_t)(p >> 32);
+#endif
+}
+
+VGPU_HD u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1) {
+   const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+   const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+   for (int r = 0; r < 10; ++r) {
+      uint32_t hi0, lo0, hi1, lo1;
+      mulhilo32(M0, c.x, hi0, lo0);
+      mulhilo32(M1, c.z, hi1, lo1);
+      u32x4 n;
+      n.x = hi1 ^ c.y ^ k0;
+      n.y = lo1;
+      n.z = hi0 ^ c.w ^ k1;
+      n.w = lo0;
+      c = n;
+      k0 += W0;
+      k1 += W1;
+   }
+   return c;
+}
+
+// uniform in (0,1): 24-bit float and 32-bit double variants
+VGPU_HD float u01f(uint32_t x) { return ((float)(x >> 8) + 0.5f) * (1.0f / 16777216.0f); }
+VGPU_HD double u01d(uint32_t x) { return ((double)x + 0.5) * (1.0 / 4294967296.0); }
+
+}  // namespace vgpu

@@ -1,0 +1,623 @@
+// C ABI of libvgpu.so (include/vgpu.h): context, system upload, LLG stepping.
+//
+// Upload turns the reference's CSR neighbour list and unrolled per-bond
+// exchange list (src/exchange/initialize.cpp:70-117,
+// unroll_normalised.cpp:37-140) into a sliced-ELL layout with slices of 32
+// atoms, and picks the most compact exchange format that reproduces every
+// bond's coupling exactly (ExchFmt in vgpu_internal.cuh): couplings that are
+// a function of the two materials go to a small table and the neighbour's
+// material rides in the top bits of its index, so the only per-bond bytes
+// left in HBM are the index and, for DMI, the antisymmetric vector.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "vgpu_ctx.cuh"
+
+using namespace vgpu;
+
+namespace vgpu {
+
+std::mutex g_err_mutex;
+std::string g_global_err;
+
+int set_err(vgpu_ctx* h, int code, const char* fmt, ...) {
+   char buf[1024];
+   va_list ap;
+   va_start(ap, fmt);
+   vsnprintf(buf, sizeof buf, fmt, ap);
+   va_end(ap);
+   if (h) h->err = buf;
+   else {
+      std::lock_guard<std::mutex> g(g_err_mutex);
+      g_global_err = buf;
+   }
+   return code;
+}
+
+int cuda_err(vgpu_ctx* h, cudaError_t e, const char* what) {
+   if (e == cudaSuccess) return VGPU_OK;
+   cudaGetLastError();
+   return set_err(h, e == cudaErrorMemoryAllocation ? VGPU_ERR_OOM : VGPU_ERR_CUDA, "%s: %s", what,
+                  cudaGetErrorString(e));
+}
+
+}  // namespace vgpu
+
+void* vgpu_ctx::alloc(size_t bytes) {
+   if (bytes == 0) bytes = 16;
+   void* p = nullptr;
+   cudaError_t e = cudaMalloc(&p, bytes);
+   if (e != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+   }
+   allocs.push_back(p);
+   return p;
+}
+namespace vgpu {
+
+}  // namespace vgpu
+
+void vgpu_ctx::free_system() {
+   for (void* p : allocs) cudaFree(p);
+   allocs.clear();
+   sys = SysDev();
+}
+namespace vgpu {
+
+template <typename R>
+static int upload_vec(vgpu_ctx* h, void** dst, const std::vector<R>& v, const char* what) {
+   *dst = h->alloc(v.size() * sizeof(R));
+   if (!*dst) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for %s (%zu bytes)", what, v.size() * sizeof(R));
+   if (v.empty()) return VGPU_OK;
+   return cuda_err(h, cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(R), cudaMemcpyHostToDevice, h->stream), what);
+}
+
+// ---------------------------------------------------------------------------
+// host-side exchange analysis
+// ---------------------------------------------------------------------------
+struct BondView {
+   int exch_type;
+   const double* jl;
+   const int32_t* nl_type;
+   int64_t num_exchange;
+   const double* get(int64_t bond) const {
+      const int64_t id = nl_type ? nl_type[bond] : bond;
+      const int w = exch_type == VGPU_EXCH_ISOTROPIC ? 1 : exch_type == VGPU_EXCH_VECTORIAL ? 3 : 9;
+      return jl + w * id;
+   }
+};
+
+// Returns the chosen format; fills table (M*M*{1,3}) when a table format is possible.
+static int choose_format(const vgpu_system_desc* d, const BondView& bv, std::vector<double>& table, bool can_pack) {
+   const int M = d->num_materials;
+   const int n = d->num_atoms;
+   const int et = d->exchange_type;
+   const int tw = et == VGPU_EXCH_ISOTROPIC ? 1 : 3;
+   table.assign((size_t)M * M * tw, 0.0);
+   std::vector<char> seen((size_t)M * M, 0);
+   bool tab_ok = can_pack || M == 1;
+   bool antisym_only = true;  // tensor: off-diagonal part antisymmetric
+   bool any_d = false;
+   for (int i = 0; i < n; ++i) {
+      const int mi = d->type[i];
+      for (int64_t b = d->nl_start[i]; b <= d->nl_end[i]; ++b) {
+         const int mj = d->type[d->nl[b]];
+         const double* J = bv.get(b);
+         double diag[3];
+         if (et == VGPU_EXCH_ISOTROPIC) diag[0] = J[0];
+         else if (et == VGPU_EXCH_VECTORIAL) { diag[0] = J[0]; diag[1] = J[1]; diag[2] = J[2]; }
+         else {
+            diag[0] = J[0]; diag[1] = J[4]; diag[2] = J[8];
+            if (J[1] + J[3] != 0.0 || J[2] + J[6] != 0.0 || J[5] + J[7] != 0.0) antisym_only = false;
+            if (J[1] != 0.0 || J[2] != 0.0 || J[5] != 0.0) any_d = true;
+         }
+         if (tab_ok) {
+            const size_t key = (size_t)mi * M + mj;
+            double* t = &table[key * tw];
+            if (!seen[key]) {
+               seen[key] = 1;
+               for (int k = 0; k < tw; ++k) t[k] = diag[k];
+            } else {
+               for (int k = 0; k < tw; ++k)
+                  if (t[k] != diag[k]) tab_ok = false;
+            }
+         }
+      }
+   }
+   if (et == VGPU_EXCH_ISOTROPIC) return tab_ok ? FMT_ISO_TAB : FMT_ISO_BOND;
+   if (et == VGPU_EXCH_VECTORIAL) return tab_ok ? FMT_VEC_TAB : FMT_VEC_BOND;
+   if (antisym_only && tab_ok) return any_d ? FMT_DMI_TAB : FMT_VEC_TAB;
+   return FMT_TENSOR_BOND;
+}
+
+static int validate(vgpu_ctx* h, const vgpu_system_desc* d) {
+   if (!d) return set_err(h, VGPU_ERR_ARG, "null system descriptor");
+   if (d->num_atoms <= 0) return set_err(h, VGPU_ERR_ARG, "num_atoms must be positive (got %d)", d->num_atoms);
+   if (d->num_atoms > (1 << 30)) return set_err(h, VGPU_ERR_ARG, "num_atoms too large");
+   if (d->num_materials <= 0 || d->num_materials > 100)
+      return set_err(h, VGPU_ERR_ARG, "num_materials must be in 1..100 (got %d)", d->num_materials);
+   if (d->exchange_type < 0 || d->exchange_type > 2)
+      return set_err(h, VGPU_ERR_ARG, "unknown exchange_type %d", d->exchange_type);
+   if (!d->nl_start || !d->nl_end || (d->num_bonds > 0 && (!d->nl || !d->jlist)) || !d->type || !d->materials ||
+       !d->sx || !d->sy || !d->sz)
+      return set_err(h, VGPU_ERR_ARG, "null array in system descriptor");
+   if (d->num_bonds < 0 || d->num_bonds >= (int64_t)1 << 31) return set_err(h, VGPU_ERR_ARG, "bad num_bonds");
+   const int64_t nex = d->nl_type ? d->num_exchange : d->num_bonds;
+   for (int i = 0; i < d->num_atoms; ++i) {
+      const int64_t s = d->nl_start[i], e = d->nl_end[i];
+      if (s < 0 || e < s - 1 || e >= d->num_bonds)
+         return set_err(h, VGPU_ERR_ARG, "corrupt CSR row %d: start %lld end %lld num_bonds %lld", i, (long long)s,
+                        (long long)e, (long long)d->num_bonds);
+      const int t = d->type[i];
+      if (t < 0 || t >= d->num_materials) return set_err(h, VGPU_ERR_ARG, "atom %d has material %d out of range", i, t);
+      for (int64_t b = s; b <= e; ++b) {
+         const int j = d->nl[b];
+         if (j < 0 || j >= d->num_atoms)
+            return set_err(h, VGPU_ERR_ARG, "corrupt CSR: bond %lld of atom %d points to %d (num_atoms %d)",
+                           (long long)b, i, j, d->num_atoms);
+         if (d->nl_type && (d->nl_type[b] < 0 || d->nl_type[b] >= nex))
+            return set_err(h, VGPU_ERR_ARG, "bond %lld interaction id out of range", (long long)b);
+      }
+      if (!std::isfinite(d->sx[i]) || !std::isfinite(d->sy[i]) || !std::isfinite(d->sz[i]))
+         return set_err(h, VGPU_ERR_NAN, "initial spin of atom %d is not finite", i);
+   }
+   return VGPU_OK;
+}
+
+template <typename R>
+static int upload_typed(vgpu_ctx* h, const vgpu_system_desc* d) {
+   const int n = d->num_atoms;
+   const int M = d->num_materials;
+   const int nslices = (n + 31) / 32;
+   const int n_alloc = nslices * 32 + 1;  // + one zero "padding" atom
+   const int pad = n_alloc - 1;
+   int shift = 1;
+   while ((1 << shift) <= pad) ++shift;
+   const bool can_pack = M == 1 || ((int64_t)(M - 1) << shift) < ((int64_t)1 << 31);
+   BondView bv{d->exchange_type, d->jlist, d->nl_type, d->num_exchange};
+   std::vector<double> table;
+   const int fmt = d->num_bonds ? choose_format(d, bv, table, can_pack) : FMT_ISO_TAB;
+   const bool tabfmt = fmt == FMT_ISO_TAB || fmt == FMT_VEC_TAB || fmt == FMT_DMI_TAB;
+   const int use_shift = (tabfmt && M > 1) ? shift : 0;
+   if (table.empty()) table.assign((size_t)M * M * 3, 0.0);
+
+   // slice widths and offsets
+   std::vector<int> off(nslices + 1, 0);
+   for (int s = 0; s < nslices; ++s) {
+      int w = 0;
+      for (int l = 0; l < 32; ++l) {
+         const int i = s * 32 + l;
+         if (i < n) w = std::max<int>(w, (int)(d->nl_end[i] - d->nl_start[i] + 1));
+      }
+      off[s + 1] = off[s] + 32 * w;
+   }
+   const size_t ne = (size_t)off[nslices];
+   std::vector<int> col(ne, pad);
+   const int nper = fmt == FMT_ISO_BOND ? 1 : (fmt == FMT_VEC_BOND || fmt == FMT_DMI_TAB) ? 3
+                  : fmt == FMT_TENSOR_BOND ? 9 : 0;
+   std::vector<std::vector<R>> jb(nper, std::vector<R>(ne, (R)0));
+   for (int i = 0; i < n; ++i) {
+      const int s = i >> 5, l = i & 31;
+      const int mi = d->type[i];
+      (void)mi;
+      int k = 0;
+      for (int64_t b = d->nl_start[i]; b <= d->nl_end[i]; ++b, ++k) {
+         const size_t e = (size_t)off[s] + 32 * (size_t)k + l;
+         const int j = d->nl[b];
+         col[e] = j | (use_shift ? (d->type[j] << use_shift) : 0);
+         const double* J = bv.get(b);
+         switch (fmt) {
+            case FMT_ISO_BOND: jb[0][e] = (R)J[0]; break;
+            case FMT_VEC_BOND: jb[0][e] = (R)J[0]; jb[1][e] = (R)J[1]; jb[2][e] = (R)J[2]; break;
+            case FMT_DMI_TAB:  // d = (T[2][1], T[0][2], T[1][0])
+               jb[0][e] = (R)J[7]; jb[1][e] = (R)J[2]; jb[2][e] = (R)J[3];
+               break;
+            case FMT_TENSOR_BOND:
+               for (int q = 0; q < 9; ++q) jb[q][e] = (R)J[q];
+               break;
+            default: break;
+         }
+      }
+   }
+   std::vector<R> tabR(table.begin(), table.end());
+   std::vector<int> mat(d->type, d->type + n);
+   std::vector<R> ax(n_alloc, (R)0), ay(n_alloc, (R)0), az(n_alloc, (R)0);
+   for (int i = 0; i < n; ++i) { ax[i] = (R)d->sx[i]; ay[i] = (R)d->sy[i]; az[i] = (R)d->sz[i]; }
+
+   h->free_system();
+   SysDev& S = h->sys;
+   S.n = n; S.M = M; S.nslices = nslices; S.n_alloc = n_alloc; S.fmt = fmt;
+   S.mat_shift = use_shift; S.idx_mask = use_shift ? ((1 << use_shift) - 1) : 0x7fffffff;
+   S.num_bonds = d->num_bonds; S.sell_entries = (int64_t)ne;
+   S.uniaxial = d->uniaxial_enabled; S.cubic = d->cubic_enabled;
+   S.type_host = mat;
+   S.materials.assign(d->materials, d->materials + M);
+   int rc;
+   if ((rc = upload_vec(h, &S.slice_off, off, "slice offsets"))) return rc;
+   if ((rc = upload_vec(h, &S.col, col, "neighbour index"))) return rc;
+   for (int q = 0; q < nper; ++q)
+      if ((rc = upload_vec(h, &S.jb[q], jb[q], "bond couplings"))) return rc;
+   if ((rc = upload_vec(h, &S.jtab, tabR, "coupling table"))) return rc;
+   if (M > 1) { if ((rc = upload_vec(h, &S.mat, mat, "materials"))) return rc; }
+   if ((rc = upload_vec(h, &S.s[0], ax, "spins"))) return rc;
+   if ((rc = upload_vec(h, &S.s[1], ay, "spins"))) return rc;
+   if ((rc = upload_vec(h, &S.s[2], az, "spins"))) return rc;
+   std::vector<R> zeros(n_alloc, (R)0);
+   for (int q = 0; q < 3; ++q)
+      if ((rc = upload_vec(h, &S.p[q], zeros, "predictor state"))) return rc;
+   S.mp = h->alloc(sizeof(MatParams<R>) * M);
+   if (!S.mp) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for material table");
+   S.status = (int*)h->alloc(sizeof(int));
+   if (!S.status) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for status word");
+   if ((rc = cuda_err(h, cudaMemsetAsync(S.status, 0, sizeof(int), h->stream), "status"))) return rc;
+   S.uploaded = true;
+   return h->refresh_materials();
+}
+
+template <typename R>
+int refresh_materials_typed(vgpu_ctx* h) {
+   SysDev& S = h->sys;
+   const vgpu_sim_params& p = h->params;
+   std::vector<MatParams<R>> mp(S.M);
+   for (int m = 0; m < S.M; ++m) {
+      const vgpu_material& q = S.materials[m];
+      const double T = p.local_temperature ? q.temperature : p.temperature;
+      const double a = q.temperature_rescaling_alpha, Tc = q.temperature_rescaling_Tc;
+      const double Tr = T < Tc ? Tc * std::pow(T / Tc, a) : T;
+      MatParams<R>& o = mp[m];
+      o.A = (R)q.one_oneplusalpha_sq;
+      o.B = (R)q.alpha_oneplusalpha_sq;
+      o.sigma = (R)(std::sqrt(Tr) * q.H_th_sigma);
+      o.ku2 = (R)q.ku2;
+      o.kux = (R)q.ku_vector[0]; o.kuy = (R)q.ku_vector[1]; o.kuz = (R)q.ku_vector[2];
+      o.kc4 = (R)q.kc4;
+      o.hlx = (R)q.applied_field[0]; o.hly = (R)q.applied_field[1]; o.hlz = (R)q.applied_field[2];
+      o.mu_s_muB = (R)(q.mu_s_SI / 9.27400915e-24);
+   }
+   return cuda_err(h, cudaMemcpyAsync(S.mp, mp.data(), sizeof(MatParams<R>) * S.M, cudaMemcpyHostToDevice, h->stream),
+                   "material upload");
+}
+
+}  // namespace vgpu
+
+int vgpu_ctx::refresh_materials() {
+   if (!sys.uploaded && sys.mp == nullptr) return VGPU_OK;
+   return prec == VGPU_PREC_FP64 ? refresh_materials_typed<double>(this) : refresh_materials_typed<float>(this);
+}
+namespace vgpu {
+
+template <typename R>
+LLGArgs<R> make_args(vgpu_ctx* h) {
+   SysDev& S = h->sys;
+   LLGArgs<R> a;
+   memset(&a, 0, sizeof a);
+   a.n = S.n;
+   a.slice_off = (const int*)S.slice_off;
+   a.col = (const int*)S.col;
+   a.idx_mask = S.idx_mask;
+   a.mat_shift = S.mat_shift;
+   for (int q = 0; q < 9; ++q) a.jb[q] = (const R*)S.jb[q];
+   a.jtab = (const R*)S.jtab;
+   a.M = S.M;
+   a.mat = (const int*)S.mat;
+   a.mp = (const MatParams<R>*)S.mp;
+   a.uniaxial = S.uniaxial;
+   a.cubic = S.cubic;
+   const vgpu_sim_params& p = h->params;
+   const double hx = p.applied_enabled ? p.H_applied * p.H_vec[0] : 0.0;
+   const double hy = p.applied_enabled ? p.H_applied * p.H_vec[1] : 0.0;
+   const double hz = p.applied_enabled ? p.H_applied * p.H_vec[2] : 0.0;
+   a.hx = (R)hx; a.hy = (R)hy; a.hz = (R)hz;
+   a.local_field = p.applied_enabled && p.local_applied_field;
+   a.thermal = p.thermal_enabled && (h->noise_mode == VGPU_NOISE_REPLAY || h->any_sigma);
+   a.noise_mode = h->noise_mode;
+   a.seed_lo = (uint32_t)h->seed;
+   a.seed_hi = (uint32_t)(h->seed >> 32);
+   a.step = h->step;
+   a.xi = (const R*)S.xi;
+   a.cell = (const int*)S.cell;
+   a.cell_field = (const R*)S.cell_field;
+   a.ncells = S.ncells;
+   a.hd_atom = (const R*)S.hd_atom;
+   a.dt = (R)p.dt;
+   a.half_dt = (R)(0.5 * p.dt);
+   a.ax = (R*)S.s[0]; a.ay = (R*)S.s[1]; a.az = (R*)S.s[2];
+   a.bx = (R*)S.p[0]; a.by = (R*)S.p[1]; a.bz = (R*)S.p[2];
+   a.fx = (R*)S.f[0]; a.fy = (R*)S.f[1]; a.fz = (R*)S.f[2];
+   a.status = S.status;
+   return a;
+}
+template LLGArgs<float> make_args<float>(vgpu_ctx*);
+template LLGArgs<double> make_args<double>(vgpu_ctx*);
+
+template <typename R>
+static int llg_steps_typed(vgpu_ctx* h, uint64_t n_steps) {
+   for (uint64_t t = 0; t < n_steps; ++t) {
+      LLGArgs<R> a = make_args<R>(h);
+      h->prof_begin(PROF_PREDICTOR);
+      cudaError_t e = launch_llg_pass<R>(a, h->sys.fmt, PASS_PREDICTOR, h->sys.nslices, h->stream);
+      h->prof_end(PROF_PREDICTOR);
+      h->prof_begin(PROF_CORRECTOR);
+      if (e == cudaSuccess) e = launch_llg_pass<R>(a, h->sys.fmt, PASS_CORRECTOR, h->sys.nslices, h->stream);
+      h->prof_end(PROF_CORRECTOR);
+      if (e != cudaSuccess) return cuda_err(h, e, "llg_heun launch");
+      h->kernel_launches += 2;
+      h->step++;
+      int rc = h->after_step();
+      if (rc) return rc;
+   }
+   return VGPU_OK;
+}
+
+}  // namespace vgpu
+
+int vgpu_ctx::check_status() {
+   if (!sys.uploaded) return VGPU_OK;
+   int st = 0;
+   int rc = cuda_err(this, cudaMemcpyAsync(&st, sys.status, sizeof(int), cudaMemcpyDeviceToHost, stream), "status read");
+   if (rc) return rc;
+   rc = cuda_err(this, cudaStreamSynchronize(stream), "synchronize");
+   if (rc) return rc;
+   if (st & 1) return set_err(this, VGPU_ERR_NAN, "non-finite or non-normalisable spin produced by the integrator");
+   return VGPU_OK;
+}
+namespace vgpu {
+
+}  // namespace vgpu
+
+void vgpu_ctx::update_sigma_flag() {
+   any_sigma = false;
+   if (!params.thermal_enabled) return;
+   for (const vgpu_material& q : sys.materials) {
+      const double T = params.local_temperature ? q.temperature : params.temperature;
+      if (T > 0.0 && q.H_th_sigma != 0.0) any_sigma = true;
+   }
+}
+namespace vgpu {
+
+}  // namespace vgpu
+
+// ===========================================================================
+// exported C ABI
+// ===========================================================================
+extern "C" const char* vgpu_version(void) { return "vgpu 0.1 sm_100a"; }
+
+extern "C" int vgpu_last_error(vgpu_handle h, char* buf, size_t n) {
+   if (!buf || n == 0) return VGPU_ERR_ARG;
+   std::string s;
+   if (h) s = h->err;
+   else {
+      std::lock_guard<std::mutex> g(g_err_mutex);
+      s = g_global_err;
+   }
+   snprintf(buf, n, "%s", s.c_str());
+   return VGPU_OK;
+}
+
+extern "C" int vgpu_create(int device, int precision, vgpu_handle* out) {
+   if (!out) return set_err(nullptr, VGPU_ERR_ARG, "null output handle");
+   *out = nullptr;
+   if (precision != VGPU_PREC_FP32 && precision != VGPU_PREC_FP64)
+      return set_err(nullptr, VGPU_ERR_ARG, "unknown precision %d", precision);
+   int count = 0;
+   cudaError_t e = cudaGetDeviceCount(&count);
+   if (e != cudaSuccess || count == 0) {
+      cudaGetLastError();
+      return set_err(nullptr, VGPU_ERR_CUDA, "no CUDA device available: %s", cudaGetErrorString(e));
+   }
+   if (device < 0) {
+      e = cudaGetDevice(&device);
+      if (e != cudaSuccess) return cuda_err(nullptr, e, "cudaGetDevice");
+   }
+   if (device >= count) return set_err(nullptr, VGPU_ERR_ARG, "device %d out of range (%d devices)", device, count);
+   if ((e = cudaSetDevice(device)) != cudaSuccess) return cuda_err(nullptr, e, "cudaSetDevice");
+   vgpu_ctx* h = new vgpu_ctx();
+   h->device = device;
+   h->prec = precision;
+   if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+      delete h;
+      return cuda_err(nullptr, e, "cudaStreamCreate");
+   }
+   memset(&h->params, 0, sizeof h->params);
+   h->params.H_vec[2] = 1.0;
+   h->params.applied_enabled = 1;
+   h->params.thermal_enabled = 1;
+   *out = h;
+   return VGPU_OK;
+}
+
+extern "C" int vgpu_destroy(vgpu_handle h) {
+   if (!h) return VGPU_OK;
+   cudaSetDevice(h->device);
+   cudaStreamSynchronize(h->stream);
+   h->destroy_extras();
+   h->free_system();
+   cudaStreamDestroy(h->stream);
+   delete h;
+   return VGPU_OK;
+}
+
+extern "C" int vgpu_upload_system(vgpu_handle h, const vgpu_system_desc* d) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   cudaSetDevice(h->device);
+   int rc = validate(h, d);
+   if (rc) return rc;
+   h->destroy_extras();
+   rc = h->prec == VGPU_PREC_FP64 ? upload_typed<double>(h, d) : upload_typed<float>(h, d);
+   if (rc) return rc;
+   h->update_sigma_flag();
+   return cuda_err(h, cudaStreamSynchronize(h->stream), "upload synchronize");
+}
+
+extern "C" int vgpu_validate_system(const vgpu_system_desc* d) { return validate(nullptr, d); }
+
+extern "C" int vgpu_set_params(vgpu_handle h, const vgpu_sim_params* p) {
+   if (!h || !p) return set_err(h, VGPU_ERR_ARG, "null argument");
+   if (!(p->dt > 0.0) || !std::isfinite(p->dt)) return set_err(h, VGPU_ERR_ARG, "dt must be positive and finite");
+   if (!(p->temperature >= 0.0)) return set_err(h, VGPU_ERR_ARG, "temperature must be >= 0");
+   cudaSetDevice(h->device);
+   h->params = *p;
+   h->update_sigma_flag();
+   return h->refresh_materials();
+}
+
+template <typename R>
+static int set_spins_typed(vgpu_handle h, const double* sx, const double* sy, const double* sz) {
+   const int n = h->sys.n;
+   const double* src[3] = {sx, sy, sz};
+   std::vector<R> buf(n);
+   for (int q = 0; q < 3; ++q) {
+      for (int i = 0; i < n; ++i) buf[i] = (R)src[q][i];
+      int rc = cuda_err(h, cudaMemcpyAsync(h->sys.s[q], buf.data(), n * sizeof(R), cudaMemcpyHostToDevice, h->stream),
+                        "set spins");
+      if (rc) return rc;
+      rc = cuda_err(h, cudaStreamSynchronize(h->stream), "set spins");
+      if (rc) return rc;
+   }
+   return VGPU_OK;
+}
+
+extern "C" int vgpu_set_spins(vgpu_handle h, const double* sx, const double* sy, const double* sz) {
+   if (!h || !sx || !sy || !sz) return set_err(h, VGPU_ERR_ARG, "null argument");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   cudaSetDevice(h->device);
+   return h->prec == VGPU_PREC_FP64 ? set_spins_typed<double>(h, sx, sy, sz) : set_spins_typed<float>(h, sx, sy, sz);
+}
+
+template <typename R>
+static int get_vec_typed(vgpu_handle h, void* const src[3], double* out[3]) {
+   const int n = h->sys.n;
+   std::vector<R> buf(n);
+   for (int q = 0; q < 3; ++q) {
+      int rc = cuda_err(h, cudaMemcpyAsync(buf.data(), src[q], n * sizeof(R), cudaMemcpyDeviceToHost, h->stream),
+                        "download");
+      if (rc) return rc;
+      rc = cuda_err(h, cudaStreamSynchronize(h->stream), "download");
+      if (rc) return rc;
+      for (int i = 0; i < n; ++i) out[q][i] = (double)buf[i];
+   }
+   return VGPU_OK;
+}
+
+extern "C" int vgpu_get_spins(vgpu_handle h, double* sx, double* sy, double* sz) {
+   if (!h || !sx || !sy || !sz) return set_err(h, VGPU_ERR_ARG, "null argument");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   cudaSetDevice(h->device);
+   double* out[3] = {sx, sy, sz};
+   int rc = h->prec == VGPU_PREC_FP64 ? get_vec_typed<double>(h, h->sys.s, out) : get_vec_typed<float>(h, h->sys.s, out);
+   if (rc) return rc;
+   return h->check_status();
+}
+
+extern "C" int vgpu_set_noise(vgpu_handle h, int mode, uint64_t seed) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (mode != VGPU_NOISE_PHILOX && mode != VGPU_NOISE_REPLAY) return set_err(h, VGPU_ERR_ARG, "unknown noise mode %d", mode);
+   if (mode == VGPU_NOISE_REPLAY && !h->sys.xi)
+      return set_err(h, VGPU_ERR_STATE, "replay mode needs vgpu_set_noise_replay first");
+   h->noise_mode = mode;
+   h->seed = seed;
+   return VGPU_OK;
+}
+
+template <typename R>
+static int set_replay_typed(vgpu_handle h, const double* xi) {
+   const size_t m = 3 * (size_t)h->sys.n;
+   if (!h->sys.xi) {
+      h->sys.xi = h->alloc(m * sizeof(R));
+      if (!h->sys.xi) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for replay noise");
+   }
+   std::vector<R> buf(xi, xi + m);
+   int rc = cuda_err(h, cudaMemcpyAsync(h->sys.xi, buf.data(), m * sizeof(R), cudaMemcpyHostToDevice, h->stream), "replay");
+   if (rc) return rc;
+   return cuda_err(h, cudaStreamSynchronize(h->stream), "replay");
+}
+
+extern "C" int vgpu_set_noise_replay(vgpu_handle h, const double* xi) {
+   if (!h || !xi) return set_err(h, VGPU_ERR_ARG, "null argument");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   cudaSetDevice(h->device);
+   int rc = h->prec == VGPU_PREC_FP64 ? set_replay_typed<double>(h, xi) : set_replay_typed<float>(h, xi);
+   if (rc) return rc;
+   h->noise_mode = VGPU_NOISE_REPLAY;
+   return VGPU_OK;
+}
+
+extern "C" int vgpu_set_step(vgpu_handle h, uint64_t step) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   h->step = step;
+   return VGPU_OK;
+}
+
+extern "C" int vgpu_get_step(vgpu_handle h, uint64_t* step) {
+   if (!h || !step) return set_err(h, VGPU_ERR_ARG, "null argument");
+   *step = h->step;
+   return VGPU_OK;
+}
+
+extern "C" int vgpu_llg_heun(vgpu_handle h, uint64_t n_steps) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (!(h->params.dt > 0.0)) return set_err(h, VGPU_ERR_STATE, "vgpu_set_params not called");
+   cudaSetDevice(h->device);
+   return h->prec == VGPU_PREC_FP64 ? llg_steps_typed<double>(h, n_steps) : llg_steps_typed<float>(h, n_steps);
+}
+
+template <typename R>
+static int fields_typed(vgpu_handle h, double* hx, double* hy, double* hz) {
+   SysDev& S = h->sys;
+   if (!S.f[0]) {
+      for (int q = 0; q < 3; ++q) {
+         S.f[q] = h->alloc(S.n_alloc * sizeof(R));
+         if (!S.f[q]) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for field buffer");
+      }
+   }
+   LLGArgs<R> a = make_args<R>(h);
+   cudaError_t e = launch_llg_pass<R>(a, S.fmt, PASS_FIELD, S.nslices, h->stream);
+   if (e != cudaSuccess) return cuda_err(h, e, "field launch");
+   double* out[3] = {hx, hy, hz};
+   return get_vec_typed<R>(h, S.f, out);
+}
+
+extern "C" int vgpu_get_fields(vgpu_handle h, double* hx, double* hy, double* hz) {
+   if (!h || !hx || !hy || !hz) return set_err(h, VGPU_ERR_ARG, "null argument");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   cudaSetDevice(h->device);
+   return h->prec == VGPU_PREC_FP64 ? fields_typed<double>(h, hx, hy, hz) : fields_typed<float>(h, hx, hy, hz);
+}
+
+
+template <typename R>
+static int noise_typed(vgpu_handle h, uint64_t step, double* xi) {
+   SysDev& S = h->sys;
+   if (!S.f[0]) {
+      for (int q = 0; q < 3; ++q) {
+         S.f[q] = h->alloc(S.n_alloc * sizeof(R));
+         if (!S.f[q]) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for field buffer");
+      }
+   }
+   LLGArgs<R> a = make_args<R>(h);
+   a.step = step;
+   a.noise_mode = VGPU_NOISE_PHILOX;
+   cudaError_t e = launch_thermal_noise<R>(a, h->stream);
+   if (e != cudaSuccess) return cuda_err(h, e, "noise launch");
+   const int n = S.n;
+   double* out[3] = {xi, xi + n, xi + 2 * (size_t)n};
+   return get_vec_typed<R>(h, S.f, out);
+}
+
+extern "C" int vgpu_thermal_noise(vgpu_handle h, uint64_t step, double* xi) {
+   if (!h || !xi) return set_err(h, VGPU_ERR_ARG, "null argument");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   cudaSetDevice(h->device);
+   return h->prec == VGPU_PREC_FP64 ? noise_typed<double>(h, step, xi) : noise_typed<float>(h, step, xi);
+}

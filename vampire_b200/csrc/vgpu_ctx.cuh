@@ -1,0 +1,96 @@
+// Context object behind a vgpu_handle.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "vgpu.h"
+#include "vgpu_internal.cuh"
+
+namespace vgpu {
+
+// Device-side system (pointers owned by vgpu_ctx::allocs).
+struct SysDev {
+   bool uploaded = false;
+   int n = 0, M = 1, nslices = 0, n_alloc = 0, fmt = 0;
+   int mat_shift = 0, idx_mask = 0x7fffffff;
+   int64_t num_bonds = 0, sell_entries = 0;
+   int uniaxial = 0, cubic = 0;
+   void* slice_off = nullptr;
+   void* col = nullptr;
+   void* jb[9] = {nullptr};
+   void* jtab = nullptr;
+   void* mat = nullptr;
+   void* mp = nullptr;
+   void* s[3] = {nullptr};   // state A
+   void* p[3] = {nullptr};   // state B (predictor)
+   void* f[3] = {nullptr};   // field output
+   void* xi = nullptr;       // replay noise
+   int* status = nullptr;
+   // macrocell dipole
+   int ncells = 0;
+   void* cell = nullptr;
+   void* cell_field = nullptr;
+   void* hd_atom = nullptr;
+   void* hm_atom = nullptr;  // per-atom mu0 Hd field for the magnetostatic energy
+   std::vector<int> type_host;
+   std::vector<vgpu_material> materials;
+};
+
+int set_err(vgpu_ctx* h, int code, const char* fmt, ...);
+int cuda_err(vgpu_ctx* h, cudaError_t e, const char* what);
+
+// kinds of timed device work (vgpu_profile_read)
+enum ProfKind : int { PROF_PREDICTOR = 0, PROF_CORRECTOR = 1, PROF_STATS = 2, PROF_DIPOLE = 3, PROF_MC = 4,
+                      PROF_OTHER = 5, PROF_KINDS = 6 };
+
+void stats_destroy(vgpu_ctx* h);
+void mc_destroy(vgpu_ctx* h);
+void dipole_destroy(vgpu_ctx* h);
+
+}  // namespace vgpu
+
+struct vgpu_ctx {
+   int device = 0;
+   int prec = VGPU_PREC_FP32;
+   cudaStream_t stream = nullptr;
+   std::string err;
+   std::vector<void*> allocs;
+   vgpu::SysDev sys;
+   vgpu_sim_params params;
+   uint64_t step = 0;
+   uint64_t seed = 0;
+   int noise_mode = VGPU_NOISE_PHILOX;
+   bool any_sigma = false;
+
+   void* alloc(size_t bytes);
+   void free_system();
+   int refresh_materials();
+   int check_status();
+   void update_sigma_flag();
+   // hooks implemented by the other subsystems
+   int after_step();          // dipole cadence (dipole.cu)
+   void destroy_extras();     // free subsystem state (stats, mc, dipole)
+   void* extras[8] = {nullptr};
+
+   // kernel accounting and optional per-launch CUDA-event timing on `stream`
+   int64_t kernel_launches = 0;
+   bool prof_on = false;
+   struct ProfRec { int kind; cudaEvent_t a, b; };
+   std::vector<ProfRec> prof_pending;
+   std::vector<cudaEvent_t> event_pool;
+   double prof_ms[vgpu::PROF_KINDS] = {0};
+   int64_t prof_count[vgpu::PROF_KINDS] = {0};
+   cudaEvent_t prof_open = nullptr;
+   cudaEvent_t get_event();
+   void prof_begin(int kind);
+   void prof_end(int kind);
+   int prof_collect();
+};
+
+namespace vgpu {
+template <typename R> LLGArgs<R> make_args(vgpu_ctx* h);
+}

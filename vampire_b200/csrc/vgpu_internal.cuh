@@ -1,0 +1,82 @@
+// Internal declarations shared by the libvgpu CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "vgpu.h"
+
+namespace vgpu {
+
+// ---------------------------------------------------------------------------
+// Exchange formats of the sliced-ELL (SELL-32) bond storage.  The uploader
+// picks the most compact one that reproduces the reference's per-bond list
+// exactly; the per-bond bytes are what the fused kernels stream from HBM.
+// ---------------------------------------------------------------------------
+enum ExchFmt : int {
+   FMT_ISO_TAB = 0,     // J = table[mi][mj]                         0 B/bond
+   FMT_ISO_BOND = 1,    // scalar per bond                            4 B/bond
+   FMT_VEC_TAB = 2,     // diag(table[mi][mj])                        0 B/bond
+   FMT_VEC_BOND = 3,    // 3 per bond                                12 B/bond
+   FMT_DMI_TAB = 4,     // diag(table[mi][mj]) + d_ij x s_j          12 B/bond
+   FMT_TENSOR_BOND = 5, // full 3x3 per bond                         36 B/bond
+   FMT_COUNT = 6
+};
+
+// Per-material constants in the device precision.
+template <typename R>
+struct MatParams {
+   R A, B;            // one_oneplusalpha_sq, alpha_oneplusalpha_sq
+   R sigma;           // sqrt(T_rescaled) * H_th_sigma
+   R ku2, kux, kuy, kuz;
+   R kc4;
+   R hlx, hly, hlz;   // local applied field (0 if disabled)
+   R mu_s_muB;        // moment in Bohr magnetons (stats)
+};
+
+// Everything one fused LLG pass needs, passed by value.
+template <typename R>
+struct LLGArgs {
+   int n;                    // atoms
+   const int* slice_off;     // [nslices+1] SELL-32 entry offsets
+   const int* col;           // packed neighbour index (| mat << mat_shift)
+   int idx_mask;             // mask of the neighbour index bits
+   int mat_shift;            // shift of the neighbour material bits (0: unpacked)
+   const R* jb[9];           // per-bond exchange arrays in SELL layout
+   const R* jtab;            // material-pair table (M*M or M*M*3)
+   int M;                    // number of materials
+   const int* mat;           // [n] material id, or nullptr when M == 1
+   const MatParams<R>* mp;   // [M]
+   int uniaxial, cubic;
+   R hx, hy, hz;             // global applied field
+   int local_field;          // add MatParams::hl*
+   int thermal;              // add sigma * xi
+   int noise_mode;           // VGPU_NOISE_*
+   uint32_t seed_lo, seed_hi;
+   uint64_t step;            // Philox counter for this step
+   const R* xi;              // replay noise, 3n (x|y|z blocks)
+   const int* cell;          // [n] macrocell id, or nullptr
+   const R* cell_field;      // [3*ncells] x|y|z blocks
+   int ncells;
+   const R* hd_atom;         // [3n] per-atom dipole field (host-computed), or nullptr
+   R dt, half_dt;
+   R* ax; R* ay; R* az;      // state A: s0 (read), s1 (written by corrector)
+   R* bx; R* by; R* bz;      // state B: s' (predictor output)
+   R* fx; R* fy; R* fz;      // field output (field-only mode)
+   int* status;              // device status word (non-finite spin flag)
+};
+
+enum PassMode : int { PASS_PREDICTOR = 0, PASS_CORRECTOR = 1, PASS_FIELD = 2 };
+
+// launch the fused Heun pass for the given format/mode (llg_kernels.cu)
+template <typename R>
+cudaError_t launch_llg_pass(const LLGArgs<R>& a, int fmt, int mode, int nslices, cudaStream_t st);
+
+// write the Philox thermal Gaussians of step a.step into a.fx/fy/fz
+template <typename R>
+cudaError_t launch_thermal_noise(const LLGArgs<R>& a, cudaStream_t st);
+
+}  // namespace vgpu

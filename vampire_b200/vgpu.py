@@ -1,0 +1,293 @@
+"""ctypes binding of libvgpu.so (include/vgpu.h).
+
+This is the Python side of the C ABI; it is what tests, bench.py and the
+PyTorch adjoint wrapper call.  It never falls back to a CPU path: if the
+shared library is missing or no CUDA device is present, calls raise
+:class:`VGPUError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+from .system import MATERIAL_DTYPE, SpinSystem
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libvgpu.so"
+
+OK, ERR_ARG, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_NAN, ERR_STATE = 0, -1, -2, -3, -4, -5, -6
+PREC_FP32, PREC_FP64 = 0, 1
+NOISE_PHILOX, NOISE_REPLAY = 0, 1
+
+_D = C.POINTER(C.c_double)
+_I32 = C.POINTER(C.c_int32)
+
+
+class VGPUError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"vgpu error {code}: {msg}")
+        self.code = code
+
+
+class SystemDesc(C.Structure):
+    _fields_ = [
+        ("num_atoms", C.c_int32), ("num_materials", C.c_int32), ("exchange_type", C.c_int32),
+        ("uniaxial_enabled", C.c_int32), ("cubic_enabled", C.c_int32), ("pad_", C.c_int32),
+        ("num_bonds", C.c_int64), ("nl_start", _I32), ("nl_end", _I32), ("nl", _I32),
+        ("nl_type", _I32), ("num_exchange", C.c_int64), ("jlist", _D), ("type", _I32),
+        ("materials", C.c_void_p), ("sx", _D), ("sy", _D), ("sz", _D),
+    ]
+
+
+class SimParamsC(C.Structure):
+    _fields_ = [
+        ("dt", C.c_double), ("temperature", C.c_double), ("H_applied", C.c_double),
+        ("H_vec", C.c_double * 3), ("thermal_enabled", C.c_int32), ("applied_enabled", C.c_int32),
+        ("local_temperature", C.c_int32), ("local_applied_field", C.c_int32),
+    ]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libvgpu.so (built in-tree by vampire_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise VGPUError(ERR_STATE, f"{LIB_PATH} not built; run python -m vampire_b200.build")
+        _lib = C.CDLL(str(LIB_PATH))
+        _lib.vgpu_version.restype = C.c_char_p
+        _lib.vgpu_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+        for name in ("vgpu_destroy",):
+            getattr(_lib, name).argtypes = [C.c_void_p]
+    return _lib
+
+
+def version() -> str:
+    return lib().vgpu_version().decode()
+
+
+def _last_error(h) -> str:
+    buf = C.create_string_buffer(1024)
+    lib().vgpu_last_error(h, buf, C.c_size_t(len(buf)))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int, h=None) -> None:
+    if rc != OK:
+        raise VGPUError(rc, _last_error(h))
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t) if a is not None else C.cast(None, t)
+
+
+def params_struct(p) -> SimParamsC:
+    c = SimParamsC()
+    c.dt = p.dt
+    c.temperature = p.temperature
+    c.H_applied = p.H_applied
+    for k in range(3):
+        c.H_vec[k] = float(p.H_vec[k])
+    c.thermal_enabled = int(p.thermal)
+    c.applied_enabled = int(p.applied)
+    c.local_temperature = int(p.local_temperature)
+    c.local_applied_field = int(p.local_applied_field)
+    return c
+
+
+def _desc(s: SpinSystem):
+    """Fill a SystemDesc from a SpinSystem; returns (desc, keep-alive dict)."""
+    keep = {}
+
+    def arr(name, a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep[name] = a
+        return a
+
+    d = SystemDesc()
+    d.num_atoms = s.n
+    d.num_materials = s.num_materials
+    d.exchange_type = s.exch_type
+    d.uniaxial_enabled = int(s.uniaxial)
+    d.cubic_enabled = int(s.cubic)
+    d.num_bonds = s.num_bonds
+    d.nl_start = _ptr(arr("st", s.nl_start, np.int32), _I32)
+    d.nl_end = _ptr(arr("en", s.nl_end, np.int32), _I32)
+    d.nl = _ptr(arr("nl", s.nl, np.int32), _I32)
+    if s.nl_type is not None:
+        d.nl_type = _ptr(arr("nt", s.nl_type, np.int32), _I32)
+        w = {0: 1, 1: 3, 2: 9}[s.exch_type]
+        d.num_exchange = s.jlist.size // w
+    else:
+        d.nl_type = C.cast(None, _I32)
+        d.num_exchange = s.num_bonds
+    d.jlist = _ptr(arr("jl", s.jlist, np.float64), _D)
+    d.type = _ptr(arr("ty", s.type, np.int32), _I32)
+    mats = arr("mats", s.materials, MATERIAL_DTYPE)
+    d.materials = mats.ctypes.data
+    sp = arr("sp", s.spins, np.float64)
+    d.sx = _ptr(sp[0], _D)
+    d.sy = _ptr(sp[1], _D)
+    d.sz = _ptr(sp[2], _D)
+    return d, keep
+
+
+def validate_system(s: SpinSystem) -> None:
+    """Host-only descriptor check (vgpu_validate_system); raises VGPUError."""
+    d, keep = _desc(s)
+    check(lib().vgpu_validate_system(C.byref(d)))
+
+
+class Simulation:
+    """One spin system resident on one GPU, driven through the C ABI."""
+
+    def __init__(self, system: SpinSystem, device: int = 0, precision: str = "fp32",
+                 noise_seed: int = 0):
+        self.system = system
+        self.n = system.n
+        self._h = C.c_void_p()
+        prec = PREC_FP64 if precision == "fp64" else PREC_FP32
+        check(lib().vgpu_create(device, prec, C.byref(self._h)))
+        self.upload(system)
+        self.set_params(system.params)
+        self.set_noise(NOISE_PHILOX, noise_seed)
+
+    # -- plumbing ----------------------------------------------------------
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, rc):
+        check(rc, self._h)
+
+    def close(self) -> None:
+        if self._h:
+            lib().vgpu_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- system ------------------------------------------------------------
+    def upload(self, s: SpinSystem) -> None:
+        d, keep = _desc(s)
+        self._check(lib().vgpu_upload_system(self._h, C.byref(d)))
+
+    def set_params(self, p) -> None:
+        c = params_struct(p)
+        self._check(lib().vgpu_set_params(self._h, C.byref(c)))
+
+    # -- spins -------------------------------------------------------------
+    def spins(self) -> np.ndarray:
+        out = np.empty((3, self.n))
+        self._check(lib().vgpu_get_spins(self._h, _ptr(out[0], _D), _ptr(out[1], _D), _ptr(out[2], _D)))
+        return out
+
+    def set_spins(self, s: np.ndarray) -> None:
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        self._check(lib().vgpu_set_spins(self._h, _ptr(s[0], _D), _ptr(s[1], _D), _ptr(s[2], _D)))
+
+    def fields(self) -> np.ndarray:
+        out = np.empty((3, self.n))
+        self._check(lib().vgpu_get_fields(self._h, _ptr(out[0], _D), _ptr(out[1], _D), _ptr(out[2], _D)))
+        return out
+
+    # -- integration -------------------------------------------------------
+    def set_noise(self, mode: int, seed: int = 0) -> None:
+        self._check(lib().vgpu_set_noise(self._h, C.c_int(mode), C.c_uint64(seed)))
+
+    def set_noise_replay(self, xi: np.ndarray) -> None:
+        xi = np.ascontiguousarray(xi, dtype=np.float64)
+        assert xi.size == 3 * self.n
+        self._check(lib().vgpu_set_noise_replay(self._h, _ptr(xi, _D)))
+
+    def thermal_noise(self, step: int) -> np.ndarray:
+        """The 3n Philox Gaussians the kernels use at `step` (x|y|z blocks)."""
+        out = np.empty(3 * self.n)
+        self._check(lib().vgpu_thermal_noise(self._h, C.c_uint64(step), _ptr(out, _D)))
+        return out
+
+    @property
+    def step(self) -> int:
+        v = C.c_uint64()
+        self._check(lib().vgpu_get_step(self._h, C.byref(v)))
+        return v.value
+
+    @step.setter
+    def step(self, v: int) -> None:
+        self._check(lib().vgpu_set_step(self._h, C.c_uint64(v)))
+
+    def llg_heun(self, n_steps: int = 1) -> None:
+        self._check(lib().vgpu_llg_heun(self._h, C.c_uint64(n_steps)))
+
+    # -- statistics --------------------------------------------------------
+    def add_mask(self, mask: np.ndarray, size: int) -> int:
+        m = np.ascontiguousarray(mask, dtype=np.int32)
+        out = C.c_int32()
+        self._check(lib().vgpu_stats_add_mask(self._h, _ptr(m, _I32), C.c_int32(size), C.byref(out)))
+        self._mask_sizes = getattr(self, "_mask_sizes", {})
+        self._mask_sizes[out.value] = size
+        return out.value
+
+    def stats_update(self, magnetization: bool = True, energy: bool = False) -> None:
+        self._check(lib().vgpu_stats_update(self._h, C.c_int32(int(magnetization) | (int(energy) << 1))))
+
+    def magnetization(self, mask_id: int = 0):
+        size = self._mask_sizes[mask_id]
+        m = np.empty(4 * size)
+        mean = np.empty(4 * size)
+        cnt = C.c_int64()
+        self._check(lib().vgpu_stats_get_magnetization(self._h, C.c_int32(mask_id), _ptr(m, _D), _ptr(mean, _D),
+                                                       C.byref(cnt)))
+        return m, mean, cnt.value
+
+    def energy(self, mask_id: int = 0):
+        size = self._mask_sizes[mask_id]
+        e = np.empty(5 * size)
+        mean = np.empty(5 * size)
+        cnt = C.c_int64()
+        self._check(lib().vgpu_stats_get_energy(self._h, C.c_int32(mask_id), _ptr(e, _D), _ptr(mean, _D),
+                                                C.byref(cnt)))
+        return e, mean, cnt.value
+
+    def stats_reset(self) -> None:
+        self._check(lib().vgpu_stats_reset(self._h))
+
+    # -- streams and timing -----------------------------------------------
+    def stream_ptr(self) -> int:
+        p = C.c_void_p()
+        self._check(lib().vgpu_get_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+    def synchronize(self) -> None:
+        self._check(lib().vgpu_synchronize(self._h))
+
+    def profile(self, enable: bool) -> None:
+        self._check(lib().vgpu_profile(self._h, C.c_int(int(enable))))
+
+    PROF_KINDS = ("predictor", "corrector", "statistics", "dipole", "monte_carlo", "other")
+
+    def profile_read(self) -> dict:
+        ms = np.zeros(6)
+        cnt = np.zeros(6, dtype=np.int64)
+        launches = C.c_int64()
+        self._check(lib().vgpu_profile_read(self._h, _ptr(ms, _D), cnt.ctypes.data_as(C.POINTER(C.c_int64)),
+                                            C.c_int32(6), C.byref(launches)))
+        out = {k: {"ms": float(ms[i]), "count": int(cnt[i])} for i, k in enumerate(self.PROF_KINDS)}
+        out["kernel_launches"] = launches.value
+        return out
