@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--L", type=int, default=100, help="FCC cells per side (100 = 4M spins)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-dipole", action="store_true", help="leave out the macrocell dipole field")
     ap.add_argument("--e2e-steps", type=int, default=200)
     return ap.parse_args()
 
@@ -52,6 +53,7 @@ def workload_config(L, n_gpus):
     return {"workload": f"FCC {L}^3 LLG-Heun, tensor exchange + 3-site DMI, 2 materials, cubic Kc, T=300K",
             "spins_per_gpu": 4 * L ** 3, "lattice": "fcc", "cells": [L, L, L], "a_nm": 0.354,
             "materials": 2, "exchange": "tensor+DMI (nn, z=12)", "anisotropy": "cubic", "temperature_K": 300.0,
+            "dipole": "macrocells 2x2x2 unit cells (125,000 at L=100), tensor solver, update every 100 steps",
             "dt_s": 1e-16, "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single GPU",
             "l2": "inputs larger than L2 (state 96 MB + topology 960 MB per GPU)"}
 
@@ -186,8 +188,10 @@ def main():
     from vampire_b200 import vgpu
     vbuild.build()
     torch.cuda.set_device(local)
-    sysm = S.config_fcc_tensor(L=args.L, seed=2024 + rank)
+    sysm = S.config_fcc_tensor(L=args.L, seed=2024 + rank, dipole=not args.no_dipole)
     sim = vgpu.Simulation(sysm, device=local, precision="fp32", noise_seed=1000 + rank)
+    if sysm.cells is not None:
+        sim.dipole_setup(sysm.cells)
     mask_id = sim.add_mask(*sysm.masks["system"])
     stream = torch.cuda.ExternalStream(sim.stream_ptr(), device=local)
 
@@ -226,7 +230,7 @@ def main():
     value = n * args.steps * world / (ms * 1e-3)
 
     # --- roofline of the dominant kernel --------------------------------
-    bm = byte_model()
+    bm = byte_model(dipole=sysm.cells is not None)
     kern = max(("predictor", "corrector"), key=lambda k: prof[k]["ms"])
     avg_ms = prof[kern]["ms"] / max(1, prof[kern]["count"])
     peak, peak_kind = measured_peak_hbm()

@@ -164,6 +164,13 @@ int vgpu_get_spins(vgpu_handle h, double* sx, double* sy, double* sz);
 int vgpu_set_noise(vgpu_handle h, int mode, uint64_t seed);
 int vgpu_set_noise_replay(vgpu_handle h, const double* xi);
 
+/* Options.  VGPU_OPT_STORE_INCREMENT: 1 = the predictor stores f(s0) for the
+ * corrector (3 extra arrays, +24 B per spin-step), 0 = the corrector recovers
+ * f(s0) dt = s'|s0|^2/(s'.s0) - s0 from the two states it reads anyway;
+ * -1 (default) = store in FP64 (bit-exact with the reference), recover in FP32. */
+#define VGPU_OPT_STORE_INCREMENT 1
+int vgpu_set_option(vgpu_handle h, int option, int value);
+
 /* Step counter that keys the Philox stream (counter = (atom, step)).  Resume
  * from a checkpoint by restoring it. */
 int vgpu_set_step(vgpu_handle h, uint64_t step);
@@ -182,6 +189,81 @@ int vgpu_thermal_noise(vgpu_handle h, uint64_t step, double* xi);
 /* Total (spin + external) field the predictor sees at the current spins, in
  * Tesla, with thermal noise excluded (debug/parity aid). */
 int vgpu_get_fields(vgpu_handle h, double* hx, double* hy, double* hz);
+
+/* ---- macrocell dipole field ---------------------------------------------- */
+
+#define VGPU_DIPOLE_MACROCELL 0   /* bare point dipoles, self term 0 (dipole/macrocell.cpp)   */
+#define VGPU_DIPOLE_TENSOR    1   /* atomistic tensors within cutoff (dipole/tensor.cpp)      */
+
+/* Macrocells as the reference's cells:: module builds them
+ * (src/cells/initialize.cpp:189-265). */
+typedef struct {
+   int32_t num_cells;              /* cells::num_cells                                   */
+   int32_t solver;                 /* VGPU_DIPOLE_*  (dipole::internal::solver)          */
+   int32_t update_rate;            /* steps between updates (dipole::update_rate); 0: never */
+   int32_t pad_;
+   double macro_cell_size;         /* cells::macro_cell_size [Angstrom]                  */
+   double cutoff;                  /* dipole::cutoff [macrocell sizes]                   */
+   const int32_t* atom_cell;       /* [num_atoms] cells::atom_cell_id_array              */
+   const double* cell_pos_mom;     /* [4*num_cells] cells::pos_and_mom_array             */
+   const double* cell_volume;      /* [num_cells] cells::volume_array [Angstrom^3]       */
+   const int32_t* cell_natoms;     /* [num_cells] cells::num_atoms_in_cell               */
+   const double* atom_x;           /* [num_atoms] atomic coordinates [Angstrom]          */
+   const double* atom_y;           /*   (tensor solver only; else may be NULL)           */
+   const double* atom_z;
+} vgpu_dipole_desc;
+
+/* Enable the device dipole solver and compute the field at the current spins
+ * (dipole::initialize, src/dipole/initialize.cpp:143).  vgpu_llg_heun then
+ * recomputes it every update_rate steps (dipole::calculate_field,
+ * src/dipole/field.cpp:43-87) without leaving the device: cell moments
+ * (cells::mag, src/cells/mag.cpp:35-77) and cell fields
+ * (dipole::internal::update_field, src/dipole/update.cpp:37-105) replace the
+ * reference's D2H-CPU-H2D round trip and its O(Nc^2) dense tensors. */
+int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* desc);
+
+/* Recompute cell moments and fields now. */
+int vgpu_dipole_update(vgpu_handle h);
+
+/* Cell moments [3*num_cells, J/T, x|y|z], B field and mu0 Hd field
+ * [3*num_cells, Tesla] of the last update (cells::mag_array_*,
+ * dipole::cells_field_array_*, dipole::cells_mu0Hd_field_array_*); any
+ * output may be NULL. */
+int vgpu_dipole_get_cells(vgpu_handle h, double* mag, double* b_field, double* hd_field);
+
+/* Host-computed per-atom dipole B field (and mu0 Hd field for energies; NULL
+ * = zero): the reference's vcuda::transfer_dipole_fields_from_cpu_to_gpu
+ * path, for hosts that keep the CPU dipole solver. */
+int vgpu_set_dipole_field(vgpu_handle h, const double* bx, const double* by, const double* bz,
+                          const double* hx, const double* hy, const double* hz);
+
+/* ---- Metropolis Monte Carlo (checkerboard) ------------------------------ */
+
+/* Colour the exchange graph for the parallel sweep: colour_in[num_atoms]
+ * (checked: no two interacting atoms share a colour) or NULL for a host
+ * greedy colouring.  The reference has no GPU Monte Carlo; this backs the
+ * gpu::mc_step() entry the simulate loop gains (src/simulate/sim.cpp:608-614
+ * calls montecarlo::mc_step, src/montecarlo/mc.cpp:29-127). */
+int vgpu_mc_setup(vgpu_handle h, const int32_t* colour_in, int32_t* n_colours_out);
+
+/* The colour of every atom chosen by vgpu_mc_setup. */
+int vgpu_mc_get_colours(vgpu_handle h, int32_t* colour);
+
+/* Replay mode: the next sweeps use these 4*num_atoms numbers (x|y|z move
+ * Gaussians, then acceptance uniforms); NULL returns to Philox. */
+int vgpu_mc_set_replay(vgpu_handle h, const double* rnd);
+
+/* n_sweeps sweeps of angle moves (mc_angle, src/montecarlo/mc_moves.cpp:71-87,
+ * sigma = 0.08 (kB T/muB)^0.2, or 0.02 below 1 K; mc.cpp:45-53) at the
+ * temperature of vgpu_set_params; one launch per colour. */
+int vgpu_mc_sweep(vgpu_handle h, uint64_t n_sweeps);
+
+/* Sweep counter keying the Philox stream. */
+int vgpu_mc_set_sweep(vgpu_handle h, uint64_t sweep);
+
+/* Attempted and rejected moves since vgpu_mc_setup
+ * (sim::mc_statistics_moves / mc_statistics_reject). */
+int vgpu_mc_counters(vgpu_handle h, double* moves, double* rejects);
 
 /* ---- statistics (masked reductions, FP64) -------------------------------- */
 

@@ -149,6 +149,36 @@ class OracleSystem:
                                    _p(h[2], _D))
         return h
 
+    def mc_params(self):
+        """Per-material (sigma, kBTBohr, mu_s/muB) of the angle move
+        (src/montecarlo/mc.cpp:45-53) at the system temperature."""
+        p, m = self.s.params, self.s.materials
+        sig, beta, ratio = [], [], []
+        for k in range(m.size):
+            T = m[k]["temperature"] if p.local_temperature else p.temperature
+            a, Tc = m[k]["temperature_rescaling_alpha"], m[k]["temperature_rescaling_Tc"]
+            Tr = Tc * (T / Tc) ** a if T < Tc else T
+            b = 9.27400915e-24 / (Tr * 1.3806503e-23) if Tr > 0 else np.inf
+            sig.append(0.02 if Tr < 1.0 else (1.0 / b) ** 0.2 * 0.08)
+            beta.append(b)
+            ratio.append(m[k]["mu_s_SI"] * 1.07828231e23)
+        return np.array(sig), np.array(beta), np.array(ratio)
+
+    def mc_colour_sweep(self, spins, colour, rnd):
+        """One colour-ordered Metropolis sweep with given random numbers (4n)."""
+        s = np.ascontiguousarray(spins, dtype=np.float64).copy()
+        colour = np.asarray(colour)
+        nc = int(colour.max()) + 1
+        order = np.ascontiguousarray(np.argsort(colour, kind="stable"), dtype=np.int32)
+        off = np.ascontiguousarray(np.r_[0, np.cumsum(np.bincount(colour, minlength=nc))], dtype=np.int32)
+        sig, beta, ratio = self.mc_params()
+        r = np.ascontiguousarray(rnd, dtype=np.float64)
+        lib().vref_mc_colour_sweep.restype = C.c_long
+        rej = lib().vref_mc_colour_sweep(C.byref(self.st), _p(s[0], _D), _p(s[1], _D), _p(s[2], _D),
+                                         _p(order, _I), _p(off, _I), C.c_int(nc), _p(r, _D), _p(sig, _D),
+                                         _p(beta, _D), _p(ratio, _D))
+        return s, int(rej)
+
     def magnetization(self, spins, mask, size) -> np.ndarray:
         s = np.ascontiguousarray(spins, dtype=np.float64)
         mm = np.ascontiguousarray(self.s.mu_s_muB(), dtype=np.float64)

@@ -225,6 +225,44 @@ void vref_spin_energy(const vref_sys* s, const double* sx, const double* sy, con
    e[3] = s->hmx ? -(s->hmx[atom] * Sx + s->hmy[atom] * Sy + s->hmz[atom] * Sz) : 0.0;
 }
 
+/* One colour-ordered Metropolis sweep with given random numbers: the
+ * reference's per-trial rule (montecarlo::mc_step, src/montecarlo/mc.cpp:59-110,
+ * mc_angle, src/montecarlo/mc_moves.cpp:71-87) applied to the sites of
+ * colour 0, then colour 1, ... (order[colour_off[c] .. colour_off[c+1]]).
+ * rnd: 4n values, x|y|z Gaussians then the acceptance uniform, per site.
+ * sigma/beta/ratio per material: move width, muB/(kB T), mu_s/muB.
+ * Returns the number of rejected trials. */
+long vref_mc_colour_sweep(const vref_sys* s, double* sx, double* sy, double* sz, const int* order,
+                          const int* colour_off, int ncolours, const double* rnd, const double* sigma,
+                          const double* beta, const double* ratio) {
+   const int n = s->n;
+   long rejects = 0;
+   for (int c = 0; c < ncolours; ++c) {
+      for (int k = colour_off[c]; k < colour_off[c + 1]; ++k) {
+         const int atom = order[k];
+         const int m = s->type[atom];
+         const double S[3] = {sx[atom], sy[atom], sz[atom]};
+         double T[3] = {S[0] + rnd[atom] * sigma[m], S[1] + rnd[n + atom] * sigma[m], S[2] + rnd[2 * n + atom] * sigma[m]};
+         const double r = 1.0 / sqrt(T[0] * T[0] + T[1] * T[1] + T[2] * T[2]);
+         T[0] *= r; T[1] *= r; T[2] *= r;
+         double eo[4], en[4];
+         vref_spin_energy(s, sx, sy, sz, atom, S[0], S[1], S[2], eo);
+         vref_spin_energy(s, sx, sy, sz, atom, T[0], T[1], T[2], en);
+         const double Eold = eo[0] + eo[1] + eo[2] + eo[3];
+         const double Enew = en[0] + en[1] + en[2] + en[3];
+         const double DE = (Enew - Eold) * ratio[m];
+         int accept = DE < 0;
+         if (!accept) accept = exp(-DE * beta[m]) >= rnd[3 * n + atom];
+         if (accept) {
+            sx[atom] = T[0]; sy[atom] = T[1]; sz[atom] = T[2];
+         } else {
+            rejects++;
+         }
+      }
+   }
+   return rejects;
+}
+
 /* magnetization_statistic_t::calculate_magnetization
  * (src/statistics/magnetization.cpp:134-180): per mask bin sum(mu s), sum(mu),
  * normalised to (m_hat, |m|/m_sat); empty bins zeroed.  out: 4*mask_size. */

@@ -49,6 +49,9 @@ void vref_llg_heun(const vref_sys* s, double* sx, double* sy, double* sz, const 
                    int64_t n_steps);
 void vref_spin_energy(const vref_sys* s, const double* sx, const double* sy, const double* sz,
                       int atom, double Sx, double Sy, double Sz, double* e);
+long vref_mc_colour_sweep(const vref_sys* s, double* sx, double* sy, double* sz, const int* order,
+                          const int* colour_off, int ncolours, const double* rnd, const double* sigma,
+                          const double* beta, const double* ratio);
 void vref_magnetization(int n, const int* mask, int mask_size, const double* sx, const double* sy,
                         const double* sz, const double* mm, double* out);
 void vref_energy(const vref_sys* s, const int* mask, int mask_size, const double* sx,

@@ -1,0 +1,125 @@
+"""Checkerboard Metropolis Monte Carlo (K3) against the reference.
+
+* colouring: no two interacting atoms share a colour (host check);
+* deterministic: one colour-ordered sweep with replayed random numbers equals
+  the oracle's restatement of the reference acceptance rule;
+* statistical: the GPU checkerboard sweep reproduces the reference's
+  sequential random-site Metropolis m(T) within 3 standard errors at every
+  temperature, and Tc within 1% (tests/golden/mc_sc16_curie.npz, produced by
+  the reference's own montecarlo::mc_step).
+"""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _colour_ok(s, colour):
+    cnt = s.nl_end - s.nl_start + 1
+    ai = np.repeat(np.arange(s.n), cnt)
+    return not np.any((colour[ai] == colour[s.nl]) & (ai != s.nl))
+
+
+@pytest.mark.parametrize("name,maxc", [("sc8_t0", 2), ("fcc4_dmi_t0", 8), ("sc6_open_t300", 2)])
+def test_colouring(vgpu_lib, name, maxc):
+    from vampire_b200 import vgpu
+    s, _ = load_golden(name)
+    with vgpu.Simulation(s) as sim:
+        nc = sim.mc_setup()
+        col = sim.mc_colours()
+    assert 2 <= nc <= maxc
+    assert _colour_ok(s, col)
+
+
+def test_bad_colouring_rejected(vgpu_lib):
+    from vampire_b200 import vgpu
+    s, _ = load_golden("sc8_t0")
+    with vgpu.Simulation(s) as sim:
+        with pytest.raises(vgpu.VGPUError) as e:
+            sim.mc_setup(np.zeros(s.n, dtype=np.int32))
+        assert "conflict" in str(e.value)
+
+
+@pytest.mark.parametrize("name", ["sc10_t300", "fcc4_dmi_t300", "sc6_open_t300"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_replayed_sweep_matches_oracle(vgpu_lib, name, prec):
+    from oracle import oracle as O
+    from vampire_b200 import vgpu
+    s, _ = load_golden(name)
+    s.params.temperature = 300.0
+    rng = np.random.default_rng(3)
+    o = O.OracleSystem(s)
+    with vgpu.Simulation(s, precision=prec) as sim:
+        sim.mc_setup()
+        col = sim.mc_colours()
+        spins = s.spins.copy()
+        for sweep in range(3):
+            rnd = np.concatenate([rng.standard_normal(3 * s.n), rng.random(s.n)])
+            sim.mc_set_replay(rnd)
+            sim.mc_sweep(1)
+            spins, rej = o.mc_colour_sweep(spins, col, rnd)
+            got = sim.spins()
+            diff = np.abs(got - spins).max(axis=0)
+            if prec == "fp64":
+                assert diff.max() < 1e-12
+            else:
+                # an FP32 acceptance decision may flip only for a trial at the
+                # threshold to within rounding; allow at most one such site
+                assert np.sum(diff > 1e-5) <= 1
+                spins = got  # continue from the GPU state
+        moves, rejects = sim.mc_counters()
+        assert moves == 3 * s.n
+        assert 0 < rejects < moves
+
+
+def _tc_fit(T, m):
+    from scipy.optimize import curve_fit
+    sel = (m > 0.3) & (T > 0)
+    f = lambda t, tc, b, a: a * np.clip(1 - t / tc, 1e-12, None) ** b
+    p, _ = curve_fit(f, T[sel], m[sel], p0=(1.05 * T[sel].max(), 0.35, 1.0), maxfev=20000)
+    return p[0]
+
+
+def _blocking(x, nb=20):
+    b = x[: len(x) // nb * nb].reshape(nb, -1).mean(1)
+    return x.mean(), b.std(ddof=1) / np.sqrt(nb)
+
+
+def test_curie_sweep_matches_reference_statistically(vgpu_lib):
+    from vampire_b200 import vgpu
+    from oracle import oracle as O
+    d = dict(np.load(GOLDEN / "mc_sc16_curie.npz"))
+    s = O.system_from_dump(d)
+    s.params.H_applied = 0.0
+    s.spins = np.tile(np.array([[0.0], [0.0], [1.0]]), (1, s.n))
+    eq, av, every = 2000, 12000, 10
+    got, se = [], []
+    with vgpu.Simulation(s, noise_seed=77) as sim:
+        mid = sim.add_mask(*s.masks["system"])
+        sim.mc_setup()
+        for T in d["T"]:
+            s.params.temperature = float(T)
+            sim.set_params(s.params)
+            sim.set_spins(s.spins)
+            sim.mc_sweep(eq)
+            tr = []
+            for _ in range(av // every):
+                sim.mc_sweep(every)
+                sim.stats_update(magnetization=True)
+                m, _, _ = sim.magnetization(mid)
+                tr.append(m[3])
+            mu, e = _blocking(np.array(tr))
+            got.append(mu)
+            se.append(e)
+    got, se = np.array(got), np.array(se)
+    ref, rse = d["m_mean"], d["m_se"]
+    z = np.abs(got - ref) / np.sqrt(se ** 2 + rse ** 2 + 1e-18)
+    print("m_gpu", np.round(got, 4))
+    print("m_ref", np.round(ref, 4))
+    print("z", np.round(z, 2))
+    assert np.all(z <= 3.0), z
+    tc_g, tc_r = _tc_fit(d["T"], got), _tc_fit(d["T"], ref)
+    print(f"Tc gpu {tc_g:.1f} K, reference {tc_r:.1f} K")
+    assert abs(tc_g - tc_r) / tc_r < 0.01

@@ -50,6 +50,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     for src in sources():
         obj = objdir / (src.stem + ".o")
         cmd = [NVCC, "-c", str(src), "-o", str(obj)] + ARCH + FLAGS
+        if src.stem.endswith("_fp64"):
+            cmd += ["-fmad=false"]  # FP64 rounding as the reference's non-FMA x86-64 build
         if verbose:
             cmd += ["-Xptxas", "-v"]
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))

@@ -1,8 +1,477 @@
-// Macrocell dipole field (K5 cell moments, K6 cell-cell field).
+// Macrocell dipole field: K5 cell moments and K6 cell-cell field.
+//
+// Reference: dipole::calculate_field (src/dipole/field.cpp:43-141) ->
+// cells::mag (src/cells/mag.cpp:35-77) -> dipole::internal::update_field
+// (src/dipole/update.cpp:37-105), with the interaction tensors of the tensor
+// solver (src/dipole/tensor.cpp:40, inter.cpp:40-150, intra.cpp:40-140) or the
+// macrocell solver (src/dipole/macrocell.cpp:175-225).  The reference stores
+// six dense Nc x Nc FP64 matrices (src/dipole/memory.cpp:29-56), 750 GB at
+// 125,000 cells; its GPU version is disabled.  Here nothing dense is stored:
+//
+//   K5  one warp per cell sums mu_s s over the cell's atoms (cell-sorted atom
+//       list, FP64), giving the cell moments in J/T and in mu_B for K6;
+//   K6  every target cell runs over all source cells in 256-cell shared-memory
+//       tiles and adds the bare point-dipole term (3 e e - 1)/r^3 m_j in FP32,
+//       folding each tile's sum into FP64;
+//   K6n for the pairs within `cutoff` macrocell sizes (tensor solver) the
+//       atomistic tensors of inter.cpp/intra.cpp minus the bare term are
+//       precomputed once in FP64 (one block per pair) and added in FP64.
+//
+// B = 0.9274 sum_j T_ij m_j (self term times 0) and mu0 Hd = 0.9274 (sum_j
+// T_ij m_j - 0.5 (8 pi / 3 V_i) m_i), as update.cpp:56-99.  Atoms read their
+// cell's field through the cell id in the fused LLG passes; atoms of
+// non-magnetic materials and of empty cells read a zero row.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <unordered_map>
+#include <vector>
+
 #include "vgpu_ctx.cuh"
 
 namespace vgpu {
-void dipole_destroy(vgpu_ctx* h) { (void)h; }
+
+struct DipoleState {
+   int nc = 0;
+   int solver = 1;
+   int update_rate = 100;
+   double size = 0.0, cutoff = 2.0;
+   int* cell_start = nullptr;   // [nc+1] offsets into cell_atoms
+   int* cell_atoms = nullptr;   // atoms sorted by cell (magnetic atoms only)
+   double* mag = nullptr;       // [3][nc] cell moment, J/T
+   float4* pos = nullptr;       // [nc] centre (Angstrom), w = 1 if the cell has atoms
+   float4* mom = nullptr;       // [nc] moment in mu_B
+   double* field = nullptr;     // [6][nc] B (3) and mu0 Hd (3), FP64
+   double* self = nullptr;      // [nc] 8 pi / (3 V)
+   int* near_start = nullptr;   // [nc+1]
+   int* near_j = nullptr;       // [npairs]
+   double* near_t = nullptr;    // [6][npairs] T_near - T_bare (xx, xy, xz, yy, yz, zz)
+   int npairs = 0;
+   void* table_b = nullptr;     // [3][nc+1] R, cell B field for the LLG passes
+   void* table_hd = nullptr;    // [3][nc+1] R, cell mu0 Hd field (energies)
+   int* atom_cell = nullptr;    // [n] cell id or nc (zero row)
+   std::vector<double> mus_host;
+};
+
+static DipoleState* dip_of(vgpu_ctx* h) { return (DipoleState*)h->extras[2]; }
+
+// K5: cell moments (cells.cpp mag()), FP64.
+template <typename R>
+__global__ void cell_moment_kernel(int nc, const int* __restrict__ start, const int* __restrict__ atoms,
+                                   const R* __restrict__ sx, const R* __restrict__ sy, const R* __restrict__ sz,
+                                   const int* __restrict__ mat, const MatParams<R>* __restrict__ mp,
+                                   const double* __restrict__ mus_SI, double* __restrict__ mag,
+                                   const float4* __restrict__ pos, float4* __restrict__ mom) {
+   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int lane = threadIdx.x & 31;
+   if (warp >= nc) return;
+   double mx = 0.0, my = 0.0, mz = 0.0;
+   for (int k = start[warp] + lane; k < start[warp + 1]; k += 32) {
+      const int i = atoms[k];
+      const double mu = mus_SI[mat ? mat[i] : 0];
+      mx += (double)sx[i] * mu;
+      my += (double)sy[i] * mu;
+      mz += (double)sz[i] * mu;
+   }
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) {
+      mx += __shfl_xor_sync(0xffffffffu, mx, o);
+      my += __shfl_xor_sync(0xffffffffu, my, o);
+      mz += __shfl_xor_sync(0xffffffffu, mz, o);
+   }
+   if (lane == 0) {
+      mag[warp] = mx; mag[nc + warp] = my; mag[2 * nc + warp] = mz;
+      const double imuB = 1.0 / 9.27400915e-24;
+      mom[warp] = make_float4((float)(mx * imuB), (float)(my * imuB), (float)(mz * imuB), 0.f);
+   }
+}
+
+// K6: far field by tiled all-pairs sum (FP32 terms, FP64 across tiles).
+__global__ void __launch_bounds__(256) cell_field_kernel(int nc, const float4* __restrict__ pos,
+                                                         const float4* __restrict__ mom,
+                                                         double* __restrict__ field) {
+   __shared__ float4 sp[256];
+   __shared__ float4 sm[256];
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   const float4 pi = i < nc ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+   double ax = 0.0, ay = 0.0, az = 0.0;
+   for (int base = 0; base < nc; base += 256) {
+      const int j = base + threadIdx.x;
+      sp[threadIdx.x] = j < nc ? pos[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+      sm[threadIdx.x] = j < nc ? mom[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+      __syncthreads();
+      float fx = 0.f, fy = 0.f, fz = 0.f;
+      const int cnt = min(256, nc - base);
+      for (int k = 0; k < cnt; ++k) {
+         const float4 pj = sp[k];
+         if (pj.w == 0.f || base + k == i) continue;
+         const float4 mj = sm[k];
+         const float rx = pj.x - pi.x, ry = pj.y - pi.y, rz = pj.z - pi.z;
+         const float r2 = rx * rx + ry * ry + rz * rz;
+         const float ri = rsqrtf(r2);
+         const float ri2 = ri * ri;
+         const float ri3 = ri2 * ri;
+         const float mr = 3.f * (mj.x * rx + mj.y * ry + mj.z * rz) * ri2;
+         fx += (mr * rx - mj.x) * ri3;
+         fy += (mr * ry - mj.y) * ri3;
+         fz += (mr * rz - mj.z) * ri3;
+      }
+      ax += fx; ay += fy; az += fz;
+      __syncthreads();
+   }
+   if (i < nc) {
+      field[i] = ax; field[nc + i] = ay; field[2 * nc + i] = az;
+   }
+}
+
+// near-field correction and final scaling (update.cpp:56-99)
+template <typename R>
+__global__ void cell_finish_kernel(int nc, const int* __restrict__ near_start, const int* __restrict__ near_j,
+                                   const double* __restrict__ near_t, int npairs, const double* __restrict__ mag,
+                                   const double* __restrict__ self, const float4* __restrict__ pos,
+                                   double* __restrict__ field, R* __restrict__ tb, R* __restrict__ thd) {
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i > nc) return;
+   if (i == nc) {  // zero row read by non-magnetic atoms
+      for (int q = 0; q < 3; ++q) { tb[q * (nc + 1) + nc] = (R)0; thd[q * (nc + 1) + nc] = (R)0; }
+      return;
+   }
+   const double imuB = 1.0 / 9.27400915e-24;
+   double fx = field[i], fy = field[nc + i], fz = field[2 * nc + i];
+   if (near_start) {
+      for (int k = near_start[i]; k < near_start[i + 1]; ++k) {
+         const int j = near_j[k];
+         const double mx = mag[j] * imuB, my = mag[nc + j] * imuB, mz = mag[2 * nc + j] * imuB;
+         const double txx = near_t[k], txy = near_t[npairs + k], txz = near_t[2 * npairs + k];
+         const double tyy = near_t[3 * npairs + k], tyz = near_t[4 * npairs + k], tzz = near_t[5 * npairs + k];
+         fx += mx * txx + my * txy + mz * txz;
+         fy += mx * txy + my * tyy + mz * tyz;
+         fz += mx * txz + my * tyz + mz * tzz;
+      }
+   }
+   const double k = 9.27400915e-01;
+   const bool has = pos[i].w != 0.f;
+   const double sd = self[i];
+   const double mxi = mag[i] * imuB, myi = mag[nc + i] * imuB, mzi = mag[2 * nc + i] * imuB;
+   const double bx = has ? fx * k : 0.0, by = has ? fy * k : 0.0, bz = has ? fz * k : 0.0;
+   const double hx = has ? (fx - 0.5 * sd * mxi) * k : 0.0;
+   const double hy = has ? (fy - 0.5 * sd * myi) * k : 0.0;
+   const double hz = has ? (fz - 0.5 * sd * mzi) * k : 0.0;
+   field[i] = bx; field[nc + i] = by; field[2 * nc + i] = bz;
+   field[3 * nc + i] = hx; field[4 * nc + i] = hy; field[5 * nc + i] = hz;
+   tb[i] = (R)bx; tb[(nc + 1) + i] = (R)by; tb[2 * (nc + 1) + i] = (R)bz;
+   thd[i] = (R)hx; thd[(nc + 1) + i] = (R)hy; thd[2 * (nc + 1) + i] = (R)hz;
+}
+
+// atomistic near tensors (inter.cpp:83-146, intra.cpp:54-138) minus the bare
+// term of inter.cpp:66-80; one block per (target, source) pair, FP64
+__global__ void near_tensor_kernel(int npairs, const int* __restrict__ pair_i, const int* __restrict__ pair_j,
+                                   const int* __restrict__ cstart, const double* __restrict__ ax,
+                                   const double* __restrict__ ay, const double* __restrict__ az,
+                                   const double* __restrict__ cpos, double* __restrict__ out) {
+   const int p = blockIdx.x;
+   if (p >= npairs) return;
+   const int ci = pair_i[p], cj = pair_j[p];
+   const int i0 = cstart[ci], ni = cstart[ci + 1] - i0;
+   const int j0 = cstart[cj], nj = cstart[cj + 1] - j0;
+   double t[6] = {0, 0, 0, 0, 0, 0};
+   for (int q = threadIdx.x; q < ni * nj; q += blockDim.x) {
+      const int a = i0 + q / nj, b = j0 + q % nj;
+      if (ci == cj && a == b) continue;
+      const double rx = ax[b] - ax[a], ry = ay[b] - ay[a], rz = az[b] - az[a];
+      const double rij = 1.0 / sqrt(rx * rx + ry * ry + rz * rz);
+      const double ex = rx * rij, ey = ry * rij, ez = rz * rij;
+      const double r3 = rij * rij * rij;
+      t[0] += (3.0 * ex * ex - 1.0) * r3;
+      t[1] += (3.0 * ex * ey) * r3;
+      t[2] += (3.0 * ex * ez) * r3;
+      t[3] += (3.0 * ey * ey - 1.0) * r3;
+      t[4] += (3.0 * ey * ez) * r3;
+      t[5] += (3.0 * ez * ez - 1.0) * r3;
+   }
+   __shared__ double red[6][256];
+   for (int k = 0; k < 6; ++k) red[k][threadIdx.x] = t[k];
+   __syncthreads();
+   for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s)
+         for (int k = 0; k < 6; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + s];
+      __syncthreads();
+   }
+   if (threadIdx.x == 0) {
+      const double norm = (double)ni * (double)nj;
+      double bare[6] = {0, 0, 0, 0, 0, 0};
+      if (ci != cj) {
+         // the far-field term K6 already added for this pair, taken out again
+         const float rx = (float)cpos[4 * cj] - (float)cpos[4 * ci];
+         const float ry = (float)cpos[4 * cj + 1] - (float)cpos[4 * ci + 1];
+         const float rz = (float)cpos[4 * cj + 2] - (float)cpos[4 * ci + 2];
+         const double r = sqrt((double)rx * rx + (double)ry * ry + (double)rz * rz);
+         const double ri = 1.0 / r, ex = rx * ri, ey = ry * ri, ez = rz * ri, r3 = ri * ri * ri;
+         bare[0] = (3.0 * ex * ex - 1.0) * r3; bare[1] = 3.0 * ex * ey * r3; bare[2] = 3.0 * ex * ez * r3;
+         bare[3] = (3.0 * ey * ey - 1.0) * r3; bare[4] = 3.0 * ey * ez * r3; bare[5] = (3.0 * ez * ez - 1.0) * r3;
+      }
+      for (int k = 0; k < 6; ++k) out[k * npairs + p] = red[k][0] / norm - bare[k];
+   }
+}
+
+void dipole_destroy(vgpu_ctx* h) {
+   DipoleState* d = dip_of(h);
+   if (!d) return;
+   cudaFree(d->cell_start); cudaFree(d->cell_atoms); cudaFree(d->mag); cudaFree(d->pos); cudaFree(d->mom);
+   cudaFree(d->field); cudaFree(d->self); cudaFree(d->near_start); cudaFree(d->near_j); cudaFree(d->near_t);
+   cudaFree(d->table_b); cudaFree(d->table_hd); cudaFree(d->atom_cell);
+   h->sys.cell = nullptr;
+   h->sys.cell_field = nullptr;
+   h->sys.cell_hd = nullptr;
+   h->sys.ncells = 0;
+   delete d;
+   h->extras[2] = nullptr;
+}
+
+template <typename R>
+static int dipole_update_typed(vgpu_ctx* h) {
+   DipoleState* d = dip_of(h);
+   SysDev& S = h->sys;
+   const int nc = d->nc;
+   h->prof_begin(PROF_DIPOLE);
+   cell_moment_kernel<R><<<(nc * 32 + 255) / 256, 256, 0, h->stream>>>(
+       nc, d->cell_start, d->cell_atoms, (const R*)S.s[0], (const R*)S.s[1], (const R*)S.s[2], (const int*)S.mat,
+       (const MatParams<R>*)S.mp, S.mus_SI, d->mag, d->pos, d->mom);
+   cell_field_kernel<<<(nc + 255) / 256, 256, 0, h->stream>>>(nc, d->pos, d->mom, d->field);
+   cell_finish_kernel<R><<<(nc + 1 + 255) / 256, 256, 0, h->stream>>>(
+       nc, d->near_start, d->near_j, d->near_t, d->npairs, d->mag, d->self, d->pos, d->field, (R*)d->table_b,
+       (R*)d->table_hd);
+   h->prof_end(PROF_DIPOLE);
+   h->kernel_launches += 3;
+   return cuda_err(h, cudaGetLastError(), "dipole update");
+}
+
+int dipole_update(vgpu_ctx* h) {
+   return h->prec == VGPU_PREC_FP64 ? dipole_update_typed<double>(h) : dipole_update_typed<float>(h);
+}
+
 }  // namespace vgpu
 
-int dipole_after_step(vgpu_ctx* h) { (void)h; return VGPU_OK; }
+using namespace vgpu;
+
+int dipole_after_step(vgpu_ctx* h) {
+   DipoleState* d = dip_of(h);
+   if (!d || d->update_rate <= 0) return VGPU_OK;
+   if (h->step % (uint64_t)d->update_rate != 0) return VGPU_OK;
+   return dipole_update(h);
+}
+
+extern "C" int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* dd) {
+   if (!h || !dd) return set_err(h, VGPU_ERR_ARG, "null argument");
+   SysDev& S = h->sys;
+   if (!S.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   const int n = S.n, nc = dd->num_cells;
+   if (nc <= 0 || !dd->atom_cell || !dd->cell_pos_mom || !dd->cell_volume || !dd->cell_natoms)
+      return set_err(h, VGPU_ERR_ARG, "incomplete dipole descriptor");
+   if (dd->solver == VGPU_DIPOLE_TENSOR && (!dd->atom_x || !dd->atom_y || !dd->atom_z))
+      return set_err(h, VGPU_ERR_ARG, "tensor solver needs atom coordinates");
+   if (!(dd->macro_cell_size > 0.0)) return set_err(h, VGPU_ERR_ARG, "macro_cell_size must be positive");
+   for (int i = 0; i < n; ++i)
+      if (dd->atom_cell[i] < 0 || dd->atom_cell[i] >= nc)
+         return set_err(h, VGPU_ERR_ARG, "atom %d has cell %d outside 0..%d", i, dd->atom_cell[i], nc - 1);
+   cudaSetDevice(h->device);
+   dipole_destroy(h);
+   DipoleState* d = new DipoleState();
+   h->extras[2] = d;
+   d->nc = nc;
+   d->solver = dd->solver;
+   d->update_rate = dd->update_rate;
+   d->size = dd->macro_cell_size;
+   d->cutoff = dd->cutoff;
+   const int M = S.M;
+   std::vector<double> mus(M);
+   std::vector<char> magnetic(M);
+   for (int m = 0; m < M; ++m) {
+      mus[m] = S.materials[m].mu_s_SI;
+      magnetic[m] = S.materials[m].non_magnetic == 0;
+   }
+   // cell-sorted atom list of magnetic atoms (cells::mag skips non-magnetic ones)
+   std::vector<int> start(nc + 1, 0), atoms;
+   std::vector<int> acell(n);
+   for (int i = 0; i < n; ++i)
+      if (magnetic[S.type_host[i]]) start[dd->atom_cell[i] + 1]++;
+   for (int c = 0; c < nc; ++c) start[c + 1] += start[c];
+   atoms.resize(start[nc]);
+   {
+      std::vector<int> fill(start.begin(), start.end() - 1);
+      for (int i = 0; i < n; ++i)
+         if (magnetic[S.type_host[i]]) atoms[fill[dd->atom_cell[i]]++] = i;
+   }
+   // atoms read the zero row when their cell is empty or they are non-magnetic
+   for (int i = 0; i < n; ++i) {
+      const int c = dd->atom_cell[i];
+      acell[i] = (dd->cell_natoms[c] > 0 && magnetic[S.type_host[i]]) ? c : nc;
+   }
+   std::vector<float4> pos(nc);
+   std::vector<double> self(nc);
+   for (int c = 0; c < nc; ++c) {
+      pos[c] = make_float4((float)dd->cell_pos_mom[4 * c], (float)dd->cell_pos_mom[4 * c + 1],
+                           (float)dd->cell_pos_mom[4 * c + 2], dd->cell_natoms[c] > 0 ? 1.f : 0.f);
+      self[c] = dd->cell_natoms[c] > 0 ? 8.0 * M_PI / (3.0 * dd->cell_volume[c]) : 0.0;
+   }
+   // near pairs (tensor solver), classified in FP64 exactly as inter.cpp:66,83
+   std::vector<int> pi, pj, nstart(nc + 1, 0);
+   if (dd->solver == VGPU_DIPOLE_TENSOR) {
+      const double bin = std::max(dd->cutoff * dd->macro_cell_size, 1e-6) * 1.0001;
+      std::unordered_map<long long, std::vector<int>> grid;
+      auto key = [&](long long x, long long y, long long z) { return (x * 1000003LL + y) * 1000033LL + z; };
+      for (int c = 0; c < nc; ++c) {
+         if (dd->cell_natoms[c] <= 0) continue;
+         const long long gx = (long long)std::floor(dd->cell_pos_mom[4 * c] / bin);
+         const long long gy = (long long)std::floor(dd->cell_pos_mom[4 * c + 1] / bin);
+         const long long gz = (long long)std::floor(dd->cell_pos_mom[4 * c + 2] / bin);
+         grid[key(gx, gy, gz)].push_back(c);
+      }
+      std::vector<std::vector<int>> near(nc);
+      for (int i = 0; i < nc; ++i) {
+         if (dd->cell_natoms[i] <= 0) continue;
+         const double* P = dd->cell_pos_mom + 4 * i;
+         const long long gx = (long long)std::floor(P[0] / bin), gy = (long long)std::floor(P[1] / bin),
+                         gz = (long long)std::floor(P[2] / bin);
+         for (long long x = gx - 1; x <= gx + 1; ++x)
+            for (long long y = gy - 1; y <= gy + 1; ++y)
+               for (long long z = gz - 1; z <= gz + 1; ++z) {
+                  auto it = grid.find(key(x, y, z));
+                  if (it == grid.end()) continue;
+                  for (int j : it->second) {
+                     if (j == i) { near[i].push_back(j); continue; }
+                     const double rx = dd->cell_pos_mom[4 * j] - P[0];
+                     const double ry = dd->cell_pos_mom[4 * j + 1] - P[1];
+                     const double rz = dd->cell_pos_mom[4 * j + 2] - P[2];
+                     const double rij = 1.0 / sqrt(rx * rx + ry * ry + rz * rz);
+                     if ((1.0 / rij) / dd->macro_cell_size <= dd->cutoff) near[i].push_back(j);
+                  }
+               }
+         std::sort(near[i].begin(), near[i].end());
+      }
+      for (int i = 0; i < nc; ++i) {
+         nstart[i + 1] = nstart[i] + (int)near[i].size();
+         for (int j : near[i]) { pi.push_back(i); pj.push_back(j); }
+      }
+   }
+   d->npairs = (int)pj.size();
+   cudaError_t e = cudaSuccess;
+   auto up = [&](void** dst, const void* src, size_t bytes) {
+      if (e != cudaSuccess) return;
+      e = cudaMalloc(dst, std::max<size_t>(bytes, 16));
+      if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
+   };
+   up((void**)&d->cell_start, start.data(), sizeof(int) * (nc + 1));
+   up((void**)&d->cell_atoms, atoms.data(), sizeof(int) * atoms.size());
+   up((void**)&d->atom_cell, acell.data(), sizeof(int) * n);
+   up((void**)&d->pos, pos.data(), sizeof(float4) * nc);
+   up((void**)&d->self, self.data(), sizeof(double) * nc);
+   if (e == cudaSuccess) e = cudaMalloc(&d->mag, sizeof(double) * 3 * nc);
+   if (e == cudaSuccess) e = cudaMalloc(&d->mom, sizeof(float4) * nc);
+   if (e == cudaSuccess) e = cudaMalloc(&d->field, sizeof(double) * 6 * nc);
+   const size_t rs = h->prec == VGPU_PREC_FP64 ? sizeof(double) : sizeof(float);
+   if (e == cudaSuccess) e = cudaMalloc(&d->table_b, rs * 3 * (nc + 1));
+   if (e == cudaSuccess) e = cudaMalloc(&d->table_hd, rs * 3 * (nc + 1));
+   if (e == cudaSuccess && !S.mus_SI) {
+      S.mus_SI = (double*)h->alloc(sizeof(double) * 100);
+      if (!S.mus_SI) e = cudaErrorMemoryAllocation;
+   }
+   if (e == cudaSuccess) e = cudaMemcpyAsync(S.mus_SI, mus.data(), sizeof(double) * M, cudaMemcpyHostToDevice, h->stream);
+   if (e == cudaSuccess && d->npairs > 0) {
+      up((void**)&d->near_start, nstart.data(), sizeof(int) * (nc + 1));
+      up((void**)&d->near_j, pj.data(), sizeof(int) * pj.size());
+      int *dpi = nullptr, *dpj = nullptr;
+      double *ax = nullptr, *ay = nullptr, *az = nullptr, *cp = nullptr;
+      // coordinates in cell-sorted order for the near-tensor kernel
+      std::vector<double> cx(atoms.size()), cy(atoms.size()), cz(atoms.size());
+      for (size_t k = 0; k < atoms.size(); ++k) {
+         cx[k] = dd->atom_x[atoms[k]]; cy[k] = dd->atom_y[atoms[k]]; cz[k] = dd->atom_z[atoms[k]];
+      }
+      up((void**)&dpi, pi.data(), sizeof(int) * pi.size());
+      up((void**)&dpj, pj.data(), sizeof(int) * pj.size());
+      up((void**)&ax, cx.data(), sizeof(double) * cx.size());
+      up((void**)&ay, cy.data(), sizeof(double) * cy.size());
+      up((void**)&az, cz.data(), sizeof(double) * cz.size());
+      up((void**)&cp, dd->cell_pos_mom, sizeof(double) * 4 * nc);
+      if (e == cudaSuccess) e = cudaMalloc(&d->near_t, sizeof(double) * 6 * d->npairs);
+      if (e == cudaSuccess) {
+         near_tensor_kernel<<<d->npairs, 256, 0, h->stream>>>(d->npairs, dpi, dpj, d->cell_start, ax, ay, az, cp,
+                                                               d->near_t);
+         e = cudaGetLastError();
+      }
+      if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+      cudaFree(dpi); cudaFree(dpj); cudaFree(ax); cudaFree(ay); cudaFree(az); cudaFree(cp);
+   }
+   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+   if (e != cudaSuccess) {
+      int rc = cuda_err(h, e, "dipole setup");
+      dipole_destroy(h);
+      return rc;
+   }
+   S.ncells = nc + 1;  // tables have a zero row at index nc
+   S.cell = d->atom_cell;
+   S.cell_field = d->table_b;
+   S.cell_hd = d->table_hd;
+   // field at the current spins (dipole::initialize calls calculate_field(0))
+   return dipole_update(h);
+}
+
+extern "C" int vgpu_dipole_update(vgpu_handle h) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!dip_of(h)) return set_err(h, VGPU_ERR_STATE, "vgpu_dipole_setup not called");
+   cudaSetDevice(h->device);
+   return dipole_update(h);
+}
+
+extern "C" int vgpu_dipole_get_cells(vgpu_handle h, double* mag, double* b_field, double* hd_field) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   DipoleState* d = dip_of(h);
+   if (!d) return set_err(h, VGPU_ERR_STATE, "vgpu_dipole_setup not called");
+   cudaSetDevice(h->device);
+   const int nc = d->nc;
+   cudaError_t e = cudaSuccess;
+   if (mag) e = cudaMemcpyAsync(mag, d->mag, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, h->stream);
+   if (e == cudaSuccess && b_field)
+      e = cudaMemcpyAsync(b_field, d->field, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, h->stream);
+   if (e == cudaSuccess && hd_field)
+      e = cudaMemcpyAsync(hd_field, d->field + 3 * nc, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, h->stream);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+   return cuda_err(h, e, "dipole download");
+}
+
+template <typename R>
+static int set_atom_field_typed(vgpu_handle h, const double* b[3], const double* m[3]) {
+   SysDev& S = h->sys;
+   const int n = S.n;
+   if (!S.hd_atom) {
+      S.hd_atom = h->alloc(3 * (size_t)n * sizeof(R));
+      S.hm_atom = h->alloc(3 * (size_t)n * sizeof(R));
+      if (!S.hd_atom || !S.hm_atom) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for atom dipole field");
+   }
+   std::vector<R> buf(3 * (size_t)n);
+   for (int q = 0; q < 3; ++q)
+      for (int i = 0; i < n; ++i) buf[(size_t)q * n + i] = (R)b[q][i];
+   int rc = cuda_err(h, cudaMemcpyAsync(S.hd_atom, buf.data(), buf.size() * sizeof(R), cudaMemcpyHostToDevice,
+                                        h->stream), "atom dipole field");
+   if (rc) return rc;
+   rc = cuda_err(h, cudaStreamSynchronize(h->stream), "atom dipole field");
+   if (rc) return rc;
+   for (int q = 0; q < 3; ++q)
+      for (int i = 0; i < n; ++i) buf[(size_t)q * n + i] = m[q] ? (R)m[q][i] : (R)0;
+   rc = cuda_err(h, cudaMemcpyAsync(S.hm_atom, buf.data(), buf.size() * sizeof(R), cudaMemcpyHostToDevice,
+                                    h->stream), "atom demag field");
+   if (rc) return rc;
+   return cuda_err(h, cudaStreamSynchronize(h->stream), "atom demag field");
+}
+
+extern "C" int vgpu_set_dipole_field(vgpu_handle h, const double* bx, const double* by, const double* bz,
+                                     const double* hx, const double* hy, const double* hz) {
+   if (!h || !bx || !by || !bz) return set_err(h, VGPU_ERR_ARG, "null argument");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (dip_of(h)) return set_err(h, VGPU_ERR_STATE, "device dipole solver active; host fields not used");
+   cudaSetDevice(h->device);
+   const double* b[3] = {bx, by, bz};
+   const double* m[3] = {hx, hy, hz};
+   return h->prec == VGPU_PREC_FP64 ? set_atom_field_typed<double>(h, b, m) : set_atom_field_typed<float>(h, b, m);
+}

@@ -18,6 +18,7 @@
 // f(s0, ...) dt is not stored: since f is perpendicular to s0 and
 // s' = (s0 + f dt)/|s0 + f dt|, the corrector recovers
 // f dt = s' |s0|^2 / (s'.s0) - s0 exactly from the two states it reads anyway.
+#pragma once
 #include <cuda_runtime.h>
 
 #include "llg_device.cuh"
@@ -42,6 +43,7 @@ __global__ void __launch_bounds__(256) llg_pass_kernel(const LLGArgs<R> a) {
       }
       R d[3];
       llg_rhs<R>(m.A, m.B, S0, H, d);
+      if (a.ex) { a.ex[i] = d[0]; a.ey[i] = d[1]; a.ez[i] = d[2]; }
       R Sn[3] = {S0[0] + d[0] * a.dt, S0[1] + d[1] * a.dt, S0[2] + d[2] * a.dt};
       const R r = rsqrt_<R>(Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2]);
       a.bx[i] = Sn[0] * r; a.by[i] = Sn[1] * r; a.bz[i] = Sn[2] * r;
@@ -53,14 +55,21 @@ __global__ void __launch_bounds__(256) llg_pass_kernel(const LLGArgs<R> a) {
       H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
       R d[3];
       llg_rhs<R>(m.A, m.B, S1, H, d);
-      // recover the predictor increment f(s0) dt from s0 and s'
-      const R s00 = S0[0] * S0[0] + S0[1] * S0[1] + S0[2] * S0[2];
-      const R c = s00 / (S1[0] * S0[0] + S1[1] * S0[1] + S1[2] * S0[2]);
       R Sn[3];
+      if (a.ex) {
+         // stored predictor increment: s0 + dt/2 (f0 + f1) as LLGHeun.cpp:264-266
+         const R e0[3] = {a.ex[i], a.ey[i], a.ez[i]};
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-         const R e = S1[k] * c - S0[k];
-         Sn[k] = S0[k] + ((R)0.5 * e + a.half_dt * d[k]);
+         for (int k = 0; k < 3; ++k) Sn[k] = S0[k] + a.half_dt * (e0[k] + d[k]);
+      } else {
+         // recover the predictor increment f(s0) dt from s0 and s'
+         const R s00 = S0[0] * S0[0] + S0[1] * S0[1] + S0[2] * S0[2];
+         const R c = s00 / (S1[0] * S0[0] + S1[1] * S0[1] + S1[2] * S0[2]);
+#pragma unroll
+         for (int k = 0; k < 3; ++k) {
+            const R e = S1[k] * c - S0[k];
+            Sn[k] = S0[k] + ((R)0.5 * e + a.half_dt * d[k]);
+         }
       }
       const R n2 = Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2];
       const R r = rsqrt_<R>(n2);
@@ -70,7 +79,7 @@ __global__ void __launch_bounds__(256) llg_pass_kernel(const LLGArgs<R> a) {
 }
 
 template <typename R, int FMT>
-static cudaError_t launch_fmt(const LLGArgs<R>& a, int mode, cudaStream_t st) {
+inline cudaError_t launch_fmt(const LLGArgs<R>& a, int mode, cudaStream_t st) {
    const int bs = 256;
    const int grid = (a.n + bs - 1) / bs;
    if (grid == 0) return cudaSuccess;
@@ -107,10 +116,4 @@ cudaError_t launch_thermal_noise(const LLGArgs<R>& a, cudaStream_t st) {
    thermal_noise_kernel<R><<<(a.n + 255) / 256, 256, 0, st>>>(a);
    return cudaGetLastError();
 }
-template cudaError_t launch_thermal_noise<float>(const LLGArgs<float>&, cudaStream_t);
-template cudaError_t launch_thermal_noise<double>(const LLGArgs<double>&, cudaStream_t);
-
-template cudaError_t launch_llg_pass<float>(const LLGArgs<float>&, int, int, int, cudaStream_t);
-template cudaError_t launch_llg_pass<double>(const LLGArgs<double>&, int, int, int, cudaStream_t);
-
 }  // namespace vgpu

@@ -82,7 +82,13 @@ __global__ void stats_partial_kernel(const LLGArgs<R> a, const int* __restrict__
          }
          const double eap = -((double)a.hx * S[0] + (double)a.hy * S[1] + (double)a.hz * S[2]);
          double ems = 0.0;
-         if (hm) ems = -((double)hm[i] * S[0] + (double)hm[a.n + i] * S[1] + (double)hm[2 * a.n + i] * S[2]);
+         if (a.cell) {
+            const int c = __ldg(a.cell + i);
+            ems = -((double)a.cell_hd[c] * S[0] + (double)a.cell_hd[a.ncells + c] * S[1] +
+                    (double)a.cell_hd[2 * a.ncells + c] * S[2]);
+         } else if (hm) {
+            ems = -((double)hm[i] * S[0] + (double)hm[a.n + i] * S[1] + (double)hm[2 * a.n + i] * S[2]);
+         }
          atomicAdd(b + ST_EEX, eex * mu);
          atomicAdd(b + ST_EAN, ean * mu);
          atomicAdd(b + ST_EAP, eap * mu);
@@ -180,7 +186,7 @@ using namespace vgpu;
 extern "C" int vgpu_stats_add_mask(vgpu_handle h, const int32_t* mask, int32_t mask_size, int32_t* id_out) {
    if (!h || !mask || !id_out) return set_err(h, VGPU_ERR_ARG, "null argument");
    if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
-   if (mask_size <= 0 || mask_size > 4096) return set_err(h, VGPU_ERR_ARG, "mask_size must be in 1..4096");
+   if (mask_size <= 0 || mask_size > 2048) return set_err(h, VGPU_ERR_ARG, "mask_size must be in 1..2048");
    const int n = h->sys.n;
    for (int i = 0; i < n; ++i)
       if (mask[i] < 0 || mask[i] >= mask_size)

@@ -242,6 +242,13 @@ static int upload_typed(vgpu_ctx* h, const vgpu_system_desc* d) {
    S.uniaxial = d->uniaxial_enabled; S.cubic = d->cubic_enabled;
    S.type_host = mat;
    S.materials.assign(d->materials, d->materials + M);
+   S.row_host.assign(n + 1, 0);
+   S.nl_host.clear();
+   S.nl_host.reserve((size_t)d->num_bonds);
+   for (int i = 0; i < n; ++i) {
+      for (int64_t b = d->nl_start[i]; b <= d->nl_end[i]; ++b) S.nl_host.push_back(d->nl[b]);
+      S.row_host[i + 1] = (int64_t)S.nl_host.size();
+   }
    int rc;
    if ((rc = upload_vec(h, &S.slice_off, off, "slice offsets"))) return rc;
    if ((rc = upload_vec(h, &S.col, col, "neighbour index"))) return rc;
@@ -327,6 +334,8 @@ LLGArgs<R> make_args(vgpu_ctx* h) {
    a.xi = (const R*)S.xi;
    a.cell = (const int*)S.cell;
    a.cell_field = (const R*)S.cell_field;
+   a.cell_hd = (const R*)S.cell_hd;
+   a.hm_atom = (const R*)S.hm_atom;
    a.ncells = S.ncells;
    a.hd_atom = (const R*)S.hd_atom;
    a.dt = (R)p.dt;
@@ -334,14 +343,38 @@ LLGArgs<R> make_args(vgpu_ctx* h) {
    a.ax = (R*)S.s[0]; a.ay = (R*)S.s[1]; a.az = (R*)S.s[2];
    a.bx = (R*)S.p[0]; a.by = (R*)S.p[1]; a.bz = (R*)S.p[2];
    a.fx = (R*)S.f[0]; a.fy = (R*)S.f[1]; a.fz = (R*)S.f[2];
+   a.ex = (R*)S.e[0]; a.ey = (R*)S.e[1]; a.ez = (R*)S.e[2];
    a.status = S.status;
    return a;
 }
 template LLGArgs<float> make_args<float>(vgpu_ctx*);
 template LLGArgs<double> make_args<double>(vgpu_ctx*);
 
+// allocate or drop the stored-increment buffers according to the option
+template <typename R>
+static int ensure_increment(vgpu_ctx* h) {
+   SysDev& S = h->sys;
+   const bool want = h->store_increment < 0 ? h->prec == VGPU_PREC_FP64 : h->store_increment != 0;
+   if (!want) {
+      S.e[0] = S.e[1] = S.e[2] = nullptr;  // buffers (if any) stay owned by allocs until re-upload
+      return VGPU_OK;
+   }
+   if (S.e_store[0]) {
+      for (int q = 0; q < 3; ++q) S.e[q] = S.e_store[q];
+      return VGPU_OK;
+   }
+   for (int q = 0; q < 3; ++q) {
+      S.e_store[q] = h->alloc(S.n_alloc * sizeof(R));
+      if (!S.e_store[q]) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for increment buffer");
+      S.e[q] = S.e_store[q];
+   }
+   return VGPU_OK;
+}
+
 template <typename R>
 static int llg_steps_typed(vgpu_ctx* h, uint64_t n_steps) {
+   int rc0 = ensure_increment<R>(h);
+   if (rc0) return rc0;
    for (uint64_t t = 0; t < n_steps; ++t) {
       LLGArgs<R> a = make_args<R>(h);
       h->prof_begin(PROF_PREDICTOR);
@@ -550,6 +583,14 @@ extern "C" int vgpu_set_noise_replay(vgpu_handle h, const double* xi) {
    if (rc) return rc;
    h->noise_mode = VGPU_NOISE_REPLAY;
    return VGPU_OK;
+}
+
+extern "C" int vgpu_set_option(vgpu_handle h, int option, int value) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   switch (option) {
+      case VGPU_OPT_STORE_INCREMENT: h->store_increment = value; return VGPU_OK;
+      default: return set_err(h, VGPU_ERR_ARG, "unknown option %d", option);
+   }
 }
 
 extern "C" int vgpu_set_step(vgpu_handle h, uint64_t step) {

@@ -28,15 +28,22 @@ struct SysDev {
    void* s[3] = {nullptr};   // state A
    void* p[3] = {nullptr};   // state B (predictor)
    void* f[3] = {nullptr};   // field output
+   void* e[3] = {nullptr};   // stored predictor increment in use (VGPU_OPT_STORE_INCREMENT)
+   void* e_store[3] = {nullptr};  // its buffers, once allocated
    void* xi = nullptr;       // replay noise
    int* status = nullptr;
    // macrocell dipole
    int ncells = 0;
    void* cell = nullptr;
-   void* cell_field = nullptr;
+   void* cell_field = nullptr;   // [3][ncells] B field (LLG)
+   void* cell_hd = nullptr;      // [3][ncells] mu0 Hd field (energies)
+   double* mus_SI = nullptr;     // [M] moments in J/T
    void* hd_atom = nullptr;
    void* hm_atom = nullptr;  // per-atom mu0 Hd field for the magnetostatic energy
+   void* mc_tab = nullptr;   // Monte Carlo per-material tables
    std::vector<int> type_host;
+   std::vector<int64_t> row_host;  // CSR kept on the host (colouring, sharding)
+   std::vector<int> nl_host;
    std::vector<vgpu_material> materials;
 };
 
@@ -65,6 +72,7 @@ struct vgpu_ctx {
    uint64_t seed = 0;
    int noise_mode = VGPU_NOISE_PHILOX;
    bool any_sigma = false;
+   int store_increment = -1;  // -1: default (on for FP64, off for FP32)
 
    void* alloc(size_t bytes);
    void free_system();

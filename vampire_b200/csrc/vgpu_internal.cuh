@@ -59,13 +59,16 @@ struct LLGArgs {
    uint64_t step;            // Philox counter for this step
    const R* xi;              // replay noise, 3n (x|y|z blocks)
    const int* cell;          // [n] macrocell id, or nullptr
-   const R* cell_field;      // [3*ncells] x|y|z blocks
+   const R* cell_field;      // [3*ncells] x|y|z blocks, B field
+   const R* cell_hd;         // [3*ncells] mu0 Hd field (magnetostatic energy)
+   const R* hm_atom;         // [3n] per-atom mu0 Hd field (host-computed), or nullptr
    int ncells;
    const R* hd_atom;         // [3n] per-atom dipole field (host-computed), or nullptr
    R dt, half_dt;
    R* ax; R* ay; R* az;      // state A: s0 (read), s1 (written by corrector)
    R* bx; R* by; R* bz;      // state B: s' (predictor output)
    R* fx; R* fy; R* fz;      // field output (field-only mode)
+   R* ex; R* ey; R* ez;      // stored predictor increment f(s0), or nullptr (recovered)
    int* status;              // device status word (non-finite spin flag)
 };
 

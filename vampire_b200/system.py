@@ -375,6 +375,35 @@ def build(kind: str, nx: int, ny: int, nz: int, a: float, mats: Sequence[Materia
     return sys_
 
 
+def dipole_cells(s: SpinSystem, size: float, atomic_volume: float, solver: str = "tensor",
+                 cutoff: float = 2.0, update_rate: int = 100) -> dict:
+    """Macrocells of edge `size` [Angstrom] on a regular grid from the atom
+    positions, as cells::initialize builds them (src/cells/initialize.cpp:
+    moment-weighted centres, volume = atoms x atomic volume).  Stored in
+    s.cells and returned (the dict vgpu.Simulation.dipole_setup takes)."""
+    c = s.coords
+    lo = c.min(axis=1)
+    idx = np.floor((c - lo[:, None]) / size + 1e-9).astype(np.int64)
+    dims = idx.max(axis=1) + 1
+    cell = (idx[0] + dims[0] * (idx[1] + dims[1] * idx[2])).astype(np.int32)
+    nc = int(np.prod(dims))
+    mu = s.materials["mu_s_SI"][s.type]
+    magnetic = s.materials["non_magnetic"][s.type] == 0
+    w = np.where(magnetic, mu, 0.0)
+    natoms = np.bincount(cell, weights=magnetic.astype(np.float64), minlength=nc).astype(np.int32)
+    pm = np.zeros((nc, 4))
+    for q in range(3):
+        pm[:, q] = np.bincount(cell, weights=c[q] * w, minlength=nc)
+    pm[:, 3] = np.bincount(cell, weights=w, minlength=nc)
+    has = pm[:, 3] > 0
+    pm[has, :3] /= pm[has, 3:4]
+    vol = natoms * atomic_volume
+    s.cells = {"atom_cell": cell, "cell_pos_mom": pm.ravel(), "cell_volume": vol.astype(np.float64),
+               "cell_natoms": natoms, "macro_cell_size": size, "cutoff": cutoff, "update_rate": update_rate,
+               "solver": solver, "coords": s.coords}
+    return s.cells
+
+
 # ----------------------------------------------------------------------------
 # benchmark configurations (synthetic inputs with the configurations' shapes)
 # ----------------------------------------------------------------------------
@@ -388,15 +417,19 @@ def config_sc_llg(L: int = 20, temperature: float = 0.0, seed: int = 123456) -> 
     return build("sc", L, L, L, 3.0, [m], [[11.2e-21]], p, spin_seed=seed)
 
 
-def config_fcc_tensor(L: int = 100, seed: int = 2024, temperature: float = 300.0) -> SpinSystem:
+def config_fcc_tensor(L: int = 100, seed: int = 2024, temperature: float = 300.0,
+                      dipole: bool = False) -> SpinSystem:
     """FCC L^3 periodic (4 L^3 spins), a=0.354 nm, two materials at random
     50/50, nn tensor exchange J_AA=J_BB=11.2e-21 J, J_AB=5e-21 J plus the
     three-site DMI with D=0.1 J, cubic Kc=1e-24 J/atom, alpha=0.05,
-    dt=1e-16 s, T=300 K, H=0."""
+    dt=1e-16 s, T=300 K, H=0; with `dipole`, 2x2x2-unit-cell macrocells."""
     mats = [Material(alpha=0.05, mu_s_muB=1.72, Kc=1e-24) for _ in range(2)]
     J = np.array([[11.2e-21, 5e-21], [5e-21, 11.2e-21]])
     p = SimParams(dt_SI=1e-16, temperature=temperature, H_applied=0.0, H_vec=(0.0, 0.0, 1.0))
     rng = np.random.default_rng(seed)
     types = (rng.random(4 * L ** 3) < 0.5).astype(np.int32)
-    return build("fcc", L, L, L, 3.54, mats, J, p, types=types, dmi_SI=0.1 * J,
-                 spin_seed=seed + 1)
+    s = build("fcc", L, L, L, 3.54, mats, J, p, types=types, dmi_SI=0.1 * J, spin_seed=seed + 1)
+    if dipole:
+        # macrocells of 2x2x2 unit cells, tensor solver, updated every 100 steps
+        dipole_cells(s, size=2 * 3.54, atomic_volume=3.54 ** 3 / 4.0, solver="tensor", update_rate=100)
+    return s

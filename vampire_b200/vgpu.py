@@ -51,6 +51,14 @@ class SimParamsC(C.Structure):
     ]
 
 
+class DipoleDesc(C.Structure):
+    _fields_ = [
+        ("num_cells", C.c_int32), ("solver", C.c_int32), ("update_rate", C.c_int32), ("pad_", C.c_int32),
+        ("macro_cell_size", C.c_double), ("cutoff", C.c_double), ("atom_cell", _I32), ("cell_pos_mom", _D),
+        ("cell_volume", _D), ("cell_natoms", _I32), ("atom_x", _D), ("atom_y", _D), ("atom_z", _D),
+    ]
+
+
 _lib = None
 
 
@@ -234,6 +242,79 @@ class Simulation:
 
     def llg_heun(self, n_steps: int = 1) -> None:
         self._check(lib().vgpu_llg_heun(self._h, C.c_uint64(n_steps)))
+
+    # -- dipole field --------------------------------------------------------
+    def dipole_setup(self, cells: dict) -> None:
+        """cells: atom_cell, cell_pos_mom, cell_volume, cell_natoms,
+        macro_cell_size, cutoff, update_rate, solver ('tensor'|'macrocell'),
+        coords (3, n) for the tensor solver (the reference's cells:: data)."""
+        keep = {}
+
+        def arr(name, a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            keep[name] = a
+            return a
+
+        d = DipoleDesc()
+        d.num_cells = int(np.asarray(cells["cell_natoms"]).size)
+        d.solver = 1 if cells.get("solver", "tensor") == "tensor" else 0
+        d.update_rate = int(cells.get("update_rate", 100))
+        d.macro_cell_size = float(cells["macro_cell_size"])
+        d.cutoff = float(cells.get("cutoff", 2.0))
+        d.atom_cell = _ptr(arr("ac", cells["atom_cell"], np.int32), _I32)
+        d.cell_pos_mom = _ptr(arr("cp", cells["cell_pos_mom"], np.float64), _D)
+        d.cell_volume = _ptr(arr("cv", cells["cell_volume"], np.float64), _D)
+        d.cell_natoms = _ptr(arr("cn", cells["cell_natoms"], np.int32), _I32)
+        if "coords" in cells and cells["coords"] is not None:
+            c = arr("xyz", cells["coords"], np.float64)
+            d.atom_x, d.atom_y, d.atom_z = _ptr(c[0], _D), _ptr(c[1], _D), _ptr(c[2], _D)
+        self._ncells = d.num_cells
+        self._check(lib().vgpu_dipole_setup(self._h, C.byref(d)))
+
+    def dipole_update(self) -> None:
+        self._check(lib().vgpu_dipole_update(self._h))
+
+    def dipole_cells(self):
+        """(moments J/T, B field T, mu0 Hd field T), each (3, ncells)."""
+        nc = self._ncells
+        m, b, hd = np.empty(3 * nc), np.empty(3 * nc), np.empty(3 * nc)
+        self._check(lib().vgpu_dipole_get_cells(self._h, _ptr(m, _D), _ptr(b, _D), _ptr(hd, _D)))
+        return m.reshape(3, nc), b.reshape(3, nc), hd.reshape(3, nc)
+
+    def set_dipole_field(self, b: np.ndarray, hd: Optional[np.ndarray] = None) -> None:
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        h = np.ascontiguousarray(hd, dtype=np.float64) if hd is not None else None
+        self._check(lib().vgpu_set_dipole_field(self._h, _ptr(b[0], _D), _ptr(b[1], _D), _ptr(b[2], _D),
+                                                _ptr(h[0] if h is not None else None, _D),
+                                                _ptr(h[1] if h is not None else None, _D),
+                                                _ptr(h[2] if h is not None else None, _D)))
+
+    # -- Monte Carlo -------------------------------------------------------
+    def mc_setup(self, colour: Optional[np.ndarray] = None) -> int:
+        nc = C.c_int32()
+        c = np.ascontiguousarray(colour, dtype=np.int32) if colour is not None else None
+        self._check(lib().vgpu_mc_setup(self._h, _ptr(c, _I32), C.byref(nc)))
+        return nc.value
+
+    def mc_colours(self) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.int32)
+        self._check(lib().vgpu_mc_get_colours(self._h, _ptr(out, _I32)))
+        return out
+
+    def mc_set_replay(self, rnd: Optional[np.ndarray]) -> None:
+        r = np.ascontiguousarray(rnd, dtype=np.float64) if rnd is not None else None
+        self._check(lib().vgpu_mc_set_replay(self._h, _ptr(r, _D)))
+
+    def mc_sweep(self, n_sweeps: int = 1) -> None:
+        self._check(lib().vgpu_mc_sweep(self._h, C.c_uint64(n_sweeps)))
+
+    def mc_set_sweep(self, sweep: int) -> None:
+        self._check(lib().vgpu_mc_set_sweep(self._h, C.c_uint64(sweep)))
+
+    def mc_counters(self):
+        mv, rj = C.c_double(), C.c_double()
+        self._check(lib().vgpu_mc_counters(self._h, C.byref(mv), C.byref(rj)))
+        return mv.value, rj.value
 
     # -- statistics --------------------------------------------------------
     def add_mask(self, mask: np.ndarray, size: int) -> int:
