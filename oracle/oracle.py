@@ -252,7 +252,10 @@ def system_from_dump(d: dict, params=None):
     if params is None:
         params = S.SimParams(dt_SI=simc[2], gamma_SI=simc[3], temperature=simc[4], H_applied=simc[5],
                              H_vec=tuple(simc[6:9]), thermal=bool(meta[8]), applied=bool(meta[9]))
-    spins = np.stack([d["sx_0"], d["sy_0"], d["sz_0"]])
+    if "sx_0" in d:
+        spins = np.stack([d["sx_0"], d["sy_0"], d["sz_0"]])
+    else:  # fixtures without a spin dump start along z
+        spins = np.tile(np.array([[0.0], [0.0], [1.0]]), (1, n))
     s = S.SpinSystem(n=n, nl_start=d["nl_start"].astype(np.int32), nl_end=d["nl_end"].astype(np.int32),
                      nl=d["nl"].astype(np.int32), jlist=d["jlist"], exch_type=et,
                      type=d["type"].astype(np.int32), materials=mats, spins=spins, params=params,

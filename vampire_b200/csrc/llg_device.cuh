@@ -21,8 +21,18 @@ __device__ __forceinline__ void thermal_xi(const LLGArgs<R>& a, int i, R& gx, R&
       gz = a.xi[2 * a.n + i];
       return;
    }
-   u32x4 c = {(uint32_t)i, (uint32_t)a.step, (uint32_t)(a.step >> 32), RNG_THERMAL};
-   u32x4 r = philox4x32_10(c, a.seed_lo, a.seed_hi);
+   // batched systems: system k's atoms draw the stream of a single system
+   // seeded seed + k, with their own local index (same numbers as a plain run)
+   uint32_t li = (uint32_t)i, klo = a.seed_lo, khi = a.seed_hi;
+   if (a.sys_off) {
+      const int k = (a.mat ? __ldg(a.mat + i) : 0) / a.m_per_sys;
+      li = (uint32_t)(i - __ldg(a.sys_off + k));
+      const uint64_t s = (((uint64_t)a.seed_hi << 32) | a.seed_lo) + (uint64_t)k;
+      klo = (uint32_t)s;
+      khi = (uint32_t)(s >> 32);
+   }
+   u32x4 c = {li, (uint32_t)a.step, (uint32_t)(a.step >> 32), RNG_THERMAL};
+   u32x4 r = philox4x32_10(c, klo, khi);
    if (sizeof(R) == 4) {
       float s1, c1, s2, c2;
       const float r1 = sqrtf(-2.0f * logf(u01f(r.x)));
@@ -45,7 +55,13 @@ __device__ __forceinline__ void thermal_xi(const LLGArgs<R>& a, int i, R& gx, R&
 }
 
 // exchange gather of atom i over its SELL row, sources (sx,sy,sz)
-template <typename R, int FMT>
+template <typename R> __device__ __forceinline__ R ld_src(const R* p, int coherent) {
+   return coherent ? __ldcg(p) : __ldg(p);
+}
+
+// LOAD = 1: source spins were written earlier in the same launch by other
+// blocks (persistent batched kernel) and are read through L2 (ld.global.cg)
+template <typename R, int FMT, int LOAD = 0>
 __device__ __forceinline__ void exchange_gather(const LLGArgs<R>& a, int i, int mi, const R* __restrict__ sx,
                                                 const R* __restrict__ sy, const R* __restrict__ sz, R& hx,
                                                 R& hy, R& hz) {
@@ -59,7 +75,7 @@ __device__ __forceinline__ void exchange_gather(const LLGArgs<R>& a, int i, int 
       const int e = base + 32 * k;
       const int c = __ldg(a.col + e);
       const int j = c & a.idx_mask;
-      const R x = __ldg(sx + j), y = __ldg(sy + j), z = __ldg(sz + j);
+      const R x = ld_src(sx + j, LOAD), y = ld_src(sy + j, LOAD), z = ld_src(sz + j, LOAD);
       if (FMT == FMT_ISO_TAB) {
          const int mj = a.mat_shift ? (c >> a.mat_shift) : 0;
          const R J = __ldg(tab + mi * a.M + mj);
@@ -94,11 +110,11 @@ __device__ __forceinline__ void exchange_gather(const LLGArgs<R>& a, int i, int 
 
 // spin-dependent field of atom i at spin S: exchange + anisotropy
 // (calculate_spin_fields, src/simulate/fields.cpp:67-118)
-template <typename R, int FMT>
+template <typename R, int FMT, int LOAD = 0>
 __device__ __forceinline__ void spin_field(const LLGArgs<R>& a, int i, int mi, const MatParams<R>& m,
                                            const R* sx, const R* sy, const R* sz, const R S[3], R H[3]) {
    R hx = 0, hy = 0, hz = 0;
-   exchange_gather<R, FMT>(a, i, mi, sx, sy, sz, hx, hy, hz);
+   exchange_gather<R, FMT, LOAD>(a, i, mi, sx, sy, sz, hx, hy, hz);
    if (a.uniaxial) {
       const R sdote = S[0] * m.kux + S[1] * m.kuy + S[2] * m.kuz;
       const R k2 = (R)2 * m.ku2 * sdote;
@@ -123,7 +139,10 @@ __device__ __forceinline__ void external_field(const LLGArgs<R>& a, int i, const
       thermal_xi(a, i, gx, gy, gz);
       ex = gx * m.sigma; ey = gy * m.sigma; ez = gz * m.sigma;
    }
-   if (a.local_field) { ex += a.hx + m.hlx; ey += a.hy + m.hly; ez += a.hz + m.hlz; }
+   if (a.ramp_n) {
+      const R f = (R)(a.step < a.ramp_n ? a.step : a.ramp_n) / (R)a.ramp_n;
+      ex += a.hx + (m.hlx + m.dhx * f); ey += a.hy + (m.hly + m.dhy * f); ez += a.hz + (m.hlz + m.dhz * f);
+   } else if (a.local_field) { ex += a.hx + m.hlx; ey += a.hy + m.hly; ez += a.hz + m.hlz; }
    else { ex += a.hx; ey += a.hy; ez += a.hz; }
    if (a.cell) {
       const int c = __ldg(a.cell + i);

@@ -35,6 +35,7 @@ struct MatParams {
    R kc4;
    R hlx, hly, hlz;   // local applied field (0 if disabled)
    R mu_s_muB;        // moment in Bohr magnetons (stats)
+   R dhx, dhy, dhz;   // field change over a linear sweep (batched systems), added as dh * min(step, n)/n
 };
 
 // Everything one fused LLG pass needs, passed by value.
@@ -53,6 +54,9 @@ struct LLGArgs {
    int uniaxial, cubic;
    R hx, hy, hz;             // global applied field
    int local_field;          // add MatParams::hl*
+   uint64_t ramp_n;          // > 0: add MatParams::dh * min(step, ramp_n) / ramp_n
+   const int* sys_off;       // batched systems: first atom of each system, or nullptr
+   int m_per_sys;            // materials per system (system = material / m_per_sys)
    int thermal;              // add sigma * xi
    int noise_mode;           // VGPU_NOISE_*
    uint32_t seed_lo, seed_hi;
