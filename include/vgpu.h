@@ -294,6 +294,48 @@ int vgpu_stats_get_energy(vgpu_handle h, int32_t id, double* e, double* mean, in
 /* Zero the running means and counters.  Replaces vcuda::stats::reset. */
 int vgpu_stats_reset(vgpu_handle h);
 
+/* ---- batched systems ------------------------------------------------------ */
+
+/* No counterpart in the reference (one system per process there).  Per-system
+ * parameters of a batch: temperature and a linear applied-field sweep
+ * H(step) = H_start + (H_end - H_start) min(step, n_ramp)/n_ramp. */
+typedef struct {
+   double temperature;             /* [K]                                              */
+   double H_start[3];              /* [T]                                              */
+   double H_end[3];                /* [T]                                              */
+   uint64_t n_ramp;                /* steps of the sweep (0: constant H_start)         */
+} vgpu_batch_system;
+
+/* One handle for n_sys independent systems of uneven sizes (same number of
+ * materials and exchange type each).  The returned handle accepts the
+ * single-system calls (vgpu_llg_heun steps all systems with two plain launches
+ * per step; vgpu_get_spins returns all systems concatenated); system k's
+ * Philox stream equals that of a single run seeded seed + k. */
+int vgpu_batch_create(int device, int precision, int32_t n_sys, const vgpu_system_desc* descs,
+                      const vgpu_batch_system* systems, const vgpu_sim_params* common, vgpu_handle* out);
+
+/* Shape of the persistent launch: thread-block cluster size (1, 2, 4, 8) and
+ * threads per block; systems are bin-packed onto the co-resident clusters. */
+int vgpu_batch_set_shape(vgpu_handle h, int32_t cluster, int32_t block);
+
+/* Time every candidate shape for trial_steps steps on this batch and keep the
+ * fastest (the state is restored afterwards). */
+int vgpu_batch_autotune(vgpu_handle h, int32_t trial_steps, int32_t* cluster_out, int32_t* block_out,
+                        double* ms_per_step_out);
+
+/* Advance n_steps with the persistent kernel (one launch per record_every
+ * steps, or per 1000 when record_every is 0); record_every > 0 also stores
+ * every system's magnetisation after each chunk; use_graph != 0 replays the
+ * chunk as a CUDA graph. */
+int vgpu_batch_run(vgpu_handle h, uint64_t n_steps, uint32_t record_every, int32_t use_graph);
+
+/* Records of the last vgpu_batch_run: out[(r*n_sys + k)*4 + {0..3}] =
+ * (m_hat_x, m_hat_y, m_hat_z, |m|/m_sat) of system k after record r. */
+int vgpu_batch_history(vgpu_handle h, double* out, int64_t max_records, int64_t* n_records);
+
+/* First atom and atom count of system k in the concatenated spin arrays. */
+int vgpu_batch_system_range(vgpu_handle h, int32_t k, int32_t* first_atom, int32_t* num_atoms);
+
 /* ---- magnetisation without device allocation ----------------------------- */
 
 /* No counterpart in the reference: an addition for callers that cannot call

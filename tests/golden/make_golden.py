@@ -132,7 +132,7 @@ def fcc10_dipole_macrocell():
 
 MC_MAT = SC_MAT.replace("initial-spin-direction=random", "initial-spin-direction=0,0,1")
 MC_TEMPS = [50.0 * k for k in range(31)]
-MC_EQ, MC_AV, MC_EVERY = 2000, 4000, 10
+MC_EQ, MC_AV, MC_EVERY = 2000, 20000, 10
 
 
 def _mc_one(T):
@@ -142,7 +142,7 @@ def _mc_one(T):
     return d
 
 
-def blocking_stats(x: np.ndarray, nblocks: int = 20):
+def blocking_stats(x: np.ndarray, nblocks: int = 10):
     """Mean and standard error of a correlated series from block means."""
     x = np.asarray(x)
     b = x[: len(x) // nblocks * nblocks].reshape(nblocks, -1).mean(1)
@@ -152,8 +152,9 @@ def blocking_stats(x: np.ndarray, nblocks: int = 20):
 def mc_sc16_curie():
     """Reference Metropolis Curie sweep (sequential random-site angle moves,
     montecarlo::mc_step): SC 16^3 periodic, config-0 material, H=0, spins
-    start along z, 31 temperatures 0..1500 K, 2000 equilibration + 4000
-    averaging sweeps, |m| sampled every 10 sweeps.  Independent processes,
+    start along z, 31 temperatures 0..1500 K, 2000 equilibration + 20000
+    averaging sweeps, |m| sampled every 10 sweeps, standard errors from 10
+    blocks of 2000 sweeps.  Independent processes,
     one per temperature."""
     from concurrent.futures import ThreadPoolExecutor
     import os

@@ -82,7 +82,7 @@ def _tc_fit(T, m):
     return p[0]
 
 
-def _blocking(x, nb=20):
+def _blocking(x, nb=10):
     b = x[: len(x) // nb * nb].reshape(nb, -1).mean(1)
     return x.mean(), b.std(ddof=1) / np.sqrt(nb)
 
@@ -94,7 +94,7 @@ def test_curie_sweep_matches_reference_statistically(vgpu_lib):
     s = O.system_from_dump(d)
     s.params.H_applied = 0.0
     s.spins = np.tile(np.array([[0.0], [0.0], [1.0]]), (1, s.n))
-    eq, av, every = 2000, 12000, 10
+    eq, av, every = 2000, 20000, 10
     got, se = [], []
     with vgpu.Simulation(s, noise_seed=77) as sim:
         mid = sim.add_mask(*s.masks["system"])
@@ -115,7 +115,8 @@ def test_curie_sweep_matches_reference_statistically(vgpu_lib):
             se.append(e)
     got, se = np.array(got), np.array(se)
     ref, rse = d["m_mean"], d["m_se"]
-    z = np.abs(got - ref) / np.sqrt(se ** 2 + rse ** 2 + 1e-18)
+    # 1e-6 floor: FP32 spins give |m| = 1 - O(1e-9) where both runs are frozen
+    z = np.abs(got - ref) / np.sqrt(se ** 2 + rse ** 2 + 1e-12)
     print("m_gpu", np.round(got, 4))
     print("m_ref", np.round(ref, 4))
     print("z", np.round(z, 2))

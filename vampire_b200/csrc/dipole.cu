@@ -88,40 +88,62 @@ __global__ void cell_moment_kernel(int nc, const int* __restrict__ start, const 
 }
 
 // K6: far field by tiled all-pairs sum (FP32 terms, FP64 across tiles).
-__global__ void __launch_bounds__(256) cell_field_kernel(int nc, const float4* __restrict__ pos,
-                                                         const float4* __restrict__ mom,
-                                                         double* __restrict__ field) {
-   __shared__ float4 sp[256];
-   __shared__ float4 sm[256];
-   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-   const float4 pi = i < nc ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-   double ax = 0.0, ay = 0.0, az = 0.0;
-   for (int base = 0; base < nc; base += 256) {
+// Each thread owns TPT target cells so that every source cell read from
+// shared memory serves TPT pair terms.  No branches in the inner loop: empty
+// cells carry zero moment and sit far away (their terms vanish), and the
+// self pair (r = 0) is removed by taking 1/r = 0 there.
+constexpr int kFieldTile = 256;
+constexpr int kTargetsPerThread = 4;
+
+__global__ void __launch_bounds__(kFieldTile) cell_field_kernel(int nc, const float4* __restrict__ pos,
+                                                                const float4* __restrict__ mom,
+                                                                double* __restrict__ field) {
+   __shared__ float4 sp[kFieldTile];
+   __shared__ float4 sm[kFieldTile];
+   constexpr int T = kTargetsPerThread;
+   const int i0 = blockIdx.x * (kFieldTile * T) + threadIdx.x;
+   float px[T], py[T], pz[T];
+   double ax[T], ay[T], az[T];
+#pragma unroll
+   for (int q = 0; q < T; ++q) {
+      const int i = i0 + q * kFieldTile;
+      const float4 p = i < nc ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      px[q] = p.x; py[q] = p.y; pz[q] = p.z;
+      ax[q] = ay[q] = az[q] = 0.0;
+   }
+   for (int base = 0; base < nc; base += kFieldTile) {
       const int j = base + threadIdx.x;
-      sp[threadIdx.x] = j < nc ? pos[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+      sp[threadIdx.x] = j < nc ? pos[j] : make_float4(1e9f, 1e9f, 1e9f, 0.f);
       sm[threadIdx.x] = j < nc ? mom[j] : make_float4(0.f, 0.f, 0.f, 0.f);
       __syncthreads();
-      float fx = 0.f, fy = 0.f, fz = 0.f;
-      const int cnt = min(256, nc - base);
-      for (int k = 0; k < cnt; ++k) {
+      float fx[T], fy[T], fz[T];
+#pragma unroll
+      for (int q = 0; q < T; ++q) fx[q] = fy[q] = fz[q] = 0.f;
+#pragma unroll 4
+      for (int k = 0; k < kFieldTile; ++k) {
          const float4 pj = sp[k];
-         if (pj.w == 0.f || base + k == i) continue;
          const float4 mj = sm[k];
-         const float rx = pj.x - pi.x, ry = pj.y - pi.y, rz = pj.z - pi.z;
-         const float r2 = rx * rx + ry * ry + rz * rz;
-         const float ri = rsqrtf(r2);
-         const float ri2 = ri * ri;
-         const float ri3 = ri2 * ri;
-         const float mr = 3.f * (mj.x * rx + mj.y * ry + mj.z * rz) * ri2;
-         fx += (mr * rx - mj.x) * ri3;
-         fy += (mr * ry - mj.y) * ri3;
-         fz += (mr * rz - mj.z) * ri3;
+#pragma unroll
+         for (int q = 0; q < T; ++q) {
+            const float rx = pj.x - px[q], ry = pj.y - py[q], rz = pj.z - pz[q];
+            const float r2 = rx * rx + ry * ry + rz * rz;
+            const float ri = r2 > 0.f ? rsqrtf(r2) : 0.f;
+            const float ri2 = ri * ri;
+            const float ri3 = ri2 * ri;
+            const float mr = 3.f * (mj.x * rx + mj.y * ry + mj.z * rz) * ri2;
+            fx[q] += (mr * rx - mj.x) * ri3;
+            fy[q] += (mr * ry - mj.y) * ri3;
+            fz[q] += (mr * rz - mj.z) * ri3;
+         }
       }
-      ax += fx; ay += fy; az += fz;
+#pragma unroll
+      for (int q = 0; q < T; ++q) { ax[q] += fx[q]; ay[q] += fy[q]; az[q] += fz[q]; }
       __syncthreads();
    }
-   if (i < nc) {
-      field[i] = ax; field[nc + i] = ay; field[2 * nc + i] = az;
+#pragma unroll
+   for (int q = 0; q < T; ++q) {
+      const int i = i0 + q * kFieldTile;
+      if (i < nc) { field[i] = ax[q]; field[nc + i] = ay[q]; field[2 * nc + i] = az[q]; }
    }
 }
 
@@ -238,7 +260,8 @@ static int dipole_update_typed(vgpu_ctx* h) {
    cell_moment_kernel<R><<<(nc * 32 + 255) / 256, 256, 0, h->stream>>>(
        nc, d->cell_start, d->cell_atoms, (const R*)S.s[0], (const R*)S.s[1], (const R*)S.s[2], (const int*)S.mat,
        (const MatParams<R>*)S.mp, S.mus_SI, d->mag, d->pos, d->mom);
-   cell_field_kernel<<<(nc + 255) / 256, 256, 0, h->stream>>>(nc, d->pos, d->mom, d->field);
+   cell_field_kernel<<<(nc + kFieldTile * kTargetsPerThread - 1) / (kFieldTile * kTargetsPerThread), kFieldTile, 0,
+                       h->stream>>>(nc, d->pos, d->mom, d->field);
    cell_finish_kernel<R><<<(nc + 1 + 255) / 256, 256, 0, h->stream>>>(
        nc, d->near_start, d->near_j, d->near_t, d->npairs, d->mag, d->self, d->pos, d->field, (R*)d->table_b,
        (R*)d->table_hd);
@@ -311,8 +334,11 @@ extern "C" int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* dd) {
    std::vector<float4> pos(nc);
    std::vector<double> self(nc);
    for (int c = 0; c < nc; ++c) {
-      pos[c] = make_float4((float)dd->cell_pos_mom[4 * c], (float)dd->cell_pos_mom[4 * c + 1],
-                           (float)dd->cell_pos_mom[4 * c + 2], dd->cell_natoms[c] > 0 ? 1.f : 0.f);
+      // empty cells (zero moment) are parked far away so K6 needs no test for them
+      pos[c] = dd->cell_natoms[c] > 0
+                   ? make_float4((float)dd->cell_pos_mom[4 * c], (float)dd->cell_pos_mom[4 * c + 1],
+                                 (float)dd->cell_pos_mom[4 * c + 2], 1.f)
+                   : make_float4(1e9f, 1e9f, 1e9f, 0.f);
       self[c] = dd->cell_natoms[c] > 0 ? 8.0 * M_PI / (3.0 * dd->cell_volume[c]) : 0.0;
    }
    // near pairs (tensor solver), classified in FP64 exactly as inter.cpp:66,83

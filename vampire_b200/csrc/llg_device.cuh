@@ -108,13 +108,77 @@ __device__ __forceinline__ void exchange_gather(const LLGArgs<R>& a, int i, int 
    }
 }
 
+// Row of compile-time width W read from packed 16-byte bond records
+// {neighbour | material bits, d_x, d_y, d_z} (FMT_DMI_TAB) or from the
+// neighbour index alone (FMT_ISO_TAB), fully unrolled so that all W record
+// loads and 3W neighbour-spin loads of a thread are in flight together.
+// Same arithmetic, in the same bond order, as exchange_gather.
+template <typename R, int FMT, int W, int LOAD>
+__device__ __forceinline__ void exchange_gather_w(const LLGArgs<R>& a, int base, int mi, const R* __restrict__ sx,
+                                                  const R* __restrict__ sy, const R* __restrict__ sz, R& hx, R& hy,
+                                                  R& hz) {
+   const R* __restrict__ tab = a.jtab;
+   if (FMT == FMT_DMI_TAB) {
+      int4 rec[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k) rec[k] = __ldg(a.rec + base + 32 * k);
+      R x[W], y[W], z[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+         const int j = rec[k].x & a.idx_mask;
+         x[k] = ld_src(sx + j, LOAD); y[k] = ld_src(sy + j, LOAD); z[k] = ld_src(sz + j, LOAD);
+      }
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+         const int mj = a.mat_shift ? (rec[k].x >> a.mat_shift) : 0;
+         const R* t = tab + 3 * (mi * a.M + mj);
+         const R dx = __int_as_float(rec[k].y), dy = __int_as_float(rec[k].z), dz = __int_as_float(rec[k].w);
+         hx += __ldg(t) * x[k] + (dy * z[k] - dz * y[k]);
+         hy += __ldg(t + 1) * y[k] + (dz * x[k] - dx * z[k]);
+         hz += __ldg(t + 2) * z[k] + (dx * y[k] - dy * x[k]);
+      }
+   } else {  // FMT_ISO_TAB
+      int c[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k) c[k] = __ldg(a.col + base + 32 * k);
+      R x[W], y[W], z[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+         const int j = c[k] & a.idx_mask;
+         x[k] = ld_src(sx + j, LOAD); y[k] = ld_src(sy + j, LOAD); z[k] = ld_src(sz + j, LOAD);
+      }
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+         const int mj = a.mat_shift ? (c[k] >> a.mat_shift) : 0;
+         const R J = __ldg(tab + mi * a.M + mj);
+         hx += J * x[k]; hy += J * y[k]; hz += J * z[k];
+      }
+   }
+}
+
+// exchange field with the fixed-width fast paths (FP32, packed records)
+template <typename R, int FMT, int LOAD>
+__device__ __forceinline__ void exchange_field(const LLGArgs<R>& a, int i, int mi, const R* __restrict__ sx,
+                                               const R* __restrict__ sy, const R* __restrict__ sz, R& hx, R& hy,
+                                               R& hz) {
+   if (sizeof(R) == 4 && (FMT == FMT_DMI_TAB || FMT == FMT_ISO_TAB) && (FMT == FMT_ISO_TAB || a.rec)) {
+      const int sl = i >> 5;
+      const int off = __ldg(a.slice_off + sl);
+      const int w = (__ldg(a.slice_off + sl + 1) - off) >> 5;
+      const int base = off + (i & 31);
+      if (w == 12) { exchange_gather_w<R, FMT, 12, LOAD>(a, base, mi, sx, sy, sz, hx, hy, hz); return; }
+      if (w == 6) { exchange_gather_w<R, FMT, 6, LOAD>(a, base, mi, sx, sy, sz, hx, hy, hz); return; }
+   }
+   exchange_gather<R, FMT, LOAD>(a, i, mi, sx, sy, sz, hx, hy, hz);
+}
+
 // spin-dependent field of atom i at spin S: exchange + anisotropy
 // (calculate_spin_fields, src/simulate/fields.cpp:67-118)
 template <typename R, int FMT, int LOAD = 0>
 __device__ __forceinline__ void spin_field(const LLGArgs<R>& a, int i, int mi, const MatParams<R>& m,
                                            const R* sx, const R* sy, const R* sz, const R S[3], R H[3]) {
    R hx = 0, hy = 0, hz = 0;
-   exchange_gather<R, FMT, LOAD>(a, i, mi, sx, sy, sz, hx, hy, hz);
+   exchange_field<R, FMT, LOAD>(a, i, mi, sx, sy, sz, hx, hy, hz);
    if (a.uniaxial) {
       const R sdote = S[0] * m.kux + S[1] * m.kuy + S[2] * m.kuz;
       const R k2 = (R)2 * m.ku2 * sdote;

@@ -25,6 +25,58 @@
 
 namespace vgpu {
 
+// Predictor of atom i: s' = n(s0 + dt f(s0, H)).  LOAD = 1 reads neighbour
+// spins through L2 (they may have been written earlier in the same launch).
+template <typename R, int FMT, int LOAD>
+__device__ __forceinline__ void llg_predict_atom(const LLGArgs<R>& a, int i) {
+   const int mi = a.mat ? __ldg(a.mat + i) : 0;
+   const MatParams<R> m = a.mp[mi];
+   const R S0[3] = {a.ax[i], a.ay[i], a.az[i]};
+   R H[3], E[3];
+   spin_field<R, FMT, LOAD>(a, i, mi, m, a.ax, a.ay, a.az, S0, H);
+   external_field<R>(a, i, m, true, E);
+   H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
+   R d[3];
+   llg_rhs<R>(m.A, m.B, S0, H, d);
+   if (a.ex) { a.ex[i] = d[0]; a.ey[i] = d[1]; a.ez[i] = d[2]; }
+   R Sn[3] = {S0[0] + d[0] * a.dt, S0[1] + d[1] * a.dt, S0[2] + d[2] * a.dt};
+   const R r = rsqrt_<R>(Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2]);
+   a.bx[i] = Sn[0] * r; a.by[i] = Sn[1] * r; a.bz[i] = Sn[2] * r;
+}
+
+// Corrector of atom i: s1 = n(s0 + dt/2 (f0 + f(s', H'))), written over s0.
+template <typename R, int FMT, int LOAD>
+__device__ __forceinline__ void llg_correct_atom(const LLGArgs<R>& a, int i) {
+   const int mi = a.mat ? __ldg(a.mat + i) : 0;
+   const MatParams<R> m = a.mp[mi];
+   const R S0[3] = {a.ax[i], a.ay[i], a.az[i]};
+   const R S1[3] = {a.bx[i], a.by[i], a.bz[i]};
+   R H[3], E[3];
+   spin_field<R, FMT, LOAD>(a, i, mi, m, a.bx, a.by, a.bz, S1, H);
+   external_field<R>(a, i, m, true, E);
+   H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
+   R d[3];
+   llg_rhs<R>(m.A, m.B, S1, H, d);
+   R Sn[3];
+   if (a.ex) {
+      const R e0[3] = {a.ex[i], a.ey[i], a.ez[i]};
+#pragma unroll
+      for (int k = 0; k < 3; ++k) Sn[k] = S0[k] + a.half_dt * (e0[k] + d[k]);
+   } else {
+      const R s00 = S0[0] * S0[0] + S0[1] * S0[1] + S0[2] * S0[2];
+      const R c = s00 / (S1[0] * S0[0] + S1[1] * S0[1] + S1[2] * S0[2]);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+         const R e = S1[k] * c - S0[k];
+         Sn[k] = S0[k] + ((R)0.5 * e + a.half_dt * d[k]);
+      }
+   }
+   const R n2 = Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2];
+   const R r = rsqrt_<R>(n2);
+   if (!(n2 > (R)0.25 && n2 < (R)4)) atomicOr(a.status, 1);
+   a.ax[i] = Sn[0] * r; a.ay[i] = Sn[1] * r; a.az[i] = Sn[2] * r;
+}
+
 template <typename R, int FMT, int MODE>
 __global__ void __launch_bounds__(256) llg_pass_kernel(const LLGArgs<R> a) {
    const int i = blockIdx.x * blockDim.x + threadIdx.x;

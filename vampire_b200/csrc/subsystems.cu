@@ -14,6 +14,7 @@ void vgpu_ctx::destroy_extras() {
    stats_destroy(this);
    mc_destroy(this);
    dipole_destroy(this);
+   batch_destroy(this);
 }
 
 cudaEvent_t vgpu_ctx::get_event() {

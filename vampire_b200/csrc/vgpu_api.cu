@@ -144,8 +144,9 @@ static int validate(vgpu_ctx* h, const vgpu_system_desc* d) {
    if (!d) return set_err(h, VGPU_ERR_ARG, "null system descriptor");
    if (d->num_atoms <= 0) return set_err(h, VGPU_ERR_ARG, "num_atoms must be positive (got %d)", d->num_atoms);
    if (d->num_atoms > (1 << 30)) return set_err(h, VGPU_ERR_ARG, "num_atoms too large");
-   if (d->num_materials <= 0 || d->num_materials > 100)
-      return set_err(h, VGPU_ERR_ARG, "num_materials must be in 1..100 (got %d)", d->num_materials);
+   const int max_mat = (h && h->batch_materials) ? 65536 : 100;  // mp::max_materials
+   if (d->num_materials <= 0 || d->num_materials > max_mat)
+      return set_err(h, VGPU_ERR_ARG, "num_materials must be in 1..%d (got %d)", max_mat, d->num_materials);
    if (d->exchange_type < 0 || d->exchange_type > 2)
       return set_err(h, VGPU_ERR_ARG, "unknown exchange_type %d", d->exchange_type);
    if (!d->nl_start || !d->nl_end || (d->num_bonds > 0 && (!d->nl || !d->jlist)) || !d->type || !d->materials ||
@@ -254,6 +255,17 @@ static int upload_typed(vgpu_ctx* h, const vgpu_system_desc* d) {
    if ((rc = upload_vec(h, &S.col, col, "neighbour index"))) return rc;
    for (int q = 0; q < nper; ++q)
       if ((rc = upload_vec(h, &S.jb[q], jb[q], "bond couplings"))) return rc;
+   if (fmt == FMT_DMI_TAB && sizeof(R) == 4) {
+      // one 16-byte record per bond for the fused passes: {index, d_x, d_y, d_z}
+      std::vector<int> rec(4 * ne);
+      for (size_t e = 0; e < ne; ++e) {
+         rec[4 * e] = col[e];
+         std::memcpy(&rec[4 * e + 1], &jb[0][e], 4);
+         std::memcpy(&rec[4 * e + 2], &jb[1][e], 4);
+         std::memcpy(&rec[4 * e + 3], &jb[2][e], 4);
+      }
+      if ((rc = upload_vec(h, &S.rec, rec, "bond records"))) return rc;
+   }
    if ((rc = upload_vec(h, &S.jtab, tabR, "coupling table"))) return rc;
    if (M > 1) { if ((rc = upload_vec(h, &S.mat, mat, "materials"))) return rc; }
    if ((rc = upload_vec(h, &S.s[0], ax, "spins"))) return rc;
@@ -290,6 +302,10 @@ int refresh_materials_typed(vgpu_ctx* h) {
       o.kc4 = (R)q.kc4;
       o.hlx = (R)q.applied_field[0]; o.hly = (R)q.applied_field[1]; o.hlz = (R)q.applied_field[2];
       o.mu_s_muB = (R)(q.mu_s_SI / 9.27400915e-24);
+      const double* rp = batch_ramp(h);
+      o.dhx = rp ? (R)rp[3 * m] : (R)0;
+      o.dhy = rp ? (R)rp[3 * m + 1] : (R)0;
+      o.dhz = rp ? (R)rp[3 * m + 2] : (R)0;
    }
    return cuda_err(h, cudaMemcpyAsync(S.mp, mp.data(), sizeof(MatParams<R>) * S.M, cudaMemcpyHostToDevice, h->stream),
                    "material upload");
@@ -314,6 +330,7 @@ LLGArgs<R> make_args(vgpu_ctx* h) {
    a.idx_mask = S.idx_mask;
    a.mat_shift = S.mat_shift;
    for (int q = 0; q < 9; ++q) a.jb[q] = (const R*)S.jb[q];
+   a.rec = (const int4*)S.rec;
    a.jtab = (const R*)S.jtab;
    a.M = S.M;
    a.mat = (const int*)S.mat;
@@ -345,6 +362,9 @@ LLGArgs<R> make_args(vgpu_ctx* h) {
    a.fx = (R*)S.f[0]; a.fy = (R*)S.f[1]; a.fz = (R*)S.f[2];
    a.ex = (R*)S.e[0]; a.ey = (R*)S.e[1]; a.ez = (R*)S.e[2];
    a.status = S.status;
+   a.sys_off = S.sys_off;
+   a.m_per_sys = S.m_per_sys;
+   a.ramp_n = S.ramp_n;
    return a;
 }
 template LLGArgs<float> make_args<float>(vgpu_ctx*);

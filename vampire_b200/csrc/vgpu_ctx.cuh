@@ -22,6 +22,7 @@ struct SysDev {
    void* slice_off = nullptr;
    void* col = nullptr;
    void* jb[9] = {nullptr};
+   void* rec = nullptr;      // packed 16-byte bond records (FP32 FMT_DMI_TAB)
    void* jtab = nullptr;
    void* mat = nullptr;
    void* mp = nullptr;
@@ -41,6 +42,9 @@ struct SysDev {
    void* hd_atom = nullptr;
    void* hm_atom = nullptr;  // per-atom mu0 Hd field for the magnetostatic energy
    void* mc_tab = nullptr;   // Monte Carlo per-material tables
+   const int* sys_off = nullptr;  // batched systems: first atom of each system
+   int m_per_sys = 1;
+   uint64_t ramp_n = 0;      // batched field sweep length (steps)
    std::vector<int> type_host;
    std::vector<int64_t> row_host;  // CSR kept on the host (colouring, sharding)
    std::vector<int> nl_host;
@@ -57,6 +61,8 @@ enum ProfKind : int { PROF_PREDICTOR = 0, PROF_CORRECTOR = 1, PROF_STATS = 2, PR
 void stats_destroy(vgpu_ctx* h);
 void mc_destroy(vgpu_ctx* h);
 void dipole_destroy(vgpu_ctx* h);
+void batch_destroy(vgpu_ctx* h);
+const double* batch_ramp(vgpu_ctx* h);
 
 }  // namespace vgpu
 
@@ -73,6 +79,7 @@ struct vgpu_ctx {
    int noise_mode = VGPU_NOISE_PHILOX;
    bool any_sigma = false;
    int store_increment = -1;  // -1: default (on for FP64, off for FP32)
+   bool batch_materials = false;  // batch handle: material rows are per system (no 100 limit)
 
    void* alloc(size_t bytes);
    void free_system();

@@ -47,6 +47,7 @@ struct LLGArgs {
    int idx_mask;             // mask of the neighbour index bits
    int mat_shift;            // shift of the neighbour material bits (0: unpacked)
    const R* jb[9];           // per-bond exchange arrays in SELL layout
+   const int4* rec;          // FP32 FMT_DMI_TAB: packed {index, d_x, d_y, d_z} per bond, or nullptr
    const R* jtab;            // material-pair table (M*M or M*M*3)
    int M;                    // number of materials
    const int* mat;           // [n] material id, or nullptr when M == 1
