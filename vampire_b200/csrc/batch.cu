@@ -525,7 +525,7 @@ extern "C" int vgpu_batch_system_range(vgpu_handle h, int32_t k, int32_t* first_
 }
 
 // field sweep of every material row (refresh_materials reads it)
-const double* batch_ramp(vgpu_ctx* h) {
+const double* vgpu::batch_ramp(vgpu_ctx* h) {
    BatchState* b = batch_of(h);
    return b ? b->ramp.data() : nullptr;
 }
