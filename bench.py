@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-dipole", action="store_true", help="leave out the macrocell dipole field")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and Monte Carlo side results")
     ap.add_argument("--e2e-steps", type=int, default=200)
     return ap.parse_args()
 
@@ -136,6 +137,81 @@ def byte_model(z=12, b_J=12, multi_mat=True, dipole=False):
     L2-served; noise is regenerated in-register (0 B)."""
     gather = 4 * (z + 1) + b_J * z + 4 * int(multi_mat) + 4 * int(dipole)
     return {"predictor": 24 + gather, "corrector": 36 + gather}
+
+
+def bench_batched(device, steps=2000, plain_steps=200):
+    """256 uneven nanoparticles (T ~ U(0,800) K, +2 T -> -2 T sweep): the
+    persistent cluster kernel replayed as a CUDA graph against one plain
+    two-launch sequence per particle (same kernels)."""
+    import torch
+    from vampire_b200 import batch as B
+    from vampire_b200 import vgpu
+    systems, params = B.nanoparticle_ensemble(256)
+    n = sum(s.n for s in systems)
+    with B.Batch(systems, params, device=device) as b:
+        tune = b.autotune(trial_steps=20)
+        b.run(100, record_every=100)
+        torch.cuda.synchronize()
+        stream = torch.cuda.ExternalStream(b_stream(b), device=device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.run(steps, record_every=100)
+        e1.record(stream)
+        e1.synchronize()
+        ms_b = e0.elapsed_time(e1)
+        hist = b.history()
+    sims = []
+    for k, s in enumerate(systems):
+        s.params.temperature = params[k]["temperature"]
+        sims.append(vgpu.Simulation(s, device=device, noise_seed=k))
+    for sim in sims:
+        sim.llg_heun(2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for sim in sims:
+        sim.llg_heun(plain_steps)
+    for sim in sims:
+        sim.synchronize()
+    ms_p = (time.perf_counter() - t0) * 1e3 * steps / plain_steps
+    for sim in sims:
+        sim.close()
+    return {"systems": 256, "spins": n, "steps": steps, "shape": tune,
+            "value": n * steps / (ms_b * 1e-3), "unit": UNIT, "ms": ms_b,
+            "plain_per_system_value": n * steps / (ms_p * 1e-3), "speedup_vs_per_system": ms_p / ms_b,
+            "records": int(hist.shape[0]),
+            "timing": "persistent: CUDA events on the batch stream; per-system: host wall clock of 256 "
+                      f"launch sequences of {plain_steps} steps, scaled to {steps}"}
+
+
+def b_stream(b):
+    import ctypes as C
+    from vampire_b200 import vgpu
+    p = C.c_void_p()
+    vgpu.check(vgpu.lib().vgpu_get_stream(b.handle, C.byref(p)), b.handle)
+    return p.value
+
+
+def bench_mc(device, L=50, sweeps=500):
+    """Checkerboard Metropolis sweep rate on SC 50^3 (125,000 spins), 300 K."""
+    import torch
+    from vampire_b200 import system as S
+    from vampire_b200 import vgpu
+    s = S.config_sc_llg(L, temperature=300.0)
+    s.params.H_applied = 0.0
+    with vgpu.Simulation(s, device=device) as sim:
+        nc = sim.mc_setup()
+        sim.mc_sweep(20)
+        stream = torch.cuda.ExternalStream(sim.stream_ptr(), device=device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sim.synchronize()
+        e0.record(stream)
+        sim.mc_sweep(sweeps)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        moves, rej = sim.mc_counters()
+    return {"spins": s.n, "colours": nc, "sweeps": sweeps, "value": s.n * sweeps / (ms * 1e-3),
+            "unit": "spin-moves/s", "acceptance": 1.0 - rej / moves}
 
 
 def reference_arm(args, rank, world):
@@ -270,6 +346,12 @@ def main():
                        "vgpu_stats_update + vgpu_stats_get_magnetization, then vgpu_get_spins"}
         assert np.isfinite(final).all()
 
+    extra = {}
+    if not args.no_extras:
+        sim.close()
+        extra["batched"] = bench_batched(local)
+        extra["monte_carlo"] = bench_mc(local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -296,6 +378,7 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     sim.close()
     if dist:
