@@ -336,6 +336,24 @@ int vgpu_batch_history(vgpu_handle h, double* out, int64_t max_records, int64_t*
 /* First atom and atom count of system k in the concatenated spin arrays. */
 int vgpu_batch_system_range(vgpu_handle h, int32_t k, int32_t* first_atom, int32_t* num_atoms);
 
+/* ---- adjoint (gradients of a trajectory loss) ----------------------------- */
+
+/* No counterpart in the reference.  From the current spins (left unchanged),
+ * run n_steps deterministic FP64 Heun steps and return
+ *   loss = sum_{t=1..n_steps} w (m_z(t) - target[t-1])^2
+ * (m_z: moment-weighted mean of s_z after step t) and
+ *   grad[0] = dL/d(common scale of every exchange coupling),
+ *   grad[1] = dL/dKu_SI (ku2 = Ku/mu_s), grad[2..4] = dL/dH_applied [1/T],
+ * by the adjoint of the step with checkpoints every `every` steps
+ * (0: ceil(sqrt(n_steps))).  Needs the FP64 build, symmetric (isotropic or
+ * vectorial) exchange, no thermal noise, no dipole field. */
+int vgpu_adjoint_llg(vgpu_handle h, uint64_t n_steps, const double* target, double w, int32_t every,
+                     double* loss_out, double* grad_out);
+
+/* m_z(t), t = 1..n_steps, of a deterministic FP64 run from the current spins
+ * (left unchanged): the targets of vgpu_adjoint_llg. */
+int vgpu_mz_trajectory(vgpu_handle h, uint64_t n_steps, double* mz_out);
+
 /* ---- magnetisation without device allocation ----------------------------- */
 
 /* No counterpart in the reference: an addition for callers that cannot call

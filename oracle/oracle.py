@@ -42,7 +42,7 @@ class VRefSys(C.Structure):
         ("kc4", _D), ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double), ("hloc", _D),
         ("hdx", _D), ("hdy", _D), ("hdz", _D), ("hmx", _D), ("hmy", _D), ("hmz", _D),
         ("dt", C.c_double), ("half_dt", C.c_double), ("H_applied", C.c_double),
-        ("H_vec", C.c_double * 3),
+        ("H_vec", C.c_double * 3), ("mus", _D), ("mus_SI", _D),
     ]
 
 
@@ -125,8 +125,36 @@ class OracleSystem:
         st.H_applied = p.H_applied
         for k in range(3):
             st.H_vec[k] = hv[k]
+        st.mus = _p(arr("mus", m["mu_s_SI"] / 9.27400915e-24, np.float64), _D)
+        st.mus_SI = _p(arr("mus_SI", m["mu_s_SI"], np.float64), _D)
         self.st = st
         self.keep = keep
+
+    # -- adjoint (FP64 CPU) ---------------------------------------------------
+    def adjoint(self, spins, target, w, every=0):
+        """(loss, grad[5]) of L = sum_t w (m_z(t) - target_t)^2 over
+        len(target) steps; grad = dL/d(exchange scale), dL/dKu_SI, dL/dH (3)."""
+        s = np.ascontiguousarray(spins, dtype=np.float64)
+        tg = np.ascontiguousarray(target, dtype=np.float64)
+        g = np.zeros(5)
+        lib().vref_adjoint.restype = C.c_double
+        loss = lib().vref_adjoint(C.byref(self.st), _p(s[0], _D), _p(s[1], _D), _p(s[2], _D),
+                                  C.c_int64(tg.size), _p(tg, _D), C.c_double(w), C.c_int64(every), _p(g, _D))
+        return loss, g
+
+    def trajectory_loss(self, spins, target, w):
+        s = np.ascontiguousarray(spins, dtype=np.float64)
+        tg = np.ascontiguousarray(target, dtype=np.float64)
+        lib().vref_trajectory_loss.restype = C.c_double
+        return lib().vref_trajectory_loss(C.byref(self.st), _p(s[0], _D), _p(s[1], _D), _p(s[2], _D),
+                                          C.c_int64(tg.size), _p(tg, _D), C.c_double(w))
+
+    def mz_trajectory(self, spins, nsteps):
+        s = np.ascontiguousarray(spins, dtype=np.float64)
+        out = np.zeros(nsteps)
+        lib().vref_mz_trajectory(C.byref(self.st), _p(s[0], _D), _p(s[1], _D), _p(s[2], _D),
+                                 C.c_int64(nsteps), _p(out, _D))
+        return out
 
     def llg_heun(self, spins: np.ndarray, n_steps: int, xi: Optional[np.ndarray] = None) -> np.ndarray:
         s = np.ascontiguousarray(spins, dtype=np.float64).copy()

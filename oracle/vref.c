@@ -263,6 +263,269 @@ long vref_mc_colour_sweep(const vref_sys* s, double* sx, double* sy, double* sz,
    return rejects;
 }
 
+/* ------------------------------------------------------------------------
+ * FP64 CPU adjoint of the deterministic Heun step (no reference counterpart:
+ * the reference has no derivatives).  Loss L = sum_{t=1..N} w (m_z(t) - T_t)^2
+ * with m_z the moment-weighted mean of s_z and w the physical time step.
+ * Gradients: dL/d(scale of every exchange coupling), dL/dKu_SI (ku2 = Ku/mu_s),
+ * dL/dH_applied (3 components, Tesla).  Symmetric exchange only (isotropic or
+ * vectorial lists): the transposed gather equals the gather.  Checkpoints
+ * every `every` steps, states recomputed per segment.
+ * ---------------------------------------------------------------------- */
+static void exch_only(const vref_sys* s, const double* x, const double* y, const double* z, double* hx,
+                      double* hy, double* hz) {
+   memset(hx, 0, sizeof(double) * s->n);
+   memset(hy, 0, sizeof(double) * s->n);
+   memset(hz, 0, sizeof(double) * s->n);
+   exchange_fields(s, x, y, z, hx, hy, hz);
+}
+
+static void aniso_field(const vref_sys* s, int i, const double S[3], double H[3]) {
+   const int m = s->type[i];
+   H[0] = H[1] = H[2] = 0.0;
+   if (s->uniaxial) {
+      const double e[3] = {s->kux[m], s->kuy[m], s->kuz[m]};
+      const double k2 = 2.0 * s->ku2[m] * (S[0] * e[0] + S[1] * e[1] + S[2] * e[2]);
+      H[0] += e[0] * k2; H[1] += e[1] * k2; H[2] += e[2] * k2;
+   }
+   if (s->cubic) {
+      const double k4 = 2.0 * s->kc4[m];
+      H[0] += S[0] * S[0] * S[0] * k4; H[1] += S[1] * S[1] * S[1] * k4; H[2] += S[2] * S[2] * S[2] * k4;
+   }
+}
+
+/* vector-Jacobian products of f(s,H) = A s x H + B s x (s x H) */
+static void f_vjp(double A, double B, const double s[3], const double H[3], const double a[3], double sb[3],
+                  double Hb[3]) {
+   const double sH = s[0] * H[0] + s[1] * H[1] + s[2] * H[2];
+   const double as = a[0] * s[0] + a[1] * s[1] + a[2] * s[2];
+   const double aH = a[0] * H[0] + a[1] * H[1] + a[2] * H[2];
+   const double ss = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
+   /* A s x H: d/ds = H x a, d/dH = a x s */
+   sb[0] = A * (H[1] * a[2] - H[2] * a[1]);
+   sb[1] = A * (H[2] * a[0] - H[0] * a[2]);
+   sb[2] = A * (H[0] * a[1] - H[1] * a[0]);
+   Hb[0] = A * (a[1] * s[2] - a[2] * s[1]);
+   Hb[1] = A * (a[2] * s[0] - a[0] * s[2]);
+   Hb[2] = A * (a[0] * s[1] - a[1] * s[0]);
+   /* B (s (s.H) - H (s.s)) */
+   for (int k = 0; k < 3; ++k) {
+      sb[k] += B * (a[k] * sH + as * H[k] - 2.0 * aH * s[k]);
+      Hb[k] += B * (as * s[k] - a[k] * ss);
+   }
+}
+
+static void f_eval(double A, double B, const double S[3], const double H[3], double d[3]) {
+   llg_rhs(A, B, S, H, d);
+}
+
+double vref_adjoint(const vref_sys* s, const double* sx0, const double* sy0, const double* sz0, int64_t nsteps,
+                    const double* target, double w, int64_t every, double* grad) {
+   const int n = s->n;
+   const double dt = s->dt;
+   const double Happ[3] = {s->hx, s->hy, s->hz};
+   double musum = 0.0;
+   for (int i = 0; i < n; ++i) musum += s->mus[s->type[i]];
+   if (every <= 0) every = (int64_t)ceil(sqrt((double)nsteps));
+   const int64_t ncp = (nsteps + every - 1) / every;
+   double* cp = (double*)malloc(sizeof(double) * 3 * n * (ncp + 1));
+   double* seg = (double*)malloc(sizeof(double) * 3 * n * (every + 1));
+   double* mz = (double*)malloc(sizeof(double) * (nsteps + 1));
+   double* work = (double*)malloc(sizeof(double) * 15 * n);
+   double* cur = (double*)malloc(sizeof(double) * 3 * n);
+   memcpy(cur, sx0, sizeof(double) * n);
+   memcpy(cur + n, sy0, sizeof(double) * n);
+   memcpy(cur + 2 * n, sz0, sizeof(double) * n);
+   /* forward with checkpoints and m_z(t) */
+   double loss = 0.0;
+   for (int64_t t = 0; t < nsteps; ++t) {
+      if (t % every == 0) memcpy(cp + 3 * n * (t / every), cur, sizeof(double) * 3 * n);
+      vref_llg_heun_step(s, cur, cur + n, cur + 2 * n, NULL, work);
+      double m = 0.0;
+      for (int i = 0; i < n; ++i) m += s->mus[s->type[i]] * cur[2 * n + i];
+      mz[t + 1] = m / musum;
+      const double r = mz[t + 1] - target[t];
+      loss += w * r * r;
+   }
+   /* backward */
+   double* lam = (double*)calloc(3 * n, sizeof(double));
+   double* ex0 = (double*)malloc(sizeof(double) * 3 * n);
+   double* ex1 = (double*)malloc(sizeof(double) * 3 * n);
+   double* sp = (double*)malloc(sizeof(double) * 3 * n);
+   double* Hb1 = (double*)malloc(sizeof(double) * 3 * n);
+   double* Hb0 = (double*)malloc(sizeof(double) * 3 * n);
+   double* tmp = (double*)malloc(sizeof(double) * 3 * n);
+   double* spb = (double*)malloc(sizeof(double) * 3 * n);
+   double* sb = (double*)malloc(sizeof(double) * 3 * n);
+   double* ub = (double*)malloc(sizeof(double) * 3 * n);
+   double* f0 = (double*)malloc(sizeof(double) * 3 * n);
+   double* nv = (double*)malloc(sizeof(double) * n);
+   double gJ = 0.0, gK = 0.0, gH[3] = {0, 0, 0};
+   /* lambda_N = dL_N/ds_N */
+   for (int i = 0; i < n; ++i) lam[2 * n + i] = 2.0 * w * (mz[nsteps] - target[nsteps - 1]) * s->mus[s->type[i]] / musum;
+   for (int64_t c = ncp - 1; c >= 0; --c) {
+      const int64_t t0 = c * every, t1 = (t0 + every < nsteps) ? t0 + every : nsteps;
+      memcpy(seg, cp + 3 * n * c, sizeof(double) * 3 * n);
+      for (int64_t t = t0; t < t1 - 1; ++t) {
+         double* a = seg + 3 * n * (t - t0);
+         double* b = seg + 3 * n * (t - t0 + 1);
+         memcpy(b, a, sizeof(double) * 3 * n);
+         vref_llg_heun_step(s, b, b + n, b + 2 * n, NULL, work);
+      }
+      for (int64_t t = t1 - 1; t >= t0; --t) {
+         const double* S = seg + 3 * n * (t - t0);
+         /* recompute the step from S */
+         exch_only(s, S, S + n, S + 2 * n, ex0, ex0 + n, ex0 + 2 * n);
+         for (int i = 0; i < n; ++i) {
+            const int m = s->type[i];
+            const double Si[3] = {S[i], S[n + i], S[2 * n + i]};
+            double Ha[3], H[3], d[3];
+            aniso_field(s, i, Si, Ha);
+            for (int k = 0; k < 3; ++k) H[k] = ex0[k * n + i] + Ha[k] + Happ[k];
+            f_eval(s->A[m], s->B[m], Si, H, d);
+            double v[3];
+            for (int k = 0; k < 3; ++k) { f0[k * n + i] = d[k]; v[k] = Si[k] + d[k] * dt; }
+            const double L = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            nv[i] = L;
+            for (int k = 0; k < 3; ++k) sp[k * n + i] = v[k] / L;
+         }
+         exch_only(s, sp, sp + n, sp + 2 * n, ex1, ex1 + n, ex1 + 2 * n);
+         for (int i = 0; i < n; ++i) {
+            const int m = s->type[i];
+            const double Si[3] = {S[i], S[n + i], S[2 * n + i]};
+            const double Sp[3] = {sp[i], sp[n + i], sp[2 * n + i]};
+            double Ha[3], H1[3], f1[3], u[3];
+            aniso_field(s, i, Sp, Ha);
+            for (int k = 0; k < 3; ++k) H1[k] = ex1[k * n + i] + Ha[k] + Happ[k];
+            f_eval(s->A[m], s->B[m], Sp, H1, f1);
+            for (int k = 0; k < 3; ++k) u[k] = Si[k] + 0.5 * dt * (f0[k * n + i] + f1[k]);
+            const double L = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+            const double s1[3] = {u[0] / L, u[1] / L, u[2] / L};
+            const double l[3] = {lam[i], lam[n + i], lam[2 * n + i]};
+            const double ls = l[0] * s1[0] + l[1] * s1[1] + l[2] * s1[2];
+            double u_b[3], a1[3], sdir[3], hb[3];
+            for (int k = 0; k < 3; ++k) { u_b[k] = (l[k] - ls * s1[k]) / L; a1[k] = 0.5 * dt * u_b[k]; }
+            f_vjp(s->A[m], s->B[m], Sp, H1, a1, sdir, hb);
+            for (int k = 0; k < 3; ++k) {
+               ub[k * n + i] = u_b[k];
+               spb[k * n + i] = sdir[k];
+               Hb1[k * n + i] = hb[k];
+               gH[k] += hb[k];
+               gJ += hb[k] * ex1[k * n + i];
+            }
+            if (s->uniaxial) {
+               const double e[3] = {s->kux[m], s->kuy[m], s->kuz[m]};
+               const double he = hb[0] * e[0] + hb[1] * e[1] + hb[2] * e[2];
+               const double se = Sp[0] * e[0] + Sp[1] * e[1] + Sp[2] * e[2];
+               gK += 2.0 * he * se / s->mus_SI[m];
+            }
+         }
+         /* s'bar += transposed exchange gather of H1bar + anisotropy */
+         exch_only(s, Hb1, Hb1 + n, Hb1 + 2 * n, tmp, tmp + n, tmp + 2 * n);
+         for (int i = 0; i < n; ++i) {
+            const int m = s->type[i];
+            const double Si[3] = {S[i], S[n + i], S[2 * n + i]};
+            const double Sp[3] = {sp[i], sp[n + i], sp[2 * n + i]};
+            double spbar[3], hb1[3] = {Hb1[i], Hb1[n + i], Hb1[2 * n + i]};
+            for (int k = 0; k < 3; ++k) spbar[k] = spb[k * n + i] + tmp[k * n + i];
+            if (s->uniaxial) {
+               const double e[3] = {s->kux[m], s->kuy[m], s->kuz[m]};
+               const double he = hb1[0] * e[0] + hb1[1] * e[1] + hb1[2] * e[2];
+               for (int k = 0; k < 3; ++k) spbar[k] += 2.0 * s->ku2[m] * he * e[k];
+            }
+            if (s->cubic)
+               for (int k = 0; k < 3; ++k) spbar[k] += 6.0 * s->kc4[m] * Sp[k] * Sp[k] * hb1[k];
+            const double sps = spbar[0] * Sp[0] + spbar[1] * Sp[1] + spbar[2] * Sp[2];
+            double vb[3], a0[3];
+            for (int k = 0; k < 3; ++k) {
+               vb[k] = (spbar[k] - sps * Sp[k]) / nv[i];
+               a0[k] = 0.5 * dt * ub[k * n + i] + dt * vb[k];
+            }
+            double Ha[3], H0[3], sdir[3], hb[3];
+            aniso_field(s, i, Si, Ha);
+            for (int k = 0; k < 3; ++k) H0[k] = ex0[k * n + i] + Ha[k] + Happ[k];
+            f_vjp(s->A[m], s->B[m], Si, H0, a0, sdir, hb);
+            for (int k = 0; k < 3; ++k) {
+               sb[k * n + i] = ub[k * n + i] + vb[k] + sdir[k];
+               Hb0[k * n + i] = hb[k];
+               gH[k] += hb[k];
+               gJ += hb[k] * ex0[k * n + i];
+            }
+            if (s->uniaxial) {
+               const double e[3] = {s->kux[m], s->kuy[m], s->kuz[m]};
+               const double he = hb[0] * e[0] + hb[1] * e[1] + hb[2] * e[2];
+               const double se = Si[0] * e[0] + Si[1] * e[1] + Si[2] * e[2];
+               gK += 2.0 * he * se / s->mus_SI[m];
+            }
+         }
+         exch_only(s, Hb0, Hb0 + n, Hb0 + 2 * n, tmp, tmp + n, tmp + 2 * n);
+         for (int i = 0; i < n; ++i) {
+            const int m = s->type[i];
+            const double Si[3] = {S[i], S[n + i], S[2 * n + i]};
+            double hb0[3] = {Hb0[i], Hb0[n + i], Hb0[2 * n + i]};
+            for (int k = 0; k < 3; ++k) lam[k * n + i] = sb[k * n + i] + tmp[k * n + i];
+            if (s->uniaxial) {
+               const double e[3] = {s->kux[m], s->kuy[m], s->kuz[m]};
+               const double he = hb0[0] * e[0] + hb0[1] * e[1] + hb0[2] * e[2];
+               for (int k = 0; k < 3; ++k) lam[k * n + i] += 2.0 * s->ku2[m] * he * e[k];
+            }
+            if (s->cubic)
+               for (int k = 0; k < 3; ++k) lam[k * n + i] += 6.0 * s->kc4[m] * Si[k] * Si[k] * hb0[k];
+            if (t >= 1) lam[2 * n + i] += 2.0 * w * (mz[t] - target[t - 1]) * s->mus[m] / musum;
+         }
+      }
+   }
+   grad[0] = gJ; grad[1] = gK; grad[2] = gH[0]; grad[3] = gH[1]; grad[4] = gH[2];
+   free(cp); free(seg); free(mz); free(work); free(cur); free(lam); free(ex0); free(ex1); free(sp);
+   free(Hb1); free(Hb0); free(tmp); free(spb); free(sb); free(ub); free(f0); free(nv);
+   return loss;
+}
+
+/* loss of the forward trajectory only (for finite differences) */
+double vref_trajectory_loss(const vref_sys* s, const double* sx0, const double* sy0, const double* sz0,
+                            int64_t nsteps, const double* target, double w) {
+   const int n = s->n;
+   double musum = 0.0;
+   for (int i = 0; i < n; ++i) musum += s->mus[s->type[i]];
+   double* cur = (double*)malloc(sizeof(double) * 3 * n);
+   double* work = (double*)malloc(sizeof(double) * 15 * n);
+   memcpy(cur, sx0, sizeof(double) * n);
+   memcpy(cur + n, sy0, sizeof(double) * n);
+   memcpy(cur + 2 * n, sz0, sizeof(double) * n);
+   double loss = 0.0;
+   for (int64_t t = 0; t < nsteps; ++t) {
+      vref_llg_heun_step(s, cur, cur + n, cur + 2 * n, NULL, work);
+      double m = 0.0;
+      for (int i = 0; i < n; ++i) m += s->mus[s->type[i]] * cur[2 * n + i];
+      const double r = m / musum - target[t];
+      loss += w * r * r;
+   }
+   free(cur);
+   free(work);
+   return loss;
+}
+
+/* m_z(t) for t = 1..nsteps (targets) */
+void vref_mz_trajectory(const vref_sys* s, const double* sx0, const double* sy0, const double* sz0,
+                        int64_t nsteps, double* mz_out) {
+   const int n = s->n;
+   double musum = 0.0;
+   for (int i = 0; i < n; ++i) musum += s->mus[s->type[i]];
+   double* cur = (double*)malloc(sizeof(double) * 3 * n);
+   double* work = (double*)malloc(sizeof(double) * 15 * n);
+   memcpy(cur, sx0, sizeof(double) * n);
+   memcpy(cur + n, sy0, sizeof(double) * n);
+   memcpy(cur + 2 * n, sz0, sizeof(double) * n);
+   for (int64_t t = 0; t < nsteps; ++t) {
+      vref_llg_heun_step(s, cur, cur + n, cur + 2 * n, NULL, work);
+      double m = 0.0;
+      for (int i = 0; i < n; ++i) m += s->mus[s->type[i]] * cur[2 * n + i];
+      mz_out[t] = m / musum;
+   }
+   free(cur);
+   free(work);
+}
+
 /* magnetization_statistic_t::calculate_magnetization
  * (src/statistics/magnetization.cpp:134-180): per mask bin sum(mu s), sum(mu),
  * normalised to (m_hat, |m|/m_sat); empty bins zeroed.  out: 4*mask_size. */

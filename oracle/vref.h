@@ -38,6 +38,8 @@ typedef struct {
    double dt, half_dt;    /* reduced time step */
    double H_applied;      /* for the applied-field energy */
    double H_vec[3];
+   const double* mus;     /* per material moment in mu_B (adjoint loss weights) */
+   const double* mus_SI;  /* per material moment in J/T */
 } vref_sys;
 
 void vref_spin_fields(const vref_sys* s, const double* sx, const double* sy, const double* sz,
@@ -52,6 +54,12 @@ void vref_spin_energy(const vref_sys* s, const double* sx, const double* sy, con
 long vref_mc_colour_sweep(const vref_sys* s, double* sx, double* sy, double* sz, const int* order,
                           const int* colour_off, int ncolours, const double* rnd, const double* sigma,
                           const double* beta, const double* ratio);
+double vref_adjoint(const vref_sys* s, const double* sx0, const double* sy0, const double* sz0, int64_t nsteps,
+                    const double* target, double w, int64_t every, double* grad);
+double vref_trajectory_loss(const vref_sys* s, const double* sx0, const double* sy0, const double* sz0,
+                            int64_t nsteps, const double* target, double w);
+void vref_mz_trajectory(const vref_sys* s, const double* sx0, const double* sy0, const double* sz0,
+                        int64_t nsteps, double* mz_out);
 void vref_magnetization(int n, const int* mask, int mask_size, const double* sx, const double* sy,
                         const double* sz, const double* mm, double* out);
 void vref_energy(const vref_sys* s, const int* mask, int mask_size, const double* sx,

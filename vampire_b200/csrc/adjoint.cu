@@ -1,0 +1,429 @@
+// Adjoint of the deterministic LLG-Heun trajectory (K8).
+//
+// No counterpart in the reference (which computes no derivatives).  For the
+// loss L = sum_{t=1..N} w (m_z(t) - target_t)^2 (m_z: moment-weighted mean of
+// s_z after step t) the reverse pass runs the step
+//
+//   s' = n(v),  v = s + dt f(s, H(s)),   s1 = n(u),  u = s + dt/2 (f(s,H(s)) + f(s',H(s')))
+//   f(s,H) = A s x H + B s x (s x H),   H(s)_i = sum_j J_ij s_j + anisotropy(s_i) + H_app
+//
+// backwards with four fused per-atom kernels per step: (1) recompute H(s), f,
+// s'; (2) recompute H(s'), f', s1 and push lambda through n(u), f' and H(s');
+// (3) the transposed exchange gather of H(s')-bar, through n(v), f and H(s);
+// (4) the transposed gather of H(s)-bar plus dL_t/ds_t gives lambda_t.  For the
+// symmetric couplings accepted here (isotropic or vectorial lists,
+// J_ij = J_ji) the transposed gather is the forward SELL gather.  Parameter
+// gradients (every coupling scaled together, Ku, H_app) are block-reduced and
+// accumulated in FP64.  States are checkpointed every ceil(sqrt(N)) steps and
+// recomputed segment by segment with the FP64 forward kernels.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "llg_kernels.cuh"
+#include "vgpu_ctx.cuh"
+
+namespace vgpu {
+
+struct AdjBufs {
+   double* S;                   // [3n] state s_t (segment slot)
+   double *sp, *ex0, *ex1, *f0, *ub, *spb, *sb, *Hb0, *Hb1, *lam;   // [3n] each, x|y|z blocks
+   double* nv;                  // [n] |v|
+   double* g;                   // [5] dL/d(J scale), dL/dKu, dL/dH
+   const double* mz;            // [N+1]
+   const double* target;        // [N]
+   double w, musum;
+   int n, stride;               // stride = n_alloc (component offset)
+};
+
+__device__ __forceinline__ void f_vjp_d(double A, double B, const double s[3], const double H[3], const double a[3],
+                                        double sb[3], double Hb[3]) {
+   const double sH = s[0] * H[0] + s[1] * H[1] + s[2] * H[2];
+   const double as = a[0] * s[0] + a[1] * s[1] + a[2] * s[2];
+   const double aH = a[0] * H[0] + a[1] * H[1] + a[2] * H[2];
+   const double ss = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
+   sb[0] = A * (H[1] * a[2] - H[2] * a[1]);
+   sb[1] = A * (H[2] * a[0] - H[0] * a[2]);
+   sb[2] = A * (H[0] * a[1] - H[1] * a[0]);
+   Hb[0] = A * (a[1] * s[2] - a[2] * s[1]);
+   Hb[1] = A * (a[2] * s[0] - a[0] * s[2]);
+   Hb[2] = A * (a[0] * s[1] - a[1] * s[0]);
+#pragma unroll
+   for (int k = 0; k < 3; ++k) {
+      sb[k] += B * (a[k] * sH + as * H[k] - 2.0 * aH * s[k]);
+      Hb[k] += B * (as * s[k] - a[k] * ss);
+   }
+}
+
+__device__ __forceinline__ void aniso_d(const LLGArgs<double>& a, const MatParams<double>& m, const double S[3],
+                                        double H[3]) {
+   H[0] = H[1] = H[2] = 0.0;
+   if (a.uniaxial) {
+      const double k2 = 2.0 * m.ku2 * (S[0] * m.kux + S[1] * m.kuy + S[2] * m.kuz);
+      H[0] += m.kux * k2; H[1] += m.kuy * k2; H[2] += m.kuz * k2;
+   }
+   if (a.cubic) {
+      const double k4 = 2.0 * m.kc4;
+      H[0] += S[0] * S[0] * S[0] * k4; H[1] += S[1] * S[1] * S[1] * k4; H[2] += S[2] * S[2] * S[2] * k4;
+   }
+}
+
+// VJP of the anisotropy field with respect to s (added to sbar)
+__device__ __forceinline__ void aniso_vjp_d(const LLGArgs<double>& a, const MatParams<double>& m, const double S[3],
+                                            const double hb[3], double sb[3]) {
+   if (a.uniaxial) {
+      const double he = hb[0] * m.kux + hb[1] * m.kuy + hb[2] * m.kuz;
+      sb[0] += 2.0 * m.ku2 * he * m.kux; sb[1] += 2.0 * m.ku2 * he * m.kuy; sb[2] += 2.0 * m.ku2 * he * m.kuz;
+   }
+   if (a.cubic) {
+      for (int k = 0; k < 3; ++k) sb[k] += 6.0 * m.kc4 * S[k] * S[k] * hb[k];
+   }
+}
+
+// block-reduce 5 gradient partials and add them to g
+__device__ __forceinline__ void grad_add(double v[5], double* g) {
+#pragma unroll
+   for (int q = 0; q < 5; ++q)
+      for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+   __shared__ double red[5][8];
+   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+   if (l == 0)
+      for (int q = 0; q < 5; ++q) red[q][w] = v[q];
+   __syncthreads();
+   if (threadIdx.x < 5) {
+      double s = 0.0;
+      for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[threadIdx.x][k];
+      atomicAdd(g + threadIdx.x, s);
+   }
+}
+
+template <int FMT>
+__global__ void __launch_bounds__(256) adj_k1(const LLGArgs<double> a, AdjBufs b) {
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= b.n) return;
+   const int st = b.stride;
+   const int mi = a.mat ? a.mat[i] : 0;
+   const MatParams<double> m = a.mp[mi];
+   const double S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
+   double ex[3] = {0, 0, 0}, Ha[3];
+   exchange_gather<double, FMT>(a, i, mi, b.S, b.S + st, b.S + 2 * st, ex[0], ex[1], ex[2]);
+   aniso_d(a, m, S, Ha);
+   const double H[3] = {ex[0] + Ha[0] + a.hx, ex[1] + Ha[1] + a.hy, ex[2] + Ha[2] + a.hz};
+   double d[3];
+   llg_rhs<double>(m.A, m.B, S, H, d);
+   double v[3];
+   for (int k = 0; k < 3; ++k) {
+      b.ex0[k * st + i] = ex[k];
+      b.f0[k * st + i] = d[k];
+      v[k] = S[k] + d[k] * a.dt;
+   }
+   const double L = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+   b.nv[i] = L;
+   for (int k = 0; k < 3; ++k) b.sp[k * st + i] = v[k] / L;
+}
+
+template <int FMT>
+__global__ void __launch_bounds__(256) adj_k2(const LLGArgs<double> a, AdjBufs b) {
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   const int st = b.stride;
+   double gv[5] = {0, 0, 0, 0, 0};
+   if (i < b.n) {
+      const int mi = a.mat ? a.mat[i] : 0;
+      const MatParams<double> m = a.mp[mi];
+      const double S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
+      const double Sp[3] = {b.sp[i], b.sp[st + i], b.sp[2 * st + i]};
+      double ex[3] = {0, 0, 0}, Ha[3];
+      exchange_gather<double, FMT>(a, i, mi, b.sp, b.sp + st, b.sp + 2 * st, ex[0], ex[1], ex[2]);
+      aniso_d(a, m, Sp, Ha);
+      const double H1[3] = {ex[0] + Ha[0] + a.hx, ex[1] + Ha[1] + a.hy, ex[2] + Ha[2] + a.hz};
+      double f1[3], u[3];
+      llg_rhs<double>(m.A, m.B, Sp, H1, f1);
+      for (int k = 0; k < 3; ++k) u[k] = S[k] + 0.5 * a.dt * (b.f0[k * st + i] + f1[k]);
+      const double L = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+      const double s1[3] = {u[0] / L, u[1] / L, u[2] / L};
+      const double l[3] = {b.lam[i], b.lam[st + i], b.lam[2 * st + i]};
+      const double ls = l[0] * s1[0] + l[1] * s1[1] + l[2] * s1[2];
+      double u_b[3], a1[3], sdir[3], hb[3];
+      for (int k = 0; k < 3; ++k) { u_b[k] = (l[k] - ls * s1[k]) / L; a1[k] = 0.5 * a.dt * u_b[k]; }
+      f_vjp_d(m.A, m.B, Sp, H1, a1, sdir, hb);
+      for (int k = 0; k < 3; ++k) {
+         b.ub[k * st + i] = u_b[k];
+         b.spb[k * st + i] = sdir[k];
+         b.Hb1[k * st + i] = hb[k];
+         b.ex1[k * st + i] = ex[k];
+         gv[0] += hb[k] * ex[k];
+         gv[2 + k] += hb[k];
+      }
+      if (a.uniaxial) {
+         const double he = hb[0] * m.kux + hb[1] * m.kuy + hb[2] * m.kuz;
+         const double se = Sp[0] * m.kux + Sp[1] * m.kuy + Sp[2] * m.kuz;
+         gv[1] += 2.0 * he * se / ((double)m.mu_s_muB * 9.27400915e-24);
+      }
+   }
+   grad_add(gv, b.g);
+}
+
+template <int FMT>
+__global__ void __launch_bounds__(256) adj_k3(const LLGArgs<double> a, AdjBufs b) {
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   const int st = b.stride;
+   double gv[5] = {0, 0, 0, 0, 0};
+   if (i < b.n) {
+      const int mi = a.mat ? a.mat[i] : 0;
+      const MatParams<double> m = a.mp[mi];
+      const double S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
+      const double Sp[3] = {b.sp[i], b.sp[st + i], b.sp[2 * st + i]};
+      double t[3] = {0, 0, 0};
+      exchange_gather<double, FMT>(a, i, mi, b.Hb1, b.Hb1 + st, b.Hb1 + 2 * st, t[0], t[1], t[2]);
+      const double hb1[3] = {b.Hb1[i], b.Hb1[st + i], b.Hb1[2 * st + i]};
+      double spbar[3];
+      for (int k = 0; k < 3; ++k) spbar[k] = b.spb[k * st + i] + t[k];
+      aniso_vjp_d(a, m, Sp, hb1, spbar);
+      const double sps = spbar[0] * Sp[0] + spbar[1] * Sp[1] + spbar[2] * Sp[2];
+      double vb[3], a0[3];
+      for (int k = 0; k < 3; ++k) {
+         vb[k] = (spbar[k] - sps * Sp[k]) / b.nv[i];
+         a0[k] = 0.5 * a.dt * b.ub[k * st + i] + a.dt * vb[k];
+      }
+      double Ha[3];
+      aniso_d(a, m, S, Ha);
+      double H0[3], ex[3];
+      for (int k = 0; k < 3; ++k) {
+         ex[k] = b.ex0[k * st + i];
+         H0[k] = ex[k] + Ha[k] + (k == 0 ? a.hx : k == 1 ? a.hy : a.hz);
+      }
+      double sdir[3], hb[3];
+      f_vjp_d(m.A, m.B, S, H0, a0, sdir, hb);
+      for (int k = 0; k < 3; ++k) {
+         b.sb[k * st + i] = b.ub[k * st + i] + vb[k] + sdir[k];
+         b.Hb0[k * st + i] = hb[k];
+         gv[0] += hb[k] * ex[k];
+         gv[2 + k] += hb[k];
+      }
+      if (a.uniaxial) {
+         const double he = hb[0] * m.kux + hb[1] * m.kuy + hb[2] * m.kuz;
+         const double se = S[0] * m.kux + S[1] * m.kuy + S[2] * m.kuz;
+         gv[1] += 2.0 * he * se / ((double)m.mu_s_muB * 9.27400915e-24);
+      }
+   }
+   grad_add(gv, b.g);
+}
+
+template <int FMT>
+__global__ void __launch_bounds__(256) adj_k4(const LLGArgs<double> a, AdjBufs b, int64_t t) {
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= b.n) return;
+   const int st = b.stride;
+   const int mi = a.mat ? a.mat[i] : 0;
+   const MatParams<double> m = a.mp[mi];
+   const double S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
+   double tg[3] = {0, 0, 0};
+   exchange_gather<double, FMT>(a, i, mi, b.Hb0, b.Hb0 + st, b.Hb0 + 2 * st, tg[0], tg[1], tg[2]);
+   const double hb0[3] = {b.Hb0[i], b.Hb0[st + i], b.Hb0[2 * st + i]};
+   double l[3];
+   for (int k = 0; k < 3; ++k) l[k] = b.sb[k * st + i] + tg[k];
+   aniso_vjp_d(a, m, S, hb0, l);
+   if (t >= 1) l[2] += 2.0 * b.w * (b.mz[t] - b.target[t - 1]) * (double)m.mu_s_muB / b.musum;
+   for (int k = 0; k < 3; ++k) b.lam[k * st + i] = l[k];
+}
+
+__global__ void adj_lambda_init(const LLGArgs<double> a, AdjBufs b, int64_t N) {
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= b.n) return;
+   const int mi = a.mat ? a.mat[i] : 0;
+   const int st = b.stride;
+   b.lam[i] = 0.0;
+   b.lam[st + i] = 0.0;
+   b.lam[2 * st + i] = 2.0 * b.w * (b.mz[N] - b.target[N - 1]) * (double)a.mp[mi].mu_s_muB / b.musum;
+}
+
+// m_z after a step: block sums of mu s_z added into out[0]
+template <typename R>
+__global__ void mz_kernel(int n, const R* __restrict__ sz, const int* __restrict__ mat,
+                          const MatParams<R>* __restrict__ mp, double* out) {
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   double v = 0.0;
+   if (i < n) v = (double)sz[i] * (double)mp[mat ? mat[i] : 0].mu_s_muB;
+   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+   __shared__ double red[8];
+   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[k];
+      atomicAdd(out, s);
+   }
+}
+
+template <int FMT>
+static void adj_step(const LLGArgs<double>& a, const AdjBufs& b, int64_t t, cudaStream_t st) {
+   const int g = (b.n + 255) / 256;
+   adj_k1<FMT><<<g, 256, 0, st>>>(a, b);
+   adj_k2<FMT><<<g, 256, 0, st>>>(a, b);
+   adj_k3<FMT><<<g, 256, 0, st>>>(a, b);
+   adj_k4<FMT><<<g, 256, 0, st>>>(a, b, t);
+}
+
+static void adj_step_fmt(int fmt, const LLGArgs<double>& a, const AdjBufs& b, int64_t t, cudaStream_t st) {
+   switch (fmt) {
+      case FMT_ISO_TAB: adj_step<FMT_ISO_TAB>(a, b, t, st); break;
+      case FMT_ISO_BOND: adj_step<FMT_ISO_BOND>(a, b, t, st); break;
+      case FMT_VEC_TAB: adj_step<FMT_VEC_TAB>(a, b, t, st); break;
+      default: adj_step<FMT_VEC_BOND>(a, b, t, st); break;
+   }
+}
+
+}  // namespace vgpu
+
+using namespace vgpu;
+
+namespace {
+
+struct DevVec {
+   double* p = nullptr;
+   ~DevVec() { if (p) cudaFree(p); }
+   cudaError_t alloc(size_t n) { return cudaMalloc(&p, sizeof(double) * std::max<size_t>(n, 1)); }
+};
+
+// one FP64 Heun step of the state in `x` (3 * stride doubles, x|y|z)
+int forward_step(vgpu_ctx* h, LLGArgs<double> a, double* x, double* pb, double* eb, int stride) {
+   a.ax = x; a.ay = x + stride; a.az = x + 2 * stride;
+   a.bx = pb; a.by = pb + stride; a.bz = pb + 2 * stride;
+   a.ex = eb; a.ey = eb + stride; a.ez = eb + 2 * stride;
+   a.thermal = 0;
+   cudaError_t e = launch_llg_pass<double>(a, h->sys.fmt, PASS_PREDICTOR, h->sys.nslices, h->stream);
+   if (e == cudaSuccess) e = launch_llg_pass<double>(a, h->sys.fmt, PASS_CORRECTOR, h->sys.nslices, h->stream);
+   h->kernel_launches += 2;
+   return cuda_err(h, e, "adjoint forward");
+}
+
+int check_adjoint_ok(vgpu_ctx* h) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (h->prec != VGPU_PREC_FP64) return set_err(h, VGPU_ERR_ARG, "the adjoint runs in the FP64 build (VGPU_PREC_FP64)");
+   const int f = h->sys.fmt;
+   if (f != FMT_ISO_TAB && f != FMT_ISO_BOND && f != FMT_VEC_TAB && f != FMT_VEC_BOND)
+      return set_err(h, VGPU_ERR_ARG, "the adjoint supports symmetric (isotropic or vectorial) exchange only");
+   if (h->sys.cell || h->sys.hd_atom || h->sys.sys_off)
+      return set_err(h, VGPU_ERR_ARG, "the adjoint does not support dipole fields or batches");
+   if (h->params.local_applied_field) return set_err(h, VGPU_ERR_ARG, "the adjoint supports the global applied field only");
+   return VGPU_OK;
+}
+
+double moment_sum(vgpu_ctx* h) {
+   double s = 0.0;
+   for (int t : h->sys.type_host) s += h->sys.materials[t].mu_s_SI / 9.27400915e-24;
+   return s;
+}
+
+}  // namespace
+
+extern "C" int vgpu_mz_trajectory(vgpu_handle h, uint64_t n_steps, double* mz_out) {
+   int rc = check_adjoint_ok(h);
+   if (rc) return rc;
+   cudaSetDevice(h->device);
+   SysDev& S = h->sys;
+   const int st = S.n_alloc;
+   DevVec cur, pb, eb, mz;
+   cudaError_t e;
+   if ((e = cur.alloc(3 * (size_t)st)) || (e = pb.alloc(3 * (size_t)st)) || (e = eb.alloc(3 * (size_t)st)) ||
+       (e = mz.alloc(n_steps + 1)))
+      return cuda_err(h, e, "trajectory buffers");
+   for (int q = 0; q < 3; ++q)
+      cudaMemcpyAsync(cur.p + (size_t)q * st, S.s[q], sizeof(double) * st, cudaMemcpyDeviceToDevice, h->stream);
+   cudaMemsetAsync(mz.p, 0, sizeof(double) * (n_steps + 1), h->stream);
+   LLGArgs<double> a = make_args<double>(h);
+   for (uint64_t t = 0; t < n_steps; ++t) {
+      if ((rc = forward_step(h, a, cur.p, pb.p, eb.p, st))) return rc;
+      mz_kernel<double><<<(S.n + 255) / 256, 256, 0, h->stream>>>(S.n, cur.p + 2 * (size_t)st, (const int*)S.mat,
+                                                                   (const MatParams<double>*)S.mp, mz.p + t + 1);
+   }
+   std::vector<double> host(n_steps + 1);
+   e = cudaMemcpyAsync(host.data(), mz.p, sizeof(double) * (n_steps + 1), cudaMemcpyDeviceToHost, h->stream);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+   if (e != cudaSuccess) return cuda_err(h, e, "trajectory");
+   const double ms = moment_sum(h);
+   for (uint64_t t = 0; t < n_steps; ++t) mz_out[t] = host[t + 1] / ms;
+   return VGPU_OK;
+}
+
+extern "C" int vgpu_adjoint_llg(vgpu_handle h, uint64_t n_steps, const double* target, double w, int32_t every,
+                                double* loss_out, double* grad_out) {
+   int rc = check_adjoint_ok(h);
+   if (rc) return rc;
+   if (!target || !loss_out || !grad_out || n_steps == 0) return set_err(h, VGPU_ERR_ARG, "bad adjoint arguments");
+   cudaSetDevice(h->device);
+   SysDev& S = h->sys;
+   const int n = S.n, st = S.n_alloc;
+   const int64_t N = (int64_t)n_steps;
+   const int64_t C = every > 0 ? every : (int64_t)std::ceil(std::sqrt((double)N));
+   const int64_t ncp = (N + C - 1) / C;
+   const size_t v3 = 3 * (size_t)st;
+   DevVec cp, seg, pb, eb, mz, tg, g, work;
+   cudaError_t e;
+   if ((e = cp.alloc(v3 * ncp)) || (e = seg.alloc(v3 * (C + 1))) || (e = pb.alloc(v3)) || (e = eb.alloc(v3)) ||
+       (e = mz.alloc(N + 1)) || (e = tg.alloc(N)) || (e = g.alloc(5)) || (e = work.alloc(v3 * 10 + st)))
+      return cuda_err(h, e, "adjoint buffers");
+   cudaMemcpyAsync(tg.p, target, sizeof(double) * N, cudaMemcpyHostToDevice, h->stream);
+   cudaMemsetAsync(mz.p, 0, sizeof(double) * (N + 1), h->stream);
+   cudaMemsetAsync(g.p, 0, sizeof(double) * 5, h->stream);
+   LLGArgs<double> a = make_args<double>(h);
+   a.thermal = 0;
+   // forward from the current spins (left untouched), checkpoint every C steps
+   double* cur = seg.p;  // first slot doubles as the running state
+   for (int q = 0; q < 3; ++q)
+      cudaMemcpyAsync(cur + (size_t)q * st, S.s[q], sizeof(double) * st, cudaMemcpyDeviceToDevice, h->stream);
+   for (int64_t t = 0; t < N; ++t) {
+      if (t % C == 0)
+         cudaMemcpyAsync(cp.p + v3 * (t / C), cur, sizeof(double) * v3, cudaMemcpyDeviceToDevice, h->stream);
+      if ((rc = forward_step(h, a, cur, pb.p, eb.p, st))) return rc;
+      mz_kernel<double><<<(n + 255) / 256, 256, 0, h->stream>>>(n, cur + 2 * (size_t)st, (const int*)S.mat,
+                                                                 (const MatParams<double>*)S.mp, mz.p + t + 1);
+   }
+   // loss on the host from m_z(t)
+   std::vector<double> mzh(N + 1);
+   e = cudaMemcpyAsync(mzh.data(), mz.p, sizeof(double) * (N + 1), cudaMemcpyDeviceToHost, h->stream);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+   if (e != cudaSuccess) return cuda_err(h, e, "adjoint forward");
+   const double musum = moment_sum(h);
+   // m_z was summed unnormalised: scale the device copy once
+   for (int64_t t = 0; t <= N; ++t) mzh[t] /= musum;
+   cudaMemcpyAsync(mz.p, mzh.data(), sizeof(double) * (N + 1), cudaMemcpyHostToDevice, h->stream);
+   double loss = 0.0;
+   for (int64_t t = 1; t <= N; ++t) {
+      const double r = mzh[t] - target[t - 1];
+      loss += w * r * r;
+   }
+   AdjBufs b;
+   std::memset(&b, 0, sizeof b);
+   double* wk = work.p;
+   b.sp = wk; b.ex0 = wk + v3; b.ex1 = wk + 2 * v3; b.f0 = wk + 3 * v3; b.ub = wk + 4 * v3;
+   b.spb = wk + 5 * v3; b.sb = wk + 6 * v3; b.Hb0 = wk + 7 * v3; b.Hb1 = wk + 8 * v3; b.lam = wk + 9 * v3;
+   b.nv = wk + 10 * v3;
+   b.g = g.p; b.mz = mz.p; b.target = tg.p; b.w = w; b.musum = musum; b.n = n; b.stride = st;
+   adj_lambda_init<<<(n + 255) / 256, 256, 0, h->stream>>>(a, b, N);
+   for (int64_t c = ncp - 1; c >= 0; --c) {
+      const int64_t t0 = c * C, t1 = std::min(t0 + C, N);
+      cudaMemcpyAsync(seg.p, cp.p + v3 * c, sizeof(double) * v3, cudaMemcpyDeviceToDevice, h->stream);
+      for (int64_t t = t0; t < t1 - 1; ++t) {
+         double* nxt = seg.p + v3 * (t - t0 + 1);
+         cudaMemcpyAsync(nxt, seg.p + v3 * (t - t0), sizeof(double) * v3, cudaMemcpyDeviceToDevice, h->stream);
+         if ((rc = forward_step(h, a, nxt, pb.p, eb.p, st))) return rc;
+      }
+      for (int64_t t = t1 - 1; t >= t0; --t) {
+         b.S = seg.p + v3 * (t - t0);
+         adj_step_fmt(S.fmt, a, b, t, h->stream);
+         h->kernel_launches += 4;
+      }
+      if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(h, e, "adjoint backward");
+   }
+   double gh[5];
+   e = cudaMemcpyAsync(gh, g.p, sizeof gh, cudaMemcpyDeviceToHost, h->stream);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+   if (e != cudaSuccess) return cuda_err(h, e, "adjoint result");
+   *loss_out = loss;
+   for (int k = 0; k < 5; ++k) grad_out[k] = gh[k];
+   return VGPU_OK;
+}
