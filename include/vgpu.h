@@ -169,6 +169,18 @@ int vgpu_set_noise_replay(vgpu_handle h, const double* xi);
  * f(s0) dt = s'|s0|^2/(s'.s0) - s0 from the two states it reads anyway;
  * -1 (default) = store in FP64 (bit-exact with the reference), recover in FP32. */
 #define VGPU_OPT_STORE_INCREMENT 1
+/* VGPU_OPT_STAGED_RECORDS (FP32 systems with DMI/vector bond records): 1 = the
+ * fused passes bring each tile's bond records into shared memory with one bulk
+ * copy per tile, 0 = every thread loads its own records, -1 (default) = staged
+ * when a tile's buffers fit in 200 KB of shared memory.  Same results bit for
+ * bit either way.  VGPU_OPT_STAGE_SLICES: 2, 4 or 8 slices of 32 atoms per
+ * tile (default 4); VGPU_OPT_STAGE_BUFFERS: 1 (one tile per block) or 2
+ * (persistent blocks, next tile's copy overlapping this one; default 1).  A
+ * copy that does not complete within a bounded wait fails the step with
+ * VGPU_ERR_TIMEOUT. */
+#define VGPU_OPT_STAGED_RECORDS 2
+#define VGPU_OPT_STAGE_SLICES 3
+#define VGPU_OPT_STAGE_BUFFERS 4
 int vgpu_set_option(vgpu_handle h, int option, int value);
 
 /* Step counter that keys the Philox stream (counter = (atom, step)).  Resume

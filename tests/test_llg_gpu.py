@@ -99,6 +99,39 @@ def test_fp32_stored_increment_option(V):
         assert np.abs(a.spins() - b.spins()).max() < 1e-6
 
 
+@pytest.mark.parametrize("L", [5, 12])
+@pytest.mark.parametrize("sl,nbuf", [(2, 1), (4, 1), (4, 2), (8, 1), (8, 2)])
+def test_staged_records_match_plain(V, L, sl, nbuf):
+    """The bulk-staged passes (records copied per tile into shared memory)
+    give the per-thread-load passes' FP32 results bit for bit: FCC L^3 tensor
+    exchange + DMI, two materials, cubic anisotropy, T=300 K Philox noise.
+    L=5 (500 spins) leaves a ragged last tile; L=12 (6912 spins) gives many
+    tiles per persistent block."""
+    from vampire_b200 import system
+    s = system.config_fcc_tensor(L=L, seed=7)
+    with V.Simulation(s, noise_seed=11) as plain, V.Simulation(s, noise_seed=11) as st:
+        plain.set_option(V.OPT_STAGED_RECORDS, 0)
+        st.set_option(V.OPT_STAGED_RECORDS, 1)
+        st.set_option(V.OPT_STAGE_SLICES, sl)
+        st.set_option(V.OPT_STAGE_BUFFERS, nbuf)
+        plain.llg_heun(25)
+        st.llg_heun(25)
+        np.testing.assert_array_equal(st.spins(), plain.spins())
+
+
+def test_stage_option_checks(V):
+    from vampire_b200 import system
+    s = system.config_fcc_tensor(L=3, seed=7)
+    with V.Simulation(s) as sim:
+        for opt, bad in ((V.OPT_STAGED_RECORDS, 2), (V.OPT_STAGE_SLICES, 6), (V.OPT_STAGE_BUFFERS, 3)):
+            with pytest.raises(V.VGPUError) as e:
+                sim.set_option(opt, bad)
+            assert e.value.code == V.ERR_ARG
+        sim.set_option(V.OPT_STAGED_RECORDS, 1)
+        sim.llg_heun(2)
+        assert np.isfinite(sim.spins()).all()
+
+
 @pytest.mark.parametrize("name,steps", [("sc10_t300", 2), ("sc6_open_t300", 3), ("fcc4_dmi_t300", 2)])
 @pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("fp32", TOL32)])
 def test_replayed_noise(V, name, steps, prec, tol):

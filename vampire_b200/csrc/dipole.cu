@@ -111,10 +111,14 @@ __global__ void __launch_bounds__(kFieldTile) cell_field_kernel(int nc, const fl
       px[q] = p.x; py[q] = p.y; pz[q] = p.z;
       ax[q] = ay[q] = az[q] = 0.0;
    }
-   for (int base = 0; base < nc; base += kFieldTile) {
+   // blockIdx.y selects a contiguous share of the source cells; partial sums
+   // of the shares meet in FP64 atomics (field is zeroed before the launch)
+   const int per = (nc + gridDim.y - 1) / gridDim.y;
+   const int src0 = blockIdx.y * per, src1 = min(nc, src0 + per);
+   for (int base = src0; base < src1; base += kFieldTile) {
       const int j = base + threadIdx.x;
-      sp[threadIdx.x] = j < nc ? pos[j] : make_float4(1e9f, 1e9f, 1e9f, 0.f);
-      sm[threadIdx.x] = j < nc ? mom[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+      sp[threadIdx.x] = j < src1 ? pos[j] : make_float4(1e9f, 1e9f, 1e9f, 0.f);
+      sm[threadIdx.x] = j < src1 ? mom[j] : make_float4(0.f, 0.f, 0.f, 0.f);
       __syncthreads();
       float fx[T], fy[T], fz[T];
 #pragma unroll
@@ -143,7 +147,11 @@ __global__ void __launch_bounds__(kFieldTile) cell_field_kernel(int nc, const fl
 #pragma unroll
    for (int q = 0; q < T; ++q) {
       const int i = i0 + q * kFieldTile;
-      if (i < nc) { field[i] = ax[q]; field[nc + i] = ay[q]; field[2 * nc + i] = az[q]; }
+      if (i < nc) {
+         atomicAdd(field + i, ax[q]);
+         atomicAdd(field + nc + i, ay[q]);
+         atomicAdd(field + 2 * nc + i, az[q]);
+      }
    }
 }
 
@@ -260,8 +268,15 @@ static int dipole_update_typed(vgpu_ctx* h) {
    cell_moment_kernel<R><<<(nc * 32 + 255) / 256, 256, 0, h->stream>>>(
        nc, d->cell_start, d->cell_atoms, (const R*)S.s[0], (const R*)S.s[1], (const R*)S.s[2], (const int*)S.mat,
        (const MatParams<R>*)S.mp, S.mus_SI, d->mag, d->pos, d->mom);
-   cell_field_kernel<<<(nc + kFieldTile * kTargetsPerThread - 1) / (kFieldTile * kTargetsPerThread), kFieldTile, 0,
-                       h->stream>>>(nc, d->pos, d->mom, d->field);
+   {
+      // enough blocks for every SM: split the sources when the targets alone are too few
+      const int tblocks = (nc + kFieldTile * kTargetsPerThread - 1) / (kFieldTile * kTargetsPerThread);
+      int sms = 148;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+      const int splits = std::max(1, std::min(64, (6 * sms + tblocks - 1) / tblocks));
+      cudaMemsetAsync(d->field, 0, sizeof(double) * 3 * nc, h->stream);
+      cell_field_kernel<<<dim3(tblocks, splits), kFieldTile, 0, h->stream>>>(nc, d->pos, d->mom, d->field);
+   }
    cell_finish_kernel<R><<<(nc + 1 + 255) / 256, 256, 0, h->stream>>>(
        nc, d->near_start, d->near_j, d->near_t, d->npairs, d->mag, d->self, d->pos, d->field, (R*)d->table_b,
        (R*)d->table_hd);

@@ -113,15 +113,17 @@ __device__ __forceinline__ void exchange_gather(const LLGArgs<R>& a, int i, int 
 // neighbour index alone (FMT_ISO_TAB), fully unrolled so that all W record
 // loads and 3W neighbour-spin loads of a thread are in flight together.
 // Same arithmetic, in the same bond order, as exchange_gather.
-template <typename R, int FMT, int W, int LOAD>
+// STAGED: the records of this row were bulk-copied to shared memory; srec
+// points at the thread's first record there (stride 32 records per bond).
+template <typename R, int FMT, int W, int LOAD, bool STAGED>
 __device__ __forceinline__ void exchange_gather_w(const LLGArgs<R>& a, int base, int mi, const R* __restrict__ sx,
                                                   const R* __restrict__ sy, const R* __restrict__ sz, R& hx, R& hy,
-                                                  R& hz) {
+                                                  R& hz, const int4* srec) {
    const R* __restrict__ tab = a.jtab;
    if (FMT == FMT_DMI_TAB) {
       int4 rec[W];
 #pragma unroll
-      for (int k = 0; k < W; ++k) rec[k] = __ldg(a.rec + base + 32 * k);
+      for (int k = 0; k < W; ++k) rec[k] = STAGED ? srec[32 * k] : __ldg(a.rec + base + 32 * k);
       R x[W], y[W], z[W];
 #pragma unroll
       for (int k = 0; k < W; ++k) {
@@ -131,11 +133,19 @@ __device__ __forceinline__ void exchange_gather_w(const LLGArgs<R>& a, int base,
 #pragma unroll
       for (int k = 0; k < W; ++k) {
          const int mj = a.mat_shift ? (rec[k].x >> a.mat_shift) : 0;
-         const R* t = tab + 3 * (mi * a.M + mj);
          const R dx = __int_as_float(rec[k].y), dy = __int_as_float(rec[k].z), dz = __int_as_float(rec[k].w);
-         hx += __ldg(t) * x[k] + (dy * z[k] - dz * y[k]);
-         hy += __ldg(t + 1) * y[k] + (dz * x[k] - dx * z[k]);
-         hz += __ldg(t + 2) * z[k] + (dx * y[k] - dy * x[k]);
+         if (a.tab_scalar) {
+            // isotropic diagonal: one coupling per material pair (scalar table)
+            const R J = __ldg(a.jtab_s + mi * a.M + mj);
+            hx += J * x[k] + (dy * z[k] - dz * y[k]);
+            hy += J * y[k] + (dz * x[k] - dx * z[k]);
+            hz += J * z[k] + (dx * y[k] - dy * x[k]);
+         } else {
+            const R* t = tab + 3 * (mi * a.M + mj);
+            hx += __ldg(t) * x[k] + (dy * z[k] - dz * y[k]);
+            hy += __ldg(t + 1) * y[k] + (dz * x[k] - dx * z[k]);
+            hz += __ldg(t + 2) * z[k] + (dx * y[k] - dy * x[k]);
+         }
       }
    } else {  // FMT_ISO_TAB
       int c[W];
@@ -156,29 +166,33 @@ __device__ __forceinline__ void exchange_gather_w(const LLGArgs<R>& a, int base,
    }
 }
 
-// exchange field with the fixed-width fast paths (FP32, packed records)
-template <typename R, int FMT, int LOAD>
+// exchange field with the fixed-width fast paths (FP32, packed records).
+// STAGED (FMT_DMI_TAB only): srec_tile is the shared-memory copy of the
+// records of the tile starting at slice_off[tile_slice0].
+template <typename R, int FMT, int LOAD, bool STAGED = false>
 __device__ __forceinline__ void exchange_field(const LLGArgs<R>& a, int i, int mi, const R* __restrict__ sx,
                                                const R* __restrict__ sy, const R* __restrict__ sz, R& hx, R& hy,
-                                               R& hz) {
+                                               R& hz, const int4* srec_tile = nullptr, int tile_off = 0) {
    if (sizeof(R) == 4 && (FMT == FMT_DMI_TAB || FMT == FMT_ISO_TAB) && (FMT == FMT_ISO_TAB || a.rec)) {
       const int sl = i >> 5;
       const int off = __ldg(a.slice_off + sl);
       const int w = (__ldg(a.slice_off + sl + 1) - off) >> 5;
       const int base = off + (i & 31);
-      if (w == 12) { exchange_gather_w<R, FMT, 12, LOAD>(a, base, mi, sx, sy, sz, hx, hy, hz); return; }
-      if (w == 6) { exchange_gather_w<R, FMT, 6, LOAD>(a, base, mi, sx, sy, sz, hx, hy, hz); return; }
+      const int4* sr = STAGED ? srec_tile + (base - tile_off) : nullptr;
+      if (w == 12) { exchange_gather_w<R, FMT, 12, LOAD, STAGED>(a, base, mi, sx, sy, sz, hx, hy, hz, sr); return; }
+      if (w == 6) { exchange_gather_w<R, FMT, 6, LOAD, STAGED>(a, base, mi, sx, sy, sz, hx, hy, hz, sr); return; }
    }
    exchange_gather<R, FMT, LOAD>(a, i, mi, sx, sy, sz, hx, hy, hz);
 }
 
 // spin-dependent field of atom i at spin S: exchange + anisotropy
 // (calculate_spin_fields, src/simulate/fields.cpp:67-118)
-template <typename R, int FMT, int LOAD = 0>
+template <typename R, int FMT, int LOAD = 0, bool STAGED = false>
 __device__ __forceinline__ void spin_field(const LLGArgs<R>& a, int i, int mi, const MatParams<R>& m,
-                                           const R* sx, const R* sy, const R* sz, const R S[3], R H[3]) {
+                                           const R* sx, const R* sy, const R* sz, const R S[3], R H[3],
+                                           const int4* srec_tile = nullptr, int tile_off = 0) {
    R hx = 0, hy = 0, hz = 0;
-   exchange_field<R, FMT, LOAD>(a, i, mi, sx, sy, sz, hx, hy, hz);
+   exchange_field<R, FMT, LOAD, STAGED>(a, i, mi, sx, sy, sz, hx, hy, hz, srec_tile, tile_off);
    if (a.uniaxial) {
       const R sdote = S[0] * m.kux + S[1] * m.kuy + S[2] * m.kuz;
       const R k2 = (R)2 * m.ku2 * sdote;

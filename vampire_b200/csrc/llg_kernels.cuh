@@ -25,6 +25,48 @@
 
 namespace vgpu {
 
+// Predictor tail of atom i, given s0 and its total field H:
+// s' = n(s0 + dt f(s0, H)) (LLGHeun.cpp:195-222).
+template <typename R>
+__device__ __forceinline__ void llg_predict_finish(const LLGArgs<R>& a, int i, const MatParams<R>& m, const R S0[3],
+                                                   const R H[3]) {
+   R d[3];
+   llg_rhs<R>(m.A, m.B, S0, H, d);
+   if (a.ex) { a.ex[i] = d[0]; a.ey[i] = d[1]; a.ez[i] = d[2]; }
+   R Sn[3] = {S0[0] + d[0] * a.dt, S0[1] + d[1] * a.dt, S0[2] + d[2] * a.dt};
+   const R r = rsqrt_<R>(Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2]);
+   a.bx[i] = Sn[0] * r; a.by[i] = Sn[1] * r; a.bz[i] = Sn[2] * r;
+}
+
+// Corrector tail of atom i, given s0, s' and the total field H' of s':
+// s1 = n(s0 + dt/2 (f0 + f(s', H'))) (LLGHeun.cpp:238-279), written over s0.
+template <typename R>
+__device__ __forceinline__ void llg_correct_finish(const LLGArgs<R>& a, int i, const MatParams<R>& m, const R S0[3],
+                                                   const R S1[3], const R H[3]) {
+   R d[3];
+   llg_rhs<R>(m.A, m.B, S1, H, d);
+   R Sn[3];
+   if (a.ex) {
+      // stored predictor increment: s0 + dt/2 (f0 + f1) as LLGHeun.cpp:264-266
+      const R e0[3] = {a.ex[i], a.ey[i], a.ez[i]};
+#pragma unroll
+      for (int k = 0; k < 3; ++k) Sn[k] = S0[k] + a.half_dt * (e0[k] + d[k]);
+   } else {
+      // recover the predictor increment f(s0) dt from s0 and s'
+      const R s00 = S0[0] * S0[0] + S0[1] * S0[1] + S0[2] * S0[2];
+      const R c = s00 / (S1[0] * S0[0] + S1[1] * S0[1] + S1[2] * S0[2]);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+         const R e = S1[k] * c - S0[k];
+         Sn[k] = S0[k] + ((R)0.5 * e + a.half_dt * d[k]);
+      }
+   }
+   const R n2 = Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2];
+   const R r = rsqrt_<R>(n2);
+   if (!(n2 > (R)0.25 && n2 < (R)4)) atomicOr(a.status, 1);  // non-finite or runaway
+   a.ax[i] = Sn[0] * r; a.ay[i] = Sn[1] * r; a.az[i] = Sn[2] * r;
+}
+
 // Predictor of atom i: s' = n(s0 + dt f(s0, H)).  LOAD = 1 reads neighbour
 // spins through L2 (they may have been written earlier in the same launch).
 template <typename R, int FMT, int LOAD>
@@ -36,12 +78,7 @@ __device__ __forceinline__ void llg_predict_atom(const LLGArgs<R>& a, int i) {
    spin_field<R, FMT, LOAD>(a, i, mi, m, a.ax, a.ay, a.az, S0, H);
    external_field<R>(a, i, m, true, E);
    H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
-   R d[3];
-   llg_rhs<R>(m.A, m.B, S0, H, d);
-   if (a.ex) { a.ex[i] = d[0]; a.ey[i] = d[1]; a.ez[i] = d[2]; }
-   R Sn[3] = {S0[0] + d[0] * a.dt, S0[1] + d[1] * a.dt, S0[2] + d[2] * a.dt};
-   const R r = rsqrt_<R>(Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2]);
-   a.bx[i] = Sn[0] * r; a.by[i] = Sn[1] * r; a.bz[i] = Sn[2] * r;
+   llg_predict_finish<R>(a, i, m, S0, H);
 }
 
 // Corrector of atom i: s1 = n(s0 + dt/2 (f0 + f(s', H'))), written over s0.
@@ -55,78 +92,26 @@ __device__ __forceinline__ void llg_correct_atom(const LLGArgs<R>& a, int i) {
    spin_field<R, FMT, LOAD>(a, i, mi, m, a.bx, a.by, a.bz, S1, H);
    external_field<R>(a, i, m, true, E);
    H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
-   R d[3];
-   llg_rhs<R>(m.A, m.B, S1, H, d);
-   R Sn[3];
-   if (a.ex) {
-      const R e0[3] = {a.ex[i], a.ey[i], a.ez[i]};
-#pragma unroll
-      for (int k = 0; k < 3; ++k) Sn[k] = S0[k] + a.half_dt * (e0[k] + d[k]);
-   } else {
-      const R s00 = S0[0] * S0[0] + S0[1] * S0[1] + S0[2] * S0[2];
-      const R c = s00 / (S1[0] * S0[0] + S1[1] * S0[1] + S1[2] * S0[2]);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-         const R e = S1[k] * c - S0[k];
-         Sn[k] = S0[k] + ((R)0.5 * e + a.half_dt * d[k]);
-      }
-   }
-   const R n2 = Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2];
-   const R r = rsqrt_<R>(n2);
-   if (!(n2 > (R)0.25 && n2 < (R)4)) atomicOr(a.status, 1);
-   a.ax[i] = Sn[0] * r; a.ay[i] = Sn[1] * r; a.az[i] = Sn[2] * r;
+   llg_correct_finish<R>(a, i, m, S0, S1, H);
 }
 
 template <typename R, int FMT, int MODE>
 __global__ void __launch_bounds__(256) llg_pass_kernel(const LLGArgs<R> a) {
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    if (i >= a.n) return;
-   const int mi = a.mat ? __ldg(a.mat + i) : 0;
-   const MatParams<R> m = a.mp[mi];
-   const R S0[3] = {a.ax[i], a.ay[i], a.az[i]};
-   if (MODE == PASS_PREDICTOR || MODE == PASS_FIELD) {
+   if (MODE == PASS_PREDICTOR) {
+      llg_predict_atom<R, FMT, 0>(a, i);
+   } else if (MODE == PASS_CORRECTOR) {
+      llg_correct_atom<R, FMT, 0>(a, i);
+   } else {
+      // field of s0: exchange, anisotropy, applied and dipole terms (no thermal term)
+      const int mi = a.mat ? __ldg(a.mat + i) : 0;
+      const MatParams<R> m = a.mp[mi];
+      const R S0[3] = {a.ax[i], a.ay[i], a.az[i]};
       R H[3], E[3];
       spin_field<R, FMT>(a, i, mi, m, a.ax, a.ay, a.az, S0, H);
-      external_field<R>(a, i, m, MODE == PASS_PREDICTOR, E);
-      H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
-      if (MODE == PASS_FIELD) {
-         a.fx[i] = H[0]; a.fy[i] = H[1]; a.fz[i] = H[2];
-         return;
-      }
-      R d[3];
-      llg_rhs<R>(m.A, m.B, S0, H, d);
-      if (a.ex) { a.ex[i] = d[0]; a.ey[i] = d[1]; a.ez[i] = d[2]; }
-      R Sn[3] = {S0[0] + d[0] * a.dt, S0[1] + d[1] * a.dt, S0[2] + d[2] * a.dt};
-      const R r = rsqrt_<R>(Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2]);
-      a.bx[i] = Sn[0] * r; a.by[i] = Sn[1] * r; a.bz[i] = Sn[2] * r;
-   } else {
-      const R S1[3] = {a.bx[i], a.by[i], a.bz[i]};
-      R H[3], E[3];
-      spin_field<R, FMT>(a, i, mi, m, a.bx, a.by, a.bz, S1, H);
-      external_field<R>(a, i, m, true, E);
-      H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
-      R d[3];
-      llg_rhs<R>(m.A, m.B, S1, H, d);
-      R Sn[3];
-      if (a.ex) {
-         // stored predictor increment: s0 + dt/2 (f0 + f1) as LLGHeun.cpp:264-266
-         const R e0[3] = {a.ex[i], a.ey[i], a.ez[i]};
-#pragma unroll
-         for (int k = 0; k < 3; ++k) Sn[k] = S0[k] + a.half_dt * (e0[k] + d[k]);
-      } else {
-         // recover the predictor increment f(s0) dt from s0 and s'
-         const R s00 = S0[0] * S0[0] + S0[1] * S0[1] + S0[2] * S0[2];
-         const R c = s00 / (S1[0] * S0[0] + S1[1] * S0[1] + S1[2] * S0[2]);
-#pragma unroll
-         for (int k = 0; k < 3; ++k) {
-            const R e = S1[k] * c - S0[k];
-            Sn[k] = S0[k] + ((R)0.5 * e + a.half_dt * d[k]);
-         }
-      }
-      const R n2 = Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2];
-      const R r = rsqrt_<R>(n2);
-      if (!(n2 > (R)0.25 && n2 < (R)4)) atomicOr(a.status, 1);  // non-finite or runaway
-      a.ax[i] = Sn[0] * r; a.ay[i] = Sn[1] * r; a.az[i] = Sn[2] * r;
+      external_field<R>(a, i, m, false, E);
+      a.fx[i] = H[0] + E[0]; a.fy[i] = H[1] + E[1]; a.fz[i] = H[2] + E[2];
    }
 }
 

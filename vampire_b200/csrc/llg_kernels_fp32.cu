@@ -1,8 +1,64 @@
 // FP32 instantiation of the fused LLG-Heun passes (production precision;
-// FMA contraction on).
-#include "llg_kernels.cuh"
+// FMA contraction on), and the bulk-staged variant of the FMT_DMI_TAB passes.
+#include "llg_staged.cuh"
 
 namespace vgpu {
 template cudaError_t launch_llg_pass<float>(const LLGArgs<float>&, int, int, int, cudaStream_t);
 template cudaError_t launch_thermal_noise<float>(const LLGArgs<float>&, cudaStream_t);
+
+int stage_tile_bytes(const std::vector<int>& slice_off, int sl) { return staged_tile_bytes(slice_off, sl); }
+
+template <int MODE, int SL, int NBUF>
+static const void* staged_fn() {
+   return (const void*)llg_staged_kernel<MODE, SL, NBUF>;
+}
+
+static const void* staged_fn(int mode, int sl, int nbuf) {
+   const bool p = mode == PASS_PREDICTOR;
+#define VGPU_FN(S, B) \
+   if (sl == S && nbuf == B) return p ? staged_fn<PASS_PREDICTOR, S, B>() : staged_fn<PASS_CORRECTOR, S, B>();
+   VGPU_FN(2, 1) VGPU_FN(2, 2) VGPU_FN(4, 1) VGPU_FN(4, 2) VGPU_FN(8, 1) VGPU_FN(8, 2)
+#undef VGPU_FN
+   return nullptr;
+}
+
+cudaError_t prepare_llg_staged(StageCfg& c, int nslices, int device) {
+   c.grid = 0;
+   if (!(c.sl == 2 || c.sl == 4 || c.sl == 8) || !(c.nbuf == 1 || c.nbuf == 2)) return cudaErrorInvalidValue;
+   const int smem = c.nbuf * c.buf_bytes;
+   int sms = 0, optin = 0;
+   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+   if (e != cudaSuccess) return e;
+   if (smem > optin - 64) return cudaErrorInvalidValue;  // room for the static mbarriers
+   int per_sm = 1 << 30;
+   for (int mode = PASS_PREDICTOR; mode <= PASS_CORRECTOR; ++mode) {
+      const void* f = staged_fn(mode, c.sl, c.nbuf);
+      if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+      int nb = 0;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, 32 * c.sl, smem)) != cudaSuccess) return e;
+      per_sm = std::min(per_sm, nb);
+   }
+   if (per_sm < 1) return cudaErrorInvalidValue;
+   c.ntiles = (nslices + c.sl - 1) / c.sl;
+   c.grid = c.nbuf == 1 ? c.ntiles : std::min(c.ntiles, per_sm * sms);
+   return cudaSuccess;
+}
+
+cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, const StageCfg& c, cudaStream_t st) {
+   if (c.grid == 0) return cudaSuccess;
+   const int smem = c.nbuf * c.buf_bytes;
+   const dim3 g(c.grid), b(32 * c.sl);
+#define VGPU_STAGED(S, B)                                                                                      \
+   if (c.sl == S && c.nbuf == B) {                                                                             \
+      if (mode == PASS_PREDICTOR)                                                                              \
+         llg_staged_kernel<PASS_PREDICTOR, S, B><<<g, b, smem, st>>>(a, nslices, c.ntiles, c.buf_bytes);       \
+      else                                                                                                     \
+         llg_staged_kernel<PASS_CORRECTOR, S, B><<<g, b, smem, st>>>(a, nslices, c.ntiles, c.buf_bytes);       \
+      return cudaGetLastError();                                                                               \
+   }
+   VGPU_STAGED(2, 1) VGPU_STAGED(2, 2) VGPU_STAGED(4, 1) VGPU_STAGED(4, 2) VGPU_STAGED(8, 1) VGPU_STAGED(8, 2)
+#undef VGPU_STAGED
+   return cudaErrorInvalidValue;
+}
 }  // namespace vgpu

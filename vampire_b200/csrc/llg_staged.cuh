@@ -1,0 +1,158 @@
+// Fused LLG-Heun passes with bulk-staged bond records (FP32, FMT_DMI_TAB).
+//
+// The per-bond records {neighbour, d_x, d_y, d_z} are the bulk of the HBM
+// stream (12 x 16 B per atom per pass).  In the plain pass every thread loads
+// its own twelve; here a block walks tiles of 32 SL atoms and thread 0
+// issues ONE cp.async.bulk (1-D bulk copy, global -> this CTA's shared memory,
+// no multicast) for the whole contiguous record range of a tile, completing on
+// an mbarrier with the byte count given by expect_tx.  Threads then read their records from shared memory;
+// neighbour spins are gathered through L1/L2 as before.  While the copy is in
+// flight each thread loads its own state and material and evaluates its
+// external field (the Philox noise is most of the pass's arithmetic).  The
+// arithmetic is the plain pass's (spin_field, external_field and the
+// llg_*_finish tails of llg_kernels.cuh), so results are identical.
+//
+// Waits on the mbarriers are bounded: if a copy has not landed after ~2M polls
+// the block records status bit 2 (VGPU_ERR_TIMEOUT on the host), waits --
+// bounded again -- for its other copy in flight, and returns.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "llg_kernels.cuh"
+
+namespace vgpu {
+
+constexpr long long kStagePolls = 1ll << 21;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* m, uint32_t count) {
+   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(m)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* m, uint32_t bytes) {
+   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(m)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* m) {
+   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_addr(dst)),
+                "l"(src), "r"(bytes), "r"(smem_addr(m))
+                : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* m, uint32_t parity) {
+   uint32_t ok;
+   asm volatile(
+       "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+       : "=r"(ok)
+       : "r"(smem_addr(m)), "r"(parity)
+       : "memory");
+   return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* m, uint32_t parity) {
+   for (long long it = 0; it < kStagePolls; ++it)
+      if (mbar_try_wait(m, parity)) return true;
+   return false;
+}
+
+// SL slices (32 SL atoms) per tile, NBUF = 1 (one tile per block, the other
+// resident blocks hide the copy) or 2 (persistent, next tile's copy in flight
+// while this one is computed).  Dynamic shared memory: NBUF * buf_bytes.
+template <int MODE, int SL, int NBUF>
+__global__ void __launch_bounds__(32 * SL) llg_staged_kernel(const LLGArgs<float> a, int nslices, int ntiles,
+                                                             int buf_bytes) {
+   extern __shared__ __align__(128) unsigned char stage_smem[];
+   __shared__ __align__(8) uint64_t mbar[2];
+   const int tid = threadIdx.x;
+   if (tid == 0) {
+      mbar_init(&mbar[0], 1);
+      mbar_init(&mbar[1], 1);
+      fence_mbar_init();
+   }
+   __syncthreads();
+   // thread 0: expect the tile's record bytes and start its bulk copy
+   auto issue = [&](int t, int b) {
+      const int s0 = t * SL;
+      const int s1 = min(s0 + SL, nslices);
+      const int o0 = __ldg(a.slice_off + s0), o1 = __ldg(a.slice_off + s1);
+      const uint32_t bytes = (uint32_t)(o1 - o0) * 16u;
+      fence_proxy_async();
+      mbar_arrive_expect_tx(&mbar[b], bytes);
+      if (bytes) bulk_copy_g2s(stage_smem + b * buf_bytes, a.rec + o0, bytes, &mbar[b]);
+   };
+   uint32_t phase = 0;  // bit b: parity of the phase of mbar[b] to wait for next
+   int t = blockIdx.x, k = 0, b = 0;
+   bool failed = false;
+   if (NBUF == 2 && t < ntiles && tid == 0) issue(t, 0);
+   for (; t < ntiles; t += gridDim.x, ++k) {
+      b = NBUF == 1 ? 0 : (k & 1);
+      if (tid == 0) {
+         if (NBUF == 1) issue(t, 0);
+         else if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, b ^ 1);
+      }
+      // own-atom work that needs no records overlaps the copy: state, material,
+      // external field (Philox noise, applied, dipole cell field)
+      const int i = t * 32 * SL + tid;
+      const bool act = i < a.n;
+      const int ii = act ? i : a.n - 1;  // idle lanes of the last tile load in bounds
+      const int mi = a.mat ? __ldg(a.mat + ii) : 0;
+      const MatParams<float> m = a.mp[mi];
+      float S0[3] = {a.ax[ii], a.ay[ii], a.az[ii]};
+      float S1[3];
+      if (MODE == PASS_CORRECTOR) { S1[0] = a.bx[ii]; S1[1] = a.by[ii]; S1[2] = a.bz[ii]; }
+      float E[3];
+      external_field<float>(a, ii, m, true, E);
+      const int tile_off = __ldg(a.slice_off + t * SL);
+      const bool done = mbar_wait_bounded(&mbar[b], (phase >> b) & 1u);
+      if (__syncthreads_or(!done)) {  // every thread takes the same branch
+         failed = true;
+         break;
+      }
+      phase ^= 1u << b;
+      const int4* sb = (const int4*)(stage_smem + b * buf_bytes);
+      if (act) {
+         float H[3];
+         if (MODE == PASS_PREDICTOR) {
+            spin_field<float, FMT_DMI_TAB, 0, true>(a, i, mi, m, a.ax, a.ay, a.az, S0, H, sb, tile_off);
+            H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
+            llg_predict_finish<float>(a, i, m, S0, H);
+         } else {
+            spin_field<float, FMT_DMI_TAB, 0, true>(a, i, mi, m, a.bx, a.by, a.bz, S1, H, sb, tile_off);
+            H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
+            llg_correct_finish<float>(a, i, m, S0, S1, H);
+         }
+      }
+      __syncthreads();  // buffer b fully read before it is refilled
+   }
+   if (failed) {
+      if (tid == 0) {
+         atomicOr(a.status, 2);
+         // copies still in flight: the one waited for and, double-buffered, the next tile's
+         mbar_wait_bounded(&mbar[b], (phase >> b) & 1u);
+         if (NBUF == 2 && t + (int)gridDim.x < ntiles) mbar_wait_bounded(&mbar[b ^ 1], (phase >> (b ^ 1)) & 1u);
+      }
+      __syncthreads();
+   }
+}
+
+// bytes of the largest tile's record range (buffer size) for the host
+inline int staged_tile_bytes(const std::vector<int>& slice_off, int sl) {
+   const int nsl = (int)slice_off.size() - 1;
+   int mx = 0;
+   for (int s0 = 0; s0 < nsl; s0 += sl) {
+      const int s1 = std::min(s0 + sl, nsl);
+      mx = std::max(mx, (slice_off[s1] - slice_off[s0]) * 16);
+   }
+   return mx;
+}
+
+}  // namespace vgpu

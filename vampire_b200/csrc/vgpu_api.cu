@@ -231,6 +231,16 @@ static int upload_typed(vgpu_ctx* h, const vgpu_system_desc* d) {
       }
    }
    std::vector<R> tabR(table.begin(), table.end());
+   // scalar table when every diagonal entry is isotropic (Jxx == Jyy == Jzz)
+   bool scalar = (fmt == FMT_VEC_TAB || fmt == FMT_DMI_TAB);
+   std::vector<R> tabS;
+   if (scalar) {
+      tabS.resize((size_t)M * M);
+      for (size_t q = 0; q < tabS.size(); ++q) {
+         if (table[3 * q] != table[3 * q + 1] || table[3 * q] != table[3 * q + 2]) scalar = false;
+         tabS[q] = (R)table[3 * q];
+      }
+   }
    std::vector<int> mat(d->type, d->type + n);
    std::vector<R> ax(n_alloc, (R)0), ay(n_alloc, (R)0), az(n_alloc, (R)0);
    for (int i = 0; i < n; ++i) { ax[i] = (R)d->sx[i]; ay[i] = (R)d->sy[i]; az[i] = (R)d->sz[i]; }
@@ -265,8 +275,13 @@ static int upload_typed(vgpu_ctx* h, const vgpu_system_desc* d) {
          std::memcpy(&rec[4 * e + 3], &jb[2][e], 4);
       }
       if ((rc = upload_vec(h, &S.rec, rec, "bond records"))) return rc;
+      S.stage_bytes[0] = stage_tile_bytes(off, 2);
+      S.stage_bytes[1] = stage_tile_bytes(off, 4);
+      S.stage_bytes[2] = stage_tile_bytes(off, 8);
    }
    if ((rc = upload_vec(h, &S.jtab, tabR, "coupling table"))) return rc;
+   S.tab_scalar = scalar;
+   if (scalar) { if ((rc = upload_vec(h, &S.jtab_s, tabS, "scalar coupling table"))) return rc; }
    if (M > 1) { if ((rc = upload_vec(h, &S.mat, mat, "materials"))) return rc; }
    if ((rc = upload_vec(h, &S.s[0], ax, "spins"))) return rc;
    if ((rc = upload_vec(h, &S.s[1], ay, "spins"))) return rc;
@@ -331,6 +346,8 @@ LLGArgs<R> make_args(vgpu_ctx* h) {
    a.mat_shift = S.mat_shift;
    for (int q = 0; q < 9; ++q) a.jb[q] = (const R*)S.jb[q];
    a.rec = (const int4*)S.rec;
+   a.tab_scalar = S.tab_scalar;
+   a.jtab_s = (const R*)S.jtab_s;
    a.jtab = (const R*)S.jtab;
    a.M = S.M;
    a.mat = (const int*)S.mat;
@@ -391,17 +408,48 @@ static int ensure_increment(vgpu_ctx* h) {
    return VGPU_OK;
 }
 
+static int stage_slot(int sl) { return sl == 2 ? 0 : sl == 4 ? 1 : 2; }
+
+// bulk-staged passes: FP32 packed records whose tiles fit shared memory.
+// Default (-1): on when the two buffers of a tile fit.
+template <typename R>
+static bool use_staged(vgpu_ctx* h) {
+   const SysDev& S = h->sys;
+   if (sizeof(R) != 4 || !S.rec || S.n == 0 || h->staged == 0) return false;
+   const int bytes = S.stage_bytes[stage_slot(h->stage_sl)];
+   return h->stage_nbuf * bytes <= kStageSmemLimit;
+}
+
+template <typename R>
+static cudaError_t launch_step_pass(vgpu_ctx* h, const LLGArgs<R>& a, int mode, bool staged) {
+   if constexpr (sizeof(R) == 4) {
+      if (staged) return launch_llg_staged(a, mode, h->sys.nslices, h->sys.stage, h->stream);
+   }
+   return launch_llg_pass<R>(a, h->sys.fmt, mode, h->sys.nslices, h->stream);
+}
+
 template <typename R>
 static int llg_steps_typed(vgpu_ctx* h, uint64_t n_steps) {
    int rc0 = ensure_increment<R>(h);
    if (rc0) return rc0;
+   const bool staged = use_staged<R>(h);
+   if (staged && h->sys.stage.grid == 0) {
+      StageCfg c;
+      c.sl = h->stage_sl;
+      c.nbuf = h->stage_nbuf;
+      c.buf_bytes = h->sys.stage_bytes[stage_slot(c.sl)];
+      cudaError_t e = prepare_llg_staged(c, h->sys.nslices, h->device);
+      if (e != cudaSuccess) return cuda_err(h, e, "staged pass setup (tile records exceed shared memory?)");
+      h->sys.stage = c;
+   }
    for (uint64_t t = 0; t < n_steps; ++t) {
       LLGArgs<R> a = make_args<R>(h);
+      cudaError_t e;
       h->prof_begin(PROF_PREDICTOR);
-      cudaError_t e = launch_llg_pass<R>(a, h->sys.fmt, PASS_PREDICTOR, h->sys.nslices, h->stream);
+      e = launch_step_pass<R>(h, a, PASS_PREDICTOR, staged);
       h->prof_end(PROF_PREDICTOR);
       h->prof_begin(PROF_CORRECTOR);
-      if (e == cudaSuccess) e = launch_llg_pass<R>(a, h->sys.fmt, PASS_CORRECTOR, h->sys.nslices, h->stream);
+      if (e == cudaSuccess) e = launch_step_pass<R>(h, a, PASS_CORRECTOR, staged);
       h->prof_end(PROF_CORRECTOR);
       if (e != cudaSuccess) return cuda_err(h, e, "llg_heun launch");
       h->kernel_launches += 2;
@@ -422,6 +470,7 @@ int vgpu_ctx::check_status() {
    rc = cuda_err(this, cudaStreamSynchronize(stream), "synchronize");
    if (rc) return rc;
    if (st & 1) return set_err(this, VGPU_ERR_NAN, "non-finite or non-normalisable spin produced by the integrator");
+   if (st & 2) return set_err(this, VGPU_ERR_TIMEOUT, "a bond-record copy into shared memory did not complete in time");
    return VGPU_OK;
 }
 namespace vgpu {
@@ -609,6 +658,21 @@ extern "C" int vgpu_set_option(vgpu_handle h, int option, int value) {
    if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
    switch (option) {
       case VGPU_OPT_STORE_INCREMENT: h->store_increment = value; return VGPU_OK;
+      case VGPU_OPT_STAGED_RECORDS:
+         if (value < -1 || value > 1) return set_err(h, VGPU_ERR_ARG, "staged records: -1, 0 or 1");
+         h->staged = value;
+         h->sys.stage.grid = 0;
+         return VGPU_OK;
+      case VGPU_OPT_STAGE_SLICES:
+         if (value != 2 && value != 4 && value != 8) return set_err(h, VGPU_ERR_ARG, "stage slices: 2, 4 or 8");
+         h->stage_sl = value;
+         h->sys.stage.grid = 0;
+         return VGPU_OK;
+      case VGPU_OPT_STAGE_BUFFERS:
+         if (value != 1 && value != 2) return set_err(h, VGPU_ERR_ARG, "stage buffers: 1 or 2");
+         h->stage_nbuf = value;
+         h->sys.stage.grid = 0;
+         return VGPU_OK;
       default: return set_err(h, VGPU_ERR_ARG, "unknown option %d", option);
    }
 }

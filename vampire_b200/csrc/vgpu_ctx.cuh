@@ -23,6 +23,8 @@ struct SysDev {
    void* col = nullptr;
    void* jb[9] = {nullptr};
    void* rec = nullptr;      // packed 16-byte bond records (FP32 FMT_DMI_TAB)
+   void* jtab_s = nullptr;   // scalar material-pair table (isotropic diagonal)
+   int tab_scalar = 0;
    void* jtab = nullptr;
    void* mat = nullptr;
    void* mp = nullptr;
@@ -45,6 +47,8 @@ struct SysDev {
    const int* sys_off = nullptr;  // batched systems: first atom of each system
    int m_per_sys = 1;
    uint64_t ramp_n = 0;      // batched field sweep length (steps)
+   int stage_bytes[3] = {0, 0, 0};  // largest tile's records, tiles of 2 / 4 / 8 slices
+   StageCfg stage;                          // prepared bulk-staged launch (grid 0: not prepared)
    std::vector<int> type_host;
    std::vector<int64_t> row_host;  // CSR kept on the host (colouring, sharding)
    std::vector<int> nl_host;
@@ -80,6 +84,8 @@ struct vgpu_ctx {
    bool any_sigma = false;
    int store_increment = -1;  // -1: default (on for FP64, off for FP32)
    bool batch_materials = false;  // batch handle: material rows are per system (no 100 limit)
+   int staged = -1;          // VGPU_OPT_STAGED_RECORDS (-1 default)
+   int stage_sl = 4, stage_nbuf = 1;
 
    void* alloc(size_t bytes);
    void free_system();

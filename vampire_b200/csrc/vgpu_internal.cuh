@@ -46,6 +46,8 @@ struct LLGArgs {
    const int* col;           // packed neighbour index (| mat << mat_shift)
    int idx_mask;             // mask of the neighbour index bits
    int mat_shift;            // shift of the neighbour material bits (0: unpacked)
+   int tab_scalar;           // diagonal table entries isotropic: use jtab_s (M*M)
+   const R* jtab_s;          // scalar material-pair table, or nullptr
    const R* jb[9];           // per-bond exchange arrays in SELL layout
    const int4* rec;          // FP32 FMT_DMI_TAB: packed {index, d_x, d_y, d_z} per bond, or nullptr
    const R* jtab;            // material-pair table (M*M or M*M*3)
@@ -82,6 +84,17 @@ enum PassMode : int { PASS_PREDICTOR = 0, PASS_CORRECTOR = 1, PASS_FIELD = 2 };
 // launch the fused Heun pass for the given format/mode (llg_kernels.cu)
 template <typename R>
 cudaError_t launch_llg_pass(const LLGArgs<R>& a, int fmt, int mode, int nslices, cudaStream_t st);
+
+// Bulk-staged FP32 FMT_DMI_TAB passes (llg_kernels_fp32.cu): tiles of sl
+// slices, nbuf shared-memory buffers of buf_bytes (the largest tile's records).
+constexpr int kStageSmemLimit = 200 * 1024;  // dynamic shared memory the staged passes may take
+struct StageCfg {
+   int sl = 4, nbuf = 1, buf_bytes = 0;
+   int ntiles = 0, grid = 0;  // set by prepare_llg_staged
+};
+int stage_tile_bytes(const std::vector<int>& slice_off, int sl);
+cudaError_t prepare_llg_staged(StageCfg& c, int nslices, int device);
+cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, const StageCfg& c, cudaStream_t st);
 
 // write the Philox thermal Gaussians of step a.step into a.fx/fy/fz
 template <typename R>

@@ -223,6 +223,28 @@ void llg_heun() {
 
 void stats_update() { stats::update(); }
 
+// Metropolis sweep on the GPU: N angle-move trials, one per atom, in colour
+// order (the reference's montecarlo::mc_step, src/montecarlo/mc.cpp:29-127,
+// makes N random-site trials on the host).  hdr/cuda.hpp has no such entry;
+// a host that adds gpu::mc_step() forwards it here.  Angle moves only: other
+// montecarlo::algorithm values stay on the host.
+void mc_step();
+void mc_step() {
+   static bool setup = false;
+   if (!setup) {
+      int32_t nc = 0;
+      fail(vgpu_mc_setup(g_h, nullptr, &nc), "mc setup");
+      fail(vgpu_mc_set_sweep(g_h, sim::time), "mc sweep counter");
+      setup = true;
+   }
+   sync_params();
+   fail(vgpu_mc_sweep(g_h, 1), "mc sweep");
+   double moves = 0.0, rejects = 0.0;
+   fail(vgpu_mc_counters(g_h, &moves, &rejects), "mc counters");
+   sim::mc_statistics_moves = moves;
+   sim::mc_statistics_reject = rejects;
+}
+
 void finalize() {
    if (!g_h) return;
    spins_to_host();

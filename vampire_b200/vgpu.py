@@ -22,6 +22,7 @@ LIB_PATH = PKG / "libvgpu.so"
 OK, ERR_ARG, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_NAN, ERR_STATE = 0, -1, -2, -3, -4, -5, -6
 PREC_FP32, PREC_FP64 = 0, 1
 NOISE_PHILOX, NOISE_REPLAY = 0, 1
+OPT_STORE_INCREMENT, OPT_STAGED_RECORDS, OPT_STAGE_SLICES, OPT_STAGE_BUFFERS = 1, 2, 3, 4
 
 _D = C.POINTER(C.c_double)
 _I32 = C.POINTER(C.c_int32)
@@ -195,6 +196,10 @@ class Simulation:
     def upload(self, s: SpinSystem) -> None:
         d, keep = _desc(s)
         self._check(lib().vgpu_upload_system(self._h, C.byref(d)))
+
+    def set_option(self, option: int, value: int) -> None:
+        """vgpu_set_option: OPT_STORE_INCREMENT, OPT_STAGED_RECORDS, OPT_STAGE_SLICES, OPT_STAGE_BUFFERS."""
+        self._check(lib().vgpu_set_option(self._h, int(option), int(value)))
 
     def set_params(self, p) -> None:
         c = params_struct(p)
