@@ -181,6 +181,16 @@ int vgpu_set_noise_replay(vgpu_handle h, const double* xi);
 #define VGPU_OPT_STAGED_RECORDS 2
 #define VGPU_OPT_STAGE_SLICES 3
 #define VGPU_OPT_STAGE_BUFFERS 4
+/* VGPU_OPT_DIPOLE_FFT (read by vgpu_dipole_setup): 1 or -1 (default) = the
+ * far-field cell sum by FP64 FFT convolution when every occupied cell centre
+ * lies on one regular grid (falls back to the direct sum otherwise), 0 =
+ * always the direct all-pairs sum. */
+#define VGPU_OPT_DIPOLE_FFT 5
+/* VGPU_OPT_STAGE_WAIT_TEST: 1 = staged passes wait for 16 bytes more than each
+ * tile's copy delivers, so their bounded wait (1 s) runs out and the step
+ * fails with VGPU_ERR_TIMEOUT (test of the timeout path; the handle stays
+ * usable after setting it back to 0). */
+#define VGPU_OPT_STAGE_WAIT_TEST 6
 int vgpu_set_option(vgpu_handle h, int option, int value);
 
 /* Step counter that keys the Philox stream (counter = (atom, step)).  Resume
@@ -241,6 +251,14 @@ int vgpu_dipole_update(vgpu_handle h);
  * [3*num_cells, Tesla] of the last update (cells::mag_array_*,
  * dipole::cells_field_array_*, dipole::cells_mu0Hd_field_array_*); any
  * output may be NULL. */
+/* Far-field method chosen by vgpu_dipole_setup: VGPU_DIPOLE_FAR_DIRECT (tiled
+ * all-pairs sum, FP32 terms) or VGPU_DIPOLE_FAR_FFT (FP64 FFT convolution on
+ * the cell grid).  No reference counterpart: the reference stores dense
+ * Nc x Nc tensors (src/dipole/memory.cpp:29-56). */
+#define VGPU_DIPOLE_FAR_DIRECT 0
+#define VGPU_DIPOLE_FAR_FFT 1
+int vgpu_dipole_method(vgpu_handle h, int32_t* method);
+
 int vgpu_dipole_get_cells(vgpu_handle h, double* mag, double* b_field, double* hd_field);
 
 /* Host-computed per-atom dipole B field (and mu0 Hd field for energies; NULL

@@ -54,18 +54,58 @@ def test_oracle_llg_with_dipole_field_matches_reference():
 @pytest.mark.gpu
 @pytest.mark.parametrize("solver", ["tensor", "macrocell"])
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
-def test_device_cell_fields(vgpu_lib, solver, prec):
+@pytest.mark.parametrize("far", ["fft", "direct"])
+def test_device_cell_fields(vgpu_lib, solver, prec, far):
+    """Cell moments and fields against the reference's own cells.  The far
+    field by FP64 FFT convolution (the golden cells sit on a regular grid)
+    matches the reference's dense FP64 sum to 1e-12 in the FP64 build; the
+    direct all-pairs sum of FP32 terms to 1e-5.  FP32 builds start from FP32
+    spins (moments to 1e-6)."""
     from vampire_b200 import vgpu
     s, d = load_golden(f"fcc10_dipole_{solver}")
     with vgpu.Simulation(s, precision=prec) as sim:
+        sim.set_option(vgpu.OPT_DIPOLE_FFT, 1 if far == "fft" else 0)
         sim.dipole_setup(_cells(d, s, solver))
+        assert sim.dipole_method() == (vgpu.DIPOLE_FAR_FFT if far == "fft" else vgpu.DIPOLE_FAR_DIRECT)
         m, b, h = sim.dipole_cells()
     m0, b0, h0 = _ref_cells(d, 0)
     mtol = 1e-12 if prec == "fp64" else 1e-6
     assert np.abs(m - m0).max() < mtol * np.abs(m0).max()
-    # far field summed from FP32 terms: 1e-5 of the largest cell field
-    assert np.abs(b - b0).max() < 1e-5 * np.abs(b0).max()
-    assert np.abs(h - h0).max() < 1e-5 * np.abs(h0).max()
+    ftol = 1e-12 if (far == "fft" and prec == "fp64") else 1e-5
+    assert np.abs(b - b0).max() < ftol * np.abs(b0).max()
+    assert np.abs(h - h0).max() < ftol * np.abs(h0).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(7, 5, 3), (1, 6, 2), (12, 1, 1)])
+def test_fft_far_field_matches_direct_sum(vgpu_lib, shape):
+    """Ragged grids (odd extents, single layers, a line of cells), random
+    moments: the FFT far field equals the FP64 direct sum of the NumPy
+    restatement, and the device all-pairs kernel to its FP32 tolerance."""
+    from oracle import dipole_ref as D
+    from vampire_b200 import system as S
+    from vampire_b200 import vgpu
+    nx, ny, nz = shape
+    s = S.build("sc", nx * 2, ny * 2, nz * 2, 3.0, [S.Material(alpha=0.1, mu_s_muB=1.72)],
+                np.array([[5e-21]]), S.SimParams(dt_SI=1e-16, temperature=0.0), spin_seed=5,
+                periodic=(False, False, False))
+    S.dipole_cells(s, size=6.0, atomic_volume=27.0, solver="macrocell", update_rate=0)
+    out = {}
+    for far in ("fft", "direct"):
+        with vgpu.Simulation(s, precision="fp64") as sim:
+            sim.set_option(vgpu.OPT_DIPOLE_FFT, 1 if far == "fft" else 0)
+            sim.dipole_setup(s.cells)
+            out[far] = sim.dipole_cells()
+    c = s.cells
+    nc = c["cell_natoms"].size
+    mag = D.cell_moments(s.spins, s.materials["mu_s_SI"][s.type], c["atom_cell"], nc)
+    T = D.tensors(c["cell_pos_mom"], c["cell_natoms"], c["macro_cell_size"], c["cutoff"], "macrocell", s.coords,
+                  c["atom_cell"])
+    B, H = D.cell_fields(mag, T, c["cell_natoms"], c["cell_volume"])
+    scale = np.abs(B).max()
+    assert np.abs(out["fft"][1] - B).max() < 1e-12 * scale
+    assert np.abs(out["direct"][1] - B).max() < 1e-5 * scale
+    assert np.abs(out["fft"][2] - H).max() < 1e-12 * np.abs(H).max()
 
 
 @pytest.mark.gpu

@@ -119,6 +119,30 @@ def test_staged_records_match_plain(V, L, sl, nbuf):
         np.testing.assert_array_equal(st.spins(), plain.spins())
 
 
+def test_staged_wait_timeout_reports_and_recovers(V):
+    """Failure path of the bounded waits: with the test option every tile's
+    barrier expects 16 bytes more than its bulk copy delivers, so the wait
+    gives up after its limit (1 s), the step reports VGPU_ERR_TIMEOUT, and
+    the handle keeps working once the option is off again."""
+    from vampire_b200 import system
+    s = system.config_fcc_tensor(L=2, seed=7)  # 32 spins: one slice, one tile
+    with V.Simulation(s) as sim, V.Simulation(s) as ref:
+        sim.set_option(V.OPT_STAGED_RECORDS, 1)
+        start = sim.spins()
+        sim.set_option(V.OPT_STAGE_WAIT_TEST, 1)
+        with pytest.raises(V.VGPUError) as e:
+            sim.llg_heun(1)
+            sim.synchronize()
+        assert e.value.code == V.ERR_TIMEOUT
+        sim.set_option(V.OPT_STAGE_WAIT_TEST, 0)
+        sim.set_spins(start)
+        sim.step = 0
+        sim.llg_heun(3)
+        ref.set_option(V.OPT_STAGED_RECORDS, 0)
+        ref.llg_heun(3)
+        np.testing.assert_array_equal(sim.spins(), ref.spins())
+
+
 def test_stage_option_checks(V):
     from vampire_b200 import system
     s = system.config_fcc_tensor(L=3, seed=7)

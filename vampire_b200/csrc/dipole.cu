@@ -25,9 +25,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <string>
 #include <unordered_map>
 #include <vector>
 
+#include "dipole_fft.cuh"
 #include "vgpu_ctx.cuh"
 
 namespace vgpu {
@@ -51,6 +53,7 @@ struct DipoleState {
    void* table_b = nullptr;     // [3][nc+1] R, cell B field for the LLG passes
    void* table_hd = nullptr;    // [3][nc+1] R, cell mu0 Hd field (energies)
    int* atom_cell = nullptr;    // [n] cell id or nc (zero row)
+   FFTField* fft = nullptr;     // far field by FFT convolution (regular cell grids), or direct sum
    std::vector<double> mus_host;
 };
 
@@ -199,7 +202,7 @@ __global__ void cell_finish_kernel(int nc, const int* __restrict__ near_start, c
 __global__ void near_tensor_kernel(int npairs, const int* __restrict__ pair_i, const int* __restrict__ pair_j,
                                    const int* __restrict__ cstart, const double* __restrict__ ax,
                                    const double* __restrict__ ay, const double* __restrict__ az,
-                                   const double* __restrict__ cpos, double* __restrict__ out) {
+                                   const double* __restrict__ cpos, int bare_fp64, double* __restrict__ out) {
    const int p = blockIdx.x;
    if (p >= npairs) return;
    const int ci = pair_i[p], cj = pair_j[p];
@@ -232,11 +235,18 @@ __global__ void near_tensor_kernel(int npairs, const int* __restrict__ pair_i, c
       const double norm = (double)ni * (double)nj;
       double bare[6] = {0, 0, 0, 0, 0, 0};
       if (ci != cj) {
-         // the far-field term K6 already added for this pair, taken out again
-         const float rx = (float)cpos[4 * cj] - (float)cpos[4 * ci];
-         const float ry = (float)cpos[4 * cj + 1] - (float)cpos[4 * ci + 1];
-         const float rz = (float)cpos[4 * cj + 2] - (float)cpos[4 * ci + 2];
-         const double r = sqrt((double)rx * rx + (double)ry * ry + (double)rz * rz);
+         // the far-field term already added for this pair, taken out again: from
+         // FP32 centres for the all-pairs kernel, FP64 for the FFT solver
+         double rx, ry, rz;
+         if (bare_fp64) {
+            rx = cpos[4 * cj] - cpos[4 * ci]; ry = cpos[4 * cj + 1] - cpos[4 * ci + 1];
+            rz = cpos[4 * cj + 2] - cpos[4 * ci + 2];
+         } else {
+            rx = (float)cpos[4 * cj] - (float)cpos[4 * ci];
+            ry = (float)cpos[4 * cj + 1] - (float)cpos[4 * ci + 1];
+            rz = (float)cpos[4 * cj + 2] - (float)cpos[4 * ci + 2];
+         }
+         const double r = sqrt(rx * rx + ry * ry + rz * rz);
          const double ri = 1.0 / r, ex = rx * ri, ey = ry * ri, ez = rz * ri, r3 = ri * ri * ri;
          bare[0] = (3.0 * ex * ex - 1.0) * r3; bare[1] = 3.0 * ex * ey * r3; bare[2] = 3.0 * ex * ez * r3;
          bare[3] = (3.0 * ey * ey - 1.0) * r3; bare[4] = 3.0 * ey * ez * r3; bare[5] = (3.0 * ez * ez - 1.0) * r3;
@@ -251,6 +261,7 @@ void dipole_destroy(vgpu_ctx* h) {
    cudaFree(d->cell_start); cudaFree(d->cell_atoms); cudaFree(d->mag); cudaFree(d->pos); cudaFree(d->mom);
    cudaFree(d->field); cudaFree(d->self); cudaFree(d->near_start); cudaFree(d->near_j); cudaFree(d->near_t);
    cudaFree(d->table_b); cudaFree(d->table_hd); cudaFree(d->atom_cell);
+   fft_field_destroy(d->fft);
    h->sys.cell = nullptr;
    h->sys.cell_field = nullptr;
    h->sys.cell_hd = nullptr;
@@ -268,7 +279,14 @@ static int dipole_update_typed(vgpu_ctx* h) {
    cell_moment_kernel<R><<<(nc * 32 + 255) / 256, 256, 0, h->stream>>>(
        nc, d->cell_start, d->cell_atoms, (const R*)S.s[0], (const R*)S.s[1], (const R*)S.s[2], (const int*)S.mat,
        (const MatParams<R>*)S.mp, S.mus_SI, d->mag, d->pos, d->mom);
-   {
+   int launches = 2;  // moments and finish, plus the far field below
+   if (d->fft) {
+      cudaError_t e = fft_field_apply(d->fft, d->mag, d->field, h->stream, &launches);
+      if (e != cudaSuccess) {
+         h->prof_end(PROF_DIPOLE);
+         return cuda_err(h, e, "dipole FFT far field");
+      }
+   } else {
       // enough blocks for every SM: split the sources when the targets alone are too few
       const int tblocks = (nc + kFieldTile * kTargetsPerThread - 1) / (kFieldTile * kTargetsPerThread);
       int sms = 148;
@@ -276,12 +294,13 @@ static int dipole_update_typed(vgpu_ctx* h) {
       const int splits = std::max(1, std::min(64, (6 * sms + tblocks - 1) / tblocks));
       cudaMemsetAsync(d->field, 0, sizeof(double) * 3 * nc, h->stream);
       cell_field_kernel<<<dim3(tblocks, splits), kFieldTile, 0, h->stream>>>(nc, d->pos, d->mom, d->field);
+      launches += 1;
    }
    cell_finish_kernel<R><<<(nc + 1 + 255) / 256, 256, 0, h->stream>>>(
        nc, d->near_start, d->near_j, d->near_t, d->npairs, d->mag, d->self, d->pos, d->field, (R*)d->table_b,
        (R*)d->table_hd);
    h->prof_end(PROF_DIPOLE);
-   h->kernel_launches += 3;
+   h->kernel_launches += launches;
    return cuda_err(h, cudaGetLastError(), "dipole update");
 }
 
@@ -355,6 +374,17 @@ extern "C" int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* dd) {
                                  (float)dd->cell_pos_mom[4 * c + 2], 1.f)
                    : make_float4(1e9f, 1e9f, 1e9f, 0.f);
       self[c] = dd->cell_natoms[c] > 0 ? 8.0 * M_PI / (3.0 * dd->cell_volume[c]) : 0.0;
+   }
+   // far field by FFT when the occupied cells form a regular grid
+   if (h->dipole_fft != 0) {
+      cudaError_t fe = cudaSuccess;
+      std::string why;
+      d->fft = fft_field_create(nc, dd->cell_pos_mom, dd->cell_natoms, dd->macro_cell_size, h->stream, &fe, &why);
+      if (fe != cudaSuccess) {
+         int rc = cuda_err(h, fe, "dipole FFT setup");
+         dipole_destroy(h);
+         return rc;
+      }
    }
    // near pairs (tensor solver), classified in FP64 exactly as inter.cpp:66,83
    std::vector<int> pi, pj, nstart(nc + 1, 0);
@@ -438,7 +468,7 @@ extern "C" int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* dd) {
       if (e == cudaSuccess) e = cudaMalloc(&d->near_t, sizeof(double) * 6 * d->npairs);
       if (e == cudaSuccess) {
          near_tensor_kernel<<<d->npairs, 256, 0, h->stream>>>(d->npairs, dpi, dpj, d->cell_start, ax, ay, az, cp,
-                                                               d->near_t);
+                                                               d->fft != nullptr, d->near_t);
          e = cudaGetLastError();
       }
       if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -463,6 +493,14 @@ extern "C" int vgpu_dipole_update(vgpu_handle h) {
    if (!dip_of(h)) return set_err(h, VGPU_ERR_STATE, "vgpu_dipole_setup not called");
    cudaSetDevice(h->device);
    return dipole_update(h);
+}
+
+extern "C" int vgpu_dipole_method(vgpu_handle h, int32_t* method) {
+   if (!h || !method) return set_err(h, VGPU_ERR_ARG, "null argument");
+   DipoleState* d = dip_of(h);
+   if (!d) return set_err(h, VGPU_ERR_STATE, "vgpu_dipole_setup not called");
+   *method = d->fft ? VGPU_DIPOLE_FAR_FFT : VGPU_DIPOLE_FAR_DIRECT;
+   return VGPU_OK;
 }
 
 extern "C" int vgpu_dipole_get_cells(vgpu_handle h, double* mag, double* b_field, double* hd_field) {

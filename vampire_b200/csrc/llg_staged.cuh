@@ -12,9 +12,12 @@
 // arithmetic is the plain pass's (spin_field, external_field and the
 // llg_*_finish tails of llg_kernels.cuh), so results are identical.
 //
-// Waits on the mbarriers are bounded: if a copy has not landed after ~2M polls
-// the block records status bit 2 (VGPU_ERR_TIMEOUT on the host), waits --
-// bounded again -- for its other copy in flight, and returns.
+// Waits on the mbarriers are bounded (1 s of wall time, and a poll count): if
+// a copy has not landed by then the block records status bit 2
+// (VGPU_ERR_TIMEOUT on the host), waits -- bounded again -- for its copies
+// still in flight, and returns.  a.stage_extra_tx > 0 makes every tile expect
+// that many bytes more than its copy delivers, so the wait runs out: the test
+// of this path.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -25,7 +28,8 @@
 
 namespace vgpu {
 
-constexpr long long kStagePolls = 1ll << 21;
+constexpr long long kStagePolls = 1ll << 26;
+constexpr uint64_t kStageWaitNs = 1000000000ull;  // 1 s
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -58,9 +62,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* m, uint32_t parity) {
    return ok != 0;
 }
 
+__device__ __forceinline__ uint64_t global_ns() {
+   uint64_t t;
+   asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+   return t;
+}
+
+// wait for phase `parity` of m: at most kStageWaitNs of wall time (checked every
+// 256 polls) and at most kStagePolls polls
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* m, uint32_t parity) {
-   for (long long it = 0; it < kStagePolls; ++it)
+   const uint64_t t0 = global_ns();
+   for (long long it = 0; it < kStagePolls; ++it) {
       if (mbar_try_wait(m, parity)) return true;
+      if ((it & 255) == 255 && global_ns() - t0 > kStageWaitNs) return false;
+   }
    return false;
 }
 
@@ -86,7 +101,7 @@ __global__ void __launch_bounds__(32 * SL) llg_staged_kernel(const LLGArgs<float
       const int o0 = __ldg(a.slice_off + s0), o1 = __ldg(a.slice_off + s1);
       const uint32_t bytes = (uint32_t)(o1 - o0) * 16u;
       fence_proxy_async();
-      mbar_arrive_expect_tx(&mbar[b], bytes);
+      mbar_arrive_expect_tx(&mbar[b], bytes + (uint32_t)a.stage_extra_tx);
       if (bytes) bulk_copy_g2s(stage_smem + b * buf_bytes, a.rec + o0, bytes, &mbar[b]);
    };
    uint32_t phase = 0;  // bit b: parity of the phase of mbar[b] to wait for next

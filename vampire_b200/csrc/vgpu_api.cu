@@ -322,8 +322,13 @@ int refresh_materials_typed(vgpu_ctx* h) {
       o.dhy = rp ? (R)rp[3 * m + 1] : (R)0;
       o.dhz = rp ? (R)rp[3 * m + 2] : (R)0;
    }
-   return cuda_err(h, cudaMemcpyAsync(S.mp, mp.data(), sizeof(MatParams<R>) * S.M, cudaMemcpyHostToDevice, h->stream),
-                   "material upload");
+   // unchanged table (the common case of a per-step parameter sync): no copy,
+   // so the call neither waits for the stream nor adds a transfer
+   const size_t bytes = sizeof(MatParams<R>) * S.M;
+   const unsigned char* raw = (const unsigned char*)mp.data();
+   if (S.mp_host.size() == bytes && std::equal(raw, raw + bytes, S.mp_host.begin())) return VGPU_OK;
+   S.mp_host.assign(raw, raw + bytes);
+   return cuda_err(h, cudaMemcpyAsync(S.mp, mp.data(), bytes, cudaMemcpyHostToDevice, h->stream), "material upload");
 }
 
 }  // namespace vgpu
@@ -379,6 +384,7 @@ LLGArgs<R> make_args(vgpu_ctx* h) {
    a.fx = (R*)S.f[0]; a.fy = (R*)S.f[1]; a.fz = (R*)S.f[2];
    a.ex = (R*)S.e[0]; a.ey = (R*)S.e[1]; a.ez = (R*)S.e[2];
    a.status = S.status;
+   a.stage_extra_tx = h->stage_wait_test ? 16 : 0;
    a.sys_off = S.sys_off;
    a.m_per_sys = S.m_per_sys;
    a.ramp_n = S.ramp_n;
@@ -468,6 +474,10 @@ int vgpu_ctx::check_status() {
    int rc = cuda_err(this, cudaMemcpyAsync(&st, sys.status, sizeof(int), cudaMemcpyDeviceToHost, stream), "status read");
    if (rc) return rc;
    rc = cuda_err(this, cudaStreamSynchronize(stream), "synchronize");
+   if (rc) return rc;
+   if (st == 0) return VGPU_OK;
+   // report once: clear the word so that the context stays usable
+   rc = cuda_err(this, cudaMemsetAsync(sys.status, 0, sizeof(int), stream), "status reset");
    if (rc) return rc;
    if (st & 1) return set_err(this, VGPU_ERR_NAN, "non-finite or non-normalisable spin produced by the integrator");
    if (st & 2) return set_err(this, VGPU_ERR_TIMEOUT, "a bond-record copy into shared memory did not complete in time");
@@ -573,20 +583,48 @@ extern "C" int vgpu_set_params(vgpu_handle h, const vgpu_sim_params* p) {
    return h->refresh_materials();
 }
 
+// host FP64 <-> device state: the caller's doubles are copied as they are
+// (a DMA straight from the caller's buffer when it is pinned) and converted on
+// the device, so no host-side conversion loop sits on the transfer path.
+__global__ void f64_to_state_kernel(const double* __restrict__ in, float* __restrict__ out, int n) {
+   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = (float)in[i];
+}
+__global__ void state_to_f64_kernel(const float* __restrict__ in, double* __restrict__ out, int n) {
+   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = (double)in[i];
+}
+
+static int convert_grid(int n) { return std::max(1, std::min((n + 255) / 256, 148 * 8)); }
+
+// device FP64 staging for host transfers of the FP32 state (3n doubles, once)
+static double* host_stage(vgpu_ctx* h) {
+   if (!h->sys.stage64) h->sys.stage64 = (double*)h->alloc(3 * (size_t)h->sys.n * sizeof(double));
+   return h->sys.stage64;
+}
+
 template <typename R>
 static int set_spins_typed(vgpu_handle h, const double* sx, const double* sy, const double* sz) {
    const int n = h->sys.n;
    const double* src[3] = {sx, sy, sz};
-   std::vector<R> buf(n);
-   for (int q = 0; q < 3; ++q) {
-      for (int i = 0; i < n; ++i) buf[i] = (R)src[q][i];
-      int rc = cuda_err(h, cudaMemcpyAsync(h->sys.s[q], buf.data(), n * sizeof(R), cudaMemcpyHostToDevice, h->stream),
-                        "set spins");
-      if (rc) return rc;
-      rc = cuda_err(h, cudaStreamSynchronize(h->stream), "set spins");
+   if (sizeof(R) == 8) {
+      for (int q = 0; q < 3; ++q) {
+         int rc = cuda_err(h, cudaMemcpyAsync(h->sys.s[q], src[q], n * sizeof(double), cudaMemcpyHostToDevice,
+                                              h->stream), "set spins");
+         if (rc) return rc;
+      }
+   } else {
+      double* st = host_stage(h);
+      if (!st) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for transfer staging");
+      for (int q = 0; q < 3; ++q) {
+         int rc = cuda_err(h, cudaMemcpyAsync(st + (size_t)q * n, src[q], n * sizeof(double), cudaMemcpyHostToDevice,
+                                              h->stream), "set spins");
+         if (rc) return rc;
+         f64_to_state_kernel<<<convert_grid(n), 256, 0, h->stream>>>(st + (size_t)q * n, (float*)h->sys.s[q], n);
+         h->kernel_launches++;
+      }
+      int rc = cuda_err(h, cudaGetLastError(), "set spins convert");
       if (rc) return rc;
    }
-   return VGPU_OK;
+   return cuda_err(h, cudaStreamSynchronize(h->stream), "set spins");
 }
 
 extern "C" int vgpu_set_spins(vgpu_handle h, const double* sx, const double* sy, const double* sz) {
@@ -599,16 +637,24 @@ extern "C" int vgpu_set_spins(vgpu_handle h, const double* sx, const double* sy,
 template <typename R>
 static int get_vec_typed(vgpu_handle h, void* const src[3], double* out[3]) {
    const int n = h->sys.n;
-   std::vector<R> buf(n);
-   for (int q = 0; q < 3; ++q) {
-      int rc = cuda_err(h, cudaMemcpyAsync(buf.data(), src[q], n * sizeof(R), cudaMemcpyDeviceToHost, h->stream),
-                        "download");
-      if (rc) return rc;
-      rc = cuda_err(h, cudaStreamSynchronize(h->stream), "download");
-      if (rc) return rc;
-      for (int i = 0; i < n; ++i) out[q][i] = (double)buf[i];
+   if (sizeof(R) == 8) {
+      for (int q = 0; q < 3; ++q) {
+         int rc = cuda_err(h, cudaMemcpyAsync(out[q], src[q], n * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+                           "download");
+         if (rc) return rc;
+      }
+   } else {
+      double* st = host_stage(h);
+      if (!st) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for transfer staging");
+      for (int q = 0; q < 3; ++q) {
+         state_to_f64_kernel<<<convert_grid(n), 256, 0, h->stream>>>((const float*)src[q], st + (size_t)q * n, n);
+         h->kernel_launches++;
+         int rc = cuda_err(h, cudaMemcpyAsync(out[q], st + (size_t)q * n, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                              h->stream), "download");
+         if (rc) return rc;
+      }
    }
-   return VGPU_OK;
+   return cuda_err(h, cudaStreamSynchronize(h->stream), "download");
 }
 
 extern "C" int vgpu_get_spins(vgpu_handle h, double* sx, double* sy, double* sz) {
@@ -667,6 +713,13 @@ extern "C" int vgpu_set_option(vgpu_handle h, int option, int value) {
          if (value != 2 && value != 4 && value != 8) return set_err(h, VGPU_ERR_ARG, "stage slices: 2, 4 or 8");
          h->stage_sl = value;
          h->sys.stage.grid = 0;
+         return VGPU_OK;
+      case VGPU_OPT_STAGE_WAIT_TEST:
+         h->stage_wait_test = value != 0;
+         return VGPU_OK;
+      case VGPU_OPT_DIPOLE_FFT:
+         if (value < -1 || value > 1) return set_err(h, VGPU_ERR_ARG, "dipole FFT: -1, 0 or 1");
+         h->dipole_fft = value;
          return VGPU_OK;
       case VGPU_OPT_STAGE_BUFFERS:
          if (value != 1 && value != 2) return set_err(h, VGPU_ERR_ARG, "stage buffers: 1 or 2");

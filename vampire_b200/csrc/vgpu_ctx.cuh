@@ -34,6 +34,7 @@ struct SysDev {
    void* e[3] = {nullptr};   // stored predictor increment in use (VGPU_OPT_STORE_INCREMENT)
    void* e_store[3] = {nullptr};  // its buffers, once allocated
    void* xi = nullptr;       // replay noise
+   double* stage64 = nullptr;  // [3n] FP64 staging of host transfers (FP32 state)
    int* status = nullptr;
    // macrocell dipole
    int ncells = 0;
@@ -53,6 +54,7 @@ struct SysDev {
    std::vector<int64_t> row_host;  // CSR kept on the host (colouring, sharding)
    std::vector<int> nl_host;
    std::vector<vgpu_material> materials;
+   std::vector<unsigned char> mp_host;  // last material table copied to mp
 };
 
 int set_err(vgpu_ctx* h, int code, const char* fmt, ...);
@@ -86,6 +88,8 @@ struct vgpu_ctx {
    bool batch_materials = false;  // batch handle: material rows are per system (no 100 limit)
    int staged = -1;          // VGPU_OPT_STAGED_RECORDS (-1 default)
    int stage_sl = 4, stage_nbuf = 1;
+   bool stage_wait_test = false;  // VGPU_OPT_STAGE_WAIT_TEST
+   int dipole_fft = -1;      // VGPU_OPT_DIPOLE_FFT (-1 default: FFT far field on regular cell grids)
 
    void* alloc(size_t bytes);
    void free_system();

@@ -77,6 +77,7 @@ struct LLGArgs {
    R* fx; R* fy; R* fz;      // field output (field-only mode)
    R* ex; R* ey; R* ez;      // stored predictor increment f(s0), or nullptr (recovered)
    int* status;              // device status word (non-finite spin flag)
+   int stage_extra_tx;       // staged passes: extra bytes each tile expects (0; > 0 tests the bounded wait)
 };
 
 enum PassMode : int { PASS_PREDICTOR = 0, PASS_CORRECTOR = 1, PASS_FIELD = 2 };

@@ -22,7 +22,9 @@ LIB_PATH = PKG / "libvgpu.so"
 OK, ERR_ARG, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_NAN, ERR_STATE = 0, -1, -2, -3, -4, -5, -6
 PREC_FP32, PREC_FP64 = 0, 1
 NOISE_PHILOX, NOISE_REPLAY = 0, 1
-OPT_STORE_INCREMENT, OPT_STAGED_RECORDS, OPT_STAGE_SLICES, OPT_STAGE_BUFFERS = 1, 2, 3, 4
+OPT_STORE_INCREMENT, OPT_STAGED_RECORDS, OPT_STAGE_SLICES, OPT_STAGE_BUFFERS, OPT_DIPOLE_FFT = 1, 2, 3, 4, 5
+OPT_STAGE_WAIT_TEST = 6
+DIPOLE_FAR_DIRECT, DIPOLE_FAR_FFT = 0, 1
 
 _D = C.POINTER(C.c_double)
 _I32 = C.POINTER(C.c_int32)
@@ -206,8 +208,12 @@ class Simulation:
         self._check(lib().vgpu_set_params(self._h, C.byref(c)))
 
     # -- spins -------------------------------------------------------------
-    def spins(self) -> np.ndarray:
-        out = np.empty((3, self.n))
+    def spins(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Current spins as (3, n) float64; `out` (e.g. a view of pinned host
+        memory) is filled in place when given."""
+        if out is None:
+            out = np.empty((3, self.n))
+        assert out.shape == (3, self.n) and out.dtype == np.float64 and out[0].flags.c_contiguous
         self._check(lib().vgpu_get_spins(self._h, _ptr(out[0], _D), _ptr(out[1], _D), _ptr(out[2], _D)))
         return out
 
@@ -278,6 +284,12 @@ class Simulation:
 
     def dipole_update(self) -> None:
         self._check(lib().vgpu_dipole_update(self._h))
+
+    def dipole_method(self) -> int:
+        """DIPOLE_FAR_DIRECT or DIPOLE_FAR_FFT (far-field method chosen at setup)."""
+        m = C.c_int32()
+        self._check(lib().vgpu_dipole_method(self._h, C.byref(m)))
+        return m.value
 
     def dipole_cells(self):
         """(moments J/T, B field T, mu0 Hd field T), each (3, ncells)."""
