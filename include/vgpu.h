@@ -203,6 +203,37 @@ int vgpu_get_step(vgpu_handle h, uint64_t* step);
  * vcuda::llg_heun (src/cuda/llg_heun.cu:32-42,121-208). */
 int vgpu_llg_heun(vgpu_handle h, uint64_t n_steps);
 
+/* ---- spatial shards (one process per GPU, halo exchange between passes) ---
+ * No reference counterpart in the gpu:: interface; they carry the reference's
+ * MPI decomposition (core/boundary/halo atoms, src/simulate/LLGHeun-mpi.cpp:
+ * 62-64, halo refresh src/mpi/mpi_comms.cpp:45-143) onto one GPU per rank. */
+
+/* One fused pass: VGPU_PASS_PREDICTOR (s' from s) or VGPU_PASS_CORRECTOR (s
+ * from s and s'; completes the step: counter and dipole cadence).
+ * vgpu_llg_heun(h, 1) is the predictor followed by the corrector. */
+#define VGPU_PASS_PREDICTOR 0
+#define VGPU_PASS_CORRECTOR 1
+int vgpu_llg_pass(vgpu_handle h, int pass);
+
+/* The uploaded system is a shard: atoms 0..n_owned-1 are owned and updated
+ * by the passes (and summed by the statistics); the rest are halo copies of
+ * other ranks' atoms that the host refreshes between passes.  noise_base is
+ * added to the atom index in the Philox counter: the global index of owned
+ * atom 0 when the owned atoms are one contiguous global range, so that the
+ * shard draws the noise of the whole system.  Not with Monte Carlo or the
+ * device dipole solver. */
+int vgpu_set_owned(vgpu_handle h, int32_t n_owned, int64_t noise_base);
+
+/* Halo transfers, queued on the handle's stream (vgpu_get_stream) with
+ * DEVICE buffers of the handle's precision: pack gathers state `which`
+ * (VGPU_STATE_SPIN = s, VGPU_STATE_PREDICTOR = s') at the count local indices
+ * idx[] into out[3*count] (x block, y, z); unpack writes in[3*count] into
+ * atoms first..first+count-1. */
+#define VGPU_STATE_SPIN 0
+#define VGPU_STATE_PREDICTOR 1
+int vgpu_halo_pack(vgpu_handle h, int which, const int32_t* idx, int32_t count, void* out);
+int vgpu_halo_unpack(vgpu_handle h, int which, int32_t first, int32_t count, const void* in);
+
 /* Write the 3*num_atoms Gaussians (x|y|z blocks) that the Philox stream
  * gives the thermal field at step `step` -- the values the fused kernels
  * regenerate in-register.  For tests and for replaying a run elsewhere. */
@@ -323,6 +354,13 @@ int vgpu_stats_get_energy(vgpu_handle h, int32_t id, double* e, double* mean, in
 
 /* Zero the running means and counters.  Replaces vcuda::stats::reset. */
 int vgpu_stats_reset(vgpu_handle h);
+
+/* Raw per-bin sums of the last vgpu_stats_update of mask `id`: sums[8*bin +
+ * {0..3}] = sum mu s_x, sum mu s_y, sum mu s_z, sum mu (mu_B), [4..7] = the
+ * exchange, anisotropy, applied and magnetostatic energy sums (exchange and
+ * magnetostatic before halving).  Shards add these over ranks and normalise
+ * as magnetization.cpp:134-180.  No reference counterpart. */
+int vgpu_stats_get_sums(vgpu_handle h, int32_t id, double* sums);
 
 /* ---- batched systems ------------------------------------------------------ */
 

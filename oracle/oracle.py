@@ -63,6 +63,7 @@ def lib():
         build_lib()
         _lib = C.CDLL(str(LIB_PATH))
         for name in ("vref_spin_fields", "vref_external_fields", "vref_llg_heun", "vref_magnetization",
+                     "vref_heun_predict", "vref_heun_correct",
                      "vref_energy", "vref_spin_energy"):
             getattr(_lib, name).restype = None
     return _lib
@@ -161,6 +162,25 @@ class OracleSystem:
         xi_c = np.ascontiguousarray(xi, dtype=np.float64) if xi is not None else None
         lib().vref_llg_heun(C.byref(self.st), _p(s[0], _D), _p(s[1], _D), _p(s[2], _D),
                             _p(xi_c, _D), C.c_int64(n_steps))
+        return s
+
+    def heun_predict(self, spins: np.ndarray, xi: Optional[np.ndarray] = None):
+        """Predictor half of one step (vref_heun_predict): returns (s', keep),
+        keep being the 12n state the corrector half needs."""
+        s = np.ascontiguousarray(spins, dtype=np.float64)
+        xi_c = np.ascontiguousarray(xi, dtype=np.float64) if xi is not None else None
+        p = np.zeros((3, self.s.n))
+        keep = np.zeros(12 * self.s.n)
+        lib().vref_heun_predict(C.byref(self.st), _p(s[0], _D), _p(s[1], _D), _p(s[2], _D), _p(xi_c, _D),
+                                _p(p[0], _D), _p(p[1], _D), _p(p[2], _D), _p(keep, _D))
+        return p, keep
+
+    def heun_correct(self, spins: np.ndarray, p: np.ndarray, keep: np.ndarray) -> np.ndarray:
+        """Corrector half (vref_heun_correct): s1 from s0 = spins, s' = p."""
+        s = np.ascontiguousarray(spins, dtype=np.float64).copy()
+        pc = np.ascontiguousarray(p, dtype=np.float64)
+        lib().vref_heun_correct(C.byref(self.st), _p(s[0], _D), _p(s[1], _D), _p(s[2], _D), _p(pc[0], _D),
+                                _p(pc[1], _D), _p(pc[2], _D), _p(keep, _D))
         return s
 
     def spin_fields(self, spins: np.ndarray) -> np.ndarray:

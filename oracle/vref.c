@@ -127,19 +127,16 @@ static inline void llg_rhs(double A, double B, const double S[3], const double H
    d[2] = A * (S[0] * H[1] - S[1] * H[0]) + B * (S[0] * (S[2] * H[0] - S[0] * H[2]) - S[1] * (S[1] * H[2] - S[2] * H[1]));
 }
 
-/* sim::LLG_Heun (src/simulate/LLGHeun.cpp:160-282): one stochastic Heun step.
- * xi: 3n Gaussians for this step (NULL = no thermal term).  work: 15n doubles. */
-void vref_llg_heun_step(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,
-                        double* work) {
+/* Predictor half of sim::LLG_Heun (src/simulate/LLGHeun.cpp:185-222): fields of
+ * s0 (spin + external, LLGHeun.cpp:185-186), f0 = rhs(s0, H) kept in keep[6n..9n)
+ * and the external field in keep[3n..6n) for the corrector, s' = n(s0 + f0 dt)
+ * into px, py, pz.  keep: 12n doubles, passed unchanged to vref_heun_correct. */
+void vref_heun_predict(const vref_sys* s, const double* sx, const double* sy, const double* sz, const double* xi,
+                       double* px, double* py, double* pz, double* keep) {
    const int n = s->n;
-   double* hsx = work;          double* hsy = work + n;      double* hsz = work + 2 * n;
-   double* hex = work + 3 * n;  double* hey = work + 4 * n;  double* hez = work + 5 * n;
-   double* ix = work + 6 * n;   double* iy = work + 7 * n;   double* iz = work + 8 * n;
-   double* ex = work + 9 * n;   double* ey = work + 10 * n;  double* ez = work + 11 * n;
-   double* hux = work + 12 * n; double* huy = work + 13 * n; double* huz = work + 14 * n;
-   memcpy(ix, sx, sizeof(double) * n);
-   memcpy(iy, sy, sizeof(double) * n);
-   memcpy(iz, sz, sizeof(double) * n);
+   double* hsx = keep;          double* hsy = keep + n;      double* hsz = keep + 2 * n;
+   double* hex = keep + 3 * n;  double* hey = keep + 4 * n;  double* hez = keep + 5 * n;
+   double* ex = keep + 6 * n;   double* ey = keep + 7 * n;   double* ez = keep + 8 * n;
    vref_spin_fields(s, sx, sy, sz, hsx, hsy, hsz);
    vref_external_fields(s, xi, hex, hey, hez);
    for (int atom = 0; atom < n; atom++) {
@@ -151,27 +148,46 @@ void vref_llg_heun_step(const vref_sys* s, double* sx, double* sy, double* sz, c
       ex[atom] = d[0]; ey[atom] = d[1]; ez[atom] = d[2];
       double Sn[3] = {S[0] + d[0] * s->dt, S[1] + d[1] * s->dt, S[2] + d[2] * s->dt};
       const double mod = 1.0 / sqrt(Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2]);
-      hux[atom] = Sn[0] * mod; huy[atom] = Sn[1] * mod; huz[atom] = Sn[2] * mod;
+      px[atom] = Sn[0] * mod; py[atom] = Sn[1] * mod; pz[atom] = Sn[2] * mod;
    }
-   memcpy(sx, hux, sizeof(double) * n);
-   memcpy(sy, huy, sizeof(double) * n);
-   memcpy(sz, huz, sizeof(double) * n);
-   vref_spin_fields(s, sx, sy, sz, hsx, hsy, hsz);
+}
+
+/* Corrector half (LLGHeun.cpp:224-279): spin fields of s' plus the predictor's
+ * external field (the same thermal field serves both halves, LLGHeun.cpp:185),
+ * f1 = rhs(s', H'), s1 = n(s0 + dt/2 (f0 + f1)) written over sx, sy, sz (s0). */
+void vref_heun_correct(const vref_sys* s, double* sx, double* sy, double* sz, const double* px, const double* py,
+                       const double* pz, double* keep) {
+   const int n = s->n;
+   double* hsx = keep;          double* hsy = keep + n;      double* hsz = keep + 2 * n;
+   double* hex = keep + 3 * n;  double* hey = keep + 4 * n;  double* hez = keep + 5 * n;
+   double* ex = keep + 6 * n;   double* ey = keep + 7 * n;   double* ez = keep + 8 * n;
+   double* hux = keep + 9 * n;  double* huy = keep + 10 * n; double* huz = keep + 11 * n;
+   vref_spin_fields(s, px, py, pz, hsx, hsy, hsz);
    for (int atom = 0; atom < n; atom++) {
       const int m = s->type[atom];
-      const double S[3] = {sx[atom], sy[atom], sz[atom]};
+      const double S[3] = {px[atom], py[atom], pz[atom]};
       const double H[3] = {hsx[atom] + hex[atom], hsy[atom] + hey[atom], hsz[atom] + hez[atom]};
       double d[3];
       llg_rhs(s->A[m], s->B[m], S, H, d);
       hux[atom] = d[0]; huy[atom] = d[1]; huz[atom] = d[2];
    }
    for (int atom = 0; atom < n; atom++) {
-      double Sn[3] = {ix[atom] + s->half_dt * (ex[atom] + hux[atom]),
-                      iy[atom] + s->half_dt * (ey[atom] + huy[atom]),
-                      iz[atom] + s->half_dt * (ez[atom] + huz[atom])};
+      double Sn[3] = {sx[atom] + s->half_dt * (ex[atom] + hux[atom]),
+                      sy[atom] + s->half_dt * (ey[atom] + huy[atom]),
+                      sz[atom] + s->half_dt * (ez[atom] + huz[atom])};
       const double mod = 1.0 / sqrt(Sn[0] * Sn[0] + Sn[1] * Sn[1] + Sn[2] * Sn[2]);
       sx[atom] = Sn[0] * mod; sy[atom] = Sn[1] * mod; sz[atom] = Sn[2] * mod;
    }
+}
+
+/* sim::LLG_Heun (src/simulate/LLGHeun.cpp:160-282): one stochastic Heun step.
+ * xi: 3n Gaussians for this step (NULL = no thermal term).  work: 15n doubles. */
+void vref_llg_heun_step(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,
+                        double* work) {
+   const int n = s->n;
+   double* px = work + 12 * n;  double* py = work + 13 * n;  double* pz = work + 14 * n;
+   vref_heun_predict(s, sx, sy, sz, xi, px, py, pz, work);
+   vref_heun_correct(s, sx, sy, sz, px, py, pz, work);
 }
 
 /* n_steps deterministic (T=0 or given-noise) steps; xi may be NULL or hold

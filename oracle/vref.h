@@ -45,6 +45,10 @@ typedef struct {
 void vref_spin_fields(const vref_sys* s, const double* sx, const double* sy, const double* sz,
                       double* hx, double* hy, double* hz);
 void vref_external_fields(const vref_sys* s, const double* xi, double* hx, double* hy, double* hz);
+void vref_heun_predict(const vref_sys* s, const double* sx, const double* sy, const double* sz, const double* xi,
+                       double* px, double* py, double* pz, double* keep);
+void vref_heun_correct(const vref_sys* s, double* sx, double* sy, double* sz, const double* px, const double* py,
+                       const double* pz, double* keep);
 void vref_llg_heun_step(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,
                         double* work);
 void vref_llg_heun(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,

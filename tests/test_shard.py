@@ -1,0 +1,152 @@
+"""Spatial sharding host logic (vampire_b200/shard.py) on CPU.
+
+The plan and local systems are checked structurally; the halo exchange runs
+as world_size-2 and -3 gloo process groups whose ranks step their shard with
+the FP64 oracle (predictor half, halo refresh of s', corrector half, halo
+refresh of s) and must reproduce the whole-system oracle bit for bit -- the
+same field sums in the same bond order, with the reference's replayed noise.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from vampire_b200 import shard as SH
+from vampire_b200 import system as S
+
+
+def _fcc(L=4, T=300.0):
+    return S.config_fcc_tensor(L=L, seed=11, temperature=T)
+
+
+def _sc_open():
+    mats = [S.Material(alpha=0.1, mu_s_muB=1.72, Ku=6.69e-24)]
+    p = S.SimParams(dt_SI=1e-16, temperature=0.0, H_applied=0.1, H_vec=(0.0, 0.0, 1.0))
+    return S.build("sc", 5, 4, 7, 3.0, mats, np.array([[11.2e-21]]), p, periodic=(False, True, False), spin_seed=3)
+
+
+@pytest.mark.parametrize("nranks", [1, 2, 3, 4])
+@pytest.mark.parametrize("maker", [_fcc, _sc_open])
+def test_plan_covers_system_and_halos_are_consistent(maker, nranks):
+    s = maker()
+    plans = SH.make_plan(s, nranks)
+    owned = np.concatenate([p.owned for p in plans])
+    assert np.array_equal(np.sort(owned), np.arange(s.n))          # a partition
+    owner = np.empty(s.n, dtype=int)
+    for p in plans:
+        owner[p.owned] = p.rank
+    for p in plans:
+        # halo = exactly the non-owned neighbours of owned atoms
+        need = set()
+        for i in p.owned:
+            for j in s.nl[s.nl_start[i]:s.nl_end[i] + 1]:
+                if owner[j] != p.rank:
+                    need.add(int(j))
+        assert set(p.halo.tolist()) == need
+        # every halo block matches what its source rank sends, in order
+        for src, (first, count) in p.recv.items():
+            sent = plans[src].send[p.rank]
+            assert sent.size == count
+            assert np.array_equal(plans[src].owned[sent], p.halo[first - p.n_owned:first - p.n_owned + count])
+        loc = SH.local_system(s, p)
+        assert loc.n == p.n_local
+        assert np.all(loc.nl_end[p.n_owned:] < loc.nl_start[p.n_owned:])  # halo rows empty
+        glob = np.concatenate([p.owned, p.halo])
+        for k in range(0, p.n_owned, max(1, p.n_owned // 17)):
+            g = p.owned[k]
+            mine = glob[loc.nl[loc.nl_start[k]:loc.nl_end[k] + 1]]
+            assert np.array_equal(mine, s.nl[s.nl_start[g]:s.nl_end[g] + 1])
+
+
+def test_contiguous_slabs_give_noise_base():
+    s = _fcc(L=4)
+    for p in SH.make_plan(s, 4):
+        assert p.noise_base == int(p.owned[0])
+
+
+def _free_port():
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def _rank_main(rank, world, port, maker_name, steps, seed, out_dir):
+    import torch
+    import torch.distributed as dist
+    from oracle import oracle as O
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        s = {"fcc": _fcc, "sc": _sc_open}[maker_name]()
+        plan = SH.make_plan(s, world)[rank]
+        loc = SH.local_system(s, plan)
+        o = O.OracleSystem(loc)
+        glob = np.concatenate([plan.owned, plan.halo])
+        rng = np.random.default_rng(seed)
+        xi_all = rng.standard_normal((steps, 3, s.n))
+        ex = SH.HaloExchange(plan)
+        state = {"cur": None}
+
+        def pack(peer, idx):
+            return torch.from_numpy(np.ascontiguousarray(state["cur"][:, idx]).ravel())
+
+        def unpack(peer, first, count, buf):
+            state["cur"][:, first:first + count] = buf.numpy().reshape(3, count)
+
+        def alloc(k):
+            return torch.empty(k, dtype=torch.float64)
+
+        spins = loc.spins.copy()
+        for t in range(steps):
+            xi = xi_all[t][:, glob].ravel()
+            p, keep = o.heun_predict(spins, xi)
+            state["cur"] = p
+            ex.exchange(pack, unpack, alloc)
+            spins = o.heun_correct(spins, p, keep)
+            state["cur"] = spins
+            ex.exchange(pack, unpack, alloc)
+        np.save(os.path.join(out_dir, f"rank{rank}.npy"), spins[:, :plan.n_owned])
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("maker_name,world", [("fcc", 2), ("sc", 3)])
+def test_gloo_sharded_oracle_equals_whole_system(tmp_path, maker_name, world):
+    import torch.multiprocessing as mp
+    from oracle import oracle as O
+    steps, seed = 5, 7
+    mp.start_processes(_rank_main, args=(world, _free_port(), maker_name, steps, seed, str(tmp_path)),
+                       nprocs=world, join=True, start_method="spawn")
+    s = {"fcc": _fcc, "sc": _sc_open}[maker_name]()
+    rng = np.random.default_rng(seed)
+    xi_all = rng.standard_normal((steps, 3, s.n))
+    whole = O.OracleSystem(s).llg_heun(s.spins, steps, xi_all.reshape(steps, -1).ravel())
+    plans = SH.make_plan(s, world)
+    got = np.zeros_like(whole)
+    for p in plans:
+        got[:, p.owned] = np.load(tmp_path / f"rank{p.rank}.npy")
+    np.testing.assert_array_equal(got, whole)
+
+
+def test_combined_magnetization_equals_whole_system():
+    s = _fcc(L=4)
+    mask, size = s.masks["material"]
+    mu = s.mu_s_muB()
+    whole = np.zeros((size, 4))
+    for q in range(3):
+        np.add.at(whole[:, q], mask, mu * s.spins[q])
+    np.add.at(whole[:, 3], mask, mu)
+    parts = np.zeros((size, 4))
+    for p in SH.make_plan(s, 3):
+        loc = SH.local_system(s, p)
+        lm, _ = loc.masks["material"]
+        lmu = loc.mu_s_muB()
+        o = slice(0, p.n_owned)
+        for q in range(3):
+            np.add.at(parts[:, q], lm[o], lmu[o] * loc.spins[q][o])
+        np.add.at(parts[:, 3], lm[o], lmu[o])
+    np.testing.assert_allclose(SH.combine_magnetization(parts), SH.combine_magnetization(whole), rtol=1e-13)

@@ -323,6 +323,7 @@ extern "C" int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* dd) {
    if (!h || !dd) return set_err(h, VGPU_ERR_ARG, "null argument");
    SysDev& S = h->sys;
    if (!S.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (S.n_owned < S.n) return set_err(h, VGPU_ERR_STATE, "the dipole solver runs on whole systems (handle holds a shard)");
    const int n = S.n, nc = dd->num_cells;
    if (nc <= 0 || !dd->atom_cell || !dd->cell_pos_mom || !dd->cell_volume || !dd->cell_natoms)
       return set_err(h, VGPU_ERR_ARG, "incomplete dipole descriptor");

@@ -23,7 +23,7 @@ __device__ __forceinline__ void thermal_xi(const LLGArgs<R>& a, int i, R& gx, R&
    }
    // batched systems: system k's atoms draw the stream of a single system
    // seeded seed + k, with their own local index (same numbers as a plain run)
-   uint32_t li = (uint32_t)i, klo = a.seed_lo, khi = a.seed_hi;
+   uint32_t li = (uint32_t)i + a.noise_base, klo = a.seed_lo, khi = a.seed_hi;
    if (a.sys_off) {
       const int k = (a.mat ? __ldg(a.mat + i) : 0) / a.m_per_sys;
       li = (uint32_t)(i - __ldg(a.sys_off + k));

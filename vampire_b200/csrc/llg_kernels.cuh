@@ -98,7 +98,7 @@ __device__ __forceinline__ void llg_correct_atom(const LLGArgs<R>& a, int i) {
 template <typename R, int FMT, int MODE>
 __global__ void __launch_bounds__(256) llg_pass_kernel(const LLGArgs<R> a) {
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-   if (i >= a.n) return;
+   if (i >= (MODE == PASS_FIELD ? a.n : a.n_upd)) return;
    if (MODE == PASS_PREDICTOR) {
       llg_predict_atom<R, FMT, 0>(a, i);
    } else if (MODE == PASS_CORRECTOR) {
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(256) llg_pass_kernel(const LLGArgs<R> a) {
 template <typename R, int FMT>
 inline cudaError_t launch_fmt(const LLGArgs<R>& a, int mode, cudaStream_t st) {
    const int bs = 256;
-   const int grid = (a.n + bs - 1) / bs;
+   const int grid = ((mode == PASS_FIELD ? a.n : a.n_upd) + bs - 1) / bs;
    if (grid == 0) return cudaSuccess;
    if (mode == PASS_PREDICTOR) llg_pass_kernel<R, FMT, PASS_PREDICTOR><<<grid, bs, 0, st>>>(a);
    else if (mode == PASS_CORRECTOR) llg_pass_kernel<R, FMT, PASS_CORRECTOR><<<grid, bs, 0, st>>>(a);

@@ -117,8 +117,8 @@ __global__ void __launch_bounds__(32 * SL) llg_staged_kernel(const LLGArgs<float
       // own-atom work that needs no records overlaps the copy: state, material,
       // external field (Philox noise, applied, dipole cell field)
       const int i = t * 32 * SL + tid;
-      const bool act = i < a.n;
-      const int ii = act ? i : a.n - 1;  // idle lanes of the last tile load in bounds
+      const bool act = i < a.n_upd;
+      const int ii = act ? i : a.n_upd - 1;  // idle lanes of the last tile load in bounds
       const int mi = a.mat ? __ldg(a.mat + ii) : 0;
       const MatParams<float> m = a.mp[mi];
       float S0[3] = {a.ax[ii], a.ay[ii], a.az[ii]};

@@ -194,6 +194,7 @@ extern "C" int vgpu_mc_setup(vgpu_handle h, const int32_t* colour_in, int32_t* n
    if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
    SysDev& S = h->sys;
    if (!S.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (S.n_owned < S.n) return set_err(h, VGPU_ERR_STATE, "Monte Carlo runs on whole systems (handle holds a shard)");
    cudaSetDevice(h->device);
    const int n = S.n;
    // neighbour lists back from the host copy kept at upload

@@ -11,8 +11,8 @@
 //   pass 1  each block accumulates, per mask bin, sum(mu s), sum(mu) and the
 //           four energy terms into shared memory (FP64) and writes one
 //           partial row per block;
-//   pass 2  one thread per (bin, quantity) sums the block partials with
-//           Neumaier compensation, then bins are normalised exactly as the
+//   pass 2  one warp per (bin, quantity) sums the block partials with
+//           compensated two-sums, then bins are normalised exactly as the
 //           reference does (unit vector and |m|/m_sat; exchange and
 //           magnetostatic energies halved) and added to the running means.
 //
@@ -37,6 +37,7 @@ struct StatsMask {
    double* partial = nullptr;  // [nblocks][size][ST_NQ]
    double* cur = nullptr;      // [size][ST_W] finalised rows
    double* mean = nullptr;     // [size][ST_W] running sums of the finalised rows
+   double* raw = nullptr;      // [size][ST_NQ] raw sums of the last update (combined across shards)
    long long counter_mag = 0, counter_en = 0;
 };
 
@@ -47,52 +48,95 @@ struct StatsState {
 
 static StatsState* stats_of(vgpu_ctx* h) { return (StatsState*)h->extras[0]; }
 
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+   return v;
+}
+
 template <typename R, int FMT>
 __global__ void stats_partial_kernel(const LLGArgs<R> a, const int* __restrict__ mask, int size, int do_energy,
                                      const R* __restrict__ hm, double* __restrict__ partial) {
    extern __shared__ double acc[];
    const int nq = ST_NQ;
+   const int nq_used = do_energy ? ST_NQ : ST_MU + 1;
+   const int lane = threadIdx.x & 31;
    for (int k = threadIdx.x; k < size * nq; k += blockDim.x) acc[k] = 0.0;
    __syncthreads();
-   const int per = (a.n + gridDim.x - 1) / gridDim.x;
+   const int per = (a.n_upd + gridDim.x - 1) / gridDim.x;  // owned atoms only
    const int begin = blockIdx.x * per;
-   const int end = min(a.n, begin + per);
-   for (int i = begin + threadIdx.x; i < end; i += blockDim.x) {
-      const int mi = a.mat ? __ldg(a.mat + i) : 0;
-      const MatParams<R> m = a.mp[mi];
-      const double mu = (double)m.mu_s_muB;
-      const R S[3] = {a.ax[i], a.ay[i], a.az[i]};
-      double* b = acc + (size_t)__ldg(mask + i) * nq;
-      atomicAdd(b + ST_MX, (double)S[0] * mu);
-      atomicAdd(b + ST_MY, (double)S[1] * mu);
-      atomicAdd(b + ST_MZ, (double)S[2] * mu);
-      atomicAdd(b + ST_MU, mu);
-      if (do_energy) {
-         R hx = 0, hy = 0, hz = 0;
-         exchange_gather<R, FMT>(a, i, mi, a.ax, a.ay, a.az, hx, hy, hz);
-         const double eex = -((double)S[0] * hx + (double)S[1] * hy + (double)S[2] * hz);
-         double ean = 0.0;
-         if (a.uniaxial) {
-            const double sd = (double)S[0] * m.kux + (double)S[1] * m.kuy + (double)S[2] * m.kuz;
-            ean += -(double)m.ku2 * (sd * sd);
+   const int end = min(a.n_upd, begin + per);
+   // block-uniform trip count: every lane of a warp runs the aggregation below
+   for (int base = begin; base < end; base += blockDim.x) {
+      const int i = base + threadIdx.x;
+      const bool on = i < end;
+      double q[ST_NQ];
+#pragma unroll
+      for (int k = 0; k < ST_NQ; ++k) q[k] = 0.0;
+      int bin = -1;
+      if (on) {
+         const int mi = a.mat ? __ldg(a.mat + i) : 0;
+         const MatParams<R> m = a.mp[mi];
+         const double mu = (double)m.mu_s_muB;
+         const R S[3] = {a.ax[i], a.ay[i], a.az[i]};
+         bin = __ldg(mask + i);
+         q[ST_MX] = (double)S[0] * mu;
+         q[ST_MY] = (double)S[1] * mu;
+         q[ST_MZ] = (double)S[2] * mu;
+         q[ST_MU] = mu;
+         if (do_energy) {
+            R hx = 0, hy = 0, hz = 0;
+            exchange_gather<R, FMT>(a, i, mi, a.ax, a.ay, a.az, hx, hy, hz);
+            const double eex = -((double)S[0] * hx + (double)S[1] * hy + (double)S[2] * hz);
+            double ean = 0.0;
+            if (a.uniaxial) {
+               const double sd = (double)S[0] * m.kux + (double)S[1] * m.kuy + (double)S[2] * m.kuz;
+               ean += -(double)m.ku2 * (sd * sd);
+            }
+            if (a.cubic) {
+               const double x2 = (double)S[0] * S[0], y2 = (double)S[1] * S[1], z2 = (double)S[2] * S[2];
+               ean += -0.5 * (double)m.kc4 * (x2 * x2 + y2 * y2 + z2 * z2);
+            }
+            const double eap = -((double)a.hx * S[0] + (double)a.hy * S[1] + (double)a.hz * S[2]);
+            double ems = 0.0;
+            if (a.cell) {
+               const int c = __ldg(a.cell + i);
+               ems = -((double)a.cell_hd[c] * S[0] + (double)a.cell_hd[a.ncells + c] * S[1] +
+                       (double)a.cell_hd[2 * a.ncells + c] * S[2]);
+            } else if (hm) {
+               ems = -((double)hm[i] * S[0] + (double)hm[a.n + i] * S[1] + (double)hm[2 * a.n + i] * S[2]);
+            }
+            q[ST_EEX] = eex * mu;
+            q[ST_EAN] = ean * mu;
+            q[ST_EAP] = eap * mu;
+            q[ST_EMS] = ems * mu;
          }
-         if (a.cubic) {
-            const double x2 = (double)S[0] * S[0], y2 = (double)S[1] * S[1], z2 = (double)S[2] * S[2];
-            ean += -0.5 * (double)m.kc4 * (x2 * x2 + y2 * y2 + z2 * z2);
+      }
+      // warp aggregation: one shuffle reduction per distinct bin in the warp
+      // (masks are mostly uniform over 32 consecutive atoms), so the shared
+      // accumulators see one atomic per bin and quantity instead of 32; a warp
+      // holding more than 4 bins adds the rest lane by lane
+      unsigned left = __ballot_sync(0xffffffffu, on);
+      for (int round = 0; left; ++round) {
+         if (round == 4) {
+            if (on && ((left >> lane) & 1u)) {
+#pragma unroll
+               for (int k = 0; k < ST_NQ; ++k)
+                  if (k < nq_used) atomicAdd(acc + (size_t)bin * nq + k, q[k]);
+            }
+            break;
          }
-         const double eap = -((double)a.hx * S[0] + (double)a.hy * S[1] + (double)a.hz * S[2]);
-         double ems = 0.0;
-         if (a.cell) {
-            const int c = __ldg(a.cell + i);
-            ems = -((double)a.cell_hd[c] * S[0] + (double)a.cell_hd[a.ncells + c] * S[1] +
-                    (double)a.cell_hd[2 * a.ncells + c] * S[2]);
-         } else if (hm) {
-            ems = -((double)hm[i] * S[0] + (double)hm[a.n + i] * S[1] + (double)hm[2 * a.n + i] * S[2]);
+         const int src = __ffs(left) - 1;
+         const int b = __shfl_sync(0xffffffffu, bin, src);
+         const bool mine = on && bin == b;
+         left &= ~__ballot_sync(0xffffffffu, mine);
+#pragma unroll
+         for (int k = 0; k < ST_NQ; ++k) {
+            if (k < nq_used) {
+               const double v = warp_sum(mine ? q[k] : 0.0);
+               if (lane == src) atomicAdd(acc + (size_t)b * nq + k, v);
+            }
          }
-         atomicAdd(b + ST_EEX, eex * mu);
-         atomicAdd(b + ST_EAN, ean * mu);
-         atomicAdd(b + ST_EAP, eap * mu);
-         atomicAdd(b + ST_EMS, ems * mu);
       }
    }
    __syncthreads();
@@ -100,22 +144,42 @@ __global__ void stats_partial_kernel(const LLGArgs<R> a, const int* __restrict__
    for (int k = threadIdx.x; k < size * nq; k += blockDim.x) out[k] = acc[k];
 }
 
-// Neumaier-compensated sum of block partials, then reference normalisation.
-__global__ void stats_final_kernel(const double* __restrict__ partial, int nblocks, int size, int do_mag,
-                                   int do_energy, double* __restrict__ cur, double* __restrict__ mean) {
-   const int bin = blockIdx.x * blockDim.x + threadIdx.x;
-   if (bin >= size) return;
-   double v[ST_NQ];
-   for (int q = 0; q < ST_NQ; ++q) {
-      double s = 0.0, c = 0.0;
-      for (int b = 0; b < nblocks; ++b) {
-         const double x = partial[((size_t)b * size + bin) * ST_NQ + q];
-         const double t = s + x;
-         c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
-         s = t;
+// Compensated sum of block partials, then reference normalisation.  One
+// block per bin, one warp per quantity: each lane keeps a Neumaier sum over a
+// strided share of the partials, and the 32 (sum, compensation) pairs are
+// merged by error-free two-sums in a fixed tree order (deterministic).
+__device__ __forceinline__ void two_sum_acc(double& s, double& c, double x) {
+   const double t = s + x;
+   c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+   s = t;
+}
+
+__global__ void __launch_bounds__(32 * ST_NQ) stats_final_kernel(const double* __restrict__ partial, int nblocks,
+                                                                  int size, int do_mag, int do_energy,
+                                                                  double* __restrict__ cur,
+                                                                  double* __restrict__ mean,
+                                                                  double* __restrict__ raw) {
+   __shared__ double vq[ST_NQ];
+   const int bin = blockIdx.x;
+   const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   double s = 0.0, c = 0.0;
+   for (int b = lane; b < nblocks; b += 32) two_sum_acc(s, c, partial[((size_t)b * size + bin) * ST_NQ + q]);
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) {
+      const double s2 = __shfl_down_sync(0xffffffffu, s, o);
+      const double c2 = __shfl_down_sync(0xffffffffu, c, o);
+      if (lane < o) {
+         two_sum_acc(s, c, s2);
+         c += c2;
       }
-      v[q] = s + c;
    }
+   if (lane == 0) {
+      vq[q] = s + c;
+      raw[(size_t)bin * ST_NQ + q] = s + c;
+   }
+   __syncthreads();
+   if (threadIdx.x != 0) return;
+   const double* v = vq;
    double* o = cur + (size_t)bin * ST_W;
    double* mn = mean + (size_t)bin * ST_W;
    if (do_mag) {
@@ -129,13 +193,13 @@ __global__ void stats_final_kernel(const double* __restrict__ partial, int nbloc
          o[2] = v[ST_MZ] / magm;
          o[3] = magm / msat;
       }
-      for (int q = 0; q < 4; ++q) mn[q] += o[q];
+      for (int k = 0; k < 4; ++k) mn[k] += o[k];
    }
    if (do_energy) {
       const double ex = 0.5 * v[ST_EEX], an = v[ST_EAN], ap = v[ST_EAP], ms = 0.5 * v[ST_EMS];
       o[4] = ex + an + ap + ms;
       o[5] = ex; o[6] = an; o[7] = ap; o[8] = ms;
-      for (int q = 4; q < 9; ++q) mn[q] += o[q];
+      for (int k = 4; k < 9; ++k) mn[k] += o[k];
    }
 }
 
@@ -151,8 +215,8 @@ static cudaError_t launch_stats(const LLGArgs<R>& a, StatsMask& m, int nblocks, 
    stats_partial_kernel<R, FMT><<<nblocks, 256, smem, st>>>(a, m.mask, m.size, do_energy, hm, m.partial);
    cudaError_t e = cudaGetLastError();
    if (e != cudaSuccess) return e;
-   stats_final_kernel<<<(m.size + 127) / 128, 128, 0, st>>>(m.partial, nblocks, m.size, do_mag, do_energy, m.cur,
-                                                           m.mean);
+   stats_final_kernel<<<m.size, 32 * ST_NQ, 0, st>>>(m.partial, nblocks, m.size, do_mag, do_energy, m.cur, m.mean,
+                                                     m.raw);
    return cudaGetLastError();
 }
 
@@ -173,7 +237,7 @@ void stats_destroy(vgpu_ctx* h) {
    StatsState* s = stats_of(h);
    if (!s) return;
    for (StatsMask& m : s->masks) {
-      cudaFree(m.mask); cudaFree(m.partial); cudaFree(m.cur); cudaFree(m.mean);
+      cudaFree(m.mask); cudaFree(m.partial); cudaFree(m.cur); cudaFree(m.mean); cudaFree(m.raw);
    }
    delete s;
    h->extras[0] = nullptr;
@@ -206,6 +270,8 @@ extern "C" int vgpu_stats_add_mask(vgpu_handle h, const int32_t* mask, int32_t m
    if ((e = cudaMalloc(&m.cur, sizeof(double) * mask_size * ST_W)) != cudaSuccess) return cuda_err(h, e, "stats");
    if ((e = cudaMalloc(&m.mean, sizeof(double) * mask_size * ST_W)) != cudaSuccess)
       return cuda_err(h, e, "stats");
+   if ((e = cudaMalloc(&m.raw, sizeof(double) * mask_size * ST_NQ)) != cudaSuccess) return cuda_err(h, e, "stats");
+   cudaMemsetAsync(m.raw, 0, sizeof(double) * mask_size * ST_NQ, h->stream);
    cudaMemcpyAsync(m.mask, mask, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream);
    cudaMemsetAsync(m.cur, 0, sizeof(double) * mask_size * ST_W, h->stream);
    cudaMemsetAsync(m.mean, 0, sizeof(double) * mask_size * ST_W, h->stream);
@@ -285,4 +351,18 @@ extern "C" int vgpu_stats_reset(vgpu_handle h) {
       m.counter_mag = m.counter_en = 0;
    }
    return cuda_err(h, cudaStreamSynchronize(h->stream), "statistics reset");
+}
+
+/* raw per-bin sums of the last update: [bin][8] = sum mu s_x, sum mu s_y,
+ * sum mu s_z, sum mu (mu_B), then the four energy sums (exchange and
+ * magnetostatic not yet halved); shards add these across ranks */
+extern "C" int vgpu_stats_get_sums(vgpu_handle h, int32_t id, double* sums) {
+   if (!h || !sums) return set_err(h, VGPU_ERR_ARG, "null argument");
+   StatsState* s = stats_of(h);
+   if (!s || id < 0 || id >= (int)s->masks.size()) return set_err(h, VGPU_ERR_ARG, "unknown statistics mask %d", id);
+   StatsMask& m = s->masks[id];
+   cudaSetDevice(h->device);
+   cudaError_t e = cudaMemcpyAsync(sums, m.raw, sizeof(double) * m.size * ST_NQ, cudaMemcpyDeviceToHost, h->stream);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+   return cuda_err(h, e, "statistics sums");
 }

@@ -248,6 +248,7 @@ static int upload_typed(vgpu_ctx* h, const vgpu_system_desc* d) {
    h->free_system();
    SysDev& S = h->sys;
    S.n = n; S.M = M; S.nslices = nslices; S.n_alloc = n_alloc; S.fmt = fmt;
+   S.n_owned = n;
    S.mat_shift = use_shift; S.idx_mask = use_shift ? ((1 << use_shift) - 1) : 0x7fffffff;
    S.num_bonds = d->num_bonds; S.sell_entries = (int64_t)ne;
    S.uniaxial = d->uniaxial_enabled; S.cubic = d->cubic_enabled;
@@ -345,6 +346,8 @@ LLGArgs<R> make_args(vgpu_ctx* h) {
    LLGArgs<R> a;
    memset(&a, 0, sizeof a);
    a.n = S.n;
+   a.n_upd = S.n_owned;
+   a.noise_base = S.noise_base;
    a.slice_off = (const int*)S.slice_off;
    a.col = (const int*)S.col;
    a.idx_mask = S.idx_mask;
@@ -434,8 +437,9 @@ static cudaError_t launch_step_pass(vgpu_ctx* h, const LLGArgs<R>& a, int mode, 
    return launch_llg_pass<R>(a, h->sys.fmt, mode, h->sys.nslices, h->stream);
 }
 
+// increment buffers and the staged launch shape, before any pass
 template <typename R>
-static int llg_steps_typed(vgpu_ctx* h, uint64_t n_steps) {
+static int prepare_passes(vgpu_ctx* h, bool* staged_out) {
    int rc0 = ensure_increment<R>(h);
    if (rc0) return rc0;
    const bool staged = use_staged<R>(h);
@@ -444,26 +448,68 @@ static int llg_steps_typed(vgpu_ctx* h, uint64_t n_steps) {
       c.sl = h->stage_sl;
       c.nbuf = h->stage_nbuf;
       c.buf_bytes = h->sys.stage_bytes[stage_slot(c.sl)];
-      cudaError_t e = prepare_llg_staged(c, h->sys.nslices, h->device);
+      cudaError_t e = prepare_llg_staged(c, (h->sys.n_owned + 31) / 32, h->device);
       if (e != cudaSuccess) return cuda_err(h, e, "staged pass setup (tile records exceed shared memory?)");
       h->sys.stage = c;
    }
-   for (uint64_t t = 0; t < n_steps; ++t) {
-      LLGArgs<R> a = make_args<R>(h);
-      cudaError_t e;
-      h->prof_begin(PROF_PREDICTOR);
-      e = launch_step_pass<R>(h, a, PASS_PREDICTOR, staged);
-      h->prof_end(PROF_PREDICTOR);
-      h->prof_begin(PROF_CORRECTOR);
-      if (e == cudaSuccess) e = launch_step_pass<R>(h, a, PASS_CORRECTOR, staged);
-      h->prof_end(PROF_CORRECTOR);
-      if (e != cudaSuccess) return cuda_err(h, e, "llg_heun launch");
-      h->kernel_launches += 2;
-      h->step++;
-      int rc = h->after_step();
-      if (rc) return rc;
-   }
+   *staged_out = staged;
    return VGPU_OK;
+}
+
+// one fused pass; the corrector completes the step (counter, dipole cadence)
+template <typename R>
+static int run_pass(vgpu_ctx* h, int mode, bool staged) {
+   LLGArgs<R> a = make_args<R>(h);
+   const int kind = mode == PASS_PREDICTOR ? PROF_PREDICTOR : PROF_CORRECTOR;
+   h->prof_begin(kind);
+   cudaError_t e = launch_step_pass<R>(h, a, mode, staged);
+   h->prof_end(kind);
+   if (e != cudaSuccess) return cuda_err(h, e, "llg_heun launch");
+   h->kernel_launches += 1;
+   if (mode == PASS_PREDICTOR) return VGPU_OK;
+   h->step++;
+   return h->after_step();
+}
+
+template <typename R>
+static int llg_steps_typed(vgpu_ctx* h, uint64_t n_steps) {
+   bool staged = false;
+   int rc = prepare_passes<R>(h, &staged);
+   for (uint64_t t = 0; t < n_steps && !rc; ++t) {
+      rc = run_pass<R>(h, PASS_PREDICTOR, staged);
+      if (!rc) rc = run_pass<R>(h, PASS_CORRECTOR, staged);
+   }
+   return rc;
+}
+
+template <typename R>
+static int llg_pass_typed(vgpu_ctx* h, int mode) {
+   bool staged = false;
+   int rc = prepare_passes<R>(h, &staged);
+   return rc ? rc : run_pass<R>(h, mode, staged);
+}
+
+// halo transfers of a shard (device buffers of the caller, handle precision)
+template <typename R>
+__global__ void halo_pack_kernel(const R* __restrict__ x, const R* __restrict__ y, const R* __restrict__ z,
+                                 const int* __restrict__ idx, int count, int n, R* __restrict__ out) {
+   const int k = blockIdx.x * blockDim.x + threadIdx.x;
+   if (k >= count) return;
+   const int i = idx[k];
+   const bool ok = i >= 0 && i < n;  // out-of-range indices send zeros
+   out[k] = ok ? x[i] : (R)0;
+   out[count + k] = ok ? y[i] : (R)0;
+   out[2 * count + k] = ok ? z[i] : (R)0;
+}
+
+template <typename R>
+__global__ void halo_unpack_kernel(R* __restrict__ x, R* __restrict__ y, R* __restrict__ z, int first, int count,
+                                   const R* __restrict__ in) {
+   const int k = blockIdx.x * blockDim.x + threadIdx.x;
+   if (k >= count) return;
+   x[first + k] = in[k];
+   y[first + k] = in[count + k];
+   z[first + k] = in[2 * count + k];
 }
 
 }  // namespace vgpu
@@ -791,6 +837,69 @@ static int noise_typed(vgpu_handle h, uint64_t step, double* xi) {
    const int n = S.n;
    double* out[3] = {xi, xi + n, xi + 2 * (size_t)n};
    return get_vec_typed<R>(h, S.f, out);
+}
+
+extern "C" int vgpu_llg_pass(vgpu_handle h, int pass) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (!(h->params.dt > 0.0)) return set_err(h, VGPU_ERR_STATE, "vgpu_set_params not called");
+   if (pass != VGPU_PASS_PREDICTOR && pass != VGPU_PASS_CORRECTOR) return set_err(h, VGPU_ERR_ARG, "unknown pass %d", pass);
+   cudaSetDevice(h->device);
+   const int mode = pass == VGPU_PASS_PREDICTOR ? PASS_PREDICTOR : PASS_CORRECTOR;
+   return h->prec == VGPU_PREC_FP64 ? llg_pass_typed<double>(h, mode) : llg_pass_typed<float>(h, mode);
+}
+
+extern "C" int vgpu_set_owned(vgpu_handle h, int32_t n_owned, int64_t noise_base) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   SysDev& S = h->sys;
+   if (!S.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (n_owned < 0 || n_owned > S.n) return set_err(h, VGPU_ERR_ARG, "n_owned %d outside 0..%d", n_owned, S.n);
+   if (noise_base < 0 || noise_base + (int64_t)n_owned > ((int64_t)1 << 32))
+      return set_err(h, VGPU_ERR_ARG, "noise_base out of the 32-bit atom counter range");
+   if (n_owned < S.n && (h->extras[1] || h->extras[2]))
+      return set_err(h, VGPU_ERR_STATE, "Monte Carlo and the dipole solver run on whole systems only");
+   S.n_owned = n_owned;
+   S.noise_base = (uint32_t)noise_base;
+   S.stage.grid = 0;
+   return VGPU_OK;
+}
+
+template <typename R>
+static int halo_typed(vgpu_handle h, int which, const int32_t* idx, int32_t first, int32_t count, void* buf,
+                      bool pack) {
+   SysDev& S = h->sys;
+   void* const* st = which == VGPU_STATE_SPIN ? S.s : S.p;
+   if (count == 0) return VGPU_OK;
+   const int grid = (count + 255) / 256;
+   if (pack)
+      halo_pack_kernel<R><<<grid, 256, 0, h->stream>>>((const R*)st[0], (const R*)st[1], (const R*)st[2], idx, count,
+                                                       S.n, (R*)buf);
+   else
+      halo_unpack_kernel<R><<<grid, 256, 0, h->stream>>>((R*)st[0], (R*)st[1], (R*)st[2], first, count,
+                                                         (const R*)buf);
+   h->kernel_launches++;
+   return cuda_err(h, cudaGetLastError(), pack ? "halo pack" : "halo unpack");
+}
+
+extern "C" int vgpu_halo_pack(vgpu_handle h, int which, const int32_t* idx, int32_t count, void* out) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (which != VGPU_STATE_SPIN && which != VGPU_STATE_PREDICTOR) return set_err(h, VGPU_ERR_ARG, "unknown state");
+   if (count < 0 || (count > 0 && (!idx || !out))) return set_err(h, VGPU_ERR_ARG, "bad halo buffer");
+   cudaSetDevice(h->device);
+   return h->prec == VGPU_PREC_FP64 ? halo_typed<double>(h, which, idx, 0, count, out, true)
+                                    : halo_typed<float>(h, which, idx, 0, count, out, true);
+}
+
+extern "C" int vgpu_halo_unpack(vgpu_handle h, int which, int32_t first, int32_t count, const void* in) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (which != VGPU_STATE_SPIN && which != VGPU_STATE_PREDICTOR) return set_err(h, VGPU_ERR_ARG, "unknown state");
+   if (count < 0 || first < 0 || (int64_t)first + count > h->sys.n || (count > 0 && !in))
+      return set_err(h, VGPU_ERR_ARG, "halo block %d..%d outside the system", first, first + count);
+   cudaSetDevice(h->device);
+   return h->prec == VGPU_PREC_FP64 ? halo_typed<double>(h, which, nullptr, first, count, const_cast<void*>(in), false)
+                                    : halo_typed<float>(h, which, nullptr, first, count, const_cast<void*>(in), false);
 }
 
 extern "C" int vgpu_thermal_noise(vgpu_handle h, uint64_t step, double* xi) {

@@ -16,6 +16,8 @@ namespace vgpu {
 struct SysDev {
    bool uploaded = false;
    int n = 0, M = 1, nslices = 0, n_alloc = 0, fmt = 0;
+   int n_owned = 0;           // atoms 0..n_owned-1 are updated (n unless vgpu_set_owned)
+   uint32_t noise_base = 0;   // Philox atom index of local atom 0
    int mat_shift = 0, idx_mask = 0x7fffffff;
    int64_t num_bonds = 0, sell_entries = 0;
    int uniaxial = 0, cubic = 0;

@@ -41,7 +41,9 @@ struct MatParams {
 // Everything one fused LLG pass needs, passed by value.
 template <typename R>
 struct LLGArgs {
-   int n;                    // atoms
+   int n;                    // atoms (array length of the per-atom inputs)
+   int n_upd;                // atoms the passes update: all, or the owned atoms of a shard (0..n_upd-1)
+   uint32_t noise_base;      // added to the atom index in the Philox counter (global index of a shard's atom 0)
    const int* slice_off;     // [nslices+1] SELL-32 entry offsets
    const int* col;           // packed neighbour index (| mat << mat_shift)
    int idx_mask;             // mask of the neighbour index bits

@@ -1,0 +1,243 @@
+"""Spatial sharding of one spin system over ranks (one process per GPU).
+
+The reference distributes a system over MPI ranks by space: each rank owns
+the atoms of its sub-domain ("core" and "boundary" atoms) and keeps copies of
+the neighbouring ranks' boundary atoms ("halo"), refreshed before every field
+evaluation (src/simulate/LLGHeun-mpi.cpp:62-64, src/mpi/mpi_comms.cpp:45-143).
+The same decomposition here, one process per GPU over NVLink/NCCL:
+
+* ``make_plan`` cuts the system into ``nranks`` slabs of equal atom count
+  along one axis (ties broken by atom index) and, for every rank, lists its
+  owned atoms, its halo atoms grouped by owning rank, and for every peer the
+  owned atoms that peer holds as halo (in the peer's halo order).  Every rank
+  computes the same plan from the same system, so no plan is exchanged.
+* ``local_system`` renumbers a rank's share: owned atoms first (global
+  order), then halo atoms by source rank.  Owned atoms keep their bonds
+  (neighbour indices renumbered, bond order and couplings unchanged, so the
+  field of an owned atom is the same sum in the same order as in the whole
+  system); halo atoms carry no bonds -- their spins are inputs only.
+* ``HaloExchange`` moves the boundary spins between the two passes of a Heun
+  step: one send and one receive per peer (three components packed into one
+  message), posted together with ``torch.distributed.batch_isend_irecv``.
+  It works with CPU tensors over gloo (tests) and device tensors over NCCL.
+* ``ShardedSimulation`` drives one rank's shard on its GPU: predictor pass,
+  halo exchange of s', corrector pass, halo exchange of s.  The fused passes
+  update the owned atoms only (``vgpu_set_owned``) and key the thermal noise
+  by global atom index, so a sharded run draws the same noise as one GPU.
+
+Statistics combine across ranks from the raw per-bin sums of each shard
+(``vgpu_stats_get_sums``) with one all-reduce.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional, Tuple
+
+import numpy as np
+
+from .system import SpinSystem
+
+
+@dataclass
+class ShardPlan:
+    rank: int
+    nranks: int
+    owned: np.ndarray                     # global ids of owned atoms (ascending)
+    halo: np.ndarray                      # global ids of halo atoms, grouped by source rank
+    recv: Dict[int, Tuple[int, int]]      # peer -> (first local index, count) of its halo block
+    send: Dict[int, np.ndarray]           # peer -> local indices of owned atoms it holds as halo
+    noise_base: Optional[int]             # global id of owned[0] when owned is one contiguous range
+
+    @property
+    def n_owned(self) -> int:
+        return int(self.owned.size)
+
+    @property
+    def n_local(self) -> int:
+        return int(self.owned.size + self.halo.size)
+
+
+def _owner_slabs(s: SpinSystem, nranks: int, axis: int) -> np.ndarray:
+    """Owner rank of every atom: equal-count slabs along `axis` (atom index
+    order when the system has no coordinates)."""
+    n = s.n
+    if s.coords is not None:
+        order = np.lexsort((np.arange(n), s.coords[axis]))
+    else:
+        order = np.arange(n)
+    owner = np.empty(n, dtype=np.int32)
+    bounds = np.linspace(0, n, nranks + 1).round().astype(np.int64)
+    for r in range(nranks):
+        owner[order[bounds[r]:bounds[r + 1]]] = r
+    return owner
+
+
+def make_plan(s: SpinSystem, nranks: int, axis: int = 2) -> List[ShardPlan]:
+    if nranks < 1:
+        raise ValueError("nranks must be >= 1")
+    n = s.n
+    owner = _owner_slabs(s, nranks, axis)
+    deg = (s.nl_end - s.nl_start + 1).astype(np.int64)
+    src = np.repeat(np.arange(n), deg)                    # bond -> atom
+    nbr = s.nl.astype(np.int64)
+    # (rank r needs atom j as halo) for bonds i -> j with owner[i] = r != owner[j]
+    cross = owner[src] != owner[nbr]
+    need = {r: set() for r in range(nranks)}
+    for r, j in zip(owner[src[cross]], nbr[cross]):
+        need[int(r)].add(int(j))
+    plans = []
+    owned_of = [np.flatnonzero(owner == r) for r in range(nranks)]
+    halo_of = {}
+    for r in range(nranks):
+        h = np.array(sorted(need[r], key=lambda j: (owner[j], j)), dtype=np.int64)
+        halo_of[r] = h
+    for r in range(nranks):
+        own = owned_of[r]
+        h = halo_of[r]
+        recv = {}
+        first = own.size
+        for p in range(nranks):
+            cnt = int(np.count_nonzero(owner[h] == p)) if h.size else 0
+            if cnt:
+                recv[p] = (first, cnt)
+                first += cnt
+        send = {}
+        pos = {int(g): k for k, g in enumerate(own)}
+        for p in range(nranks):
+            if p == r:
+                continue
+            hp = halo_of[p]
+            mine = hp[owner[hp] == r] if hp.size else hp
+            if mine.size:
+                send[p] = np.array([pos[int(g)] for g in mine], dtype=np.int32)
+        contiguous = own.size > 0 and int(own[-1]) - int(own[0]) + 1 == own.size
+        plans.append(ShardPlan(rank=r, nranks=nranks, owned=own, halo=h, recv=recv, send=send,
+                               noise_base=int(own[0]) if contiguous else None))
+    return plans
+
+
+def local_system(s: SpinSystem, plan: ShardPlan) -> SpinSystem:
+    """The rank's share of `s`: owned atoms (with their bonds) then halo atoms
+    (no bonds), neighbour indices renumbered locally."""
+    glob = np.concatenate([plan.owned, plan.halo]).astype(np.int64)
+    loc = np.full(s.n, -1, dtype=np.int64)
+    loc[glob] = np.arange(glob.size)
+    n_own, n_loc = plan.n_owned, plan.n_local
+    st = s.nl_start[plan.owned].astype(np.int64)
+    en = s.nl_end[plan.owned].astype(np.int64)
+    deg = en - st + 1
+    bonds = np.concatenate([np.arange(a, b + 1) for a, b in zip(st, en)]) if n_own else np.zeros(0, np.int64)
+    nl = loc[s.nl[bonds]]
+    if (nl < 0).any():
+        raise AssertionError("halo plan misses a neighbour")
+    start = np.zeros(n_loc, dtype=np.int32)
+    end = np.zeros(n_loc, dtype=np.int32)
+    off = np.concatenate([[0], np.cumsum(deg)])
+    start[:n_own] = off[:-1]
+    end[:n_own] = off[1:] - 1
+    start[n_own:] = off[-1]           # halo atoms: empty rows (end = start - 1)
+    end[n_own:] = off[-1] - 1
+    if s.nl_type is not None:
+        nl_type = s.nl_type[bonds].astype(np.int32)
+        jlist = s.jlist
+    else:
+        w = {0: 1, 1: 3, 2: 9}[s.exch_type]
+        nl_type = None
+        jlist = s.jlist.reshape(-1, w)[bonds].ravel() if w > 1 else s.jlist[bonds]
+    masks = {k: (np.asarray(m)[glob].astype(np.int32), size) for k, (m, size) in s.masks.items()}
+    return SpinSystem(n=n_loc, nl_start=start, nl_end=end, nl=nl.astype(np.int32), jlist=jlist,
+                      exch_type=s.exch_type, type=s.type[glob].astype(np.int32), materials=s.materials,
+                      spins=np.ascontiguousarray(s.spins[:, glob]), params=s.params, uniaxial=s.uniaxial,
+                      cubic=s.cubic, nl_type=nl_type,
+                      coords=None if s.coords is None else np.ascontiguousarray(s.coords[:, glob]),
+                      masks=masks, cells=None)
+
+
+class HaloExchange:
+    """One halo refresh: for every peer, pack(peer, local_idx) -> tensor of
+    3*count values is sent, and unpack(peer, first, count, tensor) receives
+    the peer's block.  All sends and receives of a refresh are posted at once
+    (torch.distributed.batch_isend_irecv), then waited for."""
+
+    def __init__(self, plan: ShardPlan, group=None):
+        self.plan = plan
+        self.group = group
+
+    def exchange(self, pack: Callable, unpack: Callable, alloc: Callable) -> None:
+        import torch.distributed as dist
+        ops, recv = [], {}
+        for peer, (first, count) in sorted(self.plan.recv.items()):
+            buf = alloc(3 * count)
+            recv[peer] = (first, count, buf)
+            ops.append(dist.P2POp(dist.irecv, buf, peer, self.group))
+        for peer, idx in sorted(self.plan.send.items()):
+            ops.append(dist.P2POp(dist.isend, pack(peer, idx), peer, self.group))
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        for peer, (first, count, buf) in recv.items():
+            unpack(peer, first, count, buf)
+
+
+def combine_magnetization(sums: np.ndarray) -> np.ndarray:
+    """Reference normalisation (src/statistics/magnetization.cpp:134-180) of
+    raw per-bin sums [bins, >=4] = (sum mu sx, sum mu sy, sum mu sz, sum mu)
+    added over ranks: rows (m_hat_x, m_hat_y, m_hat_z, |m|/m_sat)."""
+    out = np.zeros((sums.shape[0], 4))
+    for b, v in enumerate(sums):
+        msat = v[3]
+        mag = np.sqrt(v[0] ** 2 + v[1] ** 2 + v[2] ** 2)
+        if msat != 0.0:
+            out[b] = (v[0] / mag, v[1] / mag, v[2] / mag, mag / msat)
+    return out
+
+
+class ShardedSimulation:
+    """One rank's shard on its GPU (vampire_b200.vgpu over the C ABI), with
+    NCCL halo exchange between the passes.  Collectives are issued on the
+    library's stream, so the exchange is ordered after the pass that produced
+    the boundary spins and before the pass that reads them."""
+
+    def __init__(self, s: SpinSystem, plan: ShardPlan, device: int, precision: str = "fp32",
+                 noise_seed: int = 0, group=None):
+        import torch
+        from . import vgpu
+        self.plan = plan
+        self.local = local_system(s, plan)
+        self.sim = vgpu.Simulation(self.local, device=device, precision=precision, noise_seed=noise_seed)
+        self.sim.set_owned(plan.n_owned, plan.noise_base if plan.noise_base is not None else 0)
+        self.dtype = torch.float64 if precision == "fp64" else torch.float32
+        self.device = torch.device("cuda", device)
+        self.stream = torch.cuda.ExternalStream(self.sim.stream_ptr(), device=self.device)
+        self.idx = {p: torch.as_tensor(ix, dtype=torch.int32, device=self.device) for p, ix in plan.send.items()}
+        self.halo = HaloExchange(plan, group)
+        self._torch = torch
+
+    def _refresh(self, which: int) -> None:
+        torch = self._torch
+
+        def pack(peer, _idx):
+            ix = self.idx[peer]
+            out = torch.empty(3 * ix.numel(), dtype=self.dtype, device=self.device)
+            self.sim.halo_pack(which, ix.data_ptr(), ix.numel(), out.data_ptr())
+            return out
+
+        def unpack(peer, first, count, buf):
+            self.sim.halo_unpack(which, first, count, buf.data_ptr())
+
+        def alloc(k):
+            return torch.empty(k, dtype=self.dtype, device=self.device)
+
+        with torch.cuda.stream(self.stream):
+            self.halo.exchange(pack, unpack, alloc)
+
+    def step(self, n_steps: int = 1) -> None:
+        from . import vgpu
+        for _ in range(n_steps):
+            self.sim.llg_pass(vgpu.PASS_PREDICTOR)
+            self._refresh(vgpu.STATE_PREDICTOR)
+            self.sim.llg_pass(vgpu.PASS_CORRECTOR)
+            self._refresh(vgpu.STATE_SPIN)
+
+    def owned_spins(self) -> np.ndarray:
+        return self.sim.spins()[:, : self.plan.n_owned]

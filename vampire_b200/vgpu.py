@@ -24,6 +24,8 @@ PREC_FP32, PREC_FP64 = 0, 1
 NOISE_PHILOX, NOISE_REPLAY = 0, 1
 OPT_STORE_INCREMENT, OPT_STAGED_RECORDS, OPT_STAGE_SLICES, OPT_STAGE_BUFFERS, OPT_DIPOLE_FFT = 1, 2, 3, 4, 5
 OPT_STAGE_WAIT_TEST = 6
+PASS_PREDICTOR, PASS_CORRECTOR = 0, 1
+STATE_SPIN, STATE_PREDICTOR = 0, 1
 DIPOLE_FAR_DIRECT, DIPOLE_FAR_FFT = 0, 1
 
 _D = C.POINTER(C.c_double)
@@ -253,6 +255,29 @@ class Simulation:
 
     def llg_heun(self, n_steps: int = 1) -> None:
         self._check(lib().vgpu_llg_heun(self._h, C.c_uint64(n_steps)))
+
+    # -- shards ------------------------------------------------------------
+    def llg_pass(self, which: int) -> None:
+        """One fused pass: PASS_PREDICTOR or PASS_CORRECTOR (vgpu_llg_pass)."""
+        self._check(lib().vgpu_llg_pass(self._h, C.c_int(which)))
+
+    def set_owned(self, n_owned: int, noise_base: int = 0) -> None:
+        self._check(lib().vgpu_set_owned(self._h, C.c_int32(n_owned), C.c_int64(noise_base)))
+
+    def halo_pack(self, which: int, idx_ptr: int, count: int, out_ptr: int) -> None:
+        """Device pointers: idx (int32[count]) -> out (3*count values)."""
+        self._check(lib().vgpu_halo_pack(self._h, C.c_int(which), C.c_void_p(idx_ptr), C.c_int32(count),
+                                         C.c_void_p(out_ptr)))
+
+    def halo_unpack(self, which: int, first: int, count: int, in_ptr: int) -> None:
+        self._check(lib().vgpu_halo_unpack(self._h, C.c_int(which), C.c_int32(first), C.c_int32(count),
+                                           C.c_void_p(in_ptr)))
+
+    def stats_sums(self, mask_id: int, size: int) -> np.ndarray:
+        """Raw per-bin sums of the last statistics update, (size, 8)."""
+        out = np.zeros((size, 8))
+        self._check(lib().vgpu_stats_get_sums(self._h, C.c_int32(mask_id), _ptr(out, _D)))
+        return out
 
     # -- dipole field --------------------------------------------------------
     def dipole_setup(self, cells: dict) -> None:
