@@ -26,11 +26,12 @@ def _sc_open():
     return S.build("sc", 5, 4, 7, 3.0, mats, np.array([[11.2e-21]]), p, periodic=(False, True, False), spin_seed=3)
 
 
+@pytest.mark.parametrize("by", ["index", "z", "x"])
 @pytest.mark.parametrize("nranks", [1, 2, 3, 4])
 @pytest.mark.parametrize("maker", [_fcc, _sc_open])
-def test_plan_covers_system_and_halos_are_consistent(maker, nranks):
+def test_plan_covers_system_and_halos_are_consistent(maker, nranks, by):
     s = maker()
-    plans = SH.make_plan(s, nranks)
+    plans = SH.make_plan(s, nranks, by=by)
     owned = np.concatenate([p.owned for p in plans])
     assert np.array_equal(np.sort(owned), np.arange(s.n))          # a partition
     owner = np.empty(s.n, dtype=int)
@@ -59,9 +60,10 @@ def test_plan_covers_system_and_halos_are_consistent(maker, nranks):
             assert np.array_equal(mine, s.nl[s.nl_start[g]:s.nl_end[g] + 1])
 
 
-def test_contiguous_slabs_give_noise_base():
-    s = _fcc(L=4)
-    for p in SH.make_plan(s, 4):
+@pytest.mark.parametrize("nranks", [2, 3, 5])
+def test_index_shares_give_noise_base(nranks):
+    s = _fcc(L=3)
+    for p in SH.make_plan(s, nranks):
         assert p.noise_base == int(p.owned[0])
 
 

@@ -103,4 +103,13 @@ cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, co
 template <typename R>
 cudaError_t launch_thermal_noise(const LLGArgs<R>& a, cudaStream_t st);
 
+// The passes are instantiated once per precision, in llg_kernels_fp32.cu and
+// llg_kernels_fp64.cu (the latter without FMA contraction, for FP64 results
+// equal to the reference's); other translation units that see the template
+// bodies must not instantiate their own copies.
+extern template cudaError_t launch_llg_pass<float>(const LLGArgs<float>&, int, int, int, cudaStream_t);
+extern template cudaError_t launch_llg_pass<double>(const LLGArgs<double>&, int, int, int, cudaStream_t);
+extern template cudaError_t launch_thermal_noise<float>(const LLGArgs<float>&, cudaStream_t);
+extern template cudaError_t launch_thermal_noise<double>(const LLGArgs<double>&, cudaStream_t);
+
 }  // namespace vgpu

@@ -6,8 +6,8 @@ the neighbouring ranks' boundary atoms ("halo"), refreshed before every field
 evaluation (src/simulate/LLGHeun-mpi.cpp:62-64, src/mpi/mpi_comms.cpp:45-143).
 The same decomposition here, one process per GPU over NVLink/NCCL:
 
-* ``make_plan`` cuts the system into ``nranks`` slabs of equal atom count
-  along one axis (ties broken by atom index) and, for every rank, lists its
+* ``make_plan`` cuts the system into ``nranks`` shares of equal atom count
+  (contiguous atom-index ranges, or slabs along one axis) and, for every rank, lists its
   owned atoms, its halo atoms grouped by owning rank, and for every peer the
   owned atoms that peer holds as halo (in the peer's halo order).  Every rank
   computes the same plan from the same system, so no plan is exchanged.
@@ -57,14 +57,17 @@ class ShardPlan:
         return int(self.owned.size + self.halo.size)
 
 
-def _owner_slabs(s: SpinSystem, nranks: int, axis: int) -> np.ndarray:
-    """Owner rank of every atom: equal-count slabs along `axis` (atom index
-    order when the system has no coordinates)."""
+def _owner_slabs(s: SpinSystem, nranks: int, by: str) -> np.ndarray:
+    """Owner rank of every atom.  by="index": equal contiguous ranges of atom
+    index (cell layers for lattices numbered cell by cell along z, as the
+    builders and the reference's unit-cell loops do; a shard's noise then
+    follows the whole system's Philox stream); by="x"|"y"|"z": equal-count
+    slabs along that coordinate (ties broken by atom index)."""
     n = s.n
-    if s.coords is not None:
-        order = np.lexsort((np.arange(n), s.coords[axis]))
-    else:
+    if by == "index" or s.coords is None:
         order = np.arange(n)
+    else:
+        order = np.lexsort((np.arange(n), s.coords["xyz".index(by)]))
     owner = np.empty(n, dtype=np.int32)
     bounds = np.linspace(0, n, nranks + 1).round().astype(np.int64)
     for r in range(nranks):
@@ -72,11 +75,13 @@ def _owner_slabs(s: SpinSystem, nranks: int, axis: int) -> np.ndarray:
     return owner
 
 
-def make_plan(s: SpinSystem, nranks: int, axis: int = 2) -> List[ShardPlan]:
+def make_plan(s: SpinSystem, nranks: int, by: str = "index") -> List[ShardPlan]:
     if nranks < 1:
         raise ValueError("nranks must be >= 1")
+    if by not in ("index", "x", "y", "z"):
+        raise ValueError("by must be 'index', 'x', 'y' or 'z'")
     n = s.n
-    owner = _owner_slabs(s, nranks, axis)
+    owner = _owner_slabs(s, nranks, by)
     deg = (s.nl_end - s.nl_start + 1).astype(np.int64)
     src = np.repeat(np.arange(n), deg)                    # bond -> atom
     nbr = s.nl.astype(np.int64)
@@ -205,6 +210,7 @@ class ShardedSimulation:
         self.plan = plan
         self.local = local_system(s, plan)
         self.sim = vgpu.Simulation(self.local, device=device, precision=precision, noise_seed=noise_seed)
+        # non-contiguous shares draw their own (statistically equivalent) noise
         self.sim.set_owned(plan.n_owned, plan.noise_base if plan.noise_base is not None else 0)
         self.dtype = torch.float64 if precision == "fp64" else torch.float32
         self.device = torch.device("cuda", device)
