@@ -220,9 +220,11 @@ def reference_arm(args, rank, world):
     from oracle import cpu_baseline as B
     cfg = workload_config(args.L, args.gpus)
     procs = os.cpu_count() or 1
-    steps = max(10, min(args.steps, 100))
+    # each step: one Heun step of an FCC 20^3 sample (32,000 spins) in every
+    # process; W untimed steps, then exactly K timed ones
+    steps, warmup = args.steps, args.warmup
     try:
-        r = B.reference_rate(L=20, steps=steps, procs=procs)
+        r = B.reference_rate(L=20, steps=steps, procs=procs, warmup=warmup)
     except Exception as e:  # binary absent: fall back to the restatement
         try:
             r = B.port_rate(L=16, steps=20)
@@ -230,7 +232,7 @@ def reference_arm(args, rank, world):
             print(json.dumps({"impl": "reference", "unavailable": f"{e}; {e2}"}))
             return
     line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 0, "steps": steps,
-            "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "warmup": warmup, "ms_per_step": r.get("ms_per_step"), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg, "impl": "reference",
             "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
                              "sample": r["sample"]},

@@ -26,13 +26,14 @@ from . import oracle as O
 from .refinputs import fcc_input, fcc_mat
 
 
-def _one_reference(L: int, steps: int, T: float) -> tuple:
+def _one_reference(L: int, steps: int, T: float, warmup: int = 0) -> tuple:
     tmp = tempfile.mkdtemp(prefix="vref_bench_")
     Path(tmp, "input").write_text(fcc_input(L, T=T))
     Path(tmp, "m.mat").write_text(fcc_mat())
     out = Path(tmp, "out")
     out.mkdir()
-    r = subprocess.run([str(O.HARNESS), "--out", str(out), "--steps", str(steps), "--time"], cwd=tmp,
+    r = subprocess.run([str(O.HARNESS), "--out", str(out), "--steps", str(steps), "--warmup", str(warmup), "--time"],
+                       cwd=tmp,
                        capture_output=True, text=True, timeout=1800)
     if r.returncode != 0:
         raise RuntimeError(f"reference harness failed: {r.stdout[-500:]} {r.stderr[-500:]}")
@@ -43,22 +44,22 @@ def _one_reference(L: int, steps: int, T: float) -> tuple:
     raise RuntimeError("harness printed no loop time")
 
 
-def reference_rate(L: int = 20, steps: int = 100, procs: int = 0, T: float = 300.0) -> dict:
+def reference_rate(L: int = 20, steps: int = 100, procs: int = 0, T: float = 300.0, warmup: int = 0) -> dict:
     """Aggregate spin-steps/s of `procs` concurrent reference processes."""
     if not O.harness_available():
         raise FileNotFoundError("oracle/_ref/vampire-harness not built")
     procs = procs or (os.cpu_count() or 1)
     wall0 = time.time()
     with ThreadPoolExecutor(procs) as ex:
-        res = list(ex.map(lambda _: _one_reference(L, steps, T), range(procs)))
+        res = list(ex.map(lambda _: _one_reference(L, steps, T, warmup), range(procs)))
     loop = max(r[0] for r in res)
     atoms = res[0][1]
     total = sum(r[1] * r[2] for r in res)
     return {"value": total / loop, "unit": "spin-steps/s", "cores": procs, "kind": "reference",
             "sample": f"{procs} x reference vampire LLG-Heun (sim::LLG_Heun), FCC {L}^3 periodic "
-                      f"({atoms} spins), A/B alloy, tensor exchange + DMI + cubic, T={T:g} K, {steps} steps "
+                      f"({atoms} spins), A/B alloy, tensor exchange + DMI + cubic, T={T:g} K, {warmup} untimed + {steps} timed steps "
                       f"each; step-loop time of the slowest process",
-            "wall_s": time.time() - wall0}
+            "wall_s": time.time() - wall0, "ms_per_step": loop / steps * 1e3}
 
 
 def port_rate(L: int = 20, steps: int = 50, T: float = 300.0) -> dict:

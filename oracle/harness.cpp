@@ -204,7 +204,7 @@ static void dump_dipole(const std::string& tag) {
 }
 
 int main(int argc, char* argv[]) {
-   long steps = 0, noise = 0, mag_every = 0, mag_start = 0;
+   long steps = 0, warmup = 0, noise = 0, mag_every = 0, mag_start = 0;
    std::vector<long> snaps, stat_snaps;
    bool want_system = false, want_dipole = false, want_time = false;
    for (int i = 1; i < argc; i++) {
@@ -216,6 +216,7 @@ int main(int argc, char* argv[]) {
       if (a == "--out") g_out = next();
       else if (a == "--system") want_system = true;
       else if (a == "--steps") steps = atol(next());
+      else if (a == "--warmup") warmup = atol(next());
       else if (a == "--snaps") snaps = parse_list(next());
       else if (a == "--noise") noise = atol(next());
       else if (a == "--stats") stat_snaps = parse_list(next());
@@ -265,6 +266,15 @@ int main(int argc, char* argv[]) {
 
    const int n = atoms::num_atoms;
    std::vector<double> mag_trace;  // per recorded step: mx, my, mz, |m| (system mask, bin 0), total E
+   // untimed warm-up steps (timing runs only; nothing is dumped for them)
+   for (long w = 0; w < warmup; w++) {
+      if (sim::integrator == 1)
+         montecarlo::mc_step(atoms::x_spin_array, atoms::y_spin_array, atoms::z_spin_array,
+                             atoms::num_atoms, atoms::type_array);
+      else
+         sim::LLG_Heun();
+      sim::increment_time();
+   }
    const auto t0 = std::chrono::steady_clock::now();
    for (long step = 1; step <= steps; step++) {
       if (step <= noise) {
