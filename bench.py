@@ -191,27 +191,62 @@ def b_stream(b):
     return p.value
 
 
-def bench_mc(device, L=50, sweeps=500):
-    """Checkerboard Metropolis sweep rate on SC 50^3 (125,000 spins), 300 K."""
+def _tc_fit(T, m):
+    """Curie temperature from <|m|>(T) ~ a (1 - T/Tc)^b (points with m > 0.3)."""
+    import numpy as np
+    from scipy.optimize import curve_fit
+    sel = (m > 0.3) & (T > 0)
+    f = lambda t, tc, b, a: a * np.clip(1 - t / tc, 1e-12, None) ** b
+    p, _ = curve_fit(f, T[sel], m[sel], p0=(1.05 * T[sel].max(), 0.35, 1.0), maxfev=20000)
+    return float(p[0])
+
+
+def bench_mc(device, L=50, eq=5000, av=10000, every=10):
+    """The Curie-sweep protocol on SC 50^3 (125,000 spins, J, Ku and mu_s of
+    the SC ferromagnet, H = 0): 31 temperatures 0..1500 K as replicas of one
+    handle (3,875,000 spins), checkerboard Metropolis with angle moves,
+    `eq` equilibration then `av` averaging sweeps, device-side running means
+    of <|m|> per replica every `every` sweeps.  Timed with CUDA events over
+    the whole protocol (sweeps and statistics)."""
+    import numpy as np
     import torch
     from vampire_b200 import system as S
     from vampire_b200 import vgpu
-    s = S.config_sc_llg(L, temperature=300.0)
-    s.params.H_applied = 0.0
-    with vgpu.Simulation(s, device=device) as sim:
+    base = S.config_sc_llg(L, temperature=0.0)
+    base.params.H_applied = 0.0
+    base.spins = np.tile(np.array([[0.0], [0.0], [1.0]]), (1, base.n))
+    Ts = np.arange(0.0, 1501.0, 50.0)
+    s = S.replicas(base, Ts)
+    with vgpu.Simulation(s, device=device, noise_seed=4242) as sim:
+        mid = sim.add_mask(*s.masks["replica"])
         nc = sim.mc_setup()
-        sim.mc_sweep(20)
         stream = torch.cuda.ExternalStream(sim.stream_ptr(), device=device)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         sim.synchronize()
         e0.record(stream)
-        sim.mc_sweep(sweeps)
+        sim.mc_sweep(eq)
         e1.record(stream)
-        e1.synchronize()
-        ms = e0.elapsed_time(e1)
+        sim.stats_reset()
+        for _ in range(av // every):
+            sim.mc_sweep(every)
+            sim.stats_update(magnetization=True)
+        e2.record(stream)
+        e2.synchronize()
+        ms = e0.elapsed_time(e2)
+        ms_eq = e0.elapsed_time(e1)
+        _, mean, cnt = sim.magnetization(mid)
         moves, rej = sim.mc_counters()
-    return {"spins": s.n, "colours": nc, "sweeps": sweeps, "value": s.n * sweeps / (ms * 1e-3),
-            "unit": "spin-moves/s", "acceptance": 1.0 - rej / moves}
+    m_T = mean.reshape(-1, 4)[:, 3] / max(cnt, 1)
+    try:
+        tc = _tc_fit(Ts, m_T)
+    except Exception:
+        tc = None
+    sweeps = eq + (av // every) * every
+    return {"workload": f"SC {L}^3 x {Ts.size} temperatures {Ts[0]:g}-{Ts[-1]:g} K (replicas in one handle), "
+                        f"{eq} + {av} sweeps, <|m|> every {every} sweeps",
+            "spins": s.n, "colours": nc, "sweeps": sweeps, "value": s.n * sweeps / (ms * 1e-3),
+            "unit": "spin-moves/s", "sweep_only_value": s.n * eq / (ms_eq * 1e-3), "protocol_s": ms * 1e-3,
+            "acceptance": 1.0 - rej / moves, "Tc_K": tc, "m_T": [round(float(x), 5) for x in m_T]}
 
 
 def reference_arm(args, rank, world):

@@ -56,3 +56,22 @@ def test_sc_neighbours_match_reference():
     np.testing.assert_allclose(mine.materials[0]["ku2"], s.materials[0]["ku2"], rtol=1e-15)
     np.testing.assert_allclose(mine.materials[0]["H_th_sigma"], s.materials[0]["H_th_sigma"], rtol=1e-15)
     np.testing.assert_allclose(mine.materials[0]["one_oneplusalpha_sq"], s.materials[0]["one_oneplusalpha_sq"])
+
+
+def test_temperature_replicas_are_disjoint_copies():
+    from vampire_b200 import system as S
+    base = S.config_sc_llg(4, temperature=0.0)
+    Ts = [0.0, 300.0, 900.0]
+    r = S.replicas(base, Ts)
+    n, k = base.n, len(Ts)
+    assert r.n == k * n and r.num_bonds == k * base.num_bonds
+    assert r.params.local_temperature and not base.params.local_temperature
+    for c in range(k):
+        lo, hi = c * n, (c + 1) * n
+        nl = r.nl[r.nl_start[lo]:r.nl_end[hi - 1] + 1]
+        assert nl.min() >= lo and nl.max() < hi                     # no bond leaves its copy
+        assert np.array_equal(nl - lo, base.nl)
+        assert np.all(r.type[lo:hi] == base.type + c * base.num_materials)
+        assert np.all(r.materials["temperature"][r.type[lo:hi]] == Ts[c])
+        assert np.all(r.masks["replica"][0][lo:hi] == c)
+    np.testing.assert_array_equal(r.spins[:, n:2 * n], base.spins)

@@ -17,6 +17,7 @@ reference's three-site DMI construction (src/exchange/dmi.cpp:46-221).
 """
 from __future__ import annotations
 
+import dataclasses
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
@@ -402,6 +403,39 @@ def dipole_cells(s: SpinSystem, size: float, atomic_volume: float, solver: str =
                "cell_natoms": natoms, "macro_cell_size": size, "cutoff": cutoff, "update_rate": update_rate,
                "solver": solver, "coords": s.coords}
     return s.cells
+
+
+def replicas(s: SpinSystem, temperatures: Sequence[float]) -> SpinSystem:
+    """len(temperatures) independent copies of `s` in one system (temperature
+    replicas): copy k uses materials k*M..k*M+M-1, identical to s's except for
+    their temperature, and local temperatures are switched on.  Masks:
+    "replica" (bin k) and "material" (bin k*M+m)."""
+    k = len(temperatures)
+    M = s.num_materials
+    if k * M > 100:
+        raise ValueError("at most 100 materials (replicas x materials) per handle")
+    n, nb = s.n, s.num_bonds
+    mats = np.concatenate([s.materials.copy() for _ in range(k)])
+    for r, T in enumerate(temperatures):
+        mats["temperature"][r * M:(r + 1) * M] = T
+    off = np.repeat(np.arange(k, dtype=np.int64) * n, n)
+    boff = np.repeat(np.arange(k, dtype=np.int64) * nb, n)
+    st = (np.tile(s.nl_start.astype(np.int64), k) + boff).astype(np.int32)
+    en = (np.tile(s.nl_end.astype(np.int64), k) + boff).astype(np.int32)
+    nl = (np.tile(s.nl.astype(np.int64), k) + np.repeat(np.arange(k, dtype=np.int64) * n, nb)).astype(np.int32)
+    if s.nl_type is not None:
+        nl_type, jl = np.tile(s.nl_type, k), s.jlist
+    else:
+        nl_type, jl = None, np.tile(s.jlist, k)
+    typ = (np.tile(s.type, k) + np.repeat(np.arange(k) * M, n)).astype(np.int32)
+    p = dataclasses.replace(s.params, local_temperature=True)
+    out = SpinSystem(n=k * n, nl_start=st, nl_end=en, nl=nl, jlist=jl, exch_type=s.exch_type, type=typ,
+                     materials=mats, spins=np.tile(s.spins, (1, k)), params=p, uniaxial=s.uniaxial, cubic=s.cubic,
+                     nl_type=nl_type, coords=None)
+    out.masks["system"] = (np.zeros(k * n, dtype=np.int32), 1)
+    out.masks["replica"] = ((off // n).astype(np.int32), k)
+    out.masks["material"] = (typ.copy(), k * M)
+    return out
 
 
 # ----------------------------------------------------------------------------
