@@ -136,6 +136,32 @@ const char* vgpu_version(void);
  * materials and topology (src/cuda/initialize.cu:398-515). */
 int vgpu_upload_system(vgpu_handle h, const vgpu_system_desc* desc);
 
+/* Higher-order anisotropy beyond the descriptor's second-order uniaxial and
+ * fourth-order cubic terms, as the reference's anisotropy module evaluates
+ * them (src/anisotropy/fields.cpp:42-63, energy.cpp:27-36):
+ * uniaxial_fourth_order.cpp, uniaxial_sixth_order.cpp (along the material's
+ * ku_vector), cubic_fourth_order_rotation.cpp (kc4 of vgpu_material in the
+ * basis e1, e2, e3; replaces the plain cubic term, so cubic_enabled = 0),
+ * cubic_sixth_order.cpp and neel.cpp (per-atom surface tensors built by
+ * initialize_neel.cpp).  Constants are the reduced ones of
+ * anisotropy::internal (K / mu_s, Tesla).  Call after vgpu_upload_system;
+ * a new upload clears them.  Replaces the part of vcuda::initialize that
+ * never reached the device (src/cuda/spin_fields.cu:95-152 has no such terms). */
+typedef struct {
+   int32_t uniaxial_fourth;        /* enable_uniaxial_fourth_order                      */
+   int32_t uniaxial_sixth;         /* enable_uniaxial_sixth_order                       */
+   int32_t cubic_sixth;            /* enable_cubic_sixth_order                          */
+   int32_t cubic_rotation;         /* enable_cubic_fourth_order_rotation                */
+   int32_t neel;                   /* enable_neel_anisotropy                            */
+   int32_t pad_;
+   const double* ku4;              /* [num_materials] or NULL when off                  */
+   const double* ku6;              /* [num_materials] or NULL when off                  */
+   const double* kc6;              /* [num_materials] or NULL when off                  */
+   const double* kc_basis;         /* [num_materials][9] e1, e2, e3 (unit, orthogonal)  */
+   const double* neel_tensor;      /* [num_atoms][9] row-major 3x3 [T], or NULL         */
+} vgpu_anisotropy_ext;
+int vgpu_set_anisotropy_ext(vgpu_handle h, const vgpu_anisotropy_ext* a);
+
 /* Host-only check of a descriptor (no device needed): CSR rows inside
  * [0, num_bonds), neighbours and interaction ids in range, materials in
  * range, finite spins.  VGPU_ERR_ARG / VGPU_ERR_NAN with a message for

@@ -146,6 +146,26 @@ static void dump_system() {
       mat.insert(mat.end(), row, row + 16);
    }
    dumpd("materials", mat);
+   // higher-order anisotropy: flags, per-material reduced constants [T] and the
+   // normalised cubic basis, and the per-atom Neel tensors (anisotropy/internal.hpp)
+   {
+      namespace ai = anisotropy::internal;
+      std::vector<int> fl = {(int)ai::enable_uniaxial_fourth_order, (int)ai::enable_uniaxial_sixth_order,
+                             (int)ai::enable_cubic_sixth_order, (int)ai::enable_cubic_fourth_order_rotation,
+                             (int)ai::enable_neel_anisotropy};
+      dumpi("aniso_flags", fl);
+      std::vector<double> ext;
+      for (int m = 0; m < mp::num_materials; m++) {
+         ext.push_back(ai::enable_uniaxial_fourth_order ? ai::ku4[m] : 0.0);
+         ext.push_back(ai::enable_uniaxial_sixth_order ? ai::ku6[m] : 0.0);
+         ext.push_back(ai::enable_cubic_sixth_order ? ai::kc6[m] : 0.0);
+         for (int k = 0; k < 3; k++) ext.push_back(ai::mp[m].kc_vector1[k]);
+         for (int k = 0; k < 3; k++) ext.push_back(ai::mp[m].kc_vector2[k]);
+         for (int k = 0; k < 3; k++) ext.push_back(ai::mp[m].kc_vector3[k]);
+      }
+      dumpd("aniso_ext", ext);
+      if (ai::enable_neel_anisotropy) dumpd("neel_tensor", ai::neel_tensor);
+   }
    std::vector<double> simc = {mp::dt, mp::half_dt, mp::dt_SI, mp::gamma_SI, sim::temperature,
                                sim::H_applied, sim::H_vec[0], sim::H_vec[1], sim::H_vec[2]};
    dumpd("sim", simc);

@@ -43,6 +43,8 @@ class VRefSys(C.Structure):
         ("hdx", _D), ("hdy", _D), ("hdz", _D), ("hmx", _D), ("hmy", _D), ("hmz", _D),
         ("dt", C.c_double), ("half_dt", C.c_double), ("H_applied", C.c_double),
         ("H_vec", C.c_double * 3), ("mus", _D), ("mus_SI", _D),
+        ("u4", C.c_int), ("u6", C.c_int), ("c6", C.c_int), ("crot", C.c_int), ("neel", C.c_int),
+        ("pad2_", C.c_int), ("ku4", _D), ("ku6", _D), ("kc6", _D), ("kcb", _D), ("neelt", _D),
     ]
 
 
@@ -128,6 +130,13 @@ class OracleSystem:
             st.H_vec[k] = hv[k]
         st.mus = _p(arr("mus", m["mu_s_SI"] / 9.27400915e-24, np.float64), _D)
         st.mus_SI = _p(arr("mus_SI", m["mu_s_SI"], np.float64), _D)
+        a = getattr(s, "aniso", None)
+        if a is not None:
+            st.u4, st.u6, st.c6, st.crot, st.neel = (int(a["u4"]), int(a["u6"]), int(a["c6"]), int(a["crot"]),
+                                                     int(a["neel"]))
+            for key, f in (("ku4", "ku4"), ("ku6", "ku6"), ("kc6", "kc6"), ("kcb", "kcb"), ("neel_tensor", "neelt")):
+                if a.get(key) is not None:
+                    setattr(st, f, _p(arr(key, a[key], np.float64), _D))
         self.st = st
         self.keep = keep
 
@@ -312,6 +321,13 @@ def system_from_dump(d: dict, params=None):
     nt = d["nl_type"].astype(np.int32)
     if not np.array_equal(nt, np.arange(nt.size, dtype=np.int32)):
         s.nl_type = nt
+    if "aniso_flags" in d and int(np.sum(d["aniso_flags"])) > 0:
+        fl = [bool(x) for x in d["aniso_flags"]]
+        ext = d["aniso_ext"].reshape(nmat, 12)
+        s.aniso = {"u4": fl[0], "u6": fl[1], "c6": fl[2], "crot": fl[3], "neel": fl[4],
+                   "ku4": ext[:, 0].copy(), "ku6": ext[:, 1].copy(), "kc6": ext[:, 2].copy(),
+                   "kcb": ext[:, 3:12].copy(),
+                   "neel_tensor": d["neel_tensor"].reshape(n, 9).copy() if fl[4] else None}
     if "mask_system" in d:
         s.masks["system"] = (d["mask_system"].astype(np.int32), int(d["sat_system"].size))
         s.masks["material"] = (d["mask_material"].astype(np.int32), int(d["sat_material"].size))

@@ -75,6 +75,33 @@ void vref_spin_fields(const vref_sys* s, const double* sx, const double* sy, con
          hz[atom] += ez * k2;
       }
    }
+   if (s->u4) {  /* uniaxial_fourth_order.cpp: H += (2/3)(1/8) ku4 (140 (s.e)^3 - 60 s.e) e */
+      const double scale = 1.0 / 8.0 * 2.0 / 3.0;
+      for (int atom = 0; atom < s->n; atom++) {
+         const int mat = s->type[atom];
+         const double ex = s->kux[mat], ey = s->kuy[mat], ez = s->kuz[mat];
+         const double sdote = (sx[atom] * ex + sy[atom] * ey + sz[atom] * ez);
+         const double sdote3 = sdote * sdote * sdote;
+         const double k4 = scale * s->ku4[mat] * (140.0 * sdote3 - 60.0 * sdote);
+         hx[atom] += ex * k4;
+         hy[atom] += ey * k4;
+         hz[atom] += ez * k4;
+      }
+   }
+   if (s->u6) {  /* uniaxial_sixth_order.cpp: (2/3)(1/16) ku6 (1386 (s.e)^5 - 1260 (s.e)^3 + 210 s.e) e */
+      const double scale = 1.0 / 16.0 * 2.0 / 3.0;
+      for (int atom = 0; atom < s->n; atom++) {
+         const int mat = s->type[atom];
+         const double ex = s->kux[mat], ey = s->kuy[mat], ez = s->kuz[mat];
+         const double sdote = (sx[atom] * ex + sy[atom] * ey + sz[atom] * ez);
+         const double sdote3 = sdote * sdote * sdote;
+         const double sdote5 = sdote3 * sdote * sdote;
+         const double k6 = scale * s->ku6[mat] * (1386.0 * sdote5 - 1260.0 * sdote3 + 210.0 * sdote);
+         hx[atom] += ex * k6;
+         hy[atom] += ey * k6;
+         hz[atom] += ez * k6;
+      }
+   }
    if (s->cubic) {
       for (int atom = 0; atom < s->n; atom++) {
          const int mat = s->type[atom];
@@ -83,6 +110,41 @@ void vref_spin_fields(const vref_sys* s, const double* sx, const double* sy, con
          hx[atom] += x * x * x * k4;
          hy[atom] += y * y * y * k4;
          hz[atom] += z * z * z * k4;
+      }
+   }
+   if (s->crot) {  /* cubic_fourth_order_rotation.cpp: 2 kc4 sum_k (s.e_k)^3 e_k */
+      for (int atom = 0; atom < s->n; atom++) {
+         const int mat = s->type[atom];
+         const double* e = s->kcb + 9 * mat;
+         const double k4 = 0.5 * 4.0 * s->kc4[mat];
+         const double x = sx[atom], y = sy[atom], z = sz[atom];
+         const double d1 = x * e[0] + y * e[1] + z * e[2];
+         const double d2 = x * e[3] + y * e[4] + z * e[5];
+         const double d3 = x * e[6] + y * e[7] + z * e[8];
+         const double d13 = d1 * d1 * d1, d23 = d2 * d2 * d2, d33 = d3 * d3 * d3;
+         hx[atom] += k4 * (d13 * e[0] + d23 * e[3] + d33 * e[6]);
+         hy[atom] += k4 * (d13 * e[1] + d23 * e[4] + d33 * e[7]);
+         hz[atom] += k4 * (d13 * e[2] + d23 * e[5] + d33 * e[8]);
+      }
+   }
+   if (s->c6) {  /* cubic_sixth_order.cpp: H_x += -2 kc6 s_x s_y^2 s_z^2 (cyclic) */
+      for (int atom = 0; atom < s->n; atom++) {
+         const int mat = s->type[atom];
+         const double k6 = -2.0 * s->kc6[mat];
+         const double x = sx[atom], y = sy[atom], z = sz[atom];
+         const double x2 = x * x, y2 = y * y, z2 = z * z;
+         hx[atom] += x * y2 * z2 * k6;
+         hy[atom] += y * z2 * x2 * k6;
+         hz[atom] += z * x2 * y2 * k6;
+      }
+   }
+   if (s->neel && s->neelt) {  /* neel.cpp: H += 2 T s, per-atom tensor */
+      for (int atom = 0; atom < s->n; atom++) {
+         const double* t = s->neelt + 9 * (int64_t)atom;
+         const double x = sx[atom], y = sy[atom], z = sz[atom];
+         hx[atom] += 2.0 * (t[0] * x + t[1] * y + t[2] * z);
+         hy[atom] += 2.0 * (t[3] * x + t[4] * y + t[5] * z);
+         hz[atom] += 2.0 * (t[6] * x + t[7] * y + t[8] * z);
       }
    }
 }
@@ -231,9 +293,34 @@ void vref_spin_energy(const vref_sys* s, const double* sx, const double* sy, con
       const double sdote = Sx * s->kux[m] + Sy * s->kuy[m] + Sz * s->kuz[m];
       an += -s->ku2[m] * (sdote * sdote);
    }
+   if (s->u4) {  /* uniaxial_fourth_order.cpp energy (the reference's literal 1/12) */
+      const double sdote = Sx * s->kux[m] + Sy * s->kuy[m] + Sz * s->kuz[m];
+      const double sdote2 = sdote * sdote;
+      an += -0.08333333333 * s->ku4[m] * (35.0 * sdote2 * sdote2 - 30.0 * sdote2);
+   }
+   if (s->u6) {  /* uniaxial_sixth_order.cpp energy (literal 1/24) */
+      const double sdote = Sx * s->kux[m] + Sy * s->kuy[m] + Sz * s->kuz[m];
+      const double sdote2 = sdote * sdote;
+      an += -0.04166666666 * s->ku6[m] * (231.0 * sdote2 * sdote2 * sdote2 - 315.0 * sdote2 * sdote2 + 105.0 * sdote2);
+   }
    if (s->cubic) {
       const double sx4 = Sx * Sx * Sx * Sx, sy4 = Sy * Sy * Sy * Sy, sz4 = Sz * Sz * Sz * Sz;
       an += -0.5 * s->kc4[m] * (sx4 + sy4 + sz4);
+   }
+   if (s->crot) {
+      const double* e = s->kcb + 9 * m;
+      const double d1 = Sx * e[0] + Sy * e[1] + Sz * e[2];
+      const double d2 = Sx * e[3] + Sy * e[4] + Sz * e[5];
+      const double d3 = Sx * e[6] + Sy * e[7] + Sz * e[8];
+      const double x4 = d1 * d1 * d1 * d1, y4 = d2 * d2 * d2 * d2, z4 = d3 * d3 * d3 * d3;
+      an += -0.5 * s->kc4[m] * (x4 + y4 + z4);
+   }
+   if (s->c6) an += s->kc6[m] * Sx * Sx * Sy * Sy * Sz * Sz;
+   if (s->neel && s->neelt) {
+      const double* t = s->neelt + 9 * (int64_t)atom;
+      const double en = (Sx * t[0] * Sx + Sx * t[1] * Sy + Sx * t[2] * Sz + Sy * t[3] * Sx + Sy * t[4] * Sy +
+                         Sy * t[5] * Sz + Sz * t[6] * Sx + Sz * t[7] * Sy + Sz * t[8] * Sz);
+      an += -1.0 * en;
    }
    e[0] = ex;
    e[1] = an;

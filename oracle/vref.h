@@ -40,6 +40,14 @@ typedef struct {
    double H_vec[3];
    const double* mus;     /* per material moment in mu_B (adjoint loss weights) */
    const double* mus_SI;  /* per material moment in J/T */
+   /* higher-order anisotropy (src/anisotropy/internal.hpp) */
+   int u4, u6, c6, crot, neel, pad2_;  /* enable_uniaxial_fourth/sixth_order, cubic_sixth_order,
+                                         cubic_fourth_order_rotation, neel_anisotropy */
+   const double* ku4;     /* per material reduced constants [T] */
+   const double* ku6;
+   const double* kc6;
+   const double* kcb;     /* per material rotated cubic basis e1, e2, e3 (9 doubles) */
+   const double* neelt;   /* per atom 3x3 Neel tensor (9 doubles), or NULL */
 } vref_sys;
 
 void vref_spin_fields(const vref_sys* s, const double* sx, const double* sy, const double* sz,

@@ -25,7 +25,8 @@ from oracle.refinputs import SC_MAT, fcc_input, fcc_mat, sc_input  # noqa: E402
 
 
 SYSTEM_KEYS = ["meta", "nl_start", "nl_end", "nl", "nl_type", "type", "m_spin", "cx", "cy", "cz", "jlist",
-               "materials", "sim", "mask_system", "sat_system", "mask_material", "sat_material"]
+               "materials", "sim", "mask_system", "sat_system", "mask_material", "sat_material",
+               "aniso_flags", "aniso_ext", "neel_tensor"]
 
 
 def save(name: str, d: dict, keep: list) -> None:
@@ -106,6 +107,54 @@ def single_spin_applied():
     save("single_spin_applied", d, keep)
 
 
+HO_MAT = """material:num-materials=1
+material[1]:material-name=A
+material[1]:damping-constant=0.1
+material[1]:exchange-matrix[1]=11.2e-21
+material[1]:atomic-spin-moment=1.72 !muB
+material[1]:second-order-uniaxial-anisotropy-constant=6.69e-24
+material[1]:fourth-order-uniaxial-anisotropy-constant=2.0e-24
+material[1]:sixth-order-uniaxial-anisotropy-constant=1.0e-24
+material[1]:fourth-order-cubic-anisotropy-constant=1.0e-24
+material[1]:sixth-order-cubic-anisotropy-constant=3.0e-24
+material[1]:uniaxial-anisotropy-direction=0,0.6,0.8
+material[1]:initial-spin-direction=random
+"""
+
+
+def sc6_aniso_ho():
+    """SC 6^3, open boundaries, T=0: second-, fourth- and sixth-order uniaxial
+    anisotropy along (0, 0.6, 0.8) plus fourth- and sixth-order cubic
+    anisotropy; 200 reference steps and energies."""
+    d = O.run_harness(sc_input(6, periodic=False), {"m.mat": HO_MAT},
+                      ["--system", "--steps", 200, "--snaps", "1,200", "--stats", "0,200"])
+    keep = [f"s{c}_{t}" for t in (0, 1, 200) for c in "xyz"]
+    keep += ["mag_system_0", "energy_system_0", "energy_material_0", "mag_system_200", "energy_system_200"]
+    save("sc6_aniso_ho", d, keep)
+
+
+def fcc4_neel_rot():
+    """FCC 4^3 cube, open boundaries: rotated cubic anisotropy (axes [110],
+    [-110], [001]) and Neel surface anisotropy on atoms with fewer than 12
+    neighbours; T=0, 100 reference steps and energies."""
+    a, L = 3.54, 4
+    size = L * a / 10.0
+    inp = (f"create:crystal-structure=fcc\ndimensions:unit-cell-size={a} !A\n"
+           f"dimensions:system-size-x={size} !nm\ndimensions:system-size-y={size} !nm\n"
+           f"dimensions:system-size-z={size} !nm\nmaterial:file=m.mat\nsim:temperature=0.0\n"
+           f"sim:time-step=1.0E-16\nsim:program=time-series\nsim:integrator=llg-heun\n"
+           f"anisotropy:surface-anisotropy-threshold=12\n")
+    mat = ("material:num-materials=1\nmaterial[1]:material-name=A\nmaterial[1]:damping-constant=0.1\n"
+           "material[1]:exchange-matrix[1]=11.2e-21\nmaterial[1]:atomic-spin-moment=1.72 !muB\n"
+           "material[1]:fourth-order-cubic-anisotropy-constant=1.0e-24\n"
+           "material[1]:cubic-anisotropy-direction-1=1,1,0\nmaterial[1]:cubic-anisotropy-direction-2=-1,1,0\n"
+           "material[1]:neel-anisotropy-constant[1]=5.0e-23\nmaterial[1]:initial-spin-direction=random\n")
+    d = O.run_harness(inp, {"m.mat": mat}, ["--system", "--steps", 100, "--snaps", "1,100", "--stats", "0,100"])
+    keep = [f"s{c}_{t}" for t in (0, 1, 100) for c in "xyz"]
+    keep += ["mag_system_0", "energy_system_0", "energy_material_0", "mag_system_100", "energy_system_100"]
+    save("fcc4_neel_rot", d, keep)
+
+
 DIPOLE_KEYS = ["cell_id", "cell_natoms", "cell_volume", "cell_pos_mom"]
 
 
@@ -177,7 +226,7 @@ def mc_sc16_curie():
 
 
 ALL = [sc20_t0, sc8_t0, sc10_t300, sc6_open_t300, fcc4_dmi_t300, fcc4_dmi_t0, single_spin_applied, mc_sc16_curie,
-       fcc10_dipole_tensor, fcc10_dipole_macrocell]
+       fcc10_dipole_tensor, fcc10_dipole_macrocell, sc6_aniso_ho, fcc4_neel_rot]
 
 if __name__ == "__main__":
     names = sys.argv[1:]

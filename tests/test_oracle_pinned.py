@@ -91,3 +91,35 @@ def test_oracle_detects_a_planted_error():
     bad.jlist[7] *= 1.001
     got = O.OracleSystem(bad).llg_heun(bad.spins, 10)
     assert np.abs(got - ref_spins(d, 10)).max() > 1e-9
+
+
+@pytest.mark.parametrize("name,steps", [("sc6_aniso_ho", (1, 200)), ("fcc4_neel_rot", (1, 100))])
+def test_higher_order_anisotropy(name, steps):
+    """Fourth/sixth-order uniaxial, sixth-order cubic, rotated cubic and Neel
+    surface anisotropy (src/anisotropy/*.cpp): the oracle follows the
+    reference trajectory and reproduces its anisotropy energies."""
+    s, d = load_golden(name)
+    assert s.aniso is not None
+    o = O.OracleSystem(s)
+    got = s.spins
+    done = 0
+    for t in steps:
+        got = o.llg_heun(got, t - done)
+        done = t
+        assert np.abs(got - ref_spins(d, t)).max() < 1e-12, t
+    for t in (0, steps[-1]):
+        sp = ref_spins(d, t)
+        mask, size = s.masks["system"]
+        np.testing.assert_allclose(o.energy(sp, mask, size), d[f"energy_system_{t}"], rtol=1e-11, atol=1e-9)
+
+
+def test_higher_order_anisotropy_pins_each_term():
+    """Each higher-order term matters at the fixture's tolerance: dropping any
+    one of them moves the 200-step trajectory off the reference."""
+    s, d = load_golden("sc6_aniso_ho")
+    for key in ("u4", "u6", "c6"):
+        bad = s.copy()
+        bad.aniso = dict(s.aniso)
+        bad.aniso[key] = False
+        got = O.OracleSystem(bad).llg_heun(bad.spins, 200)
+        assert np.abs(got - ref_spins(d, 200)).max() > 1e-9, key

@@ -187,16 +187,32 @@ __device__ __forceinline__ void exchange_field(const LLGArgs<R>& a, int i, int m
 
 // spin-dependent field of atom i at spin S: exchange + anisotropy
 // (calculate_spin_fields, src/simulate/fields.cpp:67-118)
-template <typename R, int FMT, int LOAD = 0, bool STAGED = false>
+// EXT = false compiles the passes without the higher-order anisotropy terms
+// (register budget of the common case); launchers pick EXT from a.aniso_ext.
+template <typename R, int FMT, int LOAD = 0, bool STAGED = false, bool EXT = true>
 __device__ __forceinline__ void spin_field(const LLGArgs<R>& a, int i, int mi, const MatParams<R>& m,
                                            const R* sx, const R* sy, const R* sz, const R S[3], R H[3],
                                            const int4* srec_tile = nullptr, int tile_off = 0) {
    R hx = 0, hy = 0, hz = 0;
    exchange_field<R, FMT, LOAD, STAGED>(a, i, mi, sx, sy, sz, hx, hy, hz, srec_tile, tile_off);
+   // anisotropy terms in the order of anisotropy::fields (src/anisotropy/fields.cpp:42-63)
    if (a.uniaxial) {
       const R sdote = S[0] * m.kux + S[1] * m.kuy + S[2] * m.kuz;
       const R k2 = (R)2 * m.ku2 * sdote;
       hx += m.kux * k2; hy += m.kuy * k2; hz += m.kuz * k2;
+   }
+   if (EXT && (a.aniso_ext & (ANI_U4 | ANI_U6))) {
+      const R sdote = S[0] * m.kux + S[1] * m.kuy + S[2] * m.kuz;
+      const R sdote3 = sdote * sdote * sdote;
+      if (a.aniso_ext & ANI_U4) {  // uniaxial_fourth_order.cpp: (2/3)(1/8) ku4 (140 (s.e)^3 - 60 s.e) e
+         const R k4 = (R)(1.0 / 8.0 * 2.0 / 3.0) * m.ku4 * ((R)140 * sdote3 - (R)60 * sdote);
+         hx += m.kux * k4; hy += m.kuy * k4; hz += m.kuz * k4;
+      }
+      if (a.aniso_ext & ANI_U6) {  // uniaxial_sixth_order.cpp: (2/3)(1/16) ku6 (1386 s^5 - 1260 s^3 + 210 s) e
+         const R sdote5 = sdote3 * sdote * sdote;
+         const R k6 = (R)(1.0 / 16.0 * 2.0 / 3.0) * m.ku6 * ((R)1386 * sdote5 - (R)1260 * sdote3 + (R)210 * sdote);
+         hx += m.kux * k6; hy += m.kuy * k6; hz += m.kuz * k6;
+      }
    }
    if (a.cubic) {
       const R k4 = (R)2 * m.kc4;
@@ -204,7 +220,89 @@ __device__ __forceinline__ void spin_field(const LLGArgs<R>& a, int i, int mi, c
       hy += S[1] * S[1] * S[1] * k4;
       hz += S[2] * S[2] * S[2] * k4;
    }
+   if (EXT && (a.aniso_ext & (ANI_CROT | ANI_C6 | ANI_NEEL))) {
+      if (a.aniso_ext & ANI_CROT) {  // cubic_fourth_order_rotation.cpp: 2 kc4 sum_k (s.e_k)^3 e_k
+         const R* e = m.kcb;
+         const R k4 = (R)2 * m.kc4;
+         const R d1 = S[0] * e[0] + S[1] * e[1] + S[2] * e[2];
+         const R d2 = S[0] * e[3] + S[1] * e[4] + S[2] * e[5];
+         const R d3 = S[0] * e[6] + S[1] * e[7] + S[2] * e[8];
+         const R d13 = d1 * d1 * d1, d23 = d2 * d2 * d2, d33 = d3 * d3 * d3;
+         hx += k4 * (d13 * e[0] + d23 * e[3] + d33 * e[6]);
+         hy += k4 * (d13 * e[1] + d23 * e[4] + d33 * e[7]);
+         hz += k4 * (d13 * e[2] + d23 * e[5] + d33 * e[8]);
+      }
+      if (a.aniso_ext & ANI_C6) {  // cubic_sixth_order.cpp: H_x = -2 kc6 s_x s_y^2 s_z^2 (cyclic)
+         const R k6 = (R)(-2) * m.kc6;
+         const R x2 = S[0] * S[0], y2 = S[1] * S[1], z2 = S[2] * S[2];
+         hx += S[0] * y2 * z2 * k6;
+         hy += S[1] * z2 * x2 * k6;
+         hz += S[2] * x2 * y2 * k6;
+      }
+      if (a.aniso_ext & ANI_NEEL) {  // neel.cpp: H += 2 T s with the atom's surface tensor T
+         const size_t st = (size_t)a.n_alloc;
+         const R* t = a.neel + i;
+         const R t0 = __ldg(t), t1 = __ldg(t + st), t2 = __ldg(t + 2 * st), t3 = __ldg(t + 3 * st),
+                 t4 = __ldg(t + 4 * st), t5 = __ldg(t + 5 * st), t6 = __ldg(t + 6 * st), t7 = __ldg(t + 7 * st),
+                 t8 = __ldg(t + 8 * st);
+         hx += (R)2 * (t0 * S[0] + t1 * S[1] + t2 * S[2]);
+         hy += (R)2 * (t3 * S[0] + t4 * S[1] + t5 * S[2]);
+         hz += (R)2 * (t6 * S[0] + t7 * S[1] + t8 * S[2]);
+      }
+   }
    H[0] = hx; H[1] = hy; H[2] = hz;
+}
+
+// anisotropy energy of atom i at spin S in the order of
+// anisotropy::single_spin_energy (src/anisotropy/energy.cpp:27-36), E in T
+// (uniaxial_second_order.cpp, ..._fourth_order.cpp, ..._sixth_order.cpp,
+// cubic_fourth_order.cpp, cubic_fourth_order_rotation.cpp,
+// cubic_sixth_order.cpp, neel.cpp energy functions; the reference's decimal
+// 1/12 and 1/24 literals kept)
+// EXT_ONLY: the higher-order terms alone (callers that add the second-order
+// uniaxial and fourth-order cubic terms themselves).
+template <typename E, typename R, bool EXT_ONLY = false>
+__device__ __forceinline__ E anisotropy_energy(const LLGArgs<R>& a, int i, const MatParams<R>& m, const E S[3]) {
+   E an = 0;
+   const E kux = (E)m.kux, kuy = (E)m.kuy, kuz = (E)m.kuz;
+   if (!EXT_ONLY && a.uniaxial) {
+      const E sd = S[0] * kux + S[1] * kuy + S[2] * kuz;
+      an += -(E)m.ku2 * (sd * sd);
+   }
+   if (a.aniso_ext & ANI_U4) {
+      const E sd = S[0] * kux + S[1] * kuy + S[2] * kuz;
+      const E sd2 = sd * sd;
+      an += (E)(-0.08333333333) * (E)m.ku4 * ((E)35 * sd2 * sd2 - (E)30 * sd2);
+   }
+   if (a.aniso_ext & ANI_U6) {
+      const E sd = S[0] * kux + S[1] * kuy + S[2] * kuz;
+      const E sd2 = sd * sd;
+      an += (E)(-0.04166666666) * (E)m.ku6 * ((E)231 * sd2 * sd2 * sd2 - (E)315 * sd2 * sd2 + (E)105 * sd2);
+   }
+   if (!EXT_ONLY && a.cubic) {
+      const E x4 = S[0] * S[0] * S[0] * S[0], y4 = S[1] * S[1] * S[1] * S[1], z4 = S[2] * S[2] * S[2] * S[2];
+      an += (E)(-0.5) * (E)m.kc4 * (x4 + y4 + z4);
+   }
+   if (a.aniso_ext & ANI_CROT) {
+      const R* e = m.kcb;
+      const E d1 = S[0] * (E)e[0] + S[1] * (E)e[1] + S[2] * (E)e[2];
+      const E d2 = S[0] * (E)e[3] + S[1] * (E)e[4] + S[2] * (E)e[5];
+      const E d3 = S[0] * (E)e[6] + S[1] * (E)e[7] + S[2] * (E)e[8];
+      const E x4 = d1 * d1 * d1 * d1, y4 = d2 * d2 * d2 * d2, z4 = d3 * d3 * d3 * d3;
+      an += (E)(-0.5) * (E)m.kc4 * (x4 + y4 + z4);
+   }
+   if (a.aniso_ext & ANI_C6) an += (E)m.kc6 * S[0] * S[0] * S[1] * S[1] * S[2] * S[2];
+   if (a.aniso_ext & ANI_NEEL) {
+      const size_t st = (size_t)a.n_alloc;
+      const R* t = a.neel + i;
+      const E t0 = (E)__ldg(t), t1 = (E)__ldg(t + st), t2 = (E)__ldg(t + 2 * st), t3 = (E)__ldg(t + 3 * st),
+              t4 = (E)__ldg(t + 4 * st), t5 = (E)__ldg(t + 5 * st), t6 = (E)__ldg(t + 6 * st),
+              t7 = (E)__ldg(t + 7 * st), t8 = (E)__ldg(t + 8 * st);
+      const E en = S[0] * t0 * S[0] + S[0] * t1 * S[1] + S[0] * t2 * S[2] + S[1] * t3 * S[0] + S[1] * t4 * S[1] +
+                   S[1] * t5 * S[2] + S[2] * t6 * S[0] + S[2] * t7 * S[1] + S[2] * t8 * S[2];
+      an += (E)(-1) * en;
+   }
+   return an;
 }
 
 // external field (calculate_external_fields, fields.cpp:120-169)

@@ -69,47 +69,47 @@ __device__ __forceinline__ void llg_correct_finish(const LLGArgs<R>& a, int i, c
 
 // Predictor of atom i: s' = n(s0 + dt f(s0, H)).  LOAD = 1 reads neighbour
 // spins through L2 (they may have been written earlier in the same launch).
-template <typename R, int FMT, int LOAD>
+template <typename R, int FMT, int LOAD, bool EXT = true>
 __device__ __forceinline__ void llg_predict_atom(const LLGArgs<R>& a, int i) {
    const int mi = a.mat ? __ldg(a.mat + i) : 0;
    const MatParams<R> m = a.mp[mi];
    const R S0[3] = {a.ax[i], a.ay[i], a.az[i]};
    R H[3], E[3];
-   spin_field<R, FMT, LOAD>(a, i, mi, m, a.ax, a.ay, a.az, S0, H);
+   spin_field<R, FMT, LOAD, false, EXT>(a, i, mi, m, a.ax, a.ay, a.az, S0, H);
    external_field<R>(a, i, m, true, E);
    H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
    llg_predict_finish<R>(a, i, m, S0, H);
 }
 
 // Corrector of atom i: s1 = n(s0 + dt/2 (f0 + f(s', H'))), written over s0.
-template <typename R, int FMT, int LOAD>
+template <typename R, int FMT, int LOAD, bool EXT = true>
 __device__ __forceinline__ void llg_correct_atom(const LLGArgs<R>& a, int i) {
    const int mi = a.mat ? __ldg(a.mat + i) : 0;
    const MatParams<R> m = a.mp[mi];
    const R S0[3] = {a.ax[i], a.ay[i], a.az[i]};
    const R S1[3] = {a.bx[i], a.by[i], a.bz[i]};
    R H[3], E[3];
-   spin_field<R, FMT, LOAD>(a, i, mi, m, a.bx, a.by, a.bz, S1, H);
+   spin_field<R, FMT, LOAD, false, EXT>(a, i, mi, m, a.bx, a.by, a.bz, S1, H);
    external_field<R>(a, i, m, true, E);
    H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
    llg_correct_finish<R>(a, i, m, S0, S1, H);
 }
 
-template <typename R, int FMT, int MODE>
+template <typename R, int FMT, int MODE, bool EXT>
 __global__ void __launch_bounds__(256) llg_pass_kernel(const LLGArgs<R> a) {
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    if (i >= (MODE == PASS_FIELD ? a.n : a.n_upd)) return;
    if (MODE == PASS_PREDICTOR) {
-      llg_predict_atom<R, FMT, 0>(a, i);
+      llg_predict_atom<R, FMT, 0, EXT>(a, i);
    } else if (MODE == PASS_CORRECTOR) {
-      llg_correct_atom<R, FMT, 0>(a, i);
+      llg_correct_atom<R, FMT, 0, EXT>(a, i);
    } else {
       // field of s0: exchange, anisotropy, applied and dipole terms (no thermal term)
       const int mi = a.mat ? __ldg(a.mat + i) : 0;
       const MatParams<R> m = a.mp[mi];
       const R S0[3] = {a.ax[i], a.ay[i], a.az[i]};
       R H[3], E[3];
-      spin_field<R, FMT>(a, i, mi, m, a.ax, a.ay, a.az, S0, H);
+      spin_field<R, FMT, 0, false, EXT>(a, i, mi, m, a.ax, a.ay, a.az, S0, H);
       external_field<R>(a, i, m, false, E);
       a.fx[i] = H[0] + E[0]; a.fy[i] = H[1] + E[1]; a.fz[i] = H[2] + E[2];
    }
@@ -120,9 +120,15 @@ inline cudaError_t launch_fmt(const LLGArgs<R>& a, int mode, cudaStream_t st) {
    const int bs = 256;
    const int grid = ((mode == PASS_FIELD ? a.n : a.n_upd) + bs - 1) / bs;
    if (grid == 0) return cudaSuccess;
-   if (mode == PASS_PREDICTOR) llg_pass_kernel<R, FMT, PASS_PREDICTOR><<<grid, bs, 0, st>>>(a);
-   else if (mode == PASS_CORRECTOR) llg_pass_kernel<R, FMT, PASS_CORRECTOR><<<grid, bs, 0, st>>>(a);
-   else llg_pass_kernel<R, FMT, PASS_FIELD><<<grid, bs, 0, st>>>(a);
+   if (a.aniso_ext) {
+      if (mode == PASS_PREDICTOR) llg_pass_kernel<R, FMT, PASS_PREDICTOR, true><<<grid, bs, 0, st>>>(a);
+      else if (mode == PASS_CORRECTOR) llg_pass_kernel<R, FMT, PASS_CORRECTOR, true><<<grid, bs, 0, st>>>(a);
+      else llg_pass_kernel<R, FMT, PASS_FIELD, true><<<grid, bs, 0, st>>>(a);
+   } else {
+      if (mode == PASS_PREDICTOR) llg_pass_kernel<R, FMT, PASS_PREDICTOR, false><<<grid, bs, 0, st>>>(a);
+      else if (mode == PASS_CORRECTOR) llg_pass_kernel<R, FMT, PASS_CORRECTOR, false><<<grid, bs, 0, st>>>(a);
+      else llg_pass_kernel<R, FMT, PASS_FIELD, false><<<grid, bs, 0, st>>>(a);
+   }
    return cudaGetLastError();
 }
 

@@ -139,11 +139,11 @@ __global__ void __launch_bounds__(32 * SL) llg_staged_kernel(const LLGArgs<float
       if (act) {
          float H[3];
          if (MODE == PASS_PREDICTOR) {
-            spin_field<float, FMT_DMI_TAB, 0, true>(a, i, mi, m, a.ax, a.ay, a.az, S0, H, sb, tile_off);
+            spin_field<float, FMT_DMI_TAB, 0, true, false>(a, i, mi, m, a.ax, a.ay, a.az, S0, H, sb, tile_off);
             H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
             llg_predict_finish<float>(a, i, m, S0, H);
          } else {
-            spin_field<float, FMT_DMI_TAB, 0, true>(a, i, mi, m, a.bx, a.by, a.bz, S1, H, sb, tile_off);
+            spin_field<float, FMT_DMI_TAB, 0, true, false>(a, i, mi, m, a.bx, a.by, a.bz, S1, H, sb, tile_off);
             H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
             llg_correct_finish<float>(a, i, m, S0, S1, H);
          }

@@ -56,8 +56,8 @@ struct MCArgs {
 };
 
 template <typename R>
-__device__ __forceinline__ R site_energy_delta(const LLGArgs<R>& a, const MatParams<R>& m, const R S[3], const R T[3],
-                                               const R h[3]) {
+__device__ __forceinline__ R site_energy_delta(const LLGArgs<R>& a, int i, const MatParams<R>& m, const R S[3],
+                                               const R T[3], const R h[3]) {
    // dE = E(T) - E(S) for the single-spin energy (exchange field h fixed)
    R d = -((T[0] - S[0]) * (h[0] + a.hx) + (T[1] - S[1]) * (h[1] + a.hy) + (T[2] - S[2]) * (h[2] + a.hz));
    if (a.uniaxial) {
@@ -70,6 +70,7 @@ __device__ __forceinline__ R site_energy_delta(const LLGArgs<R>& a, const MatPar
       const R t4 = T[0] * T[0] * T[0] * T[0] + T[1] * T[1] * T[1] * T[1] + T[2] * T[2] * T[2] * T[2];
       d += (R)(-0.5) * m.kc4 * (t4 - s4);
    }
+   if (a.aniso_ext) d += anisotropy_energy<R, R, true>(a, i, m, T) - anisotropy_energy<R, R, true>(a, i, m, S);
    return d;
 }
 
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(256) mc_colour_kernel(const MCArgs<R> p) {
       R T[3] = {S[0] + g0 * sg, S[1] + g1 * sg, S[2] + g2 * sg};
       const R r = rsqrt_<R>(T[0] * T[0] + T[1] * T[1] + T[2] * T[2]);
       T[0] *= r; T[1] *= r; T[2] *= r;
-      const R dE = site_energy_delta<R>(a, m, S, T, h) * __ldg(p.mu_ratio + mi);
+      const R dE = site_energy_delta<R>(a, i, m, S, T, h) * __ldg(p.mu_ratio + mi);
       bool accept = dE < (R)0;
       if (!accept) {
          const R x = -dE * __ldg(p.beta + mi);

@@ -88,15 +88,8 @@ __global__ void stats_partial_kernel(const LLGArgs<R> a, const int* __restrict__
             R hx = 0, hy = 0, hz = 0;
             exchange_gather<R, FMT>(a, i, mi, a.ax, a.ay, a.az, hx, hy, hz);
             const double eex = -((double)S[0] * hx + (double)S[1] * hy + (double)S[2] * hz);
-            double ean = 0.0;
-            if (a.uniaxial) {
-               const double sd = (double)S[0] * m.kux + (double)S[1] * m.kuy + (double)S[2] * m.kuz;
-               ean += -(double)m.ku2 * (sd * sd);
-            }
-            if (a.cubic) {
-               const double x2 = (double)S[0] * S[0], y2 = (double)S[1] * S[1], z2 = (double)S[2] * S[2];
-               ean += -0.5 * (double)m.kc4 * (x2 * x2 + y2 * y2 + z2 * z2);
-            }
+            const double Sd[3] = {(double)S[0], (double)S[1], (double)S[2]};
+            const double ean = anisotropy_energy<double, R>(a, i, m, Sd);
             const double eap = -((double)a.hx * S[0] + (double)a.hy * S[1] + (double)a.hz * S[2]);
             double ems = 0.0;
             if (a.cell) {

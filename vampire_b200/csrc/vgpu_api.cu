@@ -318,6 +318,11 @@ int refresh_materials_typed(vgpu_ctx* h) {
       o.kc4 = (R)q.kc4;
       o.hlx = (R)q.applied_field[0]; o.hly = (R)q.applied_field[1]; o.hlz = (R)q.applied_field[2];
       o.mu_s_muB = (R)(q.mu_s_SI / 9.27400915e-24);
+      o.ku4 = S.ku4_h.empty() ? (R)0 : (R)S.ku4_h[m];
+      o.ku6 = S.ku6_h.empty() ? (R)0 : (R)S.ku6_h[m];
+      o.kc6 = S.kc6_h.empty() ? (R)0 : (R)S.kc6_h[m];
+      for (int k = 0; k < 9; ++k)
+         o.kcb[k] = S.kcb_h.empty() ? (R)(k % 4 == 0 ? 1 : 0) : (R)S.kcb_h[9 * (size_t)m + k];
       const double* rp = batch_ramp(h);
       o.dhx = rp ? (R)rp[3 * m] : (R)0;
       o.dhy = rp ? (R)rp[3 * m + 1] : (R)0;
@@ -346,6 +351,9 @@ LLGArgs<R> make_args(vgpu_ctx* h) {
    LLGArgs<R> a;
    memset(&a, 0, sizeof a);
    a.n = S.n;
+   a.n_alloc = S.n_alloc;
+   a.aniso_ext = S.aniso_ext;
+   a.neel = (const R*)S.neel;
    a.n_upd = S.n_owned;
    a.noise_base = S.noise_base;
    a.slice_off = (const int*)S.slice_off;
@@ -424,7 +432,8 @@ static int stage_slot(int sl) { return sl == 2 ? 0 : sl == 4 ? 1 : 2; }
 template <typename R>
 static bool use_staged(vgpu_ctx* h) {
    const SysDev& S = h->sys;
-   if (sizeof(R) != 4 || !S.rec || S.n == 0 || h->staged == 0) return false;
+   // the staged passes carry no higher-order anisotropy terms (register budget)
+   if (sizeof(R) != 4 || !S.rec || S.n == 0 || h->staged == 0 || S.aniso_ext) return false;
    const int bytes = S.stage_bytes[stage_slot(h->stage_sl)];
    return h->stage_nbuf * bytes <= kStageSmemLimit;
 }
@@ -744,6 +753,62 @@ extern "C" int vgpu_set_noise_replay(vgpu_handle h, const double* xi) {
    if (rc) return rc;
    h->noise_mode = VGPU_NOISE_REPLAY;
    return VGPU_OK;
+}
+
+template <typename R>
+static int upload_neel(vgpu_handle h, const double* t) {
+   SysDev& S = h->sys;
+   const size_t na = (size_t)S.n_alloc;
+   std::vector<R> buf(9 * na, (R)0);  // [component][atom], pad rows zero
+   for (int i = 0; i < S.n; ++i)
+      for (int k = 0; k < 9; ++k) buf[k * na + i] = (R)t[9 * (size_t)i + k];
+   if (!S.neel) {
+      S.neel = h->alloc(buf.size() * sizeof(R));
+      if (!S.neel) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for Neel tensors");
+   }
+   int rc = cuda_err(h, cudaMemcpyAsync(S.neel, buf.data(), buf.size() * sizeof(R), cudaMemcpyHostToDevice, h->stream),
+                     "Neel tensors");
+   if (rc) return rc;
+   return cuda_err(h, cudaStreamSynchronize(h->stream), "Neel tensors");
+}
+
+extern "C" int vgpu_set_anisotropy_ext(vgpu_handle h, const vgpu_anisotropy_ext* x) {
+   if (!h || !x) return set_err(h, VGPU_ERR_ARG, "null argument");
+   SysDev& S = h->sys;
+   if (!S.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (S.sys_off) return set_err(h, VGPU_ERR_STATE, "batched systems carry second-order uniaxial and cubic anisotropy only");
+   const int M = S.M;
+   if ((x->uniaxial_fourth && !x->ku4) || (x->uniaxial_sixth && !x->ku6) || (x->cubic_sixth && !x->kc6) ||
+       (x->cubic_rotation && !x->kc_basis) || (x->neel && !x->neel_tensor))
+      return set_err(h, VGPU_ERR_ARG, "an enabled anisotropy term has no data");
+   auto finite = [](const double* v, size_t k) {
+      for (size_t q = 0; q < k; ++q)
+         if (!std::isfinite(v[q])) return false;
+      return true;
+   };
+   if ((x->uniaxial_fourth && !finite(x->ku4, M)) || (x->uniaxial_sixth && !finite(x->ku6, M)) ||
+       (x->cubic_sixth && !finite(x->kc6, M)) || (x->cubic_rotation && !finite(x->kc_basis, 9 * (size_t)M)) ||
+       (x->neel && !finite(x->neel_tensor, 9 * (size_t)S.n)))
+      return set_err(h, VGPU_ERR_ARG, "non-finite anisotropy constant");
+   if (x->cubic_rotation && S.cubic)
+      return set_err(h, VGPU_ERR_ARG, "rotated cubic anisotropy replaces the plain cubic term (cubic_enabled = 0)");
+   cudaSetDevice(h->device);
+   int bits = 0;
+   S.ku4_h.assign(x->uniaxial_fourth ? x->ku4 : nullptr, x->uniaxial_fourth ? x->ku4 + M : nullptr);
+   S.ku6_h.assign(x->uniaxial_sixth ? x->ku6 : nullptr, x->uniaxial_sixth ? x->ku6 + M : nullptr);
+   S.kc6_h.assign(x->cubic_sixth ? x->kc6 : nullptr, x->cubic_sixth ? x->kc6 + M : nullptr);
+   S.kcb_h.assign(x->cubic_rotation ? x->kc_basis : nullptr, x->cubic_rotation ? x->kc_basis + 9 * (size_t)M : nullptr);
+   if (x->uniaxial_fourth) bits |= ANI_U4;
+   if (x->uniaxial_sixth) bits |= ANI_U6;
+   if (x->cubic_sixth) bits |= ANI_C6;
+   if (x->cubic_rotation) bits |= ANI_CROT;
+   if (x->neel) {
+      int rc = h->prec == VGPU_PREC_FP64 ? upload_neel<double>(h, x->neel_tensor) : upload_neel<float>(h, x->neel_tensor);
+      if (rc) return rc;
+      bits |= ANI_NEEL;
+   }
+   S.aniso_ext = bits;
+   return h->refresh_materials();
 }
 
 extern "C" int vgpu_set_option(vgpu_handle h, int option, int value) {

@@ -57,6 +57,10 @@ struct SysDev {
    std::vector<int> nl_host;
    std::vector<vgpu_material> materials;
    std::vector<unsigned char> mp_host;  // last material table copied to mp
+   // higher-order anisotropy (vgpu_set_anisotropy_ext)
+   int aniso_ext = 0;                          // AnisoExt bits
+   std::vector<double> ku4_h, ku6_h, kc6_h, kcb_h;  // per material (kcb: 9 each)
+   void* neel = nullptr;                       // [9][n_alloc] Neel tensors
 };
 
 int set_err(vgpu_ctx* h, int code, const char* fmt, ...);

@@ -36,12 +36,18 @@ struct MatParams {
    R hlx, hly, hlz;   // local applied field (0 if disabled)
    R mu_s_muB;        // moment in Bohr magnetons (stats)
    R dhx, dhy, dhz;   // field change over a linear sweep (batched systems), added as dh * min(step, n)/n
+   R ku4, ku6, kc6;   // higher-order reduced constants [T] (0 unless enabled)
+   R kcb[9];          // rotated cubic basis e1, e2, e3
 };
+
+// higher-order anisotropy terms present (LLGArgs::aniso_ext bits)
+enum AnisoExt : int { ANI_U4 = 1, ANI_U6 = 2, ANI_C6 = 4, ANI_CROT = 8, ANI_NEEL = 16 };
 
 // Everything one fused LLG pass needs, passed by value.
 template <typename R>
 struct LLGArgs {
    int n;                    // atoms (array length of the per-atom inputs)
+   int n_alloc;              // row stride of SoA per-atom tables (n rounded up to slices, + pad atom)
    int n_upd;                // atoms the passes update: all, or the owned atoms of a shard (0..n_upd-1)
    uint32_t noise_base;      // added to the atom index in the Philox counter (global index of a shard's atom 0)
    const int* slice_off;     // [nslices+1] SELL-32 entry offsets
@@ -57,6 +63,8 @@ struct LLGArgs {
    const int* mat;           // [n] material id, or nullptr when M == 1
    const MatParams<R>* mp;   // [M]
    int uniaxial, cubic;
+   int aniso_ext;            // AnisoExt bits
+   const R* neel;            // [9][n_alloc] per-atom Neel tensors (ANI_NEEL), row-major components
    R hx, hy, hz;             // global applied field
    int local_field;          // add MatParams::hl*
    uint64_t ramp_n;          // > 0: add MatParams::dh * min(step, ramp_n) / ramp_n

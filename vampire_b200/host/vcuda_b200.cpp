@@ -159,7 +159,8 @@ bool initialize(bool cpu_stats) {
       } else {
          q.ku_vector[2] = 1.0;
       }
-      if (anisotropy::internal::enable_cubic_fourth_order) q.kc4 = anisotropy::internal::kc4[m];
+      if (anisotropy::internal::enable_cubic_fourth_order || anisotropy::internal::enable_cubic_fourth_order_rotation)
+         q.kc4 = anisotropy::internal::kc4[m];
       q.temperature = src.temperature;
       if (src.applied_field_unit_vector.size() >= 3)
          for (int k = 0; k < 3; ++k) q.applied_field[k] = src.applied_field_strength * src.applied_field_unit_vector[k];
@@ -201,6 +202,37 @@ bool initialize(bool cpu_stats) {
    d.sy = ::atoms::y_spin_array.data();
    d.sz = ::atoms::z_spin_array.data();
    fail(vgpu_upload_system(g_h, &d), "system upload");
+   // higher-order anisotropy (anisotropy/internal.hpp), as anisotropy::fields evaluates it
+   {
+      namespace ai = anisotropy::internal;
+      if (ai::enable_lattice_anisotropy) {
+         std::cerr << "Error: lattice anisotropy is not evaluated by the B200 backend" << std::endl;
+         zlog << zTs() << "Error: lattice anisotropy is not evaluated by the B200 backend" << std::endl;
+         err::vexit();
+      }
+      vgpu_anisotropy_ext x;
+      std::memset(&x, 0, sizeof x);
+      x.uniaxial_fourth = ai::enable_uniaxial_fourth_order;
+      x.uniaxial_sixth = ai::enable_uniaxial_sixth_order;
+      x.cubic_sixth = ai::enable_cubic_sixth_order;
+      x.cubic_rotation = ai::enable_cubic_fourth_order_rotation;
+      x.neel = ai::enable_neel_anisotropy;
+      std::vector<double> kcb;
+      if (x.uniaxial_fourth) x.ku4 = ai::ku4.data();
+      if (x.uniaxial_sixth) x.ku6 = ai::ku6.data();
+      if (x.cubic_sixth) x.kc6 = ai::kc6.data();
+      if (x.cubic_rotation) {
+         for (int m = 0; m < M; ++m) {
+            for (int k = 0; k < 3; ++k) kcb.push_back(ai::mp[m].kc_vector1[k]);
+            for (int k = 0; k < 3; ++k) kcb.push_back(ai::mp[m].kc_vector2[k]);
+            for (int k = 0; k < 3; ++k) kcb.push_back(ai::mp[m].kc_vector3[k]);
+         }
+         x.kc_basis = kcb.data();
+      }
+      if (x.neel) x.neel_tensor = ai::neel_tensor.data();
+      if (x.uniaxial_fourth || x.uniaxial_sixth || x.cubic_sixth || x.cubic_rotation || x.neel)
+         fail(vgpu_set_anisotropy_ext(g_h, &x), "higher-order anisotropy");
+   }
    sync_params();
    fail(vgpu_set_noise(g_h, VGPU_NOISE_PHILOX, (uint64_t)(uint32_t)mtrandom::integration_seed), "noise");
    fail(vgpu_set_step(g_h, sim::time), "step counter");

@@ -150,12 +150,17 @@ def local_system(s: SpinSystem, plan: ShardPlan) -> SpinSystem:
         nl_type = None
         jlist = s.jlist.reshape(-1, w)[bonds].ravel() if w > 1 else s.jlist[bonds]
     masks = {k: (np.asarray(m)[glob].astype(np.int32), size) for k, (m, size) in s.masks.items()}
+    aniso = None
+    if s.aniso is not None:
+        aniso = dict(s.aniso)
+        if aniso.get("neel_tensor") is not None:
+            aniso["neel_tensor"] = np.ascontiguousarray(aniso["neel_tensor"][glob])
     return SpinSystem(n=n_loc, nl_start=start, nl_end=end, nl=nl.astype(np.int32), jlist=jlist,
                       exch_type=s.exch_type, type=s.type[glob].astype(np.int32), materials=s.materials,
                       spins=np.ascontiguousarray(s.spins[:, glob]), params=s.params, uniaxial=s.uniaxial,
                       cubic=s.cubic, nl_type=nl_type,
                       coords=None if s.coords is None else np.ascontiguousarray(s.coords[:, glob]),
-                      masks=masks, cells=None)
+                      masks=masks, cells=None, aniso=aniso)
 
 
 class HaloExchange:

@@ -54,10 +54,63 @@ class Material:
     non_magnetic: int = 0
     temperature: float = 0.0
     applied_field: Sequence[float] = (0.0, 0.0, 0.0)
+    Ku4: float = 0.0                         # fourth-order-uniaxial-anisotropy-constant [J/atom]
+    Ku6: float = 0.0                         # sixth-order-uniaxial-anisotropy-constant [J/atom]
+    Kc6: float = 0.0                         # sixth-order-cubic-anisotropy-constant [J/atom]
+    kc_axis1: Optional[Sequence[float]] = None   # cubic-anisotropy-direction-1 (rotated cubic basis)
+    kc_axis2: Optional[Sequence[float]] = None   # cubic-anisotropy-direction-2
 
     @property
     def mu_s_SI(self) -> float:
         return self.mu_s_muB * MU_B
+
+
+def anisotropy_ext(mats: Sequence[Material], n: int) -> Optional[dict]:
+    """Higher-order anisotropy of `mats` in the reference's reduced form
+    (anisotropy/initialize.cpp:60-120: K / mu_s, and the rotated cubic basis
+    e1, e2, e3 = e1 x e2 normalised), or None when every term is off."""
+    u4 = any(m.Ku4 != 0.0 for m in mats)
+    u6 = any(m.Ku6 != 0.0 for m in mats)
+    c6 = any(m.Kc6 != 0.0 for m in mats)
+    crot = any(m.kc_axis1 is not None or m.kc_axis2 is not None for m in mats)
+    if not (u4 or u6 or c6 or crot):
+        return None
+    M = len(mats)
+    kcb = np.zeros((M, 9))
+    for i, m in enumerate(mats):
+        e1 = np.asarray(m.kc_axis1 if m.kc_axis1 is not None else (1.0, 0.0, 0.0), dtype=np.float64)
+        e2 = np.asarray(m.kc_axis2 if m.kc_axis2 is not None else (0.0, 1.0, 0.0), dtype=np.float64)
+        e1 = e1 / np.linalg.norm(e1)
+        e2 = e2 / np.linalg.norm(e2)
+        e3 = np.cross(e1, e2)
+        e3 = e3 / np.linalg.norm(e3)
+        kcb[i] = np.concatenate([e1, e2, e3])
+    inv = np.array([1.0 / (m.mu_s_muB * MU_B) for m in mats])
+    return {"u4": u4, "u6": u6, "c6": c6, "crot": crot, "neel": False,
+            "ku4": np.array([m.Ku4 for m in mats]) * inv, "ku6": np.array([m.Ku6 for m in mats]) * inv,
+            "kc6": np.array([m.Kc6 for m in mats]) * inv, "kcb": kcb, "neel_tensor": None}
+
+
+def add_neel(s: SpinSystem, K_SI, bond_vec: np.ndarray, threshold: int) -> None:
+    """Neel pair anisotropy on atoms with fewer than `threshold` neighbours
+    (anisotropy/initialize_neel.cpp): T_i = sum_j K_ij/mu_s,i e_ij e_ij over
+    the atom's neighbours.  bond_vec: (nnz, 3) i->j vectors of s.nl."""
+    K = np.atleast_2d(np.asarray(K_SI, dtype=np.float64))
+    deg = s.nl_end - s.nl_start + 1
+    T = np.zeros((s.n, 9))
+    mus = s.materials["mu_s_SI"]
+    for i in np.flatnonzero(deg < threshold):
+        mi = s.type[i]
+        for b in range(s.nl_start[i], s.nl_end[i] + 1):
+            e = bond_vec[b] / np.linalg.norm(bond_vec[b])
+            kij = K[mi, s.type[s.nl[b]]] / mus[mi]
+            T[i] += kij * np.outer(e, e).ravel()
+    if s.aniso is None:
+        s.aniso = {"u4": False, "u6": False, "c6": False, "crot": False, "neel": True,
+                   "ku4": None, "ku6": None, "kc6": None, "kcb": None, "neel_tensor": T}
+    else:
+        s.aniso["neel"] = True
+        s.aniso["neel_tensor"] = T
 
 
 def derive_materials(mats: Sequence[Material], dt_SI: float, gamma_SI: float = GAMMA_SI) -> np.ndarray:
@@ -125,6 +178,8 @@ class SpinSystem:
     coords: Optional[np.ndarray] = None        # (3, n) Angstrom
     masks: dict = field(default_factory=dict)  # name -> (mask int32 [n], size)
     cells: Optional[dict] = None               # dipole macrocells (see dipole_cells())
+    aniso: Optional[dict] = None               # higher-order anisotropy (see anisotropy_ext())
+    bond_vectors: Optional[np.ndarray] = None  # (nnz, 3) i->j vectors [Angstrom] of the lattice builders
 
     @property
     def num_bonds(self) -> int:
@@ -367,12 +422,15 @@ def build(kind: str, nx: int, ny: int, nz: int, a: float, mats: Sequence[Materia
         jl = add_dmi(jl, st, en, nl, vec, types, materials, np.atleast_2d(dmi_SI), dmi_cutoff)
     if spins is None:
         spins = random_spins(n, spin_seed)
+    ext = anisotropy_ext(mats, n)
+    rotated = ext is not None and ext["crot"]
     sys_ = SpinSystem(n=n, nl_start=st, nl_end=en, nl=nl, jlist=jl, exch_type=exch_type,
                       type=types, materials=materials, spins=np.ascontiguousarray(spins),
                       params=params, uniaxial=any(m.Ku != 0.0 for m in mats),
-                      cubic=any(m.Kc != 0.0 for m in mats), coords=coords)
+                      cubic=any(m.Kc != 0.0 for m in mats) and not rotated, coords=coords, aniso=ext)
     sys_.masks["system"] = (np.zeros(n, dtype=np.int32), 1)
     sys_.masks["material"] = (types.copy(), len(mats))
+    sys_.bond_vectors = vec
     return sys_
 
 
@@ -432,6 +490,16 @@ def replicas(s: SpinSystem, temperatures: Sequence[float]) -> SpinSystem:
     out = SpinSystem(n=k * n, nl_start=st, nl_end=en, nl=nl, jlist=jl, exch_type=s.exch_type, type=typ,
                      materials=mats, spins=np.tile(s.spins, (1, k)), params=p, uniaxial=s.uniaxial, cubic=s.cubic,
                      nl_type=nl_type, coords=None)
+    if s.aniso is not None:
+        a = dict(s.aniso)
+        for key in ("ku4", "ku6", "kc6"):
+            if a[key] is not None:
+                a[key] = np.tile(a[key], k)
+        if a["kcb"] is not None:
+            a["kcb"] = np.tile(a["kcb"], (k, 1))
+        if a["neel_tensor"] is not None:
+            a["neel_tensor"] = np.tile(a["neel_tensor"], (k, 1))
+        out.aniso = a
     out.masks["system"] = (np.zeros(k * n, dtype=np.int32), 1)
     out.masks["replica"] = ((off // n).astype(np.int32), k)
     out.masks["material"] = (typ.copy(), k * M)

@@ -56,6 +56,36 @@ class SimParamsC(C.Structure):
     ]
 
 
+class AnisoExtC(C.Structure):
+    _fields_ = [
+        ("uniaxial_fourth", C.c_int32), ("uniaxial_sixth", C.c_int32), ("cubic_sixth", C.c_int32),
+        ("cubic_rotation", C.c_int32), ("neel", C.c_int32), ("pad_", C.c_int32),
+        ("ku4", _D), ("ku6", _D), ("kc6", _D), ("kc_basis", _D), ("neel_tensor", _D),
+    ]
+
+
+def _aniso_ext(a: dict):
+    """AnisoExtC of SpinSystem.aniso; returns (struct, keep-alive list)."""
+    keep = []
+
+    def arr(v):
+        if v is None:
+            return C.cast(None, _D)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        keep.append(v)
+        return _ptr(v, _D)
+
+    x = AnisoExtC()
+    x.uniaxial_fourth, x.uniaxial_sixth = int(a["u4"]), int(a["u6"])
+    x.cubic_sixth, x.cubic_rotation, x.neel = int(a["c6"]), int(a["crot"]), int(a["neel"])
+    x.ku4 = arr(a["ku4"] if a["u4"] else None)
+    x.ku6 = arr(a["ku6"] if a["u6"] else None)
+    x.kc6 = arr(a["kc6"] if a["c6"] else None)
+    x.kc_basis = arr(a["kcb"] if a["crot"] else None)
+    x.neel_tensor = arr(a["neel_tensor"] if a["neel"] else None)
+    return x, keep
+
+
 class DipoleDesc(C.Structure):
     _fields_ = [
         ("num_cells", C.c_int32), ("solver", C.c_int32), ("update_rate", C.c_int32), ("pad_", C.c_int32),
@@ -200,6 +230,9 @@ class Simulation:
     def upload(self, s: SpinSystem) -> None:
         d, keep = _desc(s)
         self._check(lib().vgpu_upload_system(self._h, C.byref(d)))
+        if s.aniso is not None:
+            x, keep2 = _aniso_ext(s.aniso)
+            self._check(lib().vgpu_set_anisotropy_ext(self._h, C.byref(x)))
 
     def set_option(self, option: int, value: int) -> None:
         """vgpu_set_option: OPT_STORE_INCREMENT, OPT_STAGED_RECORDS, OPT_STAGE_SLICES, OPT_STAGE_BUFFERS."""
