@@ -388,6 +388,17 @@ int vgpu_stats_reset(vgpu_handle h);
  * as magnetization.cpp:134-180.  No reference counterpart. */
 int vgpu_stats_get_sums(vgpu_handle h, int32_t id, double* sums);
 
+/* Derived statistics of mask `id` accumulated on the device at every
+ * vgpu_stats_update since the last reset, evaluated as the reference's
+ * output functions do at temperature T [K]: susceptibility[4*bin + {x,y,z,m}]
+ * (statistics/susceptibility.cpp:70-88, from the magnetisation rows),
+ * specific_heat[bin] (specific_heat.cpp:50-66, from the total energy; needs
+ * energy updates) and std_dev[4*bin + {x,y,z,m}] (standard_deviation.cpp,
+ * running Welford sums).  Any output may be NULL.  The reference computes
+ * these on the host only and skips them in GPU mode (statistics.cpp:35-37). */
+int vgpu_stats_get_derived(vgpu_handle h, int32_t id, double temperature, double* susceptibility,
+                           double* specific_heat, double* std_dev);
+
 /* ---- batched systems ------------------------------------------------------ */
 
 /* No counterpart in the reference (one system per process there).  Per-system

@@ -210,6 +210,28 @@ static void dump_stats(const std::string& tag) {
    dumpd("energy_material_" + tag, e);
 }
 
+// the reference's derived statistics (susceptibility, specific heat, standard
+// deviation), read back from their own output functions at 17 digits
+static std::vector<double> parse_doubles(const std::string& text) {
+   std::vector<double> v;
+   std::istringstream ss(text);
+   double x;
+   while (ss >> x) v.push_back(x);
+   return v;
+}
+
+static void dump_derived() {
+   vout::custom_precision = true;
+   vout::precision = 17;
+   vout::fixed = false;
+   const double T = sim::temperature;
+   dumpd("sus_system", parse_doubles(stats::system_susceptibility.output_mean_susceptibility(T, false)));
+   dumpd("sus_material", parse_doubles(stats::material_susceptibility.output_mean_susceptibility(T, false)));
+   dumpd("spec_heat_system", parse_doubles(stats::system_specific_heat.output_mean_specific_heat(T, false)));
+   dumpd("spec_heat_material", parse_doubles(stats::material_specific_heat.output_mean_specific_heat(T, false)));
+   dumpd("std_material", parse_doubles(stats::material_standard_deviation.output_standard_deviation(false)));
+}
+
 static void dump_dipole(const std::string& tag) {
    if (!dipole::activated) return;
    dumpd("cmag_x_" + tag, cells::mag_array_x);
@@ -224,7 +246,8 @@ static void dump_dipole(const std::string& tag) {
 }
 
 int main(int argc, char* argv[]) {
-   long steps = 0, warmup = 0, noise = 0, mag_every = 0, mag_start = 0;
+   long steps = 0, warmup = 0, noise = 0, mag_every = 0, mag_start = 0, stats_every = 0;
+   bool want_derived = false;
    std::vector<long> snaps, stat_snaps;
    bool want_system = false, want_dipole = false, want_time = false;
    for (int i = 1; i < argc; i++) {
@@ -243,6 +266,8 @@ int main(int argc, char* argv[]) {
       else if (a == "--mag-every") mag_every = atol(next());
       else if (a == "--mag-start") mag_start = atol(next());
       else if (a == "--dipole") want_dipole = true;
+      else if (a == "--derived") want_derived = true;
+      else if (a == "--stats-every") stats_every = atol(next());
       else if (a == "--time") want_time = true;
       else { std::cerr << "harness: unknown option " << a << std::endl; return 2; }
    }
@@ -254,6 +279,13 @@ int main(int argc, char* argv[]) {
    vout::zLogTsInit(std::string(argv[0]));
    stats::calculate_system_energy = true;
    stats::calculate_material_energy = true;
+   if (want_derived) {
+      stats::calculate_system_susceptibility = true;
+      stats::calculate_material_susceptibility = true;
+      stats::calculate_system_specific_heat = true;
+      stats::calculate_material_specific_heat = true;
+      stats::calculate_material_standard_deviation = true;
+   }
    stats::calculate_system_magnetization = true;
    stats::calculate_material_magnetization = true;
    mp::initialise("input");
@@ -311,6 +343,9 @@ int main(int argc, char* argv[]) {
       else
          sim::LLG_Heun();
       sim::increment_time();
+      if (stats_every > 0 && step % stats_every == 0)
+         stats::update(atoms::x_spin_array, atoms::y_spin_array, atoms::z_spin_array, atoms::m_spin_array,
+                       atoms::type_array, sim::temperature);
       for (long s : snaps) if (s == step) dump_spins(std::to_string(step));
       for (long s : stat_snaps) if (s == step) dump_stats(std::to_string(step));
       if (want_dipole) for (long s : snaps) if (s == step) dump_dipole(std::to_string(step));
@@ -331,6 +366,7 @@ int main(int argc, char* argv[]) {
    const double loop_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
    if (want_time) std::cout << "HARNESS_LOOP_SECONDS " << loop_s << " ATOMS " << n << " STEPS " << steps << std::endl;
    if (!mag_trace.empty()) dumpd("mag_trace", mag_trace);
+   if (want_derived) dump_derived();
    std::vector<double> mc = {sim::mc_statistics_moves, sim::mc_statistics_reject};
    dumpd("mc_counters", mc);
    g_manifest.close();

@@ -107,6 +107,17 @@ def single_spin_applied():
     save("single_spin_applied", d, keep)
 
 
+def sc6_derived_t600():
+    """SC 6^3 periodic at T=600 K: 20 stochastic steps (Gaussian stream
+    replayed), statistics after every step, and the reference's derived
+    statistics (susceptibility, specific heat, standard deviation)."""
+    d = O.run_harness(sc_input(6, T=600.0), {"m.mat": SC_MAT},
+                      ["--system", "--steps", 20, "--noise", 20, "--stats-every", 1, "--derived", "--snaps", "20"])
+    keep = [f"s{c}_{t}" for t in (0, 20) for c in "xyz"] + [f"xi_{t}" for t in range(1, 21)]
+    keep += ["sus_system", "sus_material", "spec_heat_system", "spec_heat_material", "std_material"]
+    save("sc6_derived_t600", d, keep)
+
+
 HO_MAT = """material:num-materials=1
 material[1]:material-name=A
 material[1]:damping-constant=0.1
@@ -226,7 +237,7 @@ def mc_sc16_curie():
 
 
 ALL = [sc20_t0, sc8_t0, sc10_t300, sc6_open_t300, fcc4_dmi_t300, fcc4_dmi_t0, single_spin_applied, mc_sc16_curie,
-       fcc10_dipole_tensor, fcc10_dipole_macrocell, sc6_aniso_ho, fcc4_neel_rot]
+       fcc10_dipole_tensor, fcc10_dipole_macrocell, sc6_aniso_ho, fcc4_neel_rot, sc6_derived_t600]
 
 if __name__ == "__main__":
     names = sys.argv[1:]

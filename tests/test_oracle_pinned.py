@@ -123,3 +123,40 @@ def test_higher_order_anisotropy_pins_each_term():
         bad.aniso[key] = False
         got = O.OracleSystem(bad).llg_heun(bad.spins, 200)
         assert np.abs(got - ref_spins(d, 200)).max() > 1e-9, key
+
+
+def _derived_from_rows(mag_rows, e_rows, sat, norm, T):
+    """NumPy restatement of the reference's derived statistics
+    (statistics/susceptibility.cpp, specific_heat.cpp, standard_deviation.cpp)
+    from per-update magnetisation rows (m_x, m_y, m_z, |m|) and total energies."""
+    m = np.asarray(mag_rows)
+    cnt = len(m)
+    mm = m[:, 3]
+    s1 = np.stack([m[:, 0] * mm, m[:, 1] * mm, m[:, 2] * mm, mm], 1).sum(0)
+    s2 = np.stack([m[:, 0] ** 2 * mm ** 2, m[:, 1] ** 2 * mm ** 2, m[:, 2] ** 2 * mm ** 2, mm ** 2], 1).sum(0)
+    sus = 9.274e-24 / (1.3806503e-23 * T) * sat * (s2 / cnt - s1 ** 2 / cnt ** 2)
+    E = np.asarray(e_rows)
+    sh = 9.27400999e-24 / (1.3806503e-23 * T * T) / norm * ((E ** 2).sum() / len(E) - E.sum() ** 2 / len(E) ** 2)
+    std = m.std(axis=0)
+    return sus, sh, std
+
+
+def test_derived_statistics():
+    """The oracle's replayed trajectory, reduced every step, gives the
+    reference's susceptibility, specific heat and standard deviation."""
+    s, d = load_golden("sc6_derived_t600")
+    o = O.OracleSystem(s)
+    mask, size = s.masks["system"]
+    sp = s.spins
+    rows, es = [], []
+    for t in range(0, 21):
+        if t > 0:
+            sp = o.llg_heun(sp, 1, xi=d[f"xi_{t}"])
+        rows.append(o.magnetization(sp, mask, size)[:4])
+        es.append(o.energy(sp, mask, size)[0])
+    assert np.abs(sp - ref_spins(d, 20)).max() < 1e-12
+    sat = float(s.mu_s_muB()[mask == 0].sum())
+    sus, sh, std = _derived_from_rows(rows, es, sat, float(np.sum(mask == 0)), 600.0)
+    np.testing.assert_allclose(sus, d["sus_system"], rtol=1e-9)
+    np.testing.assert_allclose(sh, d["spec_heat_system"][0], rtol=1e-9)
+    np.testing.assert_allclose(std, d["std_material"], rtol=1e-7)

@@ -56,3 +56,27 @@ def test_stats_at_scale_checksum(vgpu_lib):
         v = (sp[:, sel] * mu[sel]).sum(1)
         want = np.r_[v / np.linalg.norm(v), np.linalg.norm(v) / mu[sel].sum()]
         assert np.abs(m[4 * b:4 * b + 4] - want).max() < 1e-9
+
+
+@pytest.mark.parametrize("prec,rtol", [("fp64", 1e-9), ("fp32", 1e-3)])
+def test_derived_statistics_match_reference(vgpu_lib, prec, rtol):
+    """Susceptibility, specific heat and standard deviation accumulated on the
+    device over the reference's own 20 stochastic steps (replayed noise, one
+    statistics update per step plus the initial one) against the values the
+    reference's output functions print (tests/golden/sc6_derived_t600.npz)."""
+    from vampire_b200 import vgpu
+    s, d = load_golden("sc6_derived_t600")
+    with vgpu.Simulation(s, precision=prec) as sim:
+        mid = sim.add_mask(*s.masks["system"])
+        sim.stats_update(magnetization=True, energy=True)
+        for t in range(1, 21):
+            sim.set_noise_replay(d[f"xi_{t}"])
+            sim.llg_heun(1)
+            sim.stats_update(magnetization=True, energy=True)
+        sus, sh, sd = sim.stats_derived(mid, 600.0)
+        sim.stats_reset()
+        sus0, _, _ = sim.stats_derived(mid, 600.0)
+    np.testing.assert_allclose(sus[0], d["sus_system"], rtol=rtol)
+    np.testing.assert_allclose(sh[0], d["spec_heat_system"][0], rtol=rtol)
+    np.testing.assert_allclose(sd[0], d["std_material"], rtol=rtol)
+    assert not np.isfinite(sus0).all() or np.all(sus0 == 0)   # reset: no updates left

@@ -30,6 +30,12 @@ namespace vgpu {
 enum { ST_MX, ST_MY, ST_MZ, ST_MU, ST_EEX, ST_EAN, ST_EAP, ST_EMS, ST_NQ };
 // finalised row per bin: m_hat(3), |m|/m_sat, E_total, E_exchange, E_anisotropy, E_applied, E_magnetostatic
 constexpr int ST_W = 9;
+// derived-statistic sums per bin: susceptibility (statistics/susceptibility.cpp:40-66)
+// sum m_k|m| (4), sum (m_k|m|)^2 (4), the same of absolute values (8); specific
+// heat (specific_heat.cpp:37-44) sum E, sum E^2; standard deviation
+// (standard_deviation.cpp:37-50) running mean (4) and residual sum (4)
+enum { DV_SUS = 0, DV_SUS2 = 4, DV_ASUS = 8, DV_ASUS2 = 12, DV_E = 16, DV_E2 = 17, DV_MEAN = 18, DV_RES = 22,
+       ST_DV = 26 };
 
 struct StatsMask {
    int size = 0;
@@ -38,6 +44,9 @@ struct StatsMask {
    double* cur = nullptr;      // [size][ST_W] finalised rows
    double* mean = nullptr;     // [size][ST_W] running sums of the finalised rows
    double* raw = nullptr;      // [size][ST_NQ] raw sums of the last update (combined across shards)
+   double* derived = nullptr;  // [size][ST_DV] running sums behind the derived statistics
+   std::vector<double> saturation;     // [size] sum of mu_s (mu_B) per bin (magnetization set_mask)
+   std::vector<double> normalisation;  // [size] atoms per bin (energy set_mask)
    long long counter_mag = 0, counter_en = 0;
 };
 
@@ -151,7 +160,8 @@ __global__ void __launch_bounds__(32 * ST_NQ) stats_final_kernel(const double* _
                                                                   int size, int do_mag, int do_energy,
                                                                   double* __restrict__ cur,
                                                                   double* __restrict__ mean,
-                                                                  double* __restrict__ raw) {
+                                                                  double* __restrict__ raw,
+                                                                  double* __restrict__ derived, double mag_count) {
    __shared__ double vq[ST_NQ];
    const int bin = blockIdx.x;
    const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -187,12 +197,33 @@ __global__ void __launch_bounds__(32 * ST_NQ) stats_final_kernel(const double* _
          o[3] = magm / msat;
       }
       for (int k = 0; k < 4; ++k) mn[k] += o[k];
+      double* dv = derived + (size_t)bin * ST_DV;
+      const double mm = o[3];
+      for (int k = 0; k < 3; ++k) {
+         dv[DV_SUS + k] += o[k] * mm;
+         dv[DV_SUS2 + k] += o[k] * o[k] * mm * mm;
+         dv[DV_ASUS + k] += fabs(o[k] * mm);
+         dv[DV_ASUS2 + k] += fabs(o[k] * o[k] * mm * mm);
+      }
+      dv[DV_SUS + 3] += mm;
+      dv[DV_SUS2 + 3] += mm * mm;
+      dv[DV_ASUS + 3] += mm;
+      dv[DV_ASUS2 + 3] += mm * mm;
+      for (int k = 0; k < 4; ++k) {  // Welford update, mag_count includes this update
+         const double r1 = o[k] - dv[DV_MEAN + k];
+         dv[DV_MEAN + k] += r1 / mag_count;
+         const double r2 = o[k] - dv[DV_MEAN + k];
+         dv[DV_RES + k] += r1 * r2;
+      }
    }
    if (do_energy) {
       const double ex = 0.5 * v[ST_EEX], an = v[ST_EAN], ap = v[ST_EAP], ms = 0.5 * v[ST_EMS];
       o[4] = ex + an + ap + ms;
       o[5] = ex; o[6] = an; o[7] = ap; o[8] = ms;
       for (int k = 4; k < 9; ++k) mn[k] += o[k];
+      double* dv = derived + (size_t)bin * ST_DV;
+      dv[DV_E] += o[4];
+      dv[DV_E2] += o[4] * o[4];
    }
 }
 
@@ -209,7 +240,7 @@ static cudaError_t launch_stats(const LLGArgs<R>& a, StatsMask& m, int nblocks, 
    cudaError_t e = cudaGetLastError();
    if (e != cudaSuccess) return e;
    stats_final_kernel<<<m.size, 32 * ST_NQ, 0, st>>>(m.partial, nblocks, m.size, do_mag, do_energy, m.cur, m.mean,
-                                                     m.raw);
+                                                     m.raw, m.derived, (double)(m.counter_mag + 1));
    return cudaGetLastError();
 }
 
@@ -230,7 +261,7 @@ void stats_destroy(vgpu_ctx* h) {
    StatsState* s = stats_of(h);
    if (!s) return;
    for (StatsMask& m : s->masks) {
-      cudaFree(m.mask); cudaFree(m.partial); cudaFree(m.cur); cudaFree(m.mean); cudaFree(m.raw);
+      cudaFree(m.mask); cudaFree(m.partial); cudaFree(m.cur); cudaFree(m.mean); cudaFree(m.raw); cudaFree(m.derived);
    }
    delete s;
    h->extras[0] = nullptr;
@@ -265,6 +296,17 @@ extern "C" int vgpu_stats_add_mask(vgpu_handle h, const int32_t* mask, int32_t m
       return cuda_err(h, e, "stats");
    if ((e = cudaMalloc(&m.raw, sizeof(double) * mask_size * ST_NQ)) != cudaSuccess) return cuda_err(h, e, "stats");
    cudaMemsetAsync(m.raw, 0, sizeof(double) * mask_size * ST_NQ, h->stream);
+   if ((e = cudaMalloc(&m.derived, sizeof(double) * mask_size * ST_DV)) != cudaSuccess) return cuda_err(h, e, "stats");
+   cudaMemsetAsync(m.derived, 0, sizeof(double) * mask_size * ST_DV, h->stream);
+   // bin saturation and atom counts, summed in atom order as set_mask does
+   // (statistics/magnetization.cpp:54-116 with mm = mu_s/mu_B, energy.cpp:84-89)
+   m.saturation.assign(mask_size, 0.0);
+   m.normalisation.assign(mask_size, 0.0);
+   for (int i = 0; i < n; ++i) {
+      const vgpu_material& q = h->sys.materials[h->sys.type_host.empty() ? 0 : h->sys.type_host[i]];
+      m.saturation[mask[i]] += q.mu_s_SI / 9.27400915e-24;
+      m.normalisation[mask[i]] += 1.0;
+   }
    cudaMemcpyAsync(m.mask, mask, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream);
    cudaMemsetAsync(m.cur, 0, sizeof(double) * mask_size * ST_W, h->stream);
    cudaMemsetAsync(m.mean, 0, sizeof(double) * mask_size * ST_W, h->stream);
@@ -341,6 +383,7 @@ extern "C" int vgpu_stats_reset(vgpu_handle h) {
    cudaSetDevice(h->device);
    for (StatsMask& m : s->masks) {
       cudaMemsetAsync(m.mean, 0, sizeof(double) * m.size * ST_W, h->stream);
+      cudaMemsetAsync(m.derived, 0, sizeof(double) * m.size * ST_DV, h->stream);
       m.counter_mag = m.counter_en = 0;
    }
    return cuda_err(h, cudaStreamSynchronize(h->stream), "statistics reset");
@@ -358,4 +401,48 @@ extern "C" int vgpu_stats_get_sums(vgpu_handle h, int32_t id, double* sums) {
    cudaError_t e = cudaMemcpyAsync(sums, m.raw, sizeof(double) * m.size * ST_NQ, cudaMemcpyDeviceToHost, h->stream);
    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
    return cuda_err(h, e, "statistics sums");
+}
+
+/* Derived statistics of mask `id` over the updates since the last reset, as
+ * the reference's output functions compute them at temperature T:
+ * susceptibility[4*bin + k] (statistics/susceptibility.cpp:70-88: the
+ * 9.274e-24 / (1.3806503e-23 T) prefactor times the bin saturation),
+ * specific_heat[bin] (specific_heat.cpp:50-66: muB / (kB T^2) per atom, with
+ * constants::muB = 9.27400999e-24, kB = 1.3806503e-23) and
+ * std_dev[4*bin + k] (standard_deviation.cpp:60-70).  Any output may be NULL.
+ * The reference evaluates these on the host only, never in GPU mode. */
+extern "C" int vgpu_stats_get_derived(vgpu_handle h, int32_t id, double temperature, double* susceptibility,
+                                      double* specific_heat, double* std_dev) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   StatsState* s = stats_of(h);
+   if (!s || id < 0 || id >= (int)s->masks.size()) return set_err(h, VGPU_ERR_ARG, "unknown statistics mask %d", id);
+   StatsMask& m = s->masks[id];
+   cudaSetDevice(h->device);
+   std::vector<double> dv((size_t)m.size * ST_DV);
+   cudaError_t e = cudaMemcpyAsync(dv.data(), m.derived, dv.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+   if (e != cudaSuccess) return cuda_err(h, e, "derived statistics");
+   const double T = temperature;
+   const double cm = (double)m.counter_mag, ce = (double)m.counter_en;
+   for (int b = 0; b < m.size; ++b) {
+      const double* v = dv.data() + (size_t)b * ST_DV;
+      if (susceptibility) {
+         const double itemp = T < 1.e-300 ? 0.0 : 9.274e-24 / (1.3806503e-23 * T);
+         const double imc = 1.0 / cm, imc2 = 1.0 / (cm * cm);
+         const double pre = itemp * m.saturation[b];
+         for (int k = 0; k < 4; ++k)
+            susceptibility[4 * b + k] = pre * (v[DV_SUS2 + k] * imc - v[DV_SUS + k] * v[DV_SUS + k] * imc2);
+      }
+      if (specific_heat) {
+         const double itemp2 = T < 1.e-300 ? +0.0 : 9.27400999e-24 / (1.3806503e-23 * T * T);
+         const double imc = 1.0 / ce, imc2 = 1.0 / (ce * ce);
+         const double pre = itemp2 / m.normalisation[b];
+         specific_heat[b] = pre * ((v[DV_E2] * imc) - (v[DV_E] * v[DV_E] * imc2));
+      }
+      if (std_dev) {
+         const double imc = 1.0 / cm;
+         for (int k = 0; k < 4; ++k) std_dev[4 * b + k] = sqrt(v[DV_RES + k] * imc);
+      }
+   }
+   return VGPU_OK;
 }

@@ -306,6 +306,15 @@ class Simulation:
         self._check(lib().vgpu_halo_unpack(self._h, C.c_int(which), C.c_int32(first), C.c_int32(count),
                                            C.c_void_p(in_ptr)))
 
+    def stats_derived(self, mask_id: int, temperature: float):
+        """(susceptibility (size, 4), specific heat (size,), std dev (size, 4))
+        of the updates since the last reset (vgpu_stats_get_derived)."""
+        size = self._mask_sizes[mask_id]
+        sus, sh, sd = np.zeros(4 * size), np.zeros(size), np.zeros(4 * size)
+        self._check(lib().vgpu_stats_get_derived(self._h, C.c_int32(mask_id), C.c_double(temperature),
+                                                 _ptr(sus, _D), _ptr(sh, _D), _ptr(sd, _D)))
+        return sus.reshape(size, 4), sh, sd.reshape(size, 4)
+
     def stats_sums(self, mask_id: int, size: int) -> np.ndarray:
         """Raw per-bin sums of the last statistics update, (size, 8)."""
         out = np.zeros((size, 8))
