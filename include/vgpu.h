@@ -260,6 +260,15 @@ int vgpu_set_owned(vgpu_handle h, int32_t n_owned, int64_t noise_base);
 int vgpu_halo_pack(vgpu_handle h, int which, const int32_t* idx, int32_t count, void* out);
 int vgpu_halo_unpack(vgpu_handle h, int which, int32_t first, int32_t count, const void* in);
 
+/* Advance n_steps of the LLG-Midpoint integrator (sim::LLG_Midpoint,
+ * src/simulate/LLGMidpoint.cpp:48-150; sim:integrator=llg-midpoint): the
+ * same two fused passes per step as vgpu_llg_heun -- the first writes the
+ * midpoint M = (S + R S)/2 (Cayley rotation with F = H + alpha S x H), the
+ * second rotates S by F(M, H(M)) -- with the external field, thermal noise
+ * included, shared by both halves.  No renormalisation, as the reference.
+ * The reference runs this integrator on the host only. */
+int vgpu_llg_midpoint(vgpu_handle h, uint64_t n_steps);
+
 /* Write the 3*num_atoms Gaussians (x|y|z blocks) that the Philox stream
  * gives the thermal field at step `step` -- the values the fused kernels
  * regenerate in-register.  For tests and for replaying a run elsewhere. */

@@ -245,6 +245,19 @@ static void dump_dipole(const std::string& tag) {
    dumpd("chd_z_" + tag, dipole::cells_mu0Hd_field_array_z);
 }
 
+// one step of the selected integrator, as sim::integrate_serial dispatches it
+// (src/simulate/sim.cpp:595-640)
+static void one_step() {
+   switch (sim::integrator) {
+      case 1:
+         montecarlo::mc_step(atoms::x_spin_array, atoms::y_spin_array, atoms::z_spin_array, atoms::num_atoms,
+                             atoms::type_array);
+         break;
+      case 2: sim::LLG_Midpoint(); break;
+      default: sim::LLG_Heun(); break;
+   }
+}
+
 int main(int argc, char* argv[]) {
    long steps = 0, warmup = 0, noise = 0, mag_every = 0, mag_start = 0, stats_every = 0;
    bool want_derived = false;
@@ -320,11 +333,7 @@ int main(int argc, char* argv[]) {
    std::vector<double> mag_trace;  // per recorded step: mx, my, mz, |m| (system mask, bin 0), total E
    // untimed warm-up steps (timing runs only; nothing is dumped for them)
    for (long w = 0; w < warmup; w++) {
-      if (sim::integrator == 1)
-         montecarlo::mc_step(atoms::x_spin_array, atoms::y_spin_array, atoms::z_spin_array,
-                             atoms::num_atoms, atoms::type_array);
-      else
-         sim::LLG_Heun();
+      one_step();
       sim::increment_time();
    }
    const auto t0 = std::chrono::steady_clock::now();
@@ -337,11 +346,7 @@ int main(int argc, char* argv[]) {
          mtrandom::grnd.set_state(st, p);
          dumpd("xi_" + std::to_string(step), xi);
       }
-      if (sim::integrator == 1)
-         montecarlo::mc_step(atoms::x_spin_array, atoms::y_spin_array, atoms::z_spin_array,
-                             atoms::num_atoms, atoms::type_array);
-      else
-         sim::LLG_Heun();
+      one_step();
       sim::increment_time();
       if (stats_every > 0 && step % stats_every == 0)
          stats::update(atoms::x_spin_array, atoms::y_spin_array, atoms::z_spin_array, atoms::m_spin_array,

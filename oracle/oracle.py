@@ -173,6 +173,16 @@ class OracleSystem:
                             _p(xi_c, _D), C.c_int64(n_steps))
         return s
 
+    def llg_midpoint(self, spins: np.ndarray, n_steps: int, xi: Optional[np.ndarray] = None) -> np.ndarray:
+        """n_steps of sim::LLG_Midpoint (vref_llg_midpoint)."""
+        s = np.ascontiguousarray(spins, dtype=np.float64).copy()
+        xi_c = np.ascontiguousarray(xi, dtype=np.float64) if xi is not None else None
+        alpha = np.ascontiguousarray(self.s.materials["alpha"], dtype=np.float64)
+        lib().vref_llg_midpoint.restype = None
+        lib().vref_llg_midpoint(C.byref(self.st), _p(s[0], _D), _p(s[1], _D), _p(s[2], _D), _p(xi_c, _D),
+                                _p(alpha, _D), C.c_int64(n_steps))
+        return s
+
     def heun_predict(self, spins: np.ndarray, xi: Optional[np.ndarray] = None):
         """Predictor half of one step (vref_heun_predict): returns (s', keep),
         keep being the 12n state the corrector half needs."""

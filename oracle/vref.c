@@ -252,6 +252,72 @@ void vref_llg_heun_step(const vref_sys* s, double* sx, double* sy, double* sz, c
    vref_heun_correct(s, sx, sy, sz, px, py, pz, work);
 }
 
+/* Cayley-transform rotation of sim::LLG_Midpoint (src/simulate/LLGMidpoint.cpp:
+ * 70-105 and 117-150): with F = H + alpha M x H and beta = -dt A / 2,
+ * out = (S (1 - b2 F.F) + 2 (beta F x S + F b2 F.S)) / (1 + b2 F.F), b2 = beta^2. */
+static inline void midpoint_rotate(double alpha, double beta, const double M[3], const double S[3],
+                                   const double H[3], double out[3]) {
+   const double beta2 = beta * beta;
+   const double F[3] = {H[0] + alpha * (M[1] * H[2] - M[2] * H[1]),
+                        H[1] + alpha * (M[2] * H[0] - M[0] * H[2]),
+                        H[2] + alpha * (M[0] * H[1] - M[1] * H[0])};
+   const double FdotF = F[0] * F[0] + F[1] * F[1] + F[2] * F[2];
+   const double beta2FdotS = beta2 * (F[0] * S[0] + F[1] * S[1] + F[2] * S[2]);
+   const double c1 = 1.0 / (1.0 + beta2 * FdotF);
+   const double c2 = 1.0 - beta2 * FdotF;
+   out[0] = c1 * (S[0] * c2 + 2.0 * (beta * (F[1] * S[2] - F[2] * S[1]) + F[0] * beta2FdotS));
+   out[1] = c1 * (S[1] * c2 + 2.0 * (beta * (F[2] * S[0] - F[0] * S[2]) + F[1] * beta2FdotS));
+   out[2] = c1 * (S[2] * c2 + 2.0 * (beta * (F[0] * S[1] - F[1] * S[0]) + F[2] * beta2FdotS));
+}
+
+/* sim::LLG_Midpoint (src/simulate/LLGMidpoint.cpp:48-150): midpoint
+ * M = (S + R(S; F(S, H(S)))) / 2 (not renormalised), then
+ * S1 = R(S; F(M, H_spin(M) + H_ext)) with the external field of the first half.
+ * work: 12n doubles. */
+void vref_llg_midpoint_step(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,
+                            const double* alpha, double* work) {
+   const int n = s->n;
+   double* hsx = work;          double* hsy = work + n;      double* hsz = work + 2 * n;
+   double* hex = work + 3 * n;  double* hey = work + 4 * n;  double* hez = work + 5 * n;
+   double* ix = work + 6 * n;   double* iy = work + 7 * n;   double* iz = work + 8 * n;
+   double* mx = work + 9 * n;   double* my = work + 10 * n;  double* mz = work + 11 * n;
+   memcpy(ix, sx, sizeof(double) * n);
+   memcpy(iy, sy, sizeof(double) * n);
+   memcpy(iz, sz, sizeof(double) * n);
+   vref_spin_fields(s, sx, sy, sz, hsx, hsy, hsz);
+   vref_external_fields(s, xi, hex, hey, hez);
+   for (int atom = 0; atom < n; atom++) {
+      const int m = s->type[atom];
+      const double beta = -1.0 * s->dt * s->A[m] * 0.5;
+      const double S[3] = {sx[atom], sy[atom], sz[atom]};
+      const double H[3] = {hsx[atom] + hex[atom], hsy[atom] + hey[atom], hsz[atom] + hez[atom]};
+      double R[3];
+      midpoint_rotate(alpha[m], beta, S, S, H, R);
+      mx[atom] = (S[0] + R[0]) * 0.5;
+      my[atom] = (S[1] + R[1]) * 0.5;
+      mz[atom] = (S[2] + R[2]) * 0.5;
+   }
+   vref_spin_fields(s, mx, my, mz, hsx, hsy, hsz);
+   for (int atom = 0; atom < n; atom++) {
+      const int m = s->type[atom];
+      const double beta = -1.0 * s->dt * s->A[m] * 0.5;
+      const double M[3] = {mx[atom], my[atom], mz[atom]};
+      const double S[3] = {ix[atom], iy[atom], iz[atom]};
+      const double H[3] = {hsx[atom] + hex[atom], hsy[atom] + hey[atom], hsz[atom] + hez[atom]};
+      double R[3];
+      midpoint_rotate(alpha[m], beta, M, S, H, R);
+      sx[atom] = R[0]; sy[atom] = R[1]; sz[atom] = R[2];
+   }
+}
+
+void vref_llg_midpoint(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,
+                       const double* alpha, int64_t n_steps) {
+   double* work = (double*)malloc(sizeof(double) * 12 * (size_t)s->n);
+   for (int64_t t = 0; t < n_steps; t++)
+      vref_llg_midpoint_step(s, sx, sy, sz, xi ? xi + t * 3 * (int64_t)s->n : NULL, alpha, work);
+   free(work);
+}
+
 /* n_steps deterministic (T=0 or given-noise) steps; xi may be NULL or hold
  * n_steps * 3n values. */
 void vref_llg_heun(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,

@@ -59,6 +59,10 @@ void vref_heun_correct(const vref_sys* s, double* sx, double* sy, double* sz, co
                        const double* pz, double* keep);
 void vref_llg_heun_step(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,
                         double* work);
+void vref_llg_midpoint_step(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,
+                            const double* alpha, double* work);
+void vref_llg_midpoint(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,
+                       const double* alpha, int64_t n_steps);
 void vref_llg_heun(const vref_sys* s, double* sx, double* sy, double* sz, const double* xi,
                    int64_t n_steps);
 void vref_spin_energy(const vref_sys* s, const double* sx, const double* sy, const double* sz,

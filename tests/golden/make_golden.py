@@ -118,6 +118,20 @@ def sc6_derived_t600():
     save("sc6_derived_t600", d, keep)
 
 
+def sc8_midpoint():
+    """The LLG-Midpoint integrator (sim:integrator=llg-midpoint,
+    src/simulate/LLGMidpoint.cpp) on SC 8^3 periodic: 100 deterministic steps
+    at T=0, and 2 stochastic steps at T=300 K with the Gaussian stream."""
+    d = O.run_harness(sc_input(8, integrator="llg-midpoint"), {"m.mat": SC_MAT},
+                      ["--system", "--steps", 100, "--snaps", "1,100"])
+    keep = [f"s{c}_{t}" for t in (0, 1, 100) for c in "xyz"]
+    save("sc8_midpoint_t0", d, keep)
+    d = O.run_harness(sc_input(8, T=300.0, integrator="llg-midpoint"), {"m.mat": SC_MAT},
+                      ["--system", "--steps", 2, "--snaps", "1,2", "--noise", 2])
+    keep = [f"s{c}_{t}" for t in (0, 1, 2) for c in "xyz"] + ["xi_1", "xi_2"]
+    save("sc8_midpoint_t300", d, keep)
+
+
 HO_MAT = """material:num-materials=1
 material[1]:material-name=A
 material[1]:damping-constant=0.1
@@ -237,7 +251,7 @@ def mc_sc16_curie():
 
 
 ALL = [sc20_t0, sc8_t0, sc10_t300, sc6_open_t300, fcc4_dmi_t300, fcc4_dmi_t0, single_spin_applied, mc_sc16_curie,
-       fcc10_dipole_tensor, fcc10_dipole_macrocell, sc6_aniso_ho, fcc4_neel_rot, sc6_derived_t600]
+       fcc10_dipole_tensor, fcc10_dipole_macrocell, sc6_aniso_ho, fcc4_neel_rot, sc6_derived_t600, sc8_midpoint]
 
 if __name__ == "__main__":
     names = sys.argv[1:]

@@ -283,3 +283,24 @@ def test_status_flags_nonfinite(V):
         with pytest.raises(V.VGPUError) as e:
             sim.spins()
         assert e.value.code == V.ERR_NAN
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", TOL32)])
+def test_llg_midpoint_matches_reference(V, prec, tol):
+    """sim::LLG_Midpoint (src/simulate/LLGMidpoint.cpp) on the device: 100
+    deterministic steps of the reference's own SC 8^3 run, and two
+    stochastic steps with its Gaussian stream."""
+    s, d = load_golden("sc8_midpoint_t0")
+    with V.Simulation(s, precision=prec) as sim:
+        sim.llg_midpoint(1)
+        e1 = np.abs(sim.spins() - ref_spins(d, 1)).max()
+        sim.llg_midpoint(99)
+        e100 = np.abs(sim.spins() - ref_spins(d, 100)).max()
+    print(f"midpoint {prec}: step 1 {e1:.2e}, step 100 {e100:.2e}")
+    assert e1 <= tol and e100 <= tol
+    s, d = load_golden("sc8_midpoint_t300")
+    with V.Simulation(s, precision=prec) as sim:
+        for t in (1, 2):
+            sim.set_noise_replay(d[f"xi_{t}"])
+            sim.llg_midpoint(1)
+            assert np.abs(sim.spins() - ref_spins(d, t)).max() <= tol, t

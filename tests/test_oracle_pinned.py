@@ -160,3 +160,22 @@ def test_derived_statistics():
     np.testing.assert_allclose(sus, d["sus_system"], rtol=1e-9)
     np.testing.assert_allclose(sh, d["spec_heat_system"][0], rtol=1e-9)
     np.testing.assert_allclose(std, d["std_material"], rtol=1e-7)
+
+
+def test_llg_midpoint_deterministic():
+    """sim::LLG_Midpoint (src/simulate/LLGMidpoint.cpp): 100 T=0 steps."""
+    s, d = load_golden("sc8_midpoint_t0")
+    o = O.OracleSystem(s)
+    got = o.llg_midpoint(s.spins, 1)
+    assert np.abs(got - ref_spins(d, 1)).max() < 1e-13
+    got = o.llg_midpoint(got, 99)
+    assert np.abs(got - ref_spins(d, 100)).max() < 1e-12
+
+
+def test_llg_midpoint_replayed_noise():
+    s, d = load_golden("sc8_midpoint_t300")
+    o = O.OracleSystem(s)
+    got = s.spins
+    for t in (1, 2):
+        got = o.llg_midpoint(got, 1, xi=d[f"xi_{t}"])
+        assert np.abs(got - ref_spins(d, t)).max() < 1e-12, t

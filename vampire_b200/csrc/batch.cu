@@ -73,12 +73,12 @@ __global__ void batch_persistent_kernel(LLGArgs<R> a, const int* __restrict__ gr
       a.step = step0 + (uint64_t)s;
       for (int q = q0; q < q1; ++q) {
          const int k = grp_sys[q];
-         for (int i = off[k] + t; i < off[k + 1]; i += stride) llg_predict_atom<R, FMT, 1, false>(a, i);
+         for (int i = off[k] + t; i < off[k + 1]; i += stride) llg_predict_atom<R, FMT, 1, VAR_HEUN>(a, i);
       }
       cl.sync();  // every s' of the cluster's systems written and visible
       for (int q = q0; q < q1; ++q) {
          const int k = grp_sys[q];
-         for (int i = off[k] + t; i < off[k + 1]; i += stride) llg_correct_atom<R, FMT, 1, false>(a, i);
+         for (int i = off[k] + t; i < off[k + 1]; i += stride) llg_correct_atom<R, FMT, 1, VAR_HEUN>(a, i);
       }
       cl.sync();  // s1 complete before the next predictor gathers it
    }

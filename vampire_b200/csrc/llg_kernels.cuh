@@ -67,52 +67,103 @@ __device__ __forceinline__ void llg_correct_finish(const LLGArgs<R>& a, int i, c
    a.ax[i] = Sn[0] * r; a.ay[i] = Sn[1] * r; a.az[i] = Sn[2] * r;
 }
 
-// Predictor of atom i: s' = n(s0 + dt f(s0, H)).  LOAD = 1 reads neighbour
-// spins through L2 (they may have been written earlier in the same launch).
-template <typename R, int FMT, int LOAD, bool EXT = true>
+// Cayley-transform rotation of sim::LLG_Midpoint (src/simulate/LLGMidpoint.cpp:
+// 70-105, 117-150): F = H + alpha M x H, b2 = beta^2,
+// out = (S (1 - b2 F.F) + 2 (beta F x S + F b2 F.S)) / (1 + b2 F.F).
+template <typename R>
+__device__ __forceinline__ void midpoint_rotate(R alpha, R beta, const R M[3], const R S[3], const R H[3],
+                                                R out[3]) {
+   const R beta2 = beta * beta;
+   const R F[3] = {H[0] + alpha * (M[1] * H[2] - M[2] * H[1]), H[1] + alpha * (M[2] * H[0] - M[0] * H[2]),
+                   H[2] + alpha * (M[0] * H[1] - M[1] * H[0])};
+   const R FdotF = F[0] * F[0] + F[1] * F[1] + F[2] * F[2];
+   const R beta2FdotS = beta2 * (F[0] * S[0] + F[1] * S[1] + F[2] * S[2]);
+   const R c1 = (R)1 / ((R)1 + beta2 * FdotF);
+   const R c2 = (R)1 - beta2 * FdotF;
+   out[0] = c1 * (S[0] * c2 + (R)2 * (beta * (F[1] * S[2] - F[2] * S[1]) + F[0] * beta2FdotS));
+   out[1] = c1 * (S[1] * c2 + (R)2 * (beta * (F[2] * S[0] - F[0] * S[2]) + F[1] * beta2FdotS));
+   out[2] = c1 * (S[2] * c2 + (R)2 * (beta * (F[0] * S[1] - F[1] * S[0]) + F[2] * beta2FdotS));
+}
+
+// midpoint first half: M = (S0 + R(S0; F(S0, H))) / 2, not renormalised
+template <typename R>
+__device__ __forceinline__ void mid_predict_finish(const LLGArgs<R>& a, int i, const MatParams<R>& m, const R S0[3],
+                                                   const R H[3]) {
+   R r[3];
+   midpoint_rotate<R>(m.alpha, m.beta_mid, S0, S0, H, r);
+   a.bx[i] = (S0[0] + r[0]) * (R)0.5;
+   a.by[i] = (S0[1] + r[1]) * (R)0.5;
+   a.bz[i] = (S0[2] + r[2]) * (R)0.5;
+}
+
+// midpoint second half: S1 = R(S0; F(M, H(M))), written over S0
+template <typename R>
+__device__ __forceinline__ void mid_correct_finish(const LLGArgs<R>& a, int i, const MatParams<R>& m, const R S0[3],
+                                                   const R M[3], const R H[3]) {
+   R r[3];
+   midpoint_rotate<R>(m.alpha, m.beta_mid, M, S0, H, r);
+   const R n2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+   if (!(n2 > (R)0.25 && n2 < (R)4)) atomicOr(a.status, 1);  // non-finite or runaway
+   a.ax[i] = r[0]; a.ay[i] = r[1]; a.az[i] = r[2];
+}
+
+// Predictor of atom i: s' = n(s0 + dt f(s0, H)) (Heun) or the midpoint M.
+// LOAD = 1 reads neighbour spins through L2 (they may have been written
+// earlier in the same launch).
+template <typename R, int FMT, int LOAD, int VAR = VAR_HEUN_EXT>
 __device__ __forceinline__ void llg_predict_atom(const LLGArgs<R>& a, int i) {
    const int mi = a.mat ? __ldg(a.mat + i) : 0;
    const MatParams<R> m = a.mp[mi];
    const R S0[3] = {a.ax[i], a.ay[i], a.az[i]};
    R H[3], E[3];
-   spin_field<R, FMT, LOAD, false, EXT>(a, i, mi, m, a.ax, a.ay, a.az, S0, H);
+   spin_field<R, FMT, LOAD, false, VAR != VAR_HEUN>(a, i, mi, m, a.ax, a.ay, a.az, S0, H);
    external_field<R>(a, i, m, true, E);
    H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
-   llg_predict_finish<R>(a, i, m, S0, H);
+   if (VAR == VAR_MIDPOINT) mid_predict_finish<R>(a, i, m, S0, H);
+   else llg_predict_finish<R>(a, i, m, S0, H);
 }
 
-// Corrector of atom i: s1 = n(s0 + dt/2 (f0 + f(s', H'))), written over s0.
-template <typename R, int FMT, int LOAD, bool EXT = true>
+// Corrector of atom i: s1 = n(s0 + dt/2 (f0 + f(s', H'))) (Heun) or the
+// midpoint's second half, written over s0.
+template <typename R, int FMT, int LOAD, int VAR = VAR_HEUN_EXT>
 __device__ __forceinline__ void llg_correct_atom(const LLGArgs<R>& a, int i) {
    const int mi = a.mat ? __ldg(a.mat + i) : 0;
    const MatParams<R> m = a.mp[mi];
    const R S0[3] = {a.ax[i], a.ay[i], a.az[i]};
    const R S1[3] = {a.bx[i], a.by[i], a.bz[i]};
    R H[3], E[3];
-   spin_field<R, FMT, LOAD, false, EXT>(a, i, mi, m, a.bx, a.by, a.bz, S1, H);
+   spin_field<R, FMT, LOAD, false, VAR != VAR_HEUN>(a, i, mi, m, a.bx, a.by, a.bz, S1, H);
    external_field<R>(a, i, m, true, E);
    H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
-   llg_correct_finish<R>(a, i, m, S0, S1, H);
+   if (VAR == VAR_MIDPOINT) mid_correct_finish<R>(a, i, m, S0, S1, H);
+   else llg_correct_finish<R>(a, i, m, S0, S1, H);
 }
 
-template <typename R, int FMT, int MODE, bool EXT>
+template <typename R, int FMT, int MODE, int VAR>
 __global__ void __launch_bounds__(256) llg_pass_kernel(const LLGArgs<R> a) {
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    if (i >= (MODE == PASS_FIELD ? a.n : a.n_upd)) return;
    if (MODE == PASS_PREDICTOR) {
-      llg_predict_atom<R, FMT, 0, EXT>(a, i);
+      llg_predict_atom<R, FMT, 0, VAR>(a, i);
    } else if (MODE == PASS_CORRECTOR) {
-      llg_correct_atom<R, FMT, 0, EXT>(a, i);
+      llg_correct_atom<R, FMT, 0, VAR>(a, i);
    } else {
       // field of s0: exchange, anisotropy, applied and dipole terms (no thermal term)
       const int mi = a.mat ? __ldg(a.mat + i) : 0;
       const MatParams<R> m = a.mp[mi];
       const R S0[3] = {a.ax[i], a.ay[i], a.az[i]};
       R H[3], E[3];
-      spin_field<R, FMT, 0, false, EXT>(a, i, mi, m, a.ax, a.ay, a.az, S0, H);
+      spin_field<R, FMT, 0, false, VAR != VAR_HEUN>(a, i, mi, m, a.ax, a.ay, a.az, S0, H);
       external_field<R>(a, i, m, false, E);
       a.fx[i] = H[0] + E[0]; a.fy[i] = H[1] + E[1]; a.fz[i] = H[2] + E[2];
    }
+}
+
+template <typename R, int FMT, int VAR>
+inline void launch_mode(const LLGArgs<R>& a, int mode, int grid, int bs, cudaStream_t st) {
+   if (mode == PASS_PREDICTOR) llg_pass_kernel<R, FMT, PASS_PREDICTOR, VAR><<<grid, bs, 0, st>>>(a);
+   else if (mode == PASS_CORRECTOR) llg_pass_kernel<R, FMT, PASS_CORRECTOR, VAR><<<grid, bs, 0, st>>>(a);
+   else llg_pass_kernel<R, FMT, PASS_FIELD, VAR><<<grid, bs, 0, st>>>(a);
 }
 
 template <typename R, int FMT>
@@ -120,15 +171,9 @@ inline cudaError_t launch_fmt(const LLGArgs<R>& a, int mode, cudaStream_t st) {
    const int bs = 256;
    const int grid = ((mode == PASS_FIELD ? a.n : a.n_upd) + bs - 1) / bs;
    if (grid == 0) return cudaSuccess;
-   if (a.aniso_ext) {
-      if (mode == PASS_PREDICTOR) llg_pass_kernel<R, FMT, PASS_PREDICTOR, true><<<grid, bs, 0, st>>>(a);
-      else if (mode == PASS_CORRECTOR) llg_pass_kernel<R, FMT, PASS_CORRECTOR, true><<<grid, bs, 0, st>>>(a);
-      else llg_pass_kernel<R, FMT, PASS_FIELD, true><<<grid, bs, 0, st>>>(a);
-   } else {
-      if (mode == PASS_PREDICTOR) llg_pass_kernel<R, FMT, PASS_PREDICTOR, false><<<grid, bs, 0, st>>>(a);
-      else if (mode == PASS_CORRECTOR) llg_pass_kernel<R, FMT, PASS_CORRECTOR, false><<<grid, bs, 0, st>>>(a);
-      else llg_pass_kernel<R, FMT, PASS_FIELD, false><<<grid, bs, 0, st>>>(a);
-   }
+   if (a.integrator == INTEG_MIDPOINT && mode != PASS_FIELD) launch_mode<R, FMT, VAR_MIDPOINT>(a, mode, grid, bs, st);
+   else if (a.aniso_ext) launch_mode<R, FMT, VAR_HEUN_EXT>(a, mode, grid, bs, st);
+   else launch_mode<R, FMT, VAR_HEUN>(a, mode, grid, bs, st);
    return cudaGetLastError();
 }
 

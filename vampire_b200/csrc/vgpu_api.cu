@@ -318,6 +318,8 @@ int refresh_materials_typed(vgpu_ctx* h) {
       o.kc4 = (R)q.kc4;
       o.hlx = (R)q.applied_field[0]; o.hly = (R)q.applied_field[1]; o.hlz = (R)q.applied_field[2];
       o.mu_s_muB = (R)(q.mu_s_SI / 9.27400915e-24);
+      o.alpha = (R)q.alpha;
+      o.beta_mid = (R)(-1.0 * p.dt * q.one_oneplusalpha_sq * 0.5);
       o.ku4 = S.ku4_h.empty() ? (R)0 : (R)S.ku4_h[m];
       o.ku6 = S.ku6_h.empty() ? (R)0 : (R)S.ku6_h[m];
       o.kc6 = S.kc6_h.empty() ? (R)0 : (R)S.kc6_h[m];
@@ -448,10 +450,10 @@ static cudaError_t launch_step_pass(vgpu_ctx* h, const LLGArgs<R>& a, int mode, 
 
 // increment buffers and the staged launch shape, before any pass
 template <typename R>
-static int prepare_passes(vgpu_ctx* h, bool* staged_out) {
+static int prepare_passes(vgpu_ctx* h, bool* staged_out, int integrator = INTEG_HEUN) {
    int rc0 = ensure_increment<R>(h);
    if (rc0) return rc0;
-   const bool staged = use_staged<R>(h);
+   const bool staged = integrator == INTEG_HEUN && use_staged<R>(h);
    if (staged && h->sys.stage.grid == 0) {
       StageCfg c;
       c.sl = h->stage_sl;
@@ -467,8 +469,9 @@ static int prepare_passes(vgpu_ctx* h, bool* staged_out) {
 
 // one fused pass; the corrector completes the step (counter, dipole cadence)
 template <typename R>
-static int run_pass(vgpu_ctx* h, int mode, bool staged) {
+static int run_pass(vgpu_ctx* h, int mode, bool staged, int integrator = INTEG_HEUN) {
    LLGArgs<R> a = make_args<R>(h);
+   a.integrator = integrator;
    const int kind = mode == PASS_PREDICTOR ? PROF_PREDICTOR : PROF_CORRECTOR;
    h->prof_begin(kind);
    cudaError_t e = launch_step_pass<R>(h, a, mode, staged);
@@ -481,12 +484,12 @@ static int run_pass(vgpu_ctx* h, int mode, bool staged) {
 }
 
 template <typename R>
-static int llg_steps_typed(vgpu_ctx* h, uint64_t n_steps) {
+static int llg_steps_typed(vgpu_ctx* h, uint64_t n_steps, int integrator = INTEG_HEUN) {
    bool staged = false;
-   int rc = prepare_passes<R>(h, &staged);
+   int rc = prepare_passes<R>(h, &staged, integrator);
    for (uint64_t t = 0; t < n_steps && !rc; ++t) {
-      rc = run_pass<R>(h, PASS_PREDICTOR, staged);
-      if (!rc) rc = run_pass<R>(h, PASS_CORRECTOR, staged);
+      rc = run_pass<R>(h, PASS_PREDICTOR, staged, integrator);
+      if (!rc) rc = run_pass<R>(h, PASS_CORRECTOR, staged, integrator);
    }
    return rc;
 }
@@ -902,6 +905,15 @@ static int noise_typed(vgpu_handle h, uint64_t step, double* xi) {
    const int n = S.n;
    double* out[3] = {xi, xi + n, xi + 2 * (size_t)n};
    return get_vec_typed<R>(h, S.f, out);
+}
+
+extern "C" int vgpu_llg_midpoint(vgpu_handle h, uint64_t n_steps) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (!(h->params.dt > 0.0)) return set_err(h, VGPU_ERR_STATE, "vgpu_set_params not called");
+   cudaSetDevice(h->device);
+   return h->prec == VGPU_PREC_FP64 ? llg_steps_typed<double>(h, n_steps, INTEG_MIDPOINT)
+                                    : llg_steps_typed<float>(h, n_steps, INTEG_MIDPOINT);
 }
 
 extern "C" int vgpu_llg_pass(vgpu_handle h, int pass) {

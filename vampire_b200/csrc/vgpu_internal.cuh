@@ -36,6 +36,7 @@ struct MatParams {
    R hlx, hly, hlz;   // local applied field (0 if disabled)
    R mu_s_muB;        // moment in Bohr magnetons (stats)
    R dhx, dhy, dhz;   // field change over a linear sweep (batched systems), added as dh * min(step, n)/n
+   R alpha, beta_mid; // LLG-Midpoint: damping and -dt A / 2 (LLGMidpoint.cpp:72-73)
    R ku4, ku6, kc6;   // higher-order reduced constants [T] (0 unless enabled)
    R kcb[9];          // rotated cubic basis e1, e2, e3
 };
@@ -64,6 +65,7 @@ struct LLGArgs {
    const MatParams<R>* mp;   // [M]
    int uniaxial, cubic;
    int aniso_ext;            // AnisoExt bits
+   int integrator;           // INTEG_HEUN or INTEG_MIDPOINT
    const R* neel;            // [9][n_alloc] per-atom Neel tensors (ANI_NEEL), row-major components
    R hx, hy, hz;             // global applied field
    int local_field;          // add MatParams::hl*
@@ -91,6 +93,10 @@ struct LLGArgs {
 };
 
 enum PassMode : int { PASS_PREDICTOR = 0, PASS_CORRECTOR = 1, PASS_FIELD = 2 };
+enum Integrator : int { INTEG_HEUN = 0, INTEG_MIDPOINT = 1 };
+// compiled pass variants: Heun without / with the higher-order anisotropy
+// terms, and the midpoint integrator (with them)
+enum PassVariant : int { VAR_HEUN = 0, VAR_HEUN_EXT = 1, VAR_MIDPOINT = 2 };
 
 // launch the fused Heun pass for the given format/mode (llg_kernels.cu)
 template <typename R>

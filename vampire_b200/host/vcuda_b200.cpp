@@ -255,6 +255,15 @@ void llg_heun() {
 
 void stats_update() { stats::update(); }
 
+// LLG-Midpoint step on the GPU (sim::LLG_Midpoint, src/simulate/LLGMidpoint.cpp);
+// hdr/cuda.hpp has no such entry: a host that adds gpu::llg_midpoint()
+// forwards it here from the llg-midpoint case of sim::integrate_serial.
+void llg_midpoint();
+void llg_midpoint() {
+   sync_params();
+   fail(vgpu_llg_midpoint(g_h, 1), "llg_midpoint");
+}
+
 // Metropolis sweep on the GPU: N angle-move trials, one per atom, in colour
 // order (the reference's montecarlo::mc_step, src/montecarlo/mc.cpp:29-127,
 // makes N random-site trials on the host).  hdr/cuda.hpp has no such entry;

@@ -289,6 +289,10 @@ class Simulation:
     def llg_heun(self, n_steps: int = 1) -> None:
         self._check(lib().vgpu_llg_heun(self._h, C.c_uint64(n_steps)))
 
+    def llg_midpoint(self, n_steps: int = 1) -> None:
+        """n_steps of the LLG-Midpoint integrator (vgpu_llg_midpoint)."""
+        self._check(lib().vgpu_llg_midpoint(self._h, C.c_uint64(n_steps)))
+
     # -- shards ------------------------------------------------------------
     def llg_pass(self, which: int) -> None:
         """One fused pass: PASS_PREDICTOR or PASS_CORRECTOR (vgpu_llg_pass)."""
