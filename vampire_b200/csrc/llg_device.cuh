@@ -120,7 +120,38 @@ __device__ __forceinline__ void exchange_gather_w(const LLGArgs<R>& a, int base,
                                                   const R* __restrict__ sy, const R* __restrict__ sz, R& hx, R& hy,
                                                   R& hz, const int4* srec) {
    const R* __restrict__ tab = a.jtab;
-   if (FMT == FMT_DMI_TAB) {
+   if (FMT == FMT_DMI_TAB && STAGED) {
+      // records in shared memory: take only the neighbour words first so that
+      // the registers hold the 3W gathered spins (all in flight together), and
+      // re-read each bond's d vector from shared memory where it is used
+      const int* sw = reinterpret_cast<const int*>(srec);
+      int c[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k) c[k] = sw[128 * k];
+      R x[W], y[W], z[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+         const int j = c[k] & a.idx_mask;
+         x[k] = ld_src(sx + j, LOAD); y[k] = ld_src(sy + j, LOAD); z[k] = ld_src(sz + j, LOAD);
+      }
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+         const int mj = a.mat_shift ? (c[k] >> a.mat_shift) : 0;
+         const R dx = __int_as_float(sw[128 * k + 1]), dy = __int_as_float(sw[128 * k + 2]),
+                 dz = __int_as_float(sw[128 * k + 3]);
+         if (a.tab_scalar) {
+            const R J = __ldg(a.jtab_s + mi * a.M + mj);
+            hx += J * x[k] + (dy * z[k] - dz * y[k]);
+            hy += J * y[k] + (dz * x[k] - dx * z[k]);
+            hz += J * z[k] + (dx * y[k] - dy * x[k]);
+         } else {
+            const R* t = tab + 3 * (mi * a.M + mj);
+            hx += __ldg(t) * x[k] + (dy * z[k] - dz * y[k]);
+            hy += __ldg(t + 1) * y[k] + (dz * x[k] - dx * z[k]);
+            hz += __ldg(t + 2) * z[k] + (dx * y[k] - dy * x[k]);
+         }
+      }
+   } else if (FMT == FMT_DMI_TAB) {
       int4 rec[W];
 #pragma unroll
       for (int k = 0; k < W; ++k) rec[k] = STAGED ? srec[32 * k] : __ldg(a.rec + base + 32 * k);
