@@ -249,6 +249,26 @@ def bench_mc(device, L=50, eq=5000, av=10000, every=10):
             "acceptance": 1.0 - rej / moves, "Tc_K": tc, "m_T": [round(float(x), 5) for x in m_T]}
 
 
+def bench_adjoint(device, L=32, steps=2000):
+    """Adjoint LLG-Heun on SC 32^3 (32,768 spins), T=0, 2,000 steps: the
+    gradient of the trajectory loss w.r.t. (J, Ku, H) at J=11.2e-21 J,
+    Ku=6.69e-24 J, H=(0,0,0.4) T against the target m_z(t) of J=10e-21 J,
+    Ku=5e-24 J, H=(0,0,0.5) T; FP64, sqrt(N) checkpointing.  Timed around the
+    single C-ABI call (forward with checkpoints, segment recomputation and
+    the backward sweep)."""
+    from vampire_b200 import adjoint as A
+    run = A.AdjointRunner(L=L, device=device)
+    target = run.trajectory(10e-21, 5e-24, (0.0, 0.0, 0.5), steps)
+    run.loss_and_grad(11.2e-21, 6.69e-24, (0.0, 0.0, 0.4), target[:50])  # warm-up
+    t0 = time.perf_counter()
+    loss, grad = run.loss_and_grad(11.2e-21, 6.69e-24, (0.0, 0.0, 0.4), target)
+    dt = time.perf_counter() - t0
+    return {"workload": f"SC {L}^3, {steps} steps, loss = sum_t dt (m_z - target)^2, grad w.r.t. J, Ku, H (3)",
+            "spins": L ** 3, "steps": steps, "seconds": dt, "value": L ** 3 * steps / dt,
+            "unit": "spin-steps/s (forward + backward)", "precision": "fp64", "loss": loss,
+            "grad": [float(g) for g in grad], "checkpoints": int(-(-steps // int(steps ** 0.5 + 0.999999)))}
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -391,6 +411,7 @@ def main():
         sim.close()
         extra["batched"] = bench_batched(local)
         extra["monte_carlo"] = bench_mc(local)
+        extra["adjoint"] = bench_adjoint(local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
