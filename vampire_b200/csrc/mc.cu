@@ -33,15 +33,6 @@ struct MCState {
    std::vector<int> colour_host;      // [n]
    std::vector<int> colour_off;       // [ncolours+1] offsets into the atom list
    int* atoms = nullptr;              // [n] atoms sorted by colour
-   // colour-major copy of the SELL topology: the rows of colour c are
-   // crow_off[c]..crow_off[c+1]-1 (whole slices), row r holds atom catoms[r]
-   // (-1: padding row), so the index/coupling loads of a colour launch read
-   // whole 128-byte lines instead of every other lane of the atom-ordered rows
-   std::vector<int> crow_off;
-   int* catoms = nullptr;
-   int* cslice_off = nullptr;
-   int* ccol = nullptr;
-   void* cjb[9] = {nullptr};
    unsigned long long* rejects = nullptr;
    void* replay = nullptr;            // [4n] (x|y|z gaussians, uniform) in R
    bool use_replay = false;
@@ -53,10 +44,9 @@ static MCState* mc_of(vgpu_ctx* h) { return (MCState*)h->extras[1]; }
 
 template <typename R>
 struct MCArgs {
-   LLGArgs<R> a;           // slice_off/col/jb point at the colour-major copy
-   const int* atoms;       // atom of each row of this colour (-1: padding)
-   int row0;               // first colour-major row of this colour
-   int count;              // rows of this colour (whole slices)
+   LLGArgs<R> a;
+   const int* atoms;
+   int count;
    const R* sigma;      // [M] move width
    const R* beta;       // [M] mu_B / (kB T_rescaled)  (kBTBohr)
    const R* mu_ratio;   // [M] mu_s_SI / mu_B
@@ -88,13 +78,13 @@ template <typename R, int FMT>
 __global__ void __launch_bounds__(256) mc_colour_kernel(const MCArgs<R> p) {
    const int t = blockIdx.x * blockDim.x + threadIdx.x;
    bool rejected = false;
-   const int i = t < p.count ? __ldg(p.atoms + t) : -1;
-   if (i >= 0) {
+   if (t < p.count) {
       const LLGArgs<R>& a = p.a;
+      const int i = __ldg(p.atoms + t);
       const int mi = a.mat ? __ldg(a.mat + i) : 0;
       const MatParams<R> m = a.mp[mi];
       R h[3] = {0, 0, 0};
-      exchange_gather<R, FMT>(a, p.row0 + t, mi, a.ax, a.ay, a.az, h[0], h[1], h[2]);
+      exchange_gather<R, FMT>(a, i, mi, a.ax, a.ay, a.az, h[0], h[1], h[2]);
       // magnetostatic energy uses the mu0 Hd field (energy.cpp:123-126)
       if (a.cell) {
          const int c = __ldg(a.cell + i);
@@ -170,23 +160,9 @@ static cudaError_t mc_dispatch(const MCArgs<R>& p, int fmt, cudaStream_t st) {
    }
 }
 
-// colour-major topology: ccol/cjb[e] = col/jb[map[e]] (pad entry where map < 0)
-template <typename R>
-__global__ void colour_gather_kernel(const int* __restrict__ map, int64_t ne, const int* __restrict__ col, int pad,
-                                     int* __restrict__ ccol, int nper, const R* const* __restrict__ jb,
-                                     R* const* __restrict__ cjb) {
-   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x) {
-      const int src = map[e];
-      ccol[e] = src >= 0 ? col[src] : pad;
-      for (int q = 0; q < nper; ++q) cjb[q][e] = src >= 0 ? jb[q][src] : (R)0;
-   }
-}
-
 void mc_destroy(vgpu_ctx* h) {
    MCState* s = mc_of(h);
    if (!s) return;
-   cudaFree(s->catoms); cudaFree(s->cslice_off); cudaFree(s->ccol);
-   for (int q = 0; q < 9; ++q) cudaFree(s->cjb[q]);
    cudaFree(s->atoms);
    cudaFree(s->rejects);
    cudaFree(s->replay);
@@ -197,84 +173,6 @@ void mc_destroy(vgpu_ctx* h) {
 }  // namespace vgpu
 
 using namespace vgpu;
-
-// Colour-major SELL rows (see MCState) from the atom-ordered SELL arrays of
-// the upload (same slice widths rule: the widest row of each 32-row slice).
-template <typename R>
-static int build_colour_sell(vgpu_ctx* h, MCState* s, const std::vector<int>& order) {
-   SysDev& S = h->sys;
-   const int n = S.n, nc = s->ncolours;
-   std::vector<int> deg(n);
-   for (int i = 0; i < n; ++i) deg[i] = (int)(S.row_host[i + 1] - S.row_host[i]);
-   std::vector<int64_t> off(S.nslices + 1, 0);
-   for (int sl = 0; sl < S.nslices; ++sl) {
-      int w = 0;
-      for (int l = 0; l < 32; ++l)
-         if (sl * 32 + l < n) w = std::max(w, deg[sl * 32 + l]);
-      off[sl + 1] = off[sl] + 32 * (int64_t)w;
-   }
-   s->crow_off.assign(nc + 1, 0);
-   for (int c = 0; c < nc; ++c) {
-      const int cnt = s->colour_off[c + 1] - s->colour_off[c];
-      s->crow_off[c + 1] = s->crow_off[c] + (cnt + 31) / 32 * 32;
-   }
-   const int nrows = s->crow_off[nc], ncsl = nrows / 32;
-   std::vector<int> catoms(nrows, -1);
-   for (int c = 0; c < nc; ++c)
-      for (int k = s->colour_off[c]; k < s->colour_off[c + 1]; ++k) catoms[s->crow_off[c] + k - s->colour_off[c]] = order[k];
-   std::vector<int> csoff(ncsl + 1, 0);
-   for (int sl = 0; sl < ncsl; ++sl) {
-      int w = 0;
-      for (int l = 0; l < 32; ++l) {
-         const int i = catoms[sl * 32 + l];
-         if (i >= 0) w = std::max(w, deg[i]);
-      }
-      csoff[sl + 1] = csoff[sl] + 32 * w;
-   }
-   const int64_t ne = csoff[ncsl];
-   std::vector<int> map(std::max<int64_t>(ne, 1), -1);
-   for (int r = 0; r < nrows; ++r) {
-      const int i = catoms[r];
-      if (i < 0) continue;
-      for (int k = 0; k < deg[i]; ++k)
-         map[csoff[r >> 5] + 32 * k + (r & 31)] = (int)(off[i >> 5] + 32 * k + (i & 31));
-   }
-   const int nper = S.fmt == FMT_ISO_BOND ? 1 : (S.fmt == FMT_VEC_BOND || S.fmt == FMT_DMI_TAB) ? 3
-                  : S.fmt == FMT_TENSOR_BOND ? 9 : 0;
-   cudaError_t e = cudaSuccess;
-   int* dmap = nullptr;
-   const R** djb = nullptr;
-   R** dcjb = nullptr;
-   auto up = [&](void** dst, const void* src, size_t bytes) {
-      if (e != cudaSuccess) return;
-      e = cudaMalloc(dst, std::max<size_t>(bytes, 16));
-      if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
-   };
-   up((void**)&s->catoms, catoms.data(), sizeof(int) * nrows);
-   up((void**)&s->cslice_off, csoff.data(), sizeof(int) * (ncsl + 1));
-   up((void**)&dmap, map.data(), sizeof(int) * map.size());
-   if (e == cudaSuccess) e = cudaMalloc(&s->ccol, sizeof(int) * std::max<int64_t>(ne, 1));
-   std::vector<const R*> hjb(9, nullptr);
-   std::vector<R*> hcjb(9, nullptr);
-   for (int q = 0; q < nper && e == cudaSuccess; ++q) {
-      e = cudaMalloc(&s->cjb[q], sizeof(R) * std::max<int64_t>(ne, 1));
-      hjb[q] = (const R*)S.jb[q];
-      hcjb[q] = (R*)s->cjb[q];
-   }
-   up((void**)&djb, hjb.data(), sizeof(R*) * 9);
-   up((void**)&dcjb, hcjb.data(), sizeof(R*) * 9);
-   if (e == cudaSuccess && ne > 0) {
-      const int blocks = (int)std::min<int64_t>((ne + 255) / 256, 148 * 16);
-      colour_gather_kernel<R><<<blocks, 256, 0, h->stream>>>(dmap, ne, (const int*)S.col, S.n_alloc - 1, s->ccol,
-                                                             nper, djb, dcjb);
-      e = cudaGetLastError();
-   }
-   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-   cudaFree(dmap);
-   cudaFree(djb);
-   cudaFree(dcjb);
-   return cuda_err(h, e, "mc colour-major topology");
-}
 
 // Host-side greedy colouring of the (symmetrised) exchange graph.
 static int greedy_colour(int n, const std::vector<std::vector<int>>& adj, std::vector<int>& colour) {
@@ -342,8 +240,6 @@ extern "C" int vgpu_mc_setup(vgpu_handle h, const int32_t* colour_in, int32_t* n
    cudaMemcpyAsync(s->atoms, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->stream);
    cudaMemsetAsync(s->rejects, 0, sizeof(unsigned long long), h->stream);
    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_err(h, e, "mc setup");
-   int rc = h->prec == VGPU_PREC_FP64 ? build_colour_sell<double>(h, s, order) : build_colour_sell<float>(h, s, order);
-   if (rc) return rc;
    if (n_colours_out) *n_colours_out = nc;
    return VGPU_OK;
 }
@@ -421,13 +317,9 @@ static int mc_sweeps_typed(vgpu_handle h, uint64_t n_sweeps) {
       p.replay = s->use_replay ? (const R*)s->replay : nullptr;
       p.sweep = s->sweep;
       p.rejects = s->rejects;
-      p.a.slice_off = s->cslice_off;
-      p.a.col = s->ccol;
-      for (int q = 0; q < 9; ++q) p.a.jb[q] = (const R*)s->cjb[q];
       for (int c = 0; c < s->ncolours; ++c) {
-         p.atoms = s->catoms + s->crow_off[c];
-         p.row0 = s->crow_off[c];
-         p.count = s->crow_off[c + 1] - s->crow_off[c];
+         p.atoms = s->atoms + s->colour_off[c];
+         p.count = s->colour_off[c + 1] - s->colour_off[c];
          h->prof_begin(PROF_MC);
          cudaError_t e = mc_dispatch<R>(p, S.fmt, h->stream);
          h->prof_end(PROF_MC);
