@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--no-dipole", action="store_true", help="leave out the macrocell dipole field")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and Monte Carlo side results")
     ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--only", choices=["mc", "batched", "adjoint"], default=None,
+                    help="run one side workload alone and print its result (profiling)")
+    ap.add_argument("--mc-sweeps", type=int, nargs=2, default=(5000, 10000), metavar=("EQ", "AV"),
+                    help="Monte Carlo equilibration and averaging sweeps")
     return ap.parse_args()
 
 
@@ -315,6 +319,18 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
+    if args.only:
+        from vampire_b200 import build as vbuild
+        vbuild.build()
+        torch.cuda.set_device(local)
+        fn = {"mc": lambda: bench_mc(local, eq=args.mc_sweeps[0], av=args.mc_sweeps[1]),
+              "batched": lambda: bench_batched(local), "adjoint": lambda: bench_adjoint(local)}[args.only]
+        r = fn()
+        if rank == 0:
+            print(json.dumps({"only": args.only, **{k: v for k, v in r.items() if k != "m_T"}}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
 
     from vampire_b200 import build as vbuild
     from vampire_b200 import system as S
@@ -410,7 +426,7 @@ def main():
     if not args.no_extras:
         sim.close()
         extra["batched"] = bench_batched(local)
-        extra["monte_carlo"] = bench_mc(local)
+        extra["monte_carlo"] = bench_mc(local, eq=args.mc_sweeps[0], av=args.mc_sweeps[1])
         extra["adjoint"] = bench_adjoint(local)
 
     cpu = None
