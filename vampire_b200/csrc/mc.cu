@@ -38,32 +38,14 @@ struct MCState {
    bool use_replay = false;
    uint64_t sweep = 0;
    double moves = 0.0;
-   // Colour-major copy of the state and topology used by the sweeps: row r
-   // of colour c (rows crow_off[c]..crow_off[c+1]-1, whole slices) holds atom
-   // row_atom[r] (-1: padding); spins are copied in before and out after each
-   // vgpu_mc_sweep call, so a launch reads and writes one contiguous block of
-   // its own colour and gathers neighbours from the other colours' blocks.
-   // Row nrows is a zero spin for padded bonds.
-   bool rows_built = false;
-   std::vector<int> crow_off;
-   int nrows = 0;
-   int* row_atom = nullptr;   // [nrows]
-   int* atom_row = nullptr;   // [n]
-   int* row_mat = nullptr;    // [nrows] (M > 1)
-   void* rs[3] = {nullptr, nullptr, nullptr};  // [nrows + 1] spins in row order
-   int* rslice_off = nullptr; // [nrows/32 + 1]
-   int* rcol = nullptr;       // neighbour row | material bits
-   void* rjb[9] = {nullptr};  // per-bond couplings in row order
-   int rmat_shift = 0, ridx_mask = 0x7fffffff;
 };
 
 static MCState* mc_of(vgpu_ctx* h) { return (MCState*)h->extras[1]; }
 
 template <typename R>
 struct MCArgs {
-   LLGArgs<R> a;           // ROWS: state, materials and topology in colour-major row order
-   const int* atoms;       // atom of each thread (ROWS: of each row, -1 padding)
-   int row0;               // ROWS: first row of this colour
+   LLGArgs<R> a;
+   const int* atoms;
    int count;
    const R* sigma;      // [M] move width
    const R* beta;       // [M] mu_B / (kB T_rescaled)  (kBTBohr)
@@ -92,21 +74,17 @@ __device__ __forceinline__ R site_energy_delta(const LLGArgs<R>& a, int i, const
    return d;
 }
 
-// ROWS: thread t works on row row0 + t of the colour-major copy (state and
-// topology indexed by row q); random numbers and replay stay keyed by the
-// atom index i, so both layouts draw the same numbers for an atom.
-template <typename R, int FMT, bool ROWS>
+template <typename R, int FMT>
 __global__ void __launch_bounds__(256) mc_colour_kernel(const MCArgs<R> p) {
    const int t = blockIdx.x * blockDim.x + threadIdx.x;
    bool rejected = false;
-   const int i = t < p.count ? __ldg(p.atoms + t) : -1;
-   if (i >= 0) {
+   if (t < p.count) {
       const LLGArgs<R>& a = p.a;
-      const int q = ROWS ? p.row0 + t : i;
-      const int mi = a.mat ? __ldg(a.mat + q) : 0;
+      const int i = __ldg(p.atoms + t);
+      const int mi = a.mat ? __ldg(a.mat + i) : 0;
       const MatParams<R> m = a.mp[mi];
       R h[3] = {0, 0, 0};
-      exchange_gather<R, FMT>(a, q, mi, a.ax, a.ay, a.az, h[0], h[1], h[2]);
+      exchange_gather<R, FMT>(a, i, mi, a.ax, a.ay, a.az, h[0], h[1], h[2]);
       // magnetostatic energy uses the mu0 Hd field (energy.cpp:123-126)
       if (a.cell) {
          const int c = __ldg(a.cell + i);
@@ -116,7 +94,7 @@ __global__ void __launch_bounds__(256) mc_colour_kernel(const MCArgs<R> p) {
       } else if (a.hm_atom) {
          h[0] += __ldg(a.hm_atom + i); h[1] += __ldg(a.hm_atom + a.n + i); h[2] += __ldg(a.hm_atom + 2 * a.n + i);
       }
-      const R S[3] = {a.ax[q], a.ay[q], a.az[q]};
+      const R S[3] = {a.ax[i], a.ay[i], a.az[i]};
       R g0, g1, g2, u;
       if (p.replay) {
          g0 = p.replay[i]; g1 = p.replay[a.n + i]; g2 = p.replay[2 * a.n + i]; u = p.replay[3 * a.n + i];
@@ -154,7 +132,7 @@ __global__ void __launch_bounds__(256) mc_colour_kernel(const MCArgs<R> p) {
          accept = (sizeof(R) == 4 ? (R)expf((float)x) : (R)exp((double)x)) >= u;
       }
       if (accept) {
-         a.ax[q] = T[0]; a.ay[q] = T[1]; a.az[q] = T[2];
+         a.ax[i] = T[0]; a.ay[i] = T[1]; a.az[i] = T[2];
       } else {
          rejected = true;
       }
@@ -164,64 +142,27 @@ __global__ void __launch_bounds__(256) mc_colour_kernel(const MCArgs<R> p) {
 }
 
 template <typename R, int FMT>
-static cudaError_t launch_mc(const MCArgs<R>& p, bool rows, cudaStream_t st) {
+static cudaError_t launch_mc(const MCArgs<R>& p, cudaStream_t st) {
    if (p.count == 0) return cudaSuccess;
-   if (rows) mc_colour_kernel<R, FMT, true><<<(p.count + 255) / 256, 256, 0, st>>>(p);
-   else mc_colour_kernel<R, FMT, false><<<(p.count + 255) / 256, 256, 0, st>>>(p);
+   mc_colour_kernel<R, FMT><<<(p.count + 255) / 256, 256, 0, st>>>(p);
    return cudaGetLastError();
 }
 
 template <typename R>
-static cudaError_t mc_dispatch(const MCArgs<R>& p, int fmt, bool rows, cudaStream_t st) {
+static cudaError_t mc_dispatch(const MCArgs<R>& p, int fmt, cudaStream_t st) {
    switch (fmt) {
-      case FMT_ISO_TAB: return launch_mc<R, FMT_ISO_TAB>(p, rows, st);
-      case FMT_ISO_BOND: return launch_mc<R, FMT_ISO_BOND>(p, rows, st);
-      case FMT_VEC_TAB: return launch_mc<R, FMT_VEC_TAB>(p, rows, st);
-      case FMT_VEC_BOND: return launch_mc<R, FMT_VEC_BOND>(p, rows, st);
-      case FMT_DMI_TAB: return launch_mc<R, FMT_DMI_TAB>(p, rows, st);
-      default: return launch_mc<R, FMT_TENSOR_BOND>(p, rows, st);
-   }
-}
-
-// spins atom order <-> row order (pad rows and the zero row stay zero)
-template <typename R>
-__global__ void rows_in_kernel(int nrows, const int* __restrict__ row_atom, const R* __restrict__ sx,
-                               const R* __restrict__ sy, const R* __restrict__ sz, R* __restrict__ rx,
-                               R* __restrict__ ry, R* __restrict__ rz) {
-   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x) {
-      const int i = row_atom[r];
-      rx[r] = i >= 0 ? sx[i] : (R)0;
-      ry[r] = i >= 0 ? sy[i] : (R)0;
-      rz[r] = i >= 0 ? sz[i] : (R)0;
-   }
-}
-
-template <typename R>
-__global__ void rows_out_kernel(int n, const int* __restrict__ atom_row, const R* __restrict__ rx,
-                                const R* __restrict__ ry, const R* __restrict__ rz, R* __restrict__ sx,
-                                R* __restrict__ sy, R* __restrict__ sz) {
-   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-      const int r = atom_row[i];
-      sx[i] = rx[r]; sy[i] = ry[r]; sz[i] = rz[r];
-   }
-}
-
-// couplings of the row-order topology: rjb[q][e] = jb[q][map[e]] (0 where map < 0)
-template <typename R>
-__global__ void rows_gather_jb_kernel(const int* __restrict__ map, int64_t ne, const R* __restrict__ src,
-                                      R* __restrict__ dst) {
-   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x) {
-      const int k = map[e];
-      dst[e] = k >= 0 ? src[k] : (R)0;
+      case FMT_ISO_TAB: return launch_mc<R, FMT_ISO_TAB>(p, st);
+      case FMT_ISO_BOND: return launch_mc<R, FMT_ISO_BOND>(p, st);
+      case FMT_VEC_TAB: return launch_mc<R, FMT_VEC_TAB>(p, st);
+      case FMT_VEC_BOND: return launch_mc<R, FMT_VEC_BOND>(p, st);
+      case FMT_DMI_TAB: return launch_mc<R, FMT_DMI_TAB>(p, st);
+      default: return launch_mc<R, FMT_TENSOR_BOND>(p, st);
    }
 }
 
 void mc_destroy(vgpu_ctx* h) {
    MCState* s = mc_of(h);
    if (!s) return;
-   cudaFree(s->row_atom); cudaFree(s->atom_row); cudaFree(s->row_mat); cudaFree(s->rslice_off); cudaFree(s->rcol);
-   for (int q = 0; q < 3; ++q) cudaFree(s->rs[q]);
-   for (int q = 0; q < 9; ++q) cudaFree(s->rjb[q]);
    cudaFree(s->atoms);
    cudaFree(s->rejects);
    cudaFree(s->replay);
@@ -232,99 +173,6 @@ void mc_destroy(vgpu_ctx* h) {
 }  // namespace vgpu
 
 using namespace vgpu;
-
-// Row-order (colour-major) copy of the topology, see MCState.  Returns
-// false (and builds nothing) when the row indices leave no room for the
-// packed neighbour material bits.
-template <typename R>
-static int build_rows(vgpu_ctx* h, MCState* s, const std::vector<int>& order, bool* built) {
-   *built = false;
-   SysDev& S = h->sys;
-   const int n = S.n, nc = s->ncolours, M = S.M;
-   s->crow_off.assign(nc + 1, 0);
-   for (int c = 0; c < nc; ++c)
-      s->crow_off[c + 1] = s->crow_off[c] + (s->colour_off[c + 1] - s->colour_off[c] + 31) / 32 * 32;
-   const int nrows = s->crow_off[nc], zero_row = nrows, nrsl = nrows / 32;
-   int rshift = 0;
-   if (S.mat_shift) {
-      rshift = 1;
-      while ((1 << rshift) <= zero_row) ++rshift;
-      if (((int64_t)(M - 1) << rshift) >= ((int64_t)1 << 31)) return VGPU_OK;
-   }
-   std::vector<int> row_atom(nrows, -1), atom_row(n), row_mat(nrows, 0), deg(n);
-   for (int c = 0; c < nc; ++c)
-      for (int k = s->colour_off[c]; k < s->colour_off[c + 1]; ++k) {
-         const int r = s->crow_off[c] + k - s->colour_off[c];
-         row_atom[r] = order[k];
-         atom_row[order[k]] = r;
-      }
-   for (int i = 0; i < n; ++i) deg[i] = (int)(S.row_host[i + 1] - S.row_host[i]);
-   for (int r = 0; r < nrows; ++r)
-      if (row_atom[r] >= 0) row_mat[r] = S.type_host[row_atom[r]];
-   // atom-order SELL offsets, as the upload built them
-   std::vector<int64_t> off(S.nslices + 1, 0);
-   for (int sl = 0; sl < S.nslices; ++sl) {
-      int w = 0;
-      for (int l = 0; l < 32 && sl * 32 + l < n; ++l) w = std::max(w, deg[sl * 32 + l]);
-      off[sl + 1] = off[sl] + 32 * (int64_t)w;
-   }
-   std::vector<int> rsoff(nrsl + 1, 0);
-   for (int sl = 0; sl < nrsl; ++sl) {
-      int w = 0;
-      for (int l = 0; l < 32; ++l) {
-         const int i = row_atom[sl * 32 + l];
-         if (i >= 0) w = std::max(w, deg[i]);
-      }
-      rsoff[sl + 1] = rsoff[sl] + 32 * w;
-   }
-   const int64_t ne = rsoff[nrsl];
-   std::vector<int> rcol(std::max<int64_t>(ne, 1), zero_row), map(std::max<int64_t>(ne, 1), -1);
-   for (int r = 0; r < nrows; ++r) {
-      const int i = row_atom[r];
-      if (i < 0) continue;
-      for (int k = 0; k < deg[i]; ++k) {
-         const int j = S.nl_host[S.row_host[i] + k];
-         const int64_t e = rsoff[r >> 5] + 32 * (int64_t)k + (r & 31);
-         rcol[e] = atom_row[j] | (rshift ? (S.type_host[j] << rshift) : 0);
-         map[e] = (int)(off[i >> 5] + 32 * (int64_t)k + (i & 31));
-      }
-   }
-   const int nper = S.fmt == FMT_ISO_BOND ? 1 : (S.fmt == FMT_VEC_BOND || S.fmt == FMT_DMI_TAB) ? 3
-                  : S.fmt == FMT_TENSOR_BOND ? 9 : 0;
-   cudaError_t e = cudaSuccess;
-   auto up = [&](void** dst, const void* src, size_t bytes) {
-      if (e != cudaSuccess) return;
-      e = cudaMalloc(dst, std::max<size_t>(bytes, 16));
-      if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
-   };
-   int* dmap = nullptr;
-   up((void**)&s->row_atom, row_atom.data(), sizeof(int) * nrows);
-   up((void**)&s->atom_row, atom_row.data(), sizeof(int) * n);
-   if (M > 1) up((void**)&s->row_mat, row_mat.data(), sizeof(int) * nrows);
-   up((void**)&s->rslice_off, rsoff.data(), sizeof(int) * (nrsl + 1));
-   up((void**)&s->rcol, rcol.data(), sizeof(int) * rcol.size());
-   up((void**)&dmap, map.data(), sizeof(int) * map.size());
-   for (int q = 0; q < 3 && e == cudaSuccess; ++q) {
-      e = cudaMalloc(&s->rs[q], sizeof(R) * (nrows + 1));
-      if (e == cudaSuccess) e = cudaMemsetAsync(s->rs[q], 0, sizeof(R) * (nrows + 1), h->stream);
-   }
-   for (int q = 0; q < nper && e == cudaSuccess; ++q) {
-      e = cudaMalloc(&s->rjb[q], sizeof(R) * std::max<int64_t>(ne, 1));
-      if (e == cudaSuccess && ne > 0) {
-         const int blocks = (int)std::min<int64_t>((ne + 255) / 256, 148 * 16);
-         rows_gather_jb_kernel<R><<<blocks, 256, 0, h->stream>>>(dmap, ne, (const R*)S.jb[q], (R*)s->rjb[q]);
-         e = cudaGetLastError();
-      }
-   }
-   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-   cudaFree(dmap);
-   if (e != cudaSuccess) return cuda_err(h, e, "mc row-order topology");
-   s->nrows = nrows;
-   s->rmat_shift = rshift;
-   s->ridx_mask = rshift ? ((1 << rshift) - 1) : 0x7fffffff;
-   *built = true;
-   return VGPU_OK;
-}
 
 // Host-side greedy colouring of the (symmetrised) exchange graph.
 static int greedy_colour(int n, const std::vector<std::vector<int>>& adj, std::vector<int>& colour) {
@@ -392,10 +240,6 @@ extern "C" int vgpu_mc_setup(vgpu_handle h, const int32_t* colour_in, int32_t* n
    cudaMemcpyAsync(s->atoms, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->stream);
    cudaMemsetAsync(s->rejects, 0, sizeof(unsigned long long), h->stream);
    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_err(h, e, "mc setup");
-   bool built = false;
-   int rc = h->prec == VGPU_PREC_FP64 ? build_rows<double>(h, s, order, &built) : build_rows<float>(h, s, order, &built);
-   if (rc) return rc;
-   s->rows_built = built;
    if (n_colours_out) *n_colours_out = nc;
    return VGPU_OK;
 }
@@ -463,28 +307,10 @@ static int mc_sweeps_typed(vgpu_handle h, uint64_t n_sweeps) {
    cudaMemcpyAsync(tab, sig.data(), M * sizeof(R), cudaMemcpyHostToDevice, h->stream);
    cudaMemcpyAsync(tab + 100, beta.data(), M * sizeof(R), cudaMemcpyHostToDevice, h->stream);
    cudaMemcpyAsync(tab + 200, ratio.data(), M * sizeof(R), cudaMemcpyHostToDevice, h->stream);
-   // row-order sweeps unless a per-atom field table enters the energies
-   const bool rows = s->rows_built && !S.cell && !S.hm_atom && !(S.aniso_ext & ANI_NEEL);
-   const int grid_rows = std::max(1, std::min((std::max(s->nrows, S.n) + 255) / 256, 148 * 8));
-   if (rows && n_sweeps > 0) {
-      rows_in_kernel<R><<<grid_rows, 256, 0, h->stream>>>(s->nrows, s->row_atom, (const R*)S.s[0], (const R*)S.s[1],
-                                                         (const R*)S.s[2], (R*)s->rs[0], (R*)s->rs[1],
-                                                         (R*)s->rs[2]);
-      h->kernel_launches++;
-   }
    for (uint64_t sw = 0; sw < n_sweeps; ++sw) {
       MCArgs<R> p;
       memset(&p, 0, sizeof p);
       p.a = make_args<R>(h);
-      if (rows) {
-         p.a.ax = (R*)s->rs[0]; p.a.ay = (R*)s->rs[1]; p.a.az = (R*)s->rs[2];
-         p.a.mat = S.M > 1 ? s->row_mat : nullptr;
-         p.a.slice_off = s->rslice_off;
-         p.a.col = s->rcol;
-         for (int q = 0; q < 9; ++q) p.a.jb[q] = (const R*)s->rjb[q];
-         p.a.mat_shift = s->rmat_shift;
-         p.a.idx_mask = s->ridx_mask;
-      }
       p.sigma = tab;
       p.beta = tab + 100;
       p.mu_ratio = tab + 200;
@@ -492,28 +318,16 @@ static int mc_sweeps_typed(vgpu_handle h, uint64_t n_sweeps) {
       p.sweep = s->sweep;
       p.rejects = s->rejects;
       for (int c = 0; c < s->ncolours; ++c) {
-         if (rows) {
-            p.atoms = s->row_atom + s->crow_off[c];
-            p.row0 = s->crow_off[c];
-            p.count = s->crow_off[c + 1] - s->crow_off[c];
-         } else {
-            p.atoms = s->atoms + s->colour_off[c];
-            p.count = s->colour_off[c + 1] - s->colour_off[c];
-         }
+         p.atoms = s->atoms + s->colour_off[c];
+         p.count = s->colour_off[c + 1] - s->colour_off[c];
          h->prof_begin(PROF_MC);
-         cudaError_t e = mc_dispatch<R>(p, S.fmt, rows, h->stream);
+         cudaError_t e = mc_dispatch<R>(p, S.fmt, h->stream);
          h->prof_end(PROF_MC);
          if (e != cudaSuccess) return cuda_err(h, e, "mc launch");
          h->kernel_launches++;
       }
       s->sweep++;
       s->moves += S.n;
-   }
-   if (rows && n_sweeps > 0) {
-      rows_out_kernel<R><<<grid_rows, 256, 0, h->stream>>>(S.n, s->atom_row, (const R*)s->rs[0], (const R*)s->rs[1],
-                                                          (const R*)s->rs[2], (R*)S.s[0], (R*)S.s[1], (R*)S.s[2]);
-      h->kernel_launches++;
-      return cuda_err(h, cudaGetLastError(), "mc row order");
    }
    return VGPU_OK;
 }
