@@ -390,6 +390,15 @@ int vgpu_stats_get_energy(vgpu_handle h, int32_t id, double* e, double* mean, in
 /* Zero the running means and counters.  Replaces vcuda::stats::reset. */
 int vgpu_stats_reset(vgpu_handle h);
 
+/* Enqueue (no synchronisation) a copy of the latest finalised rows of mask
+ * `id` into out[9*bin + k]: k = 0..3 magnetisation (m_hat, |m|/m_sat), 4..8
+ * energies (total, exchange, anisotropy, applied, magnetostatic) -- the
+ * values vgpu_stats_get_* return.  out is pinned host or device memory; the
+ * copy completes in order on the handle's stream (vgpu_get_stream), so a
+ * host can read step t's result while step t+1 runs.  No reference
+ * counterpart (vcuda::stats::get blocks). */
+int vgpu_stats_copy_rows(vgpu_handle h, int32_t id, double* out);
+
 /* Raw per-bin sums of the last vgpu_stats_update of mask `id`: sums[8*bin +
  * {0..3}] = sum mu s_x, sum mu s_y, sum mu s_z, sum mu (mu_B), [4..7] = the
  * exchange, anisotropy, applied and magnetostatic energy sums (exchange and

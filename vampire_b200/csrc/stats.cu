@@ -368,6 +368,17 @@ static int stats_get(vgpu_handle h, int32_t id, int offset, int count, double* c
    return VGPU_OK;
 }
 
+/* enqueue-only copy of the latest rows of mask `id` (see vgpu.h) */
+extern "C" int vgpu_stats_copy_rows(vgpu_handle h, int32_t id, double* out) {
+   if (!h || !out) return set_err(h, VGPU_ERR_ARG, "null argument");
+   StatsState* s = stats_of(h);
+   if (!s || id < 0 || id >= (int)s->masks.size()) return set_err(h, VGPU_ERR_ARG, "unknown statistics mask %d", id);
+   StatsMask& m = s->masks[id];
+   cudaSetDevice(h->device);
+   return cuda_err(h, cudaMemcpyAsync(out, m.cur, sizeof(double) * m.size * ST_W, cudaMemcpyDefault, h->stream),
+                   "statistics rows");
+}
+
 extern "C" int vgpu_stats_get_magnetization(vgpu_handle h, int32_t id, double* m, double* mean, int64_t* counter) {
    return stats_get(h, id, 0, 4, m, mean, counter, false);
 }

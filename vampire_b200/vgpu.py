@@ -310,6 +310,11 @@ class Simulation:
         self._check(lib().vgpu_halo_unpack(self._h, C.c_int(which), C.c_int32(first), C.c_int32(count),
                                            C.c_void_p(in_ptr)))
 
+    def stats_copy_rows(self, mask_id: int, out_ptr: int) -> None:
+        """Enqueue a copy of the latest rows (9 doubles per bin) to out_ptr
+        (pinned host or device memory) on the library stream; no wait."""
+        self._check(lib().vgpu_stats_copy_rows(self._h, C.c_int32(mask_id), C.c_void_p(out_ptr)))
+
     def stats_derived(self, mask_id: int, temperature: float):
         """(susceptibility (size, 4), specific heat (size,), std dev (size, 4))
         of the updates since the last reset (vgpu_stats_get_derived)."""
