@@ -80,3 +80,21 @@ def test_derived_statistics_match_reference(vgpu_lib, prec, rtol):
     np.testing.assert_allclose(sh[0], d["spec_heat_system"][0], rtol=rtol)
     np.testing.assert_allclose(sd[0], d["std_material"], rtol=rtol)
     assert not np.isfinite(sus0).all() or np.all(sus0 == 0)   # reset: no updates left
+
+
+@pytest.mark.parametrize("name,step", [("fcc4_dmi_t300", 2), ("sc6_open_t300", 3)])
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_magnetization_only_path(vgpu_lib, name, step, prec):
+    """The magnetisation-only reduction of small masks (register sums per
+    thread) gives the reference's magnetisation like the full pass."""
+    from vampire_b200 import vgpu
+    s, d = load_golden(name)
+    with vgpu.Simulation(s, precision=prec) as sim:
+        sim.set_spins(ref_spins(d, step))
+        for k in ("system", "material"):
+            mid = sim.add_mask(*s.masks[k])
+            sim.stats_update(magnetization=True, energy=False)
+            m, _, cnt = sim.magnetization(mid)
+            if f"mag_{k}_{step}" in d:
+                tol = 2e-6 if prec == "fp32" else 1e-12
+                assert np.abs(m - d[f"mag_{k}_{step}"]).max() < tol

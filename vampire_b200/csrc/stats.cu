@@ -63,6 +63,49 @@ __device__ __forceinline__ double warp_sum(double v) {
    return v;
 }
 
+// Magnetisation only, masks of at most NB bins (system, material of a few
+// materials): per-thread register sums over a grid-stride loop (no
+// reductions inside the loop, loads of successive atoms in flight together),
+// one warp reduction and shared-memory add per block at the end.  Writes the
+// same block partial rows as stats_partial_kernel (energy quantities zero).
+template <typename R, int NB>
+__global__ void __launch_bounds__(256) stats_mag_small_kernel(const LLGArgs<R> a, const int* __restrict__ mask,
+                                                              int size, double* __restrict__ partial) {
+   __shared__ double acc[NB * ST_NQ];
+   for (int k = threadIdx.x; k < NB * ST_NQ; k += blockDim.x) acc[k] = 0.0;
+   __syncthreads();
+   double s[NB][4];
+#pragma unroll
+   for (int b = 0; b < NB; ++b) s[b][0] = s[b][1] = s[b][2] = s[b][3] = 0.0;
+   const int stride = gridDim.x * blockDim.x;
+#pragma unroll 4
+   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_upd; i += stride) {
+      const int mi = a.mat ? __ldg(a.mat + i) : 0;
+      const double mu = (double)a.mp[mi].mu_s_muB;
+      const int bin = NB == 1 ? 0 : __ldg(mask + i);
+      const double x = (double)a.ax[i] * mu, y = (double)a.ay[i] * mu, z = (double)a.az[i] * mu;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+         const bool on = bin == b;
+         s[b][0] += on ? x : 0.0;
+         s[b][1] += on ? y : 0.0;
+         s[b][2] += on ? z : 0.0;
+         s[b][3] += on ? mu : 0.0;
+      }
+   }
+   const int lane = threadIdx.x & 31;
+#pragma unroll
+   for (int b = 0; b < NB; ++b)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+         const double v = warp_sum(s[b][q]);
+         if (lane == 0) atomicAdd(acc + b * ST_NQ + q, v);
+      }
+   __syncthreads();
+   double* out = partial + (size_t)blockIdx.x * size * ST_NQ;  // size <= NB bins
+   for (int k = threadIdx.x; k < size * ST_NQ; k += blockDim.x) out[k] = acc[k];
+}
+
 template <typename R, int FMT>
 __global__ void stats_partial_kernel(const LLGArgs<R> a, const int* __restrict__ mask, int size, int do_energy,
                                      const R* __restrict__ hm, double* __restrict__ partial) {
@@ -236,7 +279,14 @@ static cudaError_t launch_stats(const LLGArgs<R>& a, StatsMask& m, int nblocks, 
                                            (int)smem);
       if (e != cudaSuccess) return e;
    }
-   stats_partial_kernel<R, FMT><<<nblocks, 256, smem, st>>>(a, m.mask, m.size, do_energy, hm, m.partial);
+   if (!do_energy && m.size <= 4) {
+      // the per-step magnetisation of small masks
+      if (m.size == 1) stats_mag_small_kernel<R, 1><<<nblocks, 256, 0, st>>>(a, m.mask, m.size, m.partial);
+      else if (m.size == 2) stats_mag_small_kernel<R, 2><<<nblocks, 256, 0, st>>>(a, m.mask, m.size, m.partial);
+      else stats_mag_small_kernel<R, 4><<<nblocks, 256, 0, st>>>(a, m.mask, m.size, m.partial);
+   } else {
+      stats_partial_kernel<R, FMT><<<nblocks, 256, smem, st>>>(a, m.mask, m.size, do_energy, hm, m.partial);
+   }
    cudaError_t e = cudaGetLastError();
    if (e != cudaSuccess) return e;
    stats_final_kernel<<<m.size, 32 * ST_NQ, 0, st>>>(m.partial, nblocks, m.size, do_mag, do_energy, m.cur, m.mean,
