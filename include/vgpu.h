@@ -162,6 +162,24 @@ typedef struct {
 } vgpu_anisotropy_ext;
 int vgpu_set_anisotropy_ext(vgpu_handle h, const vgpu_anisotropy_ext* a);
 
+/* Biquadratic exchange (exchange::biquadratic; material biquadratic-exchange
+ * or unit-cell biquadratic interactions): H_i += sum_j 2 J_bq (s_i.s_j) s_j
+ * over its own CSR list (src/exchange/biquadratic_fields.cpp:60-76), energy
+ * -sum_j J_bq (s_i.s_j)^2 counted with the exchange energy
+ * (biquadratic_energy.cpp, statistics/energy.cpp:165-173).  Isotropic
+ * constants in Tesla (bq_i_exchange_list), as the reference evaluates them.
+ * Call after vgpu_upload_system. */
+typedef struct {
+   int64_t num_bonds;
+   const int32_t* nl_start;        /* [num_atoms] biquadratic_neighbour_list_start_index */
+   const int32_t* nl_end;          /* [num_atoms] ..._end_index (inclusive)              */
+   const int32_t* nl;              /* [num_bonds] biquadratic_neighbour_list_array       */
+   const int32_t* nl_type;         /* [num_bonds] interaction id, or NULL = bond index   */
+   int64_t num_exchange;           /* entries in jlist                                   */
+   const double* jlist;            /* [num_exchange] J_bq [T]                            */
+} vgpu_biquadratic_desc;
+int vgpu_set_biquadratic(vgpu_handle h, const vgpu_biquadratic_desc* b);
+
 /* Host-only check of a descriptor (no device needed): CSR rows inside
  * [0, num_bonds), neighbours and interaction ids in range, materials in
  * range, finite spins.  VGPU_ERR_ARG / VGPU_ERR_NAN with a message for

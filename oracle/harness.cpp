@@ -166,6 +166,22 @@ static void dump_system() {
       dumpd("aniso_ext", ext);
       if (ai::enable_neel_anisotropy) dumpd("neel_tensor", ai::neel_tensor);
    }
+   // biquadratic exchange: its own neighbour list and isotropic constants
+   // (exchange/internal.hpp, exchange/biquadratic_fields.cpp)
+   {
+      namespace ei = exchange::internal;
+      std::vector<int> bq = {(int)exchange::biquadratic, (int)ei::biquadratic_exchange_type};
+      dumpi("bq_flag", bq);
+      if (exchange::biquadratic) {
+         dumpi("bq_start", ei::biquadratic_neighbour_list_start_index);
+         dumpi("bq_end", ei::biquadratic_neighbour_list_end_index);
+         dumpi("bq_nl", ei::biquadratic_neighbour_list_array);
+         dumpi("bq_type", ei::biquadratic_neighbour_interaction_type_array);
+         std::vector<double> j;
+         for (auto& e : ei::bq_i_exchange_list) j.push_back(e.Jij);
+         dumpd("bq_jlist", j);
+      }
+   }
    std::vector<double> simc = {mp::dt, mp::half_dt, mp::dt_SI, mp::gamma_SI, sim::temperature,
                                sim::H_applied, sim::H_vec[0], sim::H_vec[1], sim::H_vec[2]};
    dumpd("sim", simc);

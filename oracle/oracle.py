@@ -45,6 +45,7 @@ class VRefSys(C.Structure):
         ("H_vec", C.c_double * 3), ("mus", _D), ("mus_SI", _D),
         ("u4", C.c_int), ("u6", C.c_int), ("c6", C.c_int), ("crot", C.c_int), ("neel", C.c_int),
         ("pad2_", C.c_int), ("ku4", _D), ("ku6", _D), ("kc6", _D), ("kcb", _D), ("neelt", _D),
+        ("bq_start", _I), ("bq_end", _I), ("bq_nl", _I), ("bq_type", _I), ("bq_j", _D),
     ]
 
 
@@ -130,6 +131,14 @@ class OracleSystem:
             st.H_vec[k] = hv[k]
         st.mus = _p(arr("mus", m["mu_s_SI"] / 9.27400915e-24, np.float64), _D)
         st.mus_SI = _p(arr("mus_SI", m["mu_s_SI"], np.float64), _D)
+        bq = getattr(s, "biquadratic", None)
+        if bq is not None:
+            st.bq_start = _p(arr("bq_start", bq["start"], np.int32), _I)
+            st.bq_end = _p(arr("bq_end", bq["end"], np.int32), _I)
+            st.bq_nl = _p(arr("bq_nl", bq["nl"], np.int32), _I)
+            if bq.get("type") is not None:
+                st.bq_type = _p(arr("bq_type", bq["type"], np.int32), _I)
+            st.bq_j = _p(arr("bq_j", bq["jlist"], np.float64), _D)
         a = getattr(s, "aniso", None)
         if a is not None:
             st.u4, st.u6, st.c6, st.crot, st.neel = (int(a["u4"]), int(a["u6"]), int(a["c6"]), int(a["crot"]),
@@ -331,6 +340,10 @@ def system_from_dump(d: dict, params=None):
     nt = d["nl_type"].astype(np.int32)
     if not np.array_equal(nt, np.arange(nt.size, dtype=np.int32)):
         s.nl_type = nt
+    if "bq_flag" in d and int(d["bq_flag"][0]):
+        s.biquadratic = {"start": d["bq_start"].astype(np.int32), "end": d["bq_end"].astype(np.int32),
+                         "nl": d["bq_nl"].astype(np.int32), "type": d["bq_type"].astype(np.int32),
+                         "jlist": d["bq_jlist"]}
     if "aniso_flags" in d and int(np.sum(d["aniso_flags"])) > 0:
         fl = [bool(x) for x in d["aniso_flags"]]
         ext = d["aniso_ext"].reshape(nmat, 12)

@@ -64,6 +64,24 @@ void vref_spin_fields(const vref_sys* s, const double* sx, const double* sy, con
    memset(hy, 0, sizeof(double) * s->n);
    memset(hz, 0, sizeof(double) * s->n);
    exchange_fields(s, sx, sy, sz, hx, hy, hz);
+   if (s->bq_start) {  /* exchange/biquadratic_fields.cpp:43-79 */
+      for (int atom = 0; atom < s->n; atom++) {
+         double bx = 0.0, by = 0.0, bz = 0.0;
+         const double six = sx[atom], siy = sy[atom], siz = sz[atom];
+         for (int nn = s->bq_start[atom]; nn < s->bq_end[atom] + 1; ++nn) {
+            const int natom = s->bq_nl[nn];
+            const double twoJbq = 2.0 * s->bq_j[s->bq_type ? s->bq_type[nn] : nn];
+            const double sjx = sx[natom], sjy = sy[natom], sjz = sz[natom];
+            const double si_dot_sj = six * sjx + siy * sjy + siz * sjz;
+            bx += twoJbq * sjx * si_dot_sj;
+            by += twoJbq * sjy * si_dot_sj;
+            bz += twoJbq * sjz * si_dot_sj;
+         }
+         hx[atom] += bx;
+         hy[atom] += by;
+         hz[atom] += bz;
+      }
+   }
    if (s->uniaxial) {
       for (int atom = 0; atom < s->n; atom++) {
          const int mat = s->type[atom];
@@ -352,6 +370,16 @@ void vref_spin_energy(const vref_sys* s, const double* sx, const double* sy, con
          ex -= (J[0] * S0 * Sx + J[1] * S1 * Sx + J[2] * S2 * Sx + J[3] * S0 * Sy + J[4] * S1 * Sy +
                 J[5] * S2 * Sy + J[6] * S0 * Sz + J[7] * S1 * Sz + J[8] * S2 * Sz);
       }
+   }
+   if (s->bq_start) {  /* exchange/biquadratic_energy.cpp:24-37 */
+      double eb = 0.0;
+      for (int nn = s->bq_start[atom]; nn <= s->bq_end[atom]; ++nn) {
+         const int natom = s->bq_nl[nn];
+         const double Jbq = s->bq_j[s->bq_type ? s->bq_type[nn] : nn];
+         const double d = Sx * sx[natom] + Sy * sy[natom] + Sz * sz[natom];
+         eb -= Jbq * d * d;
+      }
+      ex += eb;
    }
    const int m = s->type[atom];
    double an = 0.0;

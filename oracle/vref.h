@@ -48,6 +48,12 @@ typedef struct {
    const double* kc6;
    const double* kcb;     /* per material rotated cubic basis e1, e2, e3 (9 doubles) */
    const double* neelt;   /* per atom 3x3 Neel tensor (9 doubles), or NULL */
+   /* biquadratic exchange (exchange/internal.hpp), NULL bq_start = off */
+   const int* bq_start;
+   const int* bq_end;     /* inclusive */
+   const int* bq_nl;
+   const int* bq_type;    /* interaction id per bond, or NULL (= bond index) */
+   const double* bq_j;    /* isotropic J_bq [T] per interaction */
 } vref_sys;
 
 void vref_spin_fields(const vref_sys* s, const double* sx, const double* sy, const double* sz,

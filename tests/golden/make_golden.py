@@ -132,6 +132,28 @@ def sc8_midpoint():
     save("sc8_midpoint_t300", d, keep)
 
 
+BQ_MAT = SC_MAT.replace("material[1]:exchange-matrix[1]=11.2e-21\n",
+                        "material[1]:exchange-matrix[1]=11.2e-21\nmaterial[1]:biquadratic-exchange[1]=2.0e-21\n")
+
+
+def sc6_biquadratic():
+    """SC 6^3, open boundaries, biquadratic exchange (material
+    biquadratic-exchange, src/exchange/biquadratic_fields.cpp) on top of the
+    bilinear exchange and uniaxial anisotropy: 200 T=0 reference steps and
+    energies, and 2 stochastic steps at 300 K with the Gaussian stream."""
+    d = O.run_harness(sc_input(6, periodic=False), {"m.mat": BQ_MAT},
+                      ["--system", "--steps", 200, "--snaps", "1,200", "--stats", "0,200"])
+    keep = [f"s{c}_{t}" for t in (0, 1, 200) for c in "xyz"]
+    keep += ["mag_system_0", "energy_system_0", "mag_system_200", "energy_system_200",
+             "bq_flag", "bq_start", "bq_end", "bq_nl", "bq_type", "bq_jlist"]
+    save("sc6_biquadratic_t0", d, keep)
+    d = O.run_harness(sc_input(6, T=300.0, periodic=False), {"m.mat": BQ_MAT},
+                      ["--system", "--steps", 2, "--snaps", "1,2", "--noise", 2])
+    keep = [f"s{c}_{t}" for t in (0, 1, 2) for c in "xyz"] + ["xi_1", "xi_2", "bq_flag", "bq_start", "bq_end",
+                                                              "bq_nl", "bq_type", "bq_jlist"]
+    save("sc6_biquadratic_t300", d, keep)
+
+
 HO_MAT = """material:num-materials=1
 material[1]:material-name=A
 material[1]:damping-constant=0.1
@@ -251,7 +273,7 @@ def mc_sc16_curie():
 
 
 ALL = [sc20_t0, sc8_t0, sc10_t300, sc6_open_t300, fcc4_dmi_t300, fcc4_dmi_t0, single_spin_applied, mc_sc16_curie,
-       fcc10_dipole_tensor, fcc10_dipole_macrocell, sc6_aniso_ho, fcc4_neel_rot, sc6_derived_t600, sc8_midpoint]
+       fcc10_dipole_tensor, fcc10_dipole_macrocell, sc6_aniso_ho, fcc4_neel_rot, sc6_derived_t600, sc8_midpoint, sc6_biquadratic]
 
 if __name__ == "__main__":
     names = sys.argv[1:]

@@ -42,7 +42,8 @@ def test_bad_colouring_rejected(vgpu_lib):
         assert "conflict" in str(e.value)
 
 
-@pytest.mark.parametrize("name", ["sc10_t300", "fcc4_dmi_t300", "sc6_open_t300", "sc6_aniso_ho", "fcc4_neel_rot"])
+@pytest.mark.parametrize("name", ["sc10_t300", "fcc4_dmi_t300", "sc6_open_t300", "sc6_aniso_ho", "fcc4_neel_rot",
+                                  "sc6_biquadratic_t300"])
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_replayed_sweep_matches_oracle(vgpu_lib, name, prec):
     from oracle import oracle as O

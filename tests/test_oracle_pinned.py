@@ -179,3 +179,29 @@ def test_llg_midpoint_replayed_noise():
     for t in (1, 2):
         got = o.llg_midpoint(got, 1, xi=d[f"xi_{t}"])
         assert np.abs(got - ref_spins(d, t)).max() < 1e-12, t
+
+
+def test_biquadratic_exchange():
+    """Biquadratic exchange (src/exchange/biquadratic_fields.cpp,
+    biquadratic_energy.cpp): 200 T=0 steps, replayed T>0 steps and the
+    exchange energy including the biquadratic term, against the reference."""
+    s, d = load_golden("sc6_biquadratic_t0")
+    assert s.biquadratic is not None
+    o = O.OracleSystem(s)
+    got = o.llg_heun(s.spins, 1)
+    assert np.abs(got - ref_spins(d, 1)).max() < 1e-13
+    got = o.llg_heun(got, 199)
+    assert np.abs(got - ref_spins(d, 200)).max() < 1e-12
+    mask, size = s.masks["system"]
+    for t in (0, 200):
+        np.testing.assert_allclose(o.energy(ref_spins(d, t), mask, size), d[f"energy_system_{t}"], rtol=1e-11,
+                                   atol=1e-9)
+    s, d = load_golden("sc6_biquadratic_t300")
+    o = O.OracleSystem(s)
+    got = s.spins
+    for t in (1, 2):
+        got = o.llg_heun(got, 1, xi=d[f"xi_{t}"])
+        assert np.abs(got - ref_spins(d, t)).max() < 1e-12, t
+    bad = s.copy()
+    bad.biquadratic = None
+    assert np.abs(O.OracleSystem(bad).llg_heun(s.spins, 1, xi=d["xi_1"]) - ref_spins(d, 1)).max() > 1e-9

@@ -309,6 +309,7 @@ int check_adjoint_ok(vgpu_ctx* h) {
    if (h->sys.cell || h->sys.hd_atom || h->sys.sys_off)
       return set_err(h, VGPU_ERR_ARG, "the adjoint does not support dipole fields or batches");
    if (h->params.local_applied_field) return set_err(h, VGPU_ERR_ARG, "the adjoint supports the global applied field only");
+   if (h->sys.bq_off) return set_err(h, VGPU_ERR_ARG, "the adjoint does not support biquadratic exchange");
    if (h->sys.aniso_ext) return set_err(h, VGPU_ERR_ARG, "the adjoint supports second-order uniaxial and cubic anisotropy only");
    if (h->sys.n_owned < h->sys.n) return set_err(h, VGPU_ERR_STATE, "the adjoint runs on whole systems (handle holds a shard)");
    return VGPU_OK;

@@ -197,6 +197,48 @@ __device__ __forceinline__ void exchange_gather_w(const LLGArgs<R>& a, int base,
    }
 }
 
+// biquadratic exchange field of atom i at own spin S over its SELL-32 list:
+// sum_j 2 J_bq (S.s_j) s_j (src/exchange/biquadratic_fields.cpp:60-76)
+template <typename R, int LOAD = 0>
+__device__ __forceinline__ void biquadratic_field(const LLGArgs<R>& a, int i, const R* __restrict__ sx,
+                                                  const R* __restrict__ sy, const R* __restrict__ sz, const R S[3],
+                                                  R& hx, R& hy, R& hz) {
+   hx = hy = hz = 0;
+   const int sl = i >> 5;
+   const int off = __ldg(a.bq_off + sl);
+   const int w = (__ldg(a.bq_off + sl + 1) - off) >> 5;
+   const int base = off + (i & 31);
+   for (int k = 0; k < w; ++k) {
+      const int e = base + 32 * k;
+      const int j = __ldg(a.bq_col + e);
+      const R twoJbq = (R)2 * __ldg(a.bq_j + e);
+      const R x = ld_src(sx + j, LOAD), y = ld_src(sy + j, LOAD), z = ld_src(sz + j, LOAD);
+      const R d = S[0] * x + S[1] * y + S[2] * z;
+      hx += twoJbq * x * d;
+      hy += twoJbq * y * d;
+      hz += twoJbq * z * d;
+   }
+}
+
+// biquadratic energy of atom i at spin S: -sum_j J_bq (S.s_j)^2
+// (src/exchange/biquadratic_energy.cpp:24-37)
+template <typename E, typename R>
+__device__ __forceinline__ E biquadratic_energy(const LLGArgs<R>& a, int i, const E S[3]) {
+   E en = 0;
+   const int sl = i >> 5;
+   const int off = __ldg(a.bq_off + sl);
+   const int w = (__ldg(a.bq_off + sl + 1) - off) >> 5;
+   const int base = off + (i & 31);
+   for (int k = 0; k < w; ++k) {
+      const int e = base + 32 * k;
+      const int j = __ldg(a.bq_col + e);
+      const E J = (E)__ldg(a.bq_j + e);
+      const E d = S[0] * (E)a.ax[j] + S[1] * (E)a.ay[j] + S[2] * (E)a.az[j];
+      en -= J * d * d;
+   }
+   return en;
+}
+
 // exchange field with the fixed-width fast paths (FP32, packed records).
 // STAGED (FMT_DMI_TAB only): srec_tile is the shared-memory copy of the
 // records of the tile starting at slice_off[tile_slice0].
@@ -226,6 +268,13 @@ __device__ __forceinline__ void spin_field(const LLGArgs<R>& a, int i, int mi, c
                                            const int4* srec_tile = nullptr, int tile_off = 0) {
    R hx = 0, hy = 0, hz = 0;
    exchange_field<R, FMT, LOAD, STAGED>(a, i, mi, sx, sy, sz, hx, hy, hz, srec_tile, tile_off);
+   if (EXT && a.bq_off) {
+      // biquadratic exchange (exchange/biquadratic_fields.cpp): its own sum,
+      // added to the bilinear field as exchange::fields does
+      R bx, by, bz;
+      biquadratic_field<R, LOAD>(a, i, sx, sy, sz, S, bx, by, bz);
+      hx += bx; hy += by; hz += bz;
+   }
    // anisotropy terms in the order of anisotropy::fields (src/anisotropy/fields.cpp:42-63)
    if (a.uniaxial) {
       const R sdote = S[0] * m.kux + S[1] * m.kuy + S[2] * m.kuz;

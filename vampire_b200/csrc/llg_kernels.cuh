@@ -172,7 +172,7 @@ inline cudaError_t launch_fmt(const LLGArgs<R>& a, int mode, cudaStream_t st) {
    const int grid = ((mode == PASS_FIELD ? a.n : a.n_upd) + bs - 1) / bs;
    if (grid == 0) return cudaSuccess;
    if (a.integrator == INTEG_MIDPOINT && mode != PASS_FIELD) launch_mode<R, FMT, VAR_MIDPOINT>(a, mode, grid, bs, st);
-   else if (a.aniso_ext) launch_mode<R, FMT, VAR_HEUN_EXT>(a, mode, grid, bs, st);
+   else if (a.aniso_ext || a.bq_off) launch_mode<R, FMT, VAR_HEUN_EXT>(a, mode, grid, bs, st);
    else launch_mode<R, FMT, VAR_HEUN>(a, mode, grid, bs, st);
    return cudaGetLastError();
 }

@@ -71,6 +71,7 @@ __device__ __forceinline__ R site_energy_delta(const LLGArgs<R>& a, int i, const
       d += (R)(-0.5) * m.kc4 * (t4 - s4);
    }
    if (a.aniso_ext) d += anisotropy_energy<R, R, true>(a, i, m, T) - anisotropy_energy<R, R, true>(a, i, m, S);
+   if (a.bq_off) d += biquadratic_energy<R, R>(a, i, T) - biquadratic_energy<R, R>(a, i, S);
    return d;
 }
 

@@ -139,7 +139,11 @@ __global__ void stats_partial_kernel(const LLGArgs<R> a, const int* __restrict__
          if (do_energy) {
             R hx = 0, hy = 0, hz = 0;
             exchange_gather<R, FMT>(a, i, mi, a.ax, a.ay, a.az, hx, hy, hz);
-            const double eex = -((double)S[0] * hx + (double)S[1] * hy + (double)S[2] * hz);
+            double eex = -((double)S[0] * hx + (double)S[1] * hy + (double)S[2] * hz);
+            if (a.bq_off) {
+               const double Sb[3] = {(double)S[0], (double)S[1], (double)S[2]};
+               eex += biquadratic_energy<double, R>(a, i, Sb);
+            }
             const double Sd[3] = {(double)S[0], (double)S[1], (double)S[2]};
             const double ean = anisotropy_energy<double, R>(a, i, m, Sd);
             const double eap = -((double)a.hx * S[0] + (double)a.hy * S[1] + (double)a.hz * S[2]);

@@ -356,6 +356,9 @@ LLGArgs<R> make_args(vgpu_ctx* h) {
    a.n_alloc = S.n_alloc;
    a.aniso_ext = S.aniso_ext;
    a.neel = (const R*)S.neel;
+   a.bq_off = (const int*)S.bq_off;
+   a.bq_col = (const int*)S.bq_col;
+   a.bq_j = (const R*)S.bq_j;
    a.n_upd = S.n_owned;
    a.noise_base = S.noise_base;
    a.slice_off = (const int*)S.slice_off;
@@ -435,7 +438,7 @@ template <typename R>
 static bool use_staged(vgpu_ctx* h) {
    const SysDev& S = h->sys;
    // the staged passes carry no higher-order anisotropy terms (register budget)
-   if (sizeof(R) != 4 || !S.rec || S.n == 0 || h->staged == 0 || S.aniso_ext) return false;
+   if (sizeof(R) != 4 || !S.rec || S.n == 0 || h->staged == 0 || S.aniso_ext || S.bq_off) return false;
    const int bytes = S.stage_bytes[stage_slot(h->stage_sl)];
    return h->stage_nbuf * bytes <= kStageSmemLimit;
 }
@@ -759,6 +762,56 @@ extern "C" int vgpu_set_noise_replay(vgpu_handle h, const double* xi) {
 }
 
 template <typename R>
+static int upload_biquadratic(vgpu_handle h, const vgpu_biquadratic_desc* b) {
+   SysDev& S = h->sys;
+   const int n = S.n, nsl = S.nslices, pad = S.n_alloc - 1;
+   std::vector<int> off(nsl + 1, 0);
+   for (int sl = 0; sl < nsl; ++sl) {
+      int w = 0;
+      for (int l = 0; l < 32 && sl * 32 + l < n; ++l) w = std::max(w, b->nl_end[sl * 32 + l] - b->nl_start[sl * 32 + l] + 1);
+      off[sl + 1] = off[sl] + 32 * w;
+   }
+   const size_t ne = (size_t)off[nsl];
+   std::vector<int> col(std::max<size_t>(ne, 1), pad);
+   std::vector<R> j(std::max<size_t>(ne, 1), (R)0);
+   for (int i = 0; i < n; ++i) {
+      int k = 0;
+      for (int32_t e = b->nl_start[i]; e <= b->nl_end[i]; ++e, ++k) {
+         const size_t q = (size_t)off[i >> 5] + 32 * (size_t)k + (i & 31);
+         col[q] = b->nl[e];
+         j[q] = (R)b->jlist[b->nl_type ? b->nl_type[e] : e];
+      }
+   }
+   int rc;
+   if ((rc = upload_vec(h, &S.bq_off, off, "biquadratic slice offsets"))) return rc;
+   if ((rc = upload_vec(h, &S.bq_col, col, "biquadratic neighbours"))) return rc;
+   if ((rc = upload_vec(h, &S.bq_j, j, "biquadratic couplings"))) return rc;
+   return cuda_err(h, cudaStreamSynchronize(h->stream), "biquadratic upload");
+}
+
+extern "C" int vgpu_set_biquadratic(vgpu_handle h, const vgpu_biquadratic_desc* b) {
+   if (!h || !b) return set_err(h, VGPU_ERR_ARG, "null argument");
+   SysDev& S = h->sys;
+   if (!S.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (S.sys_off) return set_err(h, VGPU_ERR_STATE, "batched systems carry no biquadratic exchange");
+   if (S.n_owned < S.n) return set_err(h, VGPU_ERR_STATE, "shards carry no biquadratic exchange list");
+   if (S.bq_off) return set_err(h, VGPU_ERR_STATE, "biquadratic exchange already set (upload the system again)");
+   if (!b->nl_start || !b->nl_end || (b->num_bonds > 0 && (!b->nl || !b->jlist)))
+      return set_err(h, VGPU_ERR_ARG, "incomplete biquadratic descriptor");
+   for (int i = 0; i < S.n; ++i) {
+      if (b->nl_end[i] < b->nl_start[i] - 1 || b->nl_start[i] < 0 || (int64_t)b->nl_end[i] >= b->num_bonds)
+         return set_err(h, VGPU_ERR_ARG, "biquadratic row %d out of range", i);
+      for (int32_t e = b->nl_start[i]; e <= b->nl_end[i]; ++e) {
+         if (b->nl[e] < 0 || b->nl[e] >= S.n) return set_err(h, VGPU_ERR_ARG, "biquadratic neighbour out of range");
+         const int64_t t = b->nl_type ? b->nl_type[e] : e;
+         if (t < 0 || t >= b->num_exchange) return set_err(h, VGPU_ERR_ARG, "biquadratic interaction id out of range");
+      }
+   }
+   cudaSetDevice(h->device);
+   return h->prec == VGPU_PREC_FP64 ? upload_biquadratic<double>(h, b) : upload_biquadratic<float>(h, b);
+}
+
+template <typename R>
 static int upload_neel(vgpu_handle h, const double* t) {
    SysDev& S = h->sys;
    const size_t na = (size_t)S.n_alloc;
@@ -933,6 +986,8 @@ extern "C" int vgpu_set_owned(vgpu_handle h, int32_t n_owned, int64_t noise_base
    if (n_owned < 0 || n_owned > S.n) return set_err(h, VGPU_ERR_ARG, "n_owned %d outside 0..%d", n_owned, S.n);
    if (noise_base < 0 || noise_base + (int64_t)n_owned > ((int64_t)1 << 32))
       return set_err(h, VGPU_ERR_ARG, "noise_base out of the 32-bit atom counter range");
+   if (n_owned < S.n && S.bq_off)
+      return set_err(h, VGPU_ERR_STATE, "shards carry no biquadratic exchange list");
    if (n_owned < S.n && (h->extras[1] || h->extras[2]))
       return set_err(h, VGPU_ERR_STATE, "Monte Carlo and the dipole solver run on whole systems only");
    S.n_owned = n_owned;

@@ -61,6 +61,10 @@ struct SysDev {
    int aniso_ext = 0;                          // AnisoExt bits
    std::vector<double> ku4_h, ku6_h, kc6_h, kcb_h;  // per material (kcb: 9 each)
    void* neel = nullptr;                       // [9][n_alloc] Neel tensors
+   // biquadratic exchange (vgpu_set_biquadratic): SELL-32 copy of its list
+   void* bq_off = nullptr;
+   void* bq_col = nullptr;
+   void* bq_j = nullptr;
 };
 
 int set_err(vgpu_ctx* h, int code, const char* fmt, ...);

@@ -67,6 +67,9 @@ struct LLGArgs {
    int aniso_ext;            // AnisoExt bits
    int integrator;           // INTEG_HEUN or INTEG_MIDPOINT
    const R* neel;            // [9][n_alloc] per-atom Neel tensors (ANI_NEEL), row-major components
+   const int* bq_off;        // biquadratic exchange: SELL-32 slice offsets of its own neighbour list, or nullptr
+   const int* bq_col;        // neighbour index per entry (padding: the zero pad atom)
+   const R* bq_j;            // isotropic J_bq [T] per entry
    R hx, hy, hz;             // global applied field
    int local_field;          // add MatParams::hl*
    uint64_t ramp_n;          // > 0: add MatParams::dh * min(step, ramp_n) / ramp_n

@@ -233,6 +233,27 @@ bool initialize(bool cpu_stats) {
       if (x.uniaxial_fourth || x.uniaxial_sixth || x.cubic_sixth || x.cubic_rotation || x.neel)
          fail(vgpu_set_anisotropy_ext(g_h, &x), "higher-order anisotropy");
    }
+   // biquadratic exchange (exchange/internal.hpp): isotropic constants only, as
+   // exchange::single_spin_biquadratic_energy evaluates them
+   if (exchange::biquadratic) {
+      namespace ei = exchange::internal;
+      if (ei::biquadratic_exchange_type != exchange::isotropic) {
+         std::cerr << "Error: only isotropic biquadratic exchange is evaluated by the B200 backend" << std::endl;
+         err::vexit();
+      }
+      std::vector<double> bj;
+      for (auto& e : ei::bq_i_exchange_list) bj.push_back(e.Jij);
+      vgpu_biquadratic_desc b;
+      std::memset(&b, 0, sizeof b);
+      b.num_bonds = (int64_t)ei::biquadratic_neighbour_list_array.size();
+      b.nl_start = ei::biquadratic_neighbour_list_start_index.data();
+      b.nl_end = ei::biquadratic_neighbour_list_end_index.data();
+      b.nl = ei::biquadratic_neighbour_list_array.data();
+      b.nl_type = ei::biquadratic_neighbour_interaction_type_array.data();
+      b.num_exchange = (int64_t)bj.size();
+      b.jlist = bj.data();
+      fail(vgpu_set_biquadratic(g_h, &b), "biquadratic exchange");
+   }
    sync_params();
    fail(vgpu_set_noise(g_h, VGPU_NOISE_PHILOX, (uint64_t)(uint32_t)mtrandom::integration_seed), "noise");
    fail(vgpu_set_step(g_h, sim::time), "step counter");

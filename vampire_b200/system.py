@@ -180,6 +180,7 @@ class SpinSystem:
     cells: Optional[dict] = None               # dipole macrocells (see dipole_cells())
     aniso: Optional[dict] = None               # higher-order anisotropy (see anisotropy_ext())
     bond_vectors: Optional[np.ndarray] = None  # (nnz, 3) i->j vectors [Angstrom] of the lattice builders
+    biquadratic: Optional[dict] = None         # start, end, nl, type (or None), jlist [T]: biquadratic exchange
 
     @property
     def num_bonds(self) -> int:

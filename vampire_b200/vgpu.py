@@ -86,6 +86,13 @@ def _aniso_ext(a: dict):
     return x, keep
 
 
+class BiquadDesc(C.Structure):
+    _fields_ = [
+        ("num_bonds", C.c_int64), ("nl_start", _I32), ("nl_end", _I32), ("nl", _I32), ("nl_type", _I32),
+        ("num_exchange", C.c_int64), ("jlist", _D),
+    ]
+
+
 class DipoleDesc(C.Structure):
     _fields_ = [
         ("num_cells", C.c_int32), ("solver", C.c_int32), ("update_rate", C.c_int32), ("pad_", C.c_int32),
@@ -233,6 +240,18 @@ class Simulation:
         if s.aniso is not None:
             x, keep2 = _aniso_ext(s.aniso)
             self._check(lib().vgpu_set_anisotropy_ext(self._h, C.byref(x)))
+        if s.biquadratic is not None:
+            b = s.biquadratic
+            keep3 = [np.ascontiguousarray(b[k], dtype=np.int32) for k in ("start", "end", "nl")]
+            jl = np.ascontiguousarray(b["jlist"], dtype=np.float64)
+            tp = None if b.get("type") is None else np.ascontiguousarray(b["type"], dtype=np.int32)
+            q = BiquadDesc()
+            q.num_bonds = keep3[2].size
+            q.nl_start, q.nl_end, q.nl = (_ptr(keep3[0], _I32), _ptr(keep3[1], _I32), _ptr(keep3[2], _I32))
+            q.nl_type = _ptr(tp, _I32) if tp is not None else C.cast(None, _I32)
+            q.num_exchange = jl.size
+            q.jlist = _ptr(jl, _D)
+            self._check(lib().vgpu_set_biquadratic(self._h, C.byref(q)))
 
     def set_option(self, option: int, value: int) -> None:
         """vgpu_set_option: OPT_STORE_INCREMENT, OPT_STAGED_RECORDS, OPT_STAGE_SLICES, OPT_STAGE_BUFFERS."""
