@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--no-dipole", action="store_true", help="leave out the macrocell dipole field")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and Monte Carlo side results")
     ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--records", choices=["auto", "wide"], default="auto",
+                    help="bond records: auto = compact words + coupling dictionary when the system allows, "
+                         "wide = 16-byte records")
     ap.add_argument("--only", choices=["mc", "batched", "adjoint"], default=None,
                     help="run one side workload alone and print its result (profiling)")
     ap.add_argument("--mc-sweeps", type=int, nargs=2, default=(5000, 10000), metavar=("EQ", "AV"),
@@ -136,9 +139,10 @@ def traffic_from_profiles(kernel: str):
 def byte_model(z=12, b_J=12, multi_mat=True, dipole=False):
     """Algorithmic HBM bytes per spin per pass (FP32 SoA state, int32 index):
     predictor reads s0 and writes s'; corrector reads s0 and s' and writes s1;
-    each pass streams the neighbour indices, the per-bond DMI vector, the
-    material id and (with the dipole field) the cell id; neighbour spins are
-    L2-served; noise is regenerated in-register (0 B)."""
+    each pass streams the neighbour words, the per-bond DMI vector (b_J = 12;
+    0 with compact records, whose coupling comes from a dictionary of a few
+    hundred bytes), the material id and (with the dipole field) the cell id;
+    neighbour spins are L2-served; noise is regenerated in-register (0 B)."""
     gather = 4 * (z + 1) + b_J * z + 4 * int(multi_mat) + 4 * int(dipole)
     return {"predictor": 24 + gather, "corrector": 36 + gather}
 
@@ -339,6 +343,9 @@ def main():
     torch.cuda.set_device(local)
     sysm = S.config_fcc_tensor(L=args.L, seed=2024 + rank, dipole=not args.no_dipole)
     sim = vgpu.Simulation(sysm, device=local, precision="fp32", noise_seed=1000 + rank)
+    if args.records == "wide":
+        sim.set_option(vgpu.OPT_COMPACT_RECORDS, 0)
+    layout, ndict = sim.record_layout()
     if sysm.cells is not None:
         sim.dipole_setup(sysm.cells)
     mask_id = sim.add_mask(*sysm.masks["system"])
@@ -379,7 +386,12 @@ def main():
     value = n * args.steps * world / (ms * 1e-3)
 
     # --- roofline of the dominant kernel --------------------------------
-    bm = byte_model(dipole=sysm.cells is not None)
+    compact = layout in (vgpu.RECORDS_COMPACT, vgpu.RECORDS_WINDOW)
+    bm = byte_model(b_J=0 if compact else 12, dipole=sysm.cells is not None)
+    records = (f"compact: 4 B per bond (neighbour | coupling index) + {ndict}-entry coupling dictionary"
+               if compact else "16 B per bond (neighbour, DMI vector)")
+    if layout == vgpu.RECORDS_WINDOW:
+        records += "; neighbour spins staged per tile in shared memory (window staging)"
     kern = max(("predictor", "corrector"), key=lambda k: prof[k]["ms"])
     avg_ms = prof[kern]["ms"] / max(1, prof[kern]["count"])
     peak, peak_kind = measured_peak_hbm()
@@ -464,7 +476,7 @@ def main():
             "config": workload_config(args.L, world),
             "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
-                         "algorithmic_bytes_per_spin": bm,
+                         "algorithmic_bytes_per_spin": bm, "bond_records": records,
                          "avg_launch_ms": {k: prof[k]["ms"] / max(1, prof[k]["count"])
                                            for k in ("predictor", "corrector")},
                          "step_achieved_gbs": step_gbs},

@@ -218,10 +218,11 @@ int vgpu_set_noise_replay(vgpu_handle h, const double* xi);
  * copy per tile, 0 = every thread loads its own records, -1 (default) = staged
  * when a tile's buffers fit in 200 KB of shared memory.  Same results bit for
  * bit either way.  VGPU_OPT_STAGE_SLICES: 2, 4 or 8 slices of 32 atoms per
- * tile (default 4); VGPU_OPT_STAGE_BUFFERS: 1 (one tile per block) or 2
- * (persistent blocks, next tile's copy overlapping this one; default 1).  A
- * copy that does not complete within a bounded wait fails the step with
- * VGPU_ERR_TIMEOUT. */
+ * tile; VGPU_OPT_STAGE_BUFFERS: 1 (one tile per block) or 2 (persistent
+ * blocks, next tile's copy overlapping this one); -1 (default) = the measured
+ * best for the record layout: 4 slices, 1 buffer with 16-byte records; 2
+ * slices, 2 buffers with compact records.  A copy that does not complete
+ * within a bounded wait fails the step with VGPU_ERR_TIMEOUT. */
 #define VGPU_OPT_STAGED_RECORDS 2
 #define VGPU_OPT_STAGE_SLICES 3
 #define VGPU_OPT_STAGE_BUFFERS 4
@@ -235,6 +236,32 @@ int vgpu_set_noise_replay(vgpu_handle h, const double* xi);
  * fails with VGPU_ERR_TIMEOUT (test of the timeout path; the handle stays
  * usable after setting it back to 0). */
 #define VGPU_OPT_STAGE_WAIT_TEST 6
+/* VGPU_OPT_COMPACT_RECORDS (FP32 systems with DMI bond records): 1 or -1
+ * (default) = when the system has at most 512 distinct bond couplings (and
+ * enough index bits above the neighbour index), the fused passes read one
+ * 4-byte word per bond (neighbour | coupling index) and take the coupling from
+ * a dictionary instead of a 16-byte record; 0 = always the 16-byte records.
+ * Same results bit for bit either way (the same coupling values). */
+#define VGPU_OPT_COMPACT_RECORDS 7
+/* VGPU_OPT_WINDOW_STAGING (staged passes over compact records, one buffer):
+ * 1 = each tile also stages its "window" -- the contiguous atom ranges holding
+ * every neighbour of its atoms, planned on the host at the first pass -- into
+ * shared memory with bulk copies, and gathers neighbour spins from there (used
+ * when every tile's window fits in 4096 atoms and 256 ranges); 0 or -1
+ * (default) = gathers through L1/L2 (measured faster on B200).  Same results
+ * bit for bit. */
+#define VGPU_OPT_WINDOW_STAGING 8
+/* Bond-record layout the next FP32 pass reads: *layout = VGPU_RECORDS_WINDOW
+ * (compact words with window staging), VGPU_RECORDS_COMPACT,
+ * VGPU_RECORDS_WIDE (16-byte records) or VGPU_RECORDS_NONE (formats without
+ * packed records, and FP64); *dict_entries (optional) = coupling dictionary
+ * size (0 when no compact records were built).  Plans the window if the next
+ * pass would. */
+#define VGPU_RECORDS_NONE 0
+#define VGPU_RECORDS_WIDE 1
+#define VGPU_RECORDS_COMPACT 2
+#define VGPU_RECORDS_WINDOW 3
+int vgpu_record_layout(vgpu_handle h, int32_t* layout, int32_t* dict_entries);
 int vgpu_set_option(vgpu_handle h, int option, int value);
 
 /* Step counter that keys the Philox stream (counter = (atom, step)).  Resume

@@ -20,20 +20,32 @@ def fcc100():
 
 
 def test_staged_equals_plain_with_dipole(vgpu_lib, fcc100):
+    """Plain and staged passes with 16-byte and compact bond records (the
+    default here; 96 dictionary entries: material pair x bond vector), and
+    the window-staged passes, agree bit for bit at 4M spins."""
     from vampire_b200 import system as S
     from vampire_b200 import vgpu as V
     s = copy.copy(fcc100)
     S.dipole_cells(s, size=2 * 3.54, atomic_volume=3.54 ** 3 / 4.0, solver="tensor", update_rate=100)
     out = {}
-    for staged in (0, 1):
+    for staged, compact, window, layout in ((0, 0, 0, V.RECORDS_WIDE), (0, 1, 0, V.RECORDS_COMPACT),
+                                            (1, 0, 0, V.RECORDS_WIDE), (1, 1, 0, V.RECORDS_COMPACT),
+                                            (1, 1, 1, V.RECORDS_WINDOW)):
         with V.Simulation(s, noise_seed=5) as sim:
             sim.set_option(V.OPT_STAGED_RECORDS, staged)
+            sim.set_option(V.OPT_COMPACT_RECORDS, compact)
+            sim.set_option(V.OPT_WINDOW_STAGING, window)
+            sim.set_option(V.OPT_STAGE_BUFFERS, 1 if window else -1)
+            lay, nd = sim.record_layout()
+            assert lay == layout and 0 < nd <= 512
             sim.dipole_setup(s.cells)
             assert sim.dipole_method() == V.DIPOLE_FAR_FFT
             sim.llg_heun(3)
-            out[staged] = sim.spins()
-    np.testing.assert_array_equal(out[0], out[1])
-    assert np.abs(np.linalg.norm(out[1], axis=0) - 1.0).max() < 1e-6
+            out[staged, compact, window] = sim.spins()
+    ref = out[0, 0, 0]
+    for k, v in out.items():
+        np.testing.assert_array_equal(ref, v, err_msg=str(k))
+    assert np.abs(np.linalg.norm(ref, axis=0) - 1.0).max() < 1e-6
 
 
 def test_fp32_follows_fp64_and_energy_decreases(vgpu_lib, fcc100):

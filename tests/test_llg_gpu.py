@@ -147,13 +147,117 @@ def test_stage_option_checks(V):
     from vampire_b200 import system
     s = system.config_fcc_tensor(L=3, seed=7)
     with V.Simulation(s) as sim:
-        for opt, bad in ((V.OPT_STAGED_RECORDS, 2), (V.OPT_STAGE_SLICES, 6), (V.OPT_STAGE_BUFFERS, 3)):
+        for opt, bad in ((V.OPT_STAGED_RECORDS, 2), (V.OPT_STAGE_SLICES, 6), (V.OPT_STAGE_BUFFERS, 3),
+                         (V.OPT_WINDOW_STAGING, 2)):
             with pytest.raises(V.VGPUError) as e:
                 sim.set_option(opt, bad)
             assert e.value.code == V.ERR_ARG
         sim.set_option(V.OPT_STAGED_RECORDS, 1)
         sim.llg_heun(2)
         assert np.isfinite(sim.spins()).all()
+
+
+def _fcc_variant(kind, L):
+    """FCC L^3 tensor exchange + DMI systems for the record-layout tests:
+    "scalar" (isotropic diagonal, the benchmark's physics), "diag" (Jyy, Jzz
+    scaled per bond: a non-scalar material-pair diagonal), "random_d" (a
+    random antisymmetric part per bond: more distinct couplings than the
+    dictionary holds), "open" (open z surfaces: ragged rows)."""
+    from vampire_b200 import system
+    if kind == "open":  # open z surfaces: slices of width 12 and narrower
+        return system.config_fcc_tensor(L=L, seed=7, periodic=(True, True, False))
+    s = system.config_fcc_tensor(L=L, seed=7)
+    if kind == "scalar":
+        return s
+    J = s.jlist.reshape(-1, 3, 3).copy()
+    if kind == "diag":
+        J[:, 1, 1] *= 0.9
+        J[:, 2, 2] *= 1.1
+    else:
+        d = np.random.default_rng(3).normal(scale=0.05, size=(J.shape[0], 3))
+        J[:, 2, 1], J[:, 1, 2] = d[:, 0], -d[:, 0]
+        J[:, 0, 2], J[:, 2, 0] = d[:, 1], -d[:, 1]
+        J[:, 1, 0], J[:, 0, 1] = d[:, 2], -d[:, 2]
+    s.jlist = np.ascontiguousarray(J.ravel())
+    return s
+
+
+@pytest.mark.parametrize("kind", ["scalar", "diag", "open"])
+@pytest.mark.parametrize("L", [5, 12])
+@pytest.mark.parametrize("staged,sl", [(0, 4), (1, 2), (1, 4), (1, 8)])
+def test_compact_records_match_wide(V, kind, L, staged, sl):
+    """Compact records (one word per bond + coupling dictionary) and, in the
+    staged passes, window staging (neighbour spins bulk-copied per tile too)
+    give the 16-byte records' FP32 results bit for bit, for scalar and
+    non-scalar material-pair diagonals and every tile shape."""
+    s = _fcc_variant(kind, L)
+    with V.Simulation(s, noise_seed=11) as wide, V.Simulation(s, noise_seed=11) as comp, \
+            V.Simulation(s, noise_seed=11) as win:
+        for sim in (wide, comp, win):
+            sim.set_option(V.OPT_STAGED_RECORDS, staged)
+            sim.set_option(V.OPT_STAGE_SLICES, sl)
+        wide.set_option(V.OPT_COMPACT_RECORDS, 0)
+        comp.set_option(V.OPT_WINDOW_STAGING, 0)
+        win.set_option(V.OPT_WINDOW_STAGING, 1)
+        win.set_option(V.OPT_STAGE_BUFFERS, 1)
+        lay, nd = comp.record_layout()
+        assert lay == V.RECORDS_COMPACT and 0 < nd <= 512
+        assert wide.record_layout()[0] == V.RECORDS_WIDE
+        assert win.record_layout()[0] == (V.RECORDS_WINDOW if staged else V.RECORDS_COMPACT)
+        for sim in (wide, comp, win):
+            sim.llg_heun(25)
+        np.testing.assert_array_equal(comp.spins(), wide.spins())
+        np.testing.assert_array_equal(win.spins(), wide.spins())
+
+
+def test_window_staging_shards_and_wait_timeout(V):
+    """Window-staged passes on a shard (owned atoms only: the plan is redone
+    for the owned count) match the plain passes, and their bounded wait
+    reports VGPU_ERR_TIMEOUT and recovers like the record-staged passes."""
+    s = _fcc_variant("scalar", 6)
+    with V.Simulation(s, noise_seed=4) as win, V.Simulation(s, noise_seed=4) as plain:
+        plain.set_option(V.OPT_STAGED_RECORDS, 0)
+        win.set_option(V.OPT_WINDOW_STAGING, 1)
+        win.set_option(V.OPT_STAGE_BUFFERS, 1)
+        for sim in (win, plain):
+            sim.set_owned(s.n - 100, 0)
+        assert win.record_layout()[0] == V.RECORDS_WINDOW
+        win.llg_heun(5)
+        plain.llg_heun(5)
+        np.testing.assert_array_equal(win.spins(), plain.spins())
+        start = win.spins()
+        win.set_option(V.OPT_STAGE_WAIT_TEST, 1)
+        with pytest.raises(V.VGPUError) as e:
+            win.llg_heun(1)
+            win.synchronize()
+        assert e.value.code == V.ERR_TIMEOUT
+        win.set_option(V.OPT_STAGE_WAIT_TEST, 0)
+        win.set_spins(start)
+        plain.set_spins(start)
+        win.step = plain.step = 0
+        win.llg_heun(3)
+        plain.llg_heun(3)
+        np.testing.assert_array_equal(win.spins(), plain.spins())
+
+
+def test_compact_records_fallback_and_option(V):
+    """More distinct couplings than the dictionary holds: the upload keeps the
+    16-byte records only, and the passes give the plain passes' results.
+    Option values outside -1..1 are refused."""
+    s = _fcc_variant("random_d", 5)
+    with V.Simulation(s, noise_seed=2) as st, V.Simulation(s, noise_seed=2) as plain:
+        assert st.record_layout() == (V.RECORDS_WIDE, 0)
+        with pytest.raises(V.VGPUError) as e:
+            st.set_option(V.OPT_COMPACT_RECORDS, 2)
+        assert e.value.code == V.ERR_ARG
+        st.set_option(V.OPT_STAGED_RECORDS, 1)
+        plain.set_option(V.OPT_STAGED_RECORDS, 0)
+        st.llg_heun(10)
+        plain.llg_heun(10)
+        np.testing.assert_array_equal(st.spins(), plain.spins())
+    from vampire_b200 import system
+    with V.Simulation(system.config_fcc_tensor(L=3, seed=1), precision="fp64") as sim:
+        assert sim.record_layout()[0] == V.RECORDS_NONE
 
 
 @pytest.mark.parametrize("name,steps", [("sc10_t300", 2), ("sc6_open_t300", 3), ("fcc4_dmi_t300", 2)])

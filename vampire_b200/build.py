@@ -30,7 +30,8 @@ def sources():
 
 
 def deps():
-    return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list((REPO / "include").glob("*.h")))
+    return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h"))
+                  + list((REPO / "include").glob("*.h")))
 
 
 def up_to_date() -> bool:

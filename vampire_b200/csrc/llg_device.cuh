@@ -197,6 +197,93 @@ __device__ __forceinline__ void exchange_gather_w(const LLGArgs<R>& a, int base,
    }
 }
 
+// Row of compile-time width W read from compact records: one word per bond,
+// neighbour | coupling index << crec_shift, the coupling {J, d} taken from the
+// dictionary (shared memory in the staged passes, global otherwise).  Same
+// arithmetic, in the same bond order, as the FMT_DMI_TAB branch above, on the
+// same coupling values, so the two record layouts give identical fields.
+// STAGED: sw points at the thread's first word in shared memory (stride 32).
+template <typename R, int W, int LOAD, bool STAGED>
+__device__ __forceinline__ void exchange_gather_c(const LLGArgs<R>& a, int base, const R* __restrict__ sx,
+                                                  const R* __restrict__ sy, const R* __restrict__ sz, R& hx, R& hy,
+                                                  R& hz, const uint32_t* sw, const float4* dict) {
+   const uint32_t jmask = (1u << a.crec_shift) - 1u;
+   uint32_t c[W];
+#pragma unroll
+   for (int k = 0; k < W; ++k) c[k] = STAGED ? sw[32 * k] : __ldg(a.crec + base + 32 * k);
+   R x[W], y[W], z[W];
+#pragma unroll
+   for (int k = 0; k < W; ++k) {
+      const int j = (int)(c[k] & jmask);
+      x[k] = ld_src(sx + j, LOAD); y[k] = ld_src(sy + j, LOAD); z[k] = ld_src(sz + j, LOAD);
+   }
+#pragma unroll
+   for (int k = 0; k < W; ++k) {
+      const uint32_t q = c[k] >> a.crec_shift;
+      const float4 e = dict[q];
+      const R dx = e.y, dy = e.z, dz = e.w;
+      if (a.tab_scalar) {
+         const R J = e.x;
+         hx += J * x[k] + (dy * z[k] - dz * y[k]);
+         hy += J * y[k] + (dz * x[k] - dx * z[k]);
+         hz += J * z[k] + (dx * y[k] - dy * x[k]);
+      } else {
+         const float4 e2 = dict[a.cdict_n + q];
+         hx += (R)e.x * x[k] + (dy * z[k] - dz * y[k]);
+         hy += (R)e2.x * y[k] + (dz * x[k] - dx * z[k]);
+         hz += (R)e2.y * z[k] + (dx * y[k] - dy * x[k]);
+      }
+   }
+}
+
+// Row read from window-staged records: per bond the word slot | coupling
+// index << 16, the neighbour spin taken from the tile's window of spins in
+// shared memory (wx, wx + wmax, wx + 2 wmax) and the coupling from the
+// dictionary.  W > 0: compile-time width (all loads of the row first); W = 0:
+// width w_rt.  Same arithmetic, in the same bond order, on the same values as
+// exchange_gather_c, so the results are identical.
+template <typename R, int W>
+__device__ __forceinline__ void exchange_gather_win(const LLGArgs<R>& a, int w_rt, R& hx, R& hy, R& hz,
+                                                    const uint32_t* sw, const float4* dict, const float* wx,
+                                                    int wmax) {
+   const float* wy = wx + wmax;
+   const float* wz = wy + wmax;
+   auto bond = [&](uint32_t c, R x, R y, R z) {
+      const float4 e = dict[c >> 16];
+      const R dx = e.y, dy = e.z, dz = e.w;
+      if (a.tab_scalar) {
+         const R J = e.x;
+         hx += J * x + (dy * z - dz * y);
+         hy += J * y + (dz * x - dx * z);
+         hz += J * z + (dx * y - dy * x);
+      } else {
+         const float4 e2 = dict[a.cdict_n + (c >> 16)];
+         hx += (R)e.x * x + (dy * z - dz * y);
+         hy += (R)e2.x * y + (dz * x - dx * z);
+         hz += (R)e2.y * z + (dx * y - dy * x);
+      }
+   };
+   if (W > 0) {
+      uint32_t c[W > 0 ? W : 1];
+      R x[W > 0 ? W : 1], y[W > 0 ? W : 1], z[W > 0 ? W : 1];
+#pragma unroll
+      for (int k = 0; k < W; ++k) c[k] = sw[32 * k];
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+         const int s = (int)(c[k] & 0xffffu);
+         x[k] = wx[s]; y[k] = wy[s]; z[k] = wz[s];
+      }
+#pragma unroll
+      for (int k = 0; k < W; ++k) bond(c[k], x[k], y[k], z[k]);
+   } else {
+      for (int k = 0; k < w_rt; ++k) {
+         const uint32_t c = sw[32 * k];
+         const int s = (int)(c & 0xffffu);
+         bond(c, wx[s], wy[s], wz[s]);
+      }
+   }
+}
+
 // biquadratic exchange field of atom i at own spin S over its SELL-32 list:
 // sum_j 2 J_bq (S.s_j) s_j (src/exchange/biquadratic_fields.cpp:60-76)
 template <typename R, int LOAD = 0>
@@ -241,12 +328,37 @@ __device__ __forceinline__ E biquadratic_energy(const LLGArgs<R>& a, int i, cons
 
 // exchange field with the fixed-width fast paths (FP32, packed records).
 // STAGED (FMT_DMI_TAB only): srec_tile is the shared-memory copy of the
-// records of the tile starting at slice_off[tile_slice0].
-template <typename R, int FMT, int LOAD, bool STAGED = false>
+// records of the tile starting at slice_off[tile_slice0] (16-byte records, or
+// compact words when a.crec is set, with the dictionary copied to sdict).
+// REC: which FP32 DMI record layout the caller was compiled for (REC_ANY:
+// compact when a.crec is set, else 16-byte; the staged passes fix one).
+template <typename R, int FMT, int LOAD, bool STAGED = false, int REC = REC_ANY>
 __device__ __forceinline__ void exchange_field(const LLGArgs<R>& a, int i, int mi, const R* __restrict__ sx,
                                                const R* __restrict__ sy, const R* __restrict__ sz, R& hx, R& hy,
-                                               R& hz, const int4* srec_tile = nullptr, int tile_off = 0) {
-   if (sizeof(R) == 4 && (FMT == FMT_DMI_TAB || FMT == FMT_ISO_TAB) && (FMT == FMT_ISO_TAB || a.rec)) {
+                                               R& hz, const int4* srec_tile = nullptr, int tile_off = 0,
+                                               const float4* sdict = nullptr, const float* swin = nullptr,
+                                               int wmax = 0) {
+   if (REC == REC_WINDOW) {  // staged window passes (FP32 FMT_DMI_TAB): every width from shared memory
+      const int sl = i >> 5;
+      const int off = __ldg(a.slice_off + sl);
+      const int w = (__ldg(a.slice_off + sl + 1) - off) >> 5;
+      const uint32_t* sw = reinterpret_cast<const uint32_t*>(srec_tile) + (off + (i & 31) - tile_off);
+      if (w == 12) exchange_gather_win<R, 12>(a, w, hx, hy, hz, sw, sdict, swin, wmax);
+      else if (w == 6) exchange_gather_win<R, 6>(a, w, hx, hy, hz, sw, sdict, swin, wmax);
+      else exchange_gather_win<R, 0>(a, w, hx, hy, hz, sw, sdict, swin, wmax);
+      return;
+   }
+   if (sizeof(R) == 4 && FMT == FMT_DMI_TAB && REC != REC_WIDE && (REC == REC_COMPACT || a.crec)) {
+      const int sl = i >> 5;
+      const int off = __ldg(a.slice_off + sl);
+      const int w = (__ldg(a.slice_off + sl + 1) - off) >> 5;
+      const int base = off + (i & 31);
+      const uint32_t* sw = STAGED ? reinterpret_cast<const uint32_t*>(srec_tile) + (base - tile_off) : nullptr;
+      const float4* dict = STAGED ? sdict : a.cdict;
+      if (w == 12) { exchange_gather_c<R, 12, LOAD, STAGED>(a, base, sx, sy, sz, hx, hy, hz, sw, dict); return; }
+      if (w == 6) { exchange_gather_c<R, 6, LOAD, STAGED>(a, base, sx, sy, sz, hx, hy, hz, sw, dict); return; }
+   } else if (sizeof(R) == 4 && (FMT == FMT_DMI_TAB || FMT == FMT_ISO_TAB) && REC != REC_COMPACT &&
+              (FMT == FMT_ISO_TAB || a.rec)) {
       const int sl = i >> 5;
       const int off = __ldg(a.slice_off + sl);
       const int w = (__ldg(a.slice_off + sl + 1) - off) >> 5;
@@ -262,12 +374,15 @@ __device__ __forceinline__ void exchange_field(const LLGArgs<R>& a, int i, int m
 // (calculate_spin_fields, src/simulate/fields.cpp:67-118)
 // EXT = false compiles the passes without the higher-order anisotropy terms
 // (register budget of the common case); launchers pick EXT from a.aniso_ext.
-template <typename R, int FMT, int LOAD = 0, bool STAGED = false, bool EXT = true>
+template <typename R, int FMT, int LOAD = 0, bool STAGED = false, bool EXT = true, int REC = REC_ANY>
 __device__ __forceinline__ void spin_field(const LLGArgs<R>& a, int i, int mi, const MatParams<R>& m,
                                            const R* sx, const R* sy, const R* sz, const R S[3], R H[3],
-                                           const int4* srec_tile = nullptr, int tile_off = 0) {
+                                           const int4* srec_tile = nullptr, int tile_off = 0,
+                                           const float4* sdict = nullptr, const float* swin = nullptr,
+                                           int wmax = 0) {
    R hx = 0, hy = 0, hz = 0;
-   exchange_field<R, FMT, LOAD, STAGED>(a, i, mi, sx, sy, sz, hx, hy, hz, srec_tile, tile_off);
+   exchange_field<R, FMT, LOAD, STAGED, REC>(a, i, mi, sx, sy, sz, hx, hy, hz, srec_tile, tile_off, sdict, swin,
+                                             wmax);
    if (EXT && a.bq_off) {
       // biquadratic exchange (exchange/biquadratic_fields.cpp): its own sum,
       // added to the bilinear field as exchange::fields does

@@ -8,15 +8,27 @@ template cudaError_t launch_thermal_noise<float>(const LLGArgs<float>&, cudaStre
 
 int stage_tile_bytes(const std::vector<int>& slice_off, int sl) { return staged_tile_bytes(slice_off, sl); }
 
-template <int MODE, int SL, int NBUF>
+template <int MODE, int SL, int NBUF, bool CREC>
 static const void* staged_fn() {
-   return (const void*)llg_staged_kernel<MODE, SL, NBUF>;
+   return (const void*)llg_staged_kernel<MODE, SL, NBUF, CREC>;
 }
 
-static const void* staged_fn(int mode, int sl, int nbuf) {
+static const void* window_fn(int mode, int sl) {
    const bool p = mode == PASS_PREDICTOR;
-#define VGPU_FN(S, B) \
-   if (sl == S && nbuf == B) return p ? staged_fn<PASS_PREDICTOR, S, B>() : staged_fn<PASS_CORRECTOR, S, B>();
+#define VGPU_FN(S) \
+   if (sl == S) return p ? (const void*)llg_window_kernel<PASS_PREDICTOR, S> : (const void*)llg_window_kernel<PASS_CORRECTOR, S>;
+   VGPU_FN(2) VGPU_FN(4) VGPU_FN(8)
+#undef VGPU_FN
+   return nullptr;
+}
+
+static const void* staged_fn(int mode, int sl, int nbuf, bool crec) {
+   const bool p = mode == PASS_PREDICTOR;
+#define VGPU_FN(S, B)                                                                                          \
+   if (sl == S && nbuf == B) {                                                                                 \
+      if (crec) return p ? staged_fn<PASS_PREDICTOR, S, B, true>() : staged_fn<PASS_CORRECTOR, S, B, true>();  \
+      return p ? staged_fn<PASS_PREDICTOR, S, B, false>() : staged_fn<PASS_CORRECTOR, S, B, false>();          \
+   }
    VGPU_FN(2, 1) VGPU_FN(2, 2) VGPU_FN(4, 1) VGPU_FN(4, 2) VGPU_FN(8, 1) VGPU_FN(8, 2)
 #undef VGPU_FN
    return nullptr;
@@ -25,7 +37,8 @@ static const void* staged_fn(int mode, int sl, int nbuf) {
 cudaError_t prepare_llg_staged(StageCfg& c, int nslices, int device) {
    c.grid = 0;
    if (!(c.sl == 2 || c.sl == 4 || c.sl == 8) || !(c.nbuf == 1 || c.nbuf == 2)) return cudaErrorInvalidValue;
-   const int smem = c.nbuf * c.buf_bytes;
+   if (c.win && (c.nbuf != 1 || !c.crec)) return cudaErrorInvalidValue;
+   const int smem = c.win ? c.buf_bytes + 12 * c.wmax + c.dict_bytes : c.nbuf * c.buf_bytes + c.dict_bytes;
    int sms = 0, optin = 0;
    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
@@ -33,7 +46,7 @@ cudaError_t prepare_llg_staged(StageCfg& c, int nslices, int device) {
    if (smem > optin - 64) return cudaErrorInvalidValue;  // room for the static mbarriers
    int per_sm = 1 << 30;
    for (int mode = PASS_PREDICTOR; mode <= PASS_CORRECTOR; ++mode) {
-      const void* f = staged_fn(mode, c.sl, c.nbuf);
+      const void* f = c.win ? window_fn(mode, c.sl) : staged_fn(mode, c.sl, c.nbuf, c.crec);
       if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
       int nb = 0;
       if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, 32 * c.sl, smem)) != cudaSuccess) return e;
@@ -47,18 +60,37 @@ cudaError_t prepare_llg_staged(StageCfg& c, int nslices, int device) {
 
 cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, const StageCfg& c, cudaStream_t st) {
    if (c.grid == 0) return cudaSuccess;
-   const int smem = c.nbuf * c.buf_bytes;
+   if ((a.crec != nullptr) != c.crec) return cudaErrorInvalidValue;  // record layout of the prepared shape
    const dim3 g(c.grid), b(32 * c.sl);
+   if (c.win) {
+      if (!a.lrec || !a.wseg) return cudaErrorInvalidValue;
+      const int smem = c.buf_bytes + 12 * c.wmax + c.dict_bytes;
+#define VGPU_WIN(S)                                                                                            \
+   if (c.sl == S) {                                                                                            \
+      if (mode == PASS_PREDICTOR)                                                                              \
+         llg_window_kernel<PASS_PREDICTOR, S><<<g, b, smem, st>>>(a, nslices, c.buf_bytes, c.wmax);            \
+      else                                                                                                     \
+         llg_window_kernel<PASS_CORRECTOR, S><<<g, b, smem, st>>>(a, nslices, c.buf_bytes, c.wmax);            \
+      return cudaGetLastError();                                                                               \
+   }
+      VGPU_WIN(2) VGPU_WIN(4) VGPU_WIN(8)
+#undef VGPU_WIN
+      return cudaErrorInvalidValue;
+   }
+   const int smem = c.nbuf * c.buf_bytes + c.dict_bytes;
+#define VGPU_STAGED_C(S, B, C)                                                                                 \
+   if (mode == PASS_PREDICTOR)                                                                                 \
+      llg_staged_kernel<PASS_PREDICTOR, S, B, C><<<g, b, smem, st>>>(a, nslices, c.ntiles, c.buf_bytes);       \
+   else                                                                                                        \
+      llg_staged_kernel<PASS_CORRECTOR, S, B, C><<<g, b, smem, st>>>(a, nslices, c.ntiles, c.buf_bytes);
 #define VGPU_STAGED(S, B)                                                                                      \
    if (c.sl == S && c.nbuf == B) {                                                                             \
-      if (mode == PASS_PREDICTOR)                                                                              \
-         llg_staged_kernel<PASS_PREDICTOR, S, B><<<g, b, smem, st>>>(a, nslices, c.ntiles, c.buf_bytes);       \
-      else                                                                                                     \
-         llg_staged_kernel<PASS_CORRECTOR, S, B><<<g, b, smem, st>>>(a, nslices, c.ntiles, c.buf_bytes);       \
+      if (c.crec) { VGPU_STAGED_C(S, B, true) } else { VGPU_STAGED_C(S, B, false) }                            \
       return cudaGetLastError();                                                                               \
    }
    VGPU_STAGED(2, 1) VGPU_STAGED(2, 2) VGPU_STAGED(4, 1) VGPU_STAGED(4, 2) VGPU_STAGED(8, 1) VGPU_STAGED(8, 2)
 #undef VGPU_STAGED
+#undef VGPU_STAGED_C
    return cudaErrorInvalidValue;
 }
 }  // namespace vgpu

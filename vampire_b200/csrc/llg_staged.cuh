@@ -1,7 +1,9 @@
 // Fused LLG-Heun passes with bulk-staged bond records (FP32, FMT_DMI_TAB).
 //
 // The per-bond records {neighbour, d_x, d_y, d_z} are the bulk of the HBM
-// stream (12 x 16 B per atom per pass).  In the plain pass every thread loads
+// stream (12 x 16 B per atom per pass), or with compact records (CREC) one
+// 4-byte word per bond, neighbour | coupling index, whose couplings come from
+// a dictionary that every block first copies into its shared memory.  In the plain pass every thread loads
 // its own twelve; here a block walks tiles of 32 SL atoms and thread 0
 // issues ONE cp.async.bulk (1-D bulk copy, global -> this CTA's shared memory,
 // no multicast) for the whole contiguous record range of a tile, completing on
@@ -82,39 +84,48 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* m, uint32_t parity) 
 // SL slices (32 SL atoms) per tile, NBUF = 1 (one tile per block, the other
 // resident blocks hide the copy) or 2 (persistent, next tile's copy in flight
 // while this one is computed).  Dynamic shared memory: NBUF * buf_bytes.
-// (Capping registers for more resident blocks -- the corrector at 64 -- was
-// measured 3-5 % slower: the compiler's own 56/72 are kept.)
-template <int MODE, int SL, int NBUF>
-__global__ void __launch_bounds__(32 * SL) llg_staged_kernel(const LLGArgs<float> a, int nslices, int ntiles,
+// Registers are capped for 768 resident threads per SM (85 a thread): the
+// compact-record corrector otherwise takes 92 and fits 5 blocks of 128
+// (measured 12 % slower); a cap at 64 spills and was slower again.
+template <int MODE, int SL, int NBUF, bool CREC>
+__global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGArgs<float> a, int nslices, int ntiles,
                                                              int buf_bytes) {
    extern __shared__ __align__(128) unsigned char stage_smem[];
    __shared__ __align__(8) uint64_t mbar[2];
    const int tid = threadIdx.x;
+   // compact records: the coupling dictionary follows the record buffers; it
+   // arrives with the block's first tile copy
+   float4* sdict = reinterpret_cast<float4*>(stage_smem + NBUF * buf_bytes);
+   const uint32_t dict_bytes = CREC ? 16u * (uint32_t)(a.tab_scalar ? a.cdict_n : 2 * a.cdict_n) : 0u;
    if (tid == 0) {
       mbar_init(&mbar[0], 1);
       mbar_init(&mbar[1], 1);
       fence_mbar_init();
    }
    __syncthreads();
-   // thread 0: expect the tile's record bytes and start its bulk copy
-   auto issue = [&](int t, int b) {
+   // thread 0: expect the tile's record bytes and start its bulk copy (and,
+   // with the first tile, the dictionary's)
+   auto issue = [&](int t, int b, bool first) {
       const int s0 = t * SL;
       const int s1 = min(s0 + SL, nslices);
       const int o0 = __ldg(a.slice_off + s0), o1 = __ldg(a.slice_off + s1);
-      const uint32_t bytes = (uint32_t)(o1 - o0) * 16u;
+      const uint32_t bytes = (uint32_t)(o1 - o0) * (CREC ? 4u : 16u);
+      const void* src = CREC ? (const void*)(a.crec + o0) : (const void*)(a.rec + o0);
+      const uint32_t db = first ? dict_bytes : 0u;
       fence_proxy_async();
-      mbar_arrive_expect_tx(&mbar[b], bytes + (uint32_t)a.stage_extra_tx);
-      if (bytes) bulk_copy_g2s(stage_smem + b * buf_bytes, a.rec + o0, bytes, &mbar[b]);
+      mbar_arrive_expect_tx(&mbar[b], bytes + db + (uint32_t)a.stage_extra_tx);
+      if (bytes) bulk_copy_g2s(stage_smem + b * buf_bytes, src, bytes, &mbar[b]);
+      if (db) bulk_copy_g2s(sdict, a.cdict, db, &mbar[b]);
    };
    uint32_t phase = 0;  // bit b: parity of the phase of mbar[b] to wait for next
    int t = blockIdx.x, k = 0, b = 0;
    bool failed = false;
-   if (NBUF == 2 && t < ntiles && tid == 0) issue(t, 0);
+   if (NBUF == 2 && t < ntiles && tid == 0) issue(t, 0, true);
    for (; t < ntiles; t += gridDim.x, ++k) {
       b = NBUF == 1 ? 0 : (k & 1);
       if (tid == 0) {
-         if (NBUF == 1) issue(t, 0);
-         else if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, b ^ 1);
+         if (NBUF == 1) issue(t, 0, k == 0);
+         else if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, b ^ 1, false);
       }
       // own-atom work that needs no records overlaps the copy: state, material,
       // external field (Philox noise, applied, dipole cell field)
@@ -139,16 +150,17 @@ __global__ void __launch_bounds__(32 * SL) llg_staged_kernel(const LLGArgs<float
       if (act) {
          float H[3];
          if (MODE == PASS_PREDICTOR) {
-            spin_field<float, FMT_DMI_TAB, 0, true, false>(a, i, mi, m, a.ax, a.ay, a.az, S0, H, sb, tile_off);
+            spin_field<float, FMT_DMI_TAB, 0, true, false, CREC ? REC_COMPACT : REC_WIDE>(a, i, mi, m, a.ax, a.ay, a.az, S0, H, sb, tile_off, sdict);
             H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
             llg_predict_finish<float>(a, i, m, S0, H);
          } else {
-            spin_field<float, FMT_DMI_TAB, 0, true, false>(a, i, mi, m, a.bx, a.by, a.bz, S1, H, sb, tile_off);
+            spin_field<float, FMT_DMI_TAB, 0, true, false, CREC ? REC_COMPACT : REC_WIDE>(a, i, mi, m, a.bx, a.by, a.bz, S1, H, sb, tile_off, sdict);
             H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
             llg_correct_finish<float>(a, i, m, S0, S1, H);
          }
       }
-      __syncthreads();  // buffer b fully read before it is refilled
+      // buffer b fully read before it is refilled (one tile per block: never)
+      if (NBUF == 2 || t + (int)gridDim.x < ntiles) __syncthreads();
    }
    if (failed) {
       if (tid == 0) {
@@ -161,7 +173,97 @@ __global__ void __launch_bounds__(32 * SL) llg_staged_kernel(const LLGArgs<float
    }
 }
 
-// bytes of the largest tile's record range (buffer size) for the host
+// Window-staged passes (FP32 compact records): besides the tile's bond words,
+// the neighbour spins the tile reads are bulk-copied into shared memory too,
+// as the tile's "window": the few contiguous atom ranges (segments) that hold
+// every neighbour of the tile's atoms (for a lattice numbered cell by cell,
+// the neighbouring rows of cells), planned on the host, each word naming its
+// neighbour by window slot.  Warp 0 sets the expected bytes and issues one
+// bulk copy per segment and spin component plus one for the words; the
+// gathers then read shared memory only.  One tile per block.  Shared memory:
+// words (rec_bytes), three components of wmax slots, the dictionary.
+template <int MODE, int SL>
+__global__ void __launch_bounds__(32 * SL, 24 / SL) llg_window_kernel(const LLGArgs<float> a, int nslices,
+                                                                       int rec_bytes, int wmax) {
+   extern __shared__ __align__(128) unsigned char stage_smem[];
+   __shared__ __align__(8) uint64_t mbar;
+   const int tid = threadIdx.x;
+   const int t = blockIdx.x;
+   const uint32_t* swords = reinterpret_cast<const uint32_t*>(stage_smem);
+   float* wx = reinterpret_cast<float*>(stage_smem + rec_bytes);
+   float4* sdict = reinterpret_cast<float4*>(wx + 3 * wmax);
+   const int s0 = t * SL;
+   const int tile_off = __ldg(a.slice_off + s0);
+   // warp 0 initialises the barrier and issues every copy at once (words,
+   // dictionary, window segments); the other warps see the initialised
+   // barrier after the block barrier below, before they wait on it
+   if (tid < 32) {
+      if (tid == 0) {
+         mbar_init(&mbar, 1);
+         fence_mbar_init();
+      }
+      __syncwarp();
+      const int o1 = __ldg(a.slice_off + min(s0 + SL, nslices));
+      const int sb = __ldg(a.wtile_seg + t), se = __ldg(a.wtile_seg + t + 1);
+      const uint32_t rb = (uint32_t)(o1 - tile_off) * 4u;
+      const uint32_t db = 16u * (uint32_t)(a.tab_scalar ? a.cdict_n : 2 * a.cdict_n);
+      if (tid == 0) {
+         fence_proxy_async();
+         mbar_arrive_expect_tx(&mbar, rb + db + 12u * (uint32_t)__ldg(a.wtile_w + t) + (uint32_t)a.stage_extra_tx);
+         if (rb) bulk_copy_g2s(stage_smem, a.lrec + tile_off, rb, &mbar);
+         bulk_copy_g2s(sdict, a.cdict, db, &mbar);
+      }
+      __syncwarp();
+      const float* gx = MODE == PASS_PREDICTOR ? a.ax : a.bx;
+      const float* gy = MODE == PASS_PREDICTOR ? a.ay : a.by;
+      const float* gz = MODE == PASS_PREDICTOR ? a.az : a.bz;
+      for (int q = sb + tid; q < se; q += 32) {
+         const int4 g = __ldg(a.wseg + q);  // {first atom, atoms, first slot, 0}
+         const uint32_t nb = 4u * (uint32_t)g.y;
+         bulk_copy_g2s(wx + g.z, gx + g.x, nb, &mbar);
+         bulk_copy_g2s(wx + wmax + g.z, gy + g.x, nb, &mbar);
+         bulk_copy_g2s(wx + 2 * wmax + g.z, gz + g.x, nb, &mbar);
+      }
+   }
+   // own-atom work overlapping the copies: state, material, external field
+   const int i = s0 * 32 + tid;
+   const bool act = i < a.n_upd;
+   const int ii = act ? i : a.n_upd - 1;
+   const int mi = a.mat ? __ldg(a.mat + ii) : 0;
+   const MatParams<float> m = a.mp[mi];
+   float S0[3] = {a.ax[ii], a.ay[ii], a.az[ii]};
+   float S1[3];
+   if (MODE == PASS_CORRECTOR) { S1[0] = a.bx[ii]; S1[1] = a.by[ii]; S1[2] = a.bz[ii]; }
+   float E[3];
+   external_field<float>(a, ii, m, true, E);
+   __syncthreads();  // the barrier's initialisation is visible to every thread
+   const bool done = mbar_wait_bounded(&mbar, 0);
+   if (__syncthreads_or(!done)) {
+      if (tid == 0) {
+         atomicOr(a.status, 2);
+         mbar_wait_bounded(&mbar, 0);  // copies still in flight
+      }
+      __syncthreads();
+      return;
+   }
+   if (!act) return;
+   const int4* sb = reinterpret_cast<const int4*>(swords);
+   float H[3];
+   if (MODE == PASS_PREDICTOR) {
+      spin_field<float, FMT_DMI_TAB, 0, true, false, REC_WINDOW>(a, i, mi, m, a.ax, a.ay, a.az, S0, H, sb, tile_off,
+                                                                 sdict, wx, wmax);
+      H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
+      llg_predict_finish<float>(a, i, m, S0, H);
+   } else {
+      spin_field<float, FMT_DMI_TAB, 0, true, false, REC_WINDOW>(a, i, mi, m, a.bx, a.by, a.bz, S1, H, sb, tile_off,
+                                                                 sdict, wx, wmax);
+      H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
+      llg_correct_finish<float>(a, i, m, S0, S1, H);
+   }
+}
+
+// bytes of the largest tile's 16-byte record range (buffer size) for the
+// host; compact records take a quarter of it
 inline int staged_tile_bytes(const std::vector<int>& slice_off, int sl) {
    const int nsl = (int)slice_off.size() - 1;
    int mx = 0;

@@ -7,7 +7,11 @@
 // bond's coupling exactly (ExchFmt in vgpu_internal.cuh): couplings that are
 // a function of the two materials go to a small table and the neighbour's
 // material rides in the top bits of its index, so the only per-bond bytes
-// left in HBM are the index and, for DMI, the antisymmetric vector.
+// left in HBM are the index and, for DMI, the antisymmetric vector.  When a
+// DMI system has few distinct couplings (a crystal: one per bond direction
+// and material pair), the FP32 passes take compact records instead: one word
+// per bond holding the neighbour and the index of its coupling in a small
+// dictionary (build_compact_records).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -20,6 +24,7 @@
 #include <string>
 #include <vector>
 
+#include "record_plan.h"
 #include "vgpu_ctx.cuh"
 
 using namespace vgpu;
@@ -66,6 +71,14 @@ void* vgpu_ctx::alloc(size_t bytes) {
 namespace vgpu {
 
 }  // namespace vgpu
+
+void vgpu_ctx::release(void* p) {
+   if (!p) return;
+   auto it = std::find(allocs.begin(), allocs.end(), p);
+   if (it == allocs.end()) return;
+   cudaFree(p);
+   allocs.erase(it);
+}
 
 void vgpu_ctx::free_system() {
    for (void* p : allocs) cudaFree(p);
@@ -242,7 +255,10 @@ static int upload_typed(vgpu_ctx* h, const vgpu_system_desc* d) {
       }
    }
    std::vector<int> mat(d->type, d->type + n);
-   std::vector<R> ax(n_alloc, (R)0), ay(n_alloc, (R)0), az(n_alloc, (R)0);
+   // state arrays padded to a multiple of 4 entries: window copies move whole
+   // 16-byte groups of atoms, the last one reaching up to entry n_alloc4 - 1
+   const int n_alloc4 = (n_alloc + 3) & ~3;
+   std::vector<R> ax(n_alloc4, (R)0), ay(n_alloc4, (R)0), az(n_alloc4, (R)0);
    for (int i = 0; i < n; ++i) { ax[i] = (R)d->sx[i]; ay[i] = (R)d->sy[i]; az[i] = (R)d->sz[i]; }
 
    h->free_system();
@@ -279,6 +295,20 @@ static int upload_typed(vgpu_ctx* h, const vgpu_system_desc* d) {
       S.stage_bytes[0] = stage_tile_bytes(off, 2);
       S.stage_bytes[1] = stage_tile_bytes(off, 4);
       S.stage_bytes[2] = stage_tile_bytes(off, 8);
+      if constexpr (sizeof(R) == 4) {
+         std::vector<uint32_t> crec;
+         std::vector<float> dict;
+         int ndict = 0;
+         if (build_compact_records(off, col, n, d->type, M, shift, use_shift, jb, scalar, tabS, tabR, crec, dict,
+                                   ndict)) {
+            if ((rc = upload_vec(h, &S.crec, crec, "compact bond records"))) return rc;
+            if ((rc = upload_vec(h, &S.cdict, dict, "coupling dictionary"))) return rc;
+            S.crec_shift = shift;
+            S.cdict_n = ndict;
+            S.crec_host = std::move(crec);
+            S.off_host = off;
+         }
+      }
    }
    if ((rc = upload_vec(h, &S.jtab, tabR, "coupling table"))) return rc;
    S.tab_scalar = scalar;
@@ -287,7 +317,7 @@ static int upload_typed(vgpu_ctx* h, const vgpu_system_desc* d) {
    if ((rc = upload_vec(h, &S.s[0], ax, "spins"))) return rc;
    if ((rc = upload_vec(h, &S.s[1], ay, "spins"))) return rc;
    if ((rc = upload_vec(h, &S.s[2], az, "spins"))) return rc;
-   std::vector<R> zeros(n_alloc, (R)0);
+   std::vector<R> zeros(n_alloc4, (R)0);
    for (int q = 0; q < 3; ++q)
       if ((rc = upload_vec(h, &S.p[q], zeros, "predictor state"))) return rc;
    S.mp = h->alloc(sizeof(MatParams<R>) * M);
@@ -367,6 +397,18 @@ LLGArgs<R> make_args(vgpu_ctx* h) {
    a.mat_shift = S.mat_shift;
    for (int q = 0; q < 9; ++q) a.jb[q] = (const R*)S.jb[q];
    a.rec = (const int4*)S.rec;
+   if (h->compact != 0 && S.crec) {
+      a.crec = (const uint32_t*)S.crec;
+      a.cdict = (const float4*)S.cdict;
+      a.crec_shift = S.crec_shift;
+      a.cdict_n = S.cdict_n;
+      if (S.win_ok) {
+         a.lrec = (const uint32_t*)S.lrec;
+         a.wseg = (const int4*)S.wseg;
+         a.wtile_seg = (const int*)S.wtile_seg;
+         a.wtile_w = (const int*)S.wtile_w;
+      }
+   }
    a.tab_scalar = S.tab_scalar;
    a.jtab_s = (const R*)S.jtab_s;
    a.jtab = (const R*)S.jtab;
@@ -432,6 +474,23 @@ static int ensure_increment(vgpu_ctx* h) {
 
 static int stage_slot(int sl) { return sl == 2 ? 0 : sl == 4 ? 1 : 2; }
 
+// Staged tile shape in use: the options when set, else the measured best per
+// record layout (FMT_DMI_TAB FCC 100^3 on B200): 16-byte records one tile of
+// 4 slices per block (double buffering halves the resident blocks); compact
+// records persistent blocks, two buffers of 2-slice tiles (the next tile's
+// copy in flight while this one is computed).
+static bool compact_in_use(const vgpu_ctx* h) { return h->compact != 0 && h->sys.crec; }
+static int stage_sl_of(const vgpu_ctx* h) { return h->stage_sl > 0 ? h->stage_sl : compact_in_use(h) ? 2 : 4; }
+static int stage_nbuf_of(const vgpu_ctx* h) {
+   return h->stage_nbuf > 0 ? h->stage_nbuf : compact_in_use(h) ? 2 : 1;
+}
+// window staging is opt-in: measured slower than the L1/L2 gathers of the
+// compact passes (one-tile blocks wait for the whole window to land)
+static bool window_wanted(const vgpu_ctx* h) {
+   return h->window == 1 && h->staged != 0 && compact_in_use(h) && stage_nbuf_of(h) == 1;
+}
+static int stage_dict_bytes(const SysDev& S) { return S.cdict_n * 16 * (S.tab_scalar ? 1 : 2); }
+
 // bulk-staged passes: FP32 packed records whose tiles fit shared memory.
 // Default (-1): on when the two buffers of a tile fit.
 template <typename R>
@@ -439,8 +498,9 @@ static bool use_staged(vgpu_ctx* h) {
    const SysDev& S = h->sys;
    // the staged passes carry no higher-order anisotropy terms (register budget)
    if (sizeof(R) != 4 || !S.rec || S.n == 0 || h->staged == 0 || S.aniso_ext || S.bq_off) return false;
-   const int bytes = S.stage_bytes[stage_slot(h->stage_sl)];
-   return h->stage_nbuf * bytes <= kStageSmemLimit;
+   const bool crec = h->compact != 0 && S.crec;
+   const int bytes = S.stage_bytes[stage_slot(stage_sl_of(h))] / (crec ? 4 : 1);
+   return stage_nbuf_of(h) * bytes + (crec ? stage_dict_bytes(S) : 0) <= kStageSmemLimit;
 }
 
 template <typename R>
@@ -451,6 +511,45 @@ static cudaError_t launch_step_pass(vgpu_ctx* h, const LLGArgs<R>& a, int mode, 
    return launch_llg_pass<R>(a, h->sys.fmt, mode, h->sys.nslices, h->stream);
 }
 
+// window plan for the current tile shape and owned atoms (window-staged
+// passes: FP32 compact records, staged, one buffer); S.win_ok tells whether
+// the passes use it
+static int ensure_window_plan(vgpu_ctx* h) {
+   SysDev& S = h->sys;
+   const bool want = window_wanted(h);
+   if (!want) {
+      S.win_ok = false;
+      return VGPU_OK;
+   }
+   if (S.win_sl == stage_sl_of(h) && S.win_nupd == S.n_owned) {
+      S.win_ok = S.lrec != nullptr;
+      return VGPU_OK;
+   }
+   for (void** p : {&S.lrec, &S.wseg, &S.wtile_seg, &S.wtile_w}) {
+      h->release(*p);
+      *p = nullptr;
+   }
+   S.win_sl = stage_sl_of(h);
+   S.win_nupd = S.n_owned;
+   S.win_ok = false;
+   std::vector<uint32_t> lrec;
+   std::vector<int4> segs;
+   std::vector<int> tseg, tw;
+   int wmax = 0;
+   if (S.n_owned == 0 ||
+       !build_window_plan(S.off_host, S.crec_host, S.crec_shift, S.win_sl, (S.n_owned + 31) / 32, lrec, segs, tseg,
+                          tw, wmax))
+      return VGPU_OK;
+   int rc;
+   if ((rc = upload_vec(h, &S.lrec, lrec, "window bond words"))) return rc;
+   if ((rc = upload_vec(h, &S.wseg, segs, "window segments"))) return rc;
+   if ((rc = upload_vec(h, &S.wtile_seg, tseg, "window tile segments"))) return rc;
+   if ((rc = upload_vec(h, &S.wtile_w, tw, "window tile slots"))) return rc;
+   S.wmax = (wmax + 3) & ~3;
+   S.win_ok = true;
+   return VGPU_OK;
+}
+
 // increment buffers and the staged launch shape, before any pass
 template <typename R>
 static int prepare_passes(vgpu_ctx* h, bool* staged_out, int integrator = INTEG_HEUN) {
@@ -458,10 +557,15 @@ static int prepare_passes(vgpu_ctx* h, bool* staged_out, int integrator = INTEG_
    if (rc0) return rc0;
    const bool staged = integrator == INTEG_HEUN && use_staged<R>(h);
    if (staged && h->sys.stage.grid == 0) {
+      if ((rc0 = ensure_window_plan(h))) return rc0;
       StageCfg c;
-      c.sl = h->stage_sl;
-      c.nbuf = h->stage_nbuf;
-      c.buf_bytes = h->sys.stage_bytes[stage_slot(c.sl)];
+      c.sl = stage_sl_of(h);
+      c.nbuf = stage_nbuf_of(h);
+      c.crec = h->compact != 0 && h->sys.crec;
+      c.buf_bytes = h->sys.stage_bytes[stage_slot(c.sl)] / (c.crec ? 4 : 1);
+      c.dict_bytes = c.crec ? stage_dict_bytes(h->sys) : 0;
+      c.win = c.crec && h->sys.win_ok && c.buf_bytes + 12 * h->sys.wmax + c.dict_bytes <= kStageSmemLimit;
+      c.wmax = c.win ? h->sys.wmax : 0;
       cudaError_t e = prepare_llg_staged(c, (h->sys.n_owned + 31) / 32, h->device);
       if (e != cudaSuccess) return cuda_err(h, e, "staged pass setup (tile records exceed shared memory?)");
       h->sys.stage = c;
@@ -877,7 +981,8 @@ extern "C" int vgpu_set_option(vgpu_handle h, int option, int value) {
          h->sys.stage.grid = 0;
          return VGPU_OK;
       case VGPU_OPT_STAGE_SLICES:
-         if (value != 2 && value != 4 && value != 8) return set_err(h, VGPU_ERR_ARG, "stage slices: 2, 4 or 8");
+         if (value != -1 && value != 2 && value != 4 && value != 8)
+            return set_err(h, VGPU_ERR_ARG, "stage slices: -1, 2, 4 or 8");
          h->stage_sl = value;
          h->sys.stage.grid = 0;
          return VGPU_OK;
@@ -889,12 +994,37 @@ extern "C" int vgpu_set_option(vgpu_handle h, int option, int value) {
          h->dipole_fft = value;
          return VGPU_OK;
       case VGPU_OPT_STAGE_BUFFERS:
-         if (value != 1 && value != 2) return set_err(h, VGPU_ERR_ARG, "stage buffers: 1 or 2");
+         if (value != -1 && value != 1 && value != 2) return set_err(h, VGPU_ERR_ARG, "stage buffers: -1, 1 or 2");
          h->stage_nbuf = value;
+         h->sys.stage.grid = 0;
+         return VGPU_OK;
+      case VGPU_OPT_COMPACT_RECORDS:
+         if (value < -1 || value > 1) return set_err(h, VGPU_ERR_ARG, "compact records: -1, 0 or 1");
+         h->compact = value;
+         h->sys.stage.grid = 0;
+         return VGPU_OK;
+      case VGPU_OPT_WINDOW_STAGING:
+         if (value < -1 || value > 1) return set_err(h, VGPU_ERR_ARG, "window staging: -1, 0 or 1");
+         h->window = value;
          h->sys.stage.grid = 0;
          return VGPU_OK;
       default: return set_err(h, VGPU_ERR_ARG, "unknown option %d", option);
    }
+}
+
+extern "C" int vgpu_record_layout(vgpu_handle h, int32_t* layout, int32_t* dict_entries) {
+   if (!h || !layout) return set_err(h, VGPU_ERR_ARG, "null argument");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   SysDev& S = h->sys;
+   if (dict_entries) *dict_entries = S.cdict_n;
+   const bool compact = h->compact != 0 && S.crec;
+   *layout = compact ? VGPU_RECORDS_COMPACT : S.rec ? VGPU_RECORDS_WIDE : VGPU_RECORDS_NONE;
+   if (compact && h->prec == VGPU_PREC_FP32 && use_staged<float>(h)) {
+      const int rc = ensure_window_plan(h);
+      if (rc) return rc;
+      if (S.win_ok) *layout = VGPU_RECORDS_WINDOW;
+   }
+   return VGPU_OK;
 }
 
 extern "C" int vgpu_set_step(vgpu_handle h, uint64_t step) {

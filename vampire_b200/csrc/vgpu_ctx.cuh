@@ -25,6 +25,20 @@ struct SysDev {
    void* col = nullptr;
    void* jb[9] = {nullptr};
    void* rec = nullptr;      // packed 16-byte bond records (FP32 FMT_DMI_TAB)
+   void* crec = nullptr;     // compact 4-byte records (FP32 FMT_DMI_TAB, few distinct couplings), or nullptr
+   void* cdict = nullptr;    // their coupling dictionary (float4 entries)
+   int crec_shift = 0, cdict_n = 0;
+   std::vector<uint32_t> crec_host;  // host copy of crec (window planning)
+   std::vector<int> off_host;        // host copy of slice_off
+   // window plan of the window-staged passes (built on first use for the tile
+   // shape and owned-atom count it was made for)
+   int win_sl = 0, win_nupd = -1;
+   bool win_ok = false;
+   int wmax = 0;
+   void* lrec = nullptr;
+   void* wseg = nullptr;
+   void* wtile_seg = nullptr;
+   void* wtile_w = nullptr;
    void* jtab_s = nullptr;   // scalar material-pair table (isotropic diagonal)
    int tab_scalar = 0;
    void* jtab = nullptr;
@@ -97,11 +111,14 @@ struct vgpu_ctx {
    int store_increment = -1;  // -1: default (on for FP64, off for FP32)
    bool batch_materials = false;  // batch handle: material rows are per system (no 100 limit)
    int staged = -1;          // VGPU_OPT_STAGED_RECORDS (-1 default)
-   int stage_sl = 4, stage_nbuf = 1;
+   int stage_sl = -1, stage_nbuf = -1;  // -1: per record layout (tile_shape in vgpu_api.cu)
    bool stage_wait_test = false;  // VGPU_OPT_STAGE_WAIT_TEST
    int dipole_fft = -1;      // VGPU_OPT_DIPOLE_FFT (-1 default: FFT far field on regular cell grids)
+   int compact = -1;         // VGPU_OPT_COMPACT_RECORDS (-1 default: compact records when built)
+   int window = -1;          // VGPU_OPT_WINDOW_STAGING (-1 default: off)
 
    void* alloc(size_t bytes);
+   void release(void* p);    // free one allocation made by alloc (nullptr: nothing)
    void free_system();
    int refresh_materials();
    int check_status();

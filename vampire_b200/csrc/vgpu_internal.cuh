@@ -7,6 +7,7 @@
 #include <string>
 #include <vector>
 
+#include "record_plan.h"
 #include "vgpu.h"
 
 namespace vgpu {
@@ -59,6 +60,21 @@ struct LLGArgs {
    const R* jtab_s;          // scalar material-pair table, or nullptr
    const R* jb[9];           // per-bond exchange arrays in SELL layout
    const int4* rec;          // FP32 FMT_DMI_TAB: packed {index, d_x, d_y, d_z} per bond, or nullptr
+   // FP32 FMT_DMI_TAB compact records (taken before rec when set): one word per
+   // bond, neighbour | coupling index << crec_shift, and the coupling
+   // dictionary: cdict_n entries {J (Jxx), d_x, d_y, d_z}, then (non-scalar
+   // diagonal) cdict_n entries {Jyy, Jzz, 0, 0}
+   const uint32_t* crec;
+   const float4* cdict;
+   int crec_shift, cdict_n;
+   // window-staged FP32 passes: per bond the word slot | coupling index << 16,
+   // slot indexing the tile's window of neighbour spins; per tile the window's
+   // segments {first atom, atoms, first slot, 0} (wseg[wtile_seg[t] ..
+   // wtile_seg[t+1]]) and its slot count wtile_w[t]
+   const uint32_t* lrec;
+   const int4* wseg;
+   const int* wtile_seg;
+   const int* wtile_w;
    const R* jtab;            // material-pair table (M*M or M*M*3)
    int M;                    // number of materials
    const int* mat;           // [n] material id, or nullptr when M == 1
@@ -95,6 +111,8 @@ struct LLGArgs {
    int stage_extra_tx;       // staged passes: extra bytes each tile expects (0; > 0 tests the bounded wait)
 };
 
+// FP32 DMI record layout a kernel is compiled for (exchange_field)
+enum RecLayout : int { REC_ANY = 0, REC_WIDE = 1, REC_COMPACT = 2, REC_WINDOW = 3 };
 enum PassMode : int { PASS_PREDICTOR = 0, PASS_CORRECTOR = 1, PASS_FIELD = 2 };
 enum Integrator : int { INTEG_HEUN = 0, INTEG_MIDPOINT = 1 };
 // compiled pass variants: Heun without / with the higher-order anisotropy
@@ -106,12 +124,18 @@ template <typename R>
 cudaError_t launch_llg_pass(const LLGArgs<R>& a, int fmt, int mode, int nslices, cudaStream_t st);
 
 // Bulk-staged FP32 FMT_DMI_TAB passes (llg_kernels_fp32.cu): tiles of sl
-// slices, nbuf shared-memory buffers of buf_bytes (the largest tile's records).
+// slices, nbuf shared-memory buffers of buf_bytes (the largest tile's records),
+// and with compact records (crec) the coupling dictionary (dict_bytes) after them.
 constexpr int kStageSmemLimit = 200 * 1024;  // dynamic shared memory the staged passes may take
 struct StageCfg {
    int sl = 4, nbuf = 1, buf_bytes = 0;
+   bool crec = false;
+   int dict_bytes = 0;
+   bool win = false;          // window-staged passes (neighbour spins staged too)
+   int wmax = 0;              // window slots of the largest tile (multiple of 4)
    int ntiles = 0, grid = 0;  // set by prepare_llg_staged
 };
+
 int stage_tile_bytes(const std::vector<int>& slice_off, int sl);
 cudaError_t prepare_llg_staged(StageCfg& c, int nslices, int device);
 cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, const StageCfg& c, cudaStream_t st);

@@ -521,17 +521,19 @@ def config_sc_llg(L: int = 20, temperature: float = 0.0, seed: int = 123456) -> 
 
 
 def config_fcc_tensor(L: int = 100, seed: int = 2024, temperature: float = 300.0,
-                      dipole: bool = False) -> SpinSystem:
+                      dipole: bool = False, periodic=(True, True, True)) -> SpinSystem:
     """FCC L^3 periodic (4 L^3 spins), a=0.354 nm, two materials at random
     50/50, nn tensor exchange J_AA=J_BB=11.2e-21 J, J_AB=5e-21 J plus the
     three-site DMI with D=0.1 J, cubic Kc=1e-24 J/atom, alpha=0.05,
-    dt=1e-16 s, T=300 K, H=0; with `dipole`, 2x2x2-unit-cell macrocells."""
+    dt=1e-16 s, T=300 K, H=0; with `dipole`, 2x2x2-unit-cell macrocells;
+    `periodic` per axis (open surfaces give atoms fewer than 12 bonds)."""
     mats = [Material(alpha=0.05, mu_s_muB=1.72, Kc=1e-24) for _ in range(2)]
     J = np.array([[11.2e-21, 5e-21], [5e-21, 11.2e-21]])
     p = SimParams(dt_SI=1e-16, temperature=temperature, H_applied=0.0, H_vec=(0.0, 0.0, 1.0))
     rng = np.random.default_rng(seed)
     types = (rng.random(4 * L ** 3) < 0.5).astype(np.int32)
-    s = build("fcc", L, L, L, 3.54, mats, J, p, types=types, dmi_SI=0.1 * J, spin_seed=seed + 1)
+    s = build("fcc", L, L, L, 3.54, mats, J, p, periodic=tuple(periodic), types=types, dmi_SI=0.1 * J,
+              spin_seed=seed + 1)
     if dipole:
         # macrocells of 2x2x2 unit cells, tensor solver, updated every 100 steps
         dipole_cells(s, size=2 * 3.54, atomic_volume=3.54 ** 3 / 4.0, solver="tensor", update_rate=100)

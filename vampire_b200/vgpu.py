@@ -10,7 +10,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 from pathlib import Path
-from typing import Optional
+from typing import Optional, Tuple
 
 import numpy as np
 
@@ -24,6 +24,9 @@ PREC_FP32, PREC_FP64 = 0, 1
 NOISE_PHILOX, NOISE_REPLAY = 0, 1
 OPT_STORE_INCREMENT, OPT_STAGED_RECORDS, OPT_STAGE_SLICES, OPT_STAGE_BUFFERS, OPT_DIPOLE_FFT = 1, 2, 3, 4, 5
 OPT_STAGE_WAIT_TEST = 6
+OPT_COMPACT_RECORDS = 7
+OPT_WINDOW_STAGING = 8
+RECORDS_NONE, RECORDS_WIDE, RECORDS_COMPACT, RECORDS_WINDOW = 0, 1, 2, 3
 PASS_PREDICTOR, PASS_CORRECTOR = 0, 1
 STATE_SPIN, STATE_PREDICTOR = 0, 1
 DIPOLE_FAR_DIRECT, DIPOLE_FAR_FFT = 0, 1
@@ -254,8 +257,17 @@ class Simulation:
             self._check(lib().vgpu_set_biquadratic(self._h, C.byref(q)))
 
     def set_option(self, option: int, value: int) -> None:
-        """vgpu_set_option: OPT_STORE_INCREMENT, OPT_STAGED_RECORDS, OPT_STAGE_SLICES, OPT_STAGE_BUFFERS."""
+        """vgpu_set_option: OPT_STORE_INCREMENT, OPT_STAGED_RECORDS, OPT_STAGE_SLICES,
+        OPT_STAGE_BUFFERS, OPT_DIPOLE_FFT, OPT_STAGE_WAIT_TEST, OPT_COMPACT_RECORDS,
+        OPT_WINDOW_STAGING."""
         self._check(lib().vgpu_set_option(self._h, int(option), int(value)))
+
+    def record_layout(self) -> Tuple[int, int]:
+        """(RECORDS_NONE | RECORDS_WIDE | RECORDS_COMPACT | RECORDS_WINDOW, coupling
+        dictionary entries)."""
+        lay, nd = C.c_int32(), C.c_int32()
+        self._check(lib().vgpu_record_layout(self._h, C.byref(lay), C.byref(nd)))
+        return lay.value, nd.value
 
     def set_params(self, p) -> None:
         c = params_struct(p)
