@@ -125,12 +125,13 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def traffic_from_profiles(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+def traffic_from_profiles(kernel: str, records: str):
+    """DRAM bytes per launch of `kernel` ("predictor" / "corrector") with bond
+    records `records` ("compact" / "wide") from the committed ncu summary."""
     p = REPO / "profiles" / "ncu_traffic.json"
     if p.exists():
         try:
-            return json.loads(p.read_text()).get(kernel)
+            return json.loads(p.read_text()).get(records, {}).get(kernel)
         except Exception:
             return None
     return None
@@ -396,7 +397,7 @@ def main():
     avg_ms = prof[kern]["ms"] / max(1, prof[kern]["count"])
     peak, peak_kind = measured_peak_hbm()
     achieved = bm[kern] * n / (avg_ms * 1e-3) / 1e9
-    traffic = traffic_from_profiles(kern)
+    traffic = traffic_from_profiles(kern, "compact" if compact else "wide")
     step_gbs = (bm["predictor"] + bm["corrector"]) * n * args.steps / (ms * 1e-3) / 1e9
 
     # --- e2e through the C ABI with host buffers ------------------------
