@@ -436,7 +436,8 @@ extern "C" int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* dd) {
    };
    up((void**)&d->cell_start, start.data(), sizeof(int) * (nc + 1));
    up((void**)&d->cell_atoms, atoms.data(), sizeof(int) * atoms.size());
-   up((void**)&d->atom_cell, acell.data(), sizeof(int) * n);
+   acell.resize(((size_t)S.n_alloc + 3) & ~(size_t)3, nc);  // padded like the state arrays
+   up((void**)&d->atom_cell, acell.data(), sizeof(int) * acell.size());
    up((void**)&d->pos, pos.data(), sizeof(float4) * nc);
    up((void**)&d->self, self.data(), sizeof(double) * nc);
    if (e == cudaSuccess) e = cudaMalloc(&d->mag, sizeof(double) * 3 * nc);

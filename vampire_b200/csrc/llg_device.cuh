@@ -502,21 +502,31 @@ __device__ __forceinline__ E anisotropy_energy(const LLGArgs<R>& a, int i, const
 
 // external field (calculate_external_fields, fields.cpp:120-169)
 template <typename R>
+__device__ __forceinline__ void external_field_g(const LLGArgs<R>& a, int i, const MatParams<R>& m, const R g[3],
+                                                 int cell_id, R E[3]);
+
+template <typename R>
 __device__ __forceinline__ void external_field(const LLGArgs<R>& a, int i, const MatParams<R>& m, bool with_noise,
                                                R E[3]) {
+   R g[3] = {0, 0, 0};
+   if (a.thermal && with_noise) thermal_xi(a, i, g[0], g[1], g[2]);
+   external_field_g<R>(a, i, m, g, -1, E);
+}
+
+// the same with the atom's Gaussians g (used when a.thermal) given, and its
+// macrocell id (cell_id >= 0) when the caller has it already
+template <typename R>
+__device__ __forceinline__ void external_field_g(const LLGArgs<R>& a, int i, const MatParams<R>& m, const R g[3],
+                                                 int cell_id, R E[3]) {
    R ex = 0, ey = 0, ez = 0;
-   if (a.thermal && with_noise) {
-      R gx, gy, gz;
-      thermal_xi(a, i, gx, gy, gz);
-      ex = gx * m.sigma; ey = gy * m.sigma; ez = gz * m.sigma;
-   }
+   if (a.thermal) { ex = g[0] * m.sigma; ey = g[1] * m.sigma; ez = g[2] * m.sigma; }
    if (a.ramp_n) {
       const R f = (R)(a.step < a.ramp_n ? a.step : a.ramp_n) / (R)a.ramp_n;
       ex += a.hx + (m.hlx + m.dhx * f); ey += a.hy + (m.hly + m.dhy * f); ez += a.hz + (m.hlz + m.dhz * f);
    } else if (a.local_field) { ex += a.hx + m.hlx; ey += a.hy + m.hly; ez += a.hz + m.hlz; }
    else { ex += a.hx; ey += a.hy; ez += a.hz; }
    if (a.cell) {
-      const int c = __ldg(a.cell + i);
+      const int c = cell_id >= 0 ? cell_id : __ldg(a.cell + i);
       ex += __ldg(a.cell_field + c);
       ey += __ldg(a.cell_field + a.ncells + c);
       ez += __ldg(a.cell_field + 2 * a.ncells + c);

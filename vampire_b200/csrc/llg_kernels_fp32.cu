@@ -38,7 +38,8 @@ cudaError_t prepare_llg_staged(StageCfg& c, int nslices, int device) {
    c.grid = 0;
    if (!(c.sl == 2 || c.sl == 4 || c.sl == 8) || !(c.nbuf == 1 || c.nbuf == 2)) return cudaErrorInvalidValue;
    if (c.win && (c.nbuf != 1 || !c.crec)) return cudaErrorInvalidValue;
-   const int smem = c.win ? c.buf_bytes + 12 * c.wmax + c.dict_bytes : c.nbuf * c.buf_bytes + c.dict_bytes;
+   const int smem = c.win ? c.buf_bytes + 12 * c.wmax + c.dict_bytes
+                          : staged_smem_bytes(c.sl, c.nbuf, c.buf_bytes, c.dict_bytes, c.M);
    int sms = 0, optin = 0;
    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
@@ -77,7 +78,7 @@ cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, co
 #undef VGPU_WIN
       return cudaErrorInvalidValue;
    }
-   const int smem = c.nbuf * c.buf_bytes + c.dict_bytes;
+   const int smem = staged_smem_bytes(c.sl, c.nbuf, c.buf_bytes, c.dict_bytes, c.M);
 #define VGPU_STAGED_C(S, B, C)                                                                                 \
    if (mode == PASS_PREDICTOR)                                                                                 \
       llg_staged_kernel<PASS_PREDICTOR, S, B, C><<<g, b, smem, st>>>(a, nslices, c.ntiles, c.buf_bytes);       \

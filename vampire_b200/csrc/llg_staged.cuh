@@ -83,28 +83,31 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* m, uint32_t parity) 
 
 // SL slices (32 SL atoms) per tile, NBUF = 1 (one tile per block, the other
 // resident blocks hide the copy) or 2 (persistent, next tile's copy in flight
-// while this one is computed).  Dynamic shared memory: NBUF * buf_bytes.
+// while this one is computed).  Each buffer holds the tile's bond records
+// (buf_bytes) and its own-atom arrays (kStageOwnArrays x 32 SL words: s0 x|y|z,
+// s' x|y|z for the corrector, material ids, cell ids), all brought by bulk
+// copies completing on the buffer's barrier; after the buffers come the
+// coupling dictionary (compact records, copied with the block's first tile)
+// and the material table (read into shared memory once per block when it has
+// at most kStageMaxMat rows).  The Philox Gaussians of the tile's atoms need no
+// data and are generated while the copy is in flight.
 // Registers are capped for 768 resident threads per SM (85 a thread): the
 // compact-record corrector otherwise takes 92 and fits 5 blocks of 128
 // (measured 12 % slower); a cap at 64 spills and was slower again.
 template <int MODE, int SL, int NBUF, bool CREC>
 __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGArgs<float> a, int nslices, int ntiles,
-                                                             int buf_bytes) {
+                                                                       int buf_bytes) {
+   constexpr int TS = 32 * SL;
    extern __shared__ __align__(128) unsigned char stage_smem[];
    __shared__ __align__(8) uint64_t mbar[2];
    const int tid = threadIdx.x;
-   // compact records: the coupling dictionary follows the record buffers; it
-   // arrives with the block's first tile copy
-   float4* sdict = reinterpret_cast<float4*>(stage_smem + NBUF * buf_bytes);
+   const int stride = buf_bytes + kStageOwnArrays * TS * 4;
+   float4* sdict = reinterpret_cast<float4*>(stage_smem + NBUF * stride);
    const uint32_t dict_bytes = CREC ? 16u * (uint32_t)(a.tab_scalar ? a.cdict_n : 2 * a.cdict_n) : 0u;
-   if (tid == 0) {
-      mbar_init(&mbar[0], 1);
-      mbar_init(&mbar[1], 1);
-      fence_mbar_init();
-   }
-   __syncthreads();
-   // thread 0: expect the tile's record bytes and start its bulk copy (and,
-   // with the first tile, the dictionary's)
+   MatParams<float>* smp = reinterpret_cast<MatParams<float>*>(stage_smem + NBUF * stride + dict_bytes);
+   const bool mp_shared = a.M <= kStageMaxMat;
+   // thread 0: expect the tile's bytes and start its bulk copies: records,
+   // own-atom arrays (and, with the first tile, the dictionary)
    auto issue = [&](int t, int b, bool first) {
       const int s0 = t * SL;
       const int s1 = min(s0 + SL, nslices);
@@ -112,33 +115,52 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
       const uint32_t bytes = (uint32_t)(o1 - o0) * (CREC ? 4u : 16u);
       const void* src = CREC ? (const void*)(a.crec + o0) : (const void*)(a.rec + o0);
       const uint32_t db = first ? dict_bytes : 0u;
+      const uint32_t nb = 128u * (uint32_t)(s1 - s0);  // own-array bytes: 32 atoms x 4 B per slice
+      const int na = 3 + (MODE == PASS_CORRECTOR ? 3 : 0) + (a.mat ? 1 : 0) + (a.cell ? 1 : 0);
+      unsigned char* buf = stage_smem + b * stride;
+      float* own = reinterpret_cast<float*>(buf + buf_bytes);
+      const size_t a0 = (size_t)s0 * 32;
       fence_proxy_async();
-      mbar_arrive_expect_tx(&mbar[b], bytes + db + (uint32_t)a.stage_extra_tx);
-      if (bytes) bulk_copy_g2s(stage_smem + b * buf_bytes, src, bytes, &mbar[b]);
+      mbar_arrive_expect_tx(&mbar[b], bytes + db + nb * (uint32_t)na + (uint32_t)a.stage_extra_tx);
+      if (bytes) bulk_copy_g2s(buf, src, bytes, &mbar[b]);
       if (db) bulk_copy_g2s(sdict, a.cdict, db, &mbar[b]);
+      bulk_copy_g2s(own, a.ax + a0, nb, &mbar[b]);
+      bulk_copy_g2s(own + TS, a.ay + a0, nb, &mbar[b]);
+      bulk_copy_g2s(own + 2 * TS, a.az + a0, nb, &mbar[b]);
+      if (MODE == PASS_CORRECTOR) {
+         bulk_copy_g2s(own + 3 * TS, a.bx + a0, nb, &mbar[b]);
+         bulk_copy_g2s(own + 4 * TS, a.by + a0, nb, &mbar[b]);
+         bulk_copy_g2s(own + 5 * TS, a.bz + a0, nb, &mbar[b]);
+      }
+      if (a.mat) bulk_copy_g2s(own + 6 * TS, a.mat + a0, nb, &mbar[b]);
+      if (a.cell) bulk_copy_g2s(own + 7 * TS, a.cell + a0, nb, &mbar[b]);
    };
    uint32_t phase = 0;  // bit b: parity of the phase of mbar[b] to wait for next
    int t = blockIdx.x, k = 0, b = 0;
    bool failed = false;
-   if (NBUF == 2 && t < ntiles && tid == 0) issue(t, 0, true);
+   if (tid == 0) {
+      mbar_init(&mbar[0], 1);
+      mbar_init(&mbar[1], 1);
+      fence_mbar_init();
+      if (t < ntiles) issue(t, 0, true);
+   }
+   if (mp_shared) {
+      const int nw = a.M * (int)(sizeof(MatParams<float>) / 4);
+      const float* g = reinterpret_cast<const float*>(a.mp);
+      float* d = reinterpret_cast<float*>(smp);
+      for (int q = tid; q < nw; q += TS) d[q] = __ldg(g + q);
+   }
+   __syncthreads();  // barriers initialised, material table in place
+   const MatParams<float>* mpt = mp_shared ? smp : a.mp;
    for (; t < ntiles; t += gridDim.x, ++k) {
       b = NBUF == 1 ? 0 : (k & 1);
-      if (tid == 0) {
-         if (NBUF == 1) issue(t, 0, k == 0);
-         else if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, b ^ 1, false);
-      }
-      // own-atom work that needs no records overlaps the copy: state, material,
-      // external field (Philox noise, applied, dipole cell field)
-      const int i = t * 32 * SL + tid;
+      if (tid == 0 && k > 0 && NBUF == 1) issue(t, 0, false);
+      if (tid == 0 && NBUF == 2 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x, b ^ 1, false);
+      const int i = t * TS + tid;
       const bool act = i < a.n_upd;
-      const int ii = act ? i : a.n_upd - 1;  // idle lanes of the last tile load in bounds
-      const int mi = a.mat ? __ldg(a.mat + ii) : 0;
-      const MatParams<float> m = a.mp[mi];
-      float S0[3] = {a.ax[ii], a.ay[ii], a.az[ii]};
-      float S1[3];
-      if (MODE == PASS_CORRECTOR) { S1[0] = a.bx[ii]; S1[1] = a.by[ii]; S1[2] = a.bz[ii]; }
-      float E[3];
-      external_field<float>(a, ii, m, true, E);
+      // the tile's Gaussians (the Philox noise needs no data) while the copy lands
+      float g[3] = {0.f, 0.f, 0.f};
+      if (a.thermal) thermal_xi(a, act ? i : 0, g[0], g[1], g[2]);
       const int tile_off = __ldg(a.slice_off + t * SL);
       const bool done = mbar_wait_bounded(&mbar[b], (phase >> b) & 1u);
       if (__syncthreads_or(!done)) {  // every thread takes the same branch
@@ -146,15 +168,27 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
          break;
       }
       phase ^= 1u << b;
-      const int4* sb = (const int4*)(stage_smem + b * buf_bytes);
+      const unsigned char* buf = stage_smem + b * stride;
+      const float* own = reinterpret_cast<const float*>(buf + buf_bytes);
       if (act) {
+         const int mi = a.mat ? reinterpret_cast<const int*>(own)[6 * TS + tid] : 0;
+         const MatParams<float> m = mpt[mi];
+         const float S0[3] = {own[tid], own[TS + tid], own[2 * TS + tid]};
+         float E[3];
+         external_field_g<float>(a, i, m, g, a.cell ? reinterpret_cast<const int*>(own)[7 * TS + tid] : -1, E);
+         const int4* sb = reinterpret_cast<const int4*>(buf);
          float H[3];
          if (MODE == PASS_PREDICTOR) {
-            spin_field<float, FMT_DMI_TAB, 0, true, false, CREC ? REC_COMPACT : REC_WIDE>(a, i, mi, m, a.ax, a.ay, a.az, S0, H, sb, tile_off, sdict);
+            spin_field<float, FMT_DMI_TAB, 0, true, false, CREC ? REC_COMPACT : REC_WIDE>(a, i, mi, m, a.ax, a.ay,
+                                                                                           a.az, S0, H, sb,
+                                                                                           tile_off, sdict);
             H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
             llg_predict_finish<float>(a, i, m, S0, H);
          } else {
-            spin_field<float, FMT_DMI_TAB, 0, true, false, CREC ? REC_COMPACT : REC_WIDE>(a, i, mi, m, a.bx, a.by, a.bz, S1, H, sb, tile_off, sdict);
+            const float S1[3] = {own[3 * TS + tid], own[4 * TS + tid], own[5 * TS + tid]};
+            spin_field<float, FMT_DMI_TAB, 0, true, false, CREC ? REC_COMPACT : REC_WIDE>(a, i, mi, m, a.bx, a.by,
+                                                                                           a.bz, S1, H, sb,
+                                                                                           tile_off, sdict);
             H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
             llg_correct_finish<float>(a, i, m, S0, S1, H);
          }

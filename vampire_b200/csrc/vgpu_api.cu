@@ -313,7 +313,11 @@ static int upload_typed(vgpu_ctx* h, const vgpu_system_desc* d) {
    if ((rc = upload_vec(h, &S.jtab, tabR, "coupling table"))) return rc;
    S.tab_scalar = scalar;
    if (scalar) { if ((rc = upload_vec(h, &S.jtab_s, tabS, "scalar coupling table"))) return rc; }
-   if (M > 1) { if ((rc = upload_vec(h, &S.mat, mat, "materials"))) return rc; }
+   if (M > 1) {
+      std::vector<int> matp(mat);
+      matp.resize(n_alloc4, 0);  // padded like the state arrays (whole-slice copies of the staged passes)
+      if ((rc = upload_vec(h, &S.mat, matp, "materials"))) return rc;
+   }
    if ((rc = upload_vec(h, &S.s[0], ax, "spins"))) return rc;
    if ((rc = upload_vec(h, &S.s[1], ay, "spins"))) return rc;
    if ((rc = upload_vec(h, &S.s[2], az, "spins"))) return rc;
@@ -500,7 +504,8 @@ static bool use_staged(vgpu_ctx* h) {
    if (sizeof(R) != 4 || !S.rec || S.n == 0 || h->staged == 0 || S.aniso_ext || S.bq_off) return false;
    const bool crec = h->compact != 0 && S.crec;
    const int bytes = S.stage_bytes[stage_slot(stage_sl_of(h))] / (crec ? 4 : 1);
-   return stage_nbuf_of(h) * bytes + (crec ? stage_dict_bytes(S) : 0) <= kStageSmemLimit;
+   return staged_smem_bytes(stage_sl_of(h), stage_nbuf_of(h), bytes, crec ? stage_dict_bytes(S) : 0, S.M) <=
+          kStageSmemLimit;
 }
 
 template <typename R>
@@ -562,6 +567,7 @@ static int prepare_passes(vgpu_ctx* h, bool* staged_out, int integrator = INTEG_
       c.sl = stage_sl_of(h);
       c.nbuf = stage_nbuf_of(h);
       c.crec = h->compact != 0 && h->sys.crec;
+      c.M = h->sys.M;
       c.buf_bytes = h->sys.stage_bytes[stage_slot(c.sl)] / (c.crec ? 4 : 1);
       c.dict_bytes = c.crec ? stage_dict_bytes(h->sys) : 0;
       c.win = c.crec && h->sys.win_ok && c.buf_bytes + 12 * h->sys.wmax + c.dict_bytes <= kStageSmemLimit;

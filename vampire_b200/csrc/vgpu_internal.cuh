@@ -127,8 +127,11 @@ cudaError_t launch_llg_pass(const LLGArgs<R>& a, int fmt, int mode, int nslices,
 // slices, nbuf shared-memory buffers of buf_bytes (the largest tile's records),
 // and with compact records (crec) the coupling dictionary (dict_bytes) after them.
 constexpr int kStageSmemLimit = 200 * 1024;  // dynamic shared memory the staged passes may take
+constexpr int kStageOwnArrays = 8;            // own-atom arrays per staged buffer (32 SL words each)
+constexpr int kStageMaxMat = 64;              // material rows the staged passes keep in shared memory
 struct StageCfg {
    int sl = 4, nbuf = 1, buf_bytes = 0;
+   int M = 1;                 // materials (the staged passes may keep the table in shared memory)
    bool crec = false;
    int dict_bytes = 0;
    bool win = false;          // window-staged passes (neighbour spins staged too)
@@ -136,6 +139,12 @@ struct StageCfg {
    int ntiles = 0, grid = 0;  // set by prepare_llg_staged
 };
 
+// dynamic shared memory of llg_staged_kernel: nbuf x (records + own-atom
+// arrays), the dictionary, the material table when it has <= kStageMaxMat rows
+inline int staged_smem_bytes(int sl, int nbuf, int buf_bytes, int dict_bytes, int M) {
+   const int mp = M <= kStageMaxMat ? ((M * (int)sizeof(MatParams<float>) + 15) & ~15) : 0;
+   return nbuf * (buf_bytes + kStageOwnArrays * 32 * sl * 4) + dict_bytes + mp;
+}
 int stage_tile_bytes(const std::vector<int>& slice_off, int sl);
 cudaError_t prepare_llg_staged(StageCfg& c, int nslices, int device);
 cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, const StageCfg& c, cudaStream_t st);
