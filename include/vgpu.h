@@ -444,6 +444,24 @@ int vgpu_stats_reset(vgpu_handle h);
  * counterpart (vcuda::stats::get blocks). */
 int vgpu_stats_copy_rows(vgpu_handle h, int32_t id, double* out);
 
+/* ---- spin snapshots (configuration output) ------------------------------ */
+
+/* Output atom list of the spin snapshots: `count` atom ids (the reference's
+ * config::internal::local_output_atom_list, built by config::internal::
+ * initialize, src/config/initialize.cpp: atoms inside the output bounds), in
+ * output order.  Replaces the host gather copy_data_to_buffer
+ * (src/config/buffer.cpp:28-50) that config::internal::atoms
+ * (src/config/atoms_spins.cpp) runs on every snapshot. */
+int vgpu_snapshot_setup(vgpu_handle h, const int64_t* atoms, int64_t count);
+
+/* Gather the listed atoms' spins on the device into the data block of the
+ * binary spin file (src/config/write.cpp:107-140: x, y, z per atom, FP64) and
+ * copy it to `out` (3 * count doubles, host memory; pinned memory makes the
+ * copy asynchronous on the handle's stream -- call vgpu_synchronize before
+ * reading it).  A file is a uint64 count followed by this block
+ * (vampire_b200/config.py writes it with the reference's names and meta file). */
+int vgpu_snapshot(vgpu_handle h, double* out);
+
 /* Raw per-bin sums of the last vgpu_stats_update of mask `id`: sums[8*bin +
  * {0..3}] = sum mu s_x, sum mu s_y, sum mu s_z, sum mu (mu_B), [4..7] = the
  * exchange, anisotropy, applied and magnetostatic energy sums (exchange and

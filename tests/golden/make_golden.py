@@ -272,8 +272,33 @@ def mc_sc16_curie():
     print("mc_sc16_curie:", np.round(mean, 3))
 
 
+def sc8_config():
+    """The reference program's own configuration output (binary spin
+    snapshots, src/config/atoms_spins.cpp) for the sc8_t0 input: the stock
+    serial program with config:atoms every 5 output steps of 10 time steps,
+    so snapshots at steps 10 and 60.  The spin data files and their meta files
+    are kept as the reference wrote them."""
+    import shutil
+    import subprocess
+    import tempfile
+    from oracle.refinputs import SC_MAT, sc_input
+    exe = HERE.parent.parent / "oracle" / "_ref" / "vampire-serial"
+    d = Path(tempfile.mkdtemp(prefix="cfg_"))
+    (d / "input").write_text(sc_input(8, T=0.0, extra="sim:total-time-steps=100\nsim:time-steps-increment=10\n"
+                                                       "output:time-steps\noutput:magnetisation\nconfig:atoms\n"
+                                                       "config:atoms-output-rate=5\nconfig:output-format=binary\n"))
+    (d / "m.mat").write_text(SC_MAT)
+    subprocess.run([str(exe)], cwd=d, check=True, capture_output=True, timeout=600)
+    out = HERE / "sc8_config"
+    out.mkdir(exist_ok=True)
+    for f in ("spins-00000000.data", "spins-00000000.meta", "spins-00000001.data", "spins-00000001.meta"):
+        shutil.copy(d / f, out / f)
+    print("sc8_config:", sorted(p.name for p in out.iterdir()))
+
+
 ALL = [sc20_t0, sc8_t0, sc10_t300, sc6_open_t300, fcc4_dmi_t300, fcc4_dmi_t0, single_spin_applied, mc_sc16_curie,
-       fcc10_dipole_tensor, fcc10_dipole_macrocell, sc6_aniso_ho, fcc4_neel_rot, sc6_derived_t600, sc8_midpoint, sc6_biquadratic]
+       fcc10_dipole_tensor, fcc10_dipole_macrocell, sc6_aniso_ho, fcc4_neel_rot, sc6_derived_t600, sc8_midpoint, sc6_biquadratic,
+       sc8_config]
 
 if __name__ == "__main__":
     names = sys.argv[1:]

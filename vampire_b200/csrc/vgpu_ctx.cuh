@@ -75,6 +75,10 @@ struct SysDev {
    int aniso_ext = 0;                          // AnisoExt bits
    std::vector<double> ku4_h, ku6_h, kc6_h, kcb_h;  // per material (kcb: 9 each)
    void* neel = nullptr;                       // [9][n_alloc] Neel tensors
+   // spin snapshots (vgpu_snapshot_setup): output atom list and FP64 x|y|z buffer
+   void* snap_idx = nullptr;
+   void* snap_buf = nullptr;
+   int64_t snap_n = -1;                        // -1: no list set up
    // biquadratic exchange (vgpu_set_biquadratic): SELL-32 copy of its list
    void* bq_off = nullptr;
    void* bq_col = nullptr;

@@ -346,6 +346,27 @@ class Simulation:
         (pinned host or device memory) on the library stream; no wait."""
         self._check(lib().vgpu_stats_copy_rows(self._h, C.c_int32(mask_id), C.c_void_p(out_ptr)))
 
+    def snapshot_setup(self, atoms) -> None:
+        """Output atom list of the spin snapshots (vgpu_snapshot_setup)."""
+        a = np.ascontiguousarray(atoms, dtype=np.int64)
+        self._snap_n = int(a.size)
+        self._check(lib().vgpu_snapshot_setup(self._h, a.ctypes.data_as(C.POINTER(C.c_int64)),
+                                              C.c_int64(a.size)))
+
+    def snapshot(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The listed atoms' spins, x y z interleaved in FP64 (the data block
+        of the binary spin file), gathered on the device (vgpu_snapshot).
+        `out` (e.g. a view of pinned host memory) is filled in place."""
+        n = getattr(self, "_snap_n", None)
+        if n is None:
+            raise VGPUError(ERR_STATE, "snapshot_setup not called")
+        if out is None:
+            out = np.empty(3 * n)
+        assert out.dtype == np.float64 and out.size == 3 * n and out.flags.c_contiguous
+        self._check(lib().vgpu_snapshot(self._h, _ptr(out, _D)))
+        self.synchronize()
+        return out
+
     def stats_derived(self, mask_id: int, temperature: float):
         """(susceptibility (size, 4), specific heat (size,), std dev (size, 4))
         of the updates since the last reset (vgpu_stats_get_derived)."""
