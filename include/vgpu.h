@@ -384,7 +384,10 @@ int vgpu_set_dipole_field(vgpu_handle h, const double* bx, const double* by, con
  * (checked: no two interacting atoms share a colour) or NULL for a host
  * greedy colouring.  The reference has no GPU Monte Carlo; this backs the
  * gpu::mc_step() entry the simulate loop gains (src/simulate/sim.cpp:608-614
- * calls montecarlo::mc_step, src/montecarlo/mc.cpp:29-127). */
+ * calls montecarlo::mc_step, src/montecarlo/mc.cpp:29-127).  On a shard
+ * (vgpu_set_owned, called first) the sweeps visit the owned atoms only; give
+ * the whole system's colours of the local atoms (owned and halo) so that the
+ * shards together make the whole system's sweep. */
 int vgpu_mc_setup(vgpu_handle h, const int32_t* colour_in, int32_t* n_colours_out);
 
 /* The colour of every atom chosen by vgpu_mc_setup. */
@@ -399,8 +402,18 @@ int vgpu_mc_set_replay(vgpu_handle h, const double* rnd);
  * temperature of vgpu_set_params; one launch per colour. */
 int vgpu_mc_sweep(vgpu_handle h, uint64_t n_sweeps);
 
-/* Sweep counter keying the Philox stream. */
+/* Sweep counter keying the Philox stream (counter = (noise_base + atom,
+ * sweep), so shards draw the whole system's numbers). */
 int vgpu_mc_set_sweep(vgpu_handle h, uint64_t sweep);
+
+/* One colour of the current sweep, colours in order 0, 1, ...; the last one
+ * completes the sweep.  For shards: between two colours the host refreshes
+ * the halo spins (vgpu_halo_pack / vgpu_halo_unpack of VGPU_STATE_SPIN), the
+ * exchange a colour-ordered sweep needs (the reference's parallel Monte
+ * Carlo swaps halos around each of its eight octant phases,
+ * src/montecarlo/mc-mpi.cpp:140-210).  No reference counterpart as an entry
+ * point. */
+int vgpu_mc_colour(vgpu_handle h, int32_t colour);
 
 /* Attempted and rejected moves since vgpu_mc_setup
  * (sim::mc_statistics_moves / mc_statistics_reject). */

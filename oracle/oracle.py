@@ -255,6 +255,21 @@ class OracleSystem:
                                          _p(beta, _D), _p(ratio, _D))
         return s, int(rej)
 
+    def mc_pass(self, spins, atoms, rnd):
+        """Metropolis moves of the listed atoms, in order, with given random
+        numbers (4n: x|y|z Gaussians, acceptance uniforms); the pass of one
+        colour of a sweep over one shard's owned atoms."""
+        s = np.ascontiguousarray(spins, dtype=np.float64).copy()
+        order = np.ascontiguousarray(atoms, dtype=np.int32)
+        off = np.array([0, order.size], dtype=np.int32)
+        sig, beta, ratio = self.mc_params()
+        r = np.ascontiguousarray(rnd, dtype=np.float64)
+        lib().vref_mc_colour_sweep.restype = C.c_long
+        rej = lib().vref_mc_colour_sweep(C.byref(self.st), _p(s[0], _D), _p(s[1], _D), _p(s[2], _D),
+                                         _p(order, _I), _p(off, _I), C.c_int(1), _p(r, _D), _p(sig, _D),
+                                         _p(beta, _D), _p(ratio, _D))
+        return s, int(rej)
+
     def magnetization(self, spins, mask, size) -> np.ndarray:
         s = np.ascontiguousarray(spins, dtype=np.float64)
         mm = np.ascontiguousarray(self.s.mu_s_muB(), dtype=np.float64)

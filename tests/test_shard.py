@@ -5,6 +5,8 @@ as world_size-2 and -3 gloo process groups whose ranks step their shard with
 the FP64 oracle (predictor half, halo refresh of s', corrector half, halo
 refresh of s) and must reproduce the whole-system oracle bit for bit -- the
 same field sums in the same bond order, with the reference's replayed noise.
+Monte Carlo shards run each colour's Metropolis pass over their owned atoms
+with a halo refresh after every colour, against the whole-system sweep.
 """
 import os
 import socket
@@ -132,6 +134,98 @@ def test_gloo_sharded_oracle_equals_whole_system(tmp_path, maker_name, world):
     for p in plans:
         got[:, p.owned] = np.load(tmp_path / f"rank{p.rank}.npy")
     np.testing.assert_array_equal(got, whole)
+
+
+def _greedy_colours(s):
+    colour = np.full(s.n, -1)
+    for i in range(s.n):
+        used = {colour[j] for j in s.nl[s.nl_start[i]:s.nl_end[i] + 1]}
+        c = 0
+        while c in used:
+            c += 1
+        colour[i] = c
+    return colour
+
+
+def _mc_rank_main(rank, world, port, maker_name, sweeps, seed, out_dir):
+    import torch
+    import torch.distributed as dist
+    from oracle import oracle as O
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        s = _fcc(T=600.0) if maker_name == "fcc" else _sc_open()
+        colour = _greedy_colours(s)
+        plan = SH.make_plan(s, world)[rank]
+        loc = SH.local_system(s, plan)
+        o = O.OracleSystem(loc)
+        glob = np.concatenate([plan.owned, plan.halo])
+        lcol = SH.local_colours(colour, plan)
+        rnd_all = _mc_numbers(s.n, sweeps, seed)
+        ex = SH.HaloExchange(plan)
+        state = {"cur": loc.spins.copy()}
+
+        def pack(peer, idx):
+            return torch.from_numpy(np.ascontiguousarray(state["cur"][:, idx]).ravel())
+
+        def unpack(peer, first, count, buf):
+            state["cur"][:, first:first + count] = buf.numpy().reshape(3, count)
+
+        def alloc(k):
+            return torch.empty(k, dtype=torch.float64)
+
+        rejects = 0
+        for t in range(sweeps):
+            rnd = rnd_all[t][:, glob].ravel()
+
+            def run_colour(c):
+                nonlocal rejects
+                atoms = np.flatnonzero(lcol[:plan.n_owned] == c)
+                state["cur"], r = o.mc_pass(state["cur"], atoms, rnd)
+                rejects += r
+
+            SH.mc_sweep_sharded(int(colour.max()) + 1, run_colour, lambda: ex.exchange(pack, unpack, alloc))
+        np.save(os.path.join(out_dir, f"rank{rank}.npy"), state["cur"][:, :plan.n_owned])
+        np.save(os.path.join(out_dir, f"rej{rank}.npy"), np.array([rejects]))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def _mc_numbers(n, sweeps, seed):
+    rng = np.random.default_rng(seed)
+    g = rng.standard_normal((sweeps, 3, n))
+    u = rng.random((sweeps, 1, n))
+    return np.concatenate([g, u], axis=1)
+
+
+@pytest.mark.parametrize("maker_name,world", [("fcc", 2), ("sc", 3)])
+def test_gloo_sharded_monte_carlo_equals_whole_system(tmp_path, maker_name, world):
+    """Colour-ordered Metropolis sweeps on shards (owned atoms of one colour,
+    then a halo refresh, for every colour) reproduce the whole system's
+    sweeps bit for bit with the FP64 oracle and the same random numbers, and
+    the shards' rejections add up to the whole system's."""
+    import torch.multiprocessing as mp
+    from oracle import oracle as O
+    sweeps, seed = 4, 5
+    mp.start_processes(_mc_rank_main, args=(world, _free_port(), maker_name, sweeps, seed, str(tmp_path)),
+                       nprocs=world, join=True, start_method="spawn")
+    s = _fcc(T=600.0) if maker_name == "fcc" else _sc_open()
+    colour = _greedy_colours(s)
+    o = O.OracleSystem(s)
+    spins, rejects = s.spins.copy(), 0
+    for t, rnd in enumerate(_mc_numbers(s.n, sweeps, seed)):
+        spins, r = o.mc_colour_sweep(spins, colour, rnd.ravel())
+        rejects += r
+    got = np.zeros_like(spins)
+    rej = 0
+    for p in SH.make_plan(s, world):
+        got[:, p.owned] = np.load(tmp_path / f"rank{p.rank}.npy")
+        rej += int(np.load(tmp_path / f"rej{p.rank}.npy")[0])
+    np.testing.assert_array_equal(got, spins)
+    assert rej == rejects and 0 < rejects < sweeps * s.n
 
 
 def test_combined_magnetization_equals_whole_system():

@@ -17,7 +17,8 @@ from vampire_b200 import system as S
 pytestmark = pytest.mark.gpu
 
 
-def _step_shards(V, torch, plans, sims, steps, dtype):
+def _refresher(torch, plans, sims, dtype):
+    """Host-driven halo refresh of every shard (pack, synchronise, unpack)."""
     idx = [{q: torch.as_tensor(ix, dtype=torch.int32, device="cuda") for q, ix in p.send.items()} for p in plans]
 
     def refresh(which):
@@ -37,6 +38,11 @@ def _step_shards(V, torch, plans, sims, steps, dtype):
         for sim in sims:
             sim.synchronize()
 
+    return refresh
+
+
+def _step_shards(V, torch, plans, sims, steps, dtype):
+    refresh = _refresher(torch, plans, sims, dtype)
     for _ in range(steps):
         for sim in sims:
             sim.llg_pass(V.PASS_PREDICTOR)
@@ -86,14 +92,64 @@ def test_shards_equal_whole_system(vgpu_lib, prec, nranks):
             sim.close()
 
 
-def test_shard_refuses_whole_system_solvers(vgpu_lib):
+def test_shard_setup_order_is_checked(vgpu_lib):
+    """Monte Carlo colour lists follow the owned count given before
+    vgpu_mc_setup: changing it afterwards is refused, as is an owned count
+    beyond the local atoms."""
     from vampire_b200 import vgpu as V
     s = S.config_fcc_tensor(L=3, seed=3)
     p = SH.make_plan(s, 2)[0]
     with V.Simulation(SH.local_system(s, p)) as sim:
         sim.set_owned(p.n_owned, p.noise_base)
+        sim.mc_setup()
         with pytest.raises(V.VGPUError) as e:
-            sim.mc_setup()
+            sim.set_owned(p.n_owned - 1, p.noise_base)
         assert e.value.code == V.ERR_STATE
         with pytest.raises(V.VGPUError):
             sim.set_owned(p.n_local + 1, 0)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("nranks", [2, 3])
+def test_mc_shards_equal_whole_system(vgpu_lib, prec, nranks):
+    """Monte Carlo on shards (the whole system's colouring restricted to each
+    shard, one vgpu_mc_colour per colour with a halo refresh between) equals
+    the whole system's sweeps bit for bit: owned spins and the summed move
+    and rejection counters."""
+    import torch
+    from vampire_b200 import vgpu as V
+    s = S.config_fcc_tensor(L=6, seed=3, temperature=600.0)
+    plans = SH.make_plan(s, nranks)
+    dtype = torch.float32 if prec == "fp32" else torch.float64
+    sweeps = 6
+    with V.Simulation(s, precision=prec, noise_seed=21) as whole:
+        nc = whole.mc_setup()
+        colour = whole.mc_colours()
+        whole.mc_sweep(sweeps)
+        ref = whole.spins()
+        moves_w, rej_w = whole.mc_counters()
+    sims = []
+    try:
+        for p in plans:
+            sim = V.Simulation(SH.local_system(s, p), precision=prec, noise_seed=21)
+            sim.set_owned(p.n_owned, p.noise_base)
+            assert sim.mc_setup(SH.local_colours(colour, p)) == nc
+            sims.append(sim)
+        refresh = _refresher(torch, plans, sims, dtype)
+        for _ in range(sweeps):
+            SH.mc_sweep_sharded(nc, lambda c: [sim.mc_colour(c) for sim in sims], lambda: refresh(V.STATE_SPIN))
+        got = np.zeros_like(ref)
+        moves = rej = 0.0
+        for sim, p in zip(sims, plans):
+            got[:, p.owned] = sim.spins()[:, :p.n_owned]
+            mv, rj = sim.mc_counters()
+            moves += mv
+            rej += rj
+        np.testing.assert_array_equal(got, ref)
+        assert moves == moves_w == sweeps * s.n and rej == rej_w and 0 < rej < moves
+        with pytest.raises(V.VGPUError) as e:
+            sims[0].mc_colour(1)          # a sweep starts with colour 0
+        assert e.value.code == V.ERR_ARG
+    finally:
+        for sim in sims:
+            sim.close()

@@ -38,6 +38,8 @@ struct MCState {
    bool use_replay = false;
    uint64_t sweep = 0;
    double moves = 0.0;
+   int n_owned = 0;                   // atoms the sweeps visit (a shard's owned atoms)
+   int next_colour = 0;               // vgpu_mc_colour: the colour of the current sweep to run next
 };
 
 static MCState* mc_of(vgpu_ctx* h) { return (MCState*)h->extras[1]; }
@@ -100,9 +102,11 @@ __global__ void __launch_bounds__(256) mc_colour_kernel(const MCArgs<R> p) {
       if (p.replay) {
          g0 = p.replay[i]; g1 = p.replay[a.n + i]; g2 = p.replay[2 * a.n + i]; u = p.replay[3 * a.n + i];
       } else {
-         const u32x4 c = {(uint32_t)i, (uint32_t)p.sweep, (uint32_t)(p.sweep >> 32), RNG_MC_MOVE};
+         // keyed by the global atom index (a shard's atom i is atom noise_base + i)
+         const uint32_t gi = (uint32_t)i + a.noise_base;
+         const u32x4 c = {gi, (uint32_t)p.sweep, (uint32_t)(p.sweep >> 32), RNG_MC_MOVE};
          const u32x4 r = philox4x32_10(c, a.seed_lo, a.seed_hi);
-         const u32x4 c2 = {(uint32_t)i, (uint32_t)p.sweep, (uint32_t)(p.sweep >> 32), RNG_MC_ACCEPT};
+         const u32x4 c2 = {gi, (uint32_t)p.sweep, (uint32_t)(p.sweep >> 32), RNG_MC_ACCEPT};
          const u32x4 r2 = philox4x32_10(c2, a.seed_lo, a.seed_hi);
          if (sizeof(R) == 4) {
             float s1, c1, s2, c2f;
@@ -196,7 +200,6 @@ extern "C" int vgpu_mc_setup(vgpu_handle h, const int32_t* colour_in, int32_t* n
    if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
    SysDev& S = h->sys;
    if (!S.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
-   if (S.n_owned < S.n) return set_err(h, VGPU_ERR_STATE, "Monte Carlo runs on whole systems (handle holds a shard)");
    cudaSetDevice(h->device);
    const int n = S.n;
    // neighbour lists back from the host copy kept at upload
@@ -230,15 +233,19 @@ extern "C" int vgpu_mc_setup(vgpu_handle h, const int32_t* colour_in, int32_t* n
    h->extras[1] = s;
    s->ncolours = nc;
    s->colour_host = colour;
+   // a shard's sweeps visit its owned atoms only (halo atoms are another
+   // rank's, refreshed between the colours by the host)
+   const int nu = S.n_owned;
+   s->n_owned = nu;
    s->colour_off.assign(nc + 1, 0);
-   for (int i = 0; i < n; ++i) s->colour_off[colour[i] + 1]++;
+   for (int i = 0; i < nu; ++i) s->colour_off[colour[i] + 1]++;
    for (int c = 0; c < nc; ++c) s->colour_off[c + 1] += s->colour_off[c];
-   std::vector<int> order(n), fill(s->colour_off.begin(), s->colour_off.end() - 1);
-   for (int i = 0; i < n; ++i) order[fill[colour[i]]++] = i;
+   std::vector<int> order(std::max(nu, 1)), fill(s->colour_off.begin(), s->colour_off.end() - 1);
+   for (int i = 0; i < nu; ++i) order[fill[colour[i]]++] = i;
    cudaError_t e;
-   if ((e = cudaMalloc(&s->atoms, sizeof(int) * n)) != cudaSuccess) return cuda_err(h, e, "mc atoms");
+   if ((e = cudaMalloc(&s->atoms, sizeof(int) * order.size())) != cudaSuccess) return cuda_err(h, e, "mc atoms");
    if ((e = cudaMalloc(&s->rejects, sizeof(unsigned long long))) != cudaSuccess) return cuda_err(h, e, "mc counter");
-   cudaMemcpyAsync(s->atoms, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->stream);
+   cudaMemcpyAsync(s->atoms, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice, h->stream);
    cudaMemsetAsync(s->rejects, 0, sizeof(unsigned long long), h->stream);
    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_err(h, e, "mc setup");
    if (n_colours_out) *n_colours_out = nc;
@@ -283,12 +290,12 @@ extern "C" int vgpu_mc_set_replay(vgpu_handle h, const double* r) {
    return VGPU_OK;
 }
 
+// per-material move width, inverse temperature and moment ratio (mc.cpp:45-53)
+// into the handle's device table; returns it or nullptr (error set)
 template <typename R>
-static int mc_sweeps_typed(vgpu_handle h, uint64_t n_sweeps) {
-   MCState* s = mc_of(h);
+static R* mc_tables(vgpu_handle h) {
    SysDev& S = h->sys;
    const int M = S.M;
-   // per-material move width and inverse temperature (mc.cpp:45-53)
    std::vector<R> sig(M), beta(M), ratio(M);
    for (int m = 0; m < M; ++m) {
       const vgpu_material& q = S.materials[m];
@@ -302,35 +309,64 @@ static int mc_sweeps_typed(vgpu_handle h, uint64_t n_sweeps) {
    }
    if (!S.mc_tab) {
       S.mc_tab = h->alloc(3 * 100 * sizeof(double));
-      if (!S.mc_tab) return set_err(h, VGPU_ERR_OOM, "mc tables");
+      if (!S.mc_tab) {
+         set_err(h, VGPU_ERR_OOM, "mc tables");
+         return nullptr;
+      }
    }
    R* tab = (R*)S.mc_tab;
    cudaMemcpyAsync(tab, sig.data(), M * sizeof(R), cudaMemcpyHostToDevice, h->stream);
    cudaMemcpyAsync(tab + 100, beta.data(), M * sizeof(R), cudaMemcpyHostToDevice, h->stream);
    cudaMemcpyAsync(tab + 200, ratio.data(), M * sizeof(R), cudaMemcpyHostToDevice, h->stream);
-   for (uint64_t sw = 0; sw < n_sweeps; ++sw) {
-      MCArgs<R> p;
-      memset(&p, 0, sizeof p);
-      p.a = make_args<R>(h);
-      p.sigma = tab;
-      p.beta = tab + 100;
-      p.mu_ratio = tab + 200;
-      p.replay = s->use_replay ? (const R*)s->replay : nullptr;
-      p.sweep = s->sweep;
-      p.rejects = s->rejects;
-      for (int c = 0; c < s->ncolours; ++c) {
-         p.atoms = s->atoms + s->colour_off[c];
-         p.count = s->colour_off[c + 1] - s->colour_off[c];
-         h->prof_begin(PROF_MC);
-         cudaError_t e = mc_dispatch<R>(p, S.fmt, h->stream);
-         h->prof_end(PROF_MC);
-         if (e != cudaSuccess) return cuda_err(h, e, "mc launch");
-         h->kernel_launches++;
-      }
+   return tab;
+}
+
+// one colour of the current sweep; the last colour completes the sweep
+template <typename R>
+static int mc_run_colour(vgpu_handle h, const R* tab, int c) {
+   MCState* s = mc_of(h);
+   SysDev& S = h->sys;
+   MCArgs<R> p;
+   memset(&p, 0, sizeof p);
+   p.a = make_args<R>(h);
+   p.sigma = tab;
+   p.beta = tab + 100;
+   p.mu_ratio = tab + 200;
+   p.replay = s->use_replay ? (const R*)s->replay : nullptr;
+   p.sweep = s->sweep;
+   p.rejects = s->rejects;
+   p.atoms = s->atoms + s->colour_off[c];
+   p.count = s->colour_off[c + 1] - s->colour_off[c];
+   h->prof_begin(PROF_MC);
+   cudaError_t e = mc_dispatch<R>(p, S.fmt, h->stream);
+   h->prof_end(PROF_MC);
+   if (e != cudaSuccess) return cuda_err(h, e, "mc launch");
+   h->kernel_launches++;
+   s->next_colour = c + 1;
+   if (s->next_colour == s->ncolours) {
+      s->next_colour = 0;
       s->sweep++;
-      s->moves += S.n;
+      s->moves += s->n_owned;
    }
    return VGPU_OK;
+}
+
+template <typename R>
+static int mc_sweeps_typed(vgpu_handle h, uint64_t n_sweeps) {
+   MCState* s = mc_of(h);
+   const R* tab = mc_tables<R>(h);
+   if (!tab) return VGPU_ERR_OOM;
+   for (uint64_t sw = 0; sw < n_sweeps; ++sw)
+      for (int c = 0; c < s->ncolours; ++c)
+         if (const int rc = mc_run_colour<R>(h, tab, c)) return rc;
+   return VGPU_OK;
+}
+
+template <typename R>
+static int mc_colour_typed(vgpu_handle h, int c) {
+   const R* tab = mc_tables<R>(h);
+   if (!tab) return VGPU_ERR_OOM;
+   return mc_run_colour<R>(h, tab, c);
 }
 
 extern "C" int vgpu_mc_sweep(vgpu_handle h, uint64_t n_sweeps) {
@@ -339,8 +375,23 @@ extern "C" int vgpu_mc_sweep(vgpu_handle h, uint64_t n_sweeps) {
    MCState* s = mc_of(h);
    if (!s) return set_err(h, VGPU_ERR_STATE, "vgpu_mc_setup not called");
    if (!(h->params.temperature >= 0.0)) return set_err(h, VGPU_ERR_STATE, "vgpu_set_params not called");
+   if (s->next_colour != 0)
+      return set_err(h, VGPU_ERR_STATE, "a sweep run colour by colour (vgpu_mc_colour) is unfinished");
    cudaSetDevice(h->device);
    return h->prec == VGPU_PREC_FP64 ? mc_sweeps_typed<double>(h, n_sweeps) : mc_sweeps_typed<float>(h, n_sweeps);
+}
+
+extern "C" int vgpu_mc_colour(vgpu_handle h, int32_t colour) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   MCState* s = mc_of(h);
+   if (!s) return set_err(h, VGPU_ERR_STATE, "vgpu_mc_setup not called");
+   if (!(h->params.temperature >= 0.0)) return set_err(h, VGPU_ERR_STATE, "vgpu_set_params not called");
+   if (colour != s->next_colour)
+      return set_err(h, VGPU_ERR_ARG, "colour %d out of order: the current sweep runs colour %d next (of %d)", colour,
+                     s->next_colour, s->ncolours);
+   cudaSetDevice(h->device);
+   return h->prec == VGPU_PREC_FP64 ? mc_colour_typed<double>(h, colour) : mc_colour_typed<float>(h, colour);
 }
 
 extern "C" int vgpu_mc_set_sweep(vgpu_handle h, uint64_t sweep) {
@@ -348,6 +399,7 @@ extern "C" int vgpu_mc_set_sweep(vgpu_handle h, uint64_t sweep) {
    MCState* s = mc_of(h);
    if (!s) return set_err(h, VGPU_ERR_STATE, "vgpu_mc_setup not called");
    s->sweep = sweep;
+   s->next_colour = 0;
    return VGPU_OK;
 }
 

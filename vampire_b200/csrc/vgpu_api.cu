@@ -1124,8 +1124,9 @@ extern "C" int vgpu_set_owned(vgpu_handle h, int32_t n_owned, int64_t noise_base
       return set_err(h, VGPU_ERR_ARG, "noise_base out of the 32-bit atom counter range");
    if (n_owned < S.n && S.bq_off)
       return set_err(h, VGPU_ERR_STATE, "shards carry no biquadratic exchange list");
-   if (n_owned < S.n && (h->extras[1] || h->extras[2]))
-      return set_err(h, VGPU_ERR_STATE, "Monte Carlo and the dipole solver run on whole systems only");
+   if (n_owned < S.n && h->extras[2]) return set_err(h, VGPU_ERR_STATE, "the dipole solver runs on whole systems only");
+   if (h->extras[1] && n_owned != S.n_owned)
+      return set_err(h, VGPU_ERR_STATE, "Monte Carlo colour lists are set up: call vgpu_set_owned before vgpu_mc_setup");
    S.n_owned = n_owned;
    S.noise_base = (uint32_t)noise_base;
    S.stage.grid = 0;

@@ -27,6 +27,14 @@ The same decomposition here, one process per GPU over NVLink/NCCL:
 
 Statistics combine across ranks from the raw per-bin sums of each shard
 (``vgpu_stats_get_sums``) with one all-reduce.
+
+Monte Carlo shards the same way.  A colour-ordered Metropolis sweep updates
+one colour at a time; a shard runs its owned atoms of a colour, then every
+rank refreshes its halo spins before the next colour (``mc_sweep_sharded``),
+as the reference's parallel Monte Carlo swaps halos around each of its eight
+octant phases (src/montecarlo/mc-mpi.cpp:140-210).  With the whole system's
+colouring and the move random numbers keyed by global atom index, the shards
+together make exactly the whole system's sweep.
 """
 from __future__ import annotations
 
@@ -189,6 +197,22 @@ class HaloExchange:
             unpack(peer, first, count, buf)
 
 
+def mc_sweep_sharded(ncolours: int, run_colour: Callable[[int], None], refresh: Callable[[], None]) -> None:
+    """One Monte Carlo sweep of a shard: for every colour in order, the
+    Metropolis pass over the shard's owned atoms of that colour, then the halo
+    refresh of the spins (the next colour's sites read the moved neighbours).
+    Every rank makes the same calls in the same order."""
+    for c in range(ncolours):
+        run_colour(c)
+        refresh()
+
+
+def local_colours(colour: np.ndarray, plan: ShardPlan) -> np.ndarray:
+    """The whole system's colouring restricted to a shard's local atoms
+    (owned, then halo), for vgpu_mc_setup on that shard."""
+    return np.ascontiguousarray(np.asarray(colour)[np.concatenate([plan.owned, plan.halo])], dtype=np.int32)
+
+
 def combine_magnetization(sums: np.ndarray) -> np.ndarray:
     """Reference normalisation (src/statistics/magnetization.cpp:134-180) of
     raw per-bin sums [bins, >=4] = (sum mu sx, sum mu sy, sum mu sz, sum mu)
@@ -249,6 +273,17 @@ class ShardedSimulation:
             self._refresh(vgpu.STATE_PREDICTOR)
             self.sim.llg_pass(vgpu.PASS_CORRECTOR)
             self._refresh(vgpu.STATE_SPIN)
+
+    def mc_setup(self, colour: np.ndarray) -> int:
+        """Monte Carlo on this shard with the whole system's colouring
+        `colour` (one entry per global atom); returns the number of colours."""
+        self.ncolours = self.sim.mc_setup(local_colours(colour, self.plan))
+        return self.ncolours
+
+    def mc_sweep(self, n_sweeps: int = 1) -> None:
+        from . import vgpu
+        for _ in range(n_sweeps):
+            mc_sweep_sharded(self.ncolours, self.sim.mc_colour, lambda: self._refresh(vgpu.STATE_SPIN))
 
     def owned_spins(self) -> np.ndarray:
         return self.sim.spins()[:, : self.plan.n_owned]

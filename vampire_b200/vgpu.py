@@ -453,6 +453,10 @@ class Simulation:
     def mc_sweep(self, n_sweeps: int = 1) -> None:
         self._check(lib().vgpu_mc_sweep(self._h, C.c_uint64(n_sweeps)))
 
+    def mc_colour(self, colour: int) -> None:
+        """One colour of the current sweep (vgpu_mc_colour; colours in order)."""
+        self._check(lib().vgpu_mc_colour(self._h, C.c_int32(colour)))
+
     def mc_set_sweep(self, sweep: int) -> None:
         self._check(lib().vgpu_mc_set_sweep(self._h, C.c_uint64(sweep)))
 
