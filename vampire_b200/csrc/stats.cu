@@ -45,6 +45,7 @@ struct StatsMask {
    double* mean = nullptr;     // [size][ST_W] running sums of the finalised rows
    double* raw = nullptr;      // [size][ST_NQ] raw sums of the last update (combined across shards)
    double* derived = nullptr;  // [size][ST_DV] running sums behind the derived statistics
+   int* ticket = nullptr;      // blocks finished in the running small-mask update (0 between updates)
    std::vector<double> saturation;     // [size] sum of mu_s (mu_B) per bin (magnetization set_mask)
    std::vector<double> normalisation;  // [size] atoms per bin (energy set_mask)
    long long counter_mag = 0, counter_en = 0;
@@ -63,36 +64,166 @@ __device__ __forceinline__ double warp_sum(double v) {
    return v;
 }
 
+__device__ __forceinline__ void two_sum_acc(double& s, double& c, double x) {
+   const double t = s + x;
+   c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+   s = t;
+}
+
+// Merge of the block partial rows of one bin and the finalised row, running
+// means and derived sums: warp q of the calling block merges quantity q with
+// compensated sums (32 * ST_NQ threads take part), thread 0 finalises.  The
+// partial rows are read through L2 (written by other blocks of the same
+// launch when called from the last block of stats_mag_small_kernel).
+__device__ void stats_finalize_bin(const double* __restrict__ partial, int nblocks, int size, int bin, int do_mag,
+                                   int do_energy, double* __restrict__ cur, double* __restrict__ mean,
+                                   double* __restrict__ raw, double* __restrict__ derived, double mag_count,
+                                   double* vq) {
+   const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   double s = 0.0, c = 0.0;
+   if (q < ST_NQ) {
+      // eight partial rows per lane in flight at a time, then their compensated adds
+      for (int b0 = lane; b0 < nblocks; b0 += 32 * 8) {
+         double v[8];
+#pragma unroll
+         for (int u = 0; u < 8; ++u) {
+            const int b = b0 + 32 * u;
+            v[u] = b < nblocks ? __ldcg(partial + ((size_t)b * size + bin) * ST_NQ + q) : 0.0;
+         }
+#pragma unroll
+         for (int u = 0; u < 8; ++u) two_sum_acc(s, c, v[u]);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+         const double s2 = __shfl_down_sync(0xffffffffu, s, o);
+         const double c2 = __shfl_down_sync(0xffffffffu, c, o);
+         if (lane < o) {
+            two_sum_acc(s, c, s2);
+            c += c2;
+         }
+      }
+      if (lane == 0) {
+         vq[q] = s + c;
+         raw[(size_t)bin * ST_NQ + q] = s + c;
+      }
+   }
+   __syncthreads();
+   if (threadIdx.x != 0) return;
+   const double* v = vq;
+   double* o = cur + (size_t)bin * ST_W;
+   double* mn = mean + (size_t)bin * ST_W;
+   if (do_mag) {
+      const double msat = v[ST_MU];
+      const double magm = sqrt(v[ST_MX] * v[ST_MX] + v[ST_MY] * v[ST_MY] + v[ST_MZ] * v[ST_MZ]);
+      if (msat == 0.0) {
+         o[0] = o[1] = o[2] = o[3] = 0.0;
+      } else {
+         o[0] = v[ST_MX] / magm;
+         o[1] = v[ST_MY] / magm;
+         o[2] = v[ST_MZ] / magm;
+         o[3] = magm / msat;
+      }
+      for (int k = 0; k < 4; ++k) mn[k] += o[k];
+      double* dv = derived + (size_t)bin * ST_DV;
+      const double mm = o[3];
+      for (int k = 0; k < 3; ++k) {
+         dv[DV_SUS + k] += o[k] * mm;
+         dv[DV_SUS2 + k] += o[k] * o[k] * mm * mm;
+         dv[DV_ASUS + k] += fabs(o[k] * mm);
+         dv[DV_ASUS2 + k] += fabs(o[k] * o[k] * mm * mm);
+      }
+      dv[DV_SUS + 3] += mm;
+      dv[DV_SUS2 + 3] += mm * mm;
+      dv[DV_ASUS + 3] += mm;
+      dv[DV_ASUS2 + 3] += mm * mm;
+      for (int k = 0; k < 4; ++k) {  // Welford update, mag_count includes this update
+         const double r1 = o[k] - dv[DV_MEAN + k];
+         dv[DV_MEAN + k] += r1 / mag_count;
+         const double r2 = o[k] - dv[DV_MEAN + k];
+         dv[DV_RES + k] += r1 * r2;
+      }
+   }
+   if (do_energy) {
+      const double ex = 0.5 * v[ST_EEX], an = v[ST_EAN], ap = v[ST_EAP], ms = 0.5 * v[ST_EMS];
+      o[4] = ex + an + ap + ms;
+      o[5] = ex; o[6] = an; o[7] = ap; o[8] = ms;
+      for (int k = 4; k < 9; ++k) mn[k] += o[k];
+      double* dv = derived + (size_t)bin * ST_DV;
+      dv[DV_E] += o[4];
+      dv[DV_E2] += o[4] * o[4];
+   }
+}
+
+
 // Magnetisation only, masks of at most NB bins (system, material of a few
 // materials): per-thread register sums over a grid-stride loop (no
-// reductions inside the loop, loads of successive atoms in flight together),
-// one warp reduction and shared-memory add per block at the end.  Writes the
-// same block partial rows as stats_partial_kernel (energy quantities zero).
+// reductions inside the loop), one warp reduction and shared-memory add per
+// block at the end.  FP32 state is read four atoms at a time (16-byte loads of
+// x, y, z, material and mask ids), the moments per material come from shared
+// memory (no dependent global load per atom).  Writes the same block partial
+// rows as stats_partial_kernel (energy quantities zero).
+constexpr int kStatsMuShared = 64;  // materials whose moments the kernel keeps in shared memory
+
+// The last block to finish (atomic ticket after a fence) merges every block's
+// row and finalises the bins (stats_finalize_bin), so one launch does the
+// whole update; it resets the ticket for the next launch.
+struct StatsOut {
+   int* ticket;
+   double* cur;
+   double* mean;
+   double* raw;
+   double* derived;
+   double mag_count;
+};
+
 template <typename R, int NB>
 __global__ void __launch_bounds__(256) stats_mag_small_kernel(const LLGArgs<R> a, const int* __restrict__ mask,
-                                                              int size, double* __restrict__ partial) {
+                                                              int size, double* __restrict__ partial,
+                                                              const StatsOut so) {
    __shared__ double acc[NB * ST_NQ];
+   __shared__ double smu[kStatsMuShared];
+   const bool mu_shared = a.M <= kStatsMuShared;
    for (int k = threadIdx.x; k < NB * ST_NQ; k += blockDim.x) acc[k] = 0.0;
+   if (mu_shared)
+      for (int k = threadIdx.x; k < a.M; k += blockDim.x) smu[k] = (double)a.mp[k].mu_s_muB;
    __syncthreads();
    double s[NB][4];
 #pragma unroll
    for (int b = 0; b < NB; ++b) s[b][0] = s[b][1] = s[b][2] = s[b][3] = 0.0;
-   const int stride = gridDim.x * blockDim.x;
-#pragma unroll 4
-   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_upd; i += stride) {
-      const int mi = a.mat ? __ldg(a.mat + i) : 0;
-      const double mu = (double)a.mp[mi].mu_s_muB;
-      const int bin = NB == 1 ? 0 : __ldg(mask + i);
-      const double x = (double)a.ax[i] * mu, y = (double)a.ay[i] * mu, z = (double)a.az[i] * mu;
+   auto add = [&](int mi, int bin, R sx, R sy, R sz) {
+      const double mu = mu_shared ? smu[mi] : (double)a.mp[mi].mu_s_muB;
+      const double x = (double)sx * mu, y = (double)sy * mu, z = (double)sz * mu;
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-         const bool on = bin == b;
+         const bool on = NB == 1 || bin == b;
          s[b][0] += on ? x : 0.0;
          s[b][1] += on ? y : 0.0;
          s[b][2] += on ? z : 0.0;
          s[b][3] += on ? mu : 0.0;
       }
+   };
+   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+   const int stride = gridDim.x * blockDim.x;
+   int i0 = 0;  // first atom of the scalar loop
+   if (sizeof(R) == 4) {
+      const int ng = a.n_upd >> 2;
+      const float4* X = reinterpret_cast<const float4*>(a.ax);
+      const float4* Y = reinterpret_cast<const float4*>(a.ay);
+      const float4* Z = reinterpret_cast<const float4*>(a.az);
+#pragma unroll 2
+      for (int g = tid; g < ng; g += stride) {
+         const float4 x = __ldg(X + g), y = __ldg(Y + g), z = __ldg(Z + g);
+         const int4 m = a.mat ? __ldg(reinterpret_cast<const int4*>(a.mat) + g) : make_int4(0, 0, 0, 0);
+         const int4 bn = NB == 1 ? make_int4(0, 0, 0, 0) : __ldg(reinterpret_cast<const int4*>(mask) + g);
+         add(m.x, bn.x, x.x, y.x, z.x);
+         add(m.y, bn.y, x.y, y.y, z.y);
+         add(m.z, bn.z, x.z, y.z, z.z);
+         add(m.w, bn.w, x.w, y.w, z.w);
+      }
+      i0 = ng << 2;
    }
+   for (int i = i0 + tid; i < a.n_upd; i += stride)
+      add(a.mat ? __ldg(a.mat + i) : 0, NB == 1 ? 0 : __ldg(mask + i), a.ax[i], a.ay[i], a.az[i]);
    const int lane = threadIdx.x & 31;
 #pragma unroll
    for (int b = 0; b < NB; ++b)
@@ -104,6 +235,19 @@ __global__ void __launch_bounds__(256) stats_mag_small_kernel(const LLGArgs<R> a
    __syncthreads();
    double* out = partial + (size_t)blockIdx.x * size * ST_NQ;  // size <= NB bins
    for (int k = threadIdx.x; k < size * ST_NQ; k += blockDim.x) out[k] = acc[k];
+   __shared__ int last;
+   __threadfence();  // this block's row is visible before its ticket
+   __syncthreads();
+   if (threadIdx.x == 0) last = atomicAdd(so.ticket, 1) == (int)gridDim.x - 1;
+   __syncthreads();
+   if (!last) return;
+   __threadfence();
+   __shared__ double vq[ST_NQ];
+   for (int bin = 0; bin < size; ++bin) {
+      stats_finalize_bin(partial, gridDim.x, size, bin, 1, 0, so.cur, so.mean, so.raw, so.derived, so.mag_count, vq);
+      __syncthreads();  // vq is reused by the next bin
+   }
+   if (threadIdx.x == 0) *so.ticket = 0;
 }
 
 template <typename R, int FMT>
@@ -197,12 +341,6 @@ __global__ void stats_partial_kernel(const LLGArgs<R> a, const int* __restrict__
 // block per bin, one warp per quantity: each lane keeps a Neumaier sum over a
 // strided share of the partials, and the 32 (sum, compensation) pairs are
 // merged by error-free two-sums in a fixed tree order (deterministic).
-__device__ __forceinline__ void two_sum_acc(double& s, double& c, double x) {
-   const double t = s + x;
-   c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
-   s = t;
-}
-
 __global__ void __launch_bounds__(32 * ST_NQ) stats_final_kernel(const double* __restrict__ partial, int nblocks,
                                                                   int size, int do_mag, int do_energy,
                                                                   double* __restrict__ cur,
@@ -210,68 +348,7 @@ __global__ void __launch_bounds__(32 * ST_NQ) stats_final_kernel(const double* _
                                                                   double* __restrict__ raw,
                                                                   double* __restrict__ derived, double mag_count) {
    __shared__ double vq[ST_NQ];
-   const int bin = blockIdx.x;
-   const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
-   double s = 0.0, c = 0.0;
-   for (int b = lane; b < nblocks; b += 32) two_sum_acc(s, c, partial[((size_t)b * size + bin) * ST_NQ + q]);
-#pragma unroll
-   for (int o = 16; o > 0; o >>= 1) {
-      const double s2 = __shfl_down_sync(0xffffffffu, s, o);
-      const double c2 = __shfl_down_sync(0xffffffffu, c, o);
-      if (lane < o) {
-         two_sum_acc(s, c, s2);
-         c += c2;
-      }
-   }
-   if (lane == 0) {
-      vq[q] = s + c;
-      raw[(size_t)bin * ST_NQ + q] = s + c;
-   }
-   __syncthreads();
-   if (threadIdx.x != 0) return;
-   const double* v = vq;
-   double* o = cur + (size_t)bin * ST_W;
-   double* mn = mean + (size_t)bin * ST_W;
-   if (do_mag) {
-      const double msat = v[ST_MU];
-      const double magm = sqrt(v[ST_MX] * v[ST_MX] + v[ST_MY] * v[ST_MY] + v[ST_MZ] * v[ST_MZ]);
-      if (msat == 0.0) {
-         o[0] = o[1] = o[2] = o[3] = 0.0;
-      } else {
-         o[0] = v[ST_MX] / magm;
-         o[1] = v[ST_MY] / magm;
-         o[2] = v[ST_MZ] / magm;
-         o[3] = magm / msat;
-      }
-      for (int k = 0; k < 4; ++k) mn[k] += o[k];
-      double* dv = derived + (size_t)bin * ST_DV;
-      const double mm = o[3];
-      for (int k = 0; k < 3; ++k) {
-         dv[DV_SUS + k] += o[k] * mm;
-         dv[DV_SUS2 + k] += o[k] * o[k] * mm * mm;
-         dv[DV_ASUS + k] += fabs(o[k] * mm);
-         dv[DV_ASUS2 + k] += fabs(o[k] * o[k] * mm * mm);
-      }
-      dv[DV_SUS + 3] += mm;
-      dv[DV_SUS2 + 3] += mm * mm;
-      dv[DV_ASUS + 3] += mm;
-      dv[DV_ASUS2 + 3] += mm * mm;
-      for (int k = 0; k < 4; ++k) {  // Welford update, mag_count includes this update
-         const double r1 = o[k] - dv[DV_MEAN + k];
-         dv[DV_MEAN + k] += r1 / mag_count;
-         const double r2 = o[k] - dv[DV_MEAN + k];
-         dv[DV_RES + k] += r1 * r2;
-      }
-   }
-   if (do_energy) {
-      const double ex = 0.5 * v[ST_EEX], an = v[ST_EAN], ap = v[ST_EAP], ms = 0.5 * v[ST_EMS];
-      o[4] = ex + an + ap + ms;
-      o[5] = ex; o[6] = an; o[7] = ap; o[8] = ms;
-      for (int k = 4; k < 9; ++k) mn[k] += o[k];
-      double* dv = derived + (size_t)bin * ST_DV;
-      dv[DV_E] += o[4];
-      dv[DV_E2] += o[4] * o[4];
-   }
+   stats_finalize_bin(partial, nblocks, size, blockIdx.x, do_mag, do_energy, cur, mean, raw, derived, mag_count, vq);
 }
 
 template <typename R, int FMT>
@@ -283,14 +360,16 @@ static cudaError_t launch_stats(const LLGArgs<R>& a, StatsMask& m, int nblocks, 
                                            (int)smem);
       if (e != cudaSuccess) return e;
    }
-   if (!do_energy && m.size <= 4) {
-      // the per-step magnetisation of small masks
-      if (m.size == 1) stats_mag_small_kernel<R, 1><<<nblocks, 256, 0, st>>>(a, m.mask, m.size, m.partial);
-      else if (m.size == 2) stats_mag_small_kernel<R, 2><<<nblocks, 256, 0, st>>>(a, m.mask, m.size, m.partial);
-      else stats_mag_small_kernel<R, 4><<<nblocks, 256, 0, st>>>(a, m.mask, m.size, m.partial);
-   } else {
-      stats_partial_kernel<R, FMT><<<nblocks, 256, smem, st>>>(a, m.mask, m.size, do_energy, hm, m.partial);
+   if (do_mag && !do_energy && m.size <= 4) {
+      // the per-step magnetisation of small masks: one launch, merged and
+      // finalised by its last block
+      const StatsOut so{m.ticket, m.cur, m.mean, m.raw, m.derived, (double)(m.counter_mag + 1)};
+      if (m.size == 1) stats_mag_small_kernel<R, 1><<<nblocks, 256, 0, st>>>(a, m.mask, m.size, m.partial, so);
+      else if (m.size == 2) stats_mag_small_kernel<R, 2><<<nblocks, 256, 0, st>>>(a, m.mask, m.size, m.partial, so);
+      else stats_mag_small_kernel<R, 4><<<nblocks, 256, 0, st>>>(a, m.mask, m.size, m.partial, so);
+      return cudaGetLastError();
    }
+   stats_partial_kernel<R, FMT><<<nblocks, 256, smem, st>>>(a, m.mask, m.size, do_energy, hm, m.partial);
    cudaError_t e = cudaGetLastError();
    if (e != cudaSuccess) return e;
    stats_final_kernel<<<m.size, 32 * ST_NQ, 0, st>>>(m.partial, nblocks, m.size, do_mag, do_energy, m.cur, m.mean,
@@ -316,6 +395,7 @@ void stats_destroy(vgpu_ctx* h) {
    if (!s) return;
    for (StatsMask& m : s->masks) {
       cudaFree(m.mask); cudaFree(m.partial); cudaFree(m.cur); cudaFree(m.mean); cudaFree(m.raw); cudaFree(m.derived);
+      cudaFree(m.ticket);
    }
    delete s;
    h->extras[0] = nullptr;
@@ -338,7 +418,7 @@ extern "C" int vgpu_stats_add_mask(vgpu_handle h, const int32_t* mask, int32_t m
    StatsState* s = stats_of(h);
    int dev_sms = 148;
    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, h->device);
-   s->nblocks = std::max(1, std::min(4 * dev_sms, (n + 255) / 256));
+   s->nblocks = std::max(1, std::min(8 * dev_sms, (n + 255) / 256));  // a full SM of 256-thread blocks
    StatsMask m;
    m.size = mask_size;
    cudaError_t e;
@@ -352,6 +432,8 @@ extern "C" int vgpu_stats_add_mask(vgpu_handle h, const int32_t* mask, int32_t m
    cudaMemsetAsync(m.raw, 0, sizeof(double) * mask_size * ST_NQ, h->stream);
    if ((e = cudaMalloc(&m.derived, sizeof(double) * mask_size * ST_DV)) != cudaSuccess) return cuda_err(h, e, "stats");
    cudaMemsetAsync(m.derived, 0, sizeof(double) * mask_size * ST_DV, h->stream);
+   if ((e = cudaMalloc(&m.ticket, sizeof(int))) != cudaSuccess) return cuda_err(h, e, "stats");
+   cudaMemsetAsync(m.ticket, 0, sizeof(int), h->stream);
    // bin saturation and atom counts, summed in atom order as set_mask does
    // (statistics/magnetization.cpp:54-116 with mm = mu_s/mu_B, energy.cpp:84-89)
    m.saturation.assign(mask_size, 0.0);
