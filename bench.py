@@ -137,15 +137,19 @@ def traffic_from_profiles(kernel: str, records: str):
     return None
 
 
-def byte_model(z=12, b_J=12, multi_mat=True, dipole=False):
+def byte_model(z=12, b_J=12, multi_mat=True, dipole=False, noise_store=True):
     """Algorithmic HBM bytes per spin per pass (FP32 SoA state, int32 index):
     predictor reads s0 and writes s'; corrector reads s0 and s' and writes s1;
     each pass streams the neighbour words, the per-bond DMI vector (b_J = 12;
     0 with compact records, whose coupling comes from a dictionary of a few
     hundred bytes), the material id and (with the dipole field) the cell id;
-    neighbour spins are L2-served; noise is regenerated in-register (0 B)."""
+    neighbour spins are L2-served.  The thermal Gaussians are generated
+    in-register by the predictor, which stores them (12 B) for the corrector
+    to read back (12 B) when noise_store; otherwise both passes regenerate
+    them (0 B)."""
     gather = 4 * (z + 1) + b_J * z + 4 * int(multi_mat) + 4 * int(dipole)
-    return {"predictor": 24 + gather, "corrector": 36 + gather}
+    g = 12 * int(noise_store)
+    return {"predictor": 24 + gather + g, "corrector": 36 + gather + g}
 
 
 def bench_batched(device, steps=2000, plain_steps=200):

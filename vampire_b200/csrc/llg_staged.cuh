@@ -85,12 +85,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* m, uint32_t parity) 
 // resident blocks hide the copy) or 2 (persistent, next tile's copy in flight
 // while this one is computed).  Each buffer holds the tile's bond records
 // (buf_bytes) and its own-atom arrays (kStageOwnArrays x 32 SL words: s0 x|y|z,
-// s' x|y|z for the corrector, material ids, cell ids), all brought by bulk
+// s' x|y|z for the corrector, material ids, cell ids, and for the corrector
+// the step's thermal Gaussians that the predictor stored), all brought by bulk
 // copies completing on the buffer's barrier; after the buffers come the
 // coupling dictionary (compact records, copied with the block's first tile)
 // and the material table (read into shared memory once per block when it has
-// at most kStageMaxMat rows).  The Philox Gaussians of the tile's atoms need no
-// data and are generated while the copy is in flight.
+// at most kStageMaxMat rows).  The predictor generates the Philox Gaussians of
+// the tile's atoms while the copy is in flight (they need no data) and stores
+// them (a.gx); the corrector, which needs the same numbers, copies them in
+// with the tile instead of generating them again.
 // Registers are capped for 768 resident threads per SM (85 a thread): the
 // compact-record corrector otherwise takes 92 and fits 5 blocks of 128
 // (measured 12 % slower); a cap at 64 spills and was slower again.
@@ -116,7 +119,8 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
       const void* src = CREC ? (const void*)(a.crec + o0) : (const void*)(a.rec + o0);
       const uint32_t db = first ? dict_bytes : 0u;
       const uint32_t nb = 128u * (uint32_t)(s1 - s0);  // own-array bytes: 32 atoms x 4 B per slice
-      const int na = 3 + (MODE == PASS_CORRECTOR ? 3 : 0) + (a.mat ? 1 : 0) + (a.cell ? 1 : 0);
+      const bool gin = MODE == PASS_CORRECTOR && a.gx;
+      const int na = 3 + (MODE == PASS_CORRECTOR ? 3 : 0) + (a.mat ? 1 : 0) + (a.cell ? 1 : 0) + (gin ? 3 : 0);
       unsigned char* buf = stage_smem + b * stride;
       float* own = reinterpret_cast<float*>(buf + buf_bytes);
       const size_t a0 = (size_t)s0 * 32;
@@ -134,6 +138,11 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
       }
       if (a.mat) bulk_copy_g2s(own + 6 * TS, a.mat + a0, nb, &mbar[b]);
       if (a.cell) bulk_copy_g2s(own + 7 * TS, a.cell + a0, nb, &mbar[b]);
+      if (gin) {
+         bulk_copy_g2s(own + 8 * TS, a.gx + a0, nb, &mbar[b]);
+         bulk_copy_g2s(own + 9 * TS, a.gy + a0, nb, &mbar[b]);
+         bulk_copy_g2s(own + 10 * TS, a.gz + a0, nb, &mbar[b]);
+      }
    };
    uint32_t phase = 0;  // bit b: parity of the phase of mbar[b] to wait for next
    int t = blockIdx.x, k = 0, b = 0;
@@ -158,9 +167,13 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
       if (tid == 0 && NBUF == 2 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x, b ^ 1, false);
       const int i = t * TS + tid;
       const bool act = i < a.n_upd;
-      // the tile's Gaussians (the Philox noise needs no data) while the copy lands
+      // the tile's Gaussians (the Philox noise needs no data) while the copy lands;
+      // the predictor keeps them for the corrector
       float g[3] = {0.f, 0.f, 0.f};
-      if (a.thermal) thermal_xi(a, act ? i : 0, g[0], g[1], g[2]);
+      if (a.thermal && (MODE == PASS_PREDICTOR || !a.gx)) {
+         thermal_xi(a, act ? i : 0, g[0], g[1], g[2]);
+         if (MODE == PASS_PREDICTOR && a.gx && act) { a.gx[i] = g[0]; a.gy[i] = g[1]; a.gz[i] = g[2]; }
+      }
       const int tile_off = __ldg(a.slice_off + t * SL);
       const bool done = mbar_wait_bounded(&mbar[b], (phase >> b) & 1u);
       if (__syncthreads_or(!done)) {  // every thread takes the same branch
@@ -170,6 +183,9 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
       phase ^= 1u << b;
       const unsigned char* buf = stage_smem + b * stride;
       const float* own = reinterpret_cast<const float*>(buf + buf_bytes);
+      if (MODE == PASS_CORRECTOR && a.thermal && a.gx) {
+         g[0] = own[8 * TS + tid]; g[1] = own[9 * TS + tid]; g[2] = own[10 * TS + tid];
+      }
       if (act) {
          const int mi = a.mat ? reinterpret_cast<const int*>(own)[6 * TS + tid] : 0;
          const MatParams<float> m = mpt[mi];

@@ -576,6 +576,14 @@ static int prepare_passes(vgpu_ctx* h, bool* staged_out, int integrator = INTEG_
       if (e != cudaSuccess) return cuda_err(h, e, "staged pass setup (tile records exceed shared memory?)");
       h->sys.stage = c;
    }
+   if (staged && !h->sys.stage.win && !h->sys.g_store[0]) {
+      // the step's Gaussians, passed from the predictor to the corrector
+      const size_t len = ((size_t)h->sys.n_alloc + 3) & ~(size_t)3;
+      for (int q = 0; q < 3; ++q) {
+         h->sys.g_store[q] = h->alloc(len * sizeof(R));
+         if (!h->sys.g_store[q]) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for the noise buffers");
+      }
+   }
    *staged_out = staged;
    return VGPU_OK;
 }
@@ -585,6 +593,9 @@ template <typename R>
 static int run_pass(vgpu_ctx* h, int mode, bool staged, int integrator = INTEG_HEUN) {
    LLGArgs<R> a = make_args<R>(h);
    a.integrator = integrator;
+   if (staged && !h->sys.stage.win) {
+      a.gx = (R*)h->sys.g_store[0]; a.gy = (R*)h->sys.g_store[1]; a.gz = (R*)h->sys.g_store[2];
+   }
    const int kind = mode == PASS_PREDICTOR ? PROF_PREDICTOR : PROF_CORRECTOR;
    h->prof_begin(kind);
    cudaError_t e = launch_step_pass<R>(h, a, mode, staged);

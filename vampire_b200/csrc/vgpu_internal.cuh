@@ -107,6 +107,8 @@ struct LLGArgs {
    R* bx; R* by; R* bz;      // state B: s' (predictor output)
    R* fx; R* fy; R* fz;      // field output (field-only mode)
    R* ex; R* ey; R* ez;      // stored predictor increment f(s0), or nullptr (recovered)
+   R* gx; R* gy; R* gz;      // staged passes: the step's thermal Gaussians, written by the
+                             // predictor and read back by the corrector, or nullptr
    int* status;              // device status word (non-finite spin flag)
    int stage_extra_tx;       // staged passes: extra bytes each tile expects (0; > 0 tests the bounded wait)
 };
@@ -127,7 +129,7 @@ cudaError_t launch_llg_pass(const LLGArgs<R>& a, int fmt, int mode, int nslices,
 // slices, nbuf shared-memory buffers of buf_bytes (the largest tile's records),
 // and with compact records (crec) the coupling dictionary (dict_bytes) after them.
 constexpr int kStageSmemLimit = 200 * 1024;  // dynamic shared memory the staged passes may take
-constexpr int kStageOwnArrays = 8;            // own-atom arrays per staged buffer (32 SL words each)
+constexpr int kStageOwnArrays = 11;           // own-atom arrays per staged buffer (32 SL words each)
 constexpr int kStageMaxMat = 64;              // material rows the staged passes keep in shared memory
 struct StageCfg {
    int sl = 4, nbuf = 1, buf_bytes = 0;
