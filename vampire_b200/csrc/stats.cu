@@ -460,7 +460,7 @@ static int stats_update_typed(vgpu_handle h, int flags) {
       cudaError_t e = stats_dispatch<R>(a, h->sys.fmt, m, s->nblocks, flags & 1, (flags >> 1) & 1,
                                         (const R*)h->sys.hm_atom, h->stream);
       if (e != cudaSuccess) return cuda_err(h, e, "stats launch");
-      h->kernel_launches += 2;
+      h->kernel_launches += ((flags & 3) == 1 && m.size <= 4) ? 1 : 2;  // small masks: one launch
       if (flags & 1) m.counter_mag++;
       if (flags & 2) m.counter_en++;
    }
