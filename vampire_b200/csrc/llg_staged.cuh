@@ -1,18 +1,17 @@
 // Fused LLG-Heun passes with bulk-staged bond records (FP32, FMT_DMI_TAB).
 //
-// The per-bond records {neighbour, d_x, d_y, d_z} are the bulk of the HBM
-// stream (12 x 16 B per atom per pass), or with compact records (CREC) one
+// The per-bond records are the bulk of the HBM stream: {neighbour, d_x, d_y,
+// d_z} (12 x 16 B per atom per pass) or, with compact records (CREC), one
 // 4-byte word per bond, neighbour | coupling index, whose couplings come from
-// a dictionary that every block first copies into its shared memory.  In the plain pass every thread loads
-// its own twelve; here a block walks tiles of 32 SL atoms and thread 0
-// issues ONE cp.async.bulk (1-D bulk copy, global -> this CTA's shared memory,
-// no multicast) for the whole contiguous record range of a tile, completing on
-// an mbarrier with the byte count given by expect_tx.  Threads then read their records from shared memory;
-// neighbour spins are gathered through L1/L2 as before.  While the copy is in
-// flight each thread loads its own state and material and evaluates its
-// external field (the Philox noise is most of the pass's arithmetic).  The
-// arithmetic is the plain pass's (spin_field, external_field and the
-// llg_*_finish tails of llg_kernels.cuh), so results are identical.
+// a dictionary that every block copies into its shared memory.  In the plain
+// pass every thread loads its own twelve; here a block walks tiles of 32 SL
+// atoms and thread 0 issues one cp.async.bulk (1-D bulk copy, global -> this
+// CTA's shared memory, no multicast) for the whole contiguous record range of
+// a tile, plus one per own-atom array of the tile, completing on an mbarrier
+// with the byte count given by expect_tx.  Threads read their records and
+// own-atom data from shared memory; neighbour spins are gathered through
+// L1/L2.  The arithmetic is the plain pass's (spin_field, external_field and
+// the llg_*_finish tails of llg_kernels.cuh), so results are identical.
 //
 // Waits on the mbarriers are bounded (1 s of wall time, and a poll count): if
 // a copy has not landed by then the block records status bit 2
