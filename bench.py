@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-dipole", action="store_true", help="leave out the macrocell dipole field")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and Monte Carlo side results")
-    ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--e2e-steps", type=int, default=2000,
+                    help="steps of the end-to-end run (the workload's 2,000: initial upload and final download once)")
     ap.add_argument("--records", choices=["auto", "wide"], default="auto",
                     help="bond records: auto = compact words + coupling dictionary when the system allows, "
                          "wide = 16-byte records")
