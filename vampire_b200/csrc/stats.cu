@@ -361,6 +361,7 @@ static cudaError_t launch_stats(const LLGArgs<R>& a, StatsMask& m, int nblocks, 
       if (e != cudaSuccess) return e;
    }
    if (do_mag && !do_energy && m.size <= 4) {
+      nblocks = std::max(1, nblocks / 2);  // 4 blocks per SM: measured best for this streaming kernel
       // the per-step magnetisation of small masks: one launch, merged and
       // finalised by its last block
       const StatsOut so{m.ticket, m.cur, m.mean, m.raw, m.derived, (double)(m.counter_mag + 1)};
