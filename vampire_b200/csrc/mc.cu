@@ -77,8 +77,12 @@ __device__ __forceinline__ R site_energy_delta(const LLGArgs<R>& a, int i, const
    return d;
 }
 
+// Capped at 40 registers (6 blocks of 256 per SM instead of 5): the kernel
+// is latency-bound on its gathers, and the extra warps outweigh the spilled
+// registers (2.24e10 -> 2.51e10 spin-moves/s on the Curie protocol of SC 50^3
+// x 31 temperatures; a cap at 32 spills more and gave 2.39e10).
 template <typename R, int FMT>
-__global__ void __launch_bounds__(256) mc_colour_kernel(const MCArgs<R> p) {
+__global__ void __launch_bounds__(256, 6) mc_colour_kernel(const MCArgs<R> p) {
    const int t = blockIdx.x * blockDim.x + threadIdx.x;
    bool rejected = false;
    if (t < p.count) {
