@@ -24,6 +24,77 @@ inline int4 make_seg(int a, int b, int c) {
    return v;
 }
 
+// Shared-memory bank placement of the coupling dictionary.  A 16-byte load
+// by a warp is served a quarter-warp (8 lanes) at a time, and two lanes of a
+// quarter that read different entries whose ids are equal modulo 8 fall in
+// the same four banks and are served in turn.  The ids are therefore
+// reassigned so that entries that quarter-warps read together at the same
+// bond slot get different residues modulo 8: the co-reads of every pair of
+// entries are counted over the SELL layout, then each entry (heaviest first)
+// takes the residue with the least co-read weight to the entries already
+// placed there, at most ceil(n / 8) per residue; id = residue + 8 x (its rank
+// within the residue).  Ids that no entry takes are left as zero entries.
+// Only the placement changes: every bond keeps its coupling values.
+inline void bank_order_dictionary(const std::vector<int>& off, int shift, bool scalar, size_t qmax,
+                                  std::vector<uint32_t>& crec, std::vector<float>& dict, int& ndict) {
+   const int nd = ndict;
+   const int cap = (nd + 7) / 8;
+   if (8 * (size_t)cap > qmax) return;  // no room for the spread ids: keep first-seen ids
+   const int nslices = (int)off.size() - 1;
+   const uint32_t low = (1u << shift) - 1u;
+   std::vector<double> wgt((size_t)nd * nd, 0.0);
+   int q8[8];
+   for (int sl = 0; sl < nslices; ++sl) {
+      const int w = (off[sl + 1] - off[sl]) >> 5;
+      for (int k = 0; k < w; ++k)
+         for (int g = 0; g < 4; ++g) {
+            int m = 0;
+            for (int l = 8 * g; l < 8 * g + 8; ++l) {
+               const int q = (int)(crec[(size_t)off[sl] + 32 * (size_t)k + l] >> shift);
+               bool seen = false;
+               for (int u = 0; u < m; ++u) seen |= q8[u] == q;
+               if (!seen) q8[m++] = q;
+            }
+            for (int u = 0; u < m; ++u)
+               for (int v = u + 1; v < m; ++v) {
+                  wgt[(size_t)q8[u] * nd + q8[v]] += 1.0;
+                  wgt[(size_t)q8[v] * nd + q8[u]] += 1.0;
+               }
+         }
+   }
+   std::vector<int> order(nd), res(nd, -1), count(8, 0), rank(nd, 0);
+   std::vector<double> tot(nd, 0.0);
+   for (int a = 0; a < nd; ++a) {
+      order[a] = a;
+      for (int b = 0; b < nd; ++b) tot[a] += wgt[(size_t)a * nd + b];
+   }
+   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return tot[x] > tot[y]; });
+   for (int a : order) {
+      int best = -1;
+      double bw = 0.0;
+      for (int r = 0; r < 8; ++r) {
+         if (count[r] >= cap) continue;
+         double c = 0.0;
+         for (int b = 0; b < nd; ++b)
+            if (res[b] == r) c += wgt[(size_t)a * nd + b];
+         if (best < 0 || c < bw) { best = r; bw = c; }
+      }
+      res[a] = best;
+      rank[a] = count[best]++;
+   }
+   const int nnew = 8 * cap;
+   std::vector<uint32_t> id(nd);
+   for (int a = 0; a < nd; ++a) id[a] = (uint32_t)(res[a] + 8 * rank[a]);
+   for (auto& wd : crec) wd = (wd & low) | (id[wd >> shift] << shift);
+   const int blocks = scalar ? 1 : 2;  // {J, d} entries, then {Jyy, Jzz} entries
+   std::vector<float> out((size_t)4 * nnew * blocks, 0.0f);
+   for (int bl = 0; bl < blocks; ++bl)
+      for (int a = 0; a < nd; ++a)
+         for (int c = 0; c < 4; ++c) out[4 * ((size_t)bl * nnew + id[a]) + c] = dict[4 * ((size_t)bl * nd + a) + c];
+   dict.swap(out);
+   ndict = nnew;
+}
+
 // Compact FP32 DMI records: every SELL entry e becomes the word
 // j | q << shift, q indexing a dictionary of the distinct couplings
 // {J (or Jxx), d_x, d_y, d_z} (+ {Jyy, Jzz, 0, 0} for a non-scalar diagonal),
@@ -93,6 +164,7 @@ inline bool build_compact_records(const std::vector<int>& off, const std::vector
    ndict = (int)keys.size();
    dict = A;
    if (!scalar) dict.insert(dict.end(), B.begin(), B.end());
+   if (ndict > 0) bank_order_dictionary(off, shift, scalar, qmax, crec, dict, ndict);
    return ndict > 0;
 }
 
