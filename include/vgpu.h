@@ -291,8 +291,8 @@ int vgpu_llg_pass(vgpu_handle h, int pass);
  * other ranks' atoms that the host refreshes between passes.  noise_base is
  * added to the atom index in the Philox counter: the global index of owned
  * atom 0 when the owned atoms are one contiguous global range, so that the
- * shard draws the noise of the whole system.  Not with Monte Carlo or the
- * device dipole solver. */
+ * shard draws the noise of the whole system.  Call it before vgpu_mc_setup
+ * and vgpu_dipole_setup_shard. */
 int vgpu_set_owned(vgpu_handle h, int32_t n_owned, int64_t noise_base);
 
 /* Halo transfers, queued on the handle's stream (vgpu_get_stream) with
@@ -355,13 +355,42 @@ typedef struct {
  * reference's D2H-CPU-H2D round trip and its O(Nc^2) dense tensors. */
 int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* desc);
 
-/* Recompute cell moments and fields now. */
+/* Recompute cell moments and fields now (on a shard: the partial moments,
+ * as at the dipole cadence). */
 int vgpu_dipole_update(vgpu_handle h);
 
-/* Cell moments [3*num_cells, J/T, x|y|z], B field and mu0 Hd field
- * [3*num_cells, Tesla] of the last update (cells::mag_array_*,
- * dipole::cells_field_array_*, dipole::cells_mu0Hd_field_array_*); any
- * output may be NULL. */
+/* The device dipole solver on a shard (vgpu_set_owned first).  `whole`
+ * describes the whole system of n_global atoms: the cell arrays as for
+ * vgpu_dipole_setup (cells of the whole system, the reference's cells::
+ * arrays after their MPI_Allreduce, src/cells/initialize.cpp:237-242), and
+ * atom_cell (and for the tensor solver atom_x/y/z) of every global atom;
+ * global_type[n_global] are the material ids, local[i] the global id of the
+ * shard's atom i.  The near tensors are built from all global atoms (the
+ * reference exchanges the atoms of neighbouring cells between ranks,
+ * src/dipole/tensor.cpp:63-135).
+ *
+ * At setup and at every update (the cadence in the corrector pass, or
+ * vgpu_dipole_update) the shard sums its OWNED atoms into the cell moments
+ * and stops: the caller adds the moment buffer (vgpu_dipole_moment_buffer)
+ * over all ranks in place -- the reference's MPI_Allreduce of
+ * cells::mag_array (src/cells/mag.cpp:69-74), an NCCL all-reduce here --
+ * and calls vgpu_dipole_finish, which computes the cell fields from the
+ * sums.  While the field is pending the passes, vgpu_get_fields, the
+ * statistics and Monte Carlo return VGPU_ERR_STATE. */
+int vgpu_dipole_setup_shard(vgpu_handle h, const vgpu_dipole_desc* whole, int64_t n_global,
+                            const int32_t* global_type, const int64_t* local);
+
+/* Device buffer of the cell moments [3*num_cells FP64, J/T, x|y|z blocks]
+ * (stream-ordered on vgpu_get_stream); *count = 3*num_cells. */
+int vgpu_dipole_moment_buffer(vgpu_handle h, double** dev, int64_t* count);
+
+/* *pending = 1 while a shard's cell moments await vgpu_dipole_finish. */
+int vgpu_dipole_pending(vgpu_handle h, int32_t* pending);
+
+/* Cell fields from the cell moments in the buffer (after their sum over
+ * ranks); clears the pending state. */
+int vgpu_dipole_finish(vgpu_handle h);
+
 /* Far-field method chosen by vgpu_dipole_setup: VGPU_DIPOLE_FAR_DIRECT (tiled
  * all-pairs sum, FP32 terms) or VGPU_DIPOLE_FAR_FFT (FP64 FFT convolution on
  * the cell grid).  No reference counterpart: the reference stores dense
@@ -370,6 +399,10 @@ int vgpu_dipole_update(vgpu_handle h);
 #define VGPU_DIPOLE_FAR_FFT 1
 int vgpu_dipole_method(vgpu_handle h, int32_t* method);
 
+/* Cell moments [3*num_cells, J/T, x|y|z], B field and mu0 Hd field
+ * [3*num_cells, Tesla] of the last update (cells::mag_array_*,
+ * dipole::cells_field_array_*, dipole::cells_mu0Hd_field_array_*); any
+ * output may be NULL. */
 int vgpu_dipole_get_cells(vgpu_handle h, double* mag, double* b_field, double* hd_field);
 
 /* Host-computed per-atom dipole B field (and mu0 Hd field for energies; NULL

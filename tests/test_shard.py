@@ -246,3 +246,53 @@ def test_combined_magnetization_equals_whole_system():
             np.add.at(parts[:, q], lm[o], lmu[o] * loc.spins[q][o])
         np.add.at(parts[:, 3], lm[o], lmu[o])
     np.testing.assert_allclose(SH.combine_magnetization(parts), SH.combine_magnetization(whole), rtol=1e-13)
+
+
+def _dipole_rank_main(rank, world, port, out_dir):
+    import torch
+    import torch.distributed as dist
+    from oracle import dipole_ref as D
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        s = _fcc()
+        cells = S.dipole_cells(s, size=2 * 3.54, atomic_volume=3.54 ** 3 / 4, solver="tensor", update_rate=1)
+        plan = SH.make_plan(s, world)[rank]
+        nc = cells["cell_natoms"].size
+        own = plan.owned
+        part = D.cell_moments(s.spins[:, own], s.materials["mu_s_SI"][s.type[own]], cells["atom_cell"][own], nc)
+        buf = torch.from_numpy(np.ascontiguousarray(part).ravel())
+        SH.sum_cell_moments(buf)
+        np.save(os.path.join(out_dir, f"mag{rank}.npy"), buf.numpy().reshape(3, nc))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_sharded_cell_moments_equal_whole_system(tmp_path, world):
+    """Macrocell moments on shards: every rank sums its owned atoms, one
+    all-reduce adds the partial moments (cells::mag's MPI_Allreduce), and
+    every rank holds the whole system's moments -- equal to the whole-system
+    sum up to the order of the additions -- and so the same cell fields."""
+    import torch.multiprocessing as mp
+    from oracle import dipole_ref as D
+    mp.start_processes(_dipole_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    s = _fcc()
+    c = S.dipole_cells(s, size=2 * 3.54, atomic_volume=3.54 ** 3 / 4, solver="tensor", update_rate=1)
+    nc = c["cell_natoms"].size
+    whole = D.cell_moments(s.spins, s.materials["mu_s_SI"][s.type], c["atom_cell"], nc)
+    T = D.tensors(c["cell_pos_mom"], c["cell_natoms"], c["macro_cell_size"], c["cutoff"], "tensor", s.coords,
+                  c["atom_cell"])
+    B0, H0 = D.cell_fields(whole, T, c["cell_natoms"], c["cell_volume"])
+    scale = np.abs(whole).max()
+    assert scale > 0
+    for r in range(world):
+        mag = np.load(tmp_path / f"mag{r}.npy")
+        assert np.abs(mag - whole).max() <= 1e-14 * scale
+        B, H = D.cell_fields(mag, T, c["cell_natoms"], c["cell_volume"])
+        assert np.abs(B - B0).max() <= 1e-13 * np.abs(B0).max()
+        assert np.abs(H - H0).max() <= 1e-13 * np.abs(H0).max()

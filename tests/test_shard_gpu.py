@@ -153,3 +153,79 @@ def test_mc_shards_equal_whole_system(vgpu_lib, prec, nranks):
     finally:
         for sim in sims:
             sim.close()
+
+
+def _sum_moments(torch, sims):
+    """Host stand-in for the all-reduce of the shards' cell moments: add the
+    device buffers of every shard and write the sum back into each."""
+    bufs = [sim.dipole_moment_tensor() for sim in sims]
+    for sim in sims:
+        sim.synchronize()
+    total = torch.stack(bufs).sum(0)
+    for b in bufs:
+        b.copy_(total)
+    torch.cuda.synchronize()
+    for sim in sims:
+        sim.dipole_finish()
+
+
+@pytest.mark.parametrize("solver", ["tensor", "macrocell"])
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("nranks", [2, 3])
+def test_dipole_shards_equal_whole_system(vgpu_lib, solver, prec, nranks):
+    """The macrocell dipole field on shards: each shard sums its owned atoms
+    into the cell moments, the host adds them over shards, and the cell fields
+    and the trajectory across dipole updates equal the whole system's (up to
+    the order of the moment additions).  A pass while the field awaits the sum
+    is refused."""
+    import torch
+    from vampire_b200 import vgpu as V
+    s = S.config_fcc_tensor(L=6, seed=3)
+    cells = S.dipole_cells(s, size=2 * 3.54, atomic_volume=3.54 ** 3 / 4, solver=solver, update_rate=4)
+    plans = SH.make_plan(s, nranks)
+    dtype = torch.float32 if prec == "fp32" else torch.float64
+    steps = 10
+    with V.Simulation(s, precision=prec, noise_seed=5) as whole:
+        whole.dipole_setup(cells)
+        m0, b0, h0 = whole.dipole_cells()
+        whole.llg_heun(steps)
+        ref = whole.spins()
+        m1, b1, _ = whole.dipole_cells()
+    assert np.abs(b0).max() > 0
+    sims = []
+    try:
+        for p in plans:
+            sim = V.Simulation(SH.local_system(s, p), precision=prec, noise_seed=5)
+            sim.set_owned(p.n_owned, p.noise_base)
+            sim.dipole_setup_shard(cells, s.type, np.concatenate([p.owned, p.halo]))
+            assert sim.dipole_pending()
+            sims.append(sim)
+        with pytest.raises(V.VGPUError) as e:
+            sims[0].llg_pass(V.PASS_PREDICTOR)
+        assert e.value.code == V.ERR_STATE
+        _sum_moments(torch, sims)
+        for sim in sims:
+            assert not sim.dipole_pending()
+            m, b, h = sim.dipole_cells()
+            assert np.abs(m - m0).max() <= 1e-14 * np.abs(m0).max()
+            assert np.abs(b - b0).max() <= 1e-6 * np.abs(b0).max()
+            assert np.abs(h - h0).max() <= 1e-6 * np.abs(h0).max()
+        refresh = _refresher(torch, plans, sims, dtype)
+        for _ in range(steps):
+            for sim in sims:
+                sim.llg_pass(V.PASS_PREDICTOR)
+            refresh(V.STATE_PREDICTOR)
+            for sim in sims:
+                sim.llg_pass(V.PASS_CORRECTOR)
+            refresh(V.STATE_SPIN)
+            if sims[0].dipole_pending():
+                _sum_moments(torch, sims)
+        got = np.zeros_like(ref)
+        for sim, p in zip(sims, plans):
+            got[:, p.owned] = sim.spins()[:, :p.n_owned]
+            _, b, _ = sim.dipole_cells()
+            assert np.abs(b - b1).max() <= 1e-5 * np.abs(b1).max()
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-5 if prec == "fp32" else 1e-11)
+    finally:
+        for sim in sims:
+            sim.close()

@@ -21,6 +21,12 @@
 // T_ij m_j - 0.5 (8 pi / 3 V_i) m_i), as update.cpp:56-99.  Atoms read their
 // cell's field through the cell id in the fused LLG passes; atoms of
 // non-magnetic materials and of empty cells read a zero row.
+//
+// On a shard (vgpu_set_owned) K5 sums the shard's owned atoms only and the
+// update stops there: the host adds the partial cell moments over ranks in
+// the device buffer (the reference's MPI_Allreduce of cells::mag_array,
+// src/cells/mag.cpp:69-74) and vgpu_dipole_finish runs K6 on the sums.  Until
+// then the passes, statistics and Monte Carlo refuse to run.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -55,6 +61,8 @@ struct DipoleState {
    int* atom_cell = nullptr;    // [n] cell id or nc (zero row)
    FFTField* fft = nullptr;     // far field by FFT convolution (regular cell grids), or direct sum
    std::vector<double> mus_host;
+   bool shard = false;          // K5 sums owned atoms; the field waits for the sum over ranks
+   bool pending = false;        // partial moments in `mag`, field not yet computed
 };
 
 static DipoleState* dip_of(vgpu_ctx* h) { return (DipoleState*)h->extras[2]; }
@@ -88,6 +96,14 @@ __global__ void cell_moment_kernel(int nc, const int* __restrict__ start, const 
       const double imuB = 1.0 / 9.27400915e-24;
       mom[warp] = make_float4((float)(mx * imuB), (float)(my * imuB), (float)(mz * imuB), 0.f);
    }
+}
+
+// moments in mu_B for K6 from the cell moments summed over ranks
+__global__ void cell_mom_kernel(int nc, const double* __restrict__ mag, float4* __restrict__ mom) {
+   const int c = blockIdx.x * blockDim.x + threadIdx.x;
+   if (c >= nc) return;
+   const double imuB = 1.0 / 9.27400915e-24;
+   mom[c] = make_float4((float)(mag[c] * imuB), (float)(mag[nc + c] * imuB), (float)(mag[2 * nc + c] * imuB), 0.f);
 }
 
 // K6: far field by tiled all-pairs sum (FP32 terms, FP64 across tiles).
@@ -270,8 +286,9 @@ void dipole_destroy(vgpu_ctx* h) {
    h->extras[2] = nullptr;
 }
 
+// K5 over the moment list (all magnetic atoms, or a shard's owned ones)
 template <typename R>
-static int dipole_update_typed(vgpu_ctx* h) {
+static int dipole_moments_typed(vgpu_ctx* h) {
    DipoleState* d = dip_of(h);
    SysDev& S = h->sys;
    const int nc = d->nc;
@@ -279,7 +296,23 @@ static int dipole_update_typed(vgpu_ctx* h) {
    cell_moment_kernel<R><<<(nc * 32 + 255) / 256, 256, 0, h->stream>>>(
        nc, d->cell_start, d->cell_atoms, (const R*)S.s[0], (const R*)S.s[1], (const R*)S.s[2], (const int*)S.mat,
        (const MatParams<R>*)S.mp, S.mus_SI, d->mag, d->pos, d->mom);
-   int launches = 2;  // moments and finish, plus the far field below
+   h->prof_end(PROF_DIPOLE);
+   h->kernel_launches += 1;
+   return cuda_err(h, cudaGetLastError(), "dipole cell moments");
+}
+
+// K6 and the finish from the cell moments in d->mag; with_mom: first convert
+// them to mu_B (moments summed over ranks)
+template <typename R>
+static int dipole_field_typed(vgpu_ctx* h, bool with_mom) {
+   DipoleState* d = dip_of(h);
+   const int nc = d->nc;
+   h->prof_begin(PROF_DIPOLE);
+   int launches = 1;  // the finish, plus the far field below
+   if (with_mom && !d->fft) {
+      cell_mom_kernel<<<(nc + 255) / 256, 256, 0, h->stream>>>(nc, d->mag, d->mom);
+      launches += 1;
+   }
    if (d->fft) {
       cudaError_t e = fft_field_apply(d->fft, d->mag, d->field, h->stream, &launches);
       if (e != cudaSuccess) {
@@ -301,16 +334,43 @@ static int dipole_update_typed(vgpu_ctx* h) {
        (R*)d->table_hd);
    h->prof_end(PROF_DIPOLE);
    h->kernel_launches += launches;
-   return cuda_err(h, cudaGetLastError(), "dipole update");
+   return cuda_err(h, cudaGetLastError(), "dipole field");
+}
+
+// whole system: moments and field; shard: partial moments, field pending
+template <typename R>
+static int dipole_update_typed(vgpu_ctx* h) {
+   DipoleState* d = dip_of(h);
+   int rc = dipole_moments_typed<R>(h);
+   if (rc) return rc;
+   if (d->shard) {
+      d->pending = true;
+      return VGPU_OK;
+   }
+   return dipole_field_typed<R>(h, false);
 }
 
 int dipole_update(vgpu_ctx* h) {
    return h->prec == VGPU_PREC_FP64 ? dipole_update_typed<double>(h) : dipole_update_typed<float>(h);
 }
 
+static int dipole_finish(vgpu_ctx* h) {
+   int rc = h->prec == VGPU_PREC_FP64 ? dipole_field_typed<double>(h, true) : dipole_field_typed<float>(h, true);
+   if (!rc) dip_of(h)->pending = false;
+   return rc;
+}
+
 }  // namespace vgpu
 
 using namespace vgpu;
+
+int dipole_ready(vgpu_ctx* h) {
+   DipoleState* d = dip_of(h);
+   if (d && d->pending)
+      return set_err(h, VGPU_ERR_STATE,
+                     "dipole cell moments of this shard await their sum over ranks and vgpu_dipole_finish");
+   return VGPU_OK;
+}
 
 int dipole_after_step(vgpu_ctx* h) {
    DipoleState* d = dip_of(h);
@@ -319,24 +379,39 @@ int dipole_after_step(vgpu_ctx* h) {
    return dipole_update(h);
 }
 
-extern "C" int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* dd) {
-   if (!h || !dd) return set_err(h, VGPU_ERR_ARG, "null argument");
+// Builds the solver from a descriptor of ng atoms (the whole system) with
+// material ids gtype; local[i] is the descriptor atom of the handle's atom i
+// (nullptr: the handle holds all ng atoms in descriptor order).  Cell moments
+// sum the handle's updated atoms; the near tensors use every atom of the
+// descriptor, so a shard's near field is the whole system's.
+static int dipole_build(vgpu_ctx* h, const vgpu_dipole_desc* dd, int ng, const int* gtype, const int64_t* local) {
    SysDev& S = h->sys;
-   if (!S.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
-   if (S.n_owned < S.n) return set_err(h, VGPU_ERR_STATE, "the dipole solver runs on whole systems (handle holds a shard)");
    const int n = S.n, nc = dd->num_cells;
    if (nc <= 0 || !dd->atom_cell || !dd->cell_pos_mom || !dd->cell_volume || !dd->cell_natoms)
       return set_err(h, VGPU_ERR_ARG, "incomplete dipole descriptor");
    if (dd->solver == VGPU_DIPOLE_TENSOR && (!dd->atom_x || !dd->atom_y || !dd->atom_z))
       return set_err(h, VGPU_ERR_ARG, "tensor solver needs atom coordinates");
    if (!(dd->macro_cell_size > 0.0)) return set_err(h, VGPU_ERR_ARG, "macro_cell_size must be positive");
-   for (int i = 0; i < n; ++i)
-      if (dd->atom_cell[i] < 0 || dd->atom_cell[i] >= nc)
-         return set_err(h, VGPU_ERR_ARG, "atom %d has cell %d outside 0..%d", i, dd->atom_cell[i], nc - 1);
+   for (int g = 0; g < ng; ++g) {
+      if (dd->atom_cell[g] < 0 || dd->atom_cell[g] >= nc)
+         return set_err(h, VGPU_ERR_ARG, "atom %d has cell %d outside 0..%d", g, dd->atom_cell[g], nc - 1);
+      if (gtype[g] < 0 || gtype[g] >= S.M)
+         return set_err(h, VGPU_ERR_ARG, "atom %d has material %d outside 0..%d", g, gtype[g], S.M - 1);
+   }
+   if (local)
+      for (int i = 0; i < n; ++i) {
+         if (local[i] < 0 || local[i] >= ng)
+            return set_err(h, VGPU_ERR_ARG, "local atom %d maps to %lld outside 0..%d", i, (long long)local[i], ng - 1);
+         if (gtype[local[i]] != S.type_host[i])
+            return set_err(h, VGPU_ERR_ARG, "local atom %d: material %d, whole-system atom %lld: material %d", i,
+                           S.type_host[i], (long long)local[i], gtype[local[i]]);
+      }
+   auto gid = [&](int i) { return local ? (int)local[i] : i; };
    cudaSetDevice(h->device);
    dipole_destroy(h);
    DipoleState* d = new DipoleState();
    h->extras[2] = d;
+   d->shard = local != nullptr;
    d->nc = nc;
    d->solver = dd->solver;
    d->update_rate = dd->update_rate;
@@ -349,21 +424,29 @@ extern "C" int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* dd) {
       mus[m] = S.materials[m].mu_s_SI;
       magnetic[m] = S.materials[m].non_magnetic == 0;
    }
-   // cell-sorted atom list of magnetic atoms (cells::mag skips non-magnetic ones)
-   std::vector<int> start(nc + 1, 0), atoms;
-   std::vector<int> acell(n);
-   for (int i = 0; i < n; ++i)
-      if (magnetic[S.type_host[i]]) start[dd->atom_cell[i] + 1]++;
-   for (int c = 0; c < nc; ++c) start[c + 1] += start[c];
-   atoms.resize(start[nc]);
-   {
+   // cell-sorted lists of magnetic atoms (cells::mag skips non-magnetic
+   // ones): the handle's updated atoms for the moments, every descriptor atom
+   // for the near tensors (the same list on a whole system)
+   auto cell_sort = [&](int count, auto cell_of, auto type_of, std::vector<int>& start, std::vector<int>& atoms) {
+      start.assign(nc + 1, 0);
+      for (int i = 0; i < count; ++i)
+         if (magnetic[type_of(i)]) start[cell_of(i) + 1]++;
+      for (int c = 0; c < nc; ++c) start[c + 1] += start[c];
+      atoms.resize(start[nc]);
       std::vector<int> fill(start.begin(), start.end() - 1);
-      for (int i = 0; i < n; ++i)
-         if (magnetic[S.type_host[i]]) atoms[fill[dd->atom_cell[i]]++] = i;
-   }
+      for (int i = 0; i < count; ++i)
+         if (magnetic[type_of(i)]) atoms[fill[cell_of(i)]++] = i;
+   };
+   std::vector<int> start, atoms, gstart, gatoms;
+   cell_sort(local ? S.n_owned : n, [&](int i) { return dd->atom_cell[gid(i)]; },
+             [&](int i) { return S.type_host[i]; }, start, atoms);
+   if (local) cell_sort(ng, [&](int g) { return dd->atom_cell[g]; }, [&](int g) { return gtype[g]; }, gstart, gatoms);
+   const std::vector<int>& nstart_atoms = local ? gstart : start;
+   const std::vector<int>& natoms_list = local ? gatoms : atoms;
    // atoms read the zero row when their cell is empty or they are non-magnetic
+   std::vector<int> acell(n);
    for (int i = 0; i < n; ++i) {
-      const int c = dd->atom_cell[i];
+      const int c = dd->atom_cell[gid(i)];
       acell[i] = (dd->cell_natoms[c] > 0 && magnetic[S.type_host[i]]) ? c : nc;
    }
    std::vector<float4> pos(nc);
@@ -454,13 +537,16 @@ extern "C" int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* dd) {
    if (e == cudaSuccess && d->npairs > 0) {
       up((void**)&d->near_start, nstart.data(), sizeof(int) * (nc + 1));
       up((void**)&d->near_j, pj.data(), sizeof(int) * pj.size());
-      int *dpi = nullptr, *dpj = nullptr;
+      int *dpi = nullptr, *dpj = nullptr, *gs = nullptr;
       double *ax = nullptr, *ay = nullptr, *az = nullptr, *cp = nullptr;
       // coordinates in cell-sorted order for the near-tensor kernel
-      std::vector<double> cx(atoms.size()), cy(atoms.size()), cz(atoms.size());
-      for (size_t k = 0; k < atoms.size(); ++k) {
-         cx[k] = dd->atom_x[atoms[k]]; cy[k] = dd->atom_y[atoms[k]]; cz[k] = dd->atom_z[atoms[k]];
+      const size_t na = natoms_list.size();
+      std::vector<double> cx(na), cy(na), cz(na);
+      for (size_t k = 0; k < na; ++k) {
+         const int g = local ? natoms_list[k] : gid(natoms_list[k]);
+         cx[k] = dd->atom_x[g]; cy[k] = dd->atom_y[g]; cz[k] = dd->atom_z[g];
       }
+      if (local) up((void**)&gs, nstart_atoms.data(), sizeof(int) * (nc + 1));
       up((void**)&dpi, pi.data(), sizeof(int) * pi.size());
       up((void**)&dpj, pj.data(), sizeof(int) * pj.size());
       up((void**)&ax, cx.data(), sizeof(double) * cx.size());
@@ -469,12 +555,12 @@ extern "C" int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* dd) {
       up((void**)&cp, dd->cell_pos_mom, sizeof(double) * 4 * nc);
       if (e == cudaSuccess) e = cudaMalloc(&d->near_t, sizeof(double) * 6 * d->npairs);
       if (e == cudaSuccess) {
-         near_tensor_kernel<<<d->npairs, 256, 0, h->stream>>>(d->npairs, dpi, dpj, d->cell_start, ax, ay, az, cp,
-                                                               d->fft != nullptr, d->near_t);
+         near_tensor_kernel<<<d->npairs, 256, 0, h->stream>>>(d->npairs, dpi, dpj, local ? gs : d->cell_start, ax,
+                                                               ay, az, cp, d->fft != nullptr, d->near_t);
          e = cudaGetLastError();
       }
       if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-      cudaFree(dpi); cudaFree(dpj); cudaFree(ax); cudaFree(ay); cudaFree(az); cudaFree(cp);
+      cudaFree(dpi); cudaFree(dpj); cudaFree(gs); cudaFree(ax); cudaFree(ay); cudaFree(az); cudaFree(cp);
    }
    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
    if (e != cudaSuccess) {
@@ -486,8 +572,51 @@ extern "C" int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* dd) {
    S.cell = d->atom_cell;
    S.cell_field = d->table_b;
    S.cell_hd = d->table_hd;
-   // field at the current spins (dipole::initialize calls calculate_field(0))
+   // field at the current spins (dipole::initialize calls calculate_field(0));
+   // on a shard the partial moments, the field once they are summed
    return dipole_update(h);
+}
+
+extern "C" int vgpu_dipole_setup(vgpu_handle h, const vgpu_dipole_desc* dd) {
+   if (!h || !dd) return set_err(h, VGPU_ERR_ARG, "null argument");
+   SysDev& S = h->sys;
+   if (!S.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (S.n_owned < S.n)
+      return set_err(h, VGPU_ERR_STATE, "the handle holds a shard: set the dipole solver up with vgpu_dipole_setup_shard");
+   return dipole_build(h, dd, S.n, S.type_host.data(), nullptr);
+}
+
+extern "C" int vgpu_dipole_setup_shard(vgpu_handle h, const vgpu_dipole_desc* whole, int64_t n_global,
+                                       const int32_t* global_type, const int64_t* local) {
+   if (!h || !whole || !global_type || !local) return set_err(h, VGPU_ERR_ARG, "null argument");
+   SysDev& S = h->sys;
+   if (!S.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (n_global < S.n || n_global > INT32_MAX) return set_err(h, VGPU_ERR_ARG, "n_global %lld below the shard's %d atoms or too large", (long long)n_global, S.n);
+   return dipole_build(h, whole, (int)n_global, global_type, local);
+}
+
+extern "C" int vgpu_dipole_moment_buffer(vgpu_handle h, double** dev, int64_t* count) {
+   if (!h || !dev || !count) return set_err(h, VGPU_ERR_ARG, "null argument");
+   DipoleState* d = dip_of(h);
+   if (!d) return set_err(h, VGPU_ERR_STATE, "vgpu_dipole_setup not called");
+   *dev = d->mag;
+   *count = 3 * (int64_t)d->nc;
+   return VGPU_OK;
+}
+
+extern "C" int vgpu_dipole_pending(vgpu_handle h, int32_t* pending) {
+   if (!h || !pending) return set_err(h, VGPU_ERR_ARG, "null argument");
+   DipoleState* d = dip_of(h);
+   *pending = d && d->pending ? 1 : 0;
+   return VGPU_OK;
+}
+
+extern "C" int vgpu_dipole_finish(vgpu_handle h) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   DipoleState* d = dip_of(h);
+   if (!d) return set_err(h, VGPU_ERR_STATE, "vgpu_dipole_setup not called");
+   cudaSetDevice(h->device);
+   return dipole_finish(h);
 }
 
 extern "C" int vgpu_dipole_update(vgpu_handle h) {

@@ -379,6 +379,7 @@ extern "C" int vgpu_mc_sweep(vgpu_handle h, uint64_t n_sweeps) {
    MCState* s = mc_of(h);
    if (!s) return set_err(h, VGPU_ERR_STATE, "vgpu_mc_setup not called");
    if (!(h->params.temperature >= 0.0)) return set_err(h, VGPU_ERR_STATE, "vgpu_set_params not called");
+   if (int rc = h->fields_ready()) return rc;
    if (s->next_colour != 0)
       return set_err(h, VGPU_ERR_STATE, "a sweep run colour by colour (vgpu_mc_colour) is unfinished");
    cudaSetDevice(h->device);
@@ -391,6 +392,7 @@ extern "C" int vgpu_mc_colour(vgpu_handle h, int32_t colour) {
    MCState* s = mc_of(h);
    if (!s) return set_err(h, VGPU_ERR_STATE, "vgpu_mc_setup not called");
    if (!(h->params.temperature >= 0.0)) return set_err(h, VGPU_ERR_STATE, "vgpu_set_params not called");
+   if (int rc = h->fields_ready()) return rc;
    if (colour != s->next_colour)
       return set_err(h, VGPU_ERR_ARG, "colour %d out of order: the current sweep runs colour %d next (of %d)", colour,
                      s->next_colour, s->ncolours);

@@ -473,6 +473,7 @@ extern "C" int vgpu_stats_update(vgpu_handle h, int32_t flags) {
    if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
    if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
    if (!stats_of(h) || stats_of(h)->masks.empty()) return set_err(h, VGPU_ERR_STATE, "no statistics mask registered");
+   if (int rc = h->fields_ready()) return rc;
    cudaSetDevice(h->device);
    h->prof_begin(PROF_STATS);
    int rc = h->prec == VGPU_PREC_FP64 ? stats_update_typed<double>(h, flags) : stats_update_typed<float>(h, flags);

@@ -7,8 +7,10 @@
 using namespace vgpu;
 
 int dipole_after_step(vgpu_ctx* h);
+int dipole_ready(vgpu_ctx* h);
 
 int vgpu_ctx::after_step() { return dipole_after_step(this); }
+int vgpu_ctx::fields_ready() { return dipole_ready(this); }
 
 void vgpu_ctx::destroy_extras() {
    stats_destroy(this);

@@ -612,7 +612,8 @@ static int llg_steps_typed(vgpu_ctx* h, uint64_t n_steps, int integrator = INTEG
    bool staged = false;
    int rc = prepare_passes<R>(h, &staged, integrator);
    for (uint64_t t = 0; t < n_steps && !rc; ++t) {
-      rc = run_pass<R>(h, PASS_PREDICTOR, staged, integrator);
+      rc = h->fields_ready();
+      if (!rc) rc = run_pass<R>(h, PASS_PREDICTOR, staged, integrator);
       if (!rc) rc = run_pass<R>(h, PASS_CORRECTOR, staged, integrator);
    }
    return rc;
@@ -621,7 +622,8 @@ static int llg_steps_typed(vgpu_ctx* h, uint64_t n_steps, int integrator = INTEG
 template <typename R>
 static int llg_pass_typed(vgpu_ctx* h, int mode) {
    bool staged = false;
-   int rc = prepare_passes<R>(h, &staged);
+   int rc = h->fields_ready();
+   if (!rc) rc = prepare_passes<R>(h, &staged);
    return rc ? rc : run_pass<R>(h, mode, staged);
 }
 
@@ -1083,6 +1085,7 @@ static int fields_typed(vgpu_handle h, double* hx, double* hy, double* hz) {
 extern "C" int vgpu_get_fields(vgpu_handle h, double* hx, double* hy, double* hz) {
    if (!h || !hx || !hy || !hz) return set_err(h, VGPU_ERR_ARG, "null argument");
    if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (int rc = h->fields_ready()) return rc;
    cudaSetDevice(h->device);
    return h->prec == VGPU_PREC_FP64 ? fields_typed<double>(h, hx, hy, hz) : fields_typed<float>(h, hx, hy, hz);
 }
@@ -1135,7 +1138,8 @@ extern "C" int vgpu_set_owned(vgpu_handle h, int32_t n_owned, int64_t noise_base
       return set_err(h, VGPU_ERR_ARG, "noise_base out of the 32-bit atom counter range");
    if (n_owned < S.n && S.bq_off)
       return set_err(h, VGPU_ERR_STATE, "shards carry no biquadratic exchange list");
-   if (n_owned < S.n && h->extras[2]) return set_err(h, VGPU_ERR_STATE, "the dipole solver runs on whole systems only");
+   if (h->extras[2] && n_owned != S.n_owned)
+      return set_err(h, VGPU_ERR_STATE, "the dipole solver is set up: call vgpu_set_owned before vgpu_dipole_setup_shard");
    if (h->extras[1] && n_owned != S.n_owned)
       return set_err(h, VGPU_ERR_STATE, "Monte Carlo colour lists are set up: call vgpu_set_owned before vgpu_mc_setup");
    S.n_owned = n_owned;

@@ -130,6 +130,7 @@ struct vgpu_ctx {
    void update_sigma_flag();
    // hooks implemented by the other subsystems
    int after_step();          // dipole cadence (dipole.cu)
+   int fields_ready();        // VGPU_OK, or an error while a shard's dipole field awaits its moment sum
    void destroy_extras();     // free subsystem state (stats, mc, dipole)
    void* extras[8] = {nullptr};
 

@@ -28,6 +28,12 @@ The same decomposition here, one process per GPU over NVLink/NCCL:
 Statistics combine across ranks from the raw per-bin sums of each shard
 (``vgpu_stats_get_sums``) with one all-reduce.
 
+The macrocell dipole field shards as the reference's does: every rank sums
+its owned atoms into the cell moments, one all-reduce adds them over ranks
+(cells::mag's MPI_Allreduce, src/cells/mag.cpp:69-74), and every rank then
+computes the cell fields from the sums (``sum_cell_moments``,
+``ShardedSimulation.dipole_setup``).
+
 Monte Carlo shards the same way.  A colour-ordered Metropolis sweep updates
 one colour at a time; a shard runs its owned atoms of a colour, then every
 rank refreshes its halo spins before the next colour (``mc_sweep_sharded``),
@@ -213,6 +219,14 @@ def local_colours(colour: np.ndarray, plan: ShardPlan) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(colour)[np.concatenate([plan.owned, plan.halo])], dtype=np.int32)
 
 
+def sum_cell_moments(buf, group=None) -> None:
+    """Adds a shard's partial cell moments (a tensor of 3*ncells FP64, the
+    owned atoms' sums) over all ranks in place: CPU tensors over gloo, the
+    library's device buffer over NCCL."""
+    import torch.distributed as dist
+    dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=group)
+
+
 def combine_magnetization(sums: np.ndarray) -> np.ndarray:
     """Reference normalisation (src/statistics/magnetization.cpp:134-180) of
     raw per-bin sums [bins, >=4] = (sum mu sx, sum mu sy, sum mu sz, sum mu)
@@ -246,7 +260,10 @@ class ShardedSimulation:
         self.stream = torch.cuda.ExternalStream(self.sim.stream_ptr(), device=self.device)
         self.idx = {p: torch.as_tensor(ix, dtype=torch.int32, device=self.device) for p, ix in plan.send.items()}
         self.halo = HaloExchange(plan, group)
+        self.group = group
         self._torch = torch
+        self._global_type = np.ascontiguousarray(s.type, dtype=np.int32)
+        self._moments = None
 
     def _refresh(self, which: int) -> None:
         torch = self._torch
@@ -266,6 +283,22 @@ class ShardedSimulation:
         with torch.cuda.stream(self.stream):
             self.halo.exchange(pack, unpack, alloc)
 
+    def dipole_setup(self, cells: dict) -> None:
+        """The device dipole solver on this shard from the whole system's
+        macrocells (system.dipole_cells of the whole system); every rank calls
+        it, and the fields come from the moments summed over ranks."""
+        self.sim.dipole_setup_shard(cells, self._global_type, np.concatenate([self.plan.owned, self.plan.halo]))
+        self._moments = self.sim.dipole_moment_tensor()
+        self._dipole_sum()
+
+    def _dipole_sum(self) -> None:
+        # every rank reaches the dipole cadence at the same step
+        if self._moments is None or not self.sim.dipole_pending():
+            return
+        with self._torch.cuda.stream(self.stream):
+            sum_cell_moments(self._moments, self.group)
+        self.sim.dipole_finish()
+
     def step(self, n_steps: int = 1) -> None:
         from . import vgpu
         for _ in range(n_steps):
@@ -273,6 +306,7 @@ class ShardedSimulation:
             self._refresh(vgpu.STATE_PREDICTOR)
             self.sim.llg_pass(vgpu.PASS_CORRECTOR)
             self._refresh(vgpu.STATE_SPIN)
+            self._dipole_sum()
 
     def mc_setup(self, colour: np.ndarray) -> int:
         """Monte Carlo on this shard with the whole system's colouring

@@ -204,6 +204,7 @@ class Simulation:
                  noise_seed: int = 0):
         self.system = system
         self.n = system.n
+        self.device = device
         self._h = C.c_void_p()
         prec = PREC_FP64 if precision == "fp64" else PREC_FP32
         check(lib().vgpu_create(device, prec, C.byref(self._h)))
@@ -383,11 +384,8 @@ class Simulation:
         return out
 
     # -- dipole field --------------------------------------------------------
-    def dipole_setup(self, cells: dict) -> None:
-        """cells: atom_cell, cell_pos_mom, cell_volume, cell_natoms,
-        macro_cell_size, cutoff, update_rate, solver ('tensor'|'macrocell'),
-        coords (3, n) for the tensor solver (the reference's cells:: data)."""
-        keep = {}
+    @staticmethod
+    def _dipole_desc(cells: dict, keep: dict) -> "DipoleDesc":
 
         def arr(name, a, dt):
             a = np.ascontiguousarray(a, dtype=dt)
@@ -407,8 +405,56 @@ class Simulation:
         if "coords" in cells and cells["coords"] is not None:
             c = arr("xyz", cells["coords"], np.float64)
             d.atom_x, d.atom_y, d.atom_z = _ptr(c[0], _D), _ptr(c[1], _D), _ptr(c[2], _D)
+        return d
+
+    def dipole_setup(self, cells: dict) -> None:
+        """cells: atom_cell, cell_pos_mom, cell_volume, cell_natoms,
+        macro_cell_size, cutoff, update_rate, solver ('tensor'|'macrocell'),
+        coords (3, n) for the tensor solver (the reference's cells:: data)."""
+        keep = {}
+        d = self._dipole_desc(cells, keep)
         self._ncells = d.num_cells
         self._check(lib().vgpu_dipole_setup(self._h, C.byref(d)))
+
+    def dipole_setup_shard(self, whole_cells: dict, global_type: np.ndarray, local_ids: np.ndarray) -> None:
+        """The dipole solver on a shard (vgpu_dipole_setup_shard): whole_cells
+        are the whole system's cells (dipole_setup's keys; atom_cell and
+        coords of every global atom), global_type the material id of every
+        global atom, local_ids the global id of each of the shard's atoms.
+        The field then waits for the moment sum over ranks (dipole_finish)."""
+        keep = {}
+        d = self._dipole_desc(whole_cells, keep)
+        gt = np.ascontiguousarray(global_type, dtype=np.int32)
+        loc = np.ascontiguousarray(local_ids, dtype=np.int64)
+        self._ncells = d.num_cells
+        self._check(lib().vgpu_dipole_setup_shard(self._h, C.byref(d), C.c_int64(gt.size), _ptr(gt, _I32),
+                                                  loc.ctypes.data_as(C.POINTER(C.c_int64))))
+
+    def dipole_moment_buffer(self) -> Tuple[int, int]:
+        """(device pointer, count) of the FP64 cell moment buffer (x|y|z blocks)."""
+        p, n = C.POINTER(C.c_double)(), C.c_int64()
+        self._check(lib().vgpu_dipole_moment_buffer(self._h, C.byref(p), C.byref(n)))
+        return C.cast(p, C.c_void_p).value or 0, n.value
+
+    def dipole_moment_tensor(self):
+        """The cell moment buffer as a torch CUDA tensor (no copy), for an
+        in-place all-reduce over ranks."""
+        import torch
+        ptr, count = self.dipole_moment_buffer()
+
+        class _Buf:
+            __cuda_array_interface__ = {"shape": (count,), "typestr": "<f8", "data": (ptr, False),
+                                        "version": 3, "strides": None}
+
+        return torch.as_tensor(_Buf(), device=torch.device("cuda", self.device))
+
+    def dipole_pending(self) -> bool:
+        p = C.c_int32()
+        self._check(lib().vgpu_dipole_pending(self._h, C.byref(p)))
+        return bool(p.value)
+
+    def dipole_finish(self) -> None:
+        self._check(lib().vgpu_dipole_finish(self._h))
 
     def dipole_update(self) -> None:
         self._check(lib().vgpu_dipole_update(self._h))
