@@ -56,6 +56,14 @@ struct DipoleState {
    int* near_j = nullptr;       // [npairs]
    double* near_t = nullptr;    // [6][npairs] T_near - T_bare (xx, xy, xz, yy, yz, zz)
    int npairs = 0;
+   // the near pairs in ELL form for the finish kernel: pair k of cell i at
+   // [k][i] (near_je) and [q][k][i] (near_te, q = xx, xy, xz, yy, yz, zz), so
+   // that a warp of consecutive cells reads consecutive addresses; cells keep
+   // their pairs in the CSR order (sorted by source cell)
+   int maxp = 0;
+   int* near_cnt = nullptr;     // [nc] pairs per cell
+   int* near_je = nullptr;      // [maxp][nc]
+   double* near_te = nullptr;   // [6][maxp][nc]
    void* table_b = nullptr;     // [3][nc+1] R, cell B field for the LLG passes
    void* table_hd = nullptr;    // [3][nc+1] R, cell mu0 Hd field (energies)
    int* atom_cell = nullptr;    // [n] cell id or nc (zero row)
@@ -174,10 +182,21 @@ __global__ void __launch_bounds__(kFieldTile) cell_field_kernel(int nc, const fl
    }
 }
 
+// CSR near pairs -> ELL (one thread per pair)
+__global__ void near_ell_kernel(int npairs, int nc, int maxp, const int* __restrict__ pair_i,
+                                const int* __restrict__ near_start, const int* __restrict__ near_j,
+                                const double* __restrict__ near_t, int* __restrict__ je, double* __restrict__ te) {
+   const int p = blockIdx.x * blockDim.x + threadIdx.x;
+   if (p >= npairs) return;
+   const int i = pair_i[p], k = p - near_start[i];
+   je[(size_t)k * nc + i] = near_j[p];
+   for (int q = 0; q < 6; ++q) te[((size_t)q * maxp + k) * nc + i] = near_t[(size_t)q * npairs + p];
+}
+
 // near-field correction and final scaling (update.cpp:56-99)
 template <typename R>
-__global__ void cell_finish_kernel(int nc, const int* __restrict__ near_start, const int* __restrict__ near_j,
-                                   const double* __restrict__ near_t, int npairs, const double* __restrict__ mag,
+__global__ void cell_finish_kernel(int nc, const int* __restrict__ near_cnt, const int* __restrict__ near_je,
+                                   const double* __restrict__ near_te, int maxp, const double* __restrict__ mag,
                                    const double* __restrict__ self, const float4* __restrict__ pos,
                                    double* __restrict__ field, R* __restrict__ tb, R* __restrict__ thd) {
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -188,12 +207,15 @@ __global__ void cell_finish_kernel(int nc, const int* __restrict__ near_start, c
    }
    const double imuB = 1.0 / 9.27400915e-24;
    double fx = field[i], fy = field[nc + i], fz = field[2 * nc + i];
-   if (near_start) {
-      for (int k = near_start[i]; k < near_start[i + 1]; ++k) {
-         const int j = near_j[k];
+   if (near_cnt) {
+      const size_t qs = (size_t)maxp * nc;
+      const int cnt = near_cnt[i];
+      for (int k = 0; k < cnt; ++k) {
+         const size_t e = (size_t)k * nc + i;
+         const int j = near_je[e];
          const double mx = mag[j] * imuB, my = mag[nc + j] * imuB, mz = mag[2 * nc + j] * imuB;
-         const double txx = near_t[k], txy = near_t[npairs + k], txz = near_t[2 * npairs + k];
-         const double tyy = near_t[3 * npairs + k], tyz = near_t[4 * npairs + k], tzz = near_t[5 * npairs + k];
+         const double txx = near_te[e], txy = near_te[qs + e], txz = near_te[2 * qs + e];
+         const double tyy = near_te[3 * qs + e], tyz = near_te[4 * qs + e], tzz = near_te[5 * qs + e];
          fx += mx * txx + my * txy + mz * txz;
          fy += mx * txy + my * tyy + mz * tyz;
          fz += mx * txz + my * tyz + mz * tzz;
@@ -276,6 +298,7 @@ void dipole_destroy(vgpu_ctx* h) {
    if (!d) return;
    cudaFree(d->cell_start); cudaFree(d->cell_atoms); cudaFree(d->mag); cudaFree(d->pos); cudaFree(d->mom);
    cudaFree(d->field); cudaFree(d->self); cudaFree(d->near_start); cudaFree(d->near_j); cudaFree(d->near_t);
+   cudaFree(d->near_cnt); cudaFree(d->near_je); cudaFree(d->near_te);
    cudaFree(d->table_b); cudaFree(d->table_hd); cudaFree(d->atom_cell);
    fft_field_destroy(d->fft);
    h->sys.cell = nullptr;
@@ -330,7 +353,7 @@ static int dipole_field_typed(vgpu_ctx* h, bool with_mom) {
       launches += 1;
    }
    cell_finish_kernel<R><<<(nc + 1 + 255) / 256, 256, 0, h->stream>>>(
-       nc, d->near_start, d->near_j, d->near_t, d->npairs, d->mag, d->self, d->pos, d->field, (R*)d->table_b,
+       nc, d->near_cnt, d->near_je, d->near_te, d->maxp, d->mag, d->self, d->pos, d->field, (R*)d->table_b,
        (R*)d->table_hd);
    h->prof_end(PROF_DIPOLE);
    h->kernel_launches += launches;
@@ -559,8 +582,28 @@ static int dipole_build(vgpu_ctx* h, const vgpu_dipole_desc* dd, int ng, const i
                                                                ay, az, cp, d->fft != nullptr, d->near_t);
          e = cudaGetLastError();
       }
+      // ELL copy for the finish kernel; the CSR arrays are set-up only
+      std::vector<int> cnt(nc);
+      for (int c = 0; c < nc; ++c) {
+         cnt[c] = nstart[c + 1] - nstart[c];
+         d->maxp = std::max(d->maxp, cnt[c]);
+      }
+      up((void**)&d->near_cnt, cnt.data(), sizeof(int) * nc);
+      if (e == cudaSuccess) e = cudaMalloc(&d->near_je, sizeof(int) * (size_t)d->maxp * nc);
+      if (e == cudaSuccess) e = cudaMemsetAsync(d->near_je, 0, sizeof(int) * (size_t)d->maxp * nc, h->stream);
+      if (e == cudaSuccess) e = cudaMalloc(&d->near_te, sizeof(double) * 6 * (size_t)d->maxp * nc);
+      if (e == cudaSuccess) e = cudaMemsetAsync(d->near_te, 0, sizeof(double) * 6 * (size_t)d->maxp * nc, h->stream);
+      if (e == cudaSuccess) {
+         near_ell_kernel<<<(d->npairs + 255) / 256, 256, 0, h->stream>>>(d->npairs, nc, d->maxp, dpi, d->near_start,
+                                                                          d->near_j, d->near_t, d->near_je,
+                                                                          d->near_te);
+         e = cudaGetLastError();
+      }
       if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
       cudaFree(dpi); cudaFree(dpj); cudaFree(gs); cudaFree(ax); cudaFree(ay); cudaFree(az); cudaFree(cp);
+      cudaFree(d->near_start); cudaFree(d->near_j); cudaFree(d->near_t);
+      d->near_start = d->near_j = nullptr;
+      d->near_t = nullptr;
    }
    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
    if (e != cudaSuccess) {

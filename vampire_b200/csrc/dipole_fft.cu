@@ -11,20 +11,21 @@
 //
 //   scatter  m_j (mu_B) into the G-box of three complex grids (zero at empty
 //            cells of the box)
-//   FFT      each grid along x, y, z (radix-2, one shared-memory tile of lines
+//   FFT      each grid along x and y (radix-2, one shared-memory tile of lines
 //            per block; strided axes load W adjacent x columns per block so
 //            every global access is a W*16-byte segment)
-//   multiply H(k) = T(k) M(k), T symmetric 3x3 (six spectra computed once)
-//   iFFT     along z, y, x, and gather H at the occupied cells (1/P^3 scaling).
+//   z        per z column: forward transform, H(k) = T(k) M(k) (T symmetric
+//            3x3, six spectra computed once), inverse transform, in one kernel
+//   iFFT     along y, x, and gather H at the occupied cells (1/P^3 scaling).
 //
 // The transforms skip the lines that carry only zeros or whose results are not
 // needed: the moments occupy the G-box, so the forward x pass runs only the
 // gy*gz lines of the box (points past gx read as zero), the y pass only the
-// planes z < gz (points past gy read as zero) and the z pass reads zero past
-// gz; the inverse z pass keeps only z < gz, the y pass runs and keeps only
-// those planes' y < gy, the x pass only the box lines' x < gx.  At a 50^3 grid
-// (P = 128) this is about half of the line transforms of the full passes, and
-// the grid needs no clearing.
+// planes z < gz (points past gy read as zero) and the z transform reads zero
+// past gz and keeps only z < gz; the inverse y pass runs and keeps only those
+// planes' y < gy, the inverse x pass only the box lines' x < gx.  At a 50^3
+// grid (P = 128) this is about half of the line transforms of full passes,
+// the spectra never leave shared memory, and the grid needs no clearing.
 //
 // Everything is FP64, so the result equals the direct FP64 sum to rounding
 // (~1e-15 of the field) instead of the FP32 terms of the all-pairs kernel, and
@@ -133,6 +134,77 @@ __global__ void __launch_bounds__(kFFTThreads) fft_strided_kernel(double2* __res
    }
 }
 
+// The middle of the convolution in one pass over z columns: for W adjacent x
+// columns at one y, the three moment components' forward z transforms (points
+// z >= gz read as zero), the product H(k) = T(k) M(k) at every k, and the
+// inverse z transforms, of which z < gz is stored.  The same butterflies and
+// products as separate z passes around multiply_kernel, without writing the
+// spectra to memory and reading them back.
+constexpr int kFuseTile = 3072;  // complex points per block: 3 components x W x pz (48 KB)
+
+__device__ __forceinline__ void tensor_times(const double2* __restrict__ t, size_t np, size_t q, double2 mx,
+                                             double2 my, double2 mz, double2 h[3]) {
+   const double2 xx = t[q], xy = t[np + q], xz = t[2 * np + q];
+   const double2 yy = t[3 * np + q], yz = t[4 * np + q], zz = t[5 * np + q];
+   double2 hx = cmul(xx, mx), hy = cmul(xy, mx), hz = cmul(xz, mx);
+   double2 a = cmul(xy, my), b = cmul(xz, mz);
+   hx.x += a.x + b.x; hx.y += a.y + b.y;
+   a = cmul(yy, my); b = cmul(yz, mz);
+   hy.x += a.x + b.x; hy.y += a.y + b.y;
+   a = cmul(yz, my); b = cmul(zz, mz);
+   hz.x += a.x + b.x; hz.y += a.y + b.y;
+   h[0] = hx; h[1] = hy; h[2] = hz;
+}
+
+__global__ void __launch_bounds__(kFFTThreads) fft_z_multiply_kernel(double2* __restrict__ data,
+                                                                     const double2* __restrict__ t, size_t np, int px,
+                                                                     int py, int n, int logn, int W, int gz,
+                                                                     const double2* __restrict__ tw) {
+   __shared__ double2 s[kFuseTile];
+   const size_t stride = (size_t)px * py;
+   const size_t col0 = (size_t)blockIdx.y * px + (size_t)blockIdx.x * W;  // (x0, y) in the z = 0 plane
+   const int tot = W * n;
+   for (int e = threadIdx.x; e < 3 * tot; e += blockDim.x) {
+      const int c = e / tot, r = e - c * tot;
+      const int p = r / W, w = r - p * W;
+      s[(c * W + w) * n + (int)(__brev((unsigned)p) >> (32 - logn))] =
+          p < gz ? data[(size_t)c * np + col0 + (size_t)p * stride + w] : make_double2(0.0, 0.0);
+   }
+   __syncthreads();
+   fft_smem(s, n, 3 * W, tw, false);
+   // H = T M at every (w, k), all read before any is written back at its
+   // bit-reversed position for the inverse
+   constexpr int kMaxPer = kFuseTile / 3 / kFFTThreads;  // points per thread
+   double2 h[kMaxPer][3];
+#pragma unroll
+   for (int u = 0; u < kMaxPer; ++u) {
+      const int r = threadIdx.x + u * kFFTThreads;
+      if (r < tot) {
+         const int k = r / W, w = r - k * W;
+         tensor_times(t, np, col0 + (size_t)k * stride + w, s[w * n + k], s[(W + w) * n + k], s[(2 * W + w) * n + k],
+                      h[u]);
+      }
+   }
+   __syncthreads();
+#pragma unroll
+   for (int u = 0; u < kMaxPer; ++u) {
+      const int r = threadIdx.x + u * kFFTThreads;
+      if (r < tot) {
+         const int k = r / W, w = r - k * W;
+         const int kr = (int)(__brev((unsigned)k) >> (32 - logn));
+#pragma unroll
+         for (int c = 0; c < 3; ++c) s[(c * W + w) * n + kr] = h[u][c];
+      }
+   }
+   __syncthreads();
+   fft_smem(s, n, 3 * W, tw, true);
+   for (int e = threadIdx.x; e < 3 * tot; e += blockDim.x) {
+      const int c = e / tot, r = e - c * tot;
+      const int p = r / W, w = r - p * W;
+      if (p < gz) data[(size_t)c * np + col0 + (size_t)p * stride + w] = s[(c * W + w) * n + p];
+   }
+}
+
 // bare tensor on the padded grid: offset (dx, dy, dz) cells, zero at the
 // origin and beyond the occupied extent
 __global__ void tensor_grid_kernel(double2* __restrict__ t, size_t np, int px, int py, int pz, int gx, int gy, int gz,
@@ -174,22 +246,6 @@ __global__ void scatter_moments_kernel(int nc, const int* __restrict__ box_cell,
    grid[2 * np + q] = make_double2(c >= 0 ? mag[2 * nc + c] * imuB : 0.0, 0.0);
 }
 
-__global__ void multiply_kernel(double2* __restrict__ g, const double2* __restrict__ t, size_t np) {
-   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < np; q += (size_t)gridDim.x * blockDim.x) {
-      const double2 mx = g[q], my = g[np + q], mz = g[2 * np + q];
-      const double2 xx = t[q], xy = t[np + q], xz = t[2 * np + q];
-      const double2 yy = t[3 * np + q], yz = t[4 * np + q], zz = t[5 * np + q];
-      double2 hx = cmul(xx, mx), hy = cmul(xy, mx), hz = cmul(xz, mx);
-      double2 a = cmul(xy, my), b = cmul(xz, mz);
-      hx.x += a.x + b.x; hx.y += a.y + b.y;
-      a = cmul(yy, my); b = cmul(yz, mz);
-      hy.x += a.x + b.x; hy.y += a.y + b.y;
-      a = cmul(yz, my); b = cmul(zz, mz);
-      hz.x += a.x + b.x; hz.y += a.y + b.y;
-      g[q] = hx; g[np + q] = hy; g[2 * np + q] = hz;
-   }
-}
-
 __global__ void gather_field_kernel(int nc, const int* __restrict__ lin, const double2* __restrict__ grid, size_t np,
                                     double scale, double* __restrict__ field) {
    const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -208,36 +264,53 @@ int ilog2(int v) {
 
 int grid_blocks(size_t np) { return (int)std::min<size_t>((np + 255) / 256, 148 * 16); }
 
-// 3-D FFT of `ncomp` consecutive grids.  box = false: full forward passes
-// x, y, z.  box = true: the moment transform, forward (input in the G-box)
-// x, y, z or inverse (output wanted in the G-box) z, y, x, pruned as
-// described at the top of this file.
-cudaError_t fft3d(FFTField* f, double2* data, int ncomp, bool inverse, bool box, cudaStream_t st, int* launches) {
+// forward 3-D FFT of `ncomp` consecutive grids, all lines (the tensor spectra)
+cudaError_t fft3d(FFTField* f, double2* data, int ncomp, cudaStream_t st) {
    const int px = f->p[0], py = f->p[1], pz = f->p[2];
-   const int gx = box ? f->g[0] : px, gy = box ? f->g[1] : py, gz = box ? f->g[2] : pz;
-   auto xpass = [&]() {  // lines of px points, kFFTTile / px lines per block
-      const int nrows = gy * gz;
+   {  // x: lines of px points, kFFTTile / px lines per block
+      const int nrows = py * pz;
       const int lines = std::max(1, std::min(kFFTTile / px, nrows));
       dim3 grid((unsigned)((nrows + lines - 1) / lines), (unsigned)ncomp);
-      fft_x_kernel<<<grid, kFFTThreads, 0, st>>>(data, f->np, px, f->logp[0], lines, f->tw[0], inverse, nrows, gy,
-                                                 py, inverse ? px : gx, inverse ? gx : px);
-   };
-   auto ypass = [&]() {  // stride px, W adjacent x columns, one block per (x chunk, z < gz)
+      fft_x_kernel<<<grid, kFFTThreads, 0, st>>>(data, f->np, px, f->logp[0], lines, f->tw[0], 0, nrows, py, py, px,
+                                                 px);
+   }
+   {  // y: stride px, W adjacent x columns, one block per (x chunk, z)
       const int W = std::max(1, std::min(kFFTTile / py, px));
-      dim3 grid((unsigned)(px / W), (unsigned)gz, (unsigned)ncomp);
+      dim3 grid((unsigned)(px / W), (unsigned)pz, (unsigned)ncomp);
       fft_strided_kernel<<<grid, kFFTThreads, 0, st>>>(data, f->np, py, f->logp[1], W, (size_t)px,
-                                                       (size_t)px * py, f->tw[1], inverse, inverse ? py : gy,
-                                                       inverse ? gy : py);
-   };
-   auto zpass = [&]() {  // stride px*py, one block per (x chunk, y)
+                                                       (size_t)px * py, f->tw[1], 0, py, py);
+   }
+   {  // z: stride px*py, one block per (x chunk, y)
       const int W = std::max(1, std::min(kFFTTile / pz, px));
       dim3 grid((unsigned)(px / W), (unsigned)py, (unsigned)ncomp);
       fft_strided_kernel<<<grid, kFFTThreads, 0, st>>>(data, f->np, pz, f->logp[2], W, (size_t)px * py, (size_t)px,
-                                                       f->tw[2], inverse, inverse ? pz : gz, inverse ? gz : pz);
+                                                       f->tw[2], 0, pz, pz);
+   }
+   return cudaGetLastError();
+}
+
+// the x and y passes of the moment transform (forward: x then y; inverse: y
+// then x), pruned to the G-box; the z passes run in fft_z_multiply_kernel
+cudaError_t fft_box(FFTField* f, bool inverse, cudaStream_t st, int* launches) {
+   const int px = f->p[0], py = f->p[1];
+   const int gx = f->g[0], gy = f->g[1], gz = f->g[2];
+   auto xpass = [&]() {
+      const int nrows = gy * gz;
+      const int lines = std::max(1, std::min(kFFTTile / px, nrows));
+      dim3 grid((unsigned)((nrows + lines - 1) / lines), 3u);
+      fft_x_kernel<<<grid, kFFTThreads, 0, st>>>(f->grid, f->np, px, f->logp[0], lines, f->tw[0], inverse, nrows, gy,
+                                                 py, inverse ? px : gx, inverse ? gx : px);
    };
-   if (inverse) { zpass(); ypass(); xpass(); }
-   else { xpass(); ypass(); zpass(); }
-   if (launches) *launches += 3;
+   auto ypass = [&]() {
+      const int W = std::max(1, std::min(kFFTTile / py, px));
+      dim3 grid((unsigned)(px / W), (unsigned)gz, 3u);
+      fft_strided_kernel<<<grid, kFFTThreads, 0, st>>>(f->grid, f->np, py, f->logp[1], W, (size_t)px,
+                                                       (size_t)px * py, f->tw[1], inverse, inverse ? py : gy,
+                                                       inverse ? gy : py);
+   };
+   if (inverse) { ypass(); xpass(); }
+   else { xpass(); ypass(); }
+   if (launches) *launches += 2;
    return cudaGetLastError();
 }
 
@@ -343,7 +416,7 @@ FFTField* fft_field_create(int nc, const double* cpos, const int* natoms, double
                                                           f->g[2], size);
       e = cudaGetLastError();
    }
-   if (e == cudaSuccess) e = fft3d(f, f->tspec, 6, false, false, st, nullptr);
+   if (e == cudaSuccess) e = fft3d(f, f->tspec, 6, st);
    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host tables above leave scope
    if (e != cudaSuccess) {
       *err = e;
@@ -359,9 +432,15 @@ cudaError_t fft_field_apply(FFTField* f, const double* mag, double* field, cudaS
    const int nbox = f->g[0] * f->g[1] * f->g[2];
    scatter_moments_kernel<<<(nbox + 255) / 256, 256, 0, st>>>(nc, f->box_cell, f->g[0], f->g[1], nbox, mag, f->grid,
                                                               f->p[0], f->p[1], f->np);
-   if ((e = fft3d(f, f->grid, 3, false, true, st, launches)) != cudaSuccess) return e;
-   multiply_kernel<<<grid_blocks(f->np), 256, 0, st>>>(f->grid, f->tspec, f->np);
-   if ((e = fft3d(f, f->grid, 3, true, true, st, launches)) != cudaSuccess) return e;
+   if ((e = fft_box(f, false, st, launches)) != cudaSuccess) return e;
+   {
+      const int pz = f->p[2];
+      const int W = std::max(1, std::min(kFuseTile / (3 * pz), f->p[0]));
+      dim3 grid((unsigned)(f->p[0] / W), (unsigned)f->p[1]);
+      fft_z_multiply_kernel<<<grid, kFFTThreads, 0, st>>>(f->grid, f->tspec, f->np, f->p[0], f->p[1], pz, f->logp[2],
+                                                          W, f->g[2], f->tw[2]);
+   }
+   if ((e = fft_box(f, true, st, launches)) != cudaSuccess) return e;
    gather_field_kernel<<<(nc + 255) / 256, 256, 0, st>>>(nc, f->cell_lin, f->grid, f->np, 1.0 / (double)f->np, field);
    if (launches) *launches += 3;
    return cudaGetLastError();
