@@ -251,6 +251,11 @@ int vgpu_set_noise_replay(vgpu_handle h, const double* xi);
  * (default) = gathers through L1/L2 (measured faster on B200).  Same results
  * bit for bit. */
 #define VGPU_OPT_WINDOW_STAGING 8
+/* VGPU_OPT_PROFILE_EVERY: with vgpu_profile on, time the launches of one step
+ * in `value` (>= 1; default 1 = every launch).  The events recorded around a
+ * timed launch delay the stream by a few microseconds, so sampling keeps a
+ * profiled run close to an unprofiled one. */
+#define VGPU_OPT_PROFILE_EVERY 9
 /* Bond-record layout the next FP32 pass reads: *layout = VGPU_RECORDS_WINDOW
  * (compact words with window staging), VGPU_RECORDS_COMPACT,
  * VGPU_RECORDS_WIDE (16-byte records) or VGPU_RECORDS_NONE (formats without

@@ -59,6 +59,26 @@ cudaError_t prepare_llg_staged(StageCfg& c, int nslices, int device) {
    return cudaSuccess;
 }
 
+// A staged pass launched with programmatic stream serialisation: its blocks
+// may be scheduled while the previous kernel of the stream drains; every
+// block waits for that kernel's completion (griddepcontrol.wait in
+// llg_staged_kernel) before its first global access.
+template <typename... Args>
+static cudaError_t launch_serialised(void (*kernel)(Args...), dim3 g, dim3 b, int smem, cudaStream_t st,
+                                     Args... args) {
+   cudaLaunchConfig_t cfg = {};
+   cfg.gridDim = g;
+   cfg.blockDim = b;
+   cfg.dynamicSmemBytes = (size_t)smem;
+   cfg.stream = st;
+   cudaLaunchAttribute attr[1];
+   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+   attr[0].val.programmaticStreamSerializationAllowed = 1;
+   cfg.attrs = attr;
+   cfg.numAttrs = 1;
+   return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, const StageCfg& c, cudaStream_t st) {
    if (c.grid == 0) return cudaSuccess;
    if ((a.crec != nullptr) != c.crec) return cudaErrorInvalidValue;  // record layout of the prepared shape
@@ -80,14 +100,14 @@ cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, co
    }
    const int smem = staged_smem_bytes(c.sl, c.nbuf, c.buf_bytes, c.dict_bytes, c.M);
 #define VGPU_STAGED_C(S, B, C)                                                                                 \
-   if (mode == PASS_PREDICTOR)                                                                                 \
-      llg_staged_kernel<PASS_PREDICTOR, S, B, C><<<g, b, smem, st>>>(a, nslices, c.ntiles, c.buf_bytes);       \
-   else                                                                                                        \
-      llg_staged_kernel<PASS_CORRECTOR, S, B, C><<<g, b, smem, st>>>(a, nslices, c.ntiles, c.buf_bytes);
+   e = launch_serialised(mode == PASS_PREDICTOR ? llg_staged_kernel<PASS_PREDICTOR, S, B, C>                   \
+                                                : llg_staged_kernel<PASS_CORRECTOR, S, B, C>,                  \
+                         g, b, smem, st, a, nslices, (int)c.ntiles, (int)c.buf_bytes);
 #define VGPU_STAGED(S, B)                                                                                      \
    if (c.sl == S && c.nbuf == B) {                                                                             \
+      cudaError_t e;                                                                                           \
       if (c.crec) { VGPU_STAGED_C(S, B, true) } else { VGPU_STAGED_C(S, B, false) }                            \
-      return cudaGetLastError();                                                                               \
+      return e;                                                                                                \
    }
    VGPU_STAGED(2, 1) VGPU_STAGED(2, 2) VGPU_STAGED(4, 1) VGPU_STAGED(4, 2) VGPU_STAGED(8, 1) VGPU_STAGED(8, 2)
 #undef VGPU_STAGED

@@ -102,6 +102,9 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
    constexpr int TS = 32 * SL;
    extern __shared__ __align__(128) unsigned char stage_smem[];
    __shared__ __align__(8) uint64_t mbar[2];
+   // launched with programmatic stream serialisation: the previous kernel of
+   // the stream has completed and its writes are visible after this
+   asm volatile("griddepcontrol.wait;" ::: "memory");
    const int tid = threadIdx.x;
    const int stride = buf_bytes + kStageOwnArrays * TS * 4;
    float4* sdict = reinterpret_cast<float4*>(stage_smem + NBUF * stride);

@@ -1027,6 +1027,10 @@ extern "C" int vgpu_set_option(vgpu_handle h, int option, int value) {
          h->window = value;
          h->sys.stage.grid = 0;
          return VGPU_OK;
+      case VGPU_OPT_PROFILE_EVERY:
+         if (value < 1) return set_err(h, VGPU_ERR_ARG, "profile stride must be >= 1");
+         h->prof_every = value;
+         return VGPU_OK;
       default: return set_err(h, VGPU_ERR_ARG, "unknown option %d", option);
    }
 }

@@ -137,6 +137,7 @@ struct vgpu_ctx {
    // kernel accounting and optional per-launch CUDA-event timing on `stream`
    int64_t kernel_launches = 0;
    bool prof_on = false;
+   int prof_every = 1;        // time the launches of one step in prof_every (VGPU_OPT_PROFILE_EVERY)
    struct ProfRec { int kind; cudaEvent_t a, b; };
    std::vector<ProfRec> prof_pending;
    std::vector<cudaEvent_t> event_pool;

@@ -26,6 +26,7 @@ OPT_STORE_INCREMENT, OPT_STAGED_RECORDS, OPT_STAGE_SLICES, OPT_STAGE_BUFFERS, OP
 OPT_STAGE_WAIT_TEST = 6
 OPT_COMPACT_RECORDS = 7
 OPT_WINDOW_STAGING = 8
+OPT_PROFILE_EVERY = 9
 RECORDS_NONE, RECORDS_WIDE, RECORDS_COMPACT, RECORDS_WINDOW = 0, 1, 2, 3
 PASS_PREDICTOR, PASS_CORRECTOR = 0, 1
 STATE_SPIN, STATE_PREDICTOR = 0, 1
