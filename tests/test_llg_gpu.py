@@ -389,6 +389,26 @@ def test_status_flags_nonfinite(V):
         assert e.value.code == V.ERR_NAN
 
 
+def test_profile_sampling(V):
+    """VGPU_OPT_PROFILE_EVERY = k times the launches of the steps whose
+    counter is a multiple of k; the kernel-launch count still covers every
+    launch, and a stride below 1 is refused."""
+    from vampire_b200 import system as S
+    s = S.config_fcc_tensor(L=4, seed=5)
+    with V.Simulation(s) as sim:
+        with pytest.raises(V.VGPUError) as e:
+            sim.set_option(V.OPT_PROFILE_EVERY, 0)
+        assert e.value.code == V.ERR_ARG
+        sim.set_option(V.OPT_PROFILE_EVERY, 5)
+        sim.profile(True)
+        sim.llg_heun(20)
+        prof = sim.profile_read()
+        sim.profile(False)
+    assert prof["predictor"]["count"] == 4 and prof["corrector"]["count"] == 4
+    assert prof["predictor"]["ms"] > 0.0
+    assert prof["kernel_launches"] >= 40
+
+
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", TOL32)])
 def test_llg_midpoint_matches_reference(V, prec, tol):
     """sim::LLG_Midpoint (src/simulate/LLGMidpoint.cpp) on the device: 100

@@ -261,7 +261,7 @@ class Simulation:
     def set_option(self, option: int, value: int) -> None:
         """vgpu_set_option: OPT_STORE_INCREMENT, OPT_STAGED_RECORDS, OPT_STAGE_SLICES,
         OPT_STAGE_BUFFERS, OPT_DIPOLE_FFT, OPT_STAGE_WAIT_TEST, OPT_COMPACT_RECORDS,
-        OPT_WINDOW_STAGING."""
+        OPT_WINDOW_STAGING, OPT_PROFILE_EVERY."""
         self._check(lib().vgpu_set_option(self._h, int(option), int(value)))
 
     def record_layout(self) -> Tuple[int, int]:
