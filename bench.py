@@ -268,9 +268,10 @@ def bench_adjoint(device, L=32, steps=2000):
     """Adjoint LLG-Heun on SC 32^3 (32,768 spins), T=0, 2,000 steps: the
     gradient of the trajectory loss w.r.t. (J, Ku, H) at J=11.2e-21 J,
     Ku=6.69e-24 J, H=(0,0,0.4) T against the target m_z(t) of J=10e-21 J,
-    Ku=5e-24 J, H=(0,0,0.5) T; FP64, sqrt(N) checkpointing.  Timed around the
-    single C-ABI call (forward with checkpoints, segment recomputation and
-    the backward sweep)."""
+    Ku=5e-24 J, H=(0,0,0.5) T; FP64, sqrt(N) checkpointing.  Timed around
+    AdjointRunner.loss_and_grad: the system set-up and upload and the C-ABI
+    call (forward with checkpoints, segment recomputation and the backward
+    sweep); the median of three calls, which give identical results."""
     from vampire_b200 import adjoint as A
     run = A.AdjointRunner(L=L, device=device)
     target = run.trajectory(10e-21, 5e-24, (0.0, 0.0, 0.5), steps)
