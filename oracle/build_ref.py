@@ -49,6 +49,15 @@ BASE_FLAGS = ["-std=c++11", "-O3", "-mtune=native", "-funroll-loops",
 SKIP_MODULES = {"cuda", "opencl"}
 
 
+
+# Where this recipe looks for the read-only reference tree when neither
+# --ref nor VAMPIRE_REF names one (the container that builds the oracle).
+DEFAULT_REF = "/root/reference"
+
+
+def default_ref() -> str:
+    return os.environ.get("VAMPIRE_REF", DEFAULT_REF)
+
 def object_list(ref: Path) -> list[str]:
     """Return reference sources (relative to src/, without extension)."""
     top = (ref / "makefile").read_text()
@@ -160,7 +169,7 @@ def build(ref: Path, jobs: int, with_b200: bool) -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("VAMPIRE_REF", "/root/reference"))
+    ap.add_argument("--ref", default=default_ref())
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--no-b200", action="store_true")
     a = ap.parse_args()
