@@ -594,21 +594,27 @@ int vgpu_mz_trajectory(vgpu_handle h, uint64_t n_steps, double* mz_out);
 /* ---- magnetisation without device allocation ----------------------------- */
 
 /* No counterpart in the reference: an addition for callers that cannot call
- * cudaMalloc (work recorded into a CUDA graph while capture forbids
- * allocation, or a plugin inside another framework whose caching allocator
- * owns the device memory).  All pointers are DEVICE pointers the caller
- * owns: spins sx/sy/sz and moments mu_muB [num_atoms] (FP32), mask
- * [num_atoms] with bins in [0, mask_size), output m_out [4*mask_size] (FP64:
- * m_hat_x, m_hat_y, m_hat_z, |m|/m_sat per bin, empty bins zero, as
- * vgpu_stats_get_magnetization).  Runs on `stream` (a cudaStream_t, NULL =
- * default stream) and returns without synchronising.
+ * cudaMalloc -- a plugin inside another framework whose caching allocator
+ * owns the device memory (its own cudaMalloc would fragment that pool or fail
+ * under the framework's memory cap), or a time-critical loop that must not
+ * stall on the device synchronisation cudaMalloc/cudaFree can bring.  All
+ * pointers are DEVICE pointers the caller owns: spins sx/sy/sz and moments
+ * mu_muB [num_atoms] (FP32), mask [num_atoms] with bins in [0, mask_size)
+ * (entries outside that range are skipped: counted in no bin), output m_out
+ * [4*mask_size] (FP64: m_hat_x, m_hat_y, m_hat_z, |m|/m_sat per bin, empty
+ * bins zero, as vgpu_stats_get_magnetization).  Runs on `stream` (a
+ * cudaStream_t, NULL = default stream) and returns without synchronising; a
+ * CUDA error already pending when it is called is returned, not launched over.
  * Scratch: a fixed array compiled into the library (VGPU_NOALLOC_MAX_BLOCKS x
  * VGPU_NOALLOC_MAX_BINS x 4 doubles = 512 KiB), held by every GPU that loads
  * the library until exit.  mask_size above VGPU_NOALLOC_MAX_BINS is refused
  * with VGPU_ERR_ARG.  The first call on a device looks up the array's device
- * address with that device current; make that first call before any stream
- * capture.  Every call shares the one array: calls that overlap on the GPU
- * (other streams, other threads) race and must be serialised by the caller. */
+ * address with that device current and keeps it for the process; make that
+ * first call before any stream capture, and do not call it again on a device
+ * after cudaDeviceReset.  Every call shares the one array (each call rewrites
+ * the rows it reads, so nothing needs clearing): calls that overlap on the
+ * GPU (other streams, other threads) race and must be serialised by the
+ * caller. */
 #define VGPU_NOALLOC_MAX_BLOCKS 256
 #define VGPU_NOALLOC_MAX_BINS 64
 int vgpu_magnetization_noalloc(const float* sx, const float* sy, const float* sz, const float* mu_muB,

@@ -1,10 +1,10 @@
 // Masked magnetisation reduction that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc: a host that records its work into a
-// CUDA graph while capture forbids allocation, a plugin running inside
-// another framework whose caching allocator owns the device memory (a
-// cudaMalloc of its own would fragment it or fail under a memory cap), or a
-// code path that must not block on the allocator's implicit synchronisation.
+// Some callers cannot call cudaMalloc: a plugin running inside another
+// framework whose caching allocator owns the device memory (a cudaMalloc of
+// its own would fragment that pool or fail under the framework's memory cap),
+// or a time-critical loop that must not stall on the implicit device
+// synchronisation that cudaMalloc and cudaFree can bring.
 // vgpu_magnetization_noalloc serves them: the caller passes device pointers to
 // its inputs and outputs, and the block partial sums go to a fixed-size
 // scratch array compiled into this library (a file-scope __device__ array,
@@ -32,10 +32,17 @@ static __device__ __align__(256) double g_noalloc_scratch[kMaxBlocks * kMaxBins 
 
 // Host code may not use g_noalloc_scratch as a device address (on the host it
 // names a host-side stand-in); its device address is looked up once per
-// device with that device current and cached here.
+// device with that device current and cached here.  A cudaDeviceReset
+// destroys the array with the context, and the cached address would then be
+// stale: a process that resets a device does not call this entry point on it
+// again.
 std::mutex g_scratch_mutex;
 double* g_scratch_ptr[128] = {nullptr};
 
+// Each thread keeps its running sums in registers while its atoms stay in
+// one bin and adds them to the block's shared sums when the bin changes; at
+// the end a warp whose lanes all hold the same bin adds its sums by shuffles
+// first, so a one-bin (system) mask costs four shared atomics per warp.
 __global__ void noalloc_partial_kernel(const float* __restrict__ sx, const float* __restrict__ sy,
                                        const float* __restrict__ sz, const float* __restrict__ mu,
                                        const int32_t* __restrict__ mask, int n, int size,
@@ -46,14 +53,33 @@ __global__ void noalloc_partial_kernel(const float* __restrict__ sx, const float
    const int per = (n + gridDim.x - 1) / gridDim.x;
    const int begin = blockIdx.x * per;
    const int end = min(n, begin + per);
+   int cur = -1;  // bin of the running sums (-1: none)
+   double r[4] = {0.0, 0.0, 0.0, 0.0};
    for (int i = begin + threadIdx.x; i < end; i += blockDim.x) {
       const int b = mask[i];
-      if (b < 0 || b >= size) continue;  // out-of-range bins are ignored
+      if (b < 0 || b >= size) continue;  // out-of-range bins are skipped
+      if (b != cur) {
+         if (cur >= 0)
+            for (int q = 0; q < 4; ++q) atomicAdd(&acc[4 * cur + q], r[q]);
+         cur = b;
+         r[0] = r[1] = r[2] = r[3] = 0.0;
+      }
       const double m = (double)mu[i];
-      atomicAdd(&acc[4 * b + 0], (double)sx[i] * m);
-      atomicAdd(&acc[4 * b + 1], (double)sy[i] * m);
-      atomicAdd(&acc[4 * b + 2], (double)sz[i] * m);
-      atomicAdd(&acc[4 * b + 3], m);
+      r[0] += (double)sx[i] * m;
+      r[1] += (double)sy[i] * m;
+      r[2] += (double)sz[i] * m;
+      r[3] += m;
+   }
+   const unsigned full = 0xffffffffu;
+   const int lane = threadIdx.x & 31;
+   const int cur0 = __shfl_sync(full, cur, 0);
+   if (__all_sync(full, cur == cur0)) {
+      for (int q = 0; q < 4; ++q)
+         for (int o = 16; o > 0; o >>= 1) r[q] += __shfl_down_sync(full, r[q], o);
+      if (lane == 0 && cur >= 0)
+         for (int q = 0; q < 4; ++q) atomicAdd(&acc[4 * cur + q], r[q]);
+   } else if (cur >= 0) {
+      for (int q = 0; q < 4; ++q) atomicAdd(&acc[4 * cur + q], r[q]);
    }
    __syncthreads();
    // every block writes its whole row, so the scratch needs no clearing
@@ -117,10 +143,13 @@ extern "C" int vgpu_magnetization_noalloc(const float* sx, const float* sy, cons
    double* scratch = nullptr;
    int rc = scratch_for_current_device(&scratch);
    if (rc) return rc;
+   // an error left pending by earlier work is reported as such, not as this call's
+   cudaError_t e = cudaPeekAtLastError();
+   if (e != cudaSuccess) return vgpu::cuda_err(nullptr, e, "CUDA error pending before the no-alloc call");
    cudaStream_t st = (cudaStream_t)stream;
    const int nblocks = std::max(1, std::min(kMaxBlocks, (num_atoms + 255) / 256));
    noalloc_partial_kernel<<<nblocks, 256, 0, st>>>(sx, sy, sz, mu_muB, mask, num_atoms, mask_size, scratch);
-   cudaError_t e = cudaGetLastError();
+   e = cudaGetLastError();
    if (e != cudaSuccess) return vgpu::cuda_err(nullptr, e, "no-alloc magnetisation launch");
    noalloc_final_kernel<<<(mask_size + 63) / 64, 64, 0, st>>>(scratch, nblocks, mask_size, m_out);
    e = cudaGetLastError();
