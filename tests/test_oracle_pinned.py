@@ -205,3 +205,59 @@ def test_biquadratic_exchange():
     bad = s.copy()
     bad.biquadratic = None
     assert np.abs(O.OracleSystem(bad).llg_heun(s.spins, 1, xi=d["xi_1"]) - ref_spins(d, 1)).max() > 1e-9
+
+
+EXCH_FIXTURES = ["tet_iso_bond", "tet_vec_bond", "tet_ten_bond", "sc6_vec"]
+
+
+@pytest.mark.parametrize("name", EXCH_FIXTURES)
+def test_exchange_forms_trajectory_and_energy(name):
+    """Per-bond isotropic, vectorial and tensorial exchange from a unit-cell
+    file, and the normalised vectorial form (src/exchange/exchange_fields.cpp
+    :49-163, exchange/energy.cpp): 200 T=0 steps and the energies at step
+    200 follow the reference; one replayed-noise step at 300 K."""
+    s, d = load_golden(f"{name}_t0")
+    o = O.OracleSystem(s)
+    got, done = s.spins, 0
+    for t in (1, 100, 200):
+        got = o.llg_heun(got, t - done)
+        done = t
+        assert np.abs(got - ref_spins(d, t)).max() < 1e-12, t
+    mask, size = s.masks["system"]
+    e = o.energy(ref_spins(d, 200), mask, size)
+    want = d["energy_system_200"]
+    assert np.abs(e - want).max() < 1e-11 * np.abs(want).max()
+    s3, d3 = load_golden(f"{name}_t300")
+    o3 = O.OracleSystem(s3)
+    got = s3.spins
+    for t in (1, 2):
+        got = o3.llg_heun(got, 1, xi=d3[f"xi_{t}"])
+        assert np.abs(got - ref_spins(d3, t)).max() < 1e-12, t
+
+
+def test_cmc_restatement_keeps_the_constraint():
+    """The restated constrained pair rule (cmc.cpp:282-490) in the
+    reference's own frame (tests/golden/cmc_sc12.npz): accepted pair moves
+    keep the moment perpendicular to the constraint, spins stay unit, and the
+    running moment equals the spins' moment."""
+    from conftest import GOLDEN
+    d = dict(np.load(GOLDEN / "cmc_sc12.npz"))
+    s = O.system_from_dump(d)
+    s.params.temperature = 600.0
+    P, pv = d["cmc_frame"][:9].reshape(3, 3), d["cmc_frame"][9:12]
+    sp = np.tile(pv[:, None], (1, s.n))
+    mu = s.mu_s_muB()
+    M = (sp * mu).sum(1)
+    o = O.OracleSystem(s)
+    rng = np.random.default_rng(3)
+    K = 200
+    for _ in range(5):
+        pairs = rng.permutation(s.n)[: 2 * K].reshape(K, 2)
+        rnd = np.concatenate([rng.standard_normal(3 * K), rng.random(K)])
+        sp, M2, cnt = o.cmc_pairs(sp, pairs, rnd, P, pv, M)
+        assert cnt[0] > 0
+        perp = lambda v: v - (v @ pv) * pv
+        assert np.abs(perp(M2) - perp(M)).max() < 1e-10 * np.abs(M).max()
+        assert np.abs(np.linalg.norm(sp, axis=0) - 1.0).max() < 1e-14
+        assert np.abs((sp * mu).sum(1) - M2).max() < 1e-9 * np.abs(M2).max()
+        M = M2

@@ -1050,6 +1050,17 @@ extern "C" int vgpu_record_layout(vgpu_handle h, int32_t* layout, int32_t* dict_
    return VGPU_OK;
 }
 
+extern "C" int vgpu_exchange_format(vgpu_handle h, int32_t* fmt) {
+   if (!h || !fmt) return set_err(h, VGPU_ERR_ARG, "null argument");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   static_assert(FMT_ISO_TAB == VGPU_EXCH_ISO_TAB && FMT_ISO_BOND == VGPU_EXCH_ISO_BOND &&
+                     FMT_VEC_TAB == VGPU_EXCH_VEC_TAB && FMT_VEC_BOND == VGPU_EXCH_VEC_BOND &&
+                     FMT_DMI_TAB == VGPU_EXCH_DMI_TAB && FMT_TENSOR_BOND == VGPU_EXCH_TENSOR_BOND,
+                 "exchange format numbering");
+   *fmt = h->sys.fmt;
+   return VGPU_OK;
+}
+
 extern "C" int vgpu_set_step(vgpu_handle h, uint64_t step) {
    if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
    h->step = step;
