@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-dipole", action="store_true", help="leave out the macrocell dipole field")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and Monte Carlo side results")
+    ap.add_argument("--no-error", action="store_true", help="skip the FP32-vs-FP64 error figure of the main line")
     ap.add_argument("--e2e-steps", type=int, default=2000,
                     help="steps of the end-to-end run (the workload's 2,000: initial upload and final download once)")
     ap.add_argument("--records", choices=["auto", "wide"], default="auto",
@@ -69,31 +70,81 @@ def workload_config(L, n_gpus):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region: NVML read every 5 ms from a thread (read-only queries), plus one
+    reading at the start and one at the end; nvidia-smi at 200 ms if NVML is
+    absent."""
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active")
 
-    def __init__(self, device_index=0):
+    def __init__(self, device_index=0, period_s=0.005):
         self.dev = device_index
-        self.samples = []
+        self.period = period_s
+        self.samples = []  # (sm_mhz, max_mhz, reasons bitmask)
         self.proc = None
+        self.nvml = None
+        self._stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+
+    def _read_nvml(self):
+        nv, h = self.nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        self.samples.append((float(sm), float(mx), int(rs)))
+
+    def _loop(self):
+        while not self._stop.is_set():
+            try:
+                self._read_nvml()
+            except Exception:
+                return
+            time.sleep(self.period)
 
     def start(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self._read_nvml()
+            self.th = threading.Thread(target=self._loop, daemon=True)
+            self.th.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-i", str(self.dev), "-lms", "200"], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
-            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th = threading.Thread(target=self._read_smi, daemon=True)
             self.th.start()
         except FileNotFoundError:
             self.proc = None
 
-    def _read(self):
+    def _read_smi(self):
         for line in self.proc.stdout:
-            self.samples.append([x.strip() for x in line.split(",")])
+            f = [x.strip() for x in line.split(",")]
+            try:
+                self.samples.append((float(f[1]), float(f[2]), int(f[4], 16)))
+            except (ValueError, IndexError):
+                pass
 
     def stop(self):
+        if self.nvml:
+            self._stop.set()
+            self.th.join(timeout=1.0)
+            try:
+                self._read_nvml()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -105,16 +156,10 @@ class ClockSampler:
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for s in self.samples:
-            for k, nm in enumerate(names):
-                if len(s) > 5 + k and s[5 + k].lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+        reasons = sorted({nm for _, _, r in self.samples for nm, bit in self.REASONS if r & bit})
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples),
+                "sm_max_mhz": max(s[1] for s in self.samples), "reasons": reasons,
+                "samples": len(self.samples), "source": "nvml 5 ms" if self.nvml else "nvidia-smi 200 ms"}
 
 
 def measured_peak_hbm():
@@ -261,7 +306,8 @@ def bench_mc(device, L=50, eq=5000, av=10000, every=10):
                         f"{eq} + {av} sweeps, <|m|> every {every} sweeps",
             "spins": s.n, "colours": nc, "sweeps": sweeps, "value": s.n * sweeps / (ms * 1e-3),
             "unit": "spin-moves/s", "sweep_only_value": s.n * eq / (ms_eq * 1e-3), "protocol_s": ms * 1e-3,
-            "acceptance": 1.0 - rej / moves, "Tc_K": tc, "m_T": [round(float(x), 5) for x in m_T]}
+            "acceptance": 1.0 - rej / moves, "Tc_K": tc, "m_T": [round(float(x), 5) for x in m_T],
+            "error_vs_reference": mc_reference_comparison(Ts, m_T, tc)}
 
 
 def bench_adjoint(device, L=32, steps=2000):
@@ -284,34 +330,143 @@ def bench_adjoint(device, L=32, steps=2000):
         loss, grad = run.loss_and_grad(11.2e-21, 6.69e-24, (0.0, 0.0, 0.4), target)
         times.append(time.perf_counter() - t0)
     dt = sorted(times)[1]
+    # error: the adjoint gradient against central differences (h = 1e-6
+    # relative) of the device FP64 forward loss, for J, Ku and H_z
+    import numpy as np
+    p = np.array([11.2e-21, 6.69e-24, 0.0, 0.0, 0.4])
+    rel = []
+    for k, sc in ((0, p[0]), (1, p[1]), (4, 0.4)):
+        h = 1e-6 * sc
+        pp, pm = p.copy(), p.copy()
+        pp[k] += h
+        pm[k] -= h
+        fd = (run.loss_and_grad(pp[0], pp[1], pp[2:], target)[0] -
+              run.loss_and_grad(pm[0], pm[1], pm[2:], target)[0]) / (2 * h)
+        rel.append(abs(grad[k] - fd) / abs(fd))
     return {"workload": f"SC {L}^3, {steps} steps, loss = sum_t dt (m_z - target)^2, grad w.r.t. J, Ku, H (3)",
             "spins": L ** 3, "steps": steps, "seconds": dt, "seconds_all": times, "value": L ** 3 * steps / dt,
             "unit": "spin-steps/s (forward + backward)", "precision": "fp64", "loss": loss,
-            "grad": [float(g) for g in grad], "checkpoints": int(-(-steps // int(steps ** 0.5 + 0.999999)))}
+            "grad": [float(g) for g in grad], "checkpoints": int(-(-steps // int(steps ** 0.5 + 0.999999))),
+            "error_vs_fd": {"max_rel_dev": float(max(rel)), "components": ["J", "Ku", "Hz"],
+                            "against": "central differences (h = 1e-6 relative) of the FP64 forward loss"}}
+
+
+def error_vs_fp64_llg(sysm, device, steps=100):
+    """Max per-spin component deviation of the FP32 passes from the FP64 build
+    of the same kernels (which follows the reference's own trajectories to
+    1e-12 in the tests) on the workload system at T = 0 -- deterministic, so
+    the two runs see the same dynamics -- over the first `steps` steps, the
+    dipole field included."""
+    import numpy as np
+    from vampire_b200 import vgpu
+    T0 = sysm.params.temperature
+    sysm.params.temperature = 0.0
+    out = {}
+    try:
+        for prec in ("fp32", "fp64"):
+            with vgpu.Simulation(sysm, device=device, precision=prec) as sim:
+                if sysm.cells is not None:
+                    sim.dipole_setup(sysm.cells)
+                sim.llg_heun(steps)
+                out[prec] = sim.spins()
+    finally:
+        sysm.params.temperature = T0
+    return {"max_abs_spin_dev": float(np.abs(out["fp32"] - out["fp64"]).max()), "steps": steps,
+            "against": "FP64 build of the same kernels, same system at T=0 (FP32 bound 1e-5 over 100 steps)"}
+
+
+def error_vs_fp64_batched(device, steps=100, n_plain=16):
+    """The batched ensemble at T = 0: max per-spin deviation of the FP32
+    persistent run from the FP64 persistent run, and of FP32 per-system
+    launches from FP64 ones (the first n_plain particles), after `steps`."""
+    import numpy as np
+    from vampire_b200 import batch as B
+    from vampire_b200 import vgpu
+    systems, params = B.nanoparticle_ensemble(256, temperature=0.0)
+    got = {}
+    for prec in ("fp32", "fp64"):
+        with B.Batch(systems, params, device=device, precision=prec) as b:
+            b.run(steps, record_every=0)
+            got[prec] = b.spins()
+    dev_b = max(float(np.abs(a - c).max()) for a, c in zip(got["fp32"], got["fp64"]))
+    dev_p = 0.0
+    for k in range(n_plain):
+        s = systems[k]
+        s.params.temperature = 0.0
+        r = {}
+        for prec in ("fp32", "fp64"):
+            with vgpu.Simulation(s, device=device, precision=prec) as sim:
+                sim.llg_heun(steps)
+                r[prec] = sim.spins()
+        dev_p = max(dev_p, float(np.abs(r["fp32"] - r["fp64"]).max()))
+    return {"batched_max_abs_spin_dev": dev_b, "per_system_max_abs_spin_dev": dev_p, "steps": steps,
+            "against": f"FP64 build at T=0 (batched: all 256; per-system launches: first {n_plain})"}
+
+
+def mc_reference_comparison(T, m_T, tc):
+    """The Monte Carlo m(T) against the reference's own sequential sweep of
+    the same protocol (tests/golden/mc_sc50_curie.npz, made by the reference
+    program), when that fixture is present."""
+    import numpy as np
+    p = REPO / "tests" / "golden" / "mc_sc50_curie.npz"
+    if not p.exists():
+        return None
+    d = np.load(p)
+    if not np.array_equal(d["T"], T):
+        return None
+    ref = d["m_mean"]
+    try:
+        tc_ref = _tc_fit(T, ref)
+    except Exception:
+        tc_ref = None
+    return {"max_abs_m_dev": float(np.abs(np.asarray(m_T) - ref).max()), "Tc_ref_K": tc_ref,
+            "Tc_rel_dev": (abs(tc - tc_ref) / tc_ref) if (tc and tc_ref) else None,
+            "against": "reference sequential Metropolis, SC 50^3, same temperatures and sweeps"}
+
+
+def reference_sample_L(steps, budget_s=20.0, rate_per_proc=3.0e6):
+    """FCC cells per side of the reference arm's sample: the largest of 50,
+    40, 30, 20 whose `steps` timed steps take about `budget_s` or less at
+    `rate_per_proc` spin-steps/s per process (the reference's FCC tensor rate
+    with all cores busy), so the arm stays within a few minutes at any step
+    count while its timed region lasts seconds."""
+    for L in (50, 40, 30, 20):
+        if steps * 4 * L ** 3 / rate_per_proc <= budget_s:
+            return L
+    return 20
 
 
 def reference_arm(args, rank, world):
     if rank != 0:
         return
     from oracle import cpu_baseline as B
-    cfg = workload_config(args.L, args.gpus)
     procs = os.cpu_count() or 1
-    # each step: one Heun step of an FCC 20^3 sample (32,000 spins) in every
-    # process; W untimed steps, then exactly K timed ones
+    # each step: one Heun step of an FCC L^3 sample (no dipole field: the
+    # reference's dense cell tensor does not fit at the workload's 125,000
+    # cells) in every process; W untimed steps, then exactly K timed ones
     steps, warmup = args.steps, args.warmup
+    L = reference_sample_L(steps)
     try:
-        r = B.reference_rate(L=20, steps=steps, procs=procs, warmup=warmup)
+        r = B.reference_rate(L=L, steps=steps, procs=procs, warmup=warmup)
     except Exception as e:  # binary absent: fall back to the restatement
         try:
             r = B.port_rate(L=16, steps=20)
         except Exception as e2:
             print(json.dumps({"impl": "reference", "unavailable": f"{e}; {e2}"}))
             return
+    cfg = {"workload": f"FCC {L}^3 LLG-Heun, tensor exchange + 3-site DMI, 2 materials, cubic Kc, T=300K, "
+                       "no dipole field", "spins_per_process": 4 * L ** 3, "processes": r["cores"],
+           "lattice": "fcc", "cells": [L, L, L], "a_nm": 0.354, "materials": 2, "exchange": "tensor+DMI (nn, z=12)",
+           "anisotropy": "cubic", "temperature_K": 300.0, "dipole": "off", "dt_s": 1e-16,
+           "stands_for": "the FCC 100^3 workload (4,000,000 spins, dipole on) of the GPU arm: spin-steps/s is an "
+                         "intensive rate, so a bounded sample of the same physics is timed per process",
+           "parallelism": f"{r['cores']} independent reference processes (the reference is single-threaded)"}
     line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 0, "steps": steps,
             "warmup": warmup, "ms_per_step": r.get("ms_per_step"), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg, "impl": "reference",
             "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
                              "sample": r["sample"]},
+            "timed_region_s": (r.get("ms_per_step") or 0.0) * steps * 1e-3,
             "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -367,6 +522,21 @@ def main():
     # warm-up
     sim.llg_heun(args.warmup)
     sim.synchronize()
+    # the dipole field update (every 100 steps): timed alone here so that its
+    # share enters `value` whatever the timed window holds
+    upd_ms, rate = 0.0, 0
+    if sysm.cells is not None:
+        rate = int(sysm.cells.get("update_rate", 100))
+        u0, u1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sim.dipole_update()
+        sim.synchronize()
+        u0.record(stream)
+        for _ in range(3):
+            sim.dipole_update()
+        u1.record(stream)
+        u1.synchronize()
+        upd_ms = u0.elapsed_time(u1) / 3
+    step0 = sim.step
 
     def barrier():
         if dist:
@@ -379,10 +549,11 @@ def main():
     sim.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    # per-launch CUDA events on the launches of one step in PROFILE_EVERY of
-    # the timed region (events between every pair of launches would slow the
-    # stream itself)
-    sim.set_option(vgpu.OPT_PROFILE_EVERY, PROFILE_EVERY)
+    # per-launch CUDA events on the launches of one step in `every` of the
+    # timed region (events between every pair of launches would slow the
+    # stream itself); at least 4 sampled launches per pass
+    every = max(1, min(PROFILE_EVERY, args.steps // 4))
+    sim.set_option(vgpu.OPT_PROFILE_EVERY, every)
     sim.profile(True)
     ev0.record(stream)
     sim.llg_heun(args.steps)
@@ -394,7 +565,11 @@ def main():
     prof = sim.profile_read()
     sim.profile(False)
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
+    ms_window = ev0.elapsed_time(ev1)
+    # updates that fell inside the window (after the step that brings the
+    # counter to a multiple of the rate) against the steps' share of them
+    k_in = (step0 + args.steps) // rate - step0 // rate if rate else 0
+    ms = ms_window + ((args.steps / rate - k_in) * upd_ms if rate else 0.0)
     if dist:
         t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -470,9 +645,13 @@ def main():
         assert np.isfinite(final).all()
 
     extra = {}
+    sim.close()
+    err = None
+    if not args.no_error:
+        err = error_vs_fp64_llg(sysm, local)
     if not args.no_extras:
-        sim.close()
         extra["batched"] = bench_batched(local)
+        extra["batched"]["error_vs_fp64"] = error_vs_fp64_batched(local)
         extra["monte_carlo"] = bench_mc(local, eq=args.mc_sweeps[0], av=args.mc_sweeps[1])
         extra["adjoint"] = bench_adjoint(local)
 
@@ -480,7 +659,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             from oracle import cpu_baseline as B
-            cpu = B.best_available(L=20, steps=100, procs=1)
+            cpu = B.best_available(L=40, steps=150, procs=1)
             cpu.pop("wall_s", None)
         except Exception as e:
             cpu = {"value": None, "unavailable": str(e)}
@@ -497,9 +676,14 @@ def main():
                          "avg_launch_ms": {k: prof[k]["ms"] / max(1, prof[k]["count"])
                                            for k in ("predictor", "corrector")},
                          "timed_launches": {k: prof[k]["count"] for k in ("predictor", "corrector")},
-                         "launch_timing": f"CUDA events around the launches of one step in {PROFILE_EVERY} "
+                         "launch_timing": f"CUDA events around the launches of one step in {every} "
                                           "of the timed region",
                          "step_achieved_gbs": step_gbs},
+            "dipole_update": {"ms": upd_ms, "every_steps": rate, "updates_in_window": k_in,
+                              "amortised_ms_per_step": (upd_ms / rate if rate else 0.0),
+                              "window_ms": ms_window,
+                              "note": "ms_per_step = (window + (steps/rate - updates_in_window) x update ms) / steps"},
+            "error_vs_fp64": err,
             "gpu_launches": prof["kernel_launches"],
             "clocks": clk,
             "e2e": e2e,
@@ -507,7 +691,6 @@ def main():
         }
         line.update(extra)
         print(json.dumps(line), flush=True)
-    sim.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

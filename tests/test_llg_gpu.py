@@ -40,10 +40,13 @@ def test_fields_match_oracle(V, name, prec):
     assert np.abs(got - want).max() <= tol * scale
 
 
-# FP32 trajectories from a random initial state diverge chaotically from the
-# FP64 reference (rounding of 6e-8 per step grows ~1e5x over 10^4 steps at
-# these exchange fields); the FP32 bound is held over the first 100 steps and
-# the growth is recorded.  The FP64 build follows the reference bit for bit.
+# FP32 trajectories from a random initial state diverge from the FP64
+# reference: the relaxation amplifies differences about 1e5x over 10^4 steps,
+# so the FP32 rounding of the initial state alone ends 9e-4 away at step
+# 10,000 (tests/test_lyapunov.py, on the FP64 oracle).  The FP32 bound is held
+# over the first 100 steps; later the per-spin deviation is bounded and the
+# system magnetisation and energy must still agree.  The FP64 build follows
+# the reference bit for bit.
 FP32_HORIZON = 100
 
 
@@ -71,7 +74,12 @@ def test_sc8_t0_trajectory(V, prec):
 def test_config0_t0_10000_steps(V, prec):
     """Config 0 (SC 20^3 periodic, J=11.2e-21 J, Ku=6.69e-24 J, H=0.1 T,
     alpha=0.1, dt=1e-16 s) from the reference's random initial state, 10,000
-    deterministic steps against the reference's own trajectory."""
+    deterministic steps against the reference's own trajectory.  FP64: 1e-12
+    per spin throughout.  FP32: 1e-5 per spin to step 100; at step 10,000 the
+    per-spin deviation is set by the dynamics' amplification of rounding (no
+    FP32 state can hold 1e-5 there, tests/test_lyapunov.py), so the system
+    magnetisation and total energy are checked against the reference's
+    statistics (5e-3 absolute, 1e-4 relative) and the spins to 0.1."""
     s, d = load_golden("sc20_t0")
     with V.Simulation(s, precision=prec) as sim:
         done = 0
@@ -80,12 +88,20 @@ def test_config0_t0_10000_steps(V, prec):
             sim.llg_heun(t - done)
             done = t
             errs[t] = float(np.abs(sim.spins() - ref_spins(d, t)).max())
-    print(f"config0 {prec} max per-spin error vs reference: {errs}")
+        mid = sim.add_mask(*s.masks["system"])
+        sim.stats_update(magnetization=True, energy=True)
+        m, _, _ = sim.magnetization(mid)
+        e, _, _ = sim.energy(mid)
+    dm = float(np.abs(m[:4] - d["mag_system_10000"][:4]).max())
+    de = float(abs(e[0] - d["energy_system_10000"][0]) / abs(d["energy_system_10000"][0]))
+    print(f"config0 {prec} max per-spin error vs reference: {errs}; step 10,000: |dm| {dm:.2e}, dE/E {de:.2e}")
     if prec == "fp64":
         assert max(errs.values()) <= TOL64, errs
+        assert dm < 1e-12 and de < 1e-11
     else:
         assert errs[1] <= TOL32 and errs[100] <= TOL32, errs
         assert errs[10000] < 0.1, errs
+        assert dm < 5e-3 and de < 1e-4, (dm, de)
 
 
 def test_fp32_stored_increment_option(V):
