@@ -267,6 +267,19 @@ int vgpu_set_noise_replay(vgpu_handle h, const double* xi);
 #define VGPU_RECORDS_COMPACT 2
 #define VGPU_RECORDS_WINDOW 3
 int vgpu_record_layout(vgpu_handle h, int32_t* layout, int32_t* dict_entries);
+/* Per-bond exchange format chosen at upload for the reference's unrolled
+ * exchange list (src/exchange/unroll.cpp, unroll_normalised.cpp): the
+ * coupling is read from a material-pair table when it is a function of the
+ * two materials (VGPU_EXCH_ISO_TAB / VEC_TAB / DMI_TAB: diagonal table plus
+ * the antisymmetric part per bond), else stored per bond (ISO_BOND: scalar,
+ * VEC_BOND: diagonal, TENSOR_BOND: full 3x3). */
+#define VGPU_EXCH_ISO_TAB 0
+#define VGPU_EXCH_ISO_BOND 1
+#define VGPU_EXCH_VEC_TAB 2
+#define VGPU_EXCH_VEC_BOND 3
+#define VGPU_EXCH_DMI_TAB 4
+#define VGPU_EXCH_TENSOR_BOND 5
+int vgpu_exchange_format(vgpu_handle h, int32_t* fmt);
 int vgpu_set_option(vgpu_handle h, int option, int value);
 
 /* Step counter that keys the Philox stream (counter = (atom, step)).  Resume
@@ -457,6 +470,35 @@ int vgpu_mc_colour(vgpu_handle h, int32_t colour);
  * (sim::mc_statistics_moves / mc_statistics_reject). */
 int vgpu_mc_counters(vgpu_handle h, double* moves, double* rejects);
 
+/* ---- constrained Monte Carlo -------------------------------------------- */
+
+/* Constrained Monte Carlo on the device.  Replaces montecarlo::cmc_step
+ * (src/montecarlo/cmc.cpp:282-490), sim::integrate_serial case 3 (sim.cpp:
+ * 623-629).  vgpu_cmc_setup sets the constraint direction (phi from z, theta
+ * about z, in degrees: sim::constraint_phi, sim::constraint_theta; the frame
+ * of polar_rot_matrix, cmc.cpp:53-135) and with init_spins != 0 turns every
+ * spin along it (CMCinit); it colours the exchange graph if vgpu_mc_setup was
+ * not called.  vgpu_cmc_sweep runs n_steps steps of about N pair moves each
+ * (angle move of one spin, the second spin of the pair keeping the moment
+ * perpendicular to the constraint, acceptance exp(-dE/kT) (Mz'/Mz)^2
+ * |s2z/s2z'| with Mz' > 0): the pairs of a phase are atoms of one colour, so
+ * their energy changes are independent and one warp accepts them in order
+ * with the running total moment, the reference's rule.  The pairs differ from
+ * the reference's random choice: the chains agree in distribution.
+ * vgpu_cmc_pairs runs one phase on given pairs (2*num_pairs atoms, all of one
+ * colour, each once) with given random numbers rnd[4*num_pairs] (the
+ * Gaussians of the first spin's move, x|y|z blocks, then the acceptance
+ * uniforms) from the total moment `moment` (mu_B; NULL: summed from the
+ * spins).  vgpu_cmc_get: the running total moment (mu_B) and counters[4] =
+ * pair moves, accepted, energy rejections, sphere rejections (cmc::mc_total,
+ * mc_success, energy_reject, sphere_reject).  vgpu_cmc_frame: the rotation
+ * P[9] (row-major, constraint direction to z) and the constraint vector. */
+int vgpu_cmc_setup(vgpu_handle h, double phi_deg, double theta_deg, int32_t init_spins);
+int vgpu_cmc_sweep(vgpu_handle h, uint64_t n_steps);
+int vgpu_cmc_pairs(vgpu_handle h, const int32_t* pairs, int32_t num_pairs, const double* rnd, const double* moment);
+int vgpu_cmc_get(vgpu_handle h, double* moment, double* counters);
+int vgpu_cmc_frame(vgpu_handle h, double* P9, double* pv3);
+
 /* ---- statistics (masked reductions, FP64) -------------------------------- */
 
 /* Register a statistics mask: mask[i] in [0, mask_size) is the bin of atom i
@@ -512,6 +554,24 @@ int vgpu_snapshot_setup(vgpu_handle h, const int64_t* atoms, int64_t count);
  * reading it).  A file is a uint64 count followed by this block
  * (vampire_b200/config.py writes it with the reference's names and meta file). */
 int vgpu_snapshot(vgpu_handle h, double* out);
+
+/* Torque statistics.  Replaces stats::system_torque and stats::max_torque
+ * (src/utility/statistics.cpp:221-325; output functions 14, 15 and 20 of
+ * vio/outputfunctions.cpp).  vgpu_torque_update evaluates, from the current
+ * spins and the total field H_i of every updated atom (spin fields plus
+ * external fields: applied, thermal at the handle's current step, dipole),
+ * T = sum_i mu_s,i S_i x H_i [J] for the system and per material, and
+ * max_i |S_i x H_i| [T], and adds T to running sums; it runs on the handle's
+ * stream without synchronising.  vgpu_torque_get (synchronises) returns
+ * total[3], mean[3] (running sum / updates), material[3*M] and
+ * material_mean[3*M] (x, y, z per material), max_torque and the update
+ * count; any output may be NULL.  vgpu_torque_reset (also done by
+ * vgpu_stats_reset, as the reference's mag_m_reset) zeroes the means.  On a
+ * shard the sums cover the owned atoms; the host adds them over ranks. */
+int vgpu_torque_update(vgpu_handle h);
+int vgpu_torque_get(vgpu_handle h, double* total, double* mean, double* material, double* material_mean,
+                    double* max_torque, int64_t* counter);
+int vgpu_torque_reset(vgpu_handle h);
 
 /* Raw per-bin sums of the last vgpu_stats_update of mask `id`: sums[8*bin +
  * {0..3}] = sum mu s_x, sum mu s_y, sum mu s_z, sum mu (mu_B), [4..7] = the
@@ -582,10 +642,25 @@ int vgpu_batch_system_range(vgpu_handle h, int32_t k, int32_t* first_atom, int32
  *   grad[0] = dL/d(common scale of every exchange coupling),
  *   grad[1] = dL/dKu_SI (ku2 = Ku/mu_s), grad[2..4] = dL/dH_applied [1/T],
  * by the adjoint of the step with checkpoints every `every` steps
- * (0: ceil(sqrt(n_steps))).  Needs the FP64 build, symmetric (isotropic or
- * vectorial) exchange, no thermal noise, no dipole field. */
+ * (0: ceil(sqrt(n_steps))).  Every exchange format (isotropic, vectorial,
+ * diagonal + DMI, full tensor) and any number of materials, provided the
+ * couplings are reciprocal in SI units (mu_s,j J_ji = (mu_s,i J_ij)^T, as a
+ * symmetric exchange matrix and the three-site DMI give; checked on the
+ * device, VGPU_ERR_ARG otherwise).  Needs the FP64 build, no thermal noise,
+ * no dipole field. */
 int vgpu_adjoint_llg(vgpu_handle h, uint64_t n_steps, const double* target, double w, int32_t every,
                      double* loss_out, double* grad_out);
+
+/* As vgpu_adjoint_llg, plus the gradients per pair of materials (at most 8
+ * materials): pair_out[0] = dL/d(common scale of the DMI vectors) (0 without
+ * an antisymmetric part), pair_out[1 + a*M + b] = dL/d(scale of the couplings
+ * of the bonds from atoms of material a to atoms of material b) -- for the
+ * diagonal + DMI format the diagonal, exchange-matrix part only.  Divided by
+ * the exchange-matrix entry J_ab these are dL/dJ_ab, the gradients with
+ * respect to the per-material exchange constants (material exchange-matrix,
+ * exchange/interface.cpp:76-94).  pair_out holds 1 + M*M doubles. */
+int vgpu_adjoint_llg_materials(vgpu_handle h, uint64_t n_steps, const double* target, double w, int32_t every,
+                               double* loss_out, double* grad_out, double* pair_out);
 
 /* m_z(t), t = 1..n_steps, of a deterministic FP64 run from the current spins
  * (left unchanged): the targets of vgpu_adjoint_llg. */

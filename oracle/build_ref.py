@@ -12,6 +12,9 @@ every output under ``oracle/_ref/``, which is git-ignored:
     oracle/_ref/vampire-harness    reference objects + oracle/harness.cpp: a
                                    white-box driver that dumps the reference's
                                    own CSR, exchange lists, spins and RNG stream
+    oracle/_ref/vampire-harness-b200  the harness on the -DCUDA objects with the
+                                   B200 backend: --gpu-mc runs Monte Carlo
+                                   through the gpu::mc_step hook
     oracle/_ref/vampire-b200       the unmodified reference program built with
                                    -DCUDA, whose ``vcuda::`` backend is
                                    vampire_b200/host/vcuda_b200.cpp over the
@@ -164,6 +167,16 @@ def build(ref: Path, jobs: int, with_b200: bool) -> None:
         cuda_set = set(cuda_files)
         objs = [str(OUT / ("obj_cuda" if s in cuda_set else "obj") / f"{s}.o") for s in srcs]
         link(OUT / "vampire-b200", objs + [str(shim_o)],
+             ["-L", str(lib.parent), "-lvgpu", f"-Wl,-rpath,$ORIGIN/../../vampire_b200"])
+        # the harness on the same -DCUDA objects, with the gpu::mc_step hook
+        hook_o = OUT / "harness_b200.o"
+        err = _compile((HERE / "harness.cpp", hook_o,
+                        BASE_FLAGS + inc + ["-DCUDA", "-DVGPU_MC_HOOK", "-I", str(ref / "src")]))
+        if err:
+            sys.stderr.write(err)
+            raise SystemExit(1)
+        lib_cuda = [o for s, o in zip(srcs, objs) if s != "main/main"]
+        link(OUT / "vampire-harness-b200", lib_cuda + [str(shim_o), str(hook_o)],
              ["-L", str(lib.parent), "-lvgpu", f"-Wl,-rpath,$ORIGIN/../../vampire_b200"])
 
 

@@ -22,11 +22,13 @@
 //     calculate_thermal_fields (fields.cpp:274-276) and restoring the state
 //     (hdr/mtrand.hpp:62-64), so the reference then draws the same values;
 //   * magnetisation and energy statistics (statistics/magnetization.cpp:134,
-//     statistics/energy.cpp:141) and macrocell dipole fields (dipole/field.cpp).
+//     statistics/energy.cpp:141), torque statistics (utility/statistics.cpp:
+//     221-325) and macrocell dipole fields (dipole/field.cpp).
 //
 // Output: raw little-endian arrays <name>.bin in --out, listed in manifest.txt
 // as "<name> <dtype> <count>".
 //------------------------------------------------------------------------------
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -57,6 +59,22 @@
 #include "exchange/internal.hpp"
 
 namespace sim { void increment_time(); }
+namespace stats { void system_torque(); }
+namespace montecarlo { namespace cmc {
+extern std::vector<std::vector<double> > polar_vector, polar_matrix;
+} }
+
+#ifdef VGPU_MC_HOOK
+// Built as oracle/_ref/vampire-harness-b200 (reference objects compiled -DCUDA,
+// the B200 vcuda:: backend, libvgpu.so): --gpu-mc runs the reference's
+// start-up, then gpu::initialize(), and each Monte Carlo step through the
+// gpu::mc_step hook a host adds in sim::integrate_serial (the two-line change
+// INTEGRATION.md shows), i.e. vcuda::mc_step(), instead of
+// montecarlo::mc_step.
+#include "gpu.hpp"
+namespace vcuda { void mc_step(); }
+static bool g_gpu_mc = false;
+#endif
 
 // main.cpp owns this definition; the harness replaces main.cpp
 namespace vmain { namespace internal { std::string input_file_name = "input"; } }
@@ -201,6 +219,26 @@ static void dump_system() {
    }
 }
 
+// stats::system_torque and stats::max_torque (utility/statistics.cpp:221-325)
+// at the current spins: the instantaneous system and per-material torque (the
+// reference's sublattice sums, cleared first so one call's values remain)
+// and the largest |S x H|.  Dumped as torque_<tag> = [T_x, T_y, T_z,
+// T_x per material, T_y per material, T_z per material, max |S x H|].
+static void dump_torque(const std::string& tag) {
+   const int M = mp::num_materials;
+   stats::num_atoms = atoms::num_atoms;
+   stats::sublattice_mean_torque_x_array.assign(M, 0.0);
+   stats::sublattice_mean_torque_y_array.assign(M, 0.0);
+   stats::sublattice_mean_torque_z_array.assign(M, 0.0);
+   stats::system_torque();
+   std::vector<double> out(stats::total_system_torque, stats::total_system_torque + 3);
+   for (int m = 0; m < M; m++) out.push_back(stats::sublattice_mean_torque_x_array[m]);
+   for (int m = 0; m < M; m++) out.push_back(stats::sublattice_mean_torque_y_array[m]);
+   for (int m = 0; m < M; m++) out.push_back(stats::sublattice_mean_torque_z_array[m]);
+   out.push_back(stats::max_torque());
+   dumpd("torque_" + tag, out);
+}
+
 static void dump_stats(const std::string& tag) {
    stats::update(atoms::x_spin_array, atoms::y_spin_array, atoms::z_spin_array,
                  atoms::m_spin_array, atoms::type_array, sim::temperature);
@@ -266,10 +304,17 @@ static void dump_dipole(const std::string& tag) {
 static void one_step() {
    switch (sim::integrator) {
       case 1:
+#ifdef VGPU_MC_HOOK
+         if (g_gpu_mc) {
+            vcuda::mc_step();
+            break;
+         }
+#endif
          montecarlo::mc_step(atoms::x_spin_array, atoms::y_spin_array, atoms::z_spin_array, atoms::num_atoms,
                              atoms::type_array);
          break;
       case 2: sim::LLG_Midpoint(); break;
+      case 3: montecarlo::cmc_step(); break;
       default: sim::LLG_Heun(); break;
    }
 }
@@ -277,7 +322,7 @@ static void one_step() {
 int main(int argc, char* argv[]) {
    long steps = 0, warmup = 0, noise = 0, mag_every = 0, mag_start = 0, stats_every = 0;
    bool want_derived = false;
-   std::vector<long> snaps, stat_snaps;
+   std::vector<long> snaps, stat_snaps, torque_snaps;
    bool want_system = false, want_dipole = false, want_time = false;
    for (int i = 1; i < argc; i++) {
       std::string a = argv[i];
@@ -292,12 +337,16 @@ int main(int argc, char* argv[]) {
       else if (a == "--snaps") snaps = parse_list(next());
       else if (a == "--noise") noise = atol(next());
       else if (a == "--stats") stat_snaps = parse_list(next());
+      else if (a == "--torque") torque_snaps = parse_list(next());
       else if (a == "--mag-every") mag_every = atol(next());
       else if (a == "--mag-start") mag_start = atol(next());
       else if (a == "--dipole") want_dipole = true;
       else if (a == "--derived") want_derived = true;
       else if (a == "--stats-every") stats_every = atol(next());
       else if (a == "--time") want_time = true;
+#ifdef VGPU_MC_HOOK
+      else if (a == "--gpu-mc") g_gpu_mc = true;
+#endif
       else { std::cerr << "harness: unknown option " << a << std::endl; return 2; }
    }
    g_manifest.open(g_out + "/manifest.txt");
@@ -340,10 +389,17 @@ int main(int argc, char* argv[]) {
                       atoms::y_coord_array, atoms::z_coord_array, atoms::x_spin_array,
                       atoms::y_spin_array, atoms::z_spin_array, atoms::m_spin_array, atoms::num_atoms);
 
+#ifdef VGPU_MC_HOOK
+   if (g_gpu_mc) {
+      gpu::acceleration = true;
+      gpu::initialize();
+   }
+#endif
    if (want_system) dump_system();
    dump_spins("0");
    if (want_dipole) dump_dipole("0");
    for (long s : stat_snaps) if (s == 0) dump_stats("0");
+   for (long s : torque_snaps) if (s == 0) dump_torque("0");
 
    const int n = atoms::num_atoms;
    std::vector<double> mag_trace;  // per recorded step: mx, my, mz, |m| (system mask, bin 0), total E
@@ -364,11 +420,18 @@ int main(int argc, char* argv[]) {
       }
       one_step();
       sim::increment_time();
+#ifdef VGPU_MC_HOOK
+      // the spins live on the device: bring them back where the host reads them
+      if (g_gpu_mc && ((mag_every > 0 && step > mag_start && (step - mag_start) % mag_every == 0) ||
+                       std::find(snaps.begin(), snaps.end(), step) != snaps.end()))
+         gpu::config::synchronise();
+#endif
       if (stats_every > 0 && step % stats_every == 0)
          stats::update(atoms::x_spin_array, atoms::y_spin_array, atoms::z_spin_array, atoms::m_spin_array,
                        atoms::type_array, sim::temperature);
       for (long s : snaps) if (s == step) dump_spins(std::to_string(step));
       for (long s : stat_snaps) if (s == step) dump_stats(std::to_string(step));
+      for (long s : torque_snaps) if (s == step) dump_torque(std::to_string(step));
       if (want_dipole) for (long s : snaps) if (s == step) dump_dipole(std::to_string(step));
       if (mag_every > 0 && step > mag_start && (step - mag_start) % mag_every == 0) {
          double m[4] = {0, 0, 0, 0};
@@ -388,6 +451,19 @@ int main(int argc, char* argv[]) {
    if (want_time) std::cout << "HARNESS_LOOP_SECONDS " << loop_s << " ATOMS " << n << " STEPS " << steps << std::endl;
    if (!mag_trace.empty()) dumpd("mag_trace", mag_trace);
    if (want_derived) dump_derived();
+#ifdef VGPU_MC_HOOK
+   if (g_gpu_mc) gpu::finalize();
+#endif
+   if (sim::integrator == 3 && montecarlo::cmc::is_initialised) {
+      // constrained Monte Carlo: its frame (cmc.cpp polar_rot_matrix) and counters
+      std::vector<double> fr;
+      for (auto& row : montecarlo::cmc::polar_matrix) fr.insert(fr.end(), row.begin(), row.end());
+      for (auto& row : montecarlo::cmc::polar_vector) fr.insert(fr.end(), row.begin(), row.end());
+      dumpd("cmc_frame", fr);
+      std::vector<double> cc = {montecarlo::cmc::mc_total, montecarlo::cmc::mc_success,
+                                montecarlo::cmc::energy_reject, montecarlo::cmc::sphere_reject};
+      dumpd("cmc_counters", cc);
+   }
    std::vector<double> mc = {sim::mc_statistics_moves, sim::mc_statistics_reject};
    dumpd("mc_counters", mc);
    g_manifest.close();

@@ -270,6 +270,24 @@ class OracleSystem:
                                          _p(beta, _D), _p(ratio, _D))
         return s, int(rej)
 
+    def cmc_pairs(self, spins, pairs, rnd, P, pv, M):
+        """The reference's constrained pair-move rule (vref_cmc_pairs) on the
+        given ordered pairs with given random numbers; returns (spins, M,
+        [accepted, energy rejections, sphere rejections])."""
+        s = np.ascontiguousarray(spins, dtype=np.float64).copy()
+        pr = np.ascontiguousarray(pairs, dtype=np.int32).ravel()
+        r = np.ascontiguousarray(rnd, dtype=np.float64)
+        Pm = np.ascontiguousarray(P, dtype=np.float64).ravel()
+        v = np.ascontiguousarray(pv, dtype=np.float64)
+        m = np.ascontiguousarray(M, dtype=np.float64).copy()
+        sig, beta, ratio = self.mc_params()
+        cnt = np.zeros(3, dtype=np.int64)
+        lib().vref_cmc_pairs.restype = None
+        lib().vref_cmc_pairs(C.byref(self.st), _p(s[0], _D), _p(s[1], _D), _p(s[2], _D), _p(pr, _I),
+                             C.c_int(pr.size // 2), _p(r, _D), _p(Pm, _D), _p(v, _D), _p(m, _D), _p(sig, _D),
+                             _p(beta, _D), _p(ratio, _D), cnt.ctypes.data_as(C.POINTER(C.c_long)))
+        return s, m, cnt
+
     def magnetization(self, spins, mask, size) -> np.ndarray:
         s = np.ascontiguousarray(spins, dtype=np.float64)
         mm = np.ascontiguousarray(self.s.mu_s_muB(), dtype=np.float64)

@@ -460,14 +460,83 @@ long vref_mc_colour_sweep(const vref_sys* s, double* sx, double* sy, double* sz,
    return rejects;
 }
 
+/* Constrained Monte Carlo pair moves, the rule of montecarlo::cmc_step
+ * (src/montecarlo/cmc.cpp:282-490) applied to a given ordered list of pairs
+ * (pairs[2k], pairs[2k+1]) with given random numbers rnd[4K] (Gaussians of
+ * the angle move of the first spin in x|y|z blocks of K, then the acceptance
+ * uniforms).  In the frame P (rows: P s rotates the constraint direction to
+ * z; pv the constraint direction) the second spin takes the perpendicular
+ * moment change of the first (scaled by mu1/mu2) so that the moment
+ * perpendicular to pv is kept, its parallel component from |s| = 1 with its
+ * sign kept; rejected outright when that leaves the unit sphere.  Accepted if
+ * exp(-dE) (Mz'/Mz)^2 |s2z/s2z'| >= U and Mz' > 0; M (3, mu_B) is the running
+ * total moment.  counts: [accepted, energy rejections, sphere rejections]. */
+void vref_cmc_pairs(const vref_sys* s, double* sx, double* sy, double* sz, const int* pairs, int K,
+                    const double* rnd, const double* P, const double* pv, double* M, const double* sigma,
+                    const double* beta, const double* ratio, long* counts) {
+   for (int k = 0; k < K; ++k) {
+      const int a1 = pairs[2 * k], a2 = pairs[2 * k + 1];
+      const int m1 = s->type[a1], m2 = s->type[a2];
+      const double mu1 = ratio[m1], mu2 = ratio[m2];
+      const double s1i[3] = {sx[a1], sy[a1], sz[a1]};
+      double s1f[3] = {s1i[0] + rnd[k] * sigma[m1], s1i[1] + rnd[K + k] * sigma[m1], s1i[2] + rnd[2 * K + k] * sigma[m1]};
+      const double r = 1.0 / sqrt(s1f[0] * s1f[0] + s1f[1] * s1f[1] + s1f[2] * s1f[2]);
+      s1f[0] *= r; s1f[1] *= r; s1f[2] *= r;
+      double s1im[3], s1fm[3], s2im[3], s2fm[3];
+      for (int q = 0; q < 3; ++q) {
+         s1im[q] = P[3 * q] * s1i[0] + P[3 * q + 1] * s1i[1] + P[3 * q + 2] * s1i[2];
+         s1fm[q] = P[3 * q] * s1f[0] + P[3 * q + 1] * s1f[1] + P[3 * q + 2] * s1f[2];
+      }
+      double eo[4], en[4];
+      vref_spin_energy(s, sx, sy, sz, a1, s1i[0], s1i[1], s1i[2], eo);
+      sx[a1] = s1f[0]; sy[a1] = s1f[1]; sz[a1] = s1f[2];
+      vref_spin_energy(s, sx, sy, sz, a1, s1f[0], s1f[1], s1f[2], en);
+      const double de1 = ((en[0] + en[1] + en[2] + en[3]) - (eo[0] + eo[1] + eo[2] + eo[3])) * ratio[m1];
+      const double s2i[3] = {sx[a2], sy[a2], sz[a2]};
+      for (int q = 0; q < 3; ++q) s2im[q] = P[3 * q] * s2i[0] + P[3 * q + 1] * s2i[1] + P[3 * q + 2] * s2i[2];
+      const double mr = mu1 / mu2;
+      s2fm[0] = mr * (s1im[0] - s1fm[0]) + s2im[0];
+      s2fm[1] = mr * (s1im[1] - s1fm[1]) + s2im[1];
+      if ((s2fm[0] * s2fm[0] + s2fm[1] * s2fm[1]) < 1.0 && a1 != a2) {
+         s2fm[2] = (s2im[2] >= 0.0 ? 1.0 : -1.0) * sqrt(1.0 - s2fm[0] * s2fm[0] - s2fm[1] * s2fm[1]);
+         double s2f[3];
+         for (int q = 0; q < 3; ++q) s2f[q] = P[q] * s2fm[0] + P[3 + q] * s2fm[1] + P[6 + q] * s2fm[2];
+         vref_spin_energy(s, sx, sy, sz, a2, s2i[0], s2i[1], s2i[2], eo);
+         sx[a2] = s2f[0]; sy[a2] = s2f[1]; sz[a2] = s2f[2];
+         vref_spin_energy(s, sx, sy, sz, a2, s2f[0], s2f[1], s2f[2], en);
+         const double de2 = ((en[0] + en[1] + en[2] + en[3]) - (eo[0] + eo[1] + eo[2] + eo[3])) * ratio[m2];
+         const double de21 = de1 * beta[m1] + de2 * beta[m2];
+         const double mzo = M[0] * pv[0] + M[1] * pv[1] + M[2] * pv[2];
+         double mn[3];
+         for (int q = 0; q < 3; ++q) mn[q] = M[q] + mu1 * s1f[q] + mu2 * s2f[q] - mu1 * s1i[q] - mu2 * s2i[q];
+         const double mzn = mn[0] * pv[0] + mn[1] * pv[1] + mn[2] * pv[2];
+         const double prob = exp(-de21) * ((mzn / mzo) * (mzn / mzo)) * fabs(s2im[2] / s2fm[2]);
+         if (prob >= rnd[3 * K + k] && mzn > 0.0) {
+            M[0] = mn[0]; M[1] = mn[1]; M[2] = mn[2];
+            counts[0]++;
+         } else {
+            sx[a1] = s1i[0]; sy[a1] = s1i[1]; sz[a1] = s1i[2];
+            sx[a2] = s2i[0]; sy[a2] = s2i[1]; sz[a2] = s2i[2];
+            counts[1]++;
+         }
+      } else {
+         sx[a1] = s1i[0]; sy[a1] = s1i[1]; sz[a1] = s1i[2];
+         counts[2]++;
+      }
+   }
+}
+
 /* ------------------------------------------------------------------------
  * FP64 CPU adjoint of the deterministic Heun step (no reference counterpart:
  * the reference has no derivatives).  Loss L = sum_{t=1..N} w (m_z(t) - T_t)^2
  * with m_z the moment-weighted mean of s_z and w the physical time step.
  * Gradients: dL/d(scale of every exchange coupling), dL/dKu_SI (ku2 = Ku/mu_s),
- * dL/dH_applied (3 components, Tesla).  Symmetric exchange only (isotropic or
- * vectorial lists): the transposed gather equals the gather.  Checkpoints
- * every `every` steps, states recomputed per segment.
+ * dL/dH_applied (3 components, Tesla).  Any exchange type and material
+ * set whose couplings are reciprocal in SI units (mu_s,j J_ji = (mu_s,i
+ * J_ij)^T, as the reference's symmetric exchange matrix and three-site DMI
+ * give): the transposed gather sum_j J_ji^T Hbar_j is then mu_s,i times the
+ * gather of Hbar / mu_s.  Checkpoints every `every` steps, states recomputed
+ * per segment.
  * ---------------------------------------------------------------------- */
 static void exch_only(const vref_sys* s, const double* x, const double* y, const double* z, double* hx,
                       double* hy, double* hz) {
@@ -475,6 +544,18 @@ static void exch_only(const vref_sys* s, const double* x, const double* y, const
    memset(hy, 0, sizeof(double) * s->n);
    memset(hz, 0, sizeof(double) * s->n);
    exchange_fields(s, x, y, z, hx, hy, hz);
+}
+
+/* sum_j J_ji^T hb_j = mu_s,i sum_j J_ij (hb_j / mu_s,j) for reciprocal couplings */
+static void exch_transposed(const vref_sys* s, const double* hb, double* out, double* scratch) {
+   const int n = s->n;
+   for (int i = 0; i < n; ++i) {
+      const double r = 1.0 / s->mus[s->type[i]];
+      for (int k = 0; k < 3; ++k) scratch[k * n + i] = hb[k * n + i] * r;
+   }
+   exch_only(s, scratch, scratch + n, scratch + 2 * n, out, out + n, out + 2 * n);
+   for (int i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) out[k * n + i] *= s->mus[s->type[i]];
 }
 
 static void aniso_field(const vref_sys* s, int i, const double S[3], double H[3]) {
@@ -557,6 +638,7 @@ double vref_adjoint(const vref_sys* s, const double* sx0, const double* sy0, con
    double* ub = (double*)malloc(sizeof(double) * 3 * n);
    double* f0 = (double*)malloc(sizeof(double) * 3 * n);
    double* nv = (double*)malloc(sizeof(double) * n);
+   double* f1s = (double*)malloc(sizeof(double) * 3 * n);
    double gJ = 0.0, gK = 0.0, gH[3] = {0, 0, 0};
    /* lambda_N = dL_N/ds_N */
    for (int i = 0; i < n; ++i) lam[2 * n + i] = 2.0 * w * (mz[nsteps] - target[nsteps - 1]) * s->mus[s->type[i]] / musum;
@@ -618,7 +700,7 @@ double vref_adjoint(const vref_sys* s, const double* sx0, const double* sy0, con
             }
          }
          /* s'bar += transposed exchange gather of H1bar + anisotropy */
-         exch_only(s, Hb1, Hb1 + n, Hb1 + 2 * n, tmp, tmp + n, tmp + 2 * n);
+         exch_transposed(s, Hb1, tmp, f1s);
          for (int i = 0; i < n; ++i) {
             const int m = s->type[i];
             const double Si[3] = {S[i], S[n + i], S[2 * n + i]};
@@ -655,7 +737,7 @@ double vref_adjoint(const vref_sys* s, const double* sx0, const double* sy0, con
                gK += 2.0 * he * se / s->mus_SI[m];
             }
          }
-         exch_only(s, Hb0, Hb0 + n, Hb0 + 2 * n, tmp, tmp + n, tmp + 2 * n);
+         exch_transposed(s, Hb0, tmp, f1s);
          for (int i = 0; i < n; ++i) {
             const int m = s->type[i];
             const double Si[3] = {S[i], S[n + i], S[2 * n + i]};
@@ -674,7 +756,7 @@ double vref_adjoint(const vref_sys* s, const double* sx0, const double* sy0, con
    }
    grad[0] = gJ; grad[1] = gK; grad[2] = gH[0]; grad[3] = gH[1]; grad[4] = gH[2];
    free(cp); free(seg); free(mz); free(work); free(cur); free(lam); free(ex0); free(ex1); free(sp);
-   free(Hb1); free(Hb0); free(tmp); free(spb); free(sb); free(ub); free(f0); free(nv);
+   free(Hb1); free(Hb0); free(tmp); free(spb); free(sb); free(ub); free(f0); free(nv); free(f1s);
    return loss;
 }
 

@@ -272,6 +272,207 @@ def mc_sc16_curie():
     print("mc_sc16_curie:", np.round(mean, 3))
 
 
+def _tet_ucf(kind: str) -> str:
+    """Unit-cell file (the reference's .ucf format, src/unitcell/read.cpp and
+    read_interactions.cpp) of a two-atom tetragonal cell, 3 x 3 x 6 A: atom 0
+    (material 1) at the origin, atom 1 (material 2) at z = 1/2, bonds along
+    +-x and +-y to the same sublattice and along +-z to the other.  Every
+    bond direction has its own coupling, so no coupling is a function of the
+    two materials alone: the reference holds it per bond.  kind: isotropic
+    (1 value per bond), vectorial (3) or tensorial (9, with J_ji = J_ij^T and
+    off-diagonal symmetric and antisymmetric parts)."""
+    rng = np.random.default_rng({"isotropic": 1, "vectorial": 2, "tensorial": 3}[kind])
+    bonds = []  # (i, j, dx, dy, dz, key, transpose)
+    for i in (0, 1):
+        for sgn in (1, -1):
+            bonds.append((i, i, sgn, 0, 0, ("x", i), sgn < 0))
+            bonds.append((i, i, 0, sgn, 0, ("y", i), sgn < 0))
+    bonds += [(0, 1, 0, 0, 0, ("z", 0), False), (1, 0, 0, 0, 0, ("z", 0), True),
+              (0, 1, 0, 0, -1, ("z", 1), False), (1, 0, 0, 0, 1, ("z", 1), True)]
+    base = {("x", 0): 11.2, ("y", 0): 8.0, ("x", 1): 6.0, ("y", 1): 13.0, ("z", 0): 10.0, ("z", 1): 4.0}
+    mats = {}
+    for key, j in base.items():
+        m = np.diag(j * (1.0 + 0.25 * rng.uniform(-1, 1, 3))) if kind != "isotropic" else np.eye(3) * j
+        if kind == "tensorial":
+            a = 0.15 * j * rng.uniform(-1, 1, (3, 3))
+            m = m + 0.5 * (a + a.T) + 0.5 * (a - a.T) * 0.8
+        mats[key] = m * 1e-21
+    lines = ["# Unit cell size:", "3.0 3.0 6.0", "# Unit cell vectors:", "1.0 0.0 0.0", "0.0 1.0 0.0",
+             "0.0 0.0 1.0", "# Atoms num, id cx cy cz mat lc hc", "2", "0 0.0 0.0 0.0 0 0 0",
+             "1 0.0 0.0 0.5 1 0 1", "# Interactions n exctype, id i j dx dy dz Jij", f"{len(bonds)} {kind}"]
+    for n, (i, j, dx, dy, dz, key, tr) in enumerate(bonds):
+        m = mats[key].T if tr else mats[key]
+        if kind == "isotropic":
+            vals = [m[0, 0]]
+        elif kind == "vectorial":
+            vals = [m[0, 0], m[1, 1], m[2, 2]]
+        else:
+            vals = list(m.reshape(-1))
+        lines.append(f"{n} {i} {j} {dx} {dy} {dz} " + " ".join(f"{v:.17g}" for v in vals))
+    return "\n".join(lines) + "\n"
+
+
+TET_MAT = """material:num-materials=2
+material[1]:material-name=A
+material[1]:damping-constant=0.1
+material[1]:exchange-matrix[1]=11.2e-21
+material[1]:exchange-matrix[2]=10.0e-21
+material[1]:atomic-spin-moment=1.72 !muB
+material[1]:second-order-uniaxial-anisotropy-constant=6.69e-24
+material[1]:uniaxial-anisotropy-direction=0,0,1
+material[1]:initial-spin-direction=random
+material[2]:material-name=B
+material[2]:damping-constant=0.05
+material[2]:exchange-matrix[1]=10.0e-21
+material[2]:exchange-matrix[2]=11.2e-21
+material[2]:atomic-spin-moment=2.2 !muB
+material[2]:second-order-uniaxial-anisotropy-constant=3.0e-24
+material[2]:uniaxial-anisotropy-direction=0,0.6,0.8
+material[2]:initial-spin-direction=random
+"""
+
+
+def _tet_input(T: float) -> str:
+    return ("material:unit-cell-file=cell.ucf\n" + "".join(f"create:periodic-boundaries-{c}\n" for c in "xyz") +
+            "dimensions:system-size-x=1.8 !nm\ndimensions:system-size-y=1.8 !nm\n"
+            "dimensions:system-size-z=1.8 !nm\nmaterial:file=m.mat\n"
+            f"sim:temperature={T}\nsim:time-step=1.0E-16\nsim:applied-field-strength=0.1 !T\n"
+            "sim:applied-field-unit-vector=0,0,1\nsim:program=time-series\nsim:integrator=llg-heun\n")
+
+
+def _tet_bond(kind: str):
+    files = {"m.mat": TET_MAT, "cell.ucf": _tet_ucf(kind)}
+    d = O.run_harness(_tet_input(0.0), files, ["--system", "--steps", 200, "--snaps", "1,100,200", "--stats", "0,200"])
+    keep = [f"s{c}_{t}" for t in (0, 1, 100, 200) for c in "xyz"]
+    keep += ["mag_system_0", "energy_system_0", "mag_system_200", "energy_system_200", "mag_material_200",
+             "energy_material_200"]
+    save(f"tet_{kind[:3]}_bond_t0", d, keep)
+    d = O.run_harness(_tet_input(300.0), files, ["--system", "--steps", 2, "--snaps", "1,2", "--noise", 2])
+    keep = [f"s{c}_{t}" for t in (0, 1, 2) for c in "xyz"] + ["xi_1", "xi_2"]
+    save(f"tet_{kind[:3]}_bond_t300", d, keep)
+
+
+def tet_bond_exchange():
+    """Per-bond exchange from a unit-cell file (the reference's non-normalised
+    'isotropic', 'vectorial' and 'tensorial' interaction types,
+    src/exchange/unroll.cpp:52-105): tetragonal two-material cell, 6 x 6 x 3
+    cells (216 atoms), periodic, H = 0.1 T; 200 T=0 reference steps with
+    energies, and 2 stochastic steps at 300 K with the Gaussian stream."""
+    for kind in ("isotropic", "vectorial", "tensorial"):
+        _tet_bond(kind)
+
+
+VEC_MAT = SC_MAT.replace("material[1]:exchange-matrix[1]=11.2e-21\n",
+                         "material[1]:exchange-matrix[1]=11.2e-21,8.0e-21,14.0e-21\n")
+
+
+def sc6_vec():
+    """Vectorial exchange from the material file (exchange-matrix with three
+    values: the normalised vectorial form, src/exchange/interface.cpp:86-94,
+    exchange_fields.cpp:82-117) on SC 6^3 periodic: 200 T=0 reference steps
+    with energies, and 2 stochastic steps at 300 K with the Gaussian stream."""
+    d = O.run_harness(sc_input(6), {"m.mat": VEC_MAT},
+                      ["--system", "--steps", 200, "--snaps", "1,100,200", "--stats", "0,200"])
+    keep = [f"s{c}_{t}" for t in (0, 1, 100, 200) for c in "xyz"]
+    keep += ["mag_system_0", "energy_system_0", "mag_system_200", "energy_system_200"]
+    save("sc6_vec_t0", d, keep)
+    d = O.run_harness(sc_input(6, T=300.0), {"m.mat": VEC_MAT}, ["--system", "--steps", 2, "--snaps", "1,2", "--noise", 2])
+    keep = [f"s{c}_{t}" for t in (0, 1, 2) for c in "xyz"] + ["xi_1", "xi_2"]
+    save("sc6_vec_t300", d, keep)
+
+
+def torque_fixtures():
+    """Torque statistics (stats::system_torque, stats::max_torque,
+    src/utility/statistics.cpp:221-325) at T=0: torque_<step> = system
+    torque, per-material torque (x, y, z blocks), max |S x H|.  FCC 4^3 A/B
+    alloy with tensor exchange + DMI + cubic anisotropy at steps 0 and 50;
+    the per-bond tensorial tetragonal cell at steps 0 and 50; FCC 10^3 with
+    the macrocell dipole field at step 0 (fields of the start-up update)."""
+    d = O.run_harness(fcc_input(4, T=0.0), {"m.mat": fcc_mat()},
+                      ["--system", "--steps", 50, "--snaps", "50", "--torque", "0,50"])
+    save("torque_fcc4_t0", d, [f"s{c}_{t}" for t in (0, 50) for c in "xyz"] + ["torque_0", "torque_50"])
+    files = {"m.mat": TET_MAT, "cell.ucf": _tet_ucf("tensorial")}
+    d = O.run_harness(_tet_input(0.0), files, ["--system", "--steps", 50, "--snaps", "50", "--torque", "0,50"])
+    save("torque_tet_t0", d, [f"s{c}_{t}" for t in (0, 50) for c in "xyz"] + ["torque_0", "torque_50"])
+    extra = "cells:macro-cell-size=7.08 !A\ndipole:solver=macrocell\ndipole:field-update-rate=100\n"
+    d = O.run_harness(fcc_input(10, T=0.0, extra=extra), {"m.mat": fcc_mat()},
+                      ["--system", "--steps", 0, "--dipole", "--torque", "0"])
+    keep = DIPOLE_KEYS + [f"s{c}_0" for c in "xyz"] + ["torque_0"]
+    keep += [f"{q}_{c}_0" for q in ("cmag", "cfield", "chd") for c in "xyz"]
+    save("torque_fcc10_dipole", d, keep)
+
+
+CMC_TEMPS = (400.0, 900.0)
+CMC_EQ, CMC_AV, CMC_EVERY = 2000, 20000, 10
+
+
+def cmc_sc12():
+    """Constrained Monte Carlo (montecarlo::cmc_step, src/montecarlo/cmc.cpp:
+    282-490; sim:integrator=constrained-monte-carlo, angle moves) on SC 12^3
+    periodic with the config-0 material, H = 0, constraint direction
+    phi = 30, theta = 45 degrees: the reference's own chain at 400 K and
+    900 K, 2,000 + 20,000 steps (N pair moves each), m sampled every 10
+    steps; its constraint frame and move counters."""
+    out = {}
+    for T in CMC_TEMPS:
+        inp = sc_input(12, T=T, H=0.0, integrator="constrained-monte-carlo",
+                       extra="montecarlo:algorithm=angle\nsim:constraint-angle-phi=30\nsim:constraint-angle-theta=45\n")
+        d = O.run_harness(inp, {"m.mat": SC_MAT}, ["--system", "--steps", CMC_EQ + CMC_AV, "--mag-every", CMC_EVERY,
+                                                   "--mag-start", CMC_EQ], timeout=3600)
+        tag = f"{int(T)}"
+        out[f"m_trace_{tag}"] = d["mag_trace"].reshape(-1, 4)[:, :3].astype(np.float64)
+        out[f"counters_{tag}"] = d["cmc_counters"]
+        out["cmc_frame"] = d["cmc_frame"]
+        for k in SYSTEM_KEYS:
+            if k in d:
+                out[k] = d[k]
+    out["T"] = np.array(CMC_TEMPS)
+    out["sweeps"] = np.array([CMC_EQ, CMC_AV, CMC_EVERY])
+    np.savez_compressed(HERE / "cmc_sc12.npz", **out)
+    print("cmc_sc12:", {T: out[f"counters_{int(T)}"] for T in CMC_TEMPS})
+
+
+MC50_EQ, MC50_AV = 5000, 10000
+
+
+def _mc50_one(T):
+    inp = sc_input(50, T=T, H=0.0, integrator="monte-carlo", extra="montecarlo:algorithm=angle\n")
+    return O.run_harness(inp, {"m.mat": MC_MAT}, ["--system", "--steps", MC50_EQ + MC50_AV, "--mag-every", MC_EVERY,
+                                                  "--mag-start", MC50_EQ], timeout=14400)
+
+
+def mc_sc50_curie():
+    """The Curie-sweep workload at its own size: the reference's sequential
+    random-site Metropolis (montecarlo::mc_step, angle moves) on SC 50^3
+    periodic (125,000 spins), config-0 material, H=0, spins start along z, 31
+    temperatures 0..1500 K, 5,000 equilibration + 10,000 averaging sweeps,
+    |m| sampled every 10 sweeps.  One reference process per temperature
+    (about 15 minutes each on one core).  The whole |m| series is kept so
+    that a test can choose its blocking; m_se is from 10 blocks of 1,000
+    sweeps."""
+    from concurrent.futures import ThreadPoolExecutor
+    import os
+    workers = int(os.environ.get("MC50_WORKERS", os.cpu_count() or 4))
+    with ThreadPoolExecutor(workers) as ex:
+        runs = list(ex.map(_mc50_one, MC_TEMPS))
+    mean, se, acc, traces = [], [], [], []
+    for d in runs:
+        tr = d["mag_trace"].reshape(-1, 4)[:, 3]
+        m, e = blocking_stats(tr)
+        mean.append(m)
+        se.append(e)
+        traces.append(tr)
+        mv, rj = d["mc_counters"]
+        acc.append(1.0 - rj / mv)
+    d0 = runs[0]
+    out = {k: d0[k] for k in ("meta", "materials", "sim", "m_spin")}
+    out.update(T=np.array(MC_TEMPS), m_mean=np.array(mean), m_se=np.array(se), acceptance=np.array(acc),
+               m_trace=np.array(traces, dtype=np.float32), L=np.array(50),
+               sweeps=np.array([MC50_EQ, MC50_AV, MC_EVERY]))
+    np.savez_compressed(HERE / "mc_sc50_curie.npz", **out)
+    print("mc_sc50_curie:", np.round(mean, 4))
+
+
 def sc8_config():
     """The reference program's own configuration output (binary spin
     snapshots, src/config/atoms_spins.cpp) for the sc8_t0 input: the stock
@@ -297,6 +498,7 @@ def sc8_config():
 
 
 ALL = [sc20_t0, sc8_t0, sc10_t300, sc6_open_t300, fcc4_dmi_t300, fcc4_dmi_t0, single_spin_applied, mc_sc16_curie,
+       mc_sc50_curie, tet_bond_exchange, sc6_vec, torque_fixtures, cmc_sc12,
        fcc10_dipole_tensor, fcc10_dipole_macrocell, sc6_aniso_ho, fcc4_neel_rot, sc6_derived_t600, sc8_midpoint, sc6_biquadratic,
        sc8_config]
 

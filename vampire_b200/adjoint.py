@@ -6,7 +6,10 @@ s_z after step t, and its gradient with respect to the exchange constant J
 (every coupling scaled together), the uniaxial constant Ku and the applied
 field (Hx, Hy, Hz) comes from the hand-written adjoint kernels of
 libvgpu.so (vgpu_adjoint_llg, sqrt(N)-step checkpointing with recomputation),
-wrapped as a torch.autograd.Function for fitting.
+wrapped as a torch.autograd.Function for fitting.  For systems of several
+materials, and tensor or DMI couplings, loss_and_grad_materials adds the
+gradients with respect to each material pair's exchange constant and the
+DMI strength (vgpu_adjoint_llg_materials).
 
 The benchmark problem: simple-cubic 32^3 periodic, T = 0, alpha = 0.1,
 dt = 1e-16 s, 2,000 steps, seeded initial state tilted 30 degrees from z;
@@ -70,6 +73,32 @@ class AdjointRunner:
         with V.Simulation(s, device=self.device, precision="fp64") as sim:
             sim._check(V.lib().vgpu_mz_trajectory(sim.handle, C.c_uint64(n_steps), out.ctypes.data_as(V._D)))
         return out
+
+
+def loss_and_grad_materials(s: S.SpinSystem, target: np.ndarray, device: int = 0, every: int = 0):
+    """Adjoint of the trajectory loss of any system (FP64 device build, at
+    most 8 materials, reciprocal couplings; vgpu_adjoint_llg_materials).
+    Returns (loss, grad[5] as vgpu_adjoint_llg, dL/d(DMI scale),
+    pair[M, M] = dL/d(scale of the couplings from material a to b)).  For
+    an exchange matrix J_SI, dL/dJ_ab = pair[a, b] / J_SI[a, b]."""
+    M = s.materials.size
+    tg = np.ascontiguousarray(target, dtype=np.float64)
+    g = np.zeros(5)
+    pair = np.zeros(1 + M * M)
+    loss = C.c_double()
+    with V.Simulation(s, device=device, precision="fp64") as sim:
+        sim._check(V.lib().vgpu_adjoint_llg_materials(
+            sim.handle, C.c_uint64(tg.size), tg.ctypes.data_as(V._D), C.c_double(s.params.dt_SI), C.c_int32(every),
+            C.byref(loss), g.ctypes.data_as(V._D), pair.ctypes.data_as(V._D)))
+    return loss.value, g, float(pair[0]), pair[1:].reshape(M, M)
+
+
+def mz_trajectory(s: S.SpinSystem, n_steps: int, device: int = 0) -> np.ndarray:
+    """m_z(t), t = 1..n_steps, of the device FP64 forward run of system s."""
+    out = np.zeros(n_steps)
+    with V.Simulation(s, device=device, precision="fp64") as sim:
+        sim._check(V.lib().vgpu_mz_trajectory(sim.handle, C.c_uint64(n_steps), out.ctypes.data_as(V._D)))
+    return out
 
 
 def torch_loss_fn(runner: AdjointRunner, target: np.ndarray):

@@ -10,11 +10,23 @@
 // backwards with four fused per-atom kernels per step: (1) recompute H(s), f,
 // s'; (2) recompute H(s'), f', s1 and push lambda through n(u), f' and H(s');
 // (3) the transposed exchange gather of H(s')-bar, through n(v), f and H(s);
-// (4) the transposed gather of H(s)-bar plus dL_t/ds_t gives lambda_t.  For the
-// symmetric couplings accepted here (isotropic or vectorial lists,
-// J_ij = J_ji) the transposed gather is the forward SELL gather.  Parameter
-// gradients (every coupling scaled together, Ku, H_app) are block-reduced and
-// accumulated in FP64.  States are checkpointed every ceil(sqrt(N)) steps and
+// (4) the transposed gather of H(s)-bar plus dL_t/ds_t gives lambda_t.
+//
+// Transposed gather.  The reference normalises every coupling by the moment of
+// its own atom (J_ij [T] = J_SI,ij / mu_s,i, exchange/unroll_normalised.cpp),
+// and its couplings are reciprocal in SI units (J_SI,ji = J_SI,ij^T: a
+// symmetric exchange matrix; the three-site DMI vector changes sign with the
+// bond).  So J_ji^T = (mu_s,i / mu_s,j) J_ij and the adjoint's
+// sum_j J_ji^T Hbar_j = mu_s,i sum_j J_ij (Hbar_j / mu_s,j): the forward SELL
+// gather of Hbar / mu_s, in every exchange format (isotropic, vectorial,
+// diagonal + DMI, full tensor).  A device check before the run refuses
+// couplings that are not reciprocal.
+//
+// Parameter gradients, block-reduced and accumulated in FP64: every coupling
+// scaled together, Ku, H_app; and per pair of materials (a, b) the scale of
+// the couplings of the bonds from atoms of a to atoms of b (the diagonal,
+// exchange-matrix part for the diagonal + DMI format), plus the common scale
+// of the DMI vectors.  States are checkpointed every ceil(sqrt(N)) steps and
 // recomputed segment by segment with the FP64 forward kernels.
 #include <cuda_runtime.h>
 
@@ -32,6 +44,7 @@ struct AdjBufs {
    double *sp, *ex0, *ex1, *f0, *ub, *spb, *sb, *Hb0, *Hb1, *lam;   // [3n] each, x|y|z blocks
    double* nv;                  // [n] |v|
    double* g;                   // [5] dL/d(J scale), dL/dKu, dL/dH
+   double* gp;                  // [1 + M*M] dL/d(DMI scale), dL/d(scale of the a->b couplings), or nullptr
    const double* mz;            // [N+1]
    const double* target;        // [N]
    double w, musum;
@@ -99,6 +112,113 @@ __device__ __forceinline__ void grad_add(double v[5], double* g) {
    }
 }
 
+// coupling of SELL entry e (row atom material mi, neighbour material mj) as
+// a 3x3 matrix, row-major, in the FP64 build's formats
+template <int FMT>
+__device__ __forceinline__ void bond_tensor(const LLGArgs<double>& a, int e, int mi, int mj, double T[9]) {
+#pragma unroll
+   for (int k = 0; k < 9; ++k) T[k] = 0.0;
+   if (FMT == FMT_ISO_TAB) {
+      T[0] = T[4] = T[8] = a.jtab[mi * a.M + mj];
+   } else if (FMT == FMT_ISO_BOND) {
+      T[0] = T[4] = T[8] = a.jb[0][e];
+   } else if (FMT == FMT_VEC_TAB || FMT == FMT_DMI_TAB) {
+      const double* t = a.jtab + 3 * (mi * a.M + mj);
+      T[0] = t[0]; T[4] = t[1]; T[8] = t[2];
+      if (FMT == FMT_DMI_TAB) {  // d x s: [[0, -dz, dy], [dz, 0, -dx], [-dy, dx, 0]]
+         const double dx = a.jb[0][e], dy = a.jb[1][e], dz = a.jb[2][e];
+         T[1] = -dz; T[2] = dy; T[3] = dz; T[5] = -dx; T[6] = -dy; T[7] = dx;
+      }
+   } else if (FMT == FMT_VEC_BOND) {
+      T[0] = a.jb[0][e]; T[4] = a.jb[1][e]; T[8] = a.jb[2][e];
+   } else {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) T[k] = a.jb[k][e];
+   }
+}
+
+__device__ __forceinline__ int nb_material(const LLGArgs<double>& a, int c, int j) {
+   return a.mat_shift ? (c >> a.mat_shift) : (a.mat ? a.mat[j] : 0);
+}
+
+// Parameter gradients of one atom's exchange field: hb . (J_ij s_j) summed
+// per material pair (diagonal part for the DMI format) into sp[1 + mi*M + mj]
+// and hb . (d_ij x s_j) into sp[0] (shared memory, this block's sums)
+template <int FMT>
+__device__ __forceinline__ void pair_grads(const LLGArgs<double>& a, int i, int mi, const double* sx,
+                                           const double* sy, const double* sz, const double hb[3], double* sp) {
+   const int sl = i >> 5, lane = i & 31;
+   const int off = a.slice_off[sl];
+   const int w = (a.slice_off[sl + 1] - off) >> 5;
+   double dm = 0.0;
+   for (int k = 0; k < w; ++k) {
+      const int e = off + lane + 32 * k;
+      const int c = a.col[e];
+      const int j = c & a.idx_mask;
+      if (j >= a.n) continue;  // padding entry
+      const int mj = nb_material(a, c, j);
+      const double s[3] = {sx[j], sy[j], sz[j]};
+      double T[9];
+      bond_tensor<FMT>(a, e, mi, mj, T);
+      const double diag = hb[0] * T[0] * s[0] + hb[1] * T[4] * s[1] + hb[2] * T[8] * s[2];
+      const double off_d = hb[0] * (T[1] * s[1] + T[2] * s[2]) + hb[1] * (T[3] * s[0] + T[5] * s[2]) +
+                           hb[2] * (T[6] * s[0] + T[7] * s[1]);
+      if (FMT == FMT_DMI_TAB) {
+         atomicAdd(sp + 1 + mi * a.M + mj, diag);
+         dm += off_d;
+      } else {
+         atomicAdd(sp + 1 + mi * a.M + mj, diag + off_d);
+      }
+   }
+   if (FMT == FMT_DMI_TAB) atomicAdd(sp, dm);
+}
+
+// Reciprocity of the couplings in SI units: for every bond i -> j, the sum of
+// mu_s,i J_ij over the bonds of row i to j equals the transpose of the sum of
+// mu_s,j J_ji over the bonds of row j to i (to 1e-10 of its largest entry).
+// Sets *bad = 1 + i at a failing atom.
+template <int FMT>
+__global__ void adj_reciprocal_kernel(const LLGArgs<double> a, int* bad) {
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= a.n) return;
+   const int mi = a.mat ? a.mat[i] : 0;
+   const double mui = a.mp[mi].mu_s_muB;
+   const int off = a.slice_off[i >> 5], w = (a.slice_off[(i >> 5) + 1] - off) >> 5;
+   for (int k = 0; k < w; ++k) {
+      const int c = a.col[off + (i & 31) + 32 * k];
+      const int j = c & a.idx_mask;
+      if (j >= a.n) continue;
+      const int mj = a.mat ? a.mat[j] : 0;
+      const double muj = a.mp[mj].mu_s_muB;
+      double Sij[9] = {0}, Sji[9] = {0}, T[9];
+      for (int q = 0; q < w; ++q) {
+         const int e = off + (i & 31) + 32 * q;
+         const int cq = a.col[e];
+         if ((cq & a.idx_mask) != j) continue;
+         bond_tensor<FMT>(a, e, mi, nb_material(a, cq, j), T);
+         for (int r = 0; r < 9; ++r) Sij[r] += mui * T[r];
+      }
+      const int offj = a.slice_off[j >> 5], wj = (a.slice_off[(j >> 5) + 1] - offj) >> 5;
+      for (int q = 0; q < wj; ++q) {
+         const int e = offj + (j & 31) + 32 * q;
+         const int cq = a.col[e];
+         if ((cq & a.idx_mask) != i) continue;
+         bond_tensor<FMT>(a, e, mj, nb_material(a, cq, i), T);
+         for (int r = 0; r < 9; ++r) Sji[r] += muj * T[r];
+      }
+      double mx = 0.0, dv = 0.0;
+      for (int r = 0; r < 3; ++r)
+         for (int s = 0; s < 3; ++s) {
+            mx = fmax(mx, fabs(Sij[3 * r + s]));
+            dv = fmax(dv, fabs(Sij[3 * r + s] - Sji[3 * s + r]));
+         }
+      if (dv > 1e-10 * mx) {
+         atomicCAS(bad, 0, 1 + i);
+         return;
+      }
+   }
+}
+
 template <int FMT>
 __global__ void __launch_bounds__(256) adj_k1(const LLGArgs<double> a, AdjBufs b) {
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -124,11 +244,29 @@ __global__ void __launch_bounds__(256) adj_k1(const LLGArgs<double> a, AdjBufs b
    for (int k = 0; k < 3; ++k) b.sp[k * st + i] = v[k] / L;
 }
 
+// shared sums of the pair gradients: [1 + M*M] (M <= kAdjMaxPairMat)
+constexpr int kAdjMaxPairMat = 8;
+
+__device__ __forceinline__ void pair_init(double* sp, const AdjBufs& b, int M) {
+   if (b.gp)
+      for (int k = threadIdx.x; k < 1 + M * M; k += blockDim.x) sp[k] = 0.0;
+   __syncthreads();
+}
+
+__device__ __forceinline__ void pair_flush(const double* sp, const AdjBufs& b, int M) {
+   if (!b.gp) return;
+   __syncthreads();
+   for (int k = threadIdx.x; k < 1 + M * M; k += blockDim.x)
+      if (sp[k] != 0.0) atomicAdd(b.gp + k, sp[k]);
+}
+
 template <int FMT>
 __global__ void __launch_bounds__(256) adj_k2(const LLGArgs<double> a, AdjBufs b) {
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    const int st = b.stride;
    double gv[5] = {0, 0, 0, 0, 0};
+   __shared__ double sp[1 + kAdjMaxPairMat * kAdjMaxPairMat];
+   pair_init(sp, b, a.M);
    if (i < b.n) {
       const int mi = a.mat ? a.mat[i] : 0;
       const MatParams<double> m = a.mp[mi];
@@ -148,20 +286,23 @@ __global__ void __launch_bounds__(256) adj_k2(const LLGArgs<double> a, AdjBufs b
       double u_b[3], a1[3], sdir[3], hb[3];
       for (int k = 0; k < 3; ++k) { u_b[k] = (l[k] - ls * s1[k]) / L; a1[k] = 0.5 * a.dt * u_b[k]; }
       f_vjp_d(m.A, m.B, Sp, H1, a1, sdir, hb);
+      const double imu = 1.0 / (double)m.mu_s_muB;  // Hbar / mu_s for the transposed gather
       for (int k = 0; k < 3; ++k) {
          b.ub[k * st + i] = u_b[k];
          b.spb[k * st + i] = sdir[k];
-         b.Hb1[k * st + i] = hb[k];
+         b.Hb1[k * st + i] = hb[k] * imu;
          b.ex1[k * st + i] = ex[k];
          gv[0] += hb[k] * ex[k];
          gv[2 + k] += hb[k];
       }
+      if (b.gp) pair_grads<FMT>(a, i, mi, b.sp, b.sp + st, b.sp + 2 * st, hb, sp);
       if (a.uniaxial) {
          const double he = hb[0] * m.kux + hb[1] * m.kuy + hb[2] * m.kuz;
          const double se = Sp[0] * m.kux + Sp[1] * m.kuy + Sp[2] * m.kuz;
          gv[1] += 2.0 * he * se / ((double)m.mu_s_muB * 9.27400915e-24);
       }
    }
+   pair_flush(sp, b, a.M);
    grad_add(gv, b.g);
 }
 
@@ -170,16 +311,19 @@ __global__ void __launch_bounds__(256) adj_k3(const LLGArgs<double> a, AdjBufs b
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    const int st = b.stride;
    double gv[5] = {0, 0, 0, 0, 0};
+   __shared__ double sp[1 + kAdjMaxPairMat * kAdjMaxPairMat];
+   pair_init(sp, b, a.M);
    if (i < b.n) {
       const int mi = a.mat ? a.mat[i] : 0;
       const MatParams<double> m = a.mp[mi];
+      const double mu = (double)m.mu_s_muB;
       const double S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
       const double Sp[3] = {b.sp[i], b.sp[st + i], b.sp[2 * st + i]};
       double t[3] = {0, 0, 0};
       exchange_gather<double, FMT>(a, i, mi, b.Hb1, b.Hb1 + st, b.Hb1 + 2 * st, t[0], t[1], t[2]);
-      const double hb1[3] = {b.Hb1[i], b.Hb1[st + i], b.Hb1[2 * st + i]};
+      const double hb1[3] = {b.Hb1[i] * mu, b.Hb1[st + i] * mu, b.Hb1[2 * st + i] * mu};
       double spbar[3];
-      for (int k = 0; k < 3; ++k) spbar[k] = b.spb[k * st + i] + t[k];
+      for (int k = 0; k < 3; ++k) spbar[k] = b.spb[k * st + i] + t[k] * mu;
       aniso_vjp_d(a, m, Sp, hb1, spbar);
       const double sps = spbar[0] * Sp[0] + spbar[1] * Sp[1] + spbar[2] * Sp[2];
       double vb[3], a0[3];
@@ -198,16 +342,18 @@ __global__ void __launch_bounds__(256) adj_k3(const LLGArgs<double> a, AdjBufs b
       f_vjp_d(m.A, m.B, S, H0, a0, sdir, hb);
       for (int k = 0; k < 3; ++k) {
          b.sb[k * st + i] = b.ub[k * st + i] + vb[k] + sdir[k];
-         b.Hb0[k * st + i] = hb[k];
+         b.Hb0[k * st + i] = hb[k] / mu;
          gv[0] += hb[k] * ex[k];
          gv[2 + k] += hb[k];
       }
+      if (b.gp) pair_grads<FMT>(a, i, mi, b.S, b.S + st, b.S + 2 * st, hb, sp);
       if (a.uniaxial) {
          const double he = hb[0] * m.kux + hb[1] * m.kuy + hb[2] * m.kuz;
          const double se = S[0] * m.kux + S[1] * m.kuy + S[2] * m.kuz;
          gv[1] += 2.0 * he * se / ((double)m.mu_s_muB * 9.27400915e-24);
       }
    }
+   pair_flush(sp, b, a.M);
    grad_add(gv, b.g);
 }
 
@@ -219,11 +365,12 @@ __global__ void __launch_bounds__(256) adj_k4(const LLGArgs<double> a, AdjBufs b
    const int mi = a.mat ? a.mat[i] : 0;
    const MatParams<double> m = a.mp[mi];
    const double S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
+   const double mu = (double)m.mu_s_muB;
    double tg[3] = {0, 0, 0};
    exchange_gather<double, FMT>(a, i, mi, b.Hb0, b.Hb0 + st, b.Hb0 + 2 * st, tg[0], tg[1], tg[2]);
-   const double hb0[3] = {b.Hb0[i], b.Hb0[st + i], b.Hb0[2 * st + i]};
+   const double hb0[3] = {b.Hb0[i] * mu, b.Hb0[st + i] * mu, b.Hb0[2 * st + i] * mu};
    double l[3];
-   for (int k = 0; k < 3; ++k) l[k] = b.sb[k * st + i] + tg[k];
+   for (int k = 0; k < 3; ++k) l[k] = b.sb[k * st + i] + tg[k] * mu;
    aniso_vjp_d(a, m, S, hb0, l);
    if (t >= 1) l[2] += 2.0 * b.w * (b.mz[t] - b.target[t - 1]) * (double)m.mu_s_muB / b.musum;
    for (int k = 0; k < 3; ++k) b.lam[k * st + i] = l[k];
@@ -271,8 +418,23 @@ static void adj_step_fmt(int fmt, const LLGArgs<double>& a, const AdjBufs& b, in
       case FMT_ISO_TAB: adj_step<FMT_ISO_TAB>(a, b, t, st); break;
       case FMT_ISO_BOND: adj_step<FMT_ISO_BOND>(a, b, t, st); break;
       case FMT_VEC_TAB: adj_step<FMT_VEC_TAB>(a, b, t, st); break;
-      default: adj_step<FMT_VEC_BOND>(a, b, t, st); break;
+      case FMT_VEC_BOND: adj_step<FMT_VEC_BOND>(a, b, t, st); break;
+      case FMT_DMI_TAB: adj_step<FMT_DMI_TAB>(a, b, t, st); break;
+      default: adj_step<FMT_TENSOR_BOND>(a, b, t, st); break;
    }
+}
+
+static cudaError_t launch_reciprocal(int fmt, const LLGArgs<double>& a, int* bad, cudaStream_t st) {
+   const int g = (a.n + 127) / 128;
+   switch (fmt) {
+      case FMT_ISO_TAB: adj_reciprocal_kernel<FMT_ISO_TAB><<<g, 128, 0, st>>>(a, bad); break;
+      case FMT_ISO_BOND: adj_reciprocal_kernel<FMT_ISO_BOND><<<g, 128, 0, st>>>(a, bad); break;
+      case FMT_VEC_TAB: adj_reciprocal_kernel<FMT_VEC_TAB><<<g, 128, 0, st>>>(a, bad); break;
+      case FMT_VEC_BOND: adj_reciprocal_kernel<FMT_VEC_BOND><<<g, 128, 0, st>>>(a, bad); break;
+      case FMT_DMI_TAB: adj_reciprocal_kernel<FMT_DMI_TAB><<<g, 128, 0, st>>>(a, bad); break;
+      default: adj_reciprocal_kernel<FMT_TENSOR_BOND><<<g, 128, 0, st>>>(a, bad); break;
+   }
+   return cudaGetLastError();
 }
 
 }  // namespace vgpu
@@ -303,9 +465,6 @@ int check_adjoint_ok(vgpu_ctx* h) {
    if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
    if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
    if (h->prec != VGPU_PREC_FP64) return set_err(h, VGPU_ERR_ARG, "the adjoint runs in the FP64 build (VGPU_PREC_FP64)");
-   const int f = h->sys.fmt;
-   if (f != FMT_ISO_TAB && f != FMT_ISO_BOND && f != FMT_VEC_TAB && f != FMT_VEC_BOND)
-      return set_err(h, VGPU_ERR_ARG, "the adjoint supports symmetric (isotropic or vectorial) exchange only");
    if (h->sys.cell || h->sys.hd_atom || h->sys.sys_off)
       return set_err(h, VGPU_ERR_ARG, "the adjoint does not support dipole fields or batches");
    if (h->params.local_applied_field) return set_err(h, VGPU_ERR_ARG, "the adjoint supports the global applied field only");
@@ -352,26 +511,50 @@ extern "C" int vgpu_mz_trajectory(vgpu_handle h, uint64_t n_steps, double* mz_ou
    return VGPU_OK;
 }
 
-extern "C" int vgpu_adjoint_llg(vgpu_handle h, uint64_t n_steps, const double* target, double w, int32_t every,
-                                double* loss_out, double* grad_out) {
+// the couplings must be reciprocal in SI units for the transposed gather
+static int check_reciprocal(vgpu_ctx* h) {
+   int* bad = nullptr;
+   cudaError_t e = cudaMalloc(&bad, sizeof(int));
+   if (e != cudaSuccess) return cuda_err(h, e, "adjoint check");
+   int hb = 0;
+   e = cudaMemsetAsync(bad, 0, sizeof(int), h->stream);
+   if (e == cudaSuccess) e = launch_reciprocal(h->sys.fmt, make_args<double>(h), bad, h->stream);
+   if (e == cudaSuccess) e = cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+   cudaFree(bad);
+   if (e != cudaSuccess) return cuda_err(h, e, "adjoint check");
+   h->kernel_launches++;
+   if (hb)
+      return set_err(h, VGPU_ERR_ARG,
+                     "the adjoint needs reciprocal couplings (mu_s,j J_ji = (mu_s,i J_ij)^T); atom %d breaks it", hb - 1);
+   return VGPU_OK;
+}
+
+static int adjoint_run(vgpu_handle h, uint64_t n_steps, const double* target, double w, int32_t every,
+                       double* loss_out, double* grad_out, double* pair_out) {
    int rc = check_adjoint_ok(h);
    if (rc) return rc;
    if (!target || !loss_out || !grad_out || n_steps == 0) return set_err(h, VGPU_ERR_ARG, "bad adjoint arguments");
    cudaSetDevice(h->device);
+   if ((rc = check_reciprocal(h))) return rc;
+   const int M = h->sys.M;
+   if (pair_out && M > kAdjMaxPairMat)
+      return set_err(h, VGPU_ERR_ARG, "per-material gradients support at most %d materials", kAdjMaxPairMat);
    SysDev& S = h->sys;
    const int n = S.n, st = S.n_alloc;
    const int64_t N = (int64_t)n_steps;
    const int64_t C = every > 0 ? every : (int64_t)std::ceil(std::sqrt((double)N));
    const int64_t ncp = (N + C - 1) / C;
    const size_t v3 = 3 * (size_t)st;
+   const int np = 1 + M * M;
    DevVec cp, seg, pb, eb, mz, tg, g, work;
    cudaError_t e;
    if ((e = cp.alloc(v3 * ncp)) || (e = seg.alloc(v3 * (C + 1))) || (e = pb.alloc(v3)) || (e = eb.alloc(v3)) ||
-       (e = mz.alloc(N + 1)) || (e = tg.alloc(N)) || (e = g.alloc(5)) || (e = work.alloc(v3 * 10 + st)))
+       (e = mz.alloc(N + 1)) || (e = tg.alloc(N)) || (e = g.alloc(5 + np)) || (e = work.alloc(v3 * 10 + st)))
       return cuda_err(h, e, "adjoint buffers");
    cudaMemcpyAsync(tg.p, target, sizeof(double) * N, cudaMemcpyHostToDevice, h->stream);
    cudaMemsetAsync(mz.p, 0, sizeof(double) * (N + 1), h->stream);
-   cudaMemsetAsync(g.p, 0, sizeof(double) * 5, h->stream);
+   cudaMemsetAsync(g.p, 0, sizeof(double) * (5 + np), h->stream);
    LLGArgs<double> a = make_args<double>(h);
    a.thermal = 0;
    // forward from the current spins (left untouched), checkpoint every C steps
@@ -406,6 +589,7 @@ extern "C" int vgpu_adjoint_llg(vgpu_handle h, uint64_t n_steps, const double* t
    b.spb = wk + 5 * v3; b.sb = wk + 6 * v3; b.Hb0 = wk + 7 * v3; b.Hb1 = wk + 8 * v3; b.lam = wk + 9 * v3;
    b.nv = wk + 10 * v3;
    b.g = g.p; b.mz = mz.p; b.target = tg.p; b.w = w; b.musum = musum; b.n = n; b.stride = st;
+   b.gp = pair_out ? g.p + 5 : nullptr;
    adj_lambda_init<<<(n + 255) / 256, 256, 0, h->stream>>>(a, b, N);
    for (int64_t c = ncp - 1; c >= 0; --c) {
       const int64_t t0 = c * C, t1 = std::min(t0 + C, N);
@@ -422,11 +606,24 @@ extern "C" int vgpu_adjoint_llg(vgpu_handle h, uint64_t n_steps, const double* t
       }
       if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(h, e, "adjoint backward");
    }
-   double gh[5];
-   e = cudaMemcpyAsync(gh, g.p, sizeof gh, cudaMemcpyDeviceToHost, h->stream);
+   std::vector<double> gh(5 + np);
+   e = cudaMemcpyAsync(gh.data(), g.p, sizeof(double) * gh.size(), cudaMemcpyDeviceToHost, h->stream);
    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
    if (e != cudaSuccess) return cuda_err(h, e, "adjoint result");
    *loss_out = loss;
    for (int k = 0; k < 5; ++k) grad_out[k] = gh[k];
+   if (pair_out)
+      for (int k = 0; k < np; ++k) pair_out[k] = gh[5 + k];
    return VGPU_OK;
+}
+
+extern "C" int vgpu_adjoint_llg(vgpu_handle h, uint64_t n_steps, const double* target, double w, int32_t every,
+                                double* loss_out, double* grad_out) {
+   return adjoint_run(h, n_steps, target, w, every, loss_out, grad_out, nullptr);
+}
+
+extern "C" int vgpu_adjoint_llg_materials(vgpu_handle h, uint64_t n_steps, const double* target, double w,
+                                          int32_t every, double* loss_out, double* grad_out, double* pair_out) {
+   if (!pair_out) return set_err(h, VGPU_ERR_ARG, "null pair gradient output");
+   return adjoint_run(h, n_steps, target, w, every, loss_out, grad_out, pair_out);
 }

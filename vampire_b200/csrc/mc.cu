@@ -169,9 +169,12 @@ static cudaError_t mc_dispatch(const MCArgs<R>& p, int fmt, cudaStream_t st) {
    }
 }
 
+void cmc_destroy(vgpu_ctx* h);
+
 void mc_destroy(vgpu_ctx* h) {
    MCState* s = mc_of(h);
    if (!s) return;
+   cmc_destroy(h);  // its pairing follows this colouring
    cudaFree(s->atoms);
    cudaFree(s->rejects);
    cudaFree(s->replay);
@@ -420,5 +423,499 @@ extern "C" int vgpu_mc_counters(vgpu_handle h, double* moves, double* rejects) {
    if (e != cudaSuccess) return cuda_err(h, e, "mc counters");
    if (moves) *moves = s->moves;
    if (rejects) *rejects = (double)r;
+   return VGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Constrained Monte Carlo (reference: montecarlo::cmc_step,
+// src/montecarlo/cmc.cpp:282-490; CMCinit and polar_rot_matrix, :53-270).
+//
+// The reference makes N pair moves per step: a random spin takes an angle
+// move, a second random spin compensates the moment perpendicular to the
+// constraint direction, and the pair is accepted with probability
+// exp(-dE/kT) (Mz'/Mz)^2 |s2z/s2z'| (and Mz' > 0), where Mz is the total
+// moment along the constraint -- every decision depends on all earlier ones
+// through Mz.  Here a step is phases over the colours of the exchange graph,
+// twice over (about N pairs, as the reference): in a phase the atoms of one
+// colour are paired by a random affine permutation of that colour's list, so
+// no atom of any pair interacts with an atom of another pair, and
+//
+//   propose  (one thread per pair)  the move, the compensating spin, both
+//            energy changes, exp(-dE) and the Jacobian factor, and the moment
+//            terms mu s of both spins before and after;
+//   accept   (one warp)  the pairs in order with the running total moment,
+//            exactly the reference's rule: a pair's energy change does not
+//            depend on the other pairs of the phase, so the sequence of
+//            decisions is that of the sequential chain for this order of
+//            pairs; lanes then write the accepted spins.
+//
+// Every pair move keeps the target distribution (the reference's
+// Metropolis-Hastings step with its constraint Jacobian), so the phases
+// sample it too; pair selection differs from the reference's (random pairs
+// with replacement), so the two are compared statistically.
+// ---------------------------------------------------------------------------
+
+namespace vgpu {
+
+struct CMCState {
+   double P[9] = {0}, pv[3] = {0, 0, 1};   // frame: P rotates the constraint direction to z
+   int maxK = 0;
+   int* pairs = nullptr;      // [2 maxK]
+   void* prop = nullptr;      // [6 maxK] proposed spins s1', s2' (x|y|z of each, R)
+   double* ef = nullptr;      // [maxK] exp(-dE) (negative: sphere rejection)
+   double* jac = nullptr;     // [maxK] |s2z / s2z'| in the constraint frame
+   double* mom = nullptr;     // [12 maxK] mu1 s1', mu2 s2', mu1 s1, mu2 s2 (x|y|z blocks of maxK each)
+   double* u = nullptr;       // [maxK] acceptance uniforms (replay) or nullptr
+   double* rnd = nullptr;     // [4 maxK] replayed Gaussians and uniforms
+   double* M = nullptr;       // [3] running total moment (mu_B)
+   unsigned long long* cnt = nullptr;  // [3] accepted, energy rejections, sphere rejections
+   uint64_t sweep = 0;
+   double total = 0.0;
+};
+
+static CMCState* cmc_of(vgpu_ctx* h) { return (CMCState*)h->extras[5]; }
+
+void cmc_destroy(vgpu_ctx* h) {
+   CMCState* c = cmc_of(h);
+   if (!c) return;
+   cudaFree(c->pairs); cudaFree(c->prop); cudaFree(c->ef); cudaFree(c->jac); cudaFree(c->mom);
+   cudaFree(c->rnd); cudaFree(c->M); cudaFree(c->cnt);
+   delete c;
+   h->extras[5] = nullptr;
+}
+
+template <typename R>
+struct CMCArgs {
+   LLGArgs<R> a;
+   const int* list;     // the colour's atoms (affine pairing) or nullptr
+   int count;           // atoms in the list
+   uint64_t mul, add;   // pair k = (list[(mul 2k + add) % count], list[(mul (2k+1) + add) % count])
+   const int* given;    // explicit pairs [2K] or nullptr
+   int K;
+   const R* sigma; const R* beta; const R* mu_ratio;
+   const double* rnd;   // replayed numbers [4K] or nullptr
+   uint64_t sweep; uint32_t phase;
+   double P[9];
+   int* pairs; R* prop; double* ef; double* jac; double* mom; int maxK;
+};
+
+template <typename R, int FMT>
+__device__ __forceinline__ R cmc_delta(const LLGArgs<R>& a, int i, int mi, const MatParams<R>& m, const R S[3],
+                                       const R T[3], R ratio) {
+   R h[3] = {0, 0, 0};
+   exchange_gather<R, FMT>(a, i, mi, a.ax, a.ay, a.az, h[0], h[1], h[2]);
+   if (a.cell) {
+      const int c = __ldg(a.cell + i);
+      h[0] += __ldg(a.cell_hd + c); h[1] += __ldg(a.cell_hd + a.ncells + c); h[2] += __ldg(a.cell_hd + 2 * a.ncells + c);
+   } else if (a.hm_atom) {
+      h[0] += __ldg(a.hm_atom + i); h[1] += __ldg(a.hm_atom + a.n + i); h[2] += __ldg(a.hm_atom + 2 * a.n + i);
+   }
+   return site_energy_delta<R>(a, i, m, S, T, h) * ratio;
+}
+
+template <typename R, int FMT>
+__global__ void __launch_bounds__(128) cmc_propose_kernel(const CMCArgs<R> p) {
+   const int k = blockIdx.x * blockDim.x + threadIdx.x;
+   if (k >= p.K) return;
+   const LLGArgs<R>& a = p.a;
+   int i1, i2;
+   if (p.given) {
+      i1 = p.given[2 * k]; i2 = p.given[2 * k + 1];
+   } else {
+      i1 = __ldg(p.list + (int)((p.mul * (uint64_t)(2 * k) + p.add) % (uint64_t)p.count));
+      i2 = __ldg(p.list + (int)((p.mul * (uint64_t)(2 * k + 1) + p.add) % (uint64_t)p.count));
+   }
+   p.pairs[2 * k] = i1;
+   p.pairs[2 * k + 1] = i2;
+   const int m1 = a.mat ? __ldg(a.mat + i1) : 0, m2 = a.mat ? __ldg(a.mat + i2) : 0;
+   const MatParams<R> mp1 = a.mp[m1], mp2 = a.mp[m2];
+   double g0, g1, g2;
+   if (p.rnd) {
+      g0 = p.rnd[k]; g1 = p.rnd[p.K + k]; g2 = p.rnd[2 * p.K + k];
+   } else {
+      const u32x4 c = {(uint32_t)k, (uint32_t)p.sweep, (uint32_t)(p.sweep >> 32) ^ (p.phase << 20), RNG_CMC_MOVE};
+      const u32x4 r = philox4x32_10(c, a.seed_lo, a.seed_hi);
+      double s1, c1, s2, c2;
+      const double r1 = sqrt(-2.0 * log(u01d(r.x)));
+      const double rr = sqrt(-2.0 * log(u01d(r.z)));
+      sincospi(2.0 * u01d(r.y), &s1, &c1);
+      sincospi(2.0 * u01d(r.w), &s2, &c2);
+      g0 = r1 * c1; g1 = r1 * s1; g2 = rr * c2;
+   }
+   const R sg = __ldg(p.sigma + m1);
+   const R S1[3] = {a.ax[i1], a.ay[i1], a.az[i1]};
+   const R S2[3] = {a.ax[i2], a.ay[i2], a.az[i2]};
+   R T1[3] = {S1[0] + (R)g0 * sg, S1[1] + (R)g1 * sg, S1[2] + (R)g2 * sg};
+   const R r = rsqrt_<R>(T1[0] * T1[0] + T1[1] * T1[1] + T1[2] * T1[2]);
+   T1[0] *= r; T1[1] *= r; T1[2] *= r;
+   // the constraint frame in FP64 (the compensating spin keeps the
+   // perpendicular moment to rounding)
+   const double* P = p.P;
+   double s1im[3], s1fm[3], s2im[3], s2fm[3];
+   for (int q = 0; q < 3; ++q) {
+      s1im[q] = P[3 * q] * (double)S1[0] + P[3 * q + 1] * (double)S1[1] + P[3 * q + 2] * (double)S1[2];
+      s1fm[q] = P[3 * q] * (double)T1[0] + P[3 * q + 1] * (double)T1[1] + P[3 * q + 2] * (double)T1[2];
+      s2im[q] = P[3 * q] * (double)S2[0] + P[3 * q + 1] * (double)S2[1] + P[3 * q + 2] * (double)S2[2];
+   }
+   const double mu1 = (double)__ldg(p.mu_ratio + m1), mu2 = (double)__ldg(p.mu_ratio + m2);
+   const double mr = mu1 / mu2;
+   s2fm[0] = mr * (s1im[0] - s1fm[0]) + s2im[0];
+   s2fm[1] = mr * (s1im[1] - s1fm[1]) + s2im[1];
+   const int st = p.maxK;
+   if (!((s2fm[0] * s2fm[0] + s2fm[1] * s2fm[1]) < 1.0) || i1 == i2) {
+      p.ef[k] = -1.0;  // off the unit sphere: rejected
+      return;
+   }
+   s2fm[2] = (s2im[2] >= 0.0 ? 1.0 : -1.0) * sqrt(1.0 - s2fm[0] * s2fm[0] - s2fm[1] * s2fm[1]);
+   R T2[3];
+   for (int q = 0; q < 3; ++q) T2[q] = (R)(P[q] * s2fm[0] + P[3 + q] * s2fm[1] + P[6 + q] * s2fm[2]);
+   // the two spins share no bond (one colour), so each energy change sees
+   // the other's neighbours as they are
+   const R de1 = cmc_delta<R, FMT>(a, i1, m1, mp1, S1, T1, (R)mu1);
+   const R de2 = cmc_delta<R, FMT>(a, i2, m2, mp2, S2, T2, (R)mu2);
+   const double de21 = (double)de1 * (double)__ldg(p.beta + m1) + (double)de2 * (double)__ldg(p.beta + m2);
+   p.ef[k] = exp(-de21);
+   p.jac[k] = fabs(s2im[2] / s2fm[2]);
+   for (int q = 0; q < 3; ++q) {
+      p.prop[q * st + k] = T1[q];
+      p.prop[(3 + q) * st + k] = T2[q];
+      p.mom[q * st + k] = mu1 * (double)T1[q];
+      p.mom[(3 + q) * st + k] = mu2 * (double)T2[q];
+      p.mom[(6 + q) * st + k] = mu1 * (double)S1[q];
+      p.mom[(9 + q) * st + k] = mu2 * (double)S2[q];
+   }
+}
+
+// One warp: the pairs in order with the running total moment M (the
+// reference's acceptance, cmc.cpp:459-490); each lane holds a chunk's pair,
+// every lane follows the same decisions, lane l writes pair l's spins.
+template <typename R>
+__global__ void __launch_bounds__(32) cmc_accept_kernel(LLGArgs<R> a, int K, int st, const int* __restrict__ pairs,
+                                                        const R* __restrict__ prop, const double* __restrict__ ef,
+                                                        const double* __restrict__ jac,
+                                                        const double* __restrict__ mom, const double* __restrict__ urep,
+                                                        uint64_t sweep, uint32_t phase, const double* pvp, double* M,
+                                                        unsigned long long* cnt) {
+   const int lane = threadIdx.x;
+   const unsigned full = 0xffffffffu;
+   const double pv[3] = {pvp[0], pvp[1], pvp[2]};
+   double Mx = M[0], My = M[1], Mz = M[2];
+   unsigned long long nacc = 0, nrej = 0, nsph = 0;
+   for (int base = 0; base < K; base += 32) {
+      const int k = base + lane;
+      const bool on = k < K;
+      double e = -1.0, jk = 0.0, u = 0.0, mm[12];
+      for (int q = 0; q < 12; ++q) mm[q] = 0.0;
+      if (on) {
+         e = ef[k];
+         if (e >= 0.0) {
+            jk = jac[k];
+            for (int q = 0; q < 12; ++q) mm[q] = mom[q * st + k];
+         }
+         if (urep) {
+            u = urep[k];
+         } else {
+            const u32x4 c = {(uint32_t)k, (uint32_t)sweep, (uint32_t)(sweep >> 32) ^ (phase << 20), RNG_CMC_ACCEPT};
+            u = u01d(philox4x32_10(c, a.seed_lo, a.seed_hi).x);
+         }
+      }
+      bool mine = false;
+      const int nl = min(32, K - base);
+      for (int l = 0; l < nl; ++l) {
+         const double el = __shfl_sync(full, e, l);
+         if (el < 0.0) {
+            ++nsph;
+            continue;
+         }
+         double ml[12];
+         for (int q = 0; q < 12; ++q) ml[q] = __shfl_sync(full, mm[q], l);
+         const double jl = __shfl_sync(full, jk, l), ul = __shfl_sync(full, u, l);
+         const double mzo = Mx * pv[0] + My * pv[1] + Mz * pv[2];
+         const double nx = Mx + ml[0] + ml[3] - ml[6] - ml[9];
+         const double ny = My + ml[1] + ml[4] - ml[7] - ml[10];
+         const double nz = Mz + ml[2] + ml[5] - ml[8] - ml[11];
+         const double mzn = nx * pv[0] + ny * pv[1] + nz * pv[2];
+         const double prob = el * ((mzn / mzo) * (mzn / mzo)) * jl;
+         if (prob >= ul && mzn > 0.0) {
+            Mx = nx; My = ny; Mz = nz;
+            ++nacc;
+            if (lane == l) mine = true;
+         } else {
+            ++nrej;
+         }
+      }
+      if (mine) {
+         const int i1 = pairs[2 * k], i2 = pairs[2 * k + 1];
+         a.ax[i1] = prop[k]; a.ay[i1] = prop[st + k]; a.az[i1] = prop[2 * st + k];
+         a.ax[i2] = prop[3 * st + k]; a.ay[i2] = prop[4 * st + k]; a.az[i2] = prop[5 * st + k];
+      }
+   }
+   if (lane == 0) {
+      M[0] = Mx; M[1] = My; M[2] = Mz;
+      cnt[0] += nacc; cnt[1] += nrej; cnt[2] += nsph;
+   }
+}
+
+// total moment sum_i mu_s,i s_i (mu_B) into M (zeroed first), FP64
+template <typename R>
+__global__ void cmc_moment_kernel(const LLGArgs<R> a, const R* __restrict__ mu_ratio, double* M) {
+   double v[3] = {0, 0, 0};
+   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_upd; i += gridDim.x * blockDim.x) {
+      const double mu = (double)__ldg(mu_ratio + (a.mat ? __ldg(a.mat + i) : 0));
+      v[0] += mu * (double)a.ax[i]; v[1] += mu * (double)a.ay[i]; v[2] += mu * (double)a.az[i];
+   }
+   for (int q = 0; q < 3; ++q) {
+      for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+      if ((threadIdx.x & 31) == 0) atomicAdd(M + q, v[q]);
+   }
+}
+
+template <typename R, int FMT>
+static cudaError_t launch_cmc_propose(const CMCArgs<R>& p, cudaStream_t st) {
+   if (p.K <= 0) return cudaSuccess;
+   cmc_propose_kernel<R, FMT><<<(p.K + 127) / 128, 128, 0, st>>>(p);
+   return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t cmc_propose_dispatch(const CMCArgs<R>& p, int fmt, cudaStream_t st) {
+   switch (fmt) {
+      case FMT_ISO_TAB: return launch_cmc_propose<R, FMT_ISO_TAB>(p, st);
+      case FMT_ISO_BOND: return launch_cmc_propose<R, FMT_ISO_BOND>(p, st);
+      case FMT_VEC_TAB: return launch_cmc_propose<R, FMT_VEC_TAB>(p, st);
+      case FMT_VEC_BOND: return launch_cmc_propose<R, FMT_VEC_BOND>(p, st);
+      case FMT_DMI_TAB: return launch_cmc_propose<R, FMT_DMI_TAB>(p, st);
+      default: return launch_cmc_propose<R, FMT_TENSOR_BOND>(p, st);
+   }
+}
+
+}  // namespace vgpu
+
+namespace {
+
+uint64_t splitmix64(uint64_t x) {
+   x += 0x9E3779B97F4A7C15ull;
+   x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+   x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+   return x ^ (x >> 31);
+}
+
+uint64_t gcd64(uint64_t a, uint64_t b) {
+   while (b) {
+      const uint64_t t = a % b;
+      a = b;
+      b = t;
+   }
+   return a;
+}
+
+// one phase: K pairs (explicit, or the affine pairing of colour c), proposals
+// in parallel, acceptance by one warp
+template <typename R>
+int cmc_phase(vgpu_handle h, const R* tab, int colour, const int* given, int K, const double* rnd, uint32_t phase) {
+   CMCState* c = cmc_of(h);
+   MCState* s = mc_of(h);
+   CMCArgs<R> p;
+   memset(&p, 0, sizeof p);
+   p.a = make_args<R>(h);
+   p.sigma = tab; p.beta = tab + 100; p.mu_ratio = tab + 200;
+   p.sweep = c->sweep; p.phase = phase;
+   for (int q = 0; q < 9; ++q) p.P[q] = c->P[q];
+   p.pairs = c->pairs; p.prop = (R*)c->prop; p.ef = c->ef; p.jac = c->jac; p.mom = c->mom; p.maxK = c->maxK;
+   p.K = K;
+   p.given = given;
+   p.rnd = rnd;
+   if (!given) {
+      p.list = s->atoms + s->colour_off[colour];
+      p.count = s->colour_off[colour + 1] - s->colour_off[colour];
+      const uint64_t key = splitmix64(h->seed ^ splitmix64(c->sweep * 1024 + phase));
+      const uint64_t n = (uint64_t)std::max(p.count, 1);
+      uint64_t mul = 1 + splitmix64(key) % n;
+      while (gcd64(mul, n) != 1) mul = mul % n + 1;
+      p.mul = mul;
+      p.add = splitmix64(key + 1) % n;
+   }
+   h->prof_begin(PROF_MC);
+   cudaError_t e = cmc_propose_dispatch<R>(p, h->sys.fmt, h->stream);
+   if (e == cudaSuccess && K > 0) {
+      cmc_accept_kernel<R><<<1, 32, 0, h->stream>>>(p.a, K, c->maxK, c->pairs, (const R*)c->prop, c->ef, c->jac,
+                                                    c->mom, rnd ? rnd + 3 * (size_t)K : nullptr, c->sweep, phase,
+                                                    c->M + 3, c->M, c->cnt);
+      e = cudaGetLastError();
+   }
+   h->prof_end(PROF_MC);
+   if (e != cudaSuccess) return cuda_err(h, e, "cmc launch");
+   h->kernel_launches += 2;
+   c->total += K;
+   return VGPU_OK;
+}
+
+template <typename R>
+int cmc_recount_moment(vgpu_handle h, const R* tab) {
+   CMCState* c = cmc_of(h);
+   cudaMemsetAsync(c->M, 0, 3 * sizeof(double), h->stream);
+   cmc_moment_kernel<R><<<std::max(1, std::min(1024, (h->sys.n + 255) / 256)), 256, 0, h->stream>>>(
+       make_args<R>(h), tab + 200, c->M);
+   h->kernel_launches++;
+   return cuda_err(h, cudaGetLastError(), "cmc moment");
+}
+
+template <typename R>
+int cmc_sweeps_typed(vgpu_handle h, uint64_t n_sweeps) {
+   CMCState* c = cmc_of(h);
+   MCState* s = mc_of(h);
+   const R* tab = mc_tables<R>(h);
+   if (!tab) return VGPU_ERR_OOM;
+   for (uint64_t sw = 0; sw < n_sweeps; ++sw) {
+      // the total moment from the spins at every step, as the reference does
+      if (int rc = cmc_recount_moment<R>(h, tab)) return rc;
+      uint32_t phase = 0;
+      for (int round = 0; round < 2; ++round)
+         for (int col = 0; col < s->ncolours; ++col, ++phase) {
+            const int K = (s->colour_off[col + 1] - s->colour_off[col]) / 2;
+            if (int rc = cmc_phase<R>(h, tab, col, nullptr, K, nullptr, phase)) return rc;
+         }
+      c->sweep++;
+   }
+   return VGPU_OK;
+}
+
+}  // namespace
+
+extern "C" int vgpu_cmc_setup(vgpu_handle h, double phi_deg, double theta_deg, int32_t init_spins) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (h->sys.n_owned < h->sys.n) return set_err(h, VGPU_ERR_STATE, "constrained Monte Carlo runs on whole systems");
+   cudaSetDevice(h->device);
+   if (!mc_of(h)) {
+      int32_t nc = 0;
+      if (int rc = vgpu_mc_setup(h, nullptr, &nc)) return rc;
+   }
+   cmc_destroy(h);
+   CMCState* c = new CMCState();
+   h->extras[5] = c;
+   // polar_rot_matrix (cmc.cpp:53-135): P = Ry(phi) Rz(theta) with the
+   // reference's element layout; pv = (0,0,1) P, the third row
+   const double d2r = 3.14159265358979323846264338327 / 180.0;
+   const double sy = std::sin(phi_deg * d2r), cy = std::cos(phi_deg * d2r);
+   const double sz = std::sin(theta_deg * d2r), cz = std::cos(theta_deg * d2r);
+   const double Ry[9] = {cy, 0.0, -sy, 0.0, 1.0, 0.0, sy, 0.0, cy};
+   const double Rz[9] = {cz, sz, 0.0, -sz, cz, 0.0, 0.0, 0.0, 1.0};
+   for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+         double v = 0.0;
+         for (int k = 0; k < 3; ++k) v += Ry[3 * i + k] * Rz[3 * k + j];
+         c->P[3 * i + j] = v;
+      }
+   for (int j = 0; j < 3; ++j) c->pv[j] = c->P[6 + j];
+   MCState* s = mc_of(h);
+   int maxK = 1;
+   for (int col = 0; col < s->ncolours; ++col) maxK = std::max(maxK, (s->colour_off[col + 1] - s->colour_off[col]) / 2);
+   maxK = std::max(maxK, h->sys.n / 2);
+   c->maxK = maxK;
+   const size_t rs = h->prec == VGPU_PREC_FP64 ? sizeof(double) : sizeof(float);
+   cudaError_t e;
+   if ((e = cudaMalloc(&c->pairs, sizeof(int) * 2 * maxK)) || (e = cudaMalloc(&c->prop, rs * 6 * maxK)) ||
+       (e = cudaMalloc(&c->ef, sizeof(double) * maxK)) || (e = cudaMalloc(&c->jac, sizeof(double) * maxK)) ||
+       (e = cudaMalloc(&c->mom, sizeof(double) * 12 * maxK)) || (e = cudaMalloc(&c->rnd, sizeof(double) * 4 * maxK)) ||
+       (e = cudaMalloc(&c->M, sizeof(double) * 6)) || (e = cudaMalloc(&c->cnt, sizeof(unsigned long long) * 3))) {
+      cmc_destroy(h);
+      return cuda_err(h, e, "cmc buffers");
+   }
+   cudaMemsetAsync(c->cnt, 0, sizeof(unsigned long long) * 3, h->stream);
+   cudaMemcpyAsync(c->M + 3, c->pv, sizeof(double) * 3, cudaMemcpyHostToDevice, h->stream);
+   if (init_spins) {
+      // CMCinit: every spin along the constraint direction
+      const int n = h->sys.n;
+      std::vector<double> v[3];
+      const double dir[3] = {std::sin(phi_deg * d2r) * std::cos(theta_deg * d2r),
+                             std::sin(phi_deg * d2r) * std::sin(theta_deg * d2r), std::cos(phi_deg * d2r)};
+      for (int q = 0; q < 3; ++q) v[q].assign(n, dir[q]);
+      if (int rc = vgpu_set_spins(h, v[0].data(), v[1].data(), v[2].data())) return rc;
+   }
+   return cuda_err(h, cudaStreamSynchronize(h->stream), "cmc setup");
+}
+
+extern "C" int vgpu_cmc_frame(vgpu_handle h, double* P9, double* pv3) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   CMCState* c = cmc_of(h);
+   if (!c) return set_err(h, VGPU_ERR_STATE, "vgpu_cmc_setup not called");
+   if (P9) std::copy(c->P, c->P + 9, P9);
+   if (pv3) std::copy(c->pv, c->pv + 3, pv3);
+   return VGPU_OK;
+}
+
+static int cmc_ready(vgpu_handle h) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (!cmc_of(h) || !mc_of(h)) return set_err(h, VGPU_ERR_STATE, "vgpu_cmc_setup not called");
+   if (!(h->params.temperature >= 0.0)) return set_err(h, VGPU_ERR_STATE, "vgpu_set_params not called");
+   if (int rc = h->fields_ready()) return rc;
+   cudaSetDevice(h->device);
+   return VGPU_OK;
+}
+
+extern "C" int vgpu_cmc_sweep(vgpu_handle h, uint64_t n_steps) {
+   if (int rc = cmc_ready(h)) return rc;
+   return h->prec == VGPU_PREC_FP64 ? cmc_sweeps_typed<double>(h, n_steps) : cmc_sweeps_typed<float>(h, n_steps);
+}
+
+template <typename R>
+static int cmc_pairs_typed(vgpu_handle h, const int32_t* pairs, int32_t K, const double* rnd, const double* M) {
+   CMCState* c = cmc_of(h);
+   const R* tab = mc_tables<R>(h);
+   if (!tab) return VGPU_ERR_OOM;
+   int rc = cuda_err(h, cudaMemcpyAsync(c->pairs, pairs, sizeof(int) * 2 * K, cudaMemcpyHostToDevice, h->stream),
+                     "cmc pairs");
+   if (!rc) rc = cuda_err(h, cudaMemcpyAsync(c->rnd, rnd, sizeof(double) * 4 * K, cudaMemcpyHostToDevice, h->stream),
+                          "cmc pairs");
+   if (!rc) {
+      if (M) rc = cuda_err(h, cudaMemcpyAsync(c->M, M, sizeof(double) * 3, cudaMemcpyHostToDevice, h->stream), "cmc M");
+      else rc = cmc_recount_moment<R>(h, tab);
+   }
+   if (rc) return rc;
+   // the explicit pairs are read back from c->pairs by the proposal kernel
+   // (it rewrites the same values)
+   rc = cmc_phase<R>(h, tab, 0, c->pairs, K, c->rnd, 0);
+   if (rc) return rc;
+   return cuda_err(h, cudaStreamSynchronize(h->stream), "cmc pairs");
+}
+
+extern "C" int vgpu_cmc_pairs(vgpu_handle h, const int32_t* pairs, int32_t num_pairs, const double* rnd,
+                              const double* moment) {
+   if (int rc = cmc_ready(h)) return rc;
+   CMCState* c = cmc_of(h);
+   if (!pairs || !rnd || num_pairs <= 0 || num_pairs > c->maxK)
+      return set_err(h, VGPU_ERR_ARG, "num_pairs must be in 1..%d with pairs and random numbers given", c->maxK);
+   MCState* s = mc_of(h);
+   for (int k = 0; k < 2 * num_pairs; ++k)
+      if (pairs[k] < 0 || pairs[k] >= h->sys.n) return set_err(h, VGPU_ERR_ARG, "pair atom %d out of range", pairs[k]);
+   // the pairs of one phase must not interact: all atoms of one colour, each at most once
+   std::vector<char> seen(h->sys.n, 0);
+   const int col = s->colour_host[pairs[0]];
+   for (int k = 0; k < 2 * num_pairs; ++k) {
+      if (s->colour_host[pairs[k]] != col) return set_err(h, VGPU_ERR_ARG, "pair atoms of different colours");
+      if (seen[pairs[k]]++) return set_err(h, VGPU_ERR_ARG, "atom %d appears twice in one phase", pairs[k]);
+   }
+   return h->prec == VGPU_PREC_FP64 ? cmc_pairs_typed<double>(h, pairs, num_pairs, rnd, moment)
+                                    : cmc_pairs_typed<float>(h, pairs, num_pairs, rnd, moment);
+}
+
+extern "C" int vgpu_cmc_get(vgpu_handle h, double* moment, double* counters) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   CMCState* c = cmc_of(h);
+   if (!c) return set_err(h, VGPU_ERR_STATE, "vgpu_cmc_setup not called");
+   cudaSetDevice(h->device);
+   double M[3];
+   unsigned long long cnt[3];
+   cudaError_t e = cudaMemcpyAsync(M, c->M, sizeof M, cudaMemcpyDeviceToHost, h->stream);
+   if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, c->cnt, sizeof cnt, cudaMemcpyDeviceToHost, h->stream);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+   if (e != cudaSuccess) return cuda_err(h, e, "cmc counters");
+   if (moment) std::copy(M, M + 3, moment);
+   if (counters) {
+      counters[0] = c->total;
+      for (int q = 0; q < 3; ++q) counters[1 + q] = (double)cnt[q];
+   }
    return VGPU_OK;
 }

@@ -16,7 +16,8 @@
 namespace vgpu {
 
 // purposes (4th counter word)
-enum : uint32_t { RNG_THERMAL = 0u, RNG_MC_MOVE = 1u, RNG_MC_ACCEPT = 2u, RNG_THERMAL_HI = 3u };
+enum : uint32_t { RNG_THERMAL = 0u, RNG_MC_MOVE = 1u, RNG_MC_ACCEPT = 2u, RNG_THERMAL_HI = 3u, RNG_CMC_MOVE = 4u,
+                  RNG_CMC_ACCEPT = 5u };
 
 struct u32x4 { uint32_t x, y, z, w; };
 

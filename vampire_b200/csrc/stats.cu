@@ -527,9 +527,11 @@ extern "C" int vgpu_stats_get_energy(vgpu_handle h, int32_t id, double* e, doubl
 
 extern "C" int vgpu_stats_reset(vgpu_handle h) {
    if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   cudaSetDevice(h->device);
+   // the torque means too, as the reference's mag_m_reset (utility/statistics.cpp)
+   if (int rc = torque_reset(h)) return rc;
    StatsState* s = stats_of(h);
    if (!s) return VGPU_OK;
-   cudaSetDevice(h->device);
    for (StatsMask& m : s->masks) {
       cudaMemsetAsync(m.mean, 0, sizeof(double) * m.size * ST_W, h->stream);
       cudaMemsetAsync(m.derived, 0, sizeof(double) * m.size * ST_DV, h->stream);

@@ -17,6 +17,8 @@ void vgpu_ctx::destroy_extras() {
    mc_destroy(this);
    dipole_destroy(this);
    batch_destroy(this);
+   torque_destroy(this);
+   cmc_destroy(this);
 }
 
 cudaEvent_t vgpu_ctx::get_event() {

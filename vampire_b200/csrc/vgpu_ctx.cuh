@@ -97,6 +97,9 @@ void stats_destroy(vgpu_ctx* h);
 void mc_destroy(vgpu_ctx* h);
 void dipole_destroy(vgpu_ctx* h);
 void batch_destroy(vgpu_ctx* h);
+void torque_destroy(vgpu_ctx* h);
+void cmc_destroy(vgpu_ctx* h);
+int torque_reset(vgpu_ctx* h);
 const double* batch_ramp(vgpu_ctx* h);
 
 }  // namespace vgpu

@@ -16,9 +16,15 @@
 //     the spins to the host and runs the reference's own statistics classes,
 //     as src/cuda/statistics.cu:30-49 does; otherwise statistics run on the
 //     device (vgpu_stats_*), energies included;
-//   * the dipole field follows the reference's flow: the host computes it
-//     every update_rate steps after transfer_spin_positions_from_gpu_to_cpu
-//     and hands it over in transfer_dipole_fields_from_cpu_to_gpu.
+//   * the macrocell and tensor dipole solvers run on the device: at
+//     initialisation the cells:: arrays go to vgpu_dipole_setup, and
+//     vgpu_llg_heun recomputes the field every dipole::update_rate steps
+//     without leaving the device, so transfer_spin_positions_from_gpu_to_cpu
+//     and transfer_dipole_fields_from_cpu_to_gpu -- the reference's
+//     D2H / host update / H2D round trip around dipole::calculate_field
+//     (dipole/field.cpp:43-87) -- have nothing to carry.  The atomistic
+//     solver, or VGPU_DIPOLE=host in the environment, keeps the reference's
+//     flow: the host computes the field and hands it over.
 // Changed on purpose:
 //   * finalize copies the spins back to the host first, so a checkpoint
 //     written after the run (sim.cpp:521-524) holds the final spins;
@@ -46,6 +52,8 @@
 #include "vio.hpp"
 
 #include "anisotropy/internal.hpp"
+#include "cells.hpp"
+#include "dipole/internal.hpp"
 #include "exchange/internal.hpp"
 
 #include "vgpu.h"
@@ -59,6 +67,7 @@ bool g_have_last = false;
 // device statistics masks: system, material, height, material-height
 int32_t g_mask_id[4] = {-1, -1, -1, -1};
 int32_t g_mask_size[4] = {0, 0, 0, 0};
+bool g_dipole_device = false;  // the device dipole solver holds the field
 
 void fail(int rc, const char* what) {
    if (rc == VGPU_OK) return;
@@ -264,8 +273,36 @@ bool initialize(bool cpu_stats) {
       add_mask(2, ::stats::height_magnetization, ::stats::calculate_height_magnetization);
       add_mask(3, ::stats::material_height_magnetization, ::stats::calculate_material_height_magnetization);
    }
-   // dipole: per-atom fields computed on the host at start-up (dipole::initialize)
-   if (dipole::activated) transfer_dipole_fields_from_cpu_to_gpu();
+   if (dipole::activated) {
+      const char* where = std::getenv("VGPU_DIPOLE");
+      const bool host = (where && std::string(where) == "host") ||
+                        dipole::internal::solver == dipole::internal::atomistic;
+      if (host) {
+         // per-atom fields computed on the host at start-up (dipole::initialize)
+         transfer_dipole_fields_from_cpu_to_gpu();
+      } else {
+         // the device solver: macrocells as cells::initialize built them
+         // (cells/initialize.cpp:189-265), field computed now from the spins
+         vgpu_dipole_desc dd;
+         std::memset(&dd, 0, sizeof dd);
+         dd.num_cells = cells::num_cells;
+         dd.solver = dipole::internal::solver == dipole::internal::tensor ? VGPU_DIPOLE_TENSOR : VGPU_DIPOLE_MACROCELL;
+         dd.update_rate = dipole::update_rate;
+         dd.macro_cell_size = cells::macro_cell_size;
+         dd.cutoff = dipole::cutoff;
+         dd.atom_cell = cells::atom_cell_id_array.data();
+         dd.cell_pos_mom = cells::pos_and_mom_array.data();
+         dd.cell_volume = cells::volume_array.data();
+         dd.cell_natoms = cells::num_atoms_in_cell.data();
+         dd.atom_x = ::atoms::x_coord_array.data();
+         dd.atom_y = ::atoms::y_coord_array.data();
+         dd.atom_z = ::atoms::z_coord_array.data();
+         fail(vgpu_dipole_setup(g_h, &dd), "dipole setup");
+         g_dipole_device = true;
+         zlog << zTs() << "B200 backend: macrocell dipole field on the device (" << cells::num_cells
+              << " cells, update every " << dipole::update_rate << " steps)" << std::endl;
+      }
+   }
    return true;
 }
 
@@ -312,14 +349,17 @@ void finalize() {
    spins_to_host();
    vgpu_destroy(g_h);
    g_h = nullptr;
+   g_dipole_device = false;
 }
 
+// called by dipole::calculate_field around its host update; with the device
+// solver the field is already current on the device, so nothing crosses
 void transfer_spin_positions_from_gpu_to_cpu() {
-   if (g_h) spins_to_host();
+   if (g_h && !g_dipole_device) spins_to_host();
 }
 
 void transfer_dipole_fields_from_cpu_to_gpu() {
-   if (!g_h) return;
+   if (!g_h || g_dipole_device) return;
    fail(vgpu_set_dipole_field(g_h, dipole::atom_dipolar_field_array_x.data(), dipole::atom_dipolar_field_array_y.data(),
                               dipole::atom_dipolar_field_array_z.data(), dipole::atom_mu0demag_field_array_x.data(),
                               dipole::atom_mu0demag_field_array_y.data(), dipole::atom_mu0demag_field_array_z.data()),

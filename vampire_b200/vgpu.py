@@ -27,6 +27,7 @@ OPT_STAGE_WAIT_TEST = 6
 OPT_COMPACT_RECORDS = 7
 OPT_WINDOW_STAGING = 8
 OPT_PROFILE_EVERY = 9
+EXCHANGE_FORMATS = ("iso_tab", "iso_bond", "vec_tab", "vec_bond", "dmi_tab", "tensor_bond")
 RECORDS_NONE, RECORDS_WIDE, RECORDS_COMPACT, RECORDS_WINDOW = 0, 1, 2, 3
 PASS_PREDICTOR, PASS_CORRECTOR = 0, 1
 STATE_SPIN, STATE_PREDICTOR = 0, 1
@@ -271,6 +272,13 @@ class Simulation:
         self._check(lib().vgpu_record_layout(self._h, C.byref(lay), C.byref(nd)))
         return lay.value, nd.value
 
+    def exchange_format(self) -> str:
+        """Per-bond exchange format chosen at upload: iso_tab, iso_bond,
+        vec_tab, vec_bond, dmi_tab or tensor_bond."""
+        f = C.c_int32()
+        self._check(lib().vgpu_exchange_format(self._h, C.byref(f)))
+        return EXCHANGE_FORMATS[f.value]
+
     def set_params(self, p) -> None:
         c = params_struct(p)
         self._check(lib().vgpu_set_params(self._h, C.byref(c)))
@@ -377,6 +385,25 @@ class Simulation:
         self._check(lib().vgpu_stats_get_derived(self._h, C.c_int32(mask_id), C.c_double(temperature),
                                                  _ptr(sus, _D), _ptr(sh, _D), _ptr(sd, _D)))
         return sus.reshape(size, 4), sh, sd.reshape(size, 4)
+
+    def torque_update(self) -> None:
+        """System and per-material torque of the current state, added to the
+        running means (vgpu_torque_update)."""
+        self._check(lib().vgpu_torque_update(self._h))
+
+    def torque(self) -> dict:
+        """{total[3], mean[3], material[M,3], material_mean[M,3], max, count}."""
+        M = self.system.materials.size
+        tot, mean = np.zeros(3), np.zeros(3)
+        mat, mmean = np.zeros(3 * M), np.zeros(3 * M)
+        mx, cnt = C.c_double(), C.c_int64()
+        self._check(lib().vgpu_torque_get(self._h, _ptr(tot, _D), _ptr(mean, _D), _ptr(mat, _D), _ptr(mmean, _D),
+                                          C.byref(mx), C.byref(cnt)))
+        return {"total": tot, "mean": mean, "material": mat.reshape(M, 3), "material_mean": mmean.reshape(M, 3),
+                "max": mx.value, "count": cnt.value}
+
+    def torque_reset(self) -> None:
+        self._check(lib().vgpu_torque_reset(self._h))
 
     def stats_sums(self, mask_id: int, size: int) -> np.ndarray:
         """Raw per-bin sums of the last statistics update, (size, 8)."""
@@ -513,6 +540,39 @@ class Simulation:
         return mv.value, rj.value
 
     # -- statistics --------------------------------------------------------
+    # -- constrained Monte Carlo ------------------------------------------
+    def cmc_setup(self, phi_deg: float, theta_deg: float, init_spins: bool = True) -> None:
+        """Constraint direction (phi from z, theta about z, degrees) and, with
+        init_spins, every spin along it (the reference's CMCinit)."""
+        self._check(lib().vgpu_cmc_setup(self._h, C.c_double(phi_deg), C.c_double(theta_deg),
+                                          C.c_int32(int(init_spins))))
+
+    def cmc_sweep(self, n_steps: int = 1) -> None:
+        """n_steps constrained Monte Carlo steps (about N pair moves each)."""
+        self._check(lib().vgpu_cmc_sweep(self._h, C.c_uint64(n_steps)))
+
+    def cmc_pairs(self, pairs: np.ndarray, rnd: np.ndarray, moment: Optional[np.ndarray] = None) -> None:
+        """One phase on explicit pairs (all atoms of one colour, each once) with
+        given random numbers rnd[4K] (Gaussians x|y|z of K, then uniforms)."""
+        pr = np.ascontiguousarray(pairs, dtype=np.int32).ravel()
+        r = np.ascontiguousarray(rnd, dtype=np.float64)
+        mm = None if moment is None else np.ascontiguousarray(moment, dtype=np.float64)
+        self._check(lib().vgpu_cmc_pairs(self._h, _ptr(pr, _I32), C.c_int32(pr.size // 2), _ptr(r, _D),
+                                         _ptr(mm, _D) if mm is not None else C.cast(None, _D)))
+
+    def cmc_state(self):
+        """(total moment [3] in mu_B, [pair moves, accepted, energy rejections,
+        sphere rejections])."""
+        m, c = np.zeros(3), np.zeros(4)
+        self._check(lib().vgpu_cmc_get(self._h, _ptr(m, _D), _ptr(c, _D)))
+        return m, c
+
+    def cmc_frame(self):
+        """(P[3,3] rotating the constraint direction to z, constraint vector)."""
+        P, v = np.zeros(9), np.zeros(3)
+        self._check(lib().vgpu_cmc_frame(self._h, _ptr(P, _D), _ptr(v, _D)))
+        return P.reshape(3, 3), v
+
     def add_mask(self, mask: np.ndarray, size: int) -> int:
         m = np.ascontiguousarray(mask, dtype=np.int32)
         out = C.c_int32()
