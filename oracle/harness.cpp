@@ -72,7 +72,7 @@ extern std::vector<std::vector<double> > polar_vector, polar_matrix;
 // INTEGRATION.md shows), i.e. vcuda::mc_step(), instead of
 // montecarlo::mc_step.
 #include "gpu.hpp"
-namespace vcuda { void mc_step(); }
+namespace vcuda { void mc_step(); void cmc_step(); }
 static bool g_gpu_mc = false;
 #endif
 
@@ -314,7 +314,15 @@ static void one_step() {
                              atoms::type_array);
          break;
       case 2: sim::LLG_Midpoint(); break;
-      case 3: montecarlo::cmc_step(); break;
+      case 3:
+#ifdef VGPU_MC_HOOK
+         if (g_gpu_mc) {
+            vcuda::cmc_step();
+            break;
+         }
+#endif
+         montecarlo::cmc_step();
+         break;
       default: sim::LLG_Heun(); break;
    }
 }

@@ -100,10 +100,10 @@ HARNESS = REPO / "oracle" / "_ref" / "vampire-harness"
 HARNESS_B200 = REPO / "oracle" / "_ref" / "vampire-harness-b200"
 
 
-def _mc_run(exe, extra_args, T=600.0, eq=1000, av=3000, every=10):
+def _mc_run(exe, extra_args, T=600.0, eq=1000, av=3000, every=10, integrator="monte-carlo", extra=""):
     from oracle import oracle as O
     mat = SC_MAT.replace("initial-spin-direction=random", "initial-spin-direction=0,0,1")
-    inp = sc_input(10, T=T, H=0.0, integrator="monte-carlo", extra="montecarlo:algorithm=angle\n")
+    inp = sc_input(10, T=T, H=0.0, integrator=integrator, extra="montecarlo:algorithm=angle\n" + extra)
     d = Path(tempfile.mkdtemp(prefix="dropin_mc_"))
     (d / "input").write_text(inp)
     (d / "m.mat").write_text(mat)
@@ -137,4 +137,32 @@ def test_dropin_mc_hook_matches_serial_statistically():
         assert moves == 1000 * 4000
     (ms, es), (mg, eg) = res
     print(f"<|m|> serial {ms:.5f} +- {es:.5f}, gpu hook {mg:.5f} +- {eg:.5f}")
+    assert abs(ms - mg) <= 4.0 * np.hypot(es, eg) + 1e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not HARNESS_B200.exists(), reason="B200 harness not built")
+def test_dropin_cmc_hook_matches_serial_statistically():
+    """Constrained Monte Carlo through the gpu::cmc_step hook (vcuda::cmc_step
+    -> vgpu_cmc_setup with sim::constraint_phi/theta, vgpu_cmc_sweep) inside
+    the reference's start-up: SC 10^3 at 600 K, constraint (30, 45) degrees,
+    1000 + 3000 steps, against the reference's montecarlo::cmc_step on the
+    same input.  The moment stays along the constraint and its size agrees
+    within 4 standard errors; the counters come back into montecarlo::cmc."""
+    extra = "sim:constraint-angle-phi=30\nsim:constraint-angle-theta=45\n"
+    ds, _ = _mc_run(HARNESS, [], integrator="constrained-monte-carlo", extra=extra)
+    dg, _ = _mc_run(HARNESS_B200, ["--gpu-mc"], integrator="constrained-monte-carlo", extra=extra)
+    pv = ds["cmc_frame"][9:12]
+    assert np.abs(dg["cmc_frame"] - ds["cmc_frame"]).max() < 1e-15
+    res = []
+    for d in (ds, dg):
+        tr = d["mag_trace"].reshape(-1, 4)[:, :3]
+        par = tr @ pv
+        assert np.abs(tr - np.outer(par, pv)).max() < 1e-5
+        b = par[: len(par) // 10 * 10].reshape(10, -1).mean(1)
+        res.append((par.mean(), b.std(ddof=1) / np.sqrt(10)))
+        total, success, erej, srej = d["cmc_counters"]
+        assert total >= 0.9 * 1000 * 4000 and success + erej + srej == total
+    (ms, es), (mg, eg) = res
+    print(f"<m.e> serial {ms:.5f} +- {es:.5f}, gpu hook {mg:.5f} +- {eg:.5f}")
     assert abs(ms - mg) <= 4.0 * np.hypot(es, eg) + 1e-4

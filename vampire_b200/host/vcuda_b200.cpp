@@ -46,6 +46,7 @@
 #include "exchange.hpp"
 #include "gpu.hpp"
 #include "material.hpp"
+#include "montecarlo.hpp"
 #include "random.hpp"
 #include "sim.hpp"
 #include "stats.hpp"
@@ -342,6 +343,30 @@ void mc_step() {
    fail(vgpu_mc_counters(g_h, &moves, &rejects), "mc counters");
    sim::mc_statistics_moves = moves;
    sim::mc_statistics_reject = rejects;
+}
+
+// Constrained Monte Carlo step on the GPU (montecarlo::cmc_step,
+// src/montecarlo/cmc.cpp:282-490): about N pair moves; the first call sets
+// the constraint (sim::constraint_phi, sim::constraint_theta) and, unless a
+// checkpoint was loaded, turns the spins along it as CMCinit does.  hdr/cuda.hpp
+// has no such entry; a host that adds gpu::cmc_step() forwards it here.
+void cmc_step();
+void cmc_step() {
+   static bool setup = false;
+   if (!setup) {
+      fail(vgpu_cmc_setup(g_h, sim::constraint_phi, sim::constraint_theta, sim::checkpoint_loaded_flag ? 0 : 1),
+           "cmc setup");
+      setup = true;
+   }
+   sync_params();
+   fail(vgpu_cmc_sweep(g_h, 1), "cmc step");
+   double c[4];
+   fail(vgpu_cmc_get(g_h, nullptr, c), "cmc counters");
+   montecarlo::cmc::mc_total = c[0];
+   montecarlo::cmc::mc_success = c[1];
+   montecarlo::cmc::energy_reject = c[2];
+   montecarlo::cmc::sphere_reject = c[3];
+   montecarlo::cmc::is_initialised = true;
 }
 
 void finalize() {
