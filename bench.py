@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--no-dipole", action="store_true", help="leave out the macrocell dipole field")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and Monte Carlo side results")
     ap.add_argument("--no-error", action="store_true", help="skip the FP32-vs-FP64 error figure of the main line")
+    ap.add_argument("--shard", action="store_true",
+                    help="strong scaling: one FCC L^3 system cut into N spatial shards (one per GPU), NCCL halo "
+                         "exchange of the boundary spins overlapping the core atoms' passes")
     ap.add_argument("--e2e-steps", type=int, default=2000,
                     help="steps of the end-to-end run (the workload's 2,000: initial upload and final download once)")
     ap.add_argument("--records", choices=["auto", "wide"], default="auto",
@@ -471,6 +474,56 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def shard_arm(args, rank, world, local, dist):
+    """--shard: the workload system (FCC L^3, dipole field on) cut into
+    `world` spatial shards of equal atom count (vampire_b200.shard), one per
+    GPU: each pass exchanges its input state's halo over NCCL on a
+    communication stream while the core atoms run, then runs the boundary
+    atoms; the dipole cell moments are all-reduced every 100 steps.  Strong
+    scaling: value = all spins x steps / the slowest rank's CUDA-event time."""
+    import torch
+    from vampire_b200 import shard as SH
+    from vampire_b200 import system as S
+    sysm = S.config_fcc_tensor(L=args.L, seed=2024, dipole=not args.no_dipole)
+    plan = SH.make_plan(sysm, world)[rank]
+    sh = SH.ShardedSimulation(sysm, plan, device=local, precision="fp32", noise_seed=1000)
+    if sysm.cells is not None:
+        sh.dipole_setup(sysm.cells)
+    sh.step(args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(sh.stream)
+    sh.step(args.steps)
+    ev1.record(sh.stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        tt = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = sysm.n * args.steps / (ms * 1e-3)
+    if rank == 0:
+        cfg = workload_config(args.L, world)
+        cfg["parallelism"] = (f"{world} spatial shards (index slabs), NCCL halo exchange overlapping the core atoms"
+                              if world > 1 else "one shard (no exchange)")
+        cfg["ranges"] = {"core": list(sh.ranges[0]) if sh.ranges else None, "owned": plan.n_owned,
+                         "halo": int(plan.halo.size)}
+        print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                          "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                          "config": cfg, "clocks": clk, "mode": "shard", "e2e": None,
+                          "gpu_launches": None}), flush=True)
+    sh.sim.close()
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -487,6 +540,15 @@ def main():
         dist.init_process_group(backend, timeout=timedelta(seconds=600))
     if args.impl == "reference":
         reference_arm(args, rank, world)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    if args.shard:
+        from vampire_b200 import build as vbuild
+        vbuild.build()
+        torch.cuda.set_device(local)
+        shard_arm(args, rank, world, local, dist)
         if dist:
             dist.barrier()
             dist.destroy_process_group()

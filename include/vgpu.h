@@ -304,6 +304,16 @@ int vgpu_llg_heun(vgpu_handle h, uint64_t n_steps);
 #define VGPU_PASS_CORRECTOR 1
 int vgpu_llg_pass(vgpu_handle h, int pass);
 
+/* One pass over part of the updated atoms, first_atom .. end_atom - 1
+ * (first_atom a multiple of 32, end_atom at most the owned count): a shard
+ * runs its core atoms while the halo exchange of the pass's input state is in
+ * flight, then its boundary atoms -- the reference's split around
+ * mpi_init_halo_swap / mpi_complete_halo_swap (src/mpi/LLGHeun-mpi.cpp:61-140).
+ * The corrector range that ends at the last owned atom completes the step
+ * (step counter, dipole cadence), so the ranges of a corrector pass run in
+ * ascending order of their end.  Not with window staging. */
+int vgpu_llg_pass_range(vgpu_handle h, int pass, int32_t first_atom, int32_t end_atom);
+
 /* The uploaded system is a shard: atoms 0..n_owned-1 are owned and updated
  * by the passes (and summed by the statistics); the rest are halo copies of
  * other ranks' atoms that the host refreshes between passes.  noise_base is
@@ -322,6 +332,12 @@ int vgpu_set_owned(vgpu_handle h, int32_t n_owned, int64_t noise_base);
 #define VGPU_STATE_PREDICTOR 1
 int vgpu_halo_pack(vgpu_handle h, int which, const int32_t* idx, int32_t count, void* out);
 int vgpu_halo_unpack(vgpu_handle h, int which, int32_t first, int32_t count, const void* in);
+/* The same on another stream of the handle's device (a cudaStream_t as
+ * void*), so that a shard's exchange runs beside its core-range pass; the
+ * caller orders them with events: the pack after the pass that wrote the
+ * state, the boundary-range pass after the unpack. */
+int vgpu_halo_pack_on(vgpu_handle h, int which, const int32_t* idx, int32_t count, void* out, void* stream);
+int vgpu_halo_unpack_on(vgpu_handle h, int which, int32_t first, int32_t count, const void* in, void* stream);
 
 /* Advance n_steps of the LLG-Midpoint integrator (sim::LLG_Midpoint,
  * src/simulate/LLGMidpoint.cpp:48-150; sim:integrator=llg-midpoint): the

@@ -118,6 +118,107 @@ def _rank_main(rank, world, port, maker_name, steps, seed, out_dir):
         dist.destroy_process_group()
 
 
+def _rank_main_overlap(rank, world, port, maker_name, steps, seed, out_dir):
+    """As _rank_main, in the overlapped order of ShardedSimulation.step: each
+    pass posts the exchange of its input state, updates the core atoms while
+    the halo still holds the previous values, completes the exchange, then
+    updates the boundary ranges.  A pass over a range is the oracle's pass of
+    the whole shard with only that range's atoms taken."""
+    import torch
+    import torch.distributed as dist
+    from oracle import oracle as O
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        s = {"fcc": _fcc, "sc": _sc_open, "fcc_big": lambda: _fcc(L=12)}[maker_name]()
+        plan = SH.make_plan(s, world)[rank]
+        loc = SH.local_system(s, plan)
+        o = O.OracleSystem(loc)
+        n = loc.n
+        glob = np.concatenate([plan.owned, plan.halo])
+        rng = np.random.default_rng(seed)
+        xi_all = rng.standard_normal((steps, 3, s.n))
+        ex = SH.HaloExchange(plan)
+        ranges = SH.split_ranges(loc, plan.n_owned)
+        assert ranges is not None or maker_name != "fcc_big"
+        # no core range: nothing runs during the exchange
+        order = [ranges[0]] + ranges[1] if ranges else [(0, 0), (0, plan.n_owned)]
+        state = {"s": loc.spins.copy(), "p": loc.spins.copy()}
+
+        def exchange(key, run):
+            cur = state[key]
+            pend = ex.begin(lambda peer, idx: torch.from_numpy(np.ascontiguousarray(cur[:, idx]).ravel()),
+                            lambda k: torch.empty(k, dtype=torch.float64))
+            run(order[0])                   # core: the halo still holds the old values
+            def unpack(peer, first, count, buf):
+                cur[:, first:first + count] = buf.numpy().reshape(3, count)
+            ex.end(pend, unpack)
+            for r in order[1:]:
+                run(r)
+
+        keep = np.zeros((12, n))
+        for t in range(steps):
+            xi = xi_all[t][:, glob].ravel()
+
+            def predict(r):
+                p, k = o.heun_predict(state["s"], xi)
+                state["p"][:, r[0]:r[1]] = p[:, r[0]:r[1]]
+                keep[:, r[0]:r[1]] = k.reshape(12, n)[:, r[0]:r[1]]
+
+            def correct(r):
+                s1 = o.heun_correct(state["s"], state["p"], keep.ravel().copy())
+                state["s"][:, r[0]:r[1]] = s1[:, r[0]:r[1]]
+
+            exchange("s", predict)
+            exchange("p", correct)
+        np.save(os.path.join(out_dir, f"rank{rank}.npy"), state["s"][:, :plan.n_owned])
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_split_ranges_core_needs_no_halo():
+    """The core range's atoms read no halo atom; the ranges tile the owned
+    atoms; core and boundary cuts fall on slice (32-atom) boundaries; the last
+    range ends at the owned count."""
+    s = _fcc(L=12)
+    for world in (2, 3):
+        for plan in SH.make_plan(s, world):
+            loc = SH.local_system(s, plan)
+            (c0, c1), bnd = SH.split_ranges(loc, plan.n_owned)
+            assert c0 % 32 == 0 and c1 % 32 == 0 and c1 > c0
+            for i in range(c0, c1):
+                assert np.all(loc.nl[loc.nl_start[i]:loc.nl_end[i] + 1] < plan.n_owned)
+            cover = sorted([(c0, c1)] + bnd)
+            assert cover[0][0] == 0 and cover[-1][1] == plan.n_owned
+            assert all(a[1] == b[0] for a, b in zip(cover, cover[1:]))
+            assert bnd[-1][1] == plan.n_owned
+
+
+@pytest.mark.parametrize("maker_name,world", [("fcc_big", 2), ("fcc_big", 3)])
+def test_gloo_overlapped_shards_equal_whole_system(tmp_path, maker_name, world):
+    """The overlapped schedule (core range during the exchange) reproduces
+    the whole-system oracle bit for bit over 4 stochastic steps."""
+    import torch.multiprocessing as mp
+    from oracle import oracle as O
+    steps, seed = 4, 5
+    mp.start_processes(_rank_main_overlap, args=(world, _free_port(), maker_name, steps, seed, str(tmp_path)),
+                       nprocs=world, join=True, start_method="spawn")
+    s = _fcc(L=12)
+    rng = np.random.default_rng(seed)
+    xi_all = rng.standard_normal((steps, 3, s.n))
+    o = O.OracleSystem(s)
+    ref = s.spins.copy()
+    for t in range(steps):
+        ref = o.llg_heun(ref, 1, xi=xi_all[t].ravel())
+    got = np.zeros_like(ref)
+    for plan in SH.make_plan(s, world):
+        got[:, plan.owned] = np.load(tmp_path / f"rank{plan.rank}.npy")
+    np.testing.assert_array_equal(got, ref)
+
+
 @pytest.mark.parametrize("maker_name,world", [("fcc", 2), ("sc", 3)])
 def test_gloo_sharded_oracle_equals_whole_system(tmp_path, maker_name, world):
     import torch.multiprocessing as mp

@@ -8,6 +8,8 @@ whole system stepped on one handle bit for bit (same bond order, same Philox
 counters through noise_base), and the shards' raw statistics sums must add
 up to the whole system's magnetisation.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -229,3 +231,103 @@ def test_dipole_shards_equal_whole_system(vgpu_lib, solver, prec, nranks):
     finally:
         for sim in sims:
             sim.close()
+
+
+def _step_shards_overlapped(V, torch, plans, sims, ranges, steps, dtype):
+    """The overlapped order on one GPU: every shard's core range, the halo
+    refresh (host-driven), then the boundary ranges, for each pass."""
+    refresh = _refresher(torch, plans, sims, dtype)
+    for _ in range(steps):
+        for which, state in ((V.PASS_PREDICTOR, V.STATE_SPIN), (V.PASS_CORRECTOR, V.STATE_PREDICTOR)):
+            for sim, rg in zip(sims, ranges):
+                if rg is not None:
+                    sim.llg_pass_range(which, *rg[0])
+            refresh(state)
+            for sim, rg, p in zip(sims, ranges, plans):
+                for a, b in (rg[1] if rg is not None else [(0, p.n_owned)]):
+                    sim.llg_pass_range(which, a, b)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("nranks", [2, 3])
+def test_range_passes_equal_whole_system(vgpu_lib, prec, nranks):
+    """vgpu_llg_pass_range: shards stepped core range first, boundary ranges
+    after the halo refresh (the overlapped order), staged FP32 passes
+    included, equal the whole system on one handle bit for bit; the step
+    counter advances once per step."""
+    import torch
+    from vampire_b200 import vgpu as V
+    s = S.config_fcc_tensor(L=12, seed=3)          # 6912 spins, tensor + DMI, 2 materials, T = 300 K
+    plans = SH.make_plan(s, nranks)
+    dtype = torch.float32 if prec == "fp32" else torch.float64
+    sims, ranges = [], []
+    try:
+        for p in plans:
+            loc = SH.local_system(s, p)
+            sim = V.Simulation(loc, precision=prec, noise_seed=9)
+            sim.set_owned(p.n_owned, p.noise_base)
+            sims.append(sim)
+            ranges.append(SH.split_ranges(loc, p.n_owned))
+        assert all(r is not None for r in ranges)
+        steps = 8
+        _step_shards_overlapped(V, torch, plans, sims, ranges, steps, dtype)
+        assert all(sim.step == steps for sim in sims)
+        with V.Simulation(s, precision=prec, noise_seed=9) as whole:
+            whole.llg_heun(steps)
+            ref = whole.spins()
+        got = np.zeros_like(ref)
+        for sim, p in zip(sims, plans):
+            got[:, p.owned] = sim.spins()[:, :p.n_owned]
+        np.testing.assert_array_equal(got, ref)
+    finally:
+        for sim in sims:
+            sim.close()
+
+
+def test_range_pass_arguments_checked(vgpu_lib):
+    from vampire_b200 import vgpu as V
+    s = S.config_fcc_tensor(L=3, seed=3)
+    with V.Simulation(s) as sim:
+        for first, end in ((16, 64), (0, s.n + 1), (64, 32), (-32, 0)):
+            with pytest.raises(V.VGPUError) as e:
+                sim.llg_pass_range(V.PASS_PREDICTOR, first, end)
+            assert e.value.code == V.ERR_ARG
+
+
+def _one_rank_main(rank, port, out):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=timedelta(seconds=60),
+                            device_id=torch.device("cuda", 0))
+    try:
+        from vampire_b200 import vgpu as V
+        s = S.config_fcc_tensor(L=6, seed=3)
+        plan = SH.make_plan(s, 1)[0]
+        sh = SH.ShardedSimulation(s, plan, device=0, noise_seed=9)
+        assert sh.ranges is not None
+        sh.step(6)
+        got = sh.owned_spins()
+        with V.Simulation(s, noise_seed=9) as whole:
+            whole.llg_heun(6)
+            ref = whole.spins()
+        np.save(out, np.abs(got - ref).max())
+        sh.sim.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_simulation_one_rank_nccl(vgpu_lib, tmp_path):
+    """ShardedSimulation over a one-rank NCCL group: the overlapped step
+    (communication stream, events, core and boundary ranges) with no peers
+    equals the whole system bit for bit."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    out = str(tmp_path / "dev.npy")
+    mp.start_processes(_one_rank_main, args=(port, out), nprocs=1, join=True, start_method="spawn")
+    assert float(np.load(out)) == 0.0

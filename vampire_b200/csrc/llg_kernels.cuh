@@ -141,7 +141,7 @@ __device__ __forceinline__ void llg_correct_atom(const LLGArgs<R>& a, int i) {
 
 template <typename R, int FMT, int MODE, int VAR>
 __global__ void __launch_bounds__(256) llg_pass_kernel(const LLGArgs<R> a) {
-   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   const int i = (MODE == PASS_FIELD ? 0 : 32 * a.slice_first) + blockIdx.x * blockDim.x + threadIdx.x;
    if (i >= (MODE == PASS_FIELD ? a.n : a.n_upd)) return;
    if (MODE == PASS_PREDICTOR) {
       llg_predict_atom<R, FMT, 0, VAR>(a, i);
@@ -169,8 +169,8 @@ inline void launch_mode(const LLGArgs<R>& a, int mode, int grid, int bs, cudaStr
 template <typename R, int FMT>
 inline cudaError_t launch_fmt(const LLGArgs<R>& a, int mode, cudaStream_t st) {
    const int bs = 256;
-   const int grid = ((mode == PASS_FIELD ? a.n : a.n_upd) + bs - 1) / bs;
-   if (grid == 0) return cudaSuccess;
+   const int grid = ((mode == PASS_FIELD ? a.n : a.n_upd - 32 * a.slice_first) + bs - 1) / bs;
+   if (grid <= 0) return cudaSuccess;
    if (a.integrator == INTEG_MIDPOINT && mode != PASS_FIELD) launch_mode<R, FMT, VAR_MIDPOINT>(a, mode, grid, bs, st);
    else if (a.aniso_ext || a.bq_off) launch_mode<R, FMT, VAR_HEUN_EXT>(a, mode, grid, bs, st);
    else launch_mode<R, FMT, VAR_HEUN>(a, mode, grid, bs, st);

@@ -82,7 +82,11 @@ static cudaError_t launch_serialised(void (*kernel)(Args...), dim3 g, dim3 b, in
 cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, const StageCfg& c, cudaStream_t st) {
    if (c.grid == 0) return cudaSuccess;
    if ((a.crec != nullptr) != c.crec) return cudaErrorInvalidValue;  // record layout of the prepared shape
-   const dim3 g(c.grid), b(32 * c.sl);
+   // tiles of the updated range: slices slice_first .. ceil(n_upd / 32) - 1
+   const int ntiles = ((a.n_upd + 31) / 32 - a.slice_first + c.sl - 1) / c.sl;
+   if (ntiles <= 0) return cudaSuccess;
+   if (c.win && a.slice_first != 0) return cudaErrorInvalidValue;  // window plans cover whole shards
+   const dim3 g(std::min(c.grid, ntiles)), b(32 * c.sl);
    if (c.win) {
       if (!a.lrec || !a.wseg) return cudaErrorInvalidValue;
       const int smem = c.buf_bytes + 12 * c.wmax + c.dict_bytes;
@@ -102,7 +106,7 @@ cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, co
 #define VGPU_STAGED_C(S, B, C)                                                                                 \
    e = launch_serialised(mode == PASS_PREDICTOR ? llg_staged_kernel<PASS_PREDICTOR, S, B, C>                   \
                                                 : llg_staged_kernel<PASS_CORRECTOR, S, B, C>,                  \
-                         g, b, smem, st, a, nslices, (int)c.ntiles, (int)c.buf_bytes);
+                         g, b, smem, st, a, nslices, ntiles, (int)c.buf_bytes);
 #define VGPU_STAGED(S, B)                                                                                      \
    if (c.sl == S && c.nbuf == B) {                                                                             \
       cudaError_t e;                                                                                           \

@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
    // thread 0: expect the tile's bytes and start its bulk copies: records,
    // own-atom arrays (and, with the first tile, the dictionary)
    auto issue = [&](int t, int b, bool first) {
-      const int s0 = t * SL;
+      const int s0 = a.slice_first + t * SL;
       const int s1 = min(s0 + SL, nslices);
       const int o0 = __ldg(a.slice_off + s0), o1 = __ldg(a.slice_off + s1);
       const uint32_t bytes = (uint32_t)(o1 - o0) * (CREC ? 4u : 16u);
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
       b = NBUF == 1 ? 0 : (k & 1);
       if (tid == 0 && k > 0 && NBUF == 1) issue(t, 0, false);
       if (tid == 0 && NBUF == 2 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x, b ^ 1, false);
-      const int i = t * TS + tid;
+      const int i = (a.slice_first + t * SL) * 32 + tid;
       const bool act = i < a.n_upd;
       // the tile's Gaussians (the Philox noise needs no data) while the copy lands;
       // the predictor keeps them for the corrector
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
          thermal_xi(a, act ? i : 0, g[0], g[1], g[2]);
          if (MODE == PASS_PREDICTOR && a.gx && act) { a.gx[i] = g[0]; a.gy[i] = g[1]; a.gz[i] = g[2]; }
       }
-      const int tile_off = __ldg(a.slice_off + t * SL);
+      const int tile_off = __ldg(a.slice_off + a.slice_first + t * SL);
       const bool done = mbar_wait_bounded(&mbar[b], (phase >> b) & 1u);
       if (__syncthreads_or(!done)) {  // every thread takes the same branch
          failed = true;

@@ -394,6 +394,7 @@ LLGArgs<R> make_args(vgpu_ctx* h) {
    a.bq_col = (const int*)S.bq_col;
    a.bq_j = (const R*)S.bq_j;
    a.n_upd = S.n_owned;
+   a.slice_first = 0;
    a.noise_base = S.noise_base;
    a.slice_off = (const int*)S.slice_off;
    a.col = (const int*)S.col;
@@ -588,11 +589,16 @@ static int prepare_passes(vgpu_ctx* h, bool* staged_out, int integrator = INTEG_
    return VGPU_OK;
 }
 
-// one fused pass; the corrector completes the step (counter, dipole cadence)
+// one fused pass over the updated atoms 32 first_slice .. end - 1 (end < 0:
+// all updated atoms); the corrector whose range ends at the last updated atom
+// completes the step (counter, dipole cadence)
 template <typename R>
-static int run_pass(vgpu_ctx* h, int mode, bool staged, int integrator = INTEG_HEUN) {
+static int run_pass(vgpu_ctx* h, int mode, bool staged, int integrator = INTEG_HEUN, int first_slice = 0,
+                    int end = -1) {
    LLGArgs<R> a = make_args<R>(h);
    a.integrator = integrator;
+   a.slice_first = first_slice;
+   if (end >= 0) a.n_upd = end;
    if (staged && !h->sys.stage.win) {
       a.gx = (R*)h->sys.g_store[0]; a.gy = (R*)h->sys.g_store[1]; a.gz = (R*)h->sys.g_store[2];
    }
@@ -602,7 +608,7 @@ static int run_pass(vgpu_ctx* h, int mode, bool staged, int integrator = INTEG_H
    h->prof_end(kind);
    if (e != cudaSuccess) return cuda_err(h, e, "llg_heun launch");
    h->kernel_launches += 1;
-   if (mode == PASS_PREDICTOR) return VGPU_OK;
+   if (mode == PASS_PREDICTOR || a.n_upd != h->sys.n_owned) return VGPU_OK;
    h->step++;
    return h->after_step();
 }
@@ -1144,6 +1150,31 @@ extern "C" int vgpu_llg_pass(vgpu_handle h, int pass) {
    return h->prec == VGPU_PREC_FP64 ? llg_pass_typed<double>(h, mode) : llg_pass_typed<float>(h, mode);
 }
 
+template <typename R>
+static int llg_pass_range_typed(vgpu_ctx* h, int mode, int first, int end) {
+   bool staged = false;
+   int rc = h->fields_ready();
+   if (!rc) rc = prepare_passes<R>(h, &staged);
+   if (!rc && staged && h->sys.stage.win && first != 0)
+      return set_err(h, VGPU_ERR_STATE, "window-staged passes run whole shards only");
+   return rc ? rc : run_pass<R>(h, mode, staged, INTEG_HEUN, first / 32, end);
+}
+
+extern "C" int vgpu_llg_pass_range(vgpu_handle h, int pass, int32_t first_atom, int32_t end_atom) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (!(h->params.dt > 0.0)) return set_err(h, VGPU_ERR_STATE, "vgpu_set_params not called");
+   if (pass != VGPU_PASS_PREDICTOR && pass != VGPU_PASS_CORRECTOR) return set_err(h, VGPU_ERR_ARG, "unknown pass %d", pass);
+   if (first_atom < 0 || first_atom % 32 != 0 || end_atom < first_atom || end_atom > h->sys.n_owned)
+      return set_err(h, VGPU_ERR_ARG, "range %d..%d: the first atom must be a multiple of 32 and the end at most %d",
+                     first_atom, end_atom, h->sys.n_owned);
+   if (first_atom == end_atom) return VGPU_OK;
+   cudaSetDevice(h->device);
+   const int mode = pass == VGPU_PASS_PREDICTOR ? PASS_PREDICTOR : PASS_CORRECTOR;
+   return h->prec == VGPU_PREC_FP64 ? llg_pass_range_typed<double>(h, mode, first_atom, end_atom)
+                                    : llg_pass_range_typed<float>(h, mode, first_atom, end_atom);
+}
+
 extern "C" int vgpu_set_owned(vgpu_handle h, int32_t n_owned, int64_t noise_base) {
    if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
    SysDev& S = h->sys;
@@ -1165,16 +1196,17 @@ extern "C" int vgpu_set_owned(vgpu_handle h, int32_t n_owned, int64_t noise_base
 
 template <typename R>
 static int halo_typed(vgpu_handle h, int which, const int32_t* idx, int32_t first, int32_t count, void* buf,
-                      bool pack) {
+                      bool pack, cudaStream_t stream = nullptr) {
    SysDev& S = h->sys;
    void* const* st = which == VGPU_STATE_SPIN ? S.s : S.p;
    if (count == 0) return VGPU_OK;
    const int grid = (count + 255) / 256;
+   cudaStream_t on = stream ? stream : h->stream;
    if (pack)
-      halo_pack_kernel<R><<<grid, 256, 0, h->stream>>>((const R*)st[0], (const R*)st[1], (const R*)st[2], idx, count,
-                                                       S.n, (R*)buf);
+      halo_pack_kernel<R><<<grid, 256, 0, on>>>((const R*)st[0], (const R*)st[1], (const R*)st[2], idx, count,
+                                                S.n, (R*)buf);
    else
-      halo_unpack_kernel<R><<<grid, 256, 0, h->stream>>>((R*)st[0], (R*)st[1], (R*)st[2], first, count,
+      halo_unpack_kernel<R><<<grid, 256, 0, on>>>((R*)st[0], (R*)st[1], (R*)st[2], first, count,
                                                          (const R*)buf);
    h->kernel_launches++;
    return cuda_err(h, cudaGetLastError(), pack ? "halo pack" : "halo unpack");
@@ -1199,6 +1231,30 @@ extern "C" int vgpu_halo_unpack(vgpu_handle h, int which, int32_t first, int32_t
    cudaSetDevice(h->device);
    return h->prec == VGPU_PREC_FP64 ? halo_typed<double>(h, which, nullptr, first, count, const_cast<void*>(in), false)
                                     : halo_typed<float>(h, which, nullptr, first, count, const_cast<void*>(in), false);
+}
+
+extern "C" int vgpu_halo_pack_on(vgpu_handle h, int which, const int32_t* idx, int32_t count, void* out,
+                                 void* stream) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (which != VGPU_STATE_SPIN && which != VGPU_STATE_PREDICTOR) return set_err(h, VGPU_ERR_ARG, "unknown state");
+   if (count < 0 || (count > 0 && (!idx || !out))) return set_err(h, VGPU_ERR_ARG, "bad halo buffer");
+   cudaSetDevice(h->device);
+   return h->prec == VGPU_PREC_FP64 ? halo_typed<double>(h, which, idx, 0, count, out, true, (cudaStream_t)stream)
+                                    : halo_typed<float>(h, which, idx, 0, count, out, true, (cudaStream_t)stream);
+}
+
+extern "C" int vgpu_halo_unpack_on(vgpu_handle h, int which, int32_t first, int32_t count, const void* in,
+                                   void* stream) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (which != VGPU_STATE_SPIN && which != VGPU_STATE_PREDICTOR) return set_err(h, VGPU_ERR_ARG, "unknown state");
+   if (count < 0 || first < 0 || (int64_t)first + count > h->sys.n || (count > 0 && !in))
+      return set_err(h, VGPU_ERR_ARG, "halo block %d..%d outside the system", first, first + count);
+   cudaSetDevice(h->device);
+   return h->prec == VGPU_PREC_FP64
+              ? halo_typed<double>(h, which, nullptr, first, count, const_cast<void*>(in), false, (cudaStream_t)stream)
+              : halo_typed<float>(h, which, nullptr, first, count, const_cast<void*>(in), false, (cudaStream_t)stream);
 }
 
 extern "C" int vgpu_thermal_noise(vgpu_handle h, uint64_t step, double* xi) {

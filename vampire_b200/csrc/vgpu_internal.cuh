@@ -51,6 +51,8 @@ struct LLGArgs {
    int n;                    // atoms (array length of the per-atom inputs)
    int n_alloc;              // row stride of SoA per-atom tables (n rounded up to slices, + pad atom)
    int n_upd;                // atoms the passes update: all, or the owned atoms of a shard (0..n_upd-1)
+   int slice_first;          // first slice a pass updates (0: from atom 0); the pass covers atoms
+                             // 32 slice_first .. n_upd-1 (a shard's core or boundary range)
    uint32_t noise_base;      // added to the atom index in the Philox counter (global index of a shard's atom 0)
    const int* slice_off;     // [nslices+1] SELL-32 entry offsets
    const int* col;           // packed neighbour index (| mat << mat_shift)

@@ -20,10 +20,16 @@ The same decomposition here, one process per GPU over NVLink/NCCL:
   step: one send and one receive per peer (three components packed into one
   message), posted together with ``torch.distributed.batch_isend_irecv``.
   It works with CPU tensors over gloo (tests) and device tensors over NCCL.
-* ``ShardedSimulation`` drives one rank's shard on its GPU: predictor pass,
-  halo exchange of s', corrector pass, halo exchange of s.  The fused passes
-  update the owned atoms only (``vgpu_set_owned``) and key the thermal noise
-  by global atom index, so a sharded run draws the same noise as one GPU.
+* ``ShardedSimulation`` drives one rank's shard on its GPU.  Every pass
+  starts the halo exchange of its input state (s for the predictor, s' for
+  the corrector) on a communication stream, runs the shard's core atoms --
+  the owned atoms whose neighbours are all owned (``split_ranges``) -- on the
+  library's stream meanwhile, then, once the exchange has landed, the
+  boundary atoms: the reference's mpi_init_halo_swap / core update /
+  mpi_complete_halo_swap / boundary update (src/mpi/LLGHeun-mpi.cpp:61-140).
+  The fused passes update the owned atoms only (``vgpu_set_owned``) and key
+  the thermal noise by global atom index, so a sharded run draws the same
+  noise as one GPU.
 
 Statistics combine across ranks from the raw per-bin sums of each shard
 (``vgpu_stats_get_sums``) with one all-reduce.
@@ -177,6 +183,39 @@ def local_system(s: SpinSystem, plan: ShardPlan) -> SpinSystem:
                       masks=masks, cells=None, aniso=aniso)
 
 
+def split_ranges(loc: SpinSystem, n_owned: int):
+    """Atom ranges of a shard's overlapped passes: (core, boundary) with core =
+    (c0, c1) the longest run of owned atoms whose neighbours are all owned
+    (atoms n_owned.. are the halo), cut to multiples of 32 (slice boundaries),
+    and boundary = the ranges before and after it, the last one ending at
+    n_owned (the corrector range that completes the step runs last).  None
+    when no core range of at least one slice exists."""
+    if n_owned <= 0:
+        return None
+    deg = (loc.nl_end[:n_owned] - loc.nl_start[:n_owned] + 1).astype(np.int64)
+    src = np.repeat(np.arange(n_owned), np.maximum(deg, 0))
+    bonds = np.concatenate([np.arange(a, b + 1) for a, b in zip(loc.nl_start[:n_owned], loc.nl_end[:n_owned])
+                            if b >= a]) if deg.sum() else np.zeros(0, np.int64)
+    needs = np.zeros(n_owned, dtype=bool)
+    if bonds.size:
+        np.logical_or.at(needs, src, loc.nl[bonds] >= n_owned)
+    best, start = (0, 0), None
+    for i in range(n_owned + 1):
+        if i < n_owned and not needs[i]:
+            if start is None:
+                start = i
+        elif start is not None:
+            if i - start > best[1] - best[0]:
+                best = (start, i)
+            start = None
+    c0 = -(-best[0] // 32) * 32
+    c1 = min(best[1] // 32 * 32, (n_owned - 1) // 32 * 32)
+    if c1 <= c0:
+        return None
+    boundary = [(a, b) for a, b in ((0, c0), (c1, n_owned)) if b > a]
+    return (c0, c1), boundary
+
+
 class HaloExchange:
     """One halo refresh: for every peer, pack(peer, local_idx) -> tensor of
     3*count values is sent, and unpack(peer, first, count, tensor) receives
@@ -199,6 +238,30 @@ class HaloExchange:
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
+        for peer, (first, count, buf) in recv.items():
+            unpack(peer, first, count, buf)
+
+    def begin(self, pack: Callable, alloc: Callable):
+        """Post one refresh (every receive, then every send) and return its
+        pending state; ``end`` completes it.  Work between the two must not
+        read the halo atoms."""
+        import torch.distributed as dist
+        ops, recv, keep = [], {}, []
+        for peer, (first, count) in sorted(self.plan.recv.items()):
+            buf = alloc(3 * count)
+            recv[peer] = (first, count, buf)
+            ops.append(dist.P2POp(dist.irecv, buf, peer, self.group))
+        for peer, idx in sorted(self.plan.send.items()):
+            out = pack(peer, idx)
+            keep.append(out)  # alive until the send completes
+            ops.append(dist.P2POp(dist.isend, out, peer, self.group))
+        reqs = dist.batch_isend_irecv(ops) if ops else []
+        return reqs, recv, keep
+
+    def end(self, pending, unpack: Callable) -> None:
+        reqs, recv, _ = pending
+        for req in reqs:
+            req.wait()
         for peer, (first, count, buf) in recv.items():
             unpack(peer, first, count, buf)
 
@@ -260,6 +323,9 @@ class ShardedSimulation:
         self.stream = torch.cuda.ExternalStream(self.sim.stream_ptr(), device=self.device)
         self.idx = {p: torch.as_tensor(ix, dtype=torch.int32, device=self.device) for p, ix in plan.send.items()}
         self.halo = HaloExchange(plan, group)
+        # core atoms run while the exchange is in flight (on its own stream)
+        self.ranges = split_ranges(self.local, plan.n_owned)
+        self.comm = torch.cuda.Stream(device=self.device)
         self.group = group
         self._torch = torch
         self._global_type = np.ascontiguousarray(s.type, dtype=np.int32)
@@ -299,13 +365,60 @@ class ShardedSimulation:
             sum_cell_moments(self._moments, self.group)
         self.sim.dipole_finish()
 
+    def _exchange_begin(self, which: int):
+        """Start the halo exchange of state `which` on the communication
+        stream, after everything on the library's stream so far."""
+        torch = self._torch
+        ev = torch.cuda.Event()
+        ev.record(self.stream)
+        self.comm.wait_event(ev)
+        comm = self.comm.cuda_stream
+
+        def pack(peer, _idx):
+            ix = self.idx[peer]
+            out = torch.empty(3 * ix.numel(), dtype=self.dtype, device=self.device)
+            self.sim.halo_pack_on(which, ix.data_ptr(), ix.numel(), out.data_ptr(), comm)
+            return out
+
+        def alloc(k):
+            return torch.empty(k, dtype=self.dtype, device=self.device)
+
+        with torch.cuda.stream(self.comm):
+            return self.halo.begin(pack, alloc)
+
+    def _exchange_end(self, which: int, pending) -> None:
+        """Complete the exchange; the library's stream then waits for it."""
+        torch = self._torch
+        comm = self.comm.cuda_stream
+
+        def unpack(peer, first, count, buf):
+            self.sim.halo_unpack_on(which, first, count, buf.data_ptr(), comm)
+
+        with torch.cuda.stream(self.comm):
+            self.halo.end(pending, unpack)
+            done = torch.cuda.Event()
+            done.record(self.comm)
+        self.stream.wait_event(done)
+
+    def _pass(self, which_pass: int, input_state: int) -> None:
+        if self.ranges is None:
+            self._refresh(input_state)
+            self.sim.llg_pass(which_pass)
+            return
+        (c0, c1), boundary = self.ranges
+        pending = self._exchange_begin(input_state)
+        self.sim.llg_pass_range(which_pass, c0, c1)
+        self._exchange_end(input_state, pending)
+        for a, b in boundary:
+            self.sim.llg_pass_range(which_pass, a, b)
+
     def step(self, n_steps: int = 1) -> None:
+        """Heun steps: each pass exchanges its input state's halo while the
+        core atoms run, then runs the boundary atoms."""
         from . import vgpu
         for _ in range(n_steps):
-            self.sim.llg_pass(vgpu.PASS_PREDICTOR)
-            self._refresh(vgpu.STATE_PREDICTOR)
-            self.sim.llg_pass(vgpu.PASS_CORRECTOR)
-            self._refresh(vgpu.STATE_SPIN)
+            self._pass(vgpu.PASS_PREDICTOR, vgpu.STATE_SPIN)
+            self._pass(vgpu.PASS_CORRECTOR, vgpu.STATE_PREDICTOR)
             self._dipole_sum()
 
     def mc_setup(self, colour: np.ndarray) -> int:

@@ -339,6 +339,11 @@ class Simulation:
         """One fused pass: PASS_PREDICTOR or PASS_CORRECTOR (vgpu_llg_pass)."""
         self._check(lib().vgpu_llg_pass(self._h, C.c_int(which)))
 
+    def llg_pass_range(self, which: int, first: int, end: int) -> None:
+        """One pass over the updated atoms first..end-1 (first a multiple of
+        32; vgpu_llg_pass_range)."""
+        self._check(lib().vgpu_llg_pass_range(self._h, C.c_int(which), C.c_int32(first), C.c_int32(end)))
+
     def set_owned(self, n_owned: int, noise_base: int = 0) -> None:
         self._check(lib().vgpu_set_owned(self._h, C.c_int32(n_owned), C.c_int64(noise_base)))
 
@@ -350,6 +355,15 @@ class Simulation:
     def halo_unpack(self, which: int, first: int, count: int, in_ptr: int) -> None:
         self._check(lib().vgpu_halo_unpack(self._h, C.c_int(which), C.c_int32(first), C.c_int32(count),
                                            C.c_void_p(in_ptr)))
+
+    def halo_pack_on(self, which: int, idx_ptr: int, count: int, out_ptr: int, stream: int) -> None:
+        """halo_pack on another stream (a cudaStream_t as an integer)."""
+        self._check(lib().vgpu_halo_pack_on(self._h, C.c_int(which), C.c_void_p(idx_ptr), C.c_int32(count),
+                                            C.c_void_p(out_ptr), C.c_void_p(stream)))
+
+    def halo_unpack_on(self, which: int, first: int, count: int, in_ptr: int, stream: int) -> None:
+        self._check(lib().vgpu_halo_unpack_on(self._h, C.c_int(which), C.c_int32(first), C.c_int32(count),
+                                              C.c_void_p(in_ptr), C.c_void_p(stream)))
 
     def stats_copy_rows(self, mask_id: int, out_ptr: int) -> None:
         """Enqueue a copy of the latest rows (9 doubles per bin) to out_ptr
