@@ -515,6 +515,19 @@ int vgpu_cmc_pairs(vgpu_handle h, const int32_t* pairs, int32_t num_pairs, const
 int vgpu_cmc_get(vgpu_handle h, double* moment, double* counters);
 int vgpu_cmc_frame(vgpu_handle h, double* P9, double* pv3);
 
+/* Hybrid constrained Monte Carlo (montecarlo::cmc_mc_step, src/montecarlo/
+ * cmc_mc.cpp:291-490; sim:integrator=hybrid-constrained-monte-carlo): each
+ * material m with constrained[m] != 0 keeps its own moment along (phi_deg[m],
+ * theta_deg[m]) (material[m]:constrained, constraint-angle-phi/theta), by
+ * pair moves within that material against that material's running moment;
+ * the other materials take single-spin Metropolis moves.  init_spins: the
+ * constrained materials' spins along their directions (CMCMCinit).  Then
+ * vgpu_cmc_sweep runs hybrid steps; vgpu_cmc_material_moments gives the
+ * running moments [3*M] (mu_B) of the constrained materials. */
+int vgpu_cmc_setup_materials(vgpu_handle h, const int32_t* constrained, const double* phi_deg, const double* theta_deg,
+                             int32_t init_spins);
+int vgpu_cmc_material_moments(vgpu_handle h, double* moments);
+
 /* ---- statistics (masked reductions, FP64) -------------------------------- */
 
 /* Register a statistics mask: mask[i] in [0, mask_size) is the bin of atom i

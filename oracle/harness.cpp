@@ -314,6 +314,7 @@ static void one_step() {
                              atoms::type_array);
          break;
       case 2: sim::LLG_Midpoint(); break;
+      case 4: montecarlo::cmc_mc_step(); break;
       case 3:
 #ifdef VGPU_MC_HOOK
          if (g_gpu_mc) {
@@ -411,6 +412,7 @@ int main(int argc, char* argv[]) {
 
    const int n = atoms::num_atoms;
    std::vector<double> mag_trace;  // per recorded step: mx, my, mz, |m| (system mask, bin 0), total E
+   std::vector<double> mat_trace;  // per recorded step and material: m_x, m_y, m_z of that material
    // untimed warm-up steps (timing runs only; nothing is dumped for them)
    for (long w = 0; w < warmup; w++) {
       one_step();
@@ -453,15 +455,41 @@ int main(int argc, char* argv[]) {
          mag_trace.push_back(m[1] / m[3]);
          mag_trace.push_back(m[2] / m[3]);
          mag_trace.push_back(std::sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]) / m[3]);
+         // per material: sum mu s / sum mu
+         const int M = mp::num_materials;
+         std::vector<double> mm(4 * M, 0.0);
+         for (int i = 0; i < n; i++) {
+            const int t = atoms::type_array[i];
+            mm[4 * t + 0] += atoms::x_spin_array[i] * atoms::m_spin_array[i];
+            mm[4 * t + 1] += atoms::y_spin_array[i] * atoms::m_spin_array[i];
+            mm[4 * t + 2] += atoms::z_spin_array[i] * atoms::m_spin_array[i];
+            mm[4 * t + 3] += atoms::m_spin_array[i];
+         }
+         for (int t = 0; t < M; t++)
+            for (int q = 0; q < 3; q++) mat_trace.push_back(mm[4 * t + 3] > 0 ? mm[4 * t + q] / mm[4 * t + 3] : 0.0);
       }
    }
    const double loop_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
    if (want_time) std::cout << "HARNESS_LOOP_SECONDS " << loop_s << " ATOMS " << n << " STEPS " << steps << std::endl;
    if (!mag_trace.empty()) dumpd("mag_trace", mag_trace);
+   if (!mat_trace.empty()) dumpd("mat_trace", mat_trace);
    if (want_derived) dump_derived();
 #ifdef VGPU_MC_HOOK
    if (g_gpu_mc) gpu::finalize();
 #endif
+   if (sim::integrator == 4 && montecarlo::cmc::is_initialised) {
+      // hybrid constrained Monte Carlo: every material's frame and the counters
+      std::vector<double> fr;
+      for (int m = 0; m < mp::num_materials; m++) {
+         const auto& c = montecarlo::cmc::cmc_mat[m];
+         for (int a = 0; a < 3; a++) for (int b = 0; b < 3; b++) fr.push_back(c.ppolar_matrix[a][b]);
+         for (int a = 0; a < 3; a++) fr.push_back(c.ppolar_vector[a]);
+      }
+      dumpd("cmc_frames", fr);
+      std::vector<double> cc = {montecarlo::cmc::mc_total, montecarlo::cmc::mc_success,
+                                montecarlo::cmc::energy_reject, montecarlo::cmc::sphere_reject};
+      dumpd("cmc_counters", cc);
+   }
    if (sim::integrator == 3 && montecarlo::cmc::is_initialised) {
       // constrained Monte Carlo: its frame (cmc.cpp polar_rot_matrix) and counters
       std::vector<double> fr;

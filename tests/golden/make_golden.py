@@ -432,6 +432,49 @@ def cmc_sc12():
     print("cmc_sc12:", {T: out[f"counters_{int(T)}"] for T in CMC_TEMPS})
 
 
+HYBRID_MAT = """material:num-materials=2
+material[1]:material-name=A
+material[1]:damping-constant=0.1
+material[1]:exchange-matrix[1]=11.2e-21
+material[1]:exchange-matrix[2]=8.0e-21
+material[1]:atomic-spin-moment=1.72 !muB
+material[1]:second-order-uniaxial-anisotropy-constant=6.69e-24
+material[1]:uniaxial-anisotropy-direction=0,0,1
+material[1]:constrained=true
+material[1]:constraint-angle-phi=30
+material[1]:constraint-angle-theta=45
+material[1]:initial-spin-direction=0,0,1
+material[2]:material-name=B
+material[2]:damping-constant=0.1
+material[2]:exchange-matrix[1]=8.0e-21
+material[2]:exchange-matrix[2]=11.2e-21
+material[2]:atomic-spin-moment=2.2 !muB
+material[2]:second-order-uniaxial-anisotropy-constant=3.0e-24
+material[2]:uniaxial-anisotropy-direction=0,0,1
+material[2]:constrained=false
+material[2]:initial-spin-direction=0,0,1
+material[1]:host-alloy
+material[1]:alloy-fraction[2]=0.5
+"""
+
+
+def cmc_hybrid_sc12():
+    """Hybrid constrained Monte Carlo (montecarlo::cmc_mc_step,
+    src/montecarlo/cmc_mc.cpp:291-490; sim:integrator=
+    hybrid-constrained-monte-carlo): SC 12^3 periodic random A/B alloy
+    (moments 1.72 and 2.2 mu_B), material A constrained along phi = 30,
+    theta = 45 degrees, material B free; 500 K, 2,000 + 20,000 steps, the
+    per-material magnetisation sampled every 10 steps; the reference's frames
+    and counters."""
+    inp = sc_input(12, T=500.0, H=0.0, integrator="hybrid-constrained-monte-carlo",
+                   extra="montecarlo:algorithm=angle\n")
+    d = O.run_harness(inp, {"m.mat": HYBRID_MAT}, ["--system", "--steps", CMC_EQ + CMC_AV, "--mag-every", CMC_EVERY,
+                                                   "--mag-start", CMC_EQ], timeout=3600)
+    keep = ["mat_trace", "cmc_frames", "cmc_counters"]
+    d["sweeps"] = np.array([CMC_EQ, CMC_AV, CMC_EVERY])
+    save("cmc_hybrid_sc12", d, keep + ["sweeps"])
+
+
 MC50_EQ, MC50_AV = 5000, 10000
 
 
@@ -498,7 +541,7 @@ def sc8_config():
 
 
 ALL = [sc20_t0, sc8_t0, sc10_t300, sc6_open_t300, fcc4_dmi_t300, fcc4_dmi_t0, single_spin_applied, mc_sc16_curie,
-       mc_sc50_curie, tet_bond_exchange, sc6_vec, torque_fixtures, cmc_sc12,
+       mc_sc50_curie, tet_bond_exchange, sc6_vec, torque_fixtures, cmc_sc12, cmc_hybrid_sc12,
        fcc10_dipole_tensor, fcc10_dipole_macrocell, sc6_aniso_ho, fcc4_neel_rot, sc6_derived_t600, sc8_midpoint, sc6_biquadratic,
        sc8_config]
 

@@ -118,3 +118,60 @@ def test_chain_matches_reference_statistically(vgpu_lib, T):
           f"max perpendicular {max(perps):.2e}")
     assert z <= 3.5
     assert max(perps) < 1e-5
+
+
+def test_hybrid_frames_match_reference(vgpu_lib):
+    from oracle import oracle as O
+    from vampire_b200 import vgpu
+    d = dict(np.load(GOLDEN / "cmc_hybrid_sc12.npz"))
+    s = O.system_from_dump(d)
+    fr = d["cmc_frames"].reshape(2, 12)
+    with vgpu.Simulation(s) as sim:
+        sim.cmc_setup_materials([1, 0], [30.0, 0.0], [45.0, 0.0])
+        P, pv = sim.cmc_frame()
+    np.testing.assert_allclose(P.ravel(), fr[0, :9], atol=1e-15)
+    np.testing.assert_allclose(pv, fr[0, 9:], atol=1e-15)
+
+
+def test_hybrid_chain_matches_reference_statistically(vgpu_lib):
+    """Hybrid constrained Monte Carlo (montecarlo::cmc_mc_step): SC 12^3 A/B
+    alloy at 500 K, A constrained along (30, 45) degrees, B free, against the
+    reference's own chain (tests/golden/cmc_hybrid_sc12.npz): A's moment
+    along its constraint and B's moment projected on it within 3.5 standard
+    errors; A's moment perpendicular to the constraint zero to rounding."""
+    from oracle import oracle as O
+    from vampire_b200 import vgpu
+    d = dict(np.load(GOLDEN / "cmc_hybrid_sc12.npz"))
+    s = O.system_from_dump(d)
+    s.params.H_applied = 0.0
+    s.params.temperature = 500.0
+    eq, av, every = (int(x) for x in d["sweeps"])
+    pv = d["cmc_frames"].reshape(2, 12)[0, 9:]
+    ref = d["mat_trace"].reshape(-1, 2, 3)
+    chains_a, chains_b, perp = [], [], 0.0
+    for seed in range(4):
+        with vgpu.Simulation(s, noise_seed=300 + seed) as sim:
+            sim.cmc_setup_materials([1, 0], [30.0, 0.0], [45.0, 0.0])
+            mid = sim.add_mask(*s.masks["material"])
+            sim.cmc_sweep(eq)
+            a, b = [], []
+            for _ in range(av // every):
+                sim.cmc_sweep(every)
+                sim.stats_update(magnetization=True)
+                m, _, _ = sim.magnetization(mid)
+                rows = np.asarray(m).reshape(-1, 4)[:2]
+                vec = rows[:, :3] * rows[:, 3:4]
+                a.append(vec[0] @ pv)
+                b.append(vec[1] @ pv)
+                perp = max(perp, float(np.abs(vec[0] - (vec[0] @ pv) * pv).max()))
+            _, cnt = sim.cmc_state()
+            assert cnt[1] > 0 and abs(cnt[1] + cnt[2] + cnt[3] - cnt[0]) < 0.5
+        chains_a.append(np.mean(a))
+        chains_b.append(np.mean(b))
+    for name, g, r in (("A.e", chains_a, ref[:, 0, :] @ pv), ("B.e", chains_b, ref[:, 1, :] @ pv)):
+        mg, eg = np.mean(g), np.std(g, ddof=1) / np.sqrt(len(g))
+        mr, er = _blocks(r)
+        z = abs(mg - mr) / np.hypot(eg, er)
+        print(f"hybrid {name}: gpu {mg:.5f} +- {eg:.5f}, reference {mr:.5f} +- {er:.5f}, z {z:.2f}")
+        assert z <= 3.5
+    assert perp < 1e-5

@@ -125,3 +125,49 @@ def test_curie_sweep_matches_reference_statistically(vgpu_lib):
     tc_g, tc_r = _tc_fit(d["T"], got), _tc_fit(d["T"], ref)
     print(f"Tc gpu {tc_g:.1f} K, reference {tc_r:.1f} K")
     assert abs(tc_g - tc_r) / tc_r < 0.01
+
+
+@pytest.mark.skipif(not (GOLDEN / "mc_sc50_curie.npz").exists(), reason="config-1 reference fixture not generated")
+def test_config1_curie_sweep_matches_reference_statistically(vgpu_lib):
+    """Config 1 at its own size: SC 50^3 periodic (125,000 spins), the SC
+    ferromagnet's J, Ku and mu_s, H = 0, spins start along z, 31 temperatures
+    0..1500 K, 5,000 equilibration + 10,000 averaging sweeps, <|m|> sampled
+    every 10 sweeps, against the reference's own sequential random-site
+    Metropolis on the same protocol (tests/golden/mc_sc50_curie.npz, one
+    reference process per temperature).  The GPU runs six independent
+    checkerboard chains per temperature (two handles of 3 x 31 replicas);
+    its standard error comes from the spread of the chains, the reference's
+    from 10 blocks of 1,000 sweeps.  Every temperature within 3 standard
+    errors, Tc within 1 %."""
+    from vampire_b200 import system as S
+    from vampire_b200 import vgpu
+    d = dict(np.load(GOLDEN / "mc_sc50_curie.npz"))
+    Ts = d["T"]
+    eq, av, every = (int(x) for x in d["sweeps"])
+    base = S.config_sc_llg(50, temperature=0.0)
+    base.params.H_applied = 0.0
+    base.spins = np.tile(np.array([[0.0], [0.0], [1.0]]), (1, base.n))
+    chains = []
+    for seed in (101, 202):
+        s = S.replicas(base, np.tile(Ts, 3))
+        with vgpu.Simulation(s, noise_seed=seed) as sim:
+            mid = sim.add_mask(*s.masks["replica"])
+            sim.mc_setup()
+            sim.mc_sweep(eq)
+            sim.stats_reset()
+            for _ in range(av // every):
+                sim.mc_sweep(every)
+                sim.stats_update(magnetization=True)
+            _, mean, cnt = sim.magnetization(mid)
+        chains.append((mean.reshape(-1, 4)[:, 3] / cnt).reshape(3, Ts.size))
+    g = np.concatenate(chains)                        # (6 chains, 31 temperatures)
+    got, se = g.mean(0), g.std(0, ddof=1) / np.sqrt(g.shape[0])
+    ref, rse = d["m_mean"], d["m_se"]
+    z = np.abs(got - ref) / np.sqrt(se ** 2 + rse ** 2 + 1e-12)
+    print("m_gpu", np.round(got, 4))
+    print("m_ref", np.round(ref, 4))
+    print("z", np.round(z, 2))
+    assert np.all(z <= 3.0), z
+    tc_g, tc_r = _tc_fit(Ts, got), _tc_fit(Ts, ref)
+    print(f"config 1 Tc gpu {tc_g:.1f} K, reference {tc_r:.1f} K")
+    assert abs(tc_g - tc_r) / tc_r < 0.01

@@ -468,9 +468,19 @@ struct CMCState {
    double* u = nullptr;       // [maxK] acceptance uniforms (replay) or nullptr
    double* rnd = nullptr;     // [4 maxK] replayed Gaussians and uniforms
    double* M = nullptr;       // [3] running total moment (mu_B)
-   unsigned long long* cnt = nullptr;  // [3] accepted, energy rejections, sphere rejections
+   unsigned long long* cnt = nullptr;  // [4] accepted, energy rejections, sphere rejections,
+                                       //     rejected single-spin moves (hybrid)
    uint64_t sweep = 0;
    double total = 0.0;
+   // hybrid (montecarlo::cmc_mc_step): one constraint per material
+   bool hybrid = false;
+   int nmat = 0;
+   std::vector<int> constrained;       // [nmat]
+   std::vector<double> Pm;             // [9M] frames
+   double* Mm = nullptr;               // [6M] per material: running moment (3), constraint vector (3)
+   int* lists = nullptr;               // atoms by (colour, material), unconstrained last
+   std::vector<int> list_off;          // [ncolours * (M + 1) + 1]
+   double single_moves = 0.0;
 };
 
 static CMCState* cmc_of(vgpu_ctx* h) { return (CMCState*)h->extras[5]; }
@@ -479,7 +489,7 @@ void cmc_destroy(vgpu_ctx* h) {
    CMCState* c = cmc_of(h);
    if (!c) return;
    cudaFree(c->pairs); cudaFree(c->prop); cudaFree(c->ef); cudaFree(c->jac); cudaFree(c->mom);
-   cudaFree(c->rnd); cudaFree(c->M); cudaFree(c->cnt);
+   cudaFree(c->rnd); cudaFree(c->M); cudaFree(c->cnt); cudaFree(c->Mm); cudaFree(c->lists);
    delete c;
    h->extras[5] = nullptr;
 }
@@ -656,12 +666,15 @@ __global__ void __launch_bounds__(32) cmc_accept_kernel(LLGArgs<R> a, int K, int
    }
 }
 
-// total moment sum_i mu_s,i s_i (mu_B) into M (zeroed first), FP64
+// total moment sum_i mu_s,i s_i (mu_B) into M (zeroed first), FP64; with
+// only_mat >= 0 over the atoms of that material
 template <typename R>
-__global__ void cmc_moment_kernel(const LLGArgs<R> a, const R* __restrict__ mu_ratio, double* M) {
+__global__ void cmc_moment_kernel(const LLGArgs<R> a, const R* __restrict__ mu_ratio, double* M, int only_mat) {
    double v[3] = {0, 0, 0};
    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_upd; i += gridDim.x * blockDim.x) {
-      const double mu = (double)__ldg(mu_ratio + (a.mat ? __ldg(a.mat + i) : 0));
+      const int mi = a.mat ? __ldg(a.mat + i) : 0;
+      if (only_mat >= 0 && mi != only_mat) continue;
+      const double mu = (double)__ldg(mu_ratio + mi);
       v[0] += mu * (double)a.ax[i]; v[1] += mu * (double)a.ay[i]; v[2] += mu * (double)a.az[i];
    }
    for (int q = 0; q < 3; ++q) {
@@ -712,22 +725,22 @@ uint64_t gcd64(uint64_t a, uint64_t b) {
 // one phase: K pairs (explicit, or the affine pairing of colour c), proposals
 // in parallel, acceptance by one warp
 template <typename R>
-int cmc_phase(vgpu_handle h, const R* tab, int colour, const int* given, int K, const double* rnd, uint32_t phase) {
+int cmc_phase(vgpu_handle h, const R* tab, const int* list, int count, const int* given, int K, const double* rnd,
+              uint32_t phase, const double* P, double* Mdev) {
    CMCState* c = cmc_of(h);
-   MCState* s = mc_of(h);
    CMCArgs<R> p;
    memset(&p, 0, sizeof p);
    p.a = make_args<R>(h);
    p.sigma = tab; p.beta = tab + 100; p.mu_ratio = tab + 200;
    p.sweep = c->sweep; p.phase = phase;
-   for (int q = 0; q < 9; ++q) p.P[q] = c->P[q];
+   for (int q = 0; q < 9; ++q) p.P[q] = P[q];
    p.pairs = c->pairs; p.prop = (R*)c->prop; p.ef = c->ef; p.jac = c->jac; p.mom = c->mom; p.maxK = c->maxK;
    p.K = K;
    p.given = given;
    p.rnd = rnd;
    if (!given) {
-      p.list = s->atoms + s->colour_off[colour];
-      p.count = s->colour_off[colour + 1] - s->colour_off[colour];
+      p.list = list;
+      p.count = count;
       const uint64_t key = splitmix64(h->seed ^ splitmix64(c->sweep * 1024 + phase));
       const uint64_t n = (uint64_t)std::max(p.count, 1);
       uint64_t mul = 1 + splitmix64(key) % n;
@@ -740,7 +753,7 @@ int cmc_phase(vgpu_handle h, const R* tab, int colour, const int* given, int K, 
    if (e == cudaSuccess && K > 0) {
       cmc_accept_kernel<R><<<1, 32, 0, h->stream>>>(p.a, K, c->maxK, c->pairs, (const R*)c->prop, c->ef, c->jac,
                                                     c->mom, rnd ? rnd + 3 * (size_t)K : nullptr, c->sweep, phase,
-                                                    c->M + 3, c->M, c->cnt);
+                                                    Mdev + 3, Mdev, c->cnt);
       e = cudaGetLastError();
    }
    h->prof_end(PROF_MC);
@@ -751,13 +764,62 @@ int cmc_phase(vgpu_handle h, const R* tab, int colour, const int* given, int K, 
 }
 
 template <typename R>
-int cmc_recount_moment(vgpu_handle h, const R* tab) {
-   CMCState* c = cmc_of(h);
-   cudaMemsetAsync(c->M, 0, 3 * sizeof(double), h->stream);
+int cmc_recount_moment(vgpu_handle h, const R* tab, double* M, int only_mat) {
+   cudaMemsetAsync(M, 0, 3 * sizeof(double), h->stream);
    cmc_moment_kernel<R><<<std::max(1, std::min(1024, (h->sys.n + 255) / 256)), 256, 0, h->stream>>>(
-       make_args<R>(h), tab + 200, c->M);
+       make_args<R>(h), tab + 200, M, only_mat);
    h->kernel_launches++;
    return cuda_err(h, cudaGetLastError(), "cmc moment");
+}
+
+// hybrid step (montecarlo::cmc_mc_step, src/montecarlo/cmc_mc.cpp:291-490):
+// per colour, the unconstrained materials' atoms take single-spin Metropolis
+// moves (once per step) and each constrained material's atoms of the colour
+// are paired among themselves (twice over), with that material's frame and
+// running moment
+template <typename R>
+int cmc_hybrid_sweeps(vgpu_handle h, const R* tab, uint64_t n_sweeps) {
+   CMCState* c = cmc_of(h);
+   MCState* s = mc_of(h);
+   const int M = c->nmat, nc = s->ncolours;
+   for (uint64_t sw = 0; sw < n_sweeps; ++sw) {
+      for (int m = 0; m < M; ++m)
+         if (c->constrained[m])
+            if (int rc = cmc_recount_moment<R>(h, tab, c->Mm + 6 * m, m)) return rc;
+      uint32_t phase = 0;
+      for (int round = 0; round < 2; ++round)
+         for (int col = 0; col < nc; ++col) {
+            if (round == 0) {
+               const int u0 = c->list_off[col * (M + 1) + M], u1 = c->list_off[col * (M + 1) + M + 1];
+               if (u1 > u0) {
+                  MCArgs<R> p;
+                  memset(&p, 0, sizeof p);
+                  p.a = make_args<R>(h);
+                  p.sigma = tab; p.beta = tab + 100; p.mu_ratio = tab + 200;
+                  p.sweep = c->sweep;
+                  p.rejects = c->cnt + 3;
+                  p.atoms = c->lists + u0;
+                  p.count = u1 - u0;
+                  cudaError_t e = mc_dispatch<R>(p, h->sys.fmt, h->stream);
+                  if (e != cudaSuccess) return cuda_err(h, e, "cmc single-spin launch");
+                  h->kernel_launches++;
+                  c->single_moves += p.count;
+                  c->total += p.count;
+               }
+            }
+            for (int m = 0; m < M; ++m, ++phase) {
+               if (!c->constrained[m]) continue;
+               const int a0 = c->list_off[col * (M + 1) + m], a1 = c->list_off[col * (M + 1) + m + 1];
+               const int K = (a1 - a0) / 2;
+               if (K == 0) continue;
+               if (int rc = cmc_phase<R>(h, tab, c->lists + a0, a1 - a0, nullptr, K, nullptr, phase,
+                                         c->Pm.data() + 9 * m, c->Mm + 6 * m))
+                  return rc;
+            }
+         }
+      c->sweep++;
+   }
+   return VGPU_OK;
 }
 
 template <typename R>
@@ -766,14 +828,17 @@ int cmc_sweeps_typed(vgpu_handle h, uint64_t n_sweeps) {
    MCState* s = mc_of(h);
    const R* tab = mc_tables<R>(h);
    if (!tab) return VGPU_ERR_OOM;
+   if (c->hybrid) return cmc_hybrid_sweeps<R>(h, tab, n_sweeps);
    for (uint64_t sw = 0; sw < n_sweeps; ++sw) {
       // the total moment from the spins at every step, as the reference does
-      if (int rc = cmc_recount_moment<R>(h, tab)) return rc;
+      if (int rc = cmc_recount_moment<R>(h, tab, c->M, -1)) return rc;
       uint32_t phase = 0;
       for (int round = 0; round < 2; ++round)
          for (int col = 0; col < s->ncolours; ++col, ++phase) {
             const int K = (s->colour_off[col + 1] - s->colour_off[col]) / 2;
-            if (int rc = cmc_phase<R>(h, tab, col, nullptr, K, nullptr, phase)) return rc;
+            if (int rc = cmc_phase<R>(h, tab, s->atoms + s->colour_off[col], s->colour_off[col + 1] - s->colour_off[col],
+                                      nullptr, K, nullptr, phase, c->P, c->M))
+               return rc;
          }
       c->sweep++;
    }
@@ -782,20 +847,11 @@ int cmc_sweeps_typed(vgpu_handle h, uint64_t n_sweeps) {
 
 }  // namespace
 
-extern "C" int vgpu_cmc_setup(vgpu_handle h, double phi_deg, double theta_deg, int32_t init_spins) {
-   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
-   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
-   if (h->sys.n_owned < h->sys.n) return set_err(h, VGPU_ERR_STATE, "constrained Monte Carlo runs on whole systems");
-   cudaSetDevice(h->device);
-   if (!mc_of(h)) {
-      int32_t nc = 0;
-      if (int rc = vgpu_mc_setup(h, nullptr, &nc)) return rc;
-   }
-   cmc_destroy(h);
-   CMCState* c = new CMCState();
-   h->extras[5] = c;
-   // polar_rot_matrix (cmc.cpp:53-135): P = Ry(phi) Rz(theta) with the
-   // reference's element layout; pv = (0,0,1) P, the third row
+namespace {
+
+// polar_rot_matrix (cmc.cpp:53-135): P = Ry(phi) Rz(theta) with the
+// reference's element layout; the constraint vector pv = (0,0,1) P, the third row
+void cmc_frame(double phi_deg, double theta_deg, double* P, double* pv) {
    const double d2r = 3.14159265358979323846264338327 / 180.0;
    const double sy = std::sin(phi_deg * d2r), cy = std::cos(phi_deg * d2r);
    const double sz = std::sin(theta_deg * d2r), cz = std::cos(theta_deg * d2r);
@@ -805,9 +861,27 @@ extern "C" int vgpu_cmc_setup(vgpu_handle h, double phi_deg, double theta_deg, i
       for (int j = 0; j < 3; ++j) {
          double v = 0.0;
          for (int k = 0; k < 3; ++k) v += Ry[3 * i + k] * Rz[3 * k + j];
-         c->P[3 * i + j] = v;
+         P[3 * i + j] = v;
       }
-   for (int j = 0; j < 3; ++j) c->pv[j] = c->P[6 + j];
+   for (int j = 0; j < 3; ++j) pv[j] = P[6 + j];
+}
+
+void constraint_direction(double phi_deg, double theta_deg, double dir[3]) {
+   const double d2r = 3.14159265358979323846264338327 / 180.0;
+   dir[0] = std::sin(phi_deg * d2r) * std::cos(theta_deg * d2r);
+   dir[1] = std::sin(phi_deg * d2r) * std::sin(theta_deg * d2r);
+   dir[2] = std::cos(phi_deg * d2r);
+}
+
+// a fresh CMC state with the pair buffers; nullptr on error (set)
+CMCState* cmc_new(vgpu_handle h) {
+   if (!mc_of(h)) {
+      int32_t nc = 0;
+      if (vgpu_mc_setup(h, nullptr, &nc)) return nullptr;
+   }
+   cmc_destroy(h);
+   CMCState* c = new CMCState();
+   h->extras[5] = c;
    MCState* s = mc_of(h);
    int maxK = 1;
    for (int col = 0; col < s->ncolours; ++col) maxK = std::max(maxK, (s->colour_off[col + 1] - s->colour_off[col]) / 2);
@@ -818,22 +892,114 @@ extern "C" int vgpu_cmc_setup(vgpu_handle h, double phi_deg, double theta_deg, i
    if ((e = cudaMalloc(&c->pairs, sizeof(int) * 2 * maxK)) || (e = cudaMalloc(&c->prop, rs * 6 * maxK)) ||
        (e = cudaMalloc(&c->ef, sizeof(double) * maxK)) || (e = cudaMalloc(&c->jac, sizeof(double) * maxK)) ||
        (e = cudaMalloc(&c->mom, sizeof(double) * 12 * maxK)) || (e = cudaMalloc(&c->rnd, sizeof(double) * 4 * maxK)) ||
-       (e = cudaMalloc(&c->M, sizeof(double) * 6)) || (e = cudaMalloc(&c->cnt, sizeof(unsigned long long) * 3))) {
+       (e = cudaMalloc(&c->M, sizeof(double) * 6)) || (e = cudaMalloc(&c->cnt, sizeof(unsigned long long) * 4))) {
       cmc_destroy(h);
-      return cuda_err(h, e, "cmc buffers");
+      cuda_err(h, e, "cmc buffers");
+      return nullptr;
    }
-   cudaMemsetAsync(c->cnt, 0, sizeof(unsigned long long) * 3, h->stream);
+   cudaMemsetAsync(c->cnt, 0, sizeof(unsigned long long) * 4, h->stream);
+   return c;
+}
+
+}  // namespace
+
+extern "C" int vgpu_cmc_setup(vgpu_handle h, double phi_deg, double theta_deg, int32_t init_spins) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (h->sys.n_owned < h->sys.n) return set_err(h, VGPU_ERR_STATE, "constrained Monte Carlo runs on whole systems");
+   cudaSetDevice(h->device);
+   CMCState* c = cmc_new(h);
+   if (!c) return VGPU_ERR_CUDA;
+   cmc_frame(phi_deg, theta_deg, c->P, c->pv);
    cudaMemcpyAsync(c->M + 3, c->pv, sizeof(double) * 3, cudaMemcpyHostToDevice, h->stream);
    if (init_spins) {
       // CMCinit: every spin along the constraint direction
       const int n = h->sys.n;
       std::vector<double> v[3];
-      const double dir[3] = {std::sin(phi_deg * d2r) * std::cos(theta_deg * d2r),
-                             std::sin(phi_deg * d2r) * std::sin(theta_deg * d2r), std::cos(phi_deg * d2r)};
+      double dir[3];
+      constraint_direction(phi_deg, theta_deg, dir);
       for (int q = 0; q < 3; ++q) v[q].assign(n, dir[q]);
       if (int rc = vgpu_set_spins(h, v[0].data(), v[1].data(), v[2].data())) return rc;
    }
    return cuda_err(h, cudaStreamSynchronize(h->stream), "cmc setup");
+}
+
+extern "C" int vgpu_cmc_setup_materials(vgpu_handle h, const int32_t* constrained, const double* phi_deg,
+                                        const double* theta_deg, int32_t init_spins) {
+   if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
+   if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
+   if (!constrained || !phi_deg || !theta_deg) return set_err(h, VGPU_ERR_ARG, "null argument");
+   if (h->sys.n_owned < h->sys.n) return set_err(h, VGPU_ERR_STATE, "constrained Monte Carlo runs on whole systems");
+   cudaSetDevice(h->device);
+   CMCState* c = cmc_new(h);
+   if (!c) return VGPU_ERR_CUDA;
+   const int M = h->sys.M, n = h->sys.n;
+   c->hybrid = true;
+   c->nmat = M;
+   c->constrained.assign(constrained, constrained + M);
+   c->Pm.assign(9 * (size_t)M, 0.0);
+   std::vector<double> mm(6 * (size_t)M, 0.0);
+   for (int m = 0; m < M; ++m) {
+      double pv[3];
+      cmc_frame(phi_deg[m], theta_deg[m], c->Pm.data() + 9 * m, pv);
+      for (int q = 0; q < 3; ++q) mm[6 * m + 3 + q] = pv[q];
+   }
+   // atoms by (colour, material), the unconstrained materials' atoms last
+   MCState* s = mc_of(h);
+   const int nc = s->ncolours;
+   std::vector<std::vector<int>> buckets((size_t)nc * (M + 1));
+   for (int i = 0; i < n; ++i) {
+      const int m = h->sys.type_host[i];
+      buckets[(size_t)s->colour_host[i] * (M + 1) + (constrained[m] ? m : M)].push_back(i);
+   }
+   std::vector<int> flat;
+   c->list_off.assign(buckets.size() + 1, 0);
+   for (size_t b = 0; b < buckets.size(); ++b) {
+      flat.insert(flat.end(), buckets[b].begin(), buckets[b].end());
+      c->list_off[b + 1] = (int)flat.size();
+   }
+   cudaError_t e;
+   if ((e = cudaMalloc(&c->Mm, sizeof(double) * mm.size())) ||
+       (e = cudaMalloc(&c->lists, sizeof(int) * std::max<size_t>(flat.size(), 1))))
+      return cuda_err(h, e, "cmc lists");
+   cudaMemcpyAsync(c->Mm, mm.data(), sizeof(double) * mm.size(), cudaMemcpyHostToDevice, h->stream);
+   cudaMemcpyAsync(c->lists, flat.data(), sizeof(int) * flat.size(), cudaMemcpyHostToDevice, h->stream);
+   // the plain frame and moment report the first constrained material
+   for (int m = 0; m < M; ++m)
+      if (constrained[m]) {
+         std::copy(c->Pm.begin() + 9 * m, c->Pm.begin() + 9 * m + 9, c->P);
+         for (int q = 0; q < 3; ++q) c->pv[q] = mm[6 * m + 3 + q];
+         break;
+      }
+   if (init_spins) {
+      // CMCMCinit: the constrained materials' spins along their directions
+      std::vector<double> v[3];
+      for (int q = 0; q < 3; ++q) v[q].resize(n);
+      if (int rc = vgpu_get_spins(h, v[0].data(), v[1].data(), v[2].data())) return rc;
+      for (int i = 0; i < n; ++i) {
+         const int m = h->sys.type_host[i];
+         if (!constrained[m]) continue;
+         double dir[3];
+         constraint_direction(phi_deg[m], theta_deg[m], dir);
+         for (int q = 0; q < 3; ++q) v[q][i] = dir[q];
+      }
+      if (int rc = vgpu_set_spins(h, v[0].data(), v[1].data(), v[2].data())) return rc;
+   }
+   return cuda_err(h, cudaStreamSynchronize(h->stream), "cmc setup");
+}
+
+extern "C" int vgpu_cmc_material_moments(vgpu_handle h, double* moments) {
+   if (!h || !moments) return set_err(h, VGPU_ERR_ARG, "null argument");
+   CMCState* c = cmc_of(h);
+   if (!c || !c->hybrid) return set_err(h, VGPU_ERR_STATE, "vgpu_cmc_setup_materials not called");
+   cudaSetDevice(h->device);
+   std::vector<double> mm(6 * (size_t)c->nmat);
+   cudaError_t e = cudaMemcpyAsync(mm.data(), c->Mm, sizeof(double) * mm.size(), cudaMemcpyDeviceToHost, h->stream);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+   if (e != cudaSuccess) return cuda_err(h, e, "cmc moments");
+   for (int m = 0; m < c->nmat; ++m)
+      for (int q = 0; q < 3; ++q) moments[3 * m + q] = mm[6 * m + q];
+   return VGPU_OK;
 }
 
 extern "C" int vgpu_cmc_frame(vgpu_handle h, double* P9, double* pv3) {
@@ -871,12 +1037,12 @@ static int cmc_pairs_typed(vgpu_handle h, const int32_t* pairs, int32_t K, const
                           "cmc pairs");
    if (!rc) {
       if (M) rc = cuda_err(h, cudaMemcpyAsync(c->M, M, sizeof(double) * 3, cudaMemcpyHostToDevice, h->stream), "cmc M");
-      else rc = cmc_recount_moment<R>(h, tab);
+      else rc = cmc_recount_moment<R>(h, tab, c->M, -1);
    }
    if (rc) return rc;
    // the explicit pairs are read back from c->pairs by the proposal kernel
    // (it rewrites the same values)
-   rc = cmc_phase<R>(h, tab, 0, c->pairs, K, c->rnd, 0);
+   rc = cmc_phase<R>(h, tab, nullptr, 0, c->pairs, K, c->rnd, 0, c->P, c->M);
    if (rc) return rc;
    return cuda_err(h, cudaStreamSynchronize(h->stream), "cmc pairs");
 }
@@ -907,15 +1073,19 @@ extern "C" int vgpu_cmc_get(vgpu_handle h, double* moment, double* counters) {
    if (!c) return set_err(h, VGPU_ERR_STATE, "vgpu_cmc_setup not called");
    cudaSetDevice(h->device);
    double M[3];
-   unsigned long long cnt[3];
+   unsigned long long cnt[4];
    cudaError_t e = cudaMemcpyAsync(M, c->M, sizeof M, cudaMemcpyDeviceToHost, h->stream);
    if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, c->cnt, sizeof cnt, cudaMemcpyDeviceToHost, h->stream);
    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
    if (e != cudaSuccess) return cuda_err(h, e, "cmc counters");
    if (moment) std::copy(M, M + 3, moment);
    if (counters) {
+      // single-spin moves of unconstrained materials (hybrid) count as the
+      // reference's: accepted, or energy rejections
       counters[0] = c->total;
-      for (int q = 0; q < 3; ++q) counters[1 + q] = (double)cnt[q];
+      counters[1] = (double)cnt[0] + (c->single_moves - (double)cnt[3]);
+      counters[2] = (double)(cnt[1] + cnt[3]);
+      counters[3] = (double)cnt[2];
    }
    return VGPU_OK;
 }

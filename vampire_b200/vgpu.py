@@ -561,6 +561,24 @@ class Simulation:
         self._check(lib().vgpu_cmc_setup(self._h, C.c_double(phi_deg), C.c_double(theta_deg),
                                           C.c_int32(int(init_spins))))
 
+    def cmc_setup_materials(self, constrained, phi_deg, theta_deg, init_spins: bool = True) -> None:
+        """Hybrid constrained Monte Carlo: per material a constraint flag and
+        direction (degrees); constrained materials' spins along it with
+        init_spins (the reference's CMCMCinit)."""
+        M = self.system.materials.size
+        c = np.ascontiguousarray(constrained, dtype=np.int32).reshape(M)
+        ph = np.ascontiguousarray(phi_deg, dtype=np.float64).reshape(M)
+        th = np.ascontiguousarray(theta_deg, dtype=np.float64).reshape(M)
+        self._check(lib().vgpu_cmc_setup_materials(self._h, _ptr(c, _I32), _ptr(ph, _D), _ptr(th, _D),
+                                                   C.c_int32(int(init_spins))))
+
+    def cmc_material_moments(self) -> np.ndarray:
+        """Running moments [M, 3] (mu_B) of the constrained materials (hybrid)."""
+        M = self.system.materials.size
+        out = np.zeros(3 * M)
+        self._check(lib().vgpu_cmc_material_moments(self._h, _ptr(out, _D)))
+        return out.reshape(M, 3)
+
     def cmc_sweep(self, n_steps: int = 1) -> None:
         """n_steps constrained Monte Carlo steps (about N pair moves each)."""
         self._check(lib().vgpu_cmc_sweep(self._h, C.c_uint64(n_steps)))
