@@ -256,6 +256,12 @@ int vgpu_set_noise_replay(vgpu_handle h, const double* xi);
  * timed launch delay the stream by a few microseconds, so sampling keeps a
  * profiled run close to an unprofiled one. */
 #define VGPU_OPT_PROFILE_EVERY 9
+/* VGPU_OPT_STAGE_WARPS (staged passes over compact records, no window
+ * staging): 2 or 4 = per-warp pipelined passes with that many warps per
+ * persistent block, every warp walking its own one-slice tiles with two
+ * buffers and no block-wide barrier; 0 or -1 (default) = the tile passes.
+ * The results are the same bit for bit. */
+#define VGPU_OPT_STAGE_WARPS 10
 /* Bond-record layout the next FP32 pass reads: *layout = VGPU_RECORDS_WINDOW
  * (compact words with window staging), VGPU_RECORDS_COMPACT,
  * VGPU_RECORDS_WIDE (16-byte records) or VGPU_RECORDS_NONE (formats without

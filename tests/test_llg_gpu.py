@@ -135,6 +135,41 @@ def test_staged_records_match_plain(V, L, sl, nbuf):
         np.testing.assert_array_equal(st.spins(), plain.spins())
 
 
+@pytest.mark.parametrize("L", [5, 12])
+@pytest.mark.parametrize("warps", [2, 4])
+def test_warp_pipelined_passes_match_plain(V, L, warps):
+    """The per-warp pipelined passes (VGPU_OPT_STAGE_WARPS: every warp walks
+    its own one-slice tiles with two buffers, no block-wide barrier) give the
+    plain passes' FP32 results bit for bit, with the dipole field on."""
+    from vampire_b200 import system
+    s = system.config_fcc_tensor(L=L, seed=7, dipole=True)
+    with V.Simulation(s, noise_seed=11) as plain, V.Simulation(s, noise_seed=11) as st:
+        plain.set_option(V.OPT_STAGED_RECORDS, 0)
+        st.set_option(V.OPT_STAGE_WARPS, warps)
+        assert st.record_layout()[0] == V.RECORDS_COMPACT
+        for sim in (plain, st):
+            sim.dipole_setup(s.cells)
+        plain.llg_heun(25)
+        st.llg_heun(25)
+        np.testing.assert_array_equal(st.spins(), plain.spins())
+
+
+def test_warp_pipelined_ranges_match_plain(V):
+    from vampire_b200 import system
+    s = system.config_fcc_tensor(L=8, seed=7)
+    with V.Simulation(s, noise_seed=11) as plain, V.Simulation(s, noise_seed=11) as st:
+        plain.set_option(V.OPT_STAGED_RECORDS, 0)
+        st.set_option(V.OPT_STAGE_WARPS, 4)
+        cut = (s.n // 2) // 32 * 32
+        for _ in range(5):
+            plain.llg_heun(1)
+            for which in (V.PASS_PREDICTOR, V.PASS_CORRECTOR):
+                st.llg_pass_range(which, 0, cut)
+                st.llg_pass_range(which, cut, s.n)
+        assert st.step == plain.step == 5
+        np.testing.assert_array_equal(st.spins(), plain.spins())
+
+
 def test_staged_wait_timeout_reports_and_recovers(V):
     """Failure path of the bounded waits: with the test option every tile's
     barrier expects 16 bytes more than its bulk copy delivers, so the wait

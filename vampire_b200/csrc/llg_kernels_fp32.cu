@@ -34,8 +34,40 @@ static const void* staged_fn(int mode, int sl, int nbuf, bool crec) {
    return nullptr;
 }
 
+// shared memory of the per-warp pipelined passes
+static int warp_smem_bytes(const StageCfg& c) {
+   const int mp = c.M <= kStageMaxMat ? ((c.M * (int)sizeof(MatParams<float>) + 15) & ~15) : 0;
+   return c.dict_bytes + mp + c.warps * 2 * (c.buf_bytes + kStageOwnArrays * 128);
+}
+
+static int warp_mp_bytes(const StageCfg& c) {
+   return c.M <= kStageMaxMat ? ((c.M * (int)sizeof(MatParams<float>) + 15) & ~15) : 0;
+}
+
 cudaError_t prepare_llg_staged(StageCfg& c, int nslices, int device) {
    c.grid = 0;
+   if (c.warps > 0) {
+      if (!(c.warps == 2 || c.warps == 4) || !c.crec || c.win) return cudaErrorInvalidValue;
+      const int smem = warp_smem_bytes(c);
+      int sms = 0, optin = 0;
+      cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+      if (e != cudaSuccess) return e;
+      if (smem > optin - 128) return cudaErrorInvalidValue;
+      int per_sm = 1 << 30;
+      for (int mode = PASS_PREDICTOR; mode <= PASS_CORRECTOR; ++mode) {
+         const void* f = mode == PASS_PREDICTOR ? (const void*)llg_warp_kernel<PASS_PREDICTOR>
+                                                : (const void*)llg_warp_kernel<PASS_CORRECTOR>;
+         if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+         int nb = 0;
+         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, 32 * c.warps, smem)) != cudaSuccess) return e;
+         per_sm = std::min(per_sm, nb);
+      }
+      if (per_sm < 1) return cudaErrorInvalidValue;
+      c.ntiles = nslices;
+      c.grid = std::min((nslices + c.warps - 1) / c.warps, per_sm * sms);
+      return cudaSuccess;
+   }
    if (!(c.sl == 2 || c.sl == 4 || c.sl == 8) || !(c.nbuf == 1 || c.nbuf == 2)) return cudaErrorInvalidValue;
    if (c.win && (c.nbuf != 1 || !c.crec)) return cudaErrorInvalidValue;
    const int smem = c.win ? c.buf_bytes + 12 * c.wmax + c.dict_bytes
@@ -82,6 +114,15 @@ static cudaError_t launch_serialised(void (*kernel)(Args...), dim3 g, dim3 b, in
 cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, const StageCfg& c, cudaStream_t st) {
    if (c.grid == 0) return cudaSuccess;
    if ((a.crec != nullptr) != c.crec) return cudaErrorInvalidValue;  // record layout of the prepared shape
+   if (c.warps > 0) {  // per-warp pipelined passes: one slice per warp tile
+      const int nsl = (a.n_upd + 31) / 32 - a.slice_first;
+      if (nsl <= 0) return cudaSuccess;
+      const dim3 g(std::min(c.grid, (nsl + c.warps - 1) / c.warps)), b(32 * c.warps);
+      return launch_serialised(mode == PASS_PREDICTOR ? llg_warp_kernel<PASS_PREDICTOR>
+                                                      : llg_warp_kernel<PASS_CORRECTOR>,
+                               g, b, warp_smem_bytes(c), st, a, nslices, nsl, (int)c.buf_bytes,
+                               (int)c.dict_bytes, warp_mp_bytes(c));
+   }
    // tiles of the updated range: slices slice_first .. ceil(n_upd / 32) - 1
    const int ntiles = ((a.n_upd + 31) / 32 - a.slice_first + c.sl - 1) / c.sl;
    if (ntiles <= 0) return cudaSuccess;

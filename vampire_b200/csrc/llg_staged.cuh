@@ -225,6 +225,136 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
    }
 }
 
+// Per-warp pipelined passes (FP32 compact records): every warp of a
+// persistent block walks its own tiles of one slice (32 atoms) with two
+// buffers and two mbarriers of its own -- lane 0 starts the bulk copies of the
+// warp's next slice (bond words and own-atom arrays) while the warp computes
+// the current one -- so no block-wide barrier is taken after the start (the
+// dictionary and the material table are read into shared memory once per
+// block).  The arithmetic is the staged pass's, so results are identical.
+// Shared memory: dictionary (dict_bytes), material table (mp_bytes), then per
+// warp two buffers of buf_bytes words + kStageOwnArrays x 128 bytes.
+template <int MODE>
+__global__ void __launch_bounds__(128, 6) llg_warp_kernel(const LLGArgs<float> a, int nslices, int ntiles,
+                                                          int buf_bytes, int dict_bytes, int mp_bytes) {
+   extern __shared__ __align__(128) unsigned char stage_smem[];
+   __shared__ __align__(8) uint64_t wbar[2 * 4];
+   asm volatile("griddepcontrol.wait;" ::: "memory");
+   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+   const int wpb = blockDim.x >> 5;
+   float4* sdict = reinterpret_cast<float4*>(stage_smem);
+   MatParams<float>* smp = reinterpret_cast<MatParams<float>*>(stage_smem + dict_bytes);
+   const bool mp_shared = mp_bytes > 0;
+   const int stride = buf_bytes + kStageOwnArrays * 128;
+   unsigned char* wbuf = stage_smem + dict_bytes + mp_bytes + warp * 2 * stride;
+   uint64_t* mb = wbar + 2 * warp;
+   const int tstride = gridDim.x * wpb;
+   int t = blockIdx.x * wpb + warp;
+   // lane 0: expect the slice's bytes and start its copies into buffer b
+   auto issue = [&](int tt, int b) {
+      const int s0 = a.slice_first + tt;
+      const int o0 = __ldg(a.slice_off + s0), o1 = __ldg(a.slice_off + s0 + 1);
+      const uint32_t bytes = (uint32_t)(o1 - o0) * 4u;
+      const bool gin = MODE == PASS_CORRECTOR && a.gx;
+      const int na = 3 + (MODE == PASS_CORRECTOR ? 3 : 0) + (a.mat ? 1 : 0) + (a.cell ? 1 : 0) + (gin ? 3 : 0);
+      unsigned char* buf = wbuf + b * stride;
+      float* own = reinterpret_cast<float*>(buf + buf_bytes);
+      const size_t a0 = (size_t)s0 * 32;
+      fence_proxy_async();
+      mbar_arrive_expect_tx(&mb[b], bytes + 128u * (uint32_t)na + (uint32_t)a.stage_extra_tx);
+      if (bytes) bulk_copy_g2s(buf, a.crec + o0, bytes, &mb[b]);
+      bulk_copy_g2s(own, a.ax + a0, 128, &mb[b]);
+      bulk_copy_g2s(own + 32, a.ay + a0, 128, &mb[b]);
+      bulk_copy_g2s(own + 64, a.az + a0, 128, &mb[b]);
+      if (MODE == PASS_CORRECTOR) {
+         bulk_copy_g2s(own + 96, a.bx + a0, 128, &mb[b]);
+         bulk_copy_g2s(own + 128, a.by + a0, 128, &mb[b]);
+         bulk_copy_g2s(own + 160, a.bz + a0, 128, &mb[b]);
+      }
+      if (a.mat) bulk_copy_g2s(own + 192, a.mat + a0, 128, &mb[b]);
+      if (a.cell) bulk_copy_g2s(own + 224, a.cell + a0, 128, &mb[b]);
+      if (gin) {
+         bulk_copy_g2s(own + 256, a.gx + a0, 128, &mb[b]);
+         bulk_copy_g2s(own + 288, a.gy + a0, 128, &mb[b]);
+         bulk_copy_g2s(own + 320, a.gz + a0, 128, &mb[b]);
+      }
+   };
+   if (lane == 0) {
+      mbar_init(&mb[0], 1);
+      mbar_init(&mb[1], 1);
+      fence_mbar_init();
+      if (t < ntiles) issue(t, 0);
+   }
+   {  // dictionary and material table, once per block
+      const int nd = dict_bytes / 16;
+      for (int q = tid; q < nd; q += blockDim.x) sdict[q] = __ldg(a.cdict + q);
+      if (mp_shared) {
+         const int nw = a.M * (int)(sizeof(MatParams<float>) / 4);
+         const float* g = reinterpret_cast<const float*>(a.mp);
+         float* d = reinterpret_cast<float*>(smp);
+         for (int q = tid; q < nw; q += blockDim.x) d[q] = __ldg(g + q);
+      }
+   }
+   __syncthreads();  // barriers initialised, dictionary and table in place
+   const MatParams<float>* mpt = mp_shared ? smp : a.mp;
+   uint32_t phase = 0;
+   int k = 0, b = 0;
+   bool failed = false;
+   for (; t < ntiles; t += tstride, ++k) {
+      b = k & 1;
+      // buffer b ^ 1 was last read in the previous iteration, closed by __syncwarp
+      if (lane == 0 && t + tstride < ntiles) issue(t + tstride, b ^ 1);
+      const int i = (a.slice_first + t) * 32 + lane;
+      const bool act = i < a.n_upd;
+      float g[3] = {0.f, 0.f, 0.f};
+      if (a.thermal && (MODE == PASS_PREDICTOR || !a.gx)) {
+         thermal_xi(a, act ? i : 0, g[0], g[1], g[2]);
+         if (MODE == PASS_PREDICTOR && a.gx && act) { a.gx[i] = g[0]; a.gy[i] = g[1]; a.gz[i] = g[2]; }
+      }
+      const int tile_off = __ldg(a.slice_off + a.slice_first + t);
+      const bool done = mbar_wait_bounded(&mb[b], (phase >> b) & 1u);
+      if (__any_sync(0xffffffffu, !done)) {  // every lane takes the same branch
+         failed = true;
+         break;
+      }
+      phase ^= 1u << b;
+      const unsigned char* buf = wbuf + b * stride;
+      const float* own = reinterpret_cast<const float*>(buf + buf_bytes);
+      if (MODE == PASS_CORRECTOR && a.thermal && a.gx) {
+         g[0] = own[256 + lane]; g[1] = own[288 + lane]; g[2] = own[320 + lane];
+      }
+      if (act) {
+         const int mi = a.mat ? reinterpret_cast<const int*>(own)[192 + lane] : 0;
+         const MatParams<float> m = mpt[mi];
+         const float S0[3] = {own[lane], own[32 + lane], own[64 + lane]};
+         float E[3];
+         external_field_g<float>(a, i, m, g, a.cell ? reinterpret_cast<const int*>(own)[224 + lane] : -1, E);
+         const int4* sb = reinterpret_cast<const int4*>(buf);
+         float H[3];
+         if (MODE == PASS_PREDICTOR) {
+            spin_field<float, FMT_DMI_TAB, 0, true, false, REC_COMPACT>(a, i, mi, m, a.ax, a.ay, a.az, S0, H, sb,
+                                                                        tile_off, sdict);
+            H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
+            llg_predict_finish<float>(a, i, m, S0, H);
+         } else {
+            const float S1[3] = {own[96 + lane], own[128 + lane], own[160 + lane]};
+            spin_field<float, FMT_DMI_TAB, 0, true, false, REC_COMPACT>(a, i, mi, m, a.bx, a.by, a.bz, S1, H, sb,
+                                                                        tile_off, sdict);
+            H[0] += E[0]; H[1] += E[1]; H[2] += E[2];
+            llg_correct_finish<float>(a, i, m, S0, S1, H);
+         }
+      }
+      __syncwarp();  // buffer b fully read before lane 0 refills it
+   }
+   if (failed && lane == 0) {
+      atomicOr(a.status, 2);
+      // copies still in flight: the one waited for and the next slice's
+      mbar_wait_bounded(&mb[b], (phase >> b) & 1u);
+      if (t + tstride < ntiles) mbar_wait_bounded(&mb[b ^ 1], (phase >> (b ^ 1)) & 1u);
+   }
+   __syncwarp();
+}
+
 // Window-staged passes (FP32 compact records): besides the tile's bond words,
 // the neighbour spins the tile reads are bulk-copied into shared memory too,
 // as the tile's "window": the few contiguous atom ranges (segments) that hold

@@ -295,6 +295,7 @@ static int upload_typed(vgpu_ctx* h, const vgpu_system_desc* d) {
       S.stage_bytes[0] = stage_tile_bytes(off, 2);
       S.stage_bytes[1] = stage_tile_bytes(off, 4);
       S.stage_bytes[2] = stage_tile_bytes(off, 8);
+      S.stage_bytes[3] = stage_tile_bytes(off, 1);
       if constexpr (sizeof(R) == 4) {
          std::vector<uint32_t> crec;
          std::vector<float> dict;
@@ -489,6 +490,11 @@ static int stage_sl_of(const vgpu_ctx* h) { return h->stage_sl > 0 ? h->stage_sl
 static int stage_nbuf_of(const vgpu_ctx* h) {
    return h->stage_nbuf > 0 ? h->stage_nbuf : compact_in_use(h) ? 2 : 1;
 }
+// per-warp pipelined passes (compact records, no window): warps per block, or 0
+static int stage_warps_of(const vgpu_ctx* h) {
+   if (!compact_in_use(h) || h->window == 1) return 0;
+   return h->stage_warps > 0 ? h->stage_warps : 0;
+}
 // window staging is opt-in: measured slower than the L1/L2 gathers of the
 // compact passes (one-tile blocks wait for the whole window to land)
 static bool window_wanted(const vgpu_ctx* h) {
@@ -573,6 +579,8 @@ static int prepare_passes(vgpu_ctx* h, bool* staged_out, int integrator = INTEG_
       c.dict_bytes = c.crec ? stage_dict_bytes(h->sys) : 0;
       c.win = c.crec && h->sys.win_ok && c.buf_bytes + 12 * h->sys.wmax + c.dict_bytes <= kStageSmemLimit;
       c.wmax = c.win ? h->sys.wmax : 0;
+      c.warps = c.win ? 0 : stage_warps_of(h);
+      if (c.warps > 0) c.buf_bytes = h->sys.stage_bytes[3] / 4;  // one slice of compact words
       cudaError_t e = prepare_llg_staged(c, (h->sys.n_owned + 31) / 32, h->device);
       if (e != cudaSuccess) return cuda_err(h, e, "staged pass setup (tile records exceed shared memory?)");
       h->sys.stage = c;
@@ -1031,6 +1039,12 @@ extern "C" int vgpu_set_option(vgpu_handle h, int option, int value) {
       case VGPU_OPT_WINDOW_STAGING:
          if (value < -1 || value > 1) return set_err(h, VGPU_ERR_ARG, "window staging: -1, 0 or 1");
          h->window = value;
+         h->sys.stage.grid = 0;
+         return VGPU_OK;
+      case VGPU_OPT_STAGE_WARPS:
+         if (value != -1 && value != 0 && value != 2 && value != 4)
+            return set_err(h, VGPU_ERR_ARG, "stage warps: -1, 0, 2 or 4");
+         h->stage_warps = value;
          h->sys.stage.grid = 0;
          return VGPU_OK;
       case VGPU_OPT_PROFILE_EVERY:

@@ -65,7 +65,7 @@ struct SysDev {
    const int* sys_off = nullptr;  // batched systems: first atom of each system
    int m_per_sys = 1;
    uint64_t ramp_n = 0;      // batched field sweep length (steps)
-   int stage_bytes[3] = {0, 0, 0};  // largest tile's records, tiles of 2 / 4 / 8 slices
+   int stage_bytes[4] = {0, 0, 0, 0};  // largest tile's records, tiles of 2 / 4 / 8 / 1 slices
    StageCfg stage;                          // prepared bulk-staged launch (grid 0: not prepared)
    std::vector<int> type_host;
    std::vector<int64_t> row_host;  // CSR kept on the host (colouring, sharding)
@@ -124,6 +124,7 @@ struct vgpu_ctx {
    int dipole_fft = -1;      // VGPU_OPT_DIPOLE_FFT (-1 default: FFT far field on regular cell grids)
    int compact = -1;         // VGPU_OPT_COMPACT_RECORDS (-1 default: compact records when built)
    int window = -1;          // VGPU_OPT_WINDOW_STAGING (-1 default: off)
+   int stage_warps = -1;     // VGPU_OPT_STAGE_WARPS (-1 default; 0 off; 2 or 4 warps per block)
 
    void* alloc(size_t bytes);
    void release(void* p);    // free one allocation made by alloc (nullptr: nothing)

@@ -138,6 +138,7 @@ struct StageCfg {
    int M = 1;                 // materials (the staged passes may keep the table in shared memory)
    bool crec = false;
    int dict_bytes = 0;
+   int warps = 0;             // per-warp pipelined passes: warps per block (0: tile passes)
    bool win = false;          // window-staged passes (neighbour spins staged too)
    int wmax = 0;              // window slots of the largest tile (multiple of 4)
    int ntiles = 0, grid = 0;  // set by prepare_llg_staged

@@ -27,6 +27,7 @@ OPT_STAGE_WAIT_TEST = 6
 OPT_COMPACT_RECORDS = 7
 OPT_WINDOW_STAGING = 8
 OPT_PROFILE_EVERY = 9
+OPT_STAGE_WARPS = 10
 EXCHANGE_FORMATS = ("iso_tab", "iso_bond", "vec_tab", "vec_bond", "dmi_tab", "tensor_bond")
 RECORDS_NONE, RECORDS_WIDE, RECORDS_COMPACT, RECORDS_WINDOW = 0, 1, 2, 3
 PASS_PREDICTOR, PASS_CORRECTOR = 0, 1
