@@ -310,7 +310,7 @@ def bench_mc(device, L=50, eq=5000, av=10000, every=10):
             "spins": s.n, "colours": nc, "sweeps": sweeps, "value": s.n * sweeps / (ms * 1e-3),
             "unit": "spin-moves/s", "sweep_only_value": s.n * eq / (ms_eq * 1e-3), "protocol_s": ms * 1e-3,
             "acceptance": 1.0 - rej / moves, "Tc_K": tc, "m_T": [round(float(x), 5) for x in m_T],
-            "error_vs_reference": mc_reference_comparison(Ts, m_T, tc)}
+            "error_vs_reference": mc_reference_comparison(Ts, m_T, tc, (eq, av, every))}
 
 
 def bench_adjoint(device, L=32, steps=2000):
@@ -406,16 +406,17 @@ def error_vs_fp64_batched(device, steps=100, n_plain=16):
             "against": f"FP64 build at T=0 (batched: all 256; per-system launches: first {n_plain})"}
 
 
-def mc_reference_comparison(T, m_T, tc):
+def mc_reference_comparison(T, m_T, tc, sweeps):
     """The Monte Carlo m(T) against the reference's own sequential sweep of
     the same protocol (tests/golden/mc_sc50_curie.npz, made by the reference
-    program), when that fixture is present."""
+    program), when that fixture is present and the temperatures and sweep
+    counts (equilibration, averaging, sampling interval) are the fixture's."""
     import numpy as np
     p = REPO / "tests" / "golden" / "mc_sc50_curie.npz"
     if not p.exists():
         return None
     d = np.load(p)
-    if not np.array_equal(d["T"], T):
+    if not np.array_equal(d["T"], T) or tuple(int(x) for x in d["sweeps"]) != tuple(sweeps):
         return None
     ref = d["m_mean"]
     try:

@@ -478,8 +478,33 @@ def cmc_hybrid_sc12():
 MC50_EQ, MC50_AV = 5000, 10000
 
 
-def _mc50_one(T):
-    inp = sc_input(50, T=T, H=0.0, integrator="monte-carlo", extra="montecarlo:algorithm=angle\n")
+def autocorr_se(x: np.ndarray, c: float = 6.0):
+    """Standard error of the mean of a correlated series from its integrated
+    autocorrelation time, summed up to the first lag M >= c * tau (Sokal's
+    self-consistent window).  Returns (se, tau in samples)."""
+    x = np.asarray(x, dtype=np.float64) - np.mean(x)
+    n = x.size
+    var = float(x @ x) / n
+    if var == 0.0:
+        return 0.0, 0.0
+    f = np.fft.rfft(x, 2 * n)
+    rho = np.fft.irfft(f * np.conj(f))[:n] / (np.arange(n, 0, -1) * var)
+    tau = 0.5
+    for lag in range(1, n):
+        tau += rho[lag]
+        if lag >= c * tau:
+            break
+    return float(np.sqrt(2.0 * tau * var / n)), float(tau)
+
+
+MC50_SEEDS = (None, 424242, 777001, 9051)
+
+
+def _mc50_one(T, seed=None):
+    extra = "montecarlo:algorithm=angle\n"
+    if seed is not None:
+        extra += f"sim:integrator-random-seed={seed}\n"
+    inp = sc_input(50, T=T, H=0.0, integrator="monte-carlo", extra=extra)
     return O.run_harness(inp, {"m.mat": MC_MAT}, ["--system", "--steps", MC50_EQ + MC50_AV, "--mag-every", MC_EVERY,
                                                   "--mag-start", MC50_EQ], timeout=14400)
 
@@ -489,31 +514,49 @@ def mc_sc50_curie():
     random-site Metropolis (montecarlo::mc_step, angle moves) on SC 50^3
     periodic (125,000 spins), config-0 material, H=0, spins start along z, 31
     temperatures 0..1500 K, 5,000 equilibration + 10,000 averaging sweeps,
-    |m| sampled every 10 sweeps.  One reference process per temperature
-    (about 15 minutes each on one core).  The whole |m| series is kept so
-    that a test can choose its blocking; m_se is from 10 blocks of 1,000
-    sweeps."""
+    |m| sampled every 10 sweeps.  One reference process per temperature and
+    chain (about 15 minutes each on one core); chains differ only in the
+    reference's integrator seed (the first uses its default seed).
+    MC50_CHAINS (default 2) sets the number of chains; chains already in the
+    fixture with the same seed are kept, not re-run.  m_trace holds every
+    chain's |m| series (chains, temperatures, samples); m_mean is the mean
+    over chains and m_se its standard error, each chain's from its
+    integrated autocorrelation time."""
     from concurrent.futures import ThreadPoolExecutor
     import os
     workers = int(os.environ.get("MC50_WORKERS", os.cpu_count() or 4))
+    nch = int(os.environ.get("MC50_CHAINS", 2))
+    seeds = [(-1 if s is None else s) for s in MC50_SEEDS[:nch]]
+    path = HERE / "mc_sc50_curie.npz"
+    old = dict(np.load(path)) if path.exists() else {}
+    have = {}
+    if old:
+        tr_old = old["m_trace"].reshape(-1, len(MC_TEMPS), old["m_trace"].shape[-1])
+        acc_old = old["acceptance"].reshape(-1, len(MC_TEMPS))
+        for k, s in enumerate(old.get("seeds", np.array([-1]))):
+            have[int(s)] = (tr_old[k], acc_old[k])
+    todo = [(T, s) for s in seeds if s not in have for T in MC_TEMPS]
     with ThreadPoolExecutor(workers) as ex:
-        runs = list(ex.map(_mc50_one, MC_TEMPS))
-    mean, se, acc, traces = [], [], [], []
-    for d in runs:
-        tr = d["mag_trace"].reshape(-1, 4)[:, 3]
-        m, e = blocking_stats(tr)
-        mean.append(m)
-        se.append(e)
-        traces.append(tr)
-        mv, rj = d["mc_counters"]
-        acc.append(1.0 - rj / mv)
-    d0 = runs[0]
-    out = {k: d0[k] for k in ("meta", "materials", "sim", "m_spin")}
-    out.update(T=np.array(MC_TEMPS), m_mean=np.array(mean), m_se=np.array(se), acceptance=np.array(acc),
-               m_trace=np.array(traces, dtype=np.float32), L=np.array(50),
+        runs = list(ex.map(lambda a: _mc50_one(a[0], None if a[1] < 0 else a[1]), todo))
+    for s in seeds:
+        if s in have:
+            continue
+        mine = [d for (T, s2), d in zip(todo, runs) if s2 == s]
+        tr = np.array([d["mag_trace"].reshape(-1, 4)[:, 3] for d in mine], dtype=np.float32)
+        acc = np.array([1.0 - d["mc_counters"][1] / d["mc_counters"][0] for d in mine])
+        have[s] = (tr, acc)
+        if not old:
+            old = {k: mine[0][k] for k in ("meta", "materials", "sim", "m_spin")}
+    traces = np.stack([have[s][0] for s in seeds])          # (chains, T, samples)
+    acc = np.stack([have[s][1] for s in seeds])
+    means = traces.astype(np.float64).mean(2)
+    ses = np.array([[autocorr_se(x)[0] for x in ch] for ch in traces])
+    out = {k: old[k] for k in ("meta", "materials", "sim", "m_spin")}
+    out.update(T=np.array(MC_TEMPS), m_mean=means.mean(0), m_se=np.sqrt((ses ** 2).sum(0)) / len(seeds),
+               acceptance=acc, m_trace=traces, seeds=np.array(seeds), L=np.array(50),
                sweeps=np.array([MC50_EQ, MC50_AV, MC_EVERY]))
-    np.savez_compressed(HERE / "mc_sc50_curie.npz", **out)
-    print("mc_sc50_curie:", np.round(mean, 4))
+    np.savez_compressed(path, **out)
+    print("mc_sc50_curie:", np.round(out["m_mean"], 4))
 
 
 def sc8_config():

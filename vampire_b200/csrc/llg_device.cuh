@@ -9,16 +9,6 @@
 
 namespace vgpu {
 
-// FP32 fixed-width gathers of the tensor/DMI formats: 1 = one running sum per
-// field component in bond order; 2 = even and odd bonds in two sums, added at
-// the end (two independent dependency chains).  Every fixed-width record
-// layout (16-byte, compact, window) uses the same order, so they agree bit
-// for bit; the FP64 build always sums in bond order.
-#ifndef VGPU_GATHER_SPLIT
-#define VGPU_GATHER_SPLIT 1
-#endif
-constexpr int kGatherSplit = VGPU_GATHER_SPLIT;
-
 template <typename R> __device__ __forceinline__ R rsqrt_(R x);
 template <> __device__ __forceinline__ float rsqrt_<float>(float x) { return rsqrtf(x); }
 template <> __device__ __forceinline__ double rsqrt_<double>(double x) { return 1.0 / sqrt(x); }
@@ -69,16 +59,14 @@ template <typename R> __device__ __forceinline__ R ld_src(const R* p, int cohere
    return coherent ? __ldcg(p) : __ldg(p);
 }
 
+// The row is given by its first entry (base) and width (w); exchange_gather
+// below finds them from the slice offsets of atom i.
 // LOAD = 1: source spins were written earlier in the same launch by other
 // blocks (persistent batched kernel) and are read through L2 (ld.global.cg)
 template <typename R, int FMT, int LOAD = 0>
-__device__ __forceinline__ void exchange_gather(const LLGArgs<R>& a, int i, int mi, const R* __restrict__ sx,
-                                                const R* __restrict__ sy, const R* __restrict__ sz, R& hx,
-                                                R& hy, R& hz) {
-   const int sl = i >> 5, lane = i & 31;
-   const int off = __ldg(a.slice_off + sl);
-   const int w = (__ldg(a.slice_off + sl + 1) - off) >> 5;
-   const int base = off + lane;
+__device__ __forceinline__ void exchange_gather_row(const LLGArgs<R>& a, int base, int w, int mi,
+                                                    const R* __restrict__ sx, const R* __restrict__ sy,
+                                                    const R* __restrict__ sz, R& hx, R& hy, R& hz) {
    const R* __restrict__ tab = a.jtab;
 #pragma unroll 4
    for (int k = 0; k < w; ++k) {
@@ -118,6 +106,16 @@ __device__ __forceinline__ void exchange_gather(const LLGArgs<R>& a, int i, int 
    }
 }
 
+template <typename R, int FMT, int LOAD = 0>
+__device__ __forceinline__ void exchange_gather(const LLGArgs<R>& a, int i, int mi, const R* __restrict__ sx,
+                                                const R* __restrict__ sy, const R* __restrict__ sz, R& hx,
+                                                R& hy, R& hz) {
+   const int sl = i >> 5;
+   const int off = __ldg(a.slice_off + sl);
+   const int w = (__ldg(a.slice_off + sl + 1) - off) >> 5;
+   exchange_gather_row<R, FMT, LOAD>(a, off + (i & 31), w, mi, sx, sy, sz, hx, hy, hz);
+}
+
 // Row of compile-time width W read from packed 16-byte bond records
 // {neighbour | material bits, d_x, d_y, d_z} (FMT_DMI_TAB) or from the
 // neighbour index alone (FMT_ISO_TAB), fully unrolled so that all W record
@@ -144,28 +142,23 @@ __device__ __forceinline__ void exchange_gather_w(const LLGArgs<R>& a, int base,
          const int j = c[k] & a.idx_mask;
          x[k] = ld_src(sx + j, LOAD); y[k] = ld_src(sy + j, LOAD); z[k] = ld_src(sz + j, LOAD);
       }
-      R ox = 0, oy = 0, oz = 0;  // odd bonds' sums when kGatherSplit == 2
 #pragma unroll
       for (int k = 0; k < W; ++k) {
-         R& ax = (kGatherSplit == 2 && (k & 1)) ? ox : hx;
-         R& ay = (kGatherSplit == 2 && (k & 1)) ? oy : hy;
-         R& az = (kGatherSplit == 2 && (k & 1)) ? oz : hz;
          const int mj = a.mat_shift ? (c[k] >> a.mat_shift) : 0;
          const R dx = __int_as_float(sw[128 * k + 1]), dy = __int_as_float(sw[128 * k + 2]),
                  dz = __int_as_float(sw[128 * k + 3]);
          if (a.tab_scalar) {
             const R J = __ldg(a.jtab_s + mi * a.M + mj);
-            ax += J * x[k] + (dy * z[k] - dz * y[k]);
-            ay += J * y[k] + (dz * x[k] - dx * z[k]);
-            az += J * z[k] + (dx * y[k] - dy * x[k]);
+            hx += J * x[k] + (dy * z[k] - dz * y[k]);
+            hy += J * y[k] + (dz * x[k] - dx * z[k]);
+            hz += J * z[k] + (dx * y[k] - dy * x[k]);
          } else {
             const R* t = tab + 3 * (mi * a.M + mj);
-            ax += __ldg(t) * x[k] + (dy * z[k] - dz * y[k]);
-            ay += __ldg(t + 1) * y[k] + (dz * x[k] - dx * z[k]);
-            az += __ldg(t + 2) * z[k] + (dx * y[k] - dy * x[k]);
+            hx += __ldg(t) * x[k] + (dy * z[k] - dz * y[k]);
+            hy += __ldg(t + 1) * y[k] + (dz * x[k] - dx * z[k]);
+            hz += __ldg(t + 2) * z[k] + (dx * y[k] - dy * x[k]);
          }
       }
-      if (kGatherSplit == 2) { hx += ox; hy += oy; hz += oz; }
    } else if (FMT == FMT_DMI_TAB) {
       int4 rec[W];
 #pragma unroll
@@ -176,28 +169,23 @@ __device__ __forceinline__ void exchange_gather_w(const LLGArgs<R>& a, int base,
          const int j = rec[k].x & a.idx_mask;
          x[k] = ld_src(sx + j, LOAD); y[k] = ld_src(sy + j, LOAD); z[k] = ld_src(sz + j, LOAD);
       }
-      R ox = 0, oy = 0, oz = 0;  // odd bonds' sums when kGatherSplit == 2
 #pragma unroll
       for (int k = 0; k < W; ++k) {
-         R& ax = (kGatherSplit == 2 && (k & 1)) ? ox : hx;
-         R& ay = (kGatherSplit == 2 && (k & 1)) ? oy : hy;
-         R& az = (kGatherSplit == 2 && (k & 1)) ? oz : hz;
          const int mj = a.mat_shift ? (rec[k].x >> a.mat_shift) : 0;
          const R dx = __int_as_float(rec[k].y), dy = __int_as_float(rec[k].z), dz = __int_as_float(rec[k].w);
          if (a.tab_scalar) {
             // isotropic diagonal: one coupling per material pair (scalar table)
             const R J = __ldg(a.jtab_s + mi * a.M + mj);
-            ax += J * x[k] + (dy * z[k] - dz * y[k]);
-            ay += J * y[k] + (dz * x[k] - dx * z[k]);
-            az += J * z[k] + (dx * y[k] - dy * x[k]);
+            hx += J * x[k] + (dy * z[k] - dz * y[k]);
+            hy += J * y[k] + (dz * x[k] - dx * z[k]);
+            hz += J * z[k] + (dx * y[k] - dy * x[k]);
          } else {
             const R* t = tab + 3 * (mi * a.M + mj);
-            ax += __ldg(t) * x[k] + (dy * z[k] - dz * y[k]);
-            ay += __ldg(t + 1) * y[k] + (dz * x[k] - dx * z[k]);
-            az += __ldg(t + 2) * z[k] + (dx * y[k] - dy * x[k]);
+            hx += __ldg(t) * x[k] + (dy * z[k] - dz * y[k]);
+            hy += __ldg(t + 1) * y[k] + (dz * x[k] - dx * z[k]);
+            hz += __ldg(t + 2) * z[k] + (dx * y[k] - dy * x[k]);
          }
       }
-      if (kGatherSplit == 2) { hx += ox; hy += oy; hz += oz; }
    } else {  // FMT_ISO_TAB
       int c[W];
 #pragma unroll
@@ -237,28 +225,23 @@ __device__ __forceinline__ void exchange_gather_c(const LLGArgs<R>& a, int base,
       const int j = (int)(c[k] & jmask);
       x[k] = ld_src(sx + j, LOAD); y[k] = ld_src(sy + j, LOAD); z[k] = ld_src(sz + j, LOAD);
    }
-   R ox = 0, oy = 0, oz = 0;  // odd bonds' sums when kGatherSplit == 2
 #pragma unroll
    for (int k = 0; k < W; ++k) {
-      R& ax = (kGatherSplit == 2 && (k & 1)) ? ox : hx;
-      R& ay = (kGatherSplit == 2 && (k & 1)) ? oy : hy;
-      R& az = (kGatherSplit == 2 && (k & 1)) ? oz : hz;
       const uint32_t q = c[k] >> a.crec_shift;
       const float4 e = dict[q];
       const R dx = e.y, dy = e.z, dz = e.w;
       if (a.tab_scalar) {
          const R J = e.x;
-         ax += J * x[k] + (dy * z[k] - dz * y[k]);
-         ay += J * y[k] + (dz * x[k] - dx * z[k]);
-         az += J * z[k] + (dx * y[k] - dy * x[k]);
+         hx += J * x[k] + (dy * z[k] - dz * y[k]);
+         hy += J * y[k] + (dz * x[k] - dx * z[k]);
+         hz += J * z[k] + (dx * y[k] - dy * x[k]);
       } else {
          const float4 e2 = dict[a.cdict_n + q];
-         ax += (R)e.x * x[k] + (dy * z[k] - dz * y[k]);
-         ay += (R)e2.x * y[k] + (dz * x[k] - dx * z[k]);
-         az += (R)e2.y * z[k] + (dx * y[k] - dy * x[k]);
+         hx += (R)e.x * x[k] + (dy * z[k] - dz * y[k]);
+         hy += (R)e2.x * y[k] + (dz * x[k] - dx * z[k]);
+         hz += (R)e2.y * z[k] + (dx * y[k] - dy * x[k]);
       }
    }
-   if (kGatherSplit == 2) { hx += ox; hy += oy; hz += oz; }
 }
 
 // Row read from window-staged records: per bond the word slot | coupling
@@ -273,19 +256,19 @@ __device__ __forceinline__ void exchange_gather_win(const LLGArgs<R>& a, int w_r
                                                     int wmax) {
    const float* wy = wx + wmax;
    const float* wz = wy + wmax;
-   auto bond = [&](uint32_t c, R x, R y, R z, R& ax, R& ay, R& az) {
+   auto bond = [&](uint32_t c, R x, R y, R z) {
       const float4 e = dict[c >> 16];
       const R dx = e.y, dy = e.z, dz = e.w;
       if (a.tab_scalar) {
          const R J = e.x;
-         ax += J * x + (dy * z - dz * y);
-         ay += J * y + (dz * x - dx * z);
-         az += J * z + (dx * y - dy * x);
+         hx += J * x + (dy * z - dz * y);
+         hy += J * y + (dz * x - dx * z);
+         hz += J * z + (dx * y - dy * x);
       } else {
          const float4 e2 = dict[a.cdict_n + (c >> 16)];
-         ax += (R)e.x * x + (dy * z - dz * y);
-         ay += (R)e2.x * y + (dz * x - dx * z);
-         az += (R)e2.y * z + (dx * y - dy * x);
+         hx += (R)e.x * x + (dy * z - dz * y);
+         hy += (R)e2.x * y + (dz * x - dx * z);
+         hz += (R)e2.y * z + (dx * y - dy * x);
       }
    };
    if (W > 0) {
@@ -298,19 +281,13 @@ __device__ __forceinline__ void exchange_gather_win(const LLGArgs<R>& a, int w_r
          const int s = (int)(c[k] & 0xffffu);
          x[k] = wx[s]; y[k] = wy[s]; z[k] = wz[s];
       }
-      R ox = 0, oy = 0, oz = 0;  // odd bonds' sums when kGatherSplit == 2
 #pragma unroll
-      for (int k = 0; k < W; ++k) {
-         if (kGatherSplit == 2 && (k & 1)) bond(c[k], x[k], y[k], z[k], ox, oy, oz);
-         else bond(c[k], x[k], y[k], z[k], hx, hy, hz);
-      }
-      if (kGatherSplit == 2) { hx += ox; hy += oy; hz += oz; }
+      for (int k = 0; k < W; ++k) bond(c[k], x[k], y[k], z[k]);
    } else {
-      // run-time width: one sum in bond order, as the generic gather
       for (int k = 0; k < w_rt; ++k) {
          const uint32_t c = sw[32 * k];
          const int s = (int)(c & 0xffffu);
-         bond(c, wx[s], wy[s], wz[s], hx, hy, hz);
+         bond(c, wx[s], wy[s], wz[s]);
       }
    }
 }

@@ -14,9 +14,14 @@
 // site exactly once (the reference visits N random sites with replacement);
 // the two are compared statistically (m(T), Tc).
 //
-// Random numbers: Philox counter (atom, sweep_lo, sweep_hi, RNG_MC_MOVE) gives
-// the three Gaussians of the move, (.., RNG_MC_ACCEPT) the acceptance uniform;
-// or, in replay mode, 4 host-supplied numbers per site and sweep.
+// Random numbers: one Philox draw, counter (atom, sweep_lo, sweep_hi,
+// RNG_MC_MOVE), per FP32 trial: the top 24 bits of its four words give the
+// three Gaussians of the move (Box-Muller, as everywhere in FP32), the low
+// bytes of three of them the 24-bit acceptance uniform -- disjoint bits of
+// independent uniform words, so independent uniforms.  FP64 takes the
+// acceptance uniform from a second draw (.., RNG_MC_ACCEPT), all 32 bits of
+// each word being used there.  In replay mode, 4 host-supplied numbers per
+// site and sweep.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,6 +38,7 @@ struct MCState {
    std::vector<int> colour_host;      // [n]
    std::vector<int> colour_off;       // [ncolours+1] offsets into the atom list
    int* atoms = nullptr;              // [n] atoms sorted by colour
+   int4* entries = nullptr;           // [n] per list position: atom, first SELL entry, row width, material
    unsigned long long* rejects = nullptr;
    void* replay = nullptr;            // [4n] (x|y|z gaussians, uniform) in R
    bool use_replay = false;
@@ -44,21 +50,29 @@ struct MCState {
 
 static MCState* mc_of(vgpu_ctx* h) { return (MCState*)h->extras[1]; }
 
+// What one trial needs of its material, in one aligned record (two 16-byte
+// loads in FP32): move width, mu_B / (kB T_rescaled) (kBTBohr), mu_s_SI / mu_B,
+// and the uniaxial and cubic constants of the single-spin energy.
+template <typename R>
+struct alignas(8 * sizeof(R)) MCMat {
+   R sigma, beta, mu_ratio, ku2, kux, kuy, kuz, kc4;
+};
+
 template <typename R>
 struct MCArgs {
    LLGArgs<R> a;
-   const int* atoms;
+   const int4* entries;  // the colour's trials (list positions)
    int count;
-   const R* sigma;      // [M] move width
-   const R* beta;       // [M] mu_B / (kB T_rescaled)  (kBTBohr)
-   const R* mu_ratio;   // [M] mu_s_SI / mu_B
-   const R* replay;     // [4n] or nullptr
+   const MCMat<R>* mat;  // [M]
+   const R* replay;      // [4n] or nullptr
    uint64_t sweep;
    unsigned long long* rejects;
 };
 
-template <typename R>
-__device__ __forceinline__ R site_energy_delta(const LLGArgs<R>& a, int i, const MatParams<R>& m, const R S[3],
+// dE of atom i (material mi) for the move S -> T in the fixed exchange field
+// h; P: any record with ku2, kux, kuy, kuz, kc4 (MatParams or MCMat)
+template <typename R, typename P>
+__device__ __forceinline__ R site_energy_delta(const LLGArgs<R>& a, int i, int mi, const P& m, const R S[3],
                                                const R T[3], const R h[3]) {
    // dE = E(T) - E(S) for the single-spin energy (exchange field h fixed)
    R d = -((T[0] - S[0]) * (h[0] + a.hx) + (T[1] - S[1]) * (h[1] + a.hy) + (T[2] - S[2]) * (h[2] + a.hz));
@@ -72,26 +86,43 @@ __device__ __forceinline__ R site_energy_delta(const LLGArgs<R>& a, int i, const
       const R t4 = T[0] * T[0] * T[0] * T[0] + T[1] * T[1] * T[1] * T[1] + T[2] * T[2] * T[2] * T[2];
       d += (R)(-0.5) * m.kc4 * (t4 - s4);
    }
-   if (a.aniso_ext) d += anisotropy_energy<R, R, true>(a, i, m, T) - anisotropy_energy<R, R, true>(a, i, m, S);
+   if (a.aniso_ext) {
+      const MatParams<R>& q = a.mp[mi];
+      d += anisotropy_energy<R, R, true>(a, i, q, T) - anisotropy_energy<R, R, true>(a, i, q, S);
+   }
    if (a.bq_off) d += biquadratic_energy<R, R>(a, i, T) - biquadratic_energy<R, R>(a, i, S);
    return d;
 }
 
-// Capped at 40 registers (6 blocks of 256 per SM instead of 5): the kernel
-// is latency-bound on its gathers, and the extra warps outweigh the spilled
-// registers (2.24e10 -> 2.51e10 spin-moves/s on the Curie protocol of SC 50^3
-// x 31 temperatures; a cap at 32 spills more and gave 2.39e10).
+// The trial's list entry holds its atom, row and material, so the row's bond
+// words, the own spin and the material record are all requested one load
+// after the thread starts (the atom list, the slice offsets and the material
+// id were three dependent loads before), and rows of width 6 or 12 (simple
+// cubic, FCC) are read with every bond word and neighbour spin in flight at
+// once.  Same arithmetic in the same bond order as the generic row loop.
+// Blocks of 256, at least VGPU_MC_MIN_BLOCKS per SM: 4 (64 registers, no
+// spills) measured fastest on SC 50^3 x 31 temperatures -- 2.905e10
+// spin-moves/s against 2.853e10 with 5 (48 registers), 2.70e10 with 6 (40)
+// and 2.56e10 with 7 or 8 (spilling); the sweep rate after 500 warm-up sweeps.
+#ifndef VGPU_MC_MIN_BLOCKS
+#define VGPU_MC_MIN_BLOCKS 4
+#endif
 template <typename R, int FMT>
-__global__ void __launch_bounds__(256, 6) mc_colour_kernel(const MCArgs<R> p) {
+__global__ void __launch_bounds__(256, VGPU_MC_MIN_BLOCKS) mc_colour_kernel(const MCArgs<R> p) {
    const int t = blockIdx.x * blockDim.x + threadIdx.x;
    bool rejected = false;
    if (t < p.count) {
       const LLGArgs<R>& a = p.a;
-      const int i = __ldg(p.atoms + t);
-      const int mi = a.mat ? __ldg(a.mat + i) : 0;
-      const MatParams<R> m = a.mp[mi];
+      const int4 en = __ldg(p.entries + t);
+      const int i = en.x, base = en.y, w = en.z, mi = en.w;
+      const MCMat<R> mm = p.mat[mi];
       R h[3] = {0, 0, 0};
-      exchange_gather<R, FMT>(a, i, mi, a.ax, a.ay, a.az, h[0], h[1], h[2]);
+      if (FMT == FMT_ISO_TAB && w == 6)
+         exchange_gather_w<R, FMT, 6, 0, false>(a, base, mi, a.ax, a.ay, a.az, h[0], h[1], h[2], nullptr);
+      else if (FMT == FMT_ISO_TAB && w == 12)
+         exchange_gather_w<R, FMT, 12, 0, false>(a, base, mi, a.ax, a.ay, a.az, h[0], h[1], h[2], nullptr);
+      else
+         exchange_gather_row<R, FMT>(a, base, w, mi, a.ax, a.ay, a.az, h[0], h[1], h[2]);
       // magnetostatic energy uses the mu0 Hd field (energy.cpp:123-126)
       if (a.cell) {
          const int c = __ldg(a.cell + i);
@@ -110,8 +141,6 @@ __global__ void __launch_bounds__(256, 6) mc_colour_kernel(const MCArgs<R> p) {
          const uint32_t gi = (uint32_t)i + a.noise_base;
          const u32x4 c = {gi, (uint32_t)p.sweep, (uint32_t)(p.sweep >> 32), RNG_MC_MOVE};
          const u32x4 r = philox4x32_10(c, a.seed_lo, a.seed_hi);
-         const u32x4 c2 = {gi, (uint32_t)p.sweep, (uint32_t)(p.sweep >> 32), RNG_MC_ACCEPT};
-         const u32x4 r2 = philox4x32_10(c2, a.seed_lo, a.seed_hi);
          if (sizeof(R) == 4) {
             float s1, c1, s2, c2f;
             const float r1 = sqrtf(-2.0f * logf(u01f(r.x)));
@@ -119,8 +148,11 @@ __global__ void __launch_bounds__(256, 6) mc_colour_kernel(const MCArgs<R> p) {
             sincospif(2.0f * u01f(r.y), &s1, &c1);
             sincospif(2.0f * u01f(r.w), &s2, &c2f);
             g0 = r1 * c1; g1 = r1 * s1; g2 = rr * c2f;
-            u = (R)u01f(r2.x);
+            // u01f keeps the top 24 bits: the low bytes of r.y, r.z, r.w
+            u = (R)u01f(((r.y & 0xffu) << 8) | ((r.z & 0xffu) << 16) | (r.w << 24));
          } else {
+            const u32x4 c2 = {gi, (uint32_t)p.sweep, (uint32_t)(p.sweep >> 32), RNG_MC_ACCEPT};
+            const u32x4 r2 = philox4x32_10(c2, a.seed_lo, a.seed_hi);
             double s1, c1, s2, c2d;
             const double r1 = sqrt(-2.0 * log(u01d(r.x)));
             const double rr = sqrt(-2.0 * log(u01d(r.z)));
@@ -130,14 +162,14 @@ __global__ void __launch_bounds__(256, 6) mc_colour_kernel(const MCArgs<R> p) {
             u = (R)u01d(r2.x);
          }
       }
-      const R sg = __ldg(p.sigma + mi);
+      const R sg = mm.sigma;
       R T[3] = {S[0] + g0 * sg, S[1] + g1 * sg, S[2] + g2 * sg};
       const R r = rsqrt_<R>(T[0] * T[0] + T[1] * T[1] + T[2] * T[2]);
       T[0] *= r; T[1] *= r; T[2] *= r;
-      const R dE = site_energy_delta<R>(a, i, m, S, T, h) * __ldg(p.mu_ratio + mi);
+      const R dE = site_energy_delta<R>(a, i, mi, mm, S, T, h) * mm.mu_ratio;
       bool accept = dE < (R)0;
       if (!accept) {
-         const R x = -dE * __ldg(p.beta + mi);
+         const R x = -dE * mm.beta;
          accept = (sizeof(R) == 4 ? (R)expf((float)x) : (R)exp((double)x)) >= u;
       }
       if (accept) {
@@ -148,6 +180,16 @@ __global__ void __launch_bounds__(256, 6) mc_colour_kernel(const MCArgs<R> p) {
    }
    const unsigned ballot = __ballot_sync(0xffffffffu, rejected);
    if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(p.rejects, (unsigned long long)__popc(ballot));
+}
+
+// list entries of the colour-sorted atoms (rows from the slice offsets)
+__global__ void mc_entries_kernel(const int* __restrict__ atoms, int count, const int* __restrict__ slice_off,
+                                  const int* __restrict__ mat, int4* __restrict__ out) {
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= count) return;
+   const int i = atoms[t];
+   const int off = slice_off[i >> 5];
+   out[t] = make_int4(i, off + (i & 31), (slice_off[(i >> 5) + 1] - off) >> 5, mat ? mat[i] : 0);
 }
 
 template <typename R, int FMT>
@@ -176,6 +218,7 @@ void mc_destroy(vgpu_ctx* h) {
    if (!s) return;
    cmc_destroy(h);  // its pairing follows this colouring
    cudaFree(s->atoms);
+   cudaFree(s->entries);
    cudaFree(s->rejects);
    cudaFree(s->replay);
    delete s;
@@ -251,8 +294,14 @@ extern "C" int vgpu_mc_setup(vgpu_handle h, const int32_t* colour_in, int32_t* n
    for (int i = 0; i < nu; ++i) order[fill[colour[i]]++] = i;
    cudaError_t e;
    if ((e = cudaMalloc(&s->atoms, sizeof(int) * order.size())) != cudaSuccess) return cuda_err(h, e, "mc atoms");
+   if ((e = cudaMalloc(&s->entries, sizeof(int4) * order.size())) != cudaSuccess) return cuda_err(h, e, "mc entries");
    if ((e = cudaMalloc(&s->rejects, sizeof(unsigned long long))) != cudaSuccess) return cuda_err(h, e, "mc counter");
    cudaMemcpyAsync(s->atoms, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice, h->stream);
+   if (nu > 0) {
+      mc_entries_kernel<<<(nu + 255) / 256, 256, 0, h->stream>>>(s->atoms, nu, (const int*)S.slice_off,
+                                                                   (const int*)S.mat, s->entries);
+      if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(h, e, "mc entries");
+   }
    cudaMemsetAsync(s->rejects, 0, sizeof(unsigned long long), h->stream);
    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_err(h, e, "mc setup");
    if (n_colours_out) *n_colours_out = nc;
@@ -298,12 +347,24 @@ extern "C" int vgpu_mc_set_replay(vgpu_handle h, const double* r) {
 }
 
 // per-material move width, inverse temperature and moment ratio (mc.cpp:45-53)
-// into the handle's device table; returns it or nullptr (error set)
+// into the handle's device table -- sigma [M], beta [M], mu_ratio [M], then
+// (at the next 64-byte boundary) the MCMat records [M]; returns it or nullptr
+// (error set).  An unchanged table is not copied again.
+static size_t mc_mat_offset(int M) { return (3 * (size_t)M * sizeof(double) + 63) & ~(size_t)63; }
+
+template <typename R>
+static const MCMat<R>* mc_mat_records(vgpu_handle h, const R* tab) {
+   return reinterpret_cast<const MCMat<R>*>(reinterpret_cast<const char*>(tab) + mc_mat_offset(h->sys.M));
+}
+
 template <typename R>
 static R* mc_tables(vgpu_handle h) {
    SysDev& S = h->sys;
    const int M = S.M;
-   std::vector<R> sig(M), beta(M), ratio(M);
+   const size_t off = mc_mat_offset(M), bytes = off + (size_t)M * sizeof(MCMat<R>);
+   std::vector<unsigned char> host(bytes, 0);
+   R* sig = reinterpret_cast<R*>(host.data());
+   MCMat<R>* rec = reinterpret_cast<MCMat<R>*>(host.data() + off);
    for (int m = 0; m < M; ++m) {
       const vgpu_material& q = S.materials[m];
       const double T = h->params.local_temperature ? q.temperature : h->params.temperature;
@@ -311,21 +372,25 @@ static R* mc_tables(vgpu_handle h) {
       const double Tr = T < Tc ? Tc * std::pow(T / Tc, al) : T;
       const double kBTBohr = 9.27400915e-24 / (Tr * 1.3806503e-23);
       sig[m] = (R)(Tr < 1.0 ? 0.02 : std::pow(1.0 / kBTBohr, 0.2) * 0.08);
-      beta[m] = (R)kBTBohr;
-      ratio[m] = (R)(q.mu_s_SI * 1.07828231e23);
+      sig[M + m] = (R)kBTBohr;
+      sig[2 * M + m] = (R)(q.mu_s_SI * 1.07828231e23);
+      rec[m] = MCMat<R>{sig[m], sig[M + m], sig[2 * M + m], (R)q.ku2, (R)q.ku_vector[0], (R)q.ku_vector[1],
+                        (R)q.ku_vector[2], (R)q.kc4};
    }
    if (!S.mc_tab) {
-      S.mc_tab = h->alloc(3 * 100 * sizeof(double));
+      S.mc_tab = h->alloc(mc_mat_offset(M) + (size_t)M * sizeof(MCMat<double>));
       if (!S.mc_tab) {
          set_err(h, VGPU_ERR_OOM, "mc tables");
          return nullptr;
       }
+      S.mc_tab_host.clear();
    }
-   R* tab = (R*)S.mc_tab;
-   cudaMemcpyAsync(tab, sig.data(), M * sizeof(R), cudaMemcpyHostToDevice, h->stream);
-   cudaMemcpyAsync(tab + 100, beta.data(), M * sizeof(R), cudaMemcpyHostToDevice, h->stream);
-   cudaMemcpyAsync(tab + 200, ratio.data(), M * sizeof(R), cudaMemcpyHostToDevice, h->stream);
-   return tab;
+   if (S.mc_tab_host != host) {
+      if (cuda_err(h, cudaMemcpyAsync(S.mc_tab, host.data(), bytes, cudaMemcpyHostToDevice, h->stream), "mc tables"))
+         return nullptr;
+      S.mc_tab_host.swap(host);
+   }
+   return (R*)S.mc_tab;
 }
 
 // one colour of the current sweep; the last colour completes the sweep
@@ -336,13 +401,11 @@ static int mc_run_colour(vgpu_handle h, const R* tab, int c) {
    MCArgs<R> p;
    memset(&p, 0, sizeof p);
    p.a = make_args<R>(h);
-   p.sigma = tab;
-   p.beta = tab + 100;
-   p.mu_ratio = tab + 200;
+   p.mat = mc_mat_records<R>(h, tab);
    p.replay = s->use_replay ? (const R*)s->replay : nullptr;
    p.sweep = s->sweep;
    p.rejects = s->rejects;
-   p.atoms = s->atoms + s->colour_off[c];
+   p.entries = s->entries + s->colour_off[c];
    p.count = s->colour_off[c + 1] - s->colour_off[c];
    h->prof_begin(PROF_MC);
    cudaError_t e = mc_dispatch<R>(p, S.fmt, h->stream);
@@ -479,6 +542,7 @@ struct CMCState {
    std::vector<double> Pm;             // [9M] frames
    double* Mm = nullptr;               // [6M] per material: running moment (3), constraint vector (3)
    int* lists = nullptr;               // atoms by (colour, material), unconstrained last
+   int4* list_entries = nullptr;       // MC list entries of lists (single-spin moves)
    std::vector<int> list_off;          // [ncolours * (M + 1) + 1]
    double single_moves = 0.0;
 };
@@ -489,7 +553,7 @@ void cmc_destroy(vgpu_ctx* h) {
    CMCState* c = cmc_of(h);
    if (!c) return;
    cudaFree(c->pairs); cudaFree(c->prop); cudaFree(c->ef); cudaFree(c->jac); cudaFree(c->mom);
-   cudaFree(c->rnd); cudaFree(c->M); cudaFree(c->cnt); cudaFree(c->Mm); cudaFree(c->lists);
+   cudaFree(c->rnd); cudaFree(c->M); cudaFree(c->cnt); cudaFree(c->Mm); cudaFree(c->lists); cudaFree(c->list_entries);
    delete c;
    h->extras[5] = nullptr;
 }
@@ -520,7 +584,7 @@ __device__ __forceinline__ R cmc_delta(const LLGArgs<R>& a, int i, int mi, const
    } else if (a.hm_atom) {
       h[0] += __ldg(a.hm_atom + i); h[1] += __ldg(a.hm_atom + a.n + i); h[2] += __ldg(a.hm_atom + 2 * a.n + i);
    }
-   return site_energy_delta<R>(a, i, m, S, T, h) * ratio;
+   return site_energy_delta<R>(a, i, mi, m, S, T, h) * ratio;
 }
 
 template <typename R, int FMT>
@@ -731,7 +795,7 @@ int cmc_phase(vgpu_handle h, const R* tab, const int* list, int count, const int
    CMCArgs<R> p;
    memset(&p, 0, sizeof p);
    p.a = make_args<R>(h);
-   p.sigma = tab; p.beta = tab + 100; p.mu_ratio = tab + 200;
+   p.sigma = tab; p.beta = tab + h->sys.M; p.mu_ratio = tab + 2 * h->sys.M;
    p.sweep = c->sweep; p.phase = phase;
    for (int q = 0; q < 9; ++q) p.P[q] = P[q];
    p.pairs = c->pairs; p.prop = (R*)c->prop; p.ef = c->ef; p.jac = c->jac; p.mom = c->mom; p.maxK = c->maxK;
@@ -767,7 +831,7 @@ template <typename R>
 int cmc_recount_moment(vgpu_handle h, const R* tab, double* M, int only_mat) {
    cudaMemsetAsync(M, 0, 3 * sizeof(double), h->stream);
    cmc_moment_kernel<R><<<std::max(1, std::min(1024, (h->sys.n + 255) / 256)), 256, 0, h->stream>>>(
-       make_args<R>(h), tab + 200, M, only_mat);
+       make_args<R>(h), tab + 2 * h->sys.M, M, only_mat);
    h->kernel_launches++;
    return cuda_err(h, cudaGetLastError(), "cmc moment");
 }
@@ -795,10 +859,10 @@ int cmc_hybrid_sweeps(vgpu_handle h, const R* tab, uint64_t n_sweeps) {
                   MCArgs<R> p;
                   memset(&p, 0, sizeof p);
                   p.a = make_args<R>(h);
-                  p.sigma = tab; p.beta = tab + 100; p.mu_ratio = tab + 200;
+                  p.mat = mc_mat_records<R>(h, tab);
                   p.sweep = c->sweep;
                   p.rejects = c->cnt + 3;
-                  p.atoms = c->lists + u0;
+                  p.entries = c->list_entries + u0;
                   p.count = u1 - u0;
                   cudaError_t e = mc_dispatch<R>(p, h->sys.fmt, h->stream);
                   if (e != cudaSuccess) return cuda_err(h, e, "cmc single-spin launch");
@@ -960,10 +1024,16 @@ extern "C" int vgpu_cmc_setup_materials(vgpu_handle h, const int32_t* constraine
    }
    cudaError_t e;
    if ((e = cudaMalloc(&c->Mm, sizeof(double) * mm.size())) ||
-       (e = cudaMalloc(&c->lists, sizeof(int) * std::max<size_t>(flat.size(), 1))))
+       (e = cudaMalloc(&c->lists, sizeof(int) * std::max<size_t>(flat.size(), 1))) ||
+       (e = cudaMalloc(&c->list_entries, sizeof(int4) * std::max<size_t>(flat.size(), 1))))
       return cuda_err(h, e, "cmc lists");
    cudaMemcpyAsync(c->Mm, mm.data(), sizeof(double) * mm.size(), cudaMemcpyHostToDevice, h->stream);
    cudaMemcpyAsync(c->lists, flat.data(), sizeof(int) * flat.size(), cudaMemcpyHostToDevice, h->stream);
+   if (!flat.empty()) {
+      mc_entries_kernel<<<(int)((flat.size() + 255) / 256), 256, 0, h->stream>>>(
+          c->lists, (int)flat.size(), (const int*)h->sys.slice_off, (const int*)h->sys.mat, c->list_entries);
+      if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(h, e, "cmc list entries");
+   }
    // the plain frame and moment report the first constrained material
    for (int m = 0; m < M; ++m)
       if (constrained[m]) {

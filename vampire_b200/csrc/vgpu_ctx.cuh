@@ -62,6 +62,7 @@ struct SysDev {
    void* hd_atom = nullptr;
    void* hm_atom = nullptr;  // per-atom mu0 Hd field for the magnetostatic energy
    void* mc_tab = nullptr;   // Monte Carlo per-material tables
+   std::vector<unsigned char> mc_tab_host;  // last contents copied to mc_tab
    const int* sys_off = nullptr;  // batched systems: first atom of each system
    int m_per_sys = 1;
    uint64_t ramp_n = 0;      // batched field sweep length (steps)
