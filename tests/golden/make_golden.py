@@ -520,8 +520,13 @@ def mc_sc50_curie():
     MC50_CHAINS (default 2) sets the number of chains; chains already in the
     fixture with the same seed are kept, not re-run.  m_trace holds every
     chain's |m| series (chains, temperatures, samples); m_mean is the mean
-    over chains and m_se its standard error, each chain's from its
-    integrated autocorrelation time."""
+    over chains.  A chain's standard error comes from its integrated
+    autocorrelation time; with several chains these errors are checked
+    against the spread of the chain means: kappa^2 = the mean over the
+    finite temperatures of sum_c (m_c - m)^2 / se_c^2 / (chains - 1), and when
+    kappa > 1 (the within-chain estimates too small: 10,000 sweeps hold only
+    a few autocorrelation times near the transition) every error is scaled
+    by kappa.  m_se is the standard error of m_mean."""
     from concurrent.futures import ThreadPoolExecutor
     import os
     workers = int(os.environ.get("MC50_WORKERS", os.cpu_count() or 4))
@@ -551,12 +556,18 @@ def mc_sc50_curie():
     acc = np.stack([have[s][1] for s in seeds])
     means = traces.astype(np.float64).mean(2)
     ses = np.array([[autocorr_se(x)[0] for x in ch] for ch in traces])
+    kappa = 1.0
+    if len(seeds) > 1:
+        live = np.all(ses > 0, axis=0)
+        dev = (means[:, live] - means[:, live].mean(0)) ** 2 / ses[:, live] ** 2
+        kappa = float(np.sqrt(dev.sum(0).mean() / (len(seeds) - 1)))
+    scale = max(1.0, kappa)
     out = {k: old[k] for k in ("meta", "materials", "sim", "m_spin")}
-    out.update(T=np.array(MC_TEMPS), m_mean=means.mean(0), m_se=np.sqrt((ses ** 2).sum(0)) / len(seeds),
-               acceptance=acc, m_trace=traces, seeds=np.array(seeds), L=np.array(50),
-               sweeps=np.array([MC50_EQ, MC50_AV, MC_EVERY]))
+    out.update(T=np.array(MC_TEMPS), m_mean=means.mean(0), m_se=scale * np.sqrt((ses ** 2).sum(0)) / len(seeds),
+               chain_se=ses, kappa=np.array(kappa), acceptance=acc, m_trace=traces, seeds=np.array(seeds),
+               L=np.array(50), sweeps=np.array([MC50_EQ, MC50_AV, MC_EVERY]))
     np.savez_compressed(path, **out)
-    print("mc_sc50_curie:", np.round(out["m_mean"], 4))
+    print("mc_sc50_curie:", np.round(out["m_mean"], 4), "kappa", round(kappa, 3))
 
 
 def sc8_config():

@@ -34,6 +34,27 @@ static const void* staged_fn(int mode, int sl, int nbuf, bool crec) {
    return nullptr;
 }
 
+// The default shape (2-slice tiles, two buffers, compact records) is also
+// compiled for every FEAT_FIXED feature set; the launcher takes the one that
+// stage_features names (the generic pass when it names none).
+using StagedFn = void (*)(LLGArgs<float>, int, int, int);
+
+template <int MODE>
+static StagedFn staged_fixed_fn(int feat) {
+   switch (feat) {
+#define VGPU_F(k) \
+   case FEAT_FIXED | ((k) << 1): return llg_staged_kernel<MODE, 2, 2, true, FEAT_FIXED | ((k) << 1)>;
+      VGPU_F(0) VGPU_F(1) VGPU_F(2) VGPU_F(3) VGPU_F(4) VGPU_F(5) VGPU_F(6) VGPU_F(7)
+      VGPU_F(8) VGPU_F(9) VGPU_F(10) VGPU_F(11) VGPU_F(12) VGPU_F(13) VGPU_F(14) VGPU_F(15)
+#undef VGPU_F
+      default: return llg_staged_kernel<MODE, 2, 2, true, 0>;
+   }
+}
+
+static StagedFn staged_fixed_fn(int mode, int feat) {
+   return mode == PASS_PREDICTOR ? staged_fixed_fn<PASS_PREDICTOR>(feat) : staged_fixed_fn<PASS_CORRECTOR>(feat);
+}
+
 // shared memory of the per-warp pipelined passes
 static int warp_smem_bytes(const StageCfg& c) {
    const int mp = c.M <= kStageMaxMat ? ((c.M * (int)sizeof(MatParams<float>) + 15) & ~15) : 0;
@@ -78,13 +99,18 @@ cudaError_t prepare_llg_staged(StageCfg& c, int nslices, int device) {
    if (e != cudaSuccess) return e;
    if (smem > optin - 64) return cudaErrorInvalidValue;  // room for the static mbarriers
    int per_sm = 1 << 30;
-   for (int mode = PASS_PREDICTOR; mode <= PASS_CORRECTOR; ++mode) {
-      const void* f = c.win ? window_fn(mode, c.sl) : staged_fn(mode, c.sl, c.nbuf, c.crec);
-      if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-      int nb = 0;
-      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, 32 * c.sl, smem)) != cudaSuccess) return e;
-      per_sm = std::min(per_sm, nb);
-   }
+   const bool fixed = !c.win && c.sl == 2 && c.nbuf == 2 && c.crec;
+   for (int mode = PASS_PREDICTOR; mode <= PASS_CORRECTOR; ++mode)
+      for (int k = -1; k < (fixed ? 16 : 0); ++k) {
+         const void* f = k >= 0 ? (const void*)staged_fixed_fn(mode, FEAT_FIXED | (k << 1))
+                         : c.win ? window_fn(mode, c.sl)
+                                 : staged_fn(mode, c.sl, c.nbuf, c.crec);
+         if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
+            return e;
+         int nb = 0;
+         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, 32 * c.sl, smem)) != cudaSuccess) return e;
+         per_sm = std::min(per_sm, nb);
+      }
    if (per_sm < 1) return cudaErrorInvalidValue;
    c.ntiles = (nslices + c.sl - 1) / c.sl;
    c.grid = c.nbuf == 1 ? c.ntiles : std::min(c.ntiles, per_sm * sms);
@@ -144,6 +170,9 @@ cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, co
       return cudaErrorInvalidValue;
    }
    const int smem = staged_smem_bytes(c.sl, c.nbuf, c.buf_bytes, c.dict_bytes, c.M);
+   if (c.sl == 2 && c.nbuf == 2 && c.crec)
+      return launch_serialised(staged_fixed_fn(mode, stage_features(a)), g, b, smem, st, a, nslices, ntiles,
+                               (int)c.buf_bytes);
 #define VGPU_STAGED_C(S, B, C)                                                                                 \
    e = launch_serialised(mode == PASS_PREDICTOR ? llg_staged_kernel<PASS_PREDICTOR, S, B, C>                   \
                                                 : llg_staged_kernel<PASS_CORRECTOR, S, B, C>,                  \
