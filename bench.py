@@ -465,7 +465,8 @@ def reference_arm(args, rank, world):
            "stands_for": "the FCC 100^3 workload (4,000,000 spins, dipole on) of the GPU arm: spin-steps/s is an "
                          "intensive rate, so a bounded sample of the same physics is timed per process",
            "parallelism": f"{r['cores']} independent reference processes (the reference is single-threaded)"}
-    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 0, "steps": steps,
+    # n_gpus: the N this arm was launched for (it runs on the host cores alone)
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": steps,
             "warmup": warmup, "ms_per_step": r.get("ms_per_step"), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg, "impl": "reference",
             "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
