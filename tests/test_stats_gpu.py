@@ -98,3 +98,35 @@ def test_magnetization_only_path(vgpu_lib, name, step, prec):
             if f"mag_{k}_{step}" in d:
                 tol = 2e-6 if prec == "fp32" else 1e-12
                 assert np.abs(m - d[f"mag_{k}_{step}"]).max() < tol
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_copy_rows_pinned_and_pageable(vgpu_lib, prec):
+    """vgpu_stats_copy_rows gives the same rows into pinned host memory (a
+    kernel writes them through the device mapping) and into pageable memory
+    (a copy), equal to the finalised rows vgpu_stats_get_magnetization reads,
+    and ordered on the handle's stream: rows of consecutive steps, read after
+    an event recorded behind each copy, follow the step's own update."""
+    import torch
+    from vampire_b200 import vgpu
+    s, d = load_golden("fcc4_dmi_t300")
+    s.params.temperature = 300.0
+    with vgpu.Simulation(s, precision=prec, noise_seed=5) as sim:
+        mid = sim.add_mask(*s.masks["material"])
+        nb = s.masks["material"][1]
+        pinned = [torch.zeros(9 * nb, dtype=torch.float64).pin_memory() for _ in range(2)]
+        stream = torch.cuda.ExternalStream(sim.stream_ptr())
+        for t in range(4):
+            sim.llg_heun(1)
+            sim.stats_update(magnetization=True)
+            sim.stats_copy_rows(mid, pinned[t % 2].data_ptr())
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            ev.synchronize()
+            m, _, _ = sim.magnetization(mid)
+            got = pinned[t % 2].numpy().reshape(nb, 9)[:, :4]
+            assert np.array_equal(got, m.reshape(nb, 4))
+        pageable = np.zeros(9 * nb)
+        sim.stats_copy_rows(mid, pageable.ctypes.data)
+        sim.synchronize()
+        assert np.array_equal(pageable, pinned[3 % 2].numpy())

@@ -117,26 +117,6 @@ cudaError_t prepare_llg_staged(StageCfg& c, int nslices, int device) {
    return cudaSuccess;
 }
 
-// A staged pass launched with programmatic stream serialisation: its blocks
-// may be scheduled while the previous kernel of the stream drains; every
-// block waits for that kernel's completion (griddepcontrol.wait in
-// llg_staged_kernel) before its first global access.
-template <typename... Args>
-static cudaError_t launch_serialised(void (*kernel)(Args...), dim3 g, dim3 b, int smem, cudaStream_t st,
-                                     Args... args) {
-   cudaLaunchConfig_t cfg = {};
-   cfg.gridDim = g;
-   cfg.blockDim = b;
-   cfg.dynamicSmemBytes = (size_t)smem;
-   cfg.stream = st;
-   cudaLaunchAttribute attr[1];
-   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-   attr[0].val.programmaticStreamSerializationAllowed = 1;
-   cfg.attrs = attr;
-   cfg.numAttrs = 1;
-   return cudaLaunchKernelEx(&cfg, kernel, args...);
-}
-
 cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, const StageCfg& c, cudaStream_t st) {
    if (c.grid == 0) return cudaSuccess;
    if ((a.crec != nullptr) != c.crec) return cudaErrorInvalidValue;  // record layout of the prepared shape
@@ -144,7 +124,7 @@ cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, co
       const int nsl = (a.n_upd + 31) / 32 - a.slice_first;
       if (nsl <= 0) return cudaSuccess;
       const dim3 g(std::min(c.grid, (nsl + c.warps - 1) / c.warps)), b(32 * c.warps);
-      return launch_serialised(mode == PASS_PREDICTOR ? llg_warp_kernel<PASS_PREDICTOR>
+      return launch_pdl(mode == PASS_PREDICTOR ? llg_warp_kernel<PASS_PREDICTOR>
                                                       : llg_warp_kernel<PASS_CORRECTOR>,
                                g, b, warp_smem_bytes(c), st, a, nslices, nsl, (int)c.buf_bytes,
                                (int)c.dict_bytes, warp_mp_bytes(c));
@@ -171,10 +151,10 @@ cudaError_t launch_llg_staged(const LLGArgs<float>& a, int mode, int nslices, co
    }
    const int smem = staged_smem_bytes(c.sl, c.nbuf, c.buf_bytes, c.dict_bytes, c.M);
    if (c.sl == 2 && c.nbuf == 2 && c.crec)
-      return launch_serialised(staged_fixed_fn(mode, stage_features(a)), g, b, smem, st, a, nslices, ntiles,
+      return launch_pdl(staged_fixed_fn(mode, stage_features(a)), g, b, smem, st, a, nslices, ntiles,
                                (int)c.buf_bytes);
 #define VGPU_STAGED_C(S, B, C)                                                                                 \
-   e = launch_serialised(mode == PASS_PREDICTOR ? llg_staged_kernel<PASS_PREDICTOR, S, B, C>                   \
+   e = launch_pdl(mode == PASS_PREDICTOR ? llg_staged_kernel<PASS_PREDICTOR, S, B, C>                   \
                                                 : llg_staged_kernel<PASS_CORRECTOR, S, B, C>,                  \
                          g, b, smem, st, a, nslices, ntiles, (int)c.buf_bytes);
 #define VGPU_STAGED(S, B)                                                                                      \

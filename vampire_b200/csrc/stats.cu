@@ -182,6 +182,9 @@ __global__ void __launch_bounds__(256) stats_mag_small_kernel(const LLGArgs<R> a
                                                               const StatsOut so) {
    __shared__ double acc[NB * ST_NQ];
    __shared__ double smu[kStatsMuShared];
+   // launched with programmatic stream serialisation (launch_pdl): the
+   // previous kernel of the stream (the corrector) has completed after this
+   asm volatile("griddepcontrol.wait;" ::: "memory");
    const bool mu_shared = a.M <= kStatsMuShared;
    for (int k = threadIdx.x; k < NB * ST_NQ; k += blockDim.x) acc[k] = 0.0;
    if (mu_shared)
@@ -365,10 +368,12 @@ static cudaError_t launch_stats(const LLGArgs<R>& a, StatsMask& m, int nblocks, 
       // the per-step magnetisation of small masks: one launch, merged and
       // finalised by its last block
       const StatsOut so{m.ticket, m.cur, m.mean, m.raw, m.derived, (double)(m.counter_mag + 1)};
-      if (m.size == 1) stats_mag_small_kernel<R, 1><<<nblocks, 256, 0, st>>>(a, m.mask, m.size, m.partial, so);
-      else if (m.size == 2) stats_mag_small_kernel<R, 2><<<nblocks, 256, 0, st>>>(a, m.mask, m.size, m.partial, so);
-      else stats_mag_small_kernel<R, 4><<<nblocks, 256, 0, st>>>(a, m.mask, m.size, m.partial, so);
-      return cudaGetLastError();
+      const dim3 g(nblocks), b(256);
+      const int* mk = m.mask;
+      double* pt = m.partial;
+      if (m.size == 1) return launch_pdl(stats_mag_small_kernel<R, 1>, g, b, 0, st, a, mk, m.size, pt, so);
+      if (m.size == 2) return launch_pdl(stats_mag_small_kernel<R, 2>, g, b, 0, st, a, mk, m.size, pt, so);
+      return launch_pdl(stats_mag_small_kernel<R, 4>, g, b, 0, st, a, mk, m.size, pt, so);
    }
    stats_partial_kernel<R, FMT><<<nblocks, 256, smem, st>>>(a, m.mask, m.size, do_energy, hm, m.partial);
    cudaError_t e = cudaGetLastError();
@@ -389,6 +394,12 @@ static cudaError_t stats_dispatch(const LLGArgs<R>& a, int fmt, StatsMask& m, in
       case FMT_DMI_TAB: return launch_stats<R, FMT_DMI_TAB>(a, m, nblocks, do_mag, do_en, hm, st);
       default: return launch_stats<R, FMT_TENSOR_BOND>(a, m, nblocks, do_mag, do_en, hm, st);
    }
+}
+
+// the rows of one mask into device-addressable host memory (vgpu_stats_copy_rows)
+__global__ void stats_rows_copy_kernel(const double* __restrict__ src, double* __restrict__ dst, int n) {
+   asm volatile("griddepcontrol.wait;" ::: "memory");
+   for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = src[k];
 }
 
 void stats_destroy(vgpu_ctx* h) {
@@ -513,7 +524,21 @@ extern "C" int vgpu_stats_copy_rows(vgpu_handle h, int32_t id, double* out) {
    if (!s || id < 0 || id >= (int)s->masks.size()) return set_err(h, VGPU_ERR_ARG, "unknown statistics mask %d", id);
    StatsMask& m = s->masks[id];
    cudaSetDevice(h->device);
-   return cuda_err(h, cudaMemcpyAsync(out, m.cur, sizeof(double) * m.size * ST_W, cudaMemcpyDefault, h->stream),
+   const int n = m.size * ST_W;
+   // pinned host memory the device can address (any cudaHostAlloc /
+   // cudaMallocHost buffer under unified addressing): a small kernel writes
+   // the rows there, so the copy joins the stream's chain of programmatically
+   // serialised kernels instead of waiting for a copy-engine transfer
+   cudaPointerAttributes pa;
+   if (cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost && pa.devicePointer) {
+      const double* src = m.cur;
+      double* dst = static_cast<double*>(pa.devicePointer);
+      return cuda_err(h, launch_pdl(stats_rows_copy_kernel, dim3(1), dim3(32 * ((n + 31) / 32 < 8 ? (n + 31) / 32 : 8)),
+                                    0, h->stream, src, dst, n),
+                      "statistics rows");
+   }
+   cudaGetLastError();  // a failed attribute query leaves no error behind
+   return cuda_err(h, cudaMemcpyAsync(out, m.cur, sizeof(double) * n, cudaMemcpyDefault, h->stream),
                    "statistics rows");
 }
 

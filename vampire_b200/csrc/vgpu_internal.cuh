@@ -167,4 +167,23 @@ extern template cudaError_t launch_llg_pass<double>(const LLGArgs<double>&, int,
 extern template cudaError_t launch_thermal_noise<float>(const LLGArgs<float>&, cudaStream_t);
 extern template cudaError_t launch_thermal_noise<double>(const LLGArgs<double>&, cudaStream_t);
 
+// A kernel launched with programmatic stream serialisation: its blocks may be
+// scheduled while the previous kernel of the stream drains.  The kernel must
+// execute griddepcontrol.wait before it touches anything that kernel writes
+// (the staged LLG passes, the small-mask magnetisation update, the row copy).
+template <typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(Args...), dim3 g, dim3 b, int smem, cudaStream_t st, Args... args) {
+   cudaLaunchConfig_t cfg = {};
+   cfg.gridDim = g;
+   cfg.blockDim = b;
+   cfg.dynamicSmemBytes = (size_t)smem;
+   cfg.stream = st;
+   cudaLaunchAttribute attr[1];
+   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+   attr[0].val.programmaticStreamSerializationAllowed = 1;
+   cfg.attrs = attr;
+   cfg.numAttrs = 1;
+   return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 }  // namespace vgpu
