@@ -568,8 +568,11 @@ int vgpu_stats_reset(vgpu_handle h);
  * energies (total, exchange, anisotropy, applied, magnetostatic) -- the
  * values vgpu_stats_get_* return.  out is pinned host or device memory; the
  * copy completes in order on the handle's stream (vgpu_get_stream), so a
- * host can read step t's result while step t+1 runs.  No reference
- * counterpart (vcuda::stats::get blocks). */
+ * host can read step t's result while step t+1 runs.  Into pinned host
+ * memory the device can address (cudaHostAlloc / cudaMallocHost under
+ * unified addressing) the rows are written by a small kernel through that
+ * mapping; otherwise by cudaMemcpyAsync.  No reference counterpart
+ * (vcuda::stats::get blocks). */
 int vgpu_stats_copy_rows(vgpu_handle h, int32_t id, double* out);
 
 /* ---- spin snapshots (configuration output) ------------------------------ */
