@@ -650,11 +650,16 @@ int vgpu_batch_create(int device, int precision, int32_t n_sys, const vgpu_syste
                       const vgpu_batch_system* systems, const vgpu_sim_params* common, vgpu_handle* out);
 
 /* Shape of the persistent launch: thread-block cluster size (1, 2, 4, 8) and
- * threads per block; systems are bin-packed onto the co-resident clusters. */
+ * threads per block; systems are bin-packed onto the co-resident clusters.
+ * cluster = 0 (block ignored): no persistent kernel -- vgpu_batch_run steps
+ * the whole batch with the ordinary two passes per step (as vgpu_llg_heun),
+ * with the same records; faster when one large system would dominate a
+ * cluster's share.  Results are the same for every shape. */
 int vgpu_batch_set_shape(vgpu_handle h, int32_t cluster, int32_t block);
 
-/* Time every candidate shape for trial_steps steps on this batch and keep the
- * fastest (the state is restored afterwards). */
+/* Time every candidate shape (the step passes, cluster = 0, among them) for
+ * trial_steps steps on this batch and keep the fastest (the state is
+ * restored afterwards). */
 int vgpu_batch_autotune(vgpu_handle h, int32_t trial_steps, int32_t* cluster_out, int32_t* block_out,
                         double* ms_per_step_out);
 

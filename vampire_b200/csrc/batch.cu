@@ -20,6 +20,15 @@
 // graph holds {persistent kernel, per-system magnetisation record, step
 // advance} and is replayed.  Cluster size and block size come from an
 // autotuner that times the candidates on the batch itself.
+//
+// Shape cluster = 0 runs the batch as the one system it is, with the
+// ordinary two step passes per step over all atoms (vgpu_llg_heun) and the
+// same per-system records between chunks.  No system is tied to one cluster,
+// so the largest particle no longer sets the step time: on 256 particles of
+// 150-10,000 spins (380,178 in all) 0.025 ms per step against 0.045 ms for
+// the best persistent shape (cluster 8, blocks of 128).  The passes take the
+// step number as a kernel argument, so this shape is not captured in a graph.
+// Same physics and numbers as the persistent kernel (tests/test_batch_gpu.py).
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -199,8 +208,13 @@ static void pack(const std::vector<int>& off, int groups, std::vector<int>& gsta
 template <typename R>
 static int set_shape_typed(vgpu_ctx* h, int cluster, int block) {
    BatchState* b = batch_of(h);
+   if (cluster == 0) {  // the ordinary step passes (block size is theirs)
+      b->cluster = 0;
+      b->block = 0;
+      return VGPU_OK;
+   }
    if (cluster < 1 || cluster > 8 || (cluster & (cluster - 1)))
-      return set_err(h, VGPU_ERR_ARG, "cluster size must be 1, 2, 4 or 8 (got %d)", cluster);
+      return set_err(h, VGPU_ERR_ARG, "cluster size must be 0, 1, 2, 4 or 8 (got %d)", cluster);
    if (block < 64 || block > 1024 || block % 32) return set_err(h, VGPU_ERR_ARG, "bad block size %d", block);
    cudaLaunchConfig_t cfg;
    std::memset(&cfg, 0, sizeof cfg);
@@ -243,18 +257,23 @@ int batch_set_shape(vgpu_ctx* h, int cluster, int block) {
 template <typename R>
 static int run_chunk_typed(vgpu_ctx* h, int nsteps, int record) {
    BatchState* b = batch_of(h);
-   LLGArgs<R> a = make_args<R>(h);
-   h->prof_begin(PROF_PREDICTOR);
-   cudaError_t e = launch_persistent_fmt<R>(h, a, nsteps);
-   h->prof_end(PROF_PREDICTOR);
-   if (e != cudaSuccess) return cuda_err(h, e, "persistent batch launch");
+   if (b->cluster == 0) {
+      // the step passes (they advance h->step themselves)
+      if (int rc = vgpu_llg_heun(h, (uint64_t)nsteps)) return rc;
+   } else {
+      LLGArgs<R> a = make_args<R>(h);
+      h->prof_begin(PROF_PREDICTOR);
+      cudaError_t e = launch_persistent_fmt<R>(h, a, nsteps);
+      h->prof_end(PROF_PREDICTOR);
+      if (e != cudaSuccess) return cuda_err(h, e, "persistent batch launch");
+   }
    if (record) {
       batch_record_kernel<R><<<b->n_sys, 256, 0, h->stream>>>(
           b->n_sys, b->d_off, (const R*)h->sys.s[0], (const R*)h->sys.s[1], (const R*)h->sys.s[2],
           (const int*)h->sys.mat, (const MatParams<R>*)h->sys.mp, b->d_rec, b->hist_cap, b->d_hist);
    }
    batch_advance_kernel<<<1, 1, 0, h->stream>>>(b->d_step, b->d_rec, nsteps, record);
-   h->kernel_launches += 2 + record;
+   h->kernel_launches += (b->cluster == 0 ? 1 : 2) + record;  // the step passes count their own
    return cuda_err(h, cudaGetLastError(), "batch launch");
 }
 
@@ -278,6 +297,13 @@ static int run_typed(vgpu_ctx* h, uint64_t n_steps, uint32_t record_every, int u
    }
    cudaMemcpyAsync(b->d_step, &h->step, sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream);
    cudaMemsetAsync(b->d_rec, 0, sizeof(unsigned long long), h->stream);
+   if (b->cluster == 0) {  // step passes: h->step advances with every step
+      for (uint64_t c = 0; c < chunks; ++c)
+         if (int rc = run_chunk_typed<R>(h, S, record)) return rc;
+      if (rem > 0)
+         if (int rc = run_chunk_typed<R>(h, rem, 0)) return rc;
+      return VGPU_OK;
+   }
    if (use_graph && chunks > 0) {
       if (!b->graph || b->graph_steps != S || b->graph_cluster != b->cluster || b->graph_block != b->block) {
          if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
@@ -460,7 +486,7 @@ extern "C" int vgpu_batch_autotune(vgpu_handle h, int32_t trial_steps, int32_t* 
       cudaMemcpyAsync(save[q], h->sys.s[q], bytes, cudaMemcpyDeviceToDevice, h->stream);
    }
    const uint64_t step0 = h->step;
-   const int clusters[4] = {1, 2, 4, 8};
+   const int clusters[5] = {0, 1, 2, 4, 8};
    const int blocks[3] = {128, 256, 512};
    double best = 1e300;
    int bc = 1, bb = 256;
@@ -469,7 +495,8 @@ extern "C" int vgpu_batch_autotune(vgpu_handle h, int32_t trial_steps, int32_t* 
    cudaEventCreate(&e1);
    for (int c : clusters)
       for (int bl : blocks) {
-         if (batch_set_shape(h, c, bl) != VGPU_OK) continue;
+         if (c == 0 && bl != blocks[0]) continue;  // the step passes: one candidate
+         if (batch_set_shape(h, c, c == 0 ? 0 : bl) != VGPU_OK) continue;
          if (vgpu_batch_run(h, 2, 0, 0) != VGPU_OK) continue;  // warm-up
          cudaEventRecord(e0, h->stream);
          if (vgpu_batch_run(h, trial_steps, 0, 0) != VGPU_OK) continue;
@@ -477,7 +504,7 @@ extern "C" int vgpu_batch_autotune(vgpu_handle h, int32_t trial_steps, int32_t* 
          cudaEventSynchronize(e1);
          float ms = 0.f;
          cudaEventElapsedTime(&ms, e0, e1);
-         if (ms < best) { best = ms; bc = c; bb = bl; }
+         if (ms < best) { best = ms; bc = c; bb = c == 0 ? 0 : bl; }
       }
    cudaEventDestroy(e0);
    cudaEventDestroy(e1);

@@ -141,6 +141,9 @@ __device__ __forceinline__ void llg_correct_atom(const LLGArgs<R>& a, int i) {
 
 template <typename R, int FMT, int MODE, int VAR>
 __global__ void __launch_bounds__(256) llg_pass_kernel(const LLGArgs<R> a) {
+   // launched with programmatic stream serialisation (launch_pdl): the
+   // previous kernel of the stream has completed and its writes are visible
+   asm volatile("griddepcontrol.wait;" ::: "memory");
    const int i = (MODE == PASS_FIELD ? 0 : 32 * a.slice_first) + blockIdx.x * blockDim.x + threadIdx.x;
    if (i >= (MODE == PASS_FIELD ? a.n : a.n_upd)) return;
    if (MODE == PASS_PREDICTOR) {
@@ -160,10 +163,11 @@ __global__ void __launch_bounds__(256) llg_pass_kernel(const LLGArgs<R> a) {
 }
 
 template <typename R, int FMT, int VAR>
-inline void launch_mode(const LLGArgs<R>& a, int mode, int grid, int bs, cudaStream_t st) {
-   if (mode == PASS_PREDICTOR) llg_pass_kernel<R, FMT, PASS_PREDICTOR, VAR><<<grid, bs, 0, st>>>(a);
-   else if (mode == PASS_CORRECTOR) llg_pass_kernel<R, FMT, PASS_CORRECTOR, VAR><<<grid, bs, 0, st>>>(a);
-   else llg_pass_kernel<R, FMT, PASS_FIELD, VAR><<<grid, bs, 0, st>>>(a);
+inline cudaError_t launch_mode(const LLGArgs<R>& a, int mode, int grid, int bs, cudaStream_t st) {
+   const dim3 g(grid), b(bs);
+   if (mode == PASS_PREDICTOR) return launch_pdl(llg_pass_kernel<R, FMT, PASS_PREDICTOR, VAR>, g, b, 0, st, a);
+   if (mode == PASS_CORRECTOR) return launch_pdl(llg_pass_kernel<R, FMT, PASS_CORRECTOR, VAR>, g, b, 0, st, a);
+   return launch_pdl(llg_pass_kernel<R, FMT, PASS_FIELD, VAR>, g, b, 0, st, a);
 }
 
 template <typename R, int FMT>
@@ -171,10 +175,9 @@ inline cudaError_t launch_fmt(const LLGArgs<R>& a, int mode, cudaStream_t st) {
    const int bs = 256;
    const int grid = ((mode == PASS_FIELD ? a.n : a.n_upd - 32 * a.slice_first) + bs - 1) / bs;
    if (grid <= 0) return cudaSuccess;
-   if (a.integrator == INTEG_MIDPOINT && mode != PASS_FIELD) launch_mode<R, FMT, VAR_MIDPOINT>(a, mode, grid, bs, st);
-   else if (a.aniso_ext || a.bq_off) launch_mode<R, FMT, VAR_HEUN_EXT>(a, mode, grid, bs, st);
-   else launch_mode<R, FMT, VAR_HEUN>(a, mode, grid, bs, st);
-   return cudaGetLastError();
+   if (a.integrator == INTEG_MIDPOINT && mode != PASS_FIELD) return launch_mode<R, FMT, VAR_MIDPOINT>(a, mode, grid, bs, st);
+   if (a.aniso_ext || a.bq_off) return launch_mode<R, FMT, VAR_HEUN_EXT>(a, mode, grid, bs, st);
+   return launch_mode<R, FMT, VAR_HEUN>(a, mode, grid, bs, st);
 }
 
 template <typename R>
