@@ -221,6 +221,7 @@ __global__ void adj_reciprocal_kernel(const LLGArgs<double> a, int* bad) {
 
 template <int FMT>
 __global__ void __launch_bounds__(256) adj_k1(const LLGArgs<double> a, AdjBufs b) {
+   asm volatile("griddepcontrol.wait;" ::: "memory");  // launched by launch_pdl
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    if (i >= b.n) return;
    const int st = b.stride;
@@ -262,6 +263,7 @@ __device__ __forceinline__ void pair_flush(const double* sp, const AdjBufs& b, i
 
 template <int FMT>
 __global__ void __launch_bounds__(256) adj_k2(const LLGArgs<double> a, AdjBufs b) {
+   asm volatile("griddepcontrol.wait;" ::: "memory");  // launched by launch_pdl
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    const int st = b.stride;
    double gv[5] = {0, 0, 0, 0, 0};
@@ -308,6 +310,7 @@ __global__ void __launch_bounds__(256) adj_k2(const LLGArgs<double> a, AdjBufs b
 
 template <int FMT>
 __global__ void __launch_bounds__(256) adj_k3(const LLGArgs<double> a, AdjBufs b) {
+   asm volatile("griddepcontrol.wait;" ::: "memory");  // launched by launch_pdl
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    const int st = b.stride;
    double gv[5] = {0, 0, 0, 0, 0};
@@ -359,6 +362,7 @@ __global__ void __launch_bounds__(256) adj_k3(const LLGArgs<double> a, AdjBufs b
 
 template <int FMT>
 __global__ void __launch_bounds__(256) adj_k4(const LLGArgs<double> a, AdjBufs b, int64_t t) {
+   asm volatile("griddepcontrol.wait;" ::: "memory");  // launched by launch_pdl
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    if (i >= b.n) return;
    const int st = b.stride;
@@ -390,6 +394,7 @@ __global__ void adj_lambda_init(const LLGArgs<double> a, AdjBufs b, int64_t N) {
 template <typename R>
 __global__ void mz_kernel(int n, const R* __restrict__ sz, const int* __restrict__ mat,
                           const MatParams<R>* __restrict__ mp, double* out) {
+   asm volatile("griddepcontrol.wait;" ::: "memory");  // launched by launch_pdl
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    double v = 0.0;
    if (i < n) v = (double)sz[i] * (double)mp[mat ? mat[i] : 0].mu_s_muB;
@@ -407,10 +412,11 @@ __global__ void mz_kernel(int n, const R* __restrict__ sz, const int* __restrict
 template <int FMT>
 static void adj_step(const LLGArgs<double>& a, const AdjBufs& b, int64_t t, cudaStream_t st) {
    const int g = (b.n + 255) / 256;
-   adj_k1<FMT><<<g, 256, 0, st>>>(a, b);
-   adj_k2<FMT><<<g, 256, 0, st>>>(a, b);
-   adj_k3<FMT><<<g, 256, 0, st>>>(a, b);
-   adj_k4<FMT><<<g, 256, 0, st>>>(a, b, t);
+   // consecutive small launches: programmatic serialisation hides their gaps
+   launch_pdl(adj_k1<FMT>, dim3(g), dim3(256), 0, st, a, b);
+   launch_pdl(adj_k2<FMT>, dim3(g), dim3(256), 0, st, a, b);
+   launch_pdl(adj_k3<FMT>, dim3(g), dim3(256), 0, st, a, b);
+   launch_pdl(adj_k4<FMT>, dim3(g), dim3(256), 0, st, a, b, t);
 }
 
 static void adj_step_fmt(int fmt, const LLGArgs<double>& a, const AdjBufs& b, int64_t t, cudaStream_t st) {
@@ -499,8 +505,9 @@ extern "C" int vgpu_mz_trajectory(vgpu_handle h, uint64_t n_steps, double* mz_ou
    LLGArgs<double> a = make_args<double>(h);
    for (uint64_t t = 0; t < n_steps; ++t) {
       if ((rc = forward_step(h, a, cur.p, pb.p, eb.p, st))) return rc;
-      mz_kernel<double><<<(S.n + 255) / 256, 256, 0, h->stream>>>(S.n, cur.p + 2 * (size_t)st, (const int*)S.mat,
-                                                                   (const MatParams<double>*)S.mp, mz.p + t + 1);
+      launch_pdl(mz_kernel<double>, dim3((S.n + 255) / 256), dim3(256), 0, h->stream, (int)S.n,
+                 (const double*)(cur.p + 2 * (size_t)st), (const int*)S.mat, (const MatParams<double>*)S.mp,
+                 (double*)(mz.p + t + 1));
    }
    std::vector<double> host(n_steps + 1);
    e = cudaMemcpyAsync(host.data(), mz.p, sizeof(double) * (n_steps + 1), cudaMemcpyDeviceToHost, h->stream);
@@ -565,8 +572,9 @@ static int adjoint_run(vgpu_handle h, uint64_t n_steps, const double* target, do
       if (t % C == 0)
          cudaMemcpyAsync(cp.p + v3 * (t / C), cur, sizeof(double) * v3, cudaMemcpyDeviceToDevice, h->stream);
       if ((rc = forward_step(h, a, cur, pb.p, eb.p, st))) return rc;
-      mz_kernel<double><<<(n + 255) / 256, 256, 0, h->stream>>>(n, cur + 2 * (size_t)st, (const int*)S.mat,
-                                                                 (const MatParams<double>*)S.mp, mz.p + t + 1);
+      launch_pdl(mz_kernel<double>, dim3((n + 255) / 256), dim3(256), 0, h->stream, (int)n,
+                 (const double*)(cur + 2 * (size_t)st), (const int*)S.mat, (const MatParams<double>*)S.mp,
+                 (double*)(mz.p + t + 1));
    }
    // loss on the host from m_z(t)
    std::vector<double> mzh(N + 1);

@@ -109,6 +109,7 @@ __device__ __forceinline__ R site_energy_delta(const LLGArgs<R>& a, int i, int m
 #endif
 template <typename R, int FMT>
 __global__ void __launch_bounds__(256, VGPU_MC_MIN_BLOCKS) mc_colour_kernel(const MCArgs<R> p) {
+   asm volatile("griddepcontrol.wait;" ::: "memory");  // launched by launch_pdl: the previous colour is done
    const int t = blockIdx.x * blockDim.x + threadIdx.x;
    bool rejected = false;
    if (t < p.count) {
@@ -195,8 +196,7 @@ __global__ void mc_entries_kernel(const int* __restrict__ atoms, int count, cons
 template <typename R, int FMT>
 static cudaError_t launch_mc(const MCArgs<R>& p, cudaStream_t st) {
    if (p.count == 0) return cudaSuccess;
-   mc_colour_kernel<R, FMT><<<(p.count + 255) / 256, 256, 0, st>>>(p);
-   return cudaGetLastError();
+   return launch_pdl(mc_colour_kernel<R, FMT>, dim3((p.count + 255) / 256), dim3(256), 0, st, p);
 }
 
 template <typename R>
