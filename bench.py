@@ -218,13 +218,37 @@ def bench_batched(device, steps=2000, plain_steps=200):
         b.run(100, record_every=100)
         torch.cuda.synchronize()
         stream = torch.cuda.ExternalStream(b_stream(b), device=device)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        b.run(steps, record_every=100)
-        e1.record(stream)
-        e1.synchronize()
-        ms_b = e0.elapsed_time(e1)
+
+        def timed(k):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.run(k, record_every=100)
+            e1.record(stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1)
+        ms_b = timed(steps)
         hist = b.history()
+        # the best persistent cluster kernel (CUDA graph) beside the pick, when
+        # the pick is the ordinary step passes
+        persistent = None
+        if tune["cluster"] == 0:
+            best = None
+            for c in (1, 2, 4, 8):
+                for bl in (128, 256, 512):
+                    try:
+                        b.set_shape(c, bl)
+                    except Exception:
+                        continue
+                    b.run(100, record_every=100)
+                    ms = timed(100)
+                    if best is None or ms < best[0]:
+                        best = (ms, c, bl)
+            if best:
+                b.set_shape(best[1], best[2])
+                b.run(100, record_every=100)
+                ms_p_best = timed(steps)
+                persistent = {"cluster": best[1], "block": best[2], "value": n * steps / (ms_p_best * 1e-3),
+                              "ms_per_step": ms_p_best / steps}
     sims = []
     for k, s in enumerate(systems):
         s.params.temperature = params[k]["temperature"]
@@ -241,7 +265,7 @@ def bench_batched(device, steps=2000, plain_steps=200):
     for sim in sims:
         sim.close()
     mode = "step passes over the whole batch" if tune["cluster"] == 0 else "persistent cluster kernel, CUDA graph"
-    return {"systems": 256, "spins": n, "steps": steps, "shape": tune, "mode": mode,
+    return {"systems": 256, "spins": n, "steps": steps, "shape": tune, "mode": mode, "persistent_graph": persistent,
             "value": n * steps / (ms_b * 1e-3), "unit": UNIT, "ms": ms_b,
             "plain_per_system_value": n * steps / (ms_p * 1e-3), "speedup_vs_per_system": ms_p / ms_b,
             "records": int(hist.shape[0]),
@@ -320,22 +344,32 @@ def bench_adjoint(device, L=32, steps=2000):
     """Adjoint LLG-Heun on SC 32^3 (32,768 spins), T=0, 2,000 steps: the
     gradient of the trajectory loss w.r.t. (J, Ku, H) at J=11.2e-21 J,
     Ku=6.69e-24 J, H=(0,0,0.4) T against the target m_z(t) of J=10e-21 J,
-    Ku=5e-24 J, H=(0,0,0.5) T; FP64, sqrt(N) checkpointing.  Timed around
-    AdjointRunner.loss_and_grad: the system set-up and upload and the C-ABI
-    call (forward with checkpoints, segment recomputation and the backward
-    sweep); the median of three calls, which give identical results."""
+    Ku=5e-24 J, H=(0,0,0.5) T; the FP32 production build (FP64 sums for m_z,
+    the loss and the gradients), sqrt(N) checkpointing, with the FP64 debug
+    build timed beside it.  Timed around AdjointRunner.loss_and_grad: the
+    system set-up and upload and the C-ABI call (forward with checkpoints,
+    segment recomputation and the backward sweep); the median of five calls
+    after two warm-up calls."""
     from vampire_b200 import adjoint as A
-    run = A.AdjointRunner(L=L, device=device)
-    target = run.trajectory(10e-21, 5e-24, (0.0, 0.0, 0.5), steps)
-    run.loss_and_grad(11.2e-21, 6.69e-24, (0.0, 0.0, 0.4), target[:50])  # warm-up
-    # three timed gradients, the median reported: the host wall clock around
+    run = A.AdjointRunner(L=L, device=device, precision="fp32")
+    run64 = A.AdjointRunner(L=L, device=device, precision="fp64")
+    target = run64.trajectory(10e-21, 5e-24, (0.0, 0.0, 0.5), steps)
+    for _ in range(2):  # warm-up (module loading, first allocations)
+        run.loss_and_grad(11.2e-21, 6.69e-24, (0.0, 0.0, 0.4), target)
+    # five timed gradients, the median reported: the host wall clock around
     # ~20,000 launches varies between runs on a shared host
     times = []
-    for _ in range(3):
+    for _ in range(5):
         t0 = time.perf_counter()
         loss, grad = run.loss_and_grad(11.2e-21, 6.69e-24, (0.0, 0.0, 0.4), target)
         times.append(time.perf_counter() - t0)
-    dt = sorted(times)[1]
+    dt = sorted(times)[2]
+    run64.loss_and_grad(11.2e-21, 6.69e-24, (0.0, 0.0, 0.4), target)  # warm-up
+    times64 = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        loss64, grad64 = run64.loss_and_grad(11.2e-21, 6.69e-24, (0.0, 0.0, 0.4), target)
+        times64.append(time.perf_counter() - t0)
     # error: the adjoint gradient against central differences (h = 1e-6
     # relative) of the device FP64 forward loss, for J, Ku and H_z
     import numpy as np
@@ -346,12 +380,16 @@ def bench_adjoint(device, L=32, steps=2000):
         pp, pm = p.copy(), p.copy()
         pp[k] += h
         pm[k] -= h
-        fd = (run.loss_and_grad(pp[0], pp[1], pp[2:], target)[0] -
-              run.loss_and_grad(pm[0], pm[1], pm[2:], target)[0]) / (2 * h)
+        fd = (run64.loss_and_grad(pp[0], pp[1], pp[2:], target)[0] -
+              run64.loss_and_grad(pm[0], pm[1], pm[2:], target)[0]) / (2 * h)
         rel.append(abs(grad[k] - fd) / abs(fd))
     return {"workload": f"SC {L}^3, {steps} steps, loss = sum_t dt (m_z - target)^2, grad w.r.t. J, Ku, H (3)",
             "spins": L ** 3, "steps": steps, "seconds": dt, "seconds_all": times, "value": L ** 3 * steps / dt,
-            "unit": "spin-steps/s (forward + backward)", "precision": "fp64", "loss": loss,
+            "unit": "spin-steps/s (forward + backward)", "precision": "fp32",
+            "fp64_build": {"seconds": sorted(times64)[2], "value": L ** 3 * steps / sorted(times64)[2],
+                           "max_rel_grad_dev_fp32": float(np.max(np.abs(grad - grad64)[[0, 1, 4]] /
+                                                                 np.abs(grad64)[[0, 1, 4]]))},
+            "loss": loss,
             "grad": [float(g) for g in grad], "checkpoints": int(-(-steps // int(steps ** 0.5 + 0.999999))),
             "error_vs_fd": {"max_rel_dev": float(max(rel)), "components": ["J", "Ku", "Hz"],
                             "against": "central differences (h = 1e-6 relative) of the FP64 forward loss"}}

@@ -679,7 +679,7 @@ int vgpu_batch_system_range(vgpu_handle h, int32_t k, int32_t* first_atom, int32
 /* ---- adjoint (gradients of a trajectory loss) ----------------------------- */
 
 /* No counterpart in the reference.  From the current spins (left unchanged),
- * run n_steps deterministic FP64 Heun steps and return
+ * run n_steps deterministic Heun steps and return
  *   loss = sum_{t=1..n_steps} w (m_z(t) - target[t-1])^2
  * (m_z: moment-weighted mean of s_z after step t) and
  *   grad[0] = dL/d(common scale of every exchange coupling),
@@ -689,8 +689,10 @@ int vgpu_batch_system_range(vgpu_handle h, int32_t k, int32_t* first_atom, int32
  * diagonal + DMI, full tensor) and any number of materials, provided the
  * couplings are reciprocal in SI units (mu_s,j J_ji = (mu_s,i J_ij)^T, as a
  * symmetric exchange matrix and the three-site DMI give; checked on the
- * device, VGPU_ERR_ARG otherwise).  Needs the FP64 build, no thermal noise,
- * no dipole field. */
+ * device, VGPU_ERR_ARG otherwise).  No thermal noise, no dipole field.  The
+ * state, the recomputed steps and the adjoint vectors are in the handle's
+ * precision (FP32 production, FP64 debug build); m_z, the loss and the
+ * gradients are FP64 sums. */
 int vgpu_adjoint_llg(vgpu_handle h, uint64_t n_steps, const double* target, double w, int32_t every,
                      double* loss_out, double* grad_out);
 
@@ -705,8 +707,9 @@ int vgpu_adjoint_llg(vgpu_handle h, uint64_t n_steps, const double* target, doub
 int vgpu_adjoint_llg_materials(vgpu_handle h, uint64_t n_steps, const double* target, double w, int32_t every,
                                double* loss_out, double* grad_out, double* pair_out);
 
-/* m_z(t), t = 1..n_steps, of a deterministic FP64 run from the current spins
- * (left unchanged): the targets of vgpu_adjoint_llg. */
+/* m_z(t), t = 1..n_steps, of a deterministic run (the handle's precision,
+ * FP64 sums) from the current spins (left unchanged): the targets of
+ * vgpu_adjoint_llg. */
 int vgpu_mz_trajectory(vgpu_handle h, uint64_t n_steps, double* mz_out);
 
 /* ---- magnetisation without device allocation ----------------------------- */

@@ -47,33 +47,37 @@ def test_cpu_adjoint_matches_finite_differences(every):
 
 
 @pytest.mark.gpu
-def test_device_adjoint_config4(vgpu_lib):
-    """Config 4: SC 32^3, 2,000 steps, sqrt(N) checkpointing on the device.
-    The device gradient agrees with the FP64 CPU adjoint and with central
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_device_adjoint_config4(vgpu_lib, prec):
+    """Config 4: SC 32^3, 2,000 steps, sqrt(N) checkpointing on the device,
+    in the FP32 production build and the FP64 debug build.  The device
+    gradient agrees with the FP64 CPU adjoint (1e-4 relative; the FP32
+    trajectory's own rounding is the difference there) and with central
     finite differences of the device FP64 forward loss to 1e-4 relative."""
-    runner = A.AdjointRunner(L=32, seed=2025)
+    runner = A.AdjointRunner(L=32, seed=2025, precision=prec)
+    r64 = A.AdjointRunner(L=32, seed=2025, precision="fp64")
     n = 2000
-    target = runner.trajectory(*A.TARGET_PARAMS, n)
+    target = r64.trajectory(*A.TARGET_PARAMS, n)
     J, Ku, H = A.START_PARAMS
     loss, grad = runner.loss_and_grad(J, Ku, H, target)
     # FP64 CPU adjoint on the same problem
     s = A.system(J, Ku, H, 32, 2025)
     cl, cg = O.OracleSystem(s).adjoint(s.spins, target, s.params.dt_SI)
     cgrad = np.array([cg[0] / J, cg[1], cg[2], cg[3], cg[4]])
-    assert abs(loss - cl) <= 1e-9 * abs(cl)
+    assert abs(loss - cl) <= (1e-4 if prec == "fp32" else 1e-9) * abs(cl)
     big = np.abs(cgrad).max()
     for k in range(5):
         ref = abs(cgrad[k]) if k < 2 or k == 4 else abs(cgrad[2:]).max()
         assert abs(grad[k] - cgrad[k]) <= 1e-4 * max(ref, 1e-12 * big), (k, grad[k], cgrad[k])
-    # central differences of the device forward loss for J, Ku, Hz
+    # central differences of the device FP64 forward loss for J, Ku, Hz
     p = np.array([J, Ku, *H])
     for k, sc in ((0, J), (1, Ku), (4, 0.4)):
         h = 1e-6 * sc
         pp, pm = p.copy(), p.copy()
         pp[k] += h
         pm[k] -= h
-        lp = runner.loss_and_grad(pp[0], pp[1], pp[2:], target)[0]
-        lm = runner.loss_and_grad(pm[0], pm[1], pm[2:], target)[0]
+        lp = r64.loss_and_grad(pp[0], pp[1], pp[2:], target)[0]
+        lm = r64.loss_and_grad(pm[0], pm[1], pm[2:], target)[0]
         fd = (lp - lm) / (2 * h)
         assert abs(grad[k] - fd) <= 1e-4 * abs(fd), (k, grad[k], fd)
 
@@ -144,22 +148,26 @@ def test_cpu_adjoint_two_material_dmi_matches_finite_differences():
 
 
 @pytest.mark.gpu
-def test_device_adjoint_per_material_exchange_and_dmi(vgpu_lib):
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_device_adjoint_per_material_exchange_and_dmi(vgpu_lib, prec):
     """The device adjoint on the two-material DMI alloy: the five gradients
-    equal the FP64 CPU adjoint's (1e-9 relative), and the per-material-pair
-    exchange gradients dL/dJ_ab and the DMI-scale gradient agree with central
-    differences (h = 1e-6 relative) of the oracle's forward loss to 1e-4
-    relative; their sum is the common-scale gradient."""
+    equal the FP64 CPU adjoint's (1e-9 relative in the FP64 build, 1e-4 in
+    FP32), and the per-material-pair exchange gradients dL/dJ_ab and the
+    DMI-scale gradient agree with central differences (h = 1e-6 relative) of
+    the oracle's forward loss to 1e-4 relative; their sum is the
+    common-scale gradient."""
     n = 150
     target = _alloy_target(n)
     D = 0.1 * ALLOY_J
     s = _alloy(ALLOY_J, D, ALLOY_H)
-    loss, g, gdmi, pair = A.loss_and_grad_materials(s, target)
+    loss, g, gdmi, pair = A.loss_and_grad_materials(s, target, precision=prec)
     cl, cg = O.OracleSystem(s).adjoint(s.spins, target, s.params.dt_SI)
-    assert abs(loss - cl) <= 1e-10 * abs(cl)
+    tol = 1e-4 if prec == "fp32" else 1e-9
+    assert abs(loss - cl) <= max(tol, 1e-10) * abs(cl)
     for k in (0, 1, 4):
-        assert abs(g[k] - cg[k]) <= 1e-9 * max(abs(cg[k]), 1e-30), (k, g[k], cg[k])
-    assert abs(pair.sum() + gdmi - g[0]) <= 1e-9 * abs(g[0])
+        assert abs(g[k] - cg[k]) <= tol * max(abs(cg[k]), 1e-30), (k, g[k], cg[k])
+    # the same sum by bonds and by fields: FP32 products rounded apart in FP32
+    assert abs(pair.sum() + gdmi - g[0]) <= (1e-6 if prec == "fp32" else 1e-9) * abs(g[0])
     h = 1e-6
     for a in range(2):
         for b in range(2):

@@ -27,7 +27,11 @@
 // the couplings of the bonds from atoms of a to atoms of b (the diagonal,
 // exchange-matrix part for the diagonal + DMI format), plus the common scale
 // of the DMI vectors.  States are checkpointed every ceil(sqrt(N)) steps and
-// recomputed segment by segment with the FP64 forward kernels.
+// recomputed segment by segment with the forward passes.
+//
+// Precision: the state, the recomputed steps and the adjoint vectors are in
+// the handle's precision (FP32 in production, FP64 in the debug build); the
+// parameter gradients, m_z and the loss are FP64 sums.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -39,10 +43,11 @@
 
 namespace vgpu {
 
+template <typename R>
 struct AdjBufs {
-   double* S;                   // [3n] state s_t (segment slot)
-   double *sp, *ex0, *ex1, *f0, *ub, *spb, *sb, *Hb0, *Hb1, *lam;   // [3n] each, x|y|z blocks
-   double* nv;                  // [n] |v|
+   R* S;                        // [3n] state s_t (segment slot)
+   R *sp, *ex0, *ex1, *f0, *ub, *spb, *sb, *Hb0, *Hb1, *lam;   // [3n] each, x|y|z blocks
+   R* nv;                       // [n] |v|
    double* g;                   // [5] dL/d(J scale), dL/dKu, dL/dH
    double* gp;                  // [1 + M*M] dL/d(DMI scale), dL/d(scale of the a->b couplings), or nullptr
    const double* mz;            // [N+1]
@@ -51,12 +56,12 @@ struct AdjBufs {
    int n, stride;               // stride = n_alloc (component offset)
 };
 
-__device__ __forceinline__ void f_vjp_d(double A, double B, const double s[3], const double H[3], const double a[3],
-                                        double sb[3], double Hb[3]) {
-   const double sH = s[0] * H[0] + s[1] * H[1] + s[2] * H[2];
-   const double as = a[0] * s[0] + a[1] * s[1] + a[2] * s[2];
-   const double aH = a[0] * H[0] + a[1] * H[1] + a[2] * H[2];
-   const double ss = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
+template <typename R>
+__device__ __forceinline__ void f_vjp(R A, R B, const R s[3], const R H[3], const R a[3], R sb[3], R Hb[3]) {
+   const R sH = s[0] * H[0] + s[1] * H[1] + s[2] * H[2];
+   const R as = a[0] * s[0] + a[1] * s[1] + a[2] * s[2];
+   const R aH = a[0] * H[0] + a[1] * H[1] + a[2] * H[2];
+   const R ss = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
    sb[0] = A * (H[1] * a[2] - H[2] * a[1]);
    sb[1] = A * (H[2] * a[0] - H[0] * a[2]);
    sb[2] = A * (H[0] * a[1] - H[1] * a[0]);
@@ -65,33 +70,34 @@ __device__ __forceinline__ void f_vjp_d(double A, double B, const double s[3], c
    Hb[2] = A * (a[0] * s[1] - a[1] * s[0]);
 #pragma unroll
    for (int k = 0; k < 3; ++k) {
-      sb[k] += B * (a[k] * sH + as * H[k] - 2.0 * aH * s[k]);
+      sb[k] += B * (a[k] * sH + as * H[k] - (R)2 * aH * s[k]);
       Hb[k] += B * (as * s[k] - a[k] * ss);
    }
 }
 
-__device__ __forceinline__ void aniso_d(const LLGArgs<double>& a, const MatParams<double>& m, const double S[3],
-                                        double H[3]) {
-   H[0] = H[1] = H[2] = 0.0;
+template <typename R>
+__device__ __forceinline__ void aniso_h(const LLGArgs<R>& a, const MatParams<R>& m, const R S[3], R H[3]) {
+   H[0] = H[1] = H[2] = (R)0;
    if (a.uniaxial) {
-      const double k2 = 2.0 * m.ku2 * (S[0] * m.kux + S[1] * m.kuy + S[2] * m.kuz);
+      const R k2 = (R)2 * m.ku2 * (S[0] * m.kux + S[1] * m.kuy + S[2] * m.kuz);
       H[0] += m.kux * k2; H[1] += m.kuy * k2; H[2] += m.kuz * k2;
    }
    if (a.cubic) {
-      const double k4 = 2.0 * m.kc4;
+      const R k4 = (R)2 * m.kc4;
       H[0] += S[0] * S[0] * S[0] * k4; H[1] += S[1] * S[1] * S[1] * k4; H[2] += S[2] * S[2] * S[2] * k4;
    }
 }
 
 // VJP of the anisotropy field with respect to s (added to sbar)
-__device__ __forceinline__ void aniso_vjp_d(const LLGArgs<double>& a, const MatParams<double>& m, const double S[3],
-                                            const double hb[3], double sb[3]) {
+template <typename R>
+__device__ __forceinline__ void aniso_vjp(const LLGArgs<R>& a, const MatParams<R>& m, const R S[3], const R hb[3],
+                                          R sb[3]) {
    if (a.uniaxial) {
-      const double he = hb[0] * m.kux + hb[1] * m.kuy + hb[2] * m.kuz;
-      sb[0] += 2.0 * m.ku2 * he * m.kux; sb[1] += 2.0 * m.ku2 * he * m.kuy; sb[2] += 2.0 * m.ku2 * he * m.kuz;
+      const R he = hb[0] * m.kux + hb[1] * m.kuy + hb[2] * m.kuz;
+      sb[0] += (R)2 * m.ku2 * he * m.kux; sb[1] += (R)2 * m.ku2 * he * m.kuy; sb[2] += (R)2 * m.ku2 * he * m.kuz;
    }
    if (a.cubic) {
-      for (int k = 0; k < 3; ++k) sb[k] += 6.0 * m.kc4 * S[k] * S[k] * hb[k];
+      for (int k = 0; k < 3; ++k) sb[k] += (R)6 * m.kc4 * S[k] * S[k] * hb[k];
    }
 }
 
@@ -113,20 +119,20 @@ __device__ __forceinline__ void grad_add(double v[5], double* g) {
 }
 
 // coupling of SELL entry e (row atom material mi, neighbour material mj) as
-// a 3x3 matrix, row-major, in the FP64 build's formats
-template <int FMT>
-__device__ __forceinline__ void bond_tensor(const LLGArgs<double>& a, int e, int mi, int mj, double T[9]) {
+// a 3x3 matrix, row-major, in the generic (non-compact) formats
+template <typename R, int FMT>
+__device__ __forceinline__ void bond_tensor(const LLGArgs<R>& a, int e, int mi, int mj, R T[9]) {
 #pragma unroll
-   for (int k = 0; k < 9; ++k) T[k] = 0.0;
+   for (int k = 0; k < 9; ++k) T[k] = (R)0;
    if (FMT == FMT_ISO_TAB) {
       T[0] = T[4] = T[8] = a.jtab[mi * a.M + mj];
    } else if (FMT == FMT_ISO_BOND) {
       T[0] = T[4] = T[8] = a.jb[0][e];
    } else if (FMT == FMT_VEC_TAB || FMT == FMT_DMI_TAB) {
-      const double* t = a.jtab + 3 * (mi * a.M + mj);
+      const R* t = a.jtab + 3 * (mi * a.M + mj);
       T[0] = t[0]; T[4] = t[1]; T[8] = t[2];
       if (FMT == FMT_DMI_TAB) {  // d x s: [[0, -dz, dy], [dz, 0, -dx], [-dy, dx, 0]]
-         const double dx = a.jb[0][e], dy = a.jb[1][e], dz = a.jb[2][e];
+         const R dx = a.jb[0][e], dy = a.jb[1][e], dz = a.jb[2][e];
          T[1] = -dz; T[2] = dy; T[3] = dz; T[5] = -dx; T[6] = -dy; T[7] = dx;
       }
    } else if (FMT == FMT_VEC_BOND) {
@@ -137,16 +143,17 @@ __device__ __forceinline__ void bond_tensor(const LLGArgs<double>& a, int e, int
    }
 }
 
-__device__ __forceinline__ int nb_material(const LLGArgs<double>& a, int c, int j) {
+template <typename R>
+__device__ __forceinline__ int nb_material(const LLGArgs<R>& a, int c, int j) {
    return a.mat_shift ? (c >> a.mat_shift) : (a.mat ? a.mat[j] : 0);
 }
 
 // Parameter gradients of one atom's exchange field: hb . (J_ij s_j) summed
 // per material pair (diagonal part for the DMI format) into sp[1 + mi*M + mj]
 // and hb . (d_ij x s_j) into sp[0] (shared memory, this block's sums)
-template <int FMT>
-__device__ __forceinline__ void pair_grads(const LLGArgs<double>& a, int i, int mi, const double* sx,
-                                           const double* sy, const double* sz, const double hb[3], double* sp) {
+template <typename R, int FMT>
+__device__ __forceinline__ void pair_grads(const LLGArgs<R>& a, int i, int mi, const R* sx, const R* sy, const R* sz,
+                                           const R hb[3], double* sp) {
    const int sl = i >> 5, lane = i & 31;
    const int off = a.slice_off[sl];
    const int w = (a.slice_off[sl + 1] - off) >> 5;
@@ -157,12 +164,12 @@ __device__ __forceinline__ void pair_grads(const LLGArgs<double>& a, int i, int 
       const int j = c & a.idx_mask;
       if (j >= a.n) continue;  // padding entry
       const int mj = nb_material(a, c, j);
-      const double s[3] = {sx[j], sy[j], sz[j]};
-      double T[9];
-      bond_tensor<FMT>(a, e, mi, mj, T);
-      const double diag = hb[0] * T[0] * s[0] + hb[1] * T[4] * s[1] + hb[2] * T[8] * s[2];
-      const double off_d = hb[0] * (T[1] * s[1] + T[2] * s[2]) + hb[1] * (T[3] * s[0] + T[5] * s[2]) +
-                           hb[2] * (T[6] * s[0] + T[7] * s[1]);
+      const R s[3] = {sx[j], sy[j], sz[j]};
+      R T[9];
+      bond_tensor<R, FMT>(a, e, mi, mj, T);
+      const double diag = (double)(hb[0] * T[0] * s[0] + hb[1] * T[4] * s[1] + hb[2] * T[8] * s[2]);
+      const double off_d = (double)(hb[0] * (T[1] * s[1] + T[2] * s[2]) + hb[1] * (T[3] * s[0] + T[5] * s[2]) +
+                                    hb[2] * (T[6] * s[0] + T[7] * s[1]));
       if (FMT == FMT_DMI_TAB) {
          atomicAdd(sp + 1 + mi * a.M + mj, diag);
          dm += off_d;
@@ -175,10 +182,10 @@ __device__ __forceinline__ void pair_grads(const LLGArgs<double>& a, int i, int 
 
 // Reciprocity of the couplings in SI units: for every bond i -> j, the sum of
 // mu_s,i J_ij over the bonds of row i to j equals the transpose of the sum of
-// mu_s,j J_ji over the bonds of row j to i (to 1e-10 of its largest entry).
-// Sets *bad = 1 + i at a failing atom.
-template <int FMT>
-__global__ void adj_reciprocal_kernel(const LLGArgs<double> a, int* bad) {
+// mu_s,j J_ji over the bonds of row j to i (to 1e-10 of its largest entry in
+// FP64, 1e-5 for couplings held in FP32).  Sets *bad = 1 + i at a failing atom.
+template <typename R, int FMT>
+__global__ void adj_reciprocal_kernel(const LLGArgs<R> a, int* bad) {
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    if (i >= a.n) return;
    const int mi = a.mat ? a.mat[i] : 0;
@@ -190,21 +197,22 @@ __global__ void adj_reciprocal_kernel(const LLGArgs<double> a, int* bad) {
       if (j >= a.n) continue;
       const int mj = a.mat ? a.mat[j] : 0;
       const double muj = a.mp[mj].mu_s_muB;
-      double Sij[9] = {0}, Sji[9] = {0}, T[9];
+      double Sij[9] = {0}, Sji[9] = {0};
+      R T[9];
       for (int q = 0; q < w; ++q) {
          const int e = off + (i & 31) + 32 * q;
          const int cq = a.col[e];
          if ((cq & a.idx_mask) != j) continue;
-         bond_tensor<FMT>(a, e, mi, nb_material(a, cq, j), T);
-         for (int r = 0; r < 9; ++r) Sij[r] += mui * T[r];
+         bond_tensor<R, FMT>(a, e, mi, nb_material(a, cq, j), T);
+         for (int r = 0; r < 9; ++r) Sij[r] += mui * (double)T[r];
       }
       const int offj = a.slice_off[j >> 5], wj = (a.slice_off[(j >> 5) + 1] - offj) >> 5;
       for (int q = 0; q < wj; ++q) {
          const int e = offj + (j & 31) + 32 * q;
          const int cq = a.col[e];
          if ((cq & a.idx_mask) != i) continue;
-         bond_tensor<FMT>(a, e, mj, nb_material(a, cq, i), T);
-         for (int r = 0; r < 9; ++r) Sji[r] += muj * T[r];
+         bond_tensor<R, FMT>(a, e, mj, nb_material(a, cq, i), T);
+         for (int r = 0; r < 9; ++r) Sji[r] += muj * (double)T[r];
       }
       double mx = 0.0, dv = 0.0;
       for (int r = 0; r < 3; ++r)
@@ -212,35 +220,35 @@ __global__ void adj_reciprocal_kernel(const LLGArgs<double> a, int* bad) {
             mx = fmax(mx, fabs(Sij[3 * r + s]));
             dv = fmax(dv, fabs(Sij[3 * r + s] - Sji[3 * s + r]));
          }
-      if (dv > 1e-10 * mx) {
+      if (dv > (sizeof(R) == 4 ? 1e-5 : 1e-10) * mx) {
          atomicCAS(bad, 0, 1 + i);
          return;
       }
    }
 }
 
-template <int FMT>
-__global__ void __launch_bounds__(256) adj_k1(const LLGArgs<double> a, AdjBufs b) {
+template <typename R, int FMT>
+__global__ void __launch_bounds__(256) adj_k1(const LLGArgs<R> a, AdjBufs<R> b) {
    asm volatile("griddepcontrol.wait;" ::: "memory");  // launched by launch_pdl
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    if (i >= b.n) return;
    const int st = b.stride;
    const int mi = a.mat ? a.mat[i] : 0;
-   const MatParams<double> m = a.mp[mi];
-   const double S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
-   double ex[3] = {0, 0, 0}, Ha[3];
-   exchange_gather<double, FMT>(a, i, mi, b.S, b.S + st, b.S + 2 * st, ex[0], ex[1], ex[2]);
-   aniso_d(a, m, S, Ha);
-   const double H[3] = {ex[0] + Ha[0] + a.hx, ex[1] + Ha[1] + a.hy, ex[2] + Ha[2] + a.hz};
-   double d[3];
-   llg_rhs<double>(m.A, m.B, S, H, d);
-   double v[3];
+   const MatParams<R> m = a.mp[mi];
+   const R S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
+   R ex[3] = {0, 0, 0}, Ha[3];
+   exchange_gather<R, FMT>(a, i, mi, b.S, b.S + st, b.S + 2 * st, ex[0], ex[1], ex[2]);
+   aniso_h(a, m, S, Ha);
+   const R H[3] = {ex[0] + Ha[0] + a.hx, ex[1] + Ha[1] + a.hy, ex[2] + Ha[2] + a.hz};
+   R d[3];
+   llg_rhs<R>(m.A, m.B, S, H, d);
+   R v[3];
    for (int k = 0; k < 3; ++k) {
       b.ex0[k * st + i] = ex[k];
       b.f0[k * st + i] = d[k];
       v[k] = S[k] + d[k] * a.dt;
    }
-   const double L = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+   const R L = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
    b.nv[i] = L;
    for (int k = 0; k < 3; ++k) b.sp[k * st + i] = v[k] / L;
 }
@@ -248,21 +256,31 @@ __global__ void __launch_bounds__(256) adj_k1(const LLGArgs<double> a, AdjBufs b
 // shared sums of the pair gradients: [1 + M*M] (M <= kAdjMaxPairMat)
 constexpr int kAdjMaxPairMat = 8;
 
-__device__ __forceinline__ void pair_init(double* sp, const AdjBufs& b, int M) {
+template <typename R>
+__device__ __forceinline__ void pair_init(double* sp, const AdjBufs<R>& b, int M) {
    if (b.gp)
       for (int k = threadIdx.x; k < 1 + M * M; k += blockDim.x) sp[k] = 0.0;
    __syncthreads();
 }
 
-__device__ __forceinline__ void pair_flush(const double* sp, const AdjBufs& b, int M) {
+template <typename R>
+__device__ __forceinline__ void pair_flush(const double* sp, const AdjBufs<R>& b, int M) {
    if (!b.gp) return;
    __syncthreads();
    for (int k = threadIdx.x; k < 1 + M * M; k += blockDim.x)
       if (sp[k] != 0.0) atomicAdd(b.gp + k, sp[k]);
 }
 
-template <int FMT>
-__global__ void __launch_bounds__(256) adj_k2(const LLGArgs<double> a, AdjBufs b) {
+// dL/dKu of one atom from its field adjoint hb at spin s (uniaxial term)
+template <typename R>
+__device__ __forceinline__ double ku_grad(const MatParams<R>& m, const R hb[3], const R s[3]) {
+   const double he = (double)(hb[0] * m.kux + hb[1] * m.kuy + hb[2] * m.kuz);
+   const double se = (double)(s[0] * m.kux + s[1] * m.kuy + s[2] * m.kuz);
+   return 2.0 * he * se / ((double)m.mu_s_muB * 9.27400915e-24);
+}
+
+template <typename R, int FMT>
+__global__ void __launch_bounds__(256) adj_k2(const LLGArgs<R> a, AdjBufs<R> b) {
    asm volatile("griddepcontrol.wait;" ::: "memory");  // launched by launch_pdl
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    const int st = b.stride;
@@ -271,45 +289,41 @@ __global__ void __launch_bounds__(256) adj_k2(const LLGArgs<double> a, AdjBufs b
    pair_init(sp, b, a.M);
    if (i < b.n) {
       const int mi = a.mat ? a.mat[i] : 0;
-      const MatParams<double> m = a.mp[mi];
-      const double S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
-      const double Sp[3] = {b.sp[i], b.sp[st + i], b.sp[2 * st + i]};
-      double ex[3] = {0, 0, 0}, Ha[3];
-      exchange_gather<double, FMT>(a, i, mi, b.sp, b.sp + st, b.sp + 2 * st, ex[0], ex[1], ex[2]);
-      aniso_d(a, m, Sp, Ha);
-      const double H1[3] = {ex[0] + Ha[0] + a.hx, ex[1] + Ha[1] + a.hy, ex[2] + Ha[2] + a.hz};
-      double f1[3], u[3];
-      llg_rhs<double>(m.A, m.B, Sp, H1, f1);
-      for (int k = 0; k < 3; ++k) u[k] = S[k] + 0.5 * a.dt * (b.f0[k * st + i] + f1[k]);
-      const double L = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-      const double s1[3] = {u[0] / L, u[1] / L, u[2] / L};
-      const double l[3] = {b.lam[i], b.lam[st + i], b.lam[2 * st + i]};
-      const double ls = l[0] * s1[0] + l[1] * s1[1] + l[2] * s1[2];
-      double u_b[3], a1[3], sdir[3], hb[3];
-      for (int k = 0; k < 3; ++k) { u_b[k] = (l[k] - ls * s1[k]) / L; a1[k] = 0.5 * a.dt * u_b[k]; }
-      f_vjp_d(m.A, m.B, Sp, H1, a1, sdir, hb);
-      const double imu = 1.0 / (double)m.mu_s_muB;  // Hbar / mu_s for the transposed gather
+      const MatParams<R> m = a.mp[mi];
+      const R S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
+      const R Sp[3] = {b.sp[i], b.sp[st + i], b.sp[2 * st + i]};
+      R ex[3] = {0, 0, 0}, Ha[3];
+      exchange_gather<R, FMT>(a, i, mi, b.sp, b.sp + st, b.sp + 2 * st, ex[0], ex[1], ex[2]);
+      aniso_h(a, m, Sp, Ha);
+      const R H1[3] = {ex[0] + Ha[0] + a.hx, ex[1] + Ha[1] + a.hy, ex[2] + Ha[2] + a.hz};
+      R f1[3], u[3];
+      llg_rhs<R>(m.A, m.B, Sp, H1, f1);
+      for (int k = 0; k < 3; ++k) u[k] = S[k] + (R)0.5 * a.dt * (b.f0[k * st + i] + f1[k]);
+      const R L = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+      const R s1[3] = {u[0] / L, u[1] / L, u[2] / L};
+      const R l[3] = {b.lam[i], b.lam[st + i], b.lam[2 * st + i]};
+      const R ls = l[0] * s1[0] + l[1] * s1[1] + l[2] * s1[2];
+      R u_b[3], a1[3], sdir[3], hb[3];
+      for (int k = 0; k < 3; ++k) { u_b[k] = (l[k] - ls * s1[k]) / L; a1[k] = (R)0.5 * a.dt * u_b[k]; }
+      f_vjp(m.A, m.B, Sp, H1, a1, sdir, hb);
+      const R imu = (R)1 / m.mu_s_muB;  // Hbar / mu_s for the transposed gather
       for (int k = 0; k < 3; ++k) {
          b.ub[k * st + i] = u_b[k];
          b.spb[k * st + i] = sdir[k];
          b.Hb1[k * st + i] = hb[k] * imu;
          b.ex1[k * st + i] = ex[k];
-         gv[0] += hb[k] * ex[k];
-         gv[2 + k] += hb[k];
+         gv[0] += (double)hb[k] * (double)ex[k];
+         gv[2 + k] += (double)hb[k];
       }
-      if (b.gp) pair_grads<FMT>(a, i, mi, b.sp, b.sp + st, b.sp + 2 * st, hb, sp);
-      if (a.uniaxial) {
-         const double he = hb[0] * m.kux + hb[1] * m.kuy + hb[2] * m.kuz;
-         const double se = Sp[0] * m.kux + Sp[1] * m.kuy + Sp[2] * m.kuz;
-         gv[1] += 2.0 * he * se / ((double)m.mu_s_muB * 9.27400915e-24);
-      }
+      if (b.gp) pair_grads<R, FMT>(a, i, mi, b.sp, b.sp + st, b.sp + 2 * st, hb, sp);
+      if (a.uniaxial) gv[1] += ku_grad(m, hb, Sp);
    }
    pair_flush(sp, b, a.M);
    grad_add(gv, b.g);
 }
 
-template <int FMT>
-__global__ void __launch_bounds__(256) adj_k3(const LLGArgs<double> a, AdjBufs b) {
+template <typename R, int FMT>
+__global__ void __launch_bounds__(256) adj_k3(const LLGArgs<R> a, AdjBufs<R> b) {
    asm volatile("griddepcontrol.wait;" ::: "memory");  // launched by launch_pdl
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    const int st = b.stride;
@@ -318,76 +332,73 @@ __global__ void __launch_bounds__(256) adj_k3(const LLGArgs<double> a, AdjBufs b
    pair_init(sp, b, a.M);
    if (i < b.n) {
       const int mi = a.mat ? a.mat[i] : 0;
-      const MatParams<double> m = a.mp[mi];
-      const double mu = (double)m.mu_s_muB;
-      const double S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
-      const double Sp[3] = {b.sp[i], b.sp[st + i], b.sp[2 * st + i]};
-      double t[3] = {0, 0, 0};
-      exchange_gather<double, FMT>(a, i, mi, b.Hb1, b.Hb1 + st, b.Hb1 + 2 * st, t[0], t[1], t[2]);
-      const double hb1[3] = {b.Hb1[i] * mu, b.Hb1[st + i] * mu, b.Hb1[2 * st + i] * mu};
-      double spbar[3];
+      const MatParams<R> m = a.mp[mi];
+      const R mu = m.mu_s_muB;
+      const R S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
+      const R Sp[3] = {b.sp[i], b.sp[st + i], b.sp[2 * st + i]};
+      R t[3] = {0, 0, 0};
+      exchange_gather<R, FMT>(a, i, mi, b.Hb1, b.Hb1 + st, b.Hb1 + 2 * st, t[0], t[1], t[2]);
+      const R hb1[3] = {b.Hb1[i] * mu, b.Hb1[st + i] * mu, b.Hb1[2 * st + i] * mu};
+      R spbar[3];
       for (int k = 0; k < 3; ++k) spbar[k] = b.spb[k * st + i] + t[k] * mu;
-      aniso_vjp_d(a, m, Sp, hb1, spbar);
-      const double sps = spbar[0] * Sp[0] + spbar[1] * Sp[1] + spbar[2] * Sp[2];
-      double vb[3], a0[3];
+      aniso_vjp(a, m, Sp, hb1, spbar);
+      const R sps = spbar[0] * Sp[0] + spbar[1] * Sp[1] + spbar[2] * Sp[2];
+      R vb[3], a0[3];
       for (int k = 0; k < 3; ++k) {
          vb[k] = (spbar[k] - sps * Sp[k]) / b.nv[i];
-         a0[k] = 0.5 * a.dt * b.ub[k * st + i] + a.dt * vb[k];
+         a0[k] = (R)0.5 * a.dt * b.ub[k * st + i] + a.dt * vb[k];
       }
-      double Ha[3];
-      aniso_d(a, m, S, Ha);
-      double H0[3], ex[3];
+      R Ha[3];
+      aniso_h(a, m, S, Ha);
+      R H0[3], ex[3];
       for (int k = 0; k < 3; ++k) {
          ex[k] = b.ex0[k * st + i];
          H0[k] = ex[k] + Ha[k] + (k == 0 ? a.hx : k == 1 ? a.hy : a.hz);
       }
-      double sdir[3], hb[3];
-      f_vjp_d(m.A, m.B, S, H0, a0, sdir, hb);
+      R sdir[3], hb[3];
+      f_vjp(m.A, m.B, S, H0, a0, sdir, hb);
       for (int k = 0; k < 3; ++k) {
          b.sb[k * st + i] = b.ub[k * st + i] + vb[k] + sdir[k];
          b.Hb0[k * st + i] = hb[k] / mu;
-         gv[0] += hb[k] * ex[k];
-         gv[2 + k] += hb[k];
+         gv[0] += (double)hb[k] * (double)ex[k];
+         gv[2 + k] += (double)hb[k];
       }
-      if (b.gp) pair_grads<FMT>(a, i, mi, b.S, b.S + st, b.S + 2 * st, hb, sp);
-      if (a.uniaxial) {
-         const double he = hb[0] * m.kux + hb[1] * m.kuy + hb[2] * m.kuz;
-         const double se = S[0] * m.kux + S[1] * m.kuy + S[2] * m.kuz;
-         gv[1] += 2.0 * he * se / ((double)m.mu_s_muB * 9.27400915e-24);
-      }
+      if (b.gp) pair_grads<R, FMT>(a, i, mi, b.S, b.S + st, b.S + 2 * st, hb, sp);
+      if (a.uniaxial) gv[1] += ku_grad(m, hb, S);
    }
    pair_flush(sp, b, a.M);
    grad_add(gv, b.g);
 }
 
-template <int FMT>
-__global__ void __launch_bounds__(256) adj_k4(const LLGArgs<double> a, AdjBufs b, int64_t t) {
+template <typename R, int FMT>
+__global__ void __launch_bounds__(256) adj_k4(const LLGArgs<R> a, AdjBufs<R> b, int64_t t) {
    asm volatile("griddepcontrol.wait;" ::: "memory");  // launched by launch_pdl
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    if (i >= b.n) return;
    const int st = b.stride;
    const int mi = a.mat ? a.mat[i] : 0;
-   const MatParams<double> m = a.mp[mi];
-   const double S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
-   const double mu = (double)m.mu_s_muB;
-   double tg[3] = {0, 0, 0};
-   exchange_gather<double, FMT>(a, i, mi, b.Hb0, b.Hb0 + st, b.Hb0 + 2 * st, tg[0], tg[1], tg[2]);
-   const double hb0[3] = {b.Hb0[i] * mu, b.Hb0[st + i] * mu, b.Hb0[2 * st + i] * mu};
-   double l[3];
+   const MatParams<R> m = a.mp[mi];
+   const R S[3] = {b.S[i], b.S[st + i], b.S[2 * st + i]};
+   const R mu = m.mu_s_muB;
+   R tg[3] = {0, 0, 0};
+   exchange_gather<R, FMT>(a, i, mi, b.Hb0, b.Hb0 + st, b.Hb0 + 2 * st, tg[0], tg[1], tg[2]);
+   const R hb0[3] = {b.Hb0[i] * mu, b.Hb0[st + i] * mu, b.Hb0[2 * st + i] * mu};
+   R l[3];
    for (int k = 0; k < 3; ++k) l[k] = b.sb[k * st + i] + tg[k] * mu;
-   aniso_vjp_d(a, m, S, hb0, l);
-   if (t >= 1) l[2] += 2.0 * b.w * (b.mz[t] - b.target[t - 1]) * (double)m.mu_s_muB / b.musum;
+   aniso_vjp(a, m, S, hb0, l);
+   if (t >= 1) l[2] += (R)(2.0 * b.w * (b.mz[t] - b.target[t - 1]) * (double)m.mu_s_muB / b.musum);
    for (int k = 0; k < 3; ++k) b.lam[k * st + i] = l[k];
 }
 
-__global__ void adj_lambda_init(const LLGArgs<double> a, AdjBufs b, int64_t N) {
+template <typename R>
+__global__ void adj_lambda_init(const LLGArgs<R> a, AdjBufs<R> b, int64_t N) {
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    if (i >= b.n) return;
    const int mi = a.mat ? a.mat[i] : 0;
    const int st = b.stride;
-   b.lam[i] = 0.0;
-   b.lam[st + i] = 0.0;
-   b.lam[2 * st + i] = 2.0 * b.w * (b.mz[N] - b.target[N - 1]) * (double)a.mp[mi].mu_s_muB / b.musum;
+   b.lam[i] = (R)0;
+   b.lam[st + i] = (R)0;
+   b.lam[2 * st + i] = (R)(2.0 * b.w * (b.mz[N] - b.target[N - 1]) * (double)a.mp[mi].mu_s_muB / b.musum);
 }
 
 // m_z after a step: block sums of mu s_z added into out[0]
@@ -409,36 +420,38 @@ __global__ void mz_kernel(int n, const R* __restrict__ sz, const int* __restrict
    }
 }
 
-template <int FMT>
-static void adj_step(const LLGArgs<double>& a, const AdjBufs& b, int64_t t, cudaStream_t st) {
+template <typename R, int FMT>
+static void adj_step(const LLGArgs<R>& a, const AdjBufs<R>& b, int64_t t, cudaStream_t st) {
    const int g = (b.n + 255) / 256;
    // consecutive small launches: programmatic serialisation hides their gaps
-   launch_pdl(adj_k1<FMT>, dim3(g), dim3(256), 0, st, a, b);
-   launch_pdl(adj_k2<FMT>, dim3(g), dim3(256), 0, st, a, b);
-   launch_pdl(adj_k3<FMT>, dim3(g), dim3(256), 0, st, a, b);
-   launch_pdl(adj_k4<FMT>, dim3(g), dim3(256), 0, st, a, b, t);
+   launch_pdl(adj_k1<R, FMT>, dim3(g), dim3(256), 0, st, a, b);
+   launch_pdl(adj_k2<R, FMT>, dim3(g), dim3(256), 0, st, a, b);
+   launch_pdl(adj_k3<R, FMT>, dim3(g), dim3(256), 0, st, a, b);
+   launch_pdl(adj_k4<R, FMT>, dim3(g), dim3(256), 0, st, a, b, t);
 }
 
-static void adj_step_fmt(int fmt, const LLGArgs<double>& a, const AdjBufs& b, int64_t t, cudaStream_t st) {
+template <typename R>
+static void adj_step_fmt(int fmt, const LLGArgs<R>& a, const AdjBufs<R>& b, int64_t t, cudaStream_t st) {
    switch (fmt) {
-      case FMT_ISO_TAB: adj_step<FMT_ISO_TAB>(a, b, t, st); break;
-      case FMT_ISO_BOND: adj_step<FMT_ISO_BOND>(a, b, t, st); break;
-      case FMT_VEC_TAB: adj_step<FMT_VEC_TAB>(a, b, t, st); break;
-      case FMT_VEC_BOND: adj_step<FMT_VEC_BOND>(a, b, t, st); break;
-      case FMT_DMI_TAB: adj_step<FMT_DMI_TAB>(a, b, t, st); break;
-      default: adj_step<FMT_TENSOR_BOND>(a, b, t, st); break;
+      case FMT_ISO_TAB: adj_step<R, FMT_ISO_TAB>(a, b, t, st); break;
+      case FMT_ISO_BOND: adj_step<R, FMT_ISO_BOND>(a, b, t, st); break;
+      case FMT_VEC_TAB: adj_step<R, FMT_VEC_TAB>(a, b, t, st); break;
+      case FMT_VEC_BOND: adj_step<R, FMT_VEC_BOND>(a, b, t, st); break;
+      case FMT_DMI_TAB: adj_step<R, FMT_DMI_TAB>(a, b, t, st); break;
+      default: adj_step<R, FMT_TENSOR_BOND>(a, b, t, st); break;
    }
 }
 
-static cudaError_t launch_reciprocal(int fmt, const LLGArgs<double>& a, int* bad, cudaStream_t st) {
+template <typename R>
+static cudaError_t launch_reciprocal(int fmt, const LLGArgs<R>& a, int* bad, cudaStream_t st) {
    const int g = (a.n + 127) / 128;
    switch (fmt) {
-      case FMT_ISO_TAB: adj_reciprocal_kernel<FMT_ISO_TAB><<<g, 128, 0, st>>>(a, bad); break;
-      case FMT_ISO_BOND: adj_reciprocal_kernel<FMT_ISO_BOND><<<g, 128, 0, st>>>(a, bad); break;
-      case FMT_VEC_TAB: adj_reciprocal_kernel<FMT_VEC_TAB><<<g, 128, 0, st>>>(a, bad); break;
-      case FMT_VEC_BOND: adj_reciprocal_kernel<FMT_VEC_BOND><<<g, 128, 0, st>>>(a, bad); break;
-      case FMT_DMI_TAB: adj_reciprocal_kernel<FMT_DMI_TAB><<<g, 128, 0, st>>>(a, bad); break;
-      default: adj_reciprocal_kernel<FMT_TENSOR_BOND><<<g, 128, 0, st>>>(a, bad); break;
+      case FMT_ISO_TAB: adj_reciprocal_kernel<R, FMT_ISO_TAB><<<g, 128, 0, st>>>(a, bad); break;
+      case FMT_ISO_BOND: adj_reciprocal_kernel<R, FMT_ISO_BOND><<<g, 128, 0, st>>>(a, bad); break;
+      case FMT_VEC_TAB: adj_reciprocal_kernel<R, FMT_VEC_TAB><<<g, 128, 0, st>>>(a, bad); break;
+      case FMT_VEC_BOND: adj_reciprocal_kernel<R, FMT_VEC_BOND><<<g, 128, 0, st>>>(a, bad); break;
+      case FMT_DMI_TAB: adj_reciprocal_kernel<R, FMT_DMI_TAB><<<g, 128, 0, st>>>(a, bad); break;
+      default: adj_reciprocal_kernel<R, FMT_TENSOR_BOND><<<g, 128, 0, st>>>(a, bad); break;
    }
    return cudaGetLastError();
 }
@@ -449,20 +462,23 @@ using namespace vgpu;
 
 namespace {
 
+template <typename T>
 struct DevVec {
-   double* p = nullptr;
+   T* p = nullptr;
    ~DevVec() { if (p) cudaFree(p); }
-   cudaError_t alloc(size_t n) { return cudaMalloc(&p, sizeof(double) * std::max<size_t>(n, 1)); }
+   cudaError_t alloc(size_t n) { return cudaMalloc(&p, sizeof(T) * std::max<size_t>(n, 1)); }
 };
 
-// one FP64 Heun step of the state in `x` (3 * stride doubles, x|y|z)
-int forward_step(vgpu_ctx* h, LLGArgs<double> a, double* x, double* pb, double* eb, int stride) {
+// one Heun step (the ordinary passes, no thermal term) of the state in `x`
+// (3 * stride values, x|y|z), the predictor increment stored
+template <typename R>
+int forward_step(vgpu_ctx* h, LLGArgs<R> a, R* x, R* pb, R* eb, int stride) {
    a.ax = x; a.ay = x + stride; a.az = x + 2 * stride;
    a.bx = pb; a.by = pb + stride; a.bz = pb + 2 * stride;
    a.ex = eb; a.ey = eb + stride; a.ez = eb + 2 * stride;
    a.thermal = 0;
-   cudaError_t e = launch_llg_pass<double>(a, h->sys.fmt, PASS_PREDICTOR, h->sys.nslices, h->stream);
-   if (e == cudaSuccess) e = launch_llg_pass<double>(a, h->sys.fmt, PASS_CORRECTOR, h->sys.nslices, h->stream);
+   cudaError_t e = launch_llg_pass<R>(a, h->sys.fmt, PASS_PREDICTOR, h->sys.nslices, h->stream);
+   if (e == cudaSuccess) e = launch_llg_pass<R>(a, h->sys.fmt, PASS_CORRECTOR, h->sys.nslices, h->stream);
    h->kernel_launches += 2;
    return cuda_err(h, e, "adjoint forward");
 }
@@ -470,7 +486,6 @@ int forward_step(vgpu_ctx* h, LLGArgs<double> a, double* x, double* pb, double* 
 int check_adjoint_ok(vgpu_ctx* h) {
    if (!h) return set_err(nullptr, VGPU_ERR_ARG, "null handle");
    if (!h->sys.uploaded) return set_err(h, VGPU_ERR_STATE, "no system uploaded");
-   if (h->prec != VGPU_PREC_FP64) return set_err(h, VGPU_ERR_ARG, "the adjoint runs in the FP64 build (VGPU_PREC_FP64)");
    if (h->sys.cell || h->sys.hd_atom || h->sys.sys_off)
       return set_err(h, VGPU_ERR_ARG, "the adjoint does not support dipole fields or batches");
    if (h->params.local_applied_field) return set_err(h, VGPU_ERR_ARG, "the adjoint supports the global applied field only");
@@ -486,27 +501,24 @@ double moment_sum(vgpu_ctx* h) {
    return s;
 }
 
-}  // namespace
-
-extern "C" int vgpu_mz_trajectory(vgpu_handle h, uint64_t n_steps, double* mz_out) {
-   int rc = check_adjoint_ok(h);
-   if (rc) return rc;
-   cudaSetDevice(h->device);
+template <typename R>
+int mz_trajectory_typed(vgpu_handle h, uint64_t n_steps, double* mz_out) {
    SysDev& S = h->sys;
    const int st = S.n_alloc;
-   DevVec cur, pb, eb, mz;
+   DevVec<R> cur, pb, eb;
+   DevVec<double> mz;
    cudaError_t e;
    if ((e = cur.alloc(3 * (size_t)st)) || (e = pb.alloc(3 * (size_t)st)) || (e = eb.alloc(3 * (size_t)st)) ||
        (e = mz.alloc(n_steps + 1)))
       return cuda_err(h, e, "trajectory buffers");
    for (int q = 0; q < 3; ++q)
-      cudaMemcpyAsync(cur.p + (size_t)q * st, S.s[q], sizeof(double) * st, cudaMemcpyDeviceToDevice, h->stream);
+      cudaMemcpyAsync(cur.p + (size_t)q * st, S.s[q], sizeof(R) * st, cudaMemcpyDeviceToDevice, h->stream);
    cudaMemsetAsync(mz.p, 0, sizeof(double) * (n_steps + 1), h->stream);
-   LLGArgs<double> a = make_args<double>(h);
+   LLGArgs<R> a = make_args<R>(h);
    for (uint64_t t = 0; t < n_steps; ++t) {
-      if ((rc = forward_step(h, a, cur.p, pb.p, eb.p, st))) return rc;
-      launch_pdl(mz_kernel<double>, dim3((S.n + 255) / 256), dim3(256), 0, h->stream, (int)S.n,
-                 (const double*)(cur.p + 2 * (size_t)st), (const int*)S.mat, (const MatParams<double>*)S.mp,
+      if (int rc = forward_step<R>(h, a, cur.p, pb.p, eb.p, st)) return rc;
+      launch_pdl(mz_kernel<R>, dim3((S.n + 255) / 256), dim3(256), 0, h->stream, (int)S.n,
+                 (const R*)(cur.p + 2 * (size_t)st), (const int*)S.mat, (const MatParams<R>*)S.mp,
                  (double*)(mz.p + t + 1));
    }
    std::vector<double> host(n_steps + 1);
@@ -519,13 +531,14 @@ extern "C" int vgpu_mz_trajectory(vgpu_handle h, uint64_t n_steps, double* mz_ou
 }
 
 // the couplings must be reciprocal in SI units for the transposed gather
-static int check_reciprocal(vgpu_ctx* h) {
+template <typename R>
+int check_reciprocal(vgpu_ctx* h) {
    int* bad = nullptr;
    cudaError_t e = cudaMalloc(&bad, sizeof(int));
    if (e != cudaSuccess) return cuda_err(h, e, "adjoint check");
    int hb = 0;
    e = cudaMemsetAsync(bad, 0, sizeof(int), h->stream);
-   if (e == cudaSuccess) e = launch_reciprocal(h->sys.fmt, make_args<double>(h), bad, h->stream);
+   if (e == cudaSuccess) e = launch_reciprocal<R>(h->sys.fmt, make_args<R>(h), bad, h->stream);
    if (e == cudaSuccess) e = cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
    cudaFree(bad);
@@ -537,16 +550,12 @@ static int check_reciprocal(vgpu_ctx* h) {
    return VGPU_OK;
 }
 
-static int adjoint_run(vgpu_handle h, uint64_t n_steps, const double* target, double w, int32_t every,
-                       double* loss_out, double* grad_out, double* pair_out) {
-   int rc = check_adjoint_ok(h);
-   if (rc) return rc;
-   if (!target || !loss_out || !grad_out || n_steps == 0) return set_err(h, VGPU_ERR_ARG, "bad adjoint arguments");
-   cudaSetDevice(h->device);
-   if ((rc = check_reciprocal(h))) return rc;
+template <typename R>
+int adjoint_typed(vgpu_handle h, uint64_t n_steps, const double* target, double w, int32_t every, double* loss_out,
+                  double* grad_out, double* pair_out) {
+   int rc;
+   if ((rc = check_reciprocal<R>(h))) return rc;
    const int M = h->sys.M;
-   if (pair_out && M > kAdjMaxPairMat)
-      return set_err(h, VGPU_ERR_ARG, "per-material gradients support at most %d materials", kAdjMaxPairMat);
    SysDev& S = h->sys;
    const int n = S.n, st = S.n_alloc;
    const int64_t N = (int64_t)n_steps;
@@ -554,7 +563,8 @@ static int adjoint_run(vgpu_handle h, uint64_t n_steps, const double* target, do
    const int64_t ncp = (N + C - 1) / C;
    const size_t v3 = 3 * (size_t)st;
    const int np = 1 + M * M;
-   DevVec cp, seg, pb, eb, mz, tg, g, work;
+   DevVec<R> cp, seg, pb, eb, work;
+   DevVec<double> mz, tg, g;
    cudaError_t e;
    if ((e = cp.alloc(v3 * ncp)) || (e = seg.alloc(v3 * (C + 1))) || (e = pb.alloc(v3)) || (e = eb.alloc(v3)) ||
        (e = mz.alloc(N + 1)) || (e = tg.alloc(N)) || (e = g.alloc(5 + np)) || (e = work.alloc(v3 * 10 + st)))
@@ -562,18 +572,17 @@ static int adjoint_run(vgpu_handle h, uint64_t n_steps, const double* target, do
    cudaMemcpyAsync(tg.p, target, sizeof(double) * N, cudaMemcpyHostToDevice, h->stream);
    cudaMemsetAsync(mz.p, 0, sizeof(double) * (N + 1), h->stream);
    cudaMemsetAsync(g.p, 0, sizeof(double) * (5 + np), h->stream);
-   LLGArgs<double> a = make_args<double>(h);
+   LLGArgs<R> a = make_args<R>(h);
    a.thermal = 0;
    // forward from the current spins (left untouched), checkpoint every C steps
-   double* cur = seg.p;  // first slot doubles as the running state
+   R* cur = seg.p;  // first slot doubles as the running state
    for (int q = 0; q < 3; ++q)
-      cudaMemcpyAsync(cur + (size_t)q * st, S.s[q], sizeof(double) * st, cudaMemcpyDeviceToDevice, h->stream);
+      cudaMemcpyAsync(cur + (size_t)q * st, S.s[q], sizeof(R) * st, cudaMemcpyDeviceToDevice, h->stream);
    for (int64_t t = 0; t < N; ++t) {
-      if (t % C == 0)
-         cudaMemcpyAsync(cp.p + v3 * (t / C), cur, sizeof(double) * v3, cudaMemcpyDeviceToDevice, h->stream);
-      if ((rc = forward_step(h, a, cur, pb.p, eb.p, st))) return rc;
-      launch_pdl(mz_kernel<double>, dim3((n + 255) / 256), dim3(256), 0, h->stream, (int)n,
-                 (const double*)(cur + 2 * (size_t)st), (const int*)S.mat, (const MatParams<double>*)S.mp,
+      if (t % C == 0) cudaMemcpyAsync(cp.p + v3 * (t / C), cur, sizeof(R) * v3, cudaMemcpyDeviceToDevice, h->stream);
+      if ((rc = forward_step<R>(h, a, cur, pb.p, eb.p, st))) return rc;
+      launch_pdl(mz_kernel<R>, dim3((n + 255) / 256), dim3(256), 0, h->stream, (int)n,
+                 (const R*)(cur + 2 * (size_t)st), (const int*)S.mat, (const MatParams<R>*)S.mp,
                  (double*)(mz.p + t + 1));
    }
    // loss on the host from m_z(t)
@@ -590,26 +599,26 @@ static int adjoint_run(vgpu_handle h, uint64_t n_steps, const double* target, do
       const double r = mzh[t] - target[t - 1];
       loss += w * r * r;
    }
-   AdjBufs b;
+   AdjBufs<R> b;
    std::memset(&b, 0, sizeof b);
-   double* wk = work.p;
+   R* wk = work.p;
    b.sp = wk; b.ex0 = wk + v3; b.ex1 = wk + 2 * v3; b.f0 = wk + 3 * v3; b.ub = wk + 4 * v3;
    b.spb = wk + 5 * v3; b.sb = wk + 6 * v3; b.Hb0 = wk + 7 * v3; b.Hb1 = wk + 8 * v3; b.lam = wk + 9 * v3;
    b.nv = wk + 10 * v3;
    b.g = g.p; b.mz = mz.p; b.target = tg.p; b.w = w; b.musum = musum; b.n = n; b.stride = st;
    b.gp = pair_out ? g.p + 5 : nullptr;
-   adj_lambda_init<<<(n + 255) / 256, 256, 0, h->stream>>>(a, b, N);
+   adj_lambda_init<R><<<(n + 255) / 256, 256, 0, h->stream>>>(a, b, N);
    for (int64_t c = ncp - 1; c >= 0; --c) {
       const int64_t t0 = c * C, t1 = std::min(t0 + C, N);
-      cudaMemcpyAsync(seg.p, cp.p + v3 * c, sizeof(double) * v3, cudaMemcpyDeviceToDevice, h->stream);
+      cudaMemcpyAsync(seg.p, cp.p + v3 * c, sizeof(R) * v3, cudaMemcpyDeviceToDevice, h->stream);
       for (int64_t t = t0; t < t1 - 1; ++t) {
-         double* nxt = seg.p + v3 * (t - t0 + 1);
-         cudaMemcpyAsync(nxt, seg.p + v3 * (t - t0), sizeof(double) * v3, cudaMemcpyDeviceToDevice, h->stream);
-         if ((rc = forward_step(h, a, nxt, pb.p, eb.p, st))) return rc;
+         R* nxt = seg.p + v3 * (t - t0 + 1);
+         cudaMemcpyAsync(nxt, seg.p + v3 * (t - t0), sizeof(R) * v3, cudaMemcpyDeviceToDevice, h->stream);
+         if ((rc = forward_step<R>(h, a, nxt, pb.p, eb.p, st))) return rc;
       }
       for (int64_t t = t1 - 1; t >= t0; --t) {
          b.S = seg.p + v3 * (t - t0);
-         adj_step_fmt(S.fmt, a, b, t, h->stream);
+         adj_step_fmt<R>(S.fmt, a, b, t, h->stream);
          h->kernel_launches += 4;
       }
       if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(h, e, "adjoint backward");
@@ -623,6 +632,29 @@ static int adjoint_run(vgpu_handle h, uint64_t n_steps, const double* target, do
    if (pair_out)
       for (int k = 0; k < np; ++k) pair_out[k] = gh[5 + k];
    return VGPU_OK;
+}
+
+}  // namespace
+
+extern "C" int vgpu_mz_trajectory(vgpu_handle h, uint64_t n_steps, double* mz_out) {
+   int rc = check_adjoint_ok(h);
+   if (rc) return rc;
+   cudaSetDevice(h->device);
+   return h->prec == VGPU_PREC_FP64 ? mz_trajectory_typed<double>(h, n_steps, mz_out)
+                                    : mz_trajectory_typed<float>(h, n_steps, mz_out);
+}
+
+static int adjoint_run(vgpu_handle h, uint64_t n_steps, const double* target, double w, int32_t every,
+                       double* loss_out, double* grad_out, double* pair_out) {
+   int rc = check_adjoint_ok(h);
+   if (rc) return rc;
+   if (!target || !loss_out || !grad_out || n_steps == 0) return set_err(h, VGPU_ERR_ARG, "bad adjoint arguments");
+   cudaSetDevice(h->device);
+   if (pair_out && h->sys.M > kAdjMaxPairMat)
+      return set_err(h, VGPU_ERR_ARG, "per-material gradients support at most %d materials", kAdjMaxPairMat);
+   return h->prec == VGPU_PREC_FP64
+              ? adjoint_typed<double>(h, n_steps, target, w, every, loss_out, grad_out, pair_out)
+              : adjoint_typed<float>(h, n_steps, target, w, every, loss_out, grad_out, pair_out);
 }
 
 extern "C" int vgpu_adjoint_llg(vgpu_handle h, uint64_t n_steps, const double* target, double w, int32_t every,
