@@ -6,7 +6,7 @@
 * statistical: 24 independent GPU checkerboard chains reproduce the
   reference's sequential random-site Metropolis m(T) on SC 16^3 and on the
   SC 50^3 Curie workload itself (fixtures produced by the reference's own
-  montecarlo::mc_step): every temperature within 4 combined standard errors,
+  montecarlo::mc_step): every temperature within 3 combined standard errors,
   the mean of z^2 over the 30 finite temperatures at most 2, Tc within 1 %.
 """
 import numpy as np
@@ -110,10 +110,9 @@ def _gpu_chains(base, Ts, eq, av, every, seeds):
 def _compare_curves(Ts, g, ref, rse, label):
     """GPU chains g (chains x T) against the reference mean and standard
     error per temperature.  The GPU's standard error is the spread of its
-    chain means.  With 30 temperatures compared at once and the reference's
-    error itself estimated from a finite run, the bar is: every temperature
-    within 4 combined standard errors (two-sided p = 6e-5 each, 2e-3 over 30),
-    the mean of z^2 at most 2 (1 expected), and Tc within 1 %."""
+    chain means.  The bar: every temperature within 3 combined standard
+    errors, the mean of z^2 over the temperatures at most 2 (1 expected), and
+    Tc within 1 %."""
     got, se = g.mean(0), g.std(0, ddof=1) / np.sqrt(g.shape[0])
     var = se ** 2 + rse ** 2
     live = var > 1e-14                                # T = 0: both frozen at |m| = 1
@@ -124,7 +123,7 @@ def _compare_curves(Ts, g, ref, rse, label):
     print(label, "se_ref", np.round(rse, 5))
     print(label, "z", np.round(z, 2), "mean z^2", round(float(np.mean(z ** 2)), 3))
     assert np.all(np.abs(got - ref)[~live] < 1e-6)
-    assert np.all(z <= 4.0), z
+    assert np.all(z <= 3.0), z
     assert np.mean(z ** 2) <= 2.0
     tc_g, tc_r = _tc_fit(Ts, got), _tc_fit(Ts, ref)
     print(f"{label} Tc gpu {tc_g:.1f} K, reference {tc_r:.1f} K")
@@ -155,10 +154,12 @@ def test_config1_curie_sweep_matches_reference_statistically(vgpu_lib):
     0..1500 K, 5,000 equilibration + 10,000 averaging sweeps, <|m|> sampled
     every 10 sweeps, against the reference's own sequential random-site
     Metropolis on the same protocol (tests/golden/mc_sc50_curie.npz: one
-    reference process per temperature and chain, the chains differing in the
+    reference process per temperature and chain, four chains differing in the
     reference's integrator seed; a chain's standard error from its integrated
-    autocorrelation time, the chains' combined).  The GPU runs 24 independent
-    checkerboard chains per temperature (eight handles of 3 x 31 replicas)."""
+    autocorrelation time, scaled by kappa = 1.6 so that it accounts for the
+    spread of the chain means, the chains' combined).  The GPU runs 24
+    independent checkerboard chains per temperature (eight handles of 3 x 31
+    replicas)."""
     from vampire_b200 import system as S
     d = dict(np.load(GOLDEN / "mc_sc50_curie.npz"))
     Ts = d["T"]
