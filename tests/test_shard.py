@@ -397,3 +397,15 @@ def test_gloo_sharded_cell_moments_equal_whole_system(tmp_path, world):
         B, H = D.cell_fields(mag, T, c["cell_natoms"], c["cell_volume"])
         assert np.abs(B - B0).max() <= 1e-13 * np.abs(B0).max()
         assert np.abs(H - H0).max() <= 1e-13 * np.abs(H0).max()
+
+
+def test_cell_moment_sum_without_process_group_is_the_single_shard():
+    """One shard and no process group (a single-GPU run of the sharded
+    path): the partial cell moments are already the whole system's."""
+    import torch
+    import torch.distributed as dist
+    from vampire_b200 import shard as SH
+    assert not dist.is_initialized()
+    buf = torch.arange(6, dtype=torch.float64)
+    SH.sum_cell_moments(buf)
+    assert torch.equal(buf, torch.arange(6, dtype=torch.float64))

@@ -285,8 +285,11 @@ def local_colours(colour: np.ndarray, plan: ShardPlan) -> np.ndarray:
 def sum_cell_moments(buf, group=None) -> None:
     """Adds a shard's partial cell moments (a tensor of 3*ncells FP64, the
     owned atoms' sums) over all ranks in place: CPU tensors over gloo, the
-    library's device buffer over NCCL."""
+    library's device buffer over NCCL.  Without a process group there is one
+    shard, whose sums are already the whole system's."""
     import torch.distributed as dist
+    if group is None and not (dist.is_available() and dist.is_initialized()):
+        return
     dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=group)
 
 
