@@ -486,7 +486,8 @@ static int dipole_build(vgpu_ctx* h, const vgpu_dipole_desc* dd, int ng, const i
    if (h->dipole_fft != 0) {
       cudaError_t fe = cudaSuccess;
       std::string why;
-      d->fft = fft_field_create(nc, dd->cell_pos_mom, dd->cell_natoms, dd->macro_cell_size, h->stream, &fe, &why);
+      d->fft = fft_field_create(nc, dd->cell_pos_mom, dd->cell_natoms, dd->macro_cell_size, h->prec == VGPU_PREC_FP32,
+                                h->stream, &fe, &why);
       if (fe != cudaSuccess) {
          int rc = cuda_err(h, fe, "dipole FFT setup");
          dipole_destroy(h);

@@ -27,11 +27,14 @@
 // grid (P = 128) this is about half of the line transforms of full passes,
 // the spectra never leave shared memory, and the grid needs no clearing.
 //
-// Everything is FP64, so the result equals the direct FP64 sum to rounding
-// (~1e-15 of the field) instead of the FP32 terms of the all-pairs kernel, and
-// costs O(P^3 log P) instead of O(Nc^2): at 125,000 cells (a 50^3 grid, P = 128)
-// a few hundred microseconds instead of tens of milliseconds.  Twiddle
-// factors are tabulated on the host in double precision.
+// Precision follows the handle: in the FP64 build every step is FP64, so the
+// result equals the direct FP64 sum to rounding (~1e-15 of the field); the
+// FP32 production handles transform FP32 grids (the tensor spectra computed
+// in FP64 once and rounded, twiddles rounded from FP64, moments and fields
+// FP64 at the ends), about 1e-6 of the field.  Cost O(P^3 log P) instead of
+// O(Nc^2): at 125,000 cells (a 50^3 grid, P = 128) a few hundred microseconds
+// instead of tens of milliseconds.  Twiddle factors are tabulated on the host
+// in double precision.
 #include "dipole_fft.cuh"
 
 #include <cuda_runtime.h>
@@ -51,6 +54,10 @@ struct FFTField {
    double2* tspec = nullptr;   // [6][np] spectra of Txx, Txy, Txz, Tyy, Tyz, Tzz
    double2* grid = nullptr;    // [3][np] moment grids, transformed in place
    double2* tw[3] = {nullptr, nullptr, nullptr};  // [p/2] exp(-2 pi i k / p) per axis
+   bool fp32 = false;          // FP32 transforms (the buffers below) instead of the FP64 ones
+   float2* tspec32 = nullptr;  // [6][np] the spectra rounded to FP32
+   float2* grid32 = nullptr;   // [3][np]
+   float2* tw32[3] = {nullptr, nullptr, nullptr};
    int* cell_lin = nullptr;    // [nc] linear grid index, or -1 (empty cell)
    int* box_cell = nullptr;    // [gx*gy*gz] cell at each box point (x fastest), or -1
 };
@@ -63,10 +70,20 @@ constexpr int kFFTTile = 2048;  // complex points per block tile (32 KB of share
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// complex value of the transform's precision
+template <typename C> __device__ __forceinline__ C cval(double x, double y);
+template <> __device__ __forceinline__ double2 cval<double2>(double x, double y) { return make_double2(x, y); }
+template <> __device__ __forceinline__ float2 cval<float2>(double x, double y) {
+   return make_float2((float)x, (float)y);
+}
 
 // radix-2 decimation-in-time butterflies over `nlines` lines of n points held
 // in shared memory in bit-reversed order (line-major); results in natural order
-__device__ void fft_smem(double2* s, int n, int nlines, const double2* __restrict__ tw, bool inverse) {
+template <typename C>
+__device__ void fft_smem(C* s, int n, int nlines, const C* __restrict__ tw, bool inverse) {
    const int half = n >> 1;
    for (int h = 1; h < n; h <<= 1) {
       const int step = half / h;  // twiddle stride: exp(-2 pi i j / (2h)) = tw[j * n / (2h)]
@@ -74,12 +91,12 @@ __device__ void fft_smem(double2* s, int n, int nlines, const double2* __restric
          const int line = b / half, k = b - line * half;
          const int j = k % h, grp = k / h;
          const int i0 = line * n + grp * 2 * h + j, i1 = i0 + h;
-         double2 w = tw[j * step];
+         C w = tw[j * step];
          if (inverse) w.y = -w.y;
-         const double2 u = s[i0];
-         const double2 v = cmul(w, s[i1]);
-         s[i0] = make_double2(u.x + v.x, u.y + v.y);
-         s[i1] = make_double2(u.x - v.x, u.y - v.y);
+         const C u = s[i0];
+         const C v = cmul(w, s[i1]);
+         s[i0] = {u.x + v.x, u.y + v.y};
+         s[i1] = {u.x - v.x, u.y - v.y};
       }
       __syncthreads();
    }
@@ -88,11 +105,12 @@ __device__ void fft_smem(double2* s, int n, int nlines, const double2* __restric
 // lines along x (contiguous): block = `lines` lines of one grid, line r of
 // the nrows transformed being the x line (y, z) = (r % rpp, r / rpp) at
 // (z * py + y) * n; points p >= ld read as zero, points p < st are stored
-__global__ void __launch_bounds__(kFFTThreads) fft_x_kernel(double2* __restrict__ data, size_t np, int n, int logn,
-                                                            int lines, const double2* __restrict__ tw, int inverse,
+template <typename C>
+__global__ void __launch_bounds__(kFFTThreads) fft_x_kernel(C* __restrict__ data, size_t np, int n, int logn,
+                                                            int lines, const C* __restrict__ tw, int inverse,
                                                             int nrows, int rpp, int py, int ld, int st) {
-   __shared__ double2 s[kFFTTile];
-   double2* grid = data + (size_t)blockIdx.y * np;
+   __shared__ C s[kFFTTile];
+   C* grid = data + (size_t)blockIdx.y * np;
    const int r0 = blockIdx.x * lines;
    const int tot = lines * n;
    auto row = [&](int r) { return ((size_t)(r / rpp) * py + (size_t)(r % rpp)) * n; };
@@ -100,7 +118,7 @@ __global__ void __launch_bounds__(kFFTThreads) fft_x_kernel(double2* __restrict_
       const int line = e / n, p = e - line * n;
       const int r = r0 + line;
       s[line * n + (int)(__brev((unsigned)p) >> (32 - logn))] =
-          r < nrows && p < ld ? grid[row(r) + p] : make_double2(0.0, 0.0);
+          r < nrows && p < ld ? grid[row(r) + p] : cval<C>(0.0, 0.0);
    }
    __syncthreads();
    fft_smem(s, n, lines, tw, inverse != 0);
@@ -114,17 +132,18 @@ __global__ void __launch_bounds__(kFFTThreads) fft_x_kernel(double2* __restrict_
 // lines along y or z: block = W adjacent x columns of one (other) index;
 // point p of column w sits at base + p * stride + w; points p >= ld read as
 // zero, points p < st are stored
-__global__ void __launch_bounds__(kFFTThreads) fft_strided_kernel(double2* __restrict__ data, size_t np, int n,
-                                                                  int logn, int W, size_t stride,
-                                                                  size_t other_stride, const double2* __restrict__ tw,
-                                                                  int inverse, int ld, int st) {
-   __shared__ double2 s[kFFTTile];
-   double2* base = data + (size_t)blockIdx.z * np + (size_t)blockIdx.y * other_stride + (size_t)blockIdx.x * W;
+template <typename C>
+__global__ void __launch_bounds__(kFFTThreads) fft_strided_kernel(C* __restrict__ data, size_t np, int n, int logn,
+                                                                  int W, size_t stride, size_t other_stride,
+                                                                  const C* __restrict__ tw, int inverse, int ld,
+                                                                  int st) {
+   __shared__ C s[kFFTTile];
+   C* base = data + (size_t)blockIdx.z * np + (size_t)blockIdx.y * other_stride + (size_t)blockIdx.x * W;
    const int tot = W * n;
    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
       const int p = e / W, w = e - p * W;
       s[w * n + (int)(__brev((unsigned)p) >> (32 - logn))] =
-          p < ld ? base[(size_t)p * stride + w] : make_double2(0.0, 0.0);
+          p < ld ? base[(size_t)p * stride + w] : cval<C>(0.0, 0.0);
    }
    __syncthreads();
    fft_smem(s, n, W, tw, inverse != 0);
@@ -142,12 +161,12 @@ __global__ void __launch_bounds__(kFFTThreads) fft_strided_kernel(double2* __res
 // spectra to memory and reading them back.
 constexpr int kFuseTile = 3072;  // complex points per block: 3 components x W x pz (48 KB)
 
-__device__ __forceinline__ void tensor_times(const double2* __restrict__ t, size_t np, size_t q, double2 mx,
-                                             double2 my, double2 mz, double2 h[3]) {
-   const double2 xx = t[q], xy = t[np + q], xz = t[2 * np + q];
-   const double2 yy = t[3 * np + q], yz = t[4 * np + q], zz = t[5 * np + q];
-   double2 hx = cmul(xx, mx), hy = cmul(xy, mx), hz = cmul(xz, mx);
-   double2 a = cmul(xy, my), b = cmul(xz, mz);
+template <typename C>
+__device__ __forceinline__ void tensor_times(const C* __restrict__ t, size_t np, size_t q, C mx, C my, C mz, C h[3]) {
+   const C xx = t[q], xy = t[np + q], xz = t[2 * np + q];
+   const C yy = t[3 * np + q], yz = t[4 * np + q], zz = t[5 * np + q];
+   C hx = cmul(xx, mx), hy = cmul(xy, mx), hz = cmul(xz, mx);
+   C a = cmul(xy, my), b = cmul(xz, mz);
    hx.x += a.x + b.x; hx.y += a.y + b.y;
    a = cmul(yy, my); b = cmul(yz, mz);
    hy.x += a.x + b.x; hy.y += a.y + b.y;
@@ -156,11 +175,11 @@ __device__ __forceinline__ void tensor_times(const double2* __restrict__ t, size
    h[0] = hx; h[1] = hy; h[2] = hz;
 }
 
-__global__ void __launch_bounds__(kFFTThreads) fft_z_multiply_kernel(double2* __restrict__ data,
-                                                                     const double2* __restrict__ t, size_t np, int px,
-                                                                     int py, int n, int logn, int W, int gz,
-                                                                     const double2* __restrict__ tw) {
-   __shared__ double2 s[kFuseTile];
+template <typename C>
+__global__ void __launch_bounds__(kFFTThreads) fft_z_multiply_kernel(C* __restrict__ data, const C* __restrict__ t,
+                                                                     size_t np, int px, int py, int n, int logn, int W,
+                                                                     int gz, const C* __restrict__ tw) {
+   __shared__ C s[kFuseTile];
    const size_t stride = (size_t)px * py;
    const size_t col0 = (size_t)blockIdx.y * px + (size_t)blockIdx.x * W;  // (x0, y) in the z = 0 plane
    const int tot = W * n;
@@ -168,14 +187,14 @@ __global__ void __launch_bounds__(kFFTThreads) fft_z_multiply_kernel(double2* __
       const int c = e / tot, r = e - c * tot;
       const int p = r / W, w = r - p * W;
       s[(c * W + w) * n + (int)(__brev((unsigned)p) >> (32 - logn))] =
-          p < gz ? data[(size_t)c * np + col0 + (size_t)p * stride + w] : make_double2(0.0, 0.0);
+          p < gz ? data[(size_t)c * np + col0 + (size_t)p * stride + w] : cval<C>(0.0, 0.0);
    }
    __syncthreads();
    fft_smem(s, n, 3 * W, tw, false);
    // H = T M at every (w, k), all read before any is written back at its
    // bit-reversed position for the inverse
    constexpr int kMaxPer = kFuseTile / 3 / kFFTThreads;  // points per thread
-   double2 h[kMaxPer][3];
+   C h[kMaxPer][3];
 #pragma unroll
    for (int u = 0; u < kMaxPer; ++u) {
       const int r = threadIdx.x + u * kFFTThreads;
@@ -232,8 +251,9 @@ __global__ void tensor_grid_kernel(double2* __restrict__ t, size_t np, int px, i
 }
 
 // the moments (mu_B) at every point of the G-box, zero at its empty cells
+template <typename C>
 __global__ void scatter_moments_kernel(int nc, const int* __restrict__ box_cell, int gx, int gy, int nbox,
-                                       const double* __restrict__ mag, double2* __restrict__ grid, int px, int py,
+                                       const double* __restrict__ mag, C* __restrict__ grid, int px, int py,
                                        size_t np) {
    const int b = blockIdx.x * blockDim.x + threadIdx.x;
    if (b >= nbox) return;
@@ -241,19 +261,26 @@ __global__ void scatter_moments_kernel(int nc, const int* __restrict__ box_cell,
    const int x = b % gx, y = (b / gx) % gy, z = b / (gx * gy);
    const size_t q = ((size_t)z * py + y) * px + x;
    const double imuB = 1.0 / 9.27400915e-24;
-   grid[q] = make_double2(c >= 0 ? mag[c] * imuB : 0.0, 0.0);
-   grid[np + q] = make_double2(c >= 0 ? mag[nc + c] * imuB : 0.0, 0.0);
-   grid[2 * np + q] = make_double2(c >= 0 ? mag[2 * nc + c] * imuB : 0.0, 0.0);
+   grid[q] = cval<C>(c >= 0 ? mag[c] * imuB : 0.0, 0.0);
+   grid[np + q] = cval<C>(c >= 0 ? mag[nc + c] * imuB : 0.0, 0.0);
+   grid[2 * np + q] = cval<C>(c >= 0 ? mag[2 * nc + c] * imuB : 0.0, 0.0);
 }
 
-__global__ void gather_field_kernel(int nc, const int* __restrict__ lin, const double2* __restrict__ grid, size_t np,
+template <typename C>
+__global__ void gather_field_kernel(int nc, const int* __restrict__ lin, const C* __restrict__ grid, size_t np,
                                     double scale, double* __restrict__ field) {
    const int c = blockIdx.x * blockDim.x + threadIdx.x;
    if (c >= nc) return;
    const int q = lin[c];
-   field[c] = q < 0 ? 0.0 : grid[q].x * scale;
-   field[nc + c] = q < 0 ? 0.0 : grid[np + q].x * scale;
-   field[2 * nc + c] = q < 0 ? 0.0 : grid[2 * np + q].x * scale;
+   field[c] = q < 0 ? 0.0 : (double)grid[q].x * scale;
+   field[nc + c] = q < 0 ? 0.0 : (double)grid[np + q].x * scale;
+   field[2 * nc + c] = q < 0 ? 0.0 : (double)grid[2 * np + q].x * scale;
+}
+
+// the FP64 spectra or twiddles rounded to FP32
+__global__ void round_complex_kernel(const double2* __restrict__ in, float2* __restrict__ out, size_t n) {
+   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+      out[q] = make_float2((float)in[q].x, (float)in[q].y);
 }
 
 int ilog2(int v) {
@@ -271,42 +298,43 @@ cudaError_t fft3d(FFTField* f, double2* data, int ncomp, cudaStream_t st) {
       const int nrows = py * pz;
       const int lines = std::max(1, std::min(kFFTTile / px, nrows));
       dim3 grid((unsigned)((nrows + lines - 1) / lines), (unsigned)ncomp);
-      fft_x_kernel<<<grid, kFFTThreads, 0, st>>>(data, f->np, px, f->logp[0], lines, f->tw[0], 0, nrows, py, py, px,
-                                                 px);
+      fft_x_kernel<double2><<<grid, kFFTThreads, 0, st>>>(data, f->np, px, f->logp[0], lines, f->tw[0], 0, nrows,
+                                                          py, py, px, px);
    }
    {  // y: stride px, W adjacent x columns, one block per (x chunk, z)
       const int W = std::max(1, std::min(kFFTTile / py, px));
       dim3 grid((unsigned)(px / W), (unsigned)pz, (unsigned)ncomp);
-      fft_strided_kernel<<<grid, kFFTThreads, 0, st>>>(data, f->np, py, f->logp[1], W, (size_t)px,
-                                                       (size_t)px * py, f->tw[1], 0, py, py);
+      fft_strided_kernel<double2><<<grid, kFFTThreads, 0, st>>>(data, f->np, py, f->logp[1], W, (size_t)px,
+                                                                (size_t)px * py, f->tw[1], 0, py, py);
    }
    {  // z: stride px*py, one block per (x chunk, y)
       const int W = std::max(1, std::min(kFFTTile / pz, px));
       dim3 grid((unsigned)(px / W), (unsigned)py, (unsigned)ncomp);
-      fft_strided_kernel<<<grid, kFFTThreads, 0, st>>>(data, f->np, pz, f->logp[2], W, (size_t)px * py, (size_t)px,
-                                                       f->tw[2], 0, pz, pz);
+      fft_strided_kernel<double2><<<grid, kFFTThreads, 0, st>>>(data, f->np, pz, f->logp[2], W, (size_t)px * py,
+                                                                (size_t)px, f->tw[2], 0, pz, pz);
    }
    return cudaGetLastError();
 }
 
 // the x and y passes of the moment transform (forward: x then y; inverse: y
 // then x), pruned to the G-box; the z passes run in fft_z_multiply_kernel
-cudaError_t fft_box(FFTField* f, bool inverse, cudaStream_t st, int* launches) {
+template <typename C>
+cudaError_t fft_box(FFTField* f, C* grid_data, C* const* tw, bool inverse, cudaStream_t st, int* launches) {
    const int px = f->p[0], py = f->p[1];
    const int gx = f->g[0], gy = f->g[1], gz = f->g[2];
    auto xpass = [&]() {
       const int nrows = gy * gz;
       const int lines = std::max(1, std::min(kFFTTile / px, nrows));
       dim3 grid((unsigned)((nrows + lines - 1) / lines), 3u);
-      fft_x_kernel<<<grid, kFFTThreads, 0, st>>>(f->grid, f->np, px, f->logp[0], lines, f->tw[0], inverse, nrows, gy,
-                                                 py, inverse ? px : gx, inverse ? gx : px);
+      fft_x_kernel<C><<<grid, kFFTThreads, 0, st>>>(grid_data, f->np, px, f->logp[0], lines, tw[0], inverse, nrows,
+                                                    gy, py, inverse ? px : gx, inverse ? gx : px);
    };
    auto ypass = [&]() {
       const int W = std::max(1, std::min(kFFTTile / py, px));
       dim3 grid((unsigned)(px / W), (unsigned)gz, 3u);
-      fft_strided_kernel<<<grid, kFFTThreads, 0, st>>>(f->grid, f->np, py, f->logp[1], W, (size_t)px,
-                                                       (size_t)px * py, f->tw[1], inverse, inverse ? py : gy,
-                                                       inverse ? gy : py);
+      fft_strided_kernel<C><<<grid, kFFTThreads, 0, st>>>(grid_data, f->np, py, f->logp[1], W, (size_t)px,
+                                                          (size_t)px * py, tw[1], inverse, inverse ? py : gy,
+                                                          inverse ? gy : py);
    };
    if (inverse) { ypass(); xpass(); }
    else { xpass(); ypass(); }
@@ -314,9 +342,31 @@ cudaError_t fft_box(FFTField* f, bool inverse, cudaStream_t st, int* launches) {
    return cudaGetLastError();
 }
 
+template <typename C>
+cudaError_t field_apply(FFTField* f, C* grid, const C* tspec, C* const* tw, const double* mag, double* field,
+                        cudaStream_t st, int* launches) {
+   cudaError_t e = cudaSuccess;
+   const int nc = f->nc;
+   const int nbox = f->g[0] * f->g[1] * f->g[2];
+   scatter_moments_kernel<C><<<(nbox + 255) / 256, 256, 0, st>>>(nc, f->box_cell, f->g[0], f->g[1], nbox, mag, grid,
+                                                                 f->p[0], f->p[1], f->np);
+   if ((e = fft_box<C>(f, grid, tw, false, st, launches)) != cudaSuccess) return e;
+   {
+      const int pz = f->p[2];
+      const int W = std::max(1, std::min(kFuseTile / (3 * pz), f->p[0]));
+      dim3 g((unsigned)(f->p[0] / W), (unsigned)f->p[1]);
+      fft_z_multiply_kernel<C><<<g, kFFTThreads, 0, st>>>(grid, tspec, f->np, f->p[0], f->p[1], pz, f->logp[2], W,
+                                                          f->g[2], tw[2]);
+   }
+   if ((e = fft_box<C>(f, grid, tw, true, st, launches)) != cudaSuccess) return e;
+   gather_field_kernel<C><<<(nc + 255) / 256, 256, 0, st>>>(nc, f->cell_lin, grid, f->np, 1.0 / (double)f->np, field);
+   if (launches) *launches += 3;
+   return cudaGetLastError();
+}
+
 }  // namespace
 
-FFTField* fft_field_create(int nc, const double* cpos, const int* natoms, double size, cudaStream_t st,
+FFTField* fft_field_create(int nc, const double* cpos, const int* natoms, double size, bool fp32, cudaStream_t st,
                            cudaError_t* err, std::string* why) {
    *err = cudaSuccess;
    int first = -1;
@@ -417,7 +467,31 @@ FFTField* fft_field_create(int nc, const double* cpos, const int* natoms, double
       e = cudaGetLastError();
    }
    if (e == cudaSuccess) e = fft3d(f, f->tspec, 6, st);
+   if (e == cudaSuccess && fp32) {
+      // FP32 transforms: the spectra and twiddles rounded once; the FP64
+      // moment grid is not needed
+      f->fp32 = true;
+      e = cudaMalloc(&f->tspec32, sizeof(float2) * 6 * np);
+      if (e == cudaSuccess) e = cudaMalloc(&f->grid32, sizeof(float2) * 3 * np);
+      if (e == cudaSuccess) {
+         round_complex_kernel<<<grid_blocks(6 * np), 256, 0, st>>>(f->tspec, f->tspec32, 6 * np);
+         e = cudaGetLastError();
+      }
+      for (int a = 0; a < 3 && e == cudaSuccess; ++a) {
+         e = cudaMalloc(&f->tw32[a], sizeof(float2) * (f->p[a] / 2));
+         if (e == cudaSuccess) {
+            round_complex_kernel<<<1, 256, 0, st>>>(f->tw[a], f->tw32[a], (size_t)(f->p[a] / 2));
+            e = cudaGetLastError();
+         }
+      }
+   }
    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host tables above leave scope
+   if (e == cudaSuccess && f->fp32) {
+      cudaFree(f->tspec);
+      cudaFree(f->grid);
+      f->tspec = nullptr;
+      f->grid = nullptr;
+   }
    if (e != cudaSuccess) {
       *err = e;
       fft_field_destroy(f);
@@ -427,23 +501,8 @@ FFTField* fft_field_create(int nc, const double* cpos, const int* natoms, double
 }
 
 cudaError_t fft_field_apply(FFTField* f, const double* mag, double* field, cudaStream_t st, int* launches) {
-   cudaError_t e = cudaSuccess;
-   const int nc = f->nc;
-   const int nbox = f->g[0] * f->g[1] * f->g[2];
-   scatter_moments_kernel<<<(nbox + 255) / 256, 256, 0, st>>>(nc, f->box_cell, f->g[0], f->g[1], nbox, mag, f->grid,
-                                                              f->p[0], f->p[1], f->np);
-   if ((e = fft_box(f, false, st, launches)) != cudaSuccess) return e;
-   {
-      const int pz = f->p[2];
-      const int W = std::max(1, std::min(kFuseTile / (3 * pz), f->p[0]));
-      dim3 grid((unsigned)(f->p[0] / W), (unsigned)f->p[1]);
-      fft_z_multiply_kernel<<<grid, kFFTThreads, 0, st>>>(f->grid, f->tspec, f->np, f->p[0], f->p[1], pz, f->logp[2],
-                                                          W, f->g[2], f->tw[2]);
-   }
-   if ((e = fft_box(f, true, st, launches)) != cudaSuccess) return e;
-   gather_field_kernel<<<(nc + 255) / 256, 256, 0, st>>>(nc, f->cell_lin, f->grid, f->np, 1.0 / (double)f->np, field);
-   if (launches) *launches += 3;
-   return cudaGetLastError();
+   if (f->fp32) return field_apply<float2>(f, f->grid32, f->tspec32, f->tw32, mag, field, st, launches);
+   return field_apply<double2>(f, f->grid, f->tspec, f->tw, mag, field, st, launches);
 }
 
 void fft_field_destroy(FFTField* f) {
@@ -452,7 +511,12 @@ void fft_field_destroy(FFTField* f) {
    cudaFree(f->grid);
    cudaFree(f->cell_lin);
    cudaFree(f->box_cell);
-   for (int a = 0; a < 3; ++a) cudaFree(f->tw[a]);
+   cudaFree(f->tspec32);
+   cudaFree(f->grid32);
+   for (int a = 0; a < 3; ++a) {
+      cudaFree(f->tw[a]);
+      cudaFree(f->tw32[a]);
+   }
    delete f;
 }
 

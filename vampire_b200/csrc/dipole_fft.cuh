@@ -12,8 +12,9 @@ struct FFTField;
 // regular grid of pitch `size` (to 1e-9 of the pitch) and the padded grid is
 // small enough; otherwise returns nullptr with the reason in *why (and
 // *err == cudaSuccess).  cpos holds x, y, z, w per cell (Angstrom); cells with
-// natoms <= 0 are empty.  Work is queued on `st`.
-FFTField* fft_field_create(int nc, const double* cpos, const int* natoms, double size, cudaStream_t st,
+// natoms <= 0 are empty.  fp32: the transforms of every update in FP32 (the
+// spectra computed in FP64 and rounded), else FP64.  Work is queued on `st`.
+FFTField* fft_field_create(int nc, const double* cpos, const int* natoms, double size, bool fp32, cudaStream_t st,
                            cudaError_t* err, std::string* why);
 
 // field[q * nc + c] = sum over occupied j != c of the bare point-dipole
