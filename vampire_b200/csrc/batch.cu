@@ -25,9 +25,10 @@
 // ordinary two step passes per step over all atoms (vgpu_llg_heun) and the
 // same per-system records between chunks.  No system is tied to one cluster,
 // so the largest particle no longer sets the step time: on 256 particles of
-// 150-10,000 spins (380,178 in all) 0.025 ms per step against 0.045 ms for
-// the best persistent shape (cluster 8, blocks of 128).  The passes take the
-// step number as a kernel argument, so this shape is not captured in a graph.
+// 150-10,000 spins (380,178 in all) 0.021 ms per step (the passes launched
+// with programmatic serialisation) against 0.045 ms for the best persistent
+// shape (cluster 8, blocks of 128).  The passes take the step number as a
+// kernel argument, so this shape is not captured in a graph.
 // Same physics and numbers as the persistent kernel (tests/test_batch_gpu.py).
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
