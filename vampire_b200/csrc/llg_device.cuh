@@ -34,14 +34,13 @@ __device__ __forceinline__ void thermal_xi(const LLGArgs<R>& a, int i, R& gx, R&
    u32x4 c = {li, (uint32_t)a.step, (uint32_t)(a.step >> 32), RNG_THERMAL};
    u32x4 r = philox4x32_10(c, klo, khi);
    if (sizeof(R) == 4) {
-      float s1, c1, s2, c2;
-      const float r1 = sqrtf(-2.0f * logf(u01f(r.x)));
-      const float r2 = sqrtf(-2.0f * logf(u01f(r.z)));
-      sincospif(2.0f * u01f(r.y), &s1, &c1);
-      sincospif(2.0f * u01f(r.w), &s2, &c2);
+      // fast approximations: each Gaussian within 1e-5 of the exact transform
+      float s1, c1;
+      const float r1 = bm_radius_fast(r.x);
+      bm_angle_fast(r.y, c1, s1);
       gx = (R)(r1 * c1);
       gy = (R)(r1 * s1);
-      gz = (R)(r2 * c2);
+      gz = (R)(bm_radius_fast(r.z) * bm_cos_fast(r.w));
    } else {
       double s1, c1, s2, c2;
       const double r1 = sqrt(-2.0 * log(u01d(r.x)));

@@ -143,12 +143,11 @@ __global__ void __launch_bounds__(256, VGPU_MC_MIN_BLOCKS) mc_colour_kernel(cons
          const u32x4 c = {gi, (uint32_t)p.sweep, (uint32_t)(p.sweep >> 32), RNG_MC_MOVE};
          const u32x4 r = philox4x32_10(c, a.seed_lo, a.seed_hi);
          if (sizeof(R) == 4) {
-            float s1, c1, s2, c2f;
-            const float r1 = sqrtf(-2.0f * logf(u01f(r.x)));
-            const float rr = sqrtf(-2.0f * logf(u01f(r.z)));
-            sincospif(2.0f * u01f(r.y), &s1, &c1);
-            sincospif(2.0f * u01f(r.w), &s2, &c2f);
-            g0 = r1 * c1; g1 = r1 * s1; g2 = rr * c2f;
+            // Box-Muller on the fast approximations (each Gaussian within 1e-5)
+            float s1, c1;
+            const float r1 = bm_radius_fast(r.x);
+            bm_angle_fast(r.y, c1, s1);
+            g0 = r1 * c1; g1 = r1 * s1; g2 = bm_radius_fast(r.z) * bm_cos_fast(r.w);
             // u01f keeps the top 24 bits: the low bytes of r.y, r.z, r.w
             u = (R)u01f(((r.y & 0xffu) << 8) | ((r.z & 0xffu) << 16) | (r.w << 24));
          } else {
