@@ -53,6 +53,29 @@ __device__ __forceinline__ void thermal_xi(const LLGArgs<R>& a, int i, R& gx, R&
    }
 }
 
+// One bond of the diagonal-plus-DMI exchange: h += J s_j + d x s_j, with J
+// the diagonal (jx, jy, jz) and d the antisymmetric part.  FP32: three fused
+// multiply-adds per component chained through the field (one instruction per
+// component fewer than the products summed first); FP64: the products summed
+// first, then added.  Every FP32 record layout uses this one form, so their
+// fields stay identical.
+template <typename R>
+__device__ __forceinline__ void dmi_bond(R jx, R jy, R jz, R dx, R dy, R dz, R x, R y, R z, R& hx, R& hy, R& hz);
+template <>
+__device__ __forceinline__ void dmi_bond<float>(float jx, float jy, float jz, float dx, float dy, float dz, float x,
+                                                float y, float z, float& hx, float& hy, float& hz) {
+   hx = fmaf(-dz, y, fmaf(dy, z, fmaf(jx, x, hx)));
+   hy = fmaf(-dx, z, fmaf(dz, x, fmaf(jy, y, hy)));
+   hz = fmaf(-dy, x, fmaf(dx, y, fmaf(jz, z, hz)));
+}
+template <>
+__device__ __forceinline__ void dmi_bond<double>(double jx, double jy, double jz, double dx, double dy, double dz,
+                                                 double x, double y, double z, double& hx, double& hy, double& hz) {
+   hx += jx * x + (dy * z - dz * y);
+   hy += jy * y + (dz * x - dx * z);
+   hz += jz * z + (dx * y - dy * x);
+}
+
 // exchange gather of atom i over its SELL row, sources (sx,sy,sz)
 template <typename R> __device__ __forceinline__ R ld_src(const R* p, int coherent) {
    return coherent ? __ldcg(p) : __ldg(p);
@@ -91,9 +114,7 @@ __device__ __forceinline__ void exchange_gather_row(const LLGArgs<R>& a, int bas
          const R* t = tab + 3 * (mi * a.M + mj);
          const R dx = __ldg(a.jb[0] + e), dy = __ldg(a.jb[1] + e), dz = __ldg(a.jb[2] + e);
          // diag part plus the antisymmetric part written as d x s_j
-         hx += __ldg(t) * x + (dy * z - dz * y);
-         hy += __ldg(t + 1) * y + (dz * x - dx * z);
-         hz += __ldg(t + 2) * z + (dx * y - dy * x);
+         dmi_bond<R>(__ldg(t), __ldg(t + 1), __ldg(t + 2), dx, dy, dz, x, y, z, hx, hy, hz);
       } else {  // FMT_TENSOR_BOND
          const R t0 = __ldg(a.jb[0] + e), t1 = __ldg(a.jb[1] + e), t2 = __ldg(a.jb[2] + e);
          const R t3 = __ldg(a.jb[3] + e), t4 = __ldg(a.jb[4] + e), t5 = __ldg(a.jb[5] + e);
@@ -148,14 +169,10 @@ __device__ __forceinline__ void exchange_gather_w(const LLGArgs<R>& a, int base,
                  dz = __int_as_float(sw[128 * k + 3]);
          if (a.tab_scalar) {
             const R J = __ldg(a.jtab_s + mi * a.M + mj);
-            hx += J * x[k] + (dy * z[k] - dz * y[k]);
-            hy += J * y[k] + (dz * x[k] - dx * z[k]);
-            hz += J * z[k] + (dx * y[k] - dy * x[k]);
+            dmi_bond<R>(J, J, J, dx, dy, dz, x[k], y[k], z[k], hx, hy, hz);
          } else {
             const R* t = tab + 3 * (mi * a.M + mj);
-            hx += __ldg(t) * x[k] + (dy * z[k] - dz * y[k]);
-            hy += __ldg(t + 1) * y[k] + (dz * x[k] - dx * z[k]);
-            hz += __ldg(t + 2) * z[k] + (dx * y[k] - dy * x[k]);
+            dmi_bond<R>(__ldg(t), __ldg(t + 1), __ldg(t + 2), dx, dy, dz, x[k], y[k], z[k], hx, hy, hz);
          }
       }
    } else if (FMT == FMT_DMI_TAB) {
@@ -175,14 +192,10 @@ __device__ __forceinline__ void exchange_gather_w(const LLGArgs<R>& a, int base,
          if (a.tab_scalar) {
             // isotropic diagonal: one coupling per material pair (scalar table)
             const R J = __ldg(a.jtab_s + mi * a.M + mj);
-            hx += J * x[k] + (dy * z[k] - dz * y[k]);
-            hy += J * y[k] + (dz * x[k] - dx * z[k]);
-            hz += J * z[k] + (dx * y[k] - dy * x[k]);
+            dmi_bond<R>(J, J, J, dx, dy, dz, x[k], y[k], z[k], hx, hy, hz);
          } else {
             const R* t = tab + 3 * (mi * a.M + mj);
-            hx += __ldg(t) * x[k] + (dy * z[k] - dz * y[k]);
-            hy += __ldg(t + 1) * y[k] + (dz * x[k] - dx * z[k]);
-            hz += __ldg(t + 2) * z[k] + (dx * y[k] - dy * x[k]);
+            dmi_bond<R>(__ldg(t), __ldg(t + 1), __ldg(t + 2), dx, dy, dz, x[k], y[k], z[k], hx, hy, hz);
          }
       }
    } else {  // FMT_ISO_TAB
@@ -231,14 +244,10 @@ __device__ __forceinline__ void exchange_gather_c(const LLGArgs<R>& a, int base,
       const R dx = e.y, dy = e.z, dz = e.w;
       if (a.tab_scalar) {
          const R J = e.x;
-         hx += J * x[k] + (dy * z[k] - dz * y[k]);
-         hy += J * y[k] + (dz * x[k] - dx * z[k]);
-         hz += J * z[k] + (dx * y[k] - dy * x[k]);
+         dmi_bond<R>(J, J, J, dx, dy, dz, x[k], y[k], z[k], hx, hy, hz);
       } else {
          const float4 e2 = dict[a.cdict_n + q];
-         hx += (R)e.x * x[k] + (dy * z[k] - dz * y[k]);
-         hy += (R)e2.x * y[k] + (dz * x[k] - dx * z[k]);
-         hz += (R)e2.y * z[k] + (dx * y[k] - dy * x[k]);
+         dmi_bond<R>((R)e.x, (R)e2.x, (R)e2.y, dx, dy, dz, x[k], y[k], z[k], hx, hy, hz);
       }
    }
 }
@@ -260,14 +269,10 @@ __device__ __forceinline__ void exchange_gather_win(const LLGArgs<R>& a, int w_r
       const R dx = e.y, dy = e.z, dz = e.w;
       if (a.tab_scalar) {
          const R J = e.x;
-         hx += J * x + (dy * z - dz * y);
-         hy += J * y + (dz * x - dx * z);
-         hz += J * z + (dx * y - dy * x);
+         dmi_bond<R>(J, J, J, dx, dy, dz, x, y, z, hx, hy, hz);
       } else {
          const float4 e2 = dict[a.cdict_n + (c >> 16)];
-         hx += (R)e.x * x + (dy * z - dz * y);
-         hy += (R)e2.x * y + (dz * x - dx * z);
-         hz += (R)e2.y * z + (dx * y - dy * x);
+         dmi_bond<R>((R)e.x, (R)e2.x, (R)e2.y, dx, dy, dz, x, y, z, hx, hy, hz);
       }
    };
    if (W > 0) {
