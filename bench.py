@@ -194,12 +194,14 @@ def byte_model(z=12, b_J=12, multi_mat=True, dipole=False, noise_store=True):
     0 with compact records, whose coupling comes from a dictionary of a few
     hundred bytes), the material id and (with the dipole field) the cell id;
     neighbour spins are L2-served.  The thermal Gaussians are generated
-    in-register by the predictor, which stores them (12 B) for the corrector
-    to read back (12 B) when noise_store; otherwise both passes regenerate
-    them (0 B)."""
+    in-register by the predictor; when noise_store it stores the step's
+    external field (12 B) for the corrector to read back (12 B) in place of
+    the cell id and the field's recomputation; otherwise both passes
+    regenerate the noise (0 B)."""
     gather = 4 * (z + 1) + b_J * z + 4 * int(multi_mat) + 4 * int(dipole)
     g = 12 * int(noise_store)
-    return {"predictor": 24 + gather + g, "corrector": 36 + gather + g}
+    cell_c = 4 * int(dipole) * int(noise_store)  # the corrector reads no cell id
+    return {"predictor": 24 + gather + g, "corrector": 36 + gather + g - cell_c}
 
 
 def bench_batched(device, steps=2000, plain_steps=200):

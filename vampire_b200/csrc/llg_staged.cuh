@@ -124,15 +124,17 @@ __device__ __forceinline__ LLGArgs<float> fold_features(const LLGArgs<float>& in
 // resident blocks hide the copy) or 2 (persistent, next tile's copy in flight
 // while this one is computed).  Each buffer holds the tile's bond records
 // (buf_bytes) and its own-atom arrays (kStageOwnArrays x 32 SL words: s0 x|y|z,
-// s' x|y|z for the corrector, material ids, cell ids, and for the corrector
-// the step's thermal Gaussians that the predictor stored), all brought by bulk
+// s' x|y|z for the corrector, material ids, cell ids (predictor), and for the
+// corrector the step's external field that the predictor stored), all brought by bulk
 // copies completing on the buffer's barrier; after the buffers come the
 // coupling dictionary (compact records, copied with the block's first tile)
 // and the material table (read into shared memory once per block when it has
 // at most kStageMaxMat rows).  The predictor generates the Philox Gaussians of
 // the tile's atoms while the copy is in flight (they need no data) and stores
-// them (a.gx); the corrector, which needs the same numbers, copies them in
-// with the tile instead of generating them again.
+// the atoms' external field of the step (thermal, applied and macrocell
+// dipole; a.gx); the corrector, which needs the same field (nothing it depends
+// on changes between the two passes of a step), copies it in with the tile
+// instead of computing it again.
 // Registers are capped for 768 resident threads per SM (85 a thread): the
 // compact-record corrector otherwise takes 92 and fits 5 blocks of 128
 // (measured 12 % slower); a cap at 64 spills and was slower again.
@@ -168,8 +170,9 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
       const void* src = CREC ? (const void*)(a.crec + o0) : (const void*)(a.rec + o0);
       const uint32_t db = first ? dict_bytes : 0u;
       const uint32_t nb = 128u * (uint32_t)(s1 - s0);  // own-array bytes: 32 atoms x 4 B per slice
-      const bool gin = MODE == PASS_CORRECTOR && a.gx;
-      const int na = 3 + (MODE == PASS_CORRECTOR ? 3 : 0) + (a.mat ? 1 : 0) + (a.cell ? 1 : 0) + (gin ? 3 : 0);
+      // the corrector with the predictor's stored field needs no cell ids
+      const bool gin = MODE == PASS_CORRECTOR && a.gx, cin = a.cell && !gin;
+      const int na = 3 + (MODE == PASS_CORRECTOR ? 3 : 0) + (a.mat ? 1 : 0) + (cin ? 1 : 0) + (gin ? 3 : 0);
       unsigned char* buf = stage_smem + b * stride;
       float* own = reinterpret_cast<float*>(buf + buf_bytes);
       const size_t a0 = (size_t)s0 * 32;
@@ -186,7 +189,7 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
          bulk_copy_g2s(own + 5 * TS, a.bz + a0, nb, &mbar[b]);
       }
       if (a.mat) bulk_copy_g2s(own + 6 * TS, a.mat + a0, nb, &mbar[b]);
-      if (a.cell) bulk_copy_g2s(own + 7 * TS, a.cell + a0, nb, &mbar[b]);
+      if (cin) bulk_copy_g2s(own + 7 * TS, a.cell + a0, nb, &mbar[b]);
       if (gin) {
          bulk_copy_g2s(own + 8 * TS, a.gx + a0, nb, &mbar[b]);
          bulk_copy_g2s(own + 9 * TS, a.gy + a0, nb, &mbar[b]);
@@ -216,13 +219,10 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
       if (tid == 0 && NBUF == 2 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x, b ^ 1, false);
       const int i = (a.slice_first + t * SL) * 32 + tid;
       const bool act = i < a.n_upd;
-      // the tile's Gaussians (the Philox noise needs no data) while the copy lands;
-      // the predictor keeps them for the corrector
+      // the tile's Gaussians (the Philox noise needs no data) while the copy
+      // lands; a corrector with the predictor's stored field needs none
       float g[3] = {0.f, 0.f, 0.f};
-      if (a.thermal && (MODE == PASS_PREDICTOR || !a.gx)) {
-         thermal_xi(a, act ? i : 0, g[0], g[1], g[2]);
-         if (MODE == PASS_PREDICTOR && a.gx && act) { a.gx[i] = g[0]; a.gy[i] = g[1]; a.gz[i] = g[2]; }
-      }
+      if (a.thermal && (MODE == PASS_PREDICTOR || !a.gx)) thermal_xi(a, act ? i : 0, g[0], g[1], g[2]);
       const int tile_off = __ldg(a.slice_off + a.slice_first + t * SL);
       const bool done = mbar_wait_bounded(&mbar[b], (phase >> b) & 1u);
       if (__syncthreads_or(!done)) {  // every thread takes the same branch
@@ -232,15 +232,17 @@ __global__ void __launch_bounds__(32 * SL, 24 / SL) llg_staged_kernel(const LLGA
       phase ^= 1u << b;
       const unsigned char* buf = stage_smem + b * stride;
       const float* own = reinterpret_cast<const float*>(buf + buf_bytes);
-      if (MODE == PASS_CORRECTOR && a.thermal && a.gx) {
-         g[0] = own[8 * TS + tid]; g[1] = own[9 * TS + tid]; g[2] = own[10 * TS + tid];
-      }
       if (act) {
          const int mi = a.mat ? reinterpret_cast<const int*>(own)[6 * TS + tid] : 0;
          const MatParams<float> m = mpt[mi];
          const float S0[3] = {own[tid], own[TS + tid], own[2 * TS + tid]};
          float E[3];
-         external_field_g<float>(a, i, m, g, a.cell ? reinterpret_cast<const int*>(own)[7 * TS + tid] : -1, E);
+         if (MODE == PASS_CORRECTOR && a.gx) {  // the predictor's field of this step
+            E[0] = own[8 * TS + tid]; E[1] = own[9 * TS + tid]; E[2] = own[10 * TS + tid];
+         } else {
+            external_field_g<float>(a, i, m, g, a.cell ? reinterpret_cast<const int*>(own)[7 * TS + tid] : -1, E);
+            if (MODE == PASS_PREDICTOR && a.gx) { a.gx[i] = E[0]; a.gy[i] = E[1]; a.gz[i] = E[2]; }
+         }
          const int4* sb = reinterpret_cast<const int4*>(buf);
          float H[3];
          if (MODE == PASS_PREDICTOR) {
@@ -302,8 +304,8 @@ __global__ void __launch_bounds__(128, 6) llg_warp_kernel(const LLGArgs<float> a
       const int s0 = a.slice_first + tt;
       const int o0 = __ldg(a.slice_off + s0), o1 = __ldg(a.slice_off + s0 + 1);
       const uint32_t bytes = (uint32_t)(o1 - o0) * 4u;
-      const bool gin = MODE == PASS_CORRECTOR && a.gx;
-      const int na = 3 + (MODE == PASS_CORRECTOR ? 3 : 0) + (a.mat ? 1 : 0) + (a.cell ? 1 : 0) + (gin ? 3 : 0);
+      const bool gin = MODE == PASS_CORRECTOR && a.gx, cin = a.cell && !gin;
+      const int na = 3 + (MODE == PASS_CORRECTOR ? 3 : 0) + (a.mat ? 1 : 0) + (cin ? 1 : 0) + (gin ? 3 : 0);
       unsigned char* buf = wbuf + b * stride;
       float* own = reinterpret_cast<float*>(buf + buf_bytes);
       const size_t a0 = (size_t)s0 * 32;
@@ -319,7 +321,7 @@ __global__ void __launch_bounds__(128, 6) llg_warp_kernel(const LLGArgs<float> a
          bulk_copy_g2s(own + 160, a.bz + a0, 128, &mb[b]);
       }
       if (a.mat) bulk_copy_g2s(own + 192, a.mat + a0, 128, &mb[b]);
-      if (a.cell) bulk_copy_g2s(own + 224, a.cell + a0, 128, &mb[b]);
+      if (cin) bulk_copy_g2s(own + 224, a.cell + a0, 128, &mb[b]);
       if (gin) {
          bulk_copy_g2s(own + 256, a.gx + a0, 128, &mb[b]);
          bulk_copy_g2s(own + 288, a.gy + a0, 128, &mb[b]);
@@ -354,10 +356,7 @@ __global__ void __launch_bounds__(128, 6) llg_warp_kernel(const LLGArgs<float> a
       const int i = (a.slice_first + t) * 32 + lane;
       const bool act = i < a.n_upd;
       float g[3] = {0.f, 0.f, 0.f};
-      if (a.thermal && (MODE == PASS_PREDICTOR || !a.gx)) {
-         thermal_xi(a, act ? i : 0, g[0], g[1], g[2]);
-         if (MODE == PASS_PREDICTOR && a.gx && act) { a.gx[i] = g[0]; a.gy[i] = g[1]; a.gz[i] = g[2]; }
-      }
+      if (a.thermal && (MODE == PASS_PREDICTOR || !a.gx)) thermal_xi(a, act ? i : 0, g[0], g[1], g[2]);
       const int tile_off = __ldg(a.slice_off + a.slice_first + t);
       const bool done = mbar_wait_bounded(&mb[b], (phase >> b) & 1u);
       if (__any_sync(0xffffffffu, !done)) {  // every lane takes the same branch
@@ -367,15 +366,17 @@ __global__ void __launch_bounds__(128, 6) llg_warp_kernel(const LLGArgs<float> a
       phase ^= 1u << b;
       const unsigned char* buf = wbuf + b * stride;
       const float* own = reinterpret_cast<const float*>(buf + buf_bytes);
-      if (MODE == PASS_CORRECTOR && a.thermal && a.gx) {
-         g[0] = own[256 + lane]; g[1] = own[288 + lane]; g[2] = own[320 + lane];
-      }
       if (act) {
          const int mi = a.mat ? reinterpret_cast<const int*>(own)[192 + lane] : 0;
          const MatParams<float> m = mpt[mi];
          const float S0[3] = {own[lane], own[32 + lane], own[64 + lane]};
          float E[3];
-         external_field_g<float>(a, i, m, g, a.cell ? reinterpret_cast<const int*>(own)[224 + lane] : -1, E);
+         if (MODE == PASS_CORRECTOR && a.gx) {  // the predictor's field of this step
+            E[0] = own[256 + lane]; E[1] = own[288 + lane]; E[2] = own[320 + lane];
+         } else {
+            external_field_g<float>(a, i, m, g, a.cell ? reinterpret_cast<const int*>(own)[224 + lane] : -1, E);
+            if (MODE == PASS_PREDICTOR && a.gx) { a.gx[i] = E[0]; a.gy[i] = E[1]; a.gz[i] = E[2]; }
+         }
          const int4* sb = reinterpret_cast<const int4*>(buf);
          float H[3];
          if (MODE == PASS_PREDICTOR) {

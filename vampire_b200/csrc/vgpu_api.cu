@@ -586,11 +586,11 @@ static int prepare_passes(vgpu_ctx* h, bool* staged_out, int integrator = INTEG_
       h->sys.stage = c;
    }
    if (staged && !h->sys.stage.win && !h->sys.g_store[0]) {
-      // the step's Gaussians, passed from the predictor to the corrector
+      // the step's external field, passed from the predictor to the corrector
       const size_t len = ((size_t)h->sys.n_alloc + 3) & ~(size_t)3;
       for (int q = 0; q < 3; ++q) {
          h->sys.g_store[q] = h->alloc(len * sizeof(R));
-         if (!h->sys.g_store[q]) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for the noise buffers");
+         if (!h->sys.g_store[q]) return set_err(h, VGPU_ERR_OOM, "cudaMalloc failed for the external-field buffers");
       }
    }
    *staged_out = staged;

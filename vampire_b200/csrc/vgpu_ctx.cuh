@@ -49,7 +49,7 @@ struct SysDev {
    void* f[3] = {nullptr};   // field output
    void* e[3] = {nullptr};   // stored predictor increment in use (VGPU_OPT_STORE_INCREMENT)
    void* e_store[3] = {nullptr};  // its buffers, once allocated
-   void* g_store[3] = {nullptr};  // staged passes: the step's thermal Gaussians (predictor -> corrector)
+   void* g_store[3] = {nullptr};  // staged passes: the step's external field (predictor -> corrector)
    void* xi = nullptr;       // replay noise
    double* stage64 = nullptr;  // [3n] FP64 staging of host transfers (FP32 state)
    int* status = nullptr;

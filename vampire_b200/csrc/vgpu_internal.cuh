@@ -109,8 +109,9 @@ struct LLGArgs {
    R* bx; R* by; R* bz;      // state B: s' (predictor output)
    R* fx; R* fy; R* fz;      // field output (field-only mode)
    R* ex; R* ey; R* ez;      // stored predictor increment f(s0), or nullptr (recovered)
-   R* gx; R* gy; R* gz;      // staged passes: the step's thermal Gaussians, written by the
-                             // predictor and read back by the corrector, or nullptr
+   R* gx; R* gy; R* gz;      // staged passes: the step's external field (thermal, applied,
+                             // macrocell dipole), written by the predictor and read back by
+                             // the corrector, or nullptr
    int* status;              // device status word (non-finite spin flag)
    int stage_extra_tx;       // staged passes: extra bytes each tile expects (0; > 0 tests the bounded wait)
 };
