@@ -305,7 +305,11 @@ int vgpu_llg_heun(vgpu_handle h, uint64_t n_steps);
 
 /* One fused pass: VGPU_PASS_PREDICTOR (s' from s) or VGPU_PASS_CORRECTOR (s
  * from s and s'; completes the step: counter and dipole cadence).
- * vgpu_llg_heun(h, 1) is the predictor followed by the corrector. */
+ * vgpu_llg_heun(h, 1) is the predictor followed by the corrector.  The
+ * external field (thermal, applied, macrocell dipole) belongs to the step, as
+ * in the reference, which computes it once per step: with the record-staged
+ * passes the corrector uses the field the predictor computed, so parameters
+ * changed between the two passes of a step take effect at the next step. */
 #define VGPU_PASS_PREDICTOR 0
 #define VGPU_PASS_CORRECTOR 1
 int vgpu_llg_pass(vgpu_handle h, int pass);
