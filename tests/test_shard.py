@@ -1,7 +1,7 @@
 """Spatial sharding host logic (vampire_b200/shard.py) on CPU.
 
 The plan and local systems are checked structurally; the halo exchange runs
-as world_size-2 and -3 gloo process groups whose ranks step their shard with
+as world_size-2, -3 and -4 gloo process groups whose ranks step their shard with
 the FP64 oracle (predictor half, halo refresh of s', corrector half, halo
 refresh of s) and must reproduce the whole-system oracle bit for bit -- the
 same field sums in the same bond order, with the reference's replayed noise.
@@ -197,7 +197,7 @@ def test_split_ranges_core_needs_no_halo():
             assert bnd[-1][1] == plan.n_owned
 
 
-@pytest.mark.parametrize("maker_name,world", [("fcc_big", 2), ("fcc_big", 3)])
+@pytest.mark.parametrize("maker_name,world", [("fcc_big", 2), ("fcc_big", 3), ("fcc_big", 4)])
 def test_gloo_overlapped_shards_equal_whole_system(tmp_path, maker_name, world):
     """The overlapped schedule (core range during the exchange) reproduces
     the whole-system oracle bit for bit over 4 stochastic steps."""
@@ -302,7 +302,7 @@ def _mc_numbers(n, sweeps, seed):
     return np.concatenate([g, u], axis=1)
 
 
-@pytest.mark.parametrize("maker_name,world", [("fcc", 2), ("sc", 3)])
+@pytest.mark.parametrize("maker_name,world", [("fcc", 2), ("sc", 3), ("fcc", 4)])
 def test_gloo_sharded_monte_carlo_equals_whole_system(tmp_path, maker_name, world):
     """Colour-ordered Metropolis sweeps on shards (owned atoms of one colour,
     then a halo refresh, for every colour) reproduce the whole system's
@@ -372,7 +372,7 @@ def _dipole_rank_main(rank, world, port, out_dir):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("world", [2, 3, 4])
 def test_gloo_sharded_cell_moments_equal_whole_system(tmp_path, world):
     """Macrocell moments on shards: every rank sums its owned atoms, one
     all-reduce adds the partial moments (cells::mag's MPI_Allreduce), and
