@@ -79,7 +79,8 @@ class Batch:
                 bs[k].H_start[c] = p["H_start"][c]
                 bs[k].H_end[c] = p["H_end"][c]
             bs[k].n_ramp = int(p.get("n_ramp", 0))
-        cp = V.params_struct(common or self.systems[0].params)
+        # an empty batch reaches the library, which refuses it (VGPU_ERR_ARG)
+        cp = V.params_struct(common or (self.systems[0].params if self.systems else S.SimParams()))
         self._h = C.c_void_p()
         prec = V.PREC_FP64 if precision == "fp64" else V.PREC_FP32
         V.check(V.lib().vgpu_batch_create(device, prec, C.c_int32(self.n_sys), descs, bs, C.byref(cp),
