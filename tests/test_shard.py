@@ -184,7 +184,7 @@ def test_split_ranges_core_needs_no_halo():
     atoms; core and boundary cuts fall on slice (32-atom) boundaries; the last
     range ends at the owned count."""
     s = _fcc(L=12)
-    for world in (2, 3):
+    for world in (2, 3, 4):
         for plan in SH.make_plan(s, world):
             loc = SH.local_system(s, plan)
             (c0, c1), bnd = SH.split_ranges(loc, plan.n_owned)
